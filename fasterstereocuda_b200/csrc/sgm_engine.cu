@@ -1,0 +1,909 @@
+// Host side of the SGM engine: device buffers, the launch sequence of one matching level,
+// the on-device pyramid driver and the C ABI declared in include/sgm_b200.h.
+//
+// Reference orchestration being replaced: StereoCudaImpl::Init/Match/Release
+// (SgmStereoCuda/StereoCudaImpl.cpp:128-546) and HierSgmCudaImpl (FasterStereoCuda/
+// FasterStereoCuda.cpp:201-635). Differences by design: all allocation happens in init;
+// a match is one stream of kernels with no host synchronisation inside it; small-region
+// removal runs on the GPU; the pyramid keeps every level on the device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/sgm_b200.h"
+#include "sgm_kernels.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+void set_error(std::string* dst, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  if (dst) *dst = buf;
+}
+
+int default_peaks_strips() {
+  const unsigned hc = std::thread::hardware_concurrency();
+  const int n = (int)(hc * 3 / 4);
+  return n > 0 ? n : 1;
+}
+
+sgm_ext_options_t default_ext() {
+  sgm_ext_options_t e;
+  e.tie_rule = sgm::kTieLowest;
+  e.init_tie_rule = sgm::kTieLowest;
+  e.peaks_strips = 0;
+  e.peaks_abs_mode = sgm::kPeaksAbsInt;
+  e.p2_div0 = -1;
+  return e;
+}
+
+// Optional per-launch timing with CUDA events recorded on the launching stream
+// (process-wide; enable from one thread while no match is in flight).
+struct Profiler {
+  bool on = false;
+  struct Rec { const char* name; cudaEvent_t a, b; };
+  std::vector<Rec> pending;
+  std::vector<cudaEvent_t> pool;
+  struct Stat { std::string name; int64_t launches = 0; double ms = 0.0; };
+  std::vector<Stat> stats;
+  cudaEvent_t take() {
+    if (pool.empty()) {
+      cudaEvent_t ev;
+      cudaEventCreate(&ev);
+      return ev;
+    }
+    cudaEvent_t ev = pool.back();
+    pool.pop_back();
+    return ev;
+  }
+  void collect() {
+    for (auto& r : pending) {
+      float ms = 0.f;
+      cudaEventSynchronize(r.b);
+      cudaEventElapsedTime(&ms, r.a, r.b);
+      Stat* st = nullptr;
+      for (auto& x : stats)
+        if (x.name == r.name) st = &x;
+      if (!st) {
+        stats.push_back(Stat{r.name, 0, 0.0});
+        st = &stats.back();
+      }
+      st->launches++;
+      st->ms += ms;
+      pool.push_back(r.a);
+      pool.push_back(r.b);
+    }
+    pending.clear();
+  }
+};
+Profiler g_prof;
+std::mutex g_prof_mu;
+thread_local cudaEvent_t t_prof_start = nullptr;
+thread_local cudaStream_t t_prof_stream = nullptr;
+
+void prof_start(cudaStream_t s) {
+  if (!g_prof.on) return;
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  t_prof_start = g_prof.take();
+  t_prof_stream = s;
+  cudaEventRecord(t_prof_start, s);
+}
+
+void prof_end(const char* name) {
+  if (!g_prof.on || !t_prof_start) return;
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  cudaEvent_t b = g_prof.take();
+  cudaEventRecord(b, t_prof_stream);
+  g_prof.pending.push_back(Profiler::Rec{name, t_prof_start, b});
+  t_prof_start = nullptr;
+  if (g_prof.pending.size() > 4096) g_prof.collect();
+}
+
+template <typename T>
+cudaError_t dalloc(T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) return cudaSuccess;
+  return cudaMalloc(reinterpret_cast<void**>(p), count * sizeof(T));
+}
+
+template <typename T>
+void dfree(T*& p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+}  // namespace
+
+// One matching level (the state of one StereoCuda instance).
+struct sgm_engine {
+  bool ready = false;
+  int dev = 0;
+  int W = 0, H = 0, M = 0, D = 0;
+  sgm_option_t opt{};
+  sgm_ext_options_t ext = default_ext();
+  bool print_log = false;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  int64_t launches = 0;
+  // device buffers
+  uint8_t* img[2] = {nullptr, nullptr};
+  void* cs[2] = {nullptr, nullptr};
+  uint8_t *cost = nullptr, *lr = nullptr, *rl = nullptr, *bt = nullptr;
+  float* wta = nullptr;     // [2][H][W]
+  float* post = nullptr;    // LR/median output
+  float* post2 = nullptr;   // dilation output
+  float* dr_out = nullptr;  // right map after the LR marks
+  float* out = nullptr;     // final left map for the host path
+  int16_t* init[2] = {nullptr, nullptr};
+  int16_t* init_tmp = nullptr;
+  unsigned* key = nullptr;
+  int* label = nullptr;
+  int* count = nullptr;
+
+  int nviews() const { return opt.do_lr_check ? 2 : 1; }
+  size_t npix() const { return (size_t)W * H; }
+  size_t vol() const { return (size_t)W * H * D; }
+  int census_bytes() const { return opt.cs_type == 1 ? 8 : 4; }
+
+  void free_all() {
+    for (int i = 0; i < 2; ++i) {
+      dfree(img[i]);
+      dfree(init[i]);
+      if (cs[i]) cudaFree(cs[i]);
+      cs[i] = nullptr;
+    }
+    dfree(cost); dfree(lr); dfree(rl); dfree(bt);
+    dfree(wta); dfree(post); dfree(post2); dfree(dr_out); dfree(out);
+    dfree(init_tmp); dfree(key); dfree(label); dfree(count);
+    if (stream) cudaStreamDestroy(stream);
+    stream = nullptr;
+    ready = false;
+  }
+};
+
+namespace {
+
+#define SGM_CUDA_TRY(e, expr)                                                          \
+  do {                                                                                 \
+    cudaError_t _st = (expr);                                                          \
+    if (_st != cudaSuccess) {                                                          \
+      set_error(&(e)->err, "%s failed: %s", #expr, cudaGetErrorString(_st));           \
+      return _st == cudaErrorMemoryAllocation ? SGM_ERR_NOMEM : SGM_ERR_CUDA;          \
+    }                                                                                  \
+  } while (0)
+
+int check_launch(sgm_engine* e, const char* what) {
+  prof_end(what);
+  e->launches++;
+  const cudaError_t st = cudaGetLastError();
+  if (st != cudaSuccess) {
+    set_error(&e->err, "launch of %s failed: %s", what, cudaGetErrorString(st));
+    return SGM_ERR_CUDA;
+  }
+  return SGM_OK;
+}
+
+// Launches `...` (a kernel launch expression) on stream s, timed when profiling is on.
+#define SGM_LAUNCH(e, s, name, ...) (prof_start(s), __VA_ARGS__, check_launch(e, name))
+
+bool supported_range(int D) { return D == 32 || D == 64 || D == 128 || D == 256; }
+
+int validate(sgm_engine* e, int W, int H, int D, const sgm_option_t* o) {
+  if (W <= 0 || H <= 0 || D <= 0) {
+    set_error(&e->err, "image size or disparity range error (w=%d h=%d d=%d)", W, H, D);
+    return SGM_ERR_ARG;
+  }
+  if (!supported_range(D)) {
+    set_error(&e->err, "disparity range %d unsupported (32, 64, 128, 256)", D);
+    return SGM_ERR_UNSUPPORTED;
+  }
+  if (o->cs_type != 0 && o->cs_type != 1) {
+    set_error(&e->err, "census type %d invalid", o->cs_type);
+    return SGM_ERR_ARG;
+  }
+  if (o->p1 < 0 || o->p2_init < 0) {
+    set_error(&e->err, "negative penalties (p1=%d p2=%d)", o->p1, o->p2_init);
+    return SGM_ERR_ARG;
+  }
+  if (o->post_filter_type != 0) {
+    set_error(&e->err, "post filter type %d unsupported", o->post_filter_type);
+    return SGM_ERR_UNSUPPORTED;
+  }
+  if (o->morphology_type != 0 && o->morphology_type != 2) {
+    set_error(&e->err, "morphology type %d unsupported (none or dilation)", o->morphology_type);
+    return SGM_ERR_UNSUPPORTED;
+  }
+  if ((size_t)W * H > (size_t)INT32_MAX / 2) {
+    set_error(&e->err, "image too large");
+    return SGM_ERR_ARG;
+  }
+  return SGM_OK;
+}
+
+int engine_init(sgm_engine* e, int W, int H, int M, int D, const sgm_option_t* o, bool log) {
+  if (e->ready) e->free_all();
+  const int v = validate(e, W, H, D, o);
+  if (v != SGM_OK) return v;
+  SGM_CUDA_TRY(e, cudaGetDevice(&e->dev));
+  e->W = W; e->H = H; e->M = M; e->D = D;
+  e->opt = *o;
+  e->print_log = log;
+  SGM_CUDA_TRY(e, cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+  const size_t N = e->npix();
+  const size_t V = e->vol() * 2;  // room for both views whatever the options
+  for (int i = 0; i < 2; ++i) {
+    SGM_CUDA_TRY(e, dalloc(&e->img[i], N));
+    SGM_CUDA_TRY(e, cudaMalloc(&e->cs[i], N * 8));
+    SGM_CUDA_TRY(e, dalloc(&e->init[i], N));
+  }
+  SGM_CUDA_TRY(e, dalloc(&e->cost, V));
+  SGM_CUDA_TRY(e, dalloc(&e->lr, V));
+  SGM_CUDA_TRY(e, dalloc(&e->rl, V));
+  SGM_CUDA_TRY(e, dalloc(&e->bt, V));
+  SGM_CUDA_TRY(e, dalloc(&e->wta, 2 * N));
+  SGM_CUDA_TRY(e, dalloc(&e->post, N));
+  SGM_CUDA_TRY(e, dalloc(&e->post2, N));
+  SGM_CUDA_TRY(e, dalloc(&e->dr_out, N));
+  SGM_CUDA_TRY(e, dalloc(&e->out, N));
+  SGM_CUDA_TRY(e, dalloc(&e->init_tmp, N));
+  SGM_CUDA_TRY(e, dalloc(&e->key, N));
+  SGM_CUDA_TRY(e, dalloc(&e->label, N));
+  SGM_CUDA_TRY(e, dalloc(&e->count, N));
+  e->ready = true;
+  if (log) printf("sgm-b200: init %dx%d, disparities %d..%d, census %s\n", W, H, M, M + D, o->cs_type ? "9x7" : "5x5");
+  return SGM_OK;
+}
+
+int rows_per_cta(int W, int word_bytes, bool with_init) {
+  const size_t per_row = (size_t)W * (2 * word_bytes + (with_init ? 2 : 0));
+  int R = 4;
+  while (R > 1 && per_row * R > 160 * 1024) R >>= 1;
+  return R;
+}
+
+template <int K, typename Word>
+int launch_plain(sgm_engine* e, const Word* csl, const Word* csr, float* wta) {
+  sgm::PlainParams P;
+  P.W = e->W; P.H = e->H; P.min_d = e->M; P.x0 = std::max(0, e->M);
+  P.p1 = (uint32_t)e->opt.p1; P.p2 = (uint32_t)e->opt.p2_init;
+  P.vstride = e->vol();
+  const int nv = e->nviews();
+  const int R = rows_per_cta(e->W, sizeof(Word), false);
+  const size_t smem = (size_t)R * 2 * e->W * sizeof(Word);
+  if (smem > 227 * 1024) {
+    set_error(&e->err, "image width %d too large for the row kernel", e->W);
+    return SGM_ERR_UNSUPPORTED;
+  }
+  auto hk = sgm::k_hpaths_plain<K, Word>;
+  SGM_CUDA_TRY(e, cudaFuncSetAttribute(hk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  dim3 hg((e->H + R - 1) / R, nv), hb(32, 2 * R);
+  int st = SGM_LAUNCH(e, e->stream, "hpaths_plain", hk<<<hg, hb, smem, e->stream>>>(csl, csr, e->cost, e->lr, e->rl, P));
+  if (st) return st;
+  sgm::WtaParams Q;
+  Q.uniqueness = e->opt.unique_threshold;
+  Q.tie_rule = e->ext.tie_rule;
+  const bool warp_kernel = (K <= 4);
+  Q.rows = warp_kernel ? (e->H / 2) * 2 : e->H;
+  Q.dmax_excl = warp_kernel ? 32 * K : 32 * K - 1;
+  Q.dstride = e->npix();
+  dim3 vg((e->W + 7) / 8, nv), vb(32, 8);
+  return SGM_LAUNCH(e, e->stream, "vpaths_wta_plain",
+                    sgm::k_vpaths_wta_plain<K><<<vg, vb, 0, e->stream>>>(e->cost, e->lr, e->rl, e->bt, wta, P, Q));
+}
+
+template <typename Word>
+int launch_init(sgm_engine* e, const Word* csl, const Word* csr, const int16_t* il, const int16_t* ir, float* wta) {
+  sgm::InitParams P;
+  P.W = e->W; P.H = e->H; P.x0 = std::max(0, e->M);
+  P.p1 = (uint32_t)e->opt.p1; P.p1s = e->opt.p1; P.p2s = e->opt.p2_init; P.p2_div0 = e->ext.p2_div0;
+  P.invalid_cost = e->opt.cs_type == 1 ? 0xFFu : sgm::kInvalidCost;
+  P.vstride = e->vol();
+  const int nv = e->nviews();
+  const int R = rows_per_cta(e->W, sizeof(Word), true);
+  const size_t smem = (size_t)R * e->W * (2 * sizeof(Word) + 2);
+  if (smem > 227 * 1024) {
+    set_error(&e->err, "image width %d too large for the row kernel", e->W);
+    return SGM_ERR_UNSUPPORTED;
+  }
+  auto hk = sgm::k_hpaths_init<Word>;
+  SGM_CUDA_TRY(e, cudaFuncSetAttribute(hk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  dim3 hg((e->H + R - 1) / R, nv), hb(32, 2 * R);
+  int st = SGM_LAUNCH(e, e->stream, "hpaths_init", hk<<<hg, hb, smem, e->stream>>>(csl, csr, il, ir, e->cost, e->lr, e->rl, P));
+  if (st) return st;
+  sgm::WtaParams Q;
+  Q.uniqueness = e->opt.unique_threshold;
+  Q.tie_rule = e->ext.init_tie_rule;
+  Q.rows = (e->H / 4) * 4;
+  Q.dmax_excl = sgm::kLevelRange - 1;
+  Q.dstride = e->npix();
+  dim3 vg((e->W + 7) / 8, nv), vb(32, 8);
+  return SGM_LAUNCH(e, e->stream, "vpaths_wta_init",
+                    sgm::k_vpaths_wta_init<<<vg, vb, 0, e->stream>>>(e->cost, e->lr, e->rl, il, ir, e->bt, wta, P, Q));
+}
+
+// Enqueues one full match of this level on s. Inputs/outputs are dense device arrays.
+int engine_enqueue(sgm_engine* e, const uint8_t* dl_img, const uint8_t* dr_img, const int16_t* dinit, float* dout,
+                   float* dout_r, cudaStream_t s) {
+  if (!e->ready) {
+    set_error(&e->err, "matcher not initialised");
+    return SGM_ERR_STATE;
+  }
+  if (dinit && e->D != sgm::kLevelRange) {
+    set_error(&e->err, "initial disparities need a disparity range of %d (got %d)", sgm::kLevelRange, e->D);
+    return SGM_ERR_UNSUPPORTED;
+  }
+  if (dinit && !e->opt.using_constant_p2) {
+    set_error(&e->err, "initial disparities need using_constant_p2 (the reference launches no aggregation otherwise)");
+    return SGM_ERR_UNSUPPORTED;
+  }
+  cudaStream_t saved = e->stream;
+  e->stream = s ? s : e->stream;
+  const int W = e->W, H = e->H;
+  const size_t N = e->npix();
+  int st = SGM_OK;
+  // census of both images
+  {
+    dim3 g((W + 127) / 128, H, 2), b(128);
+    if (e->opt.cs_type == 1)
+      st = SGM_LAUNCH(e, e->stream, "census", sgm::k_census<uint64_t, 4, 3><<<g, b, 0, e->stream>>>(
+                                                  dl_img, dr_img, (uint64_t*)e->cs[0], (uint64_t*)e->cs[1], W, H));
+    else
+      st = SGM_LAUNCH(e, e->stream, "census", sgm::k_census<uint32_t, 2, 2><<<g, b, 0, e->stream>>>(
+                                                  dl_img, dr_img, (uint32_t*)e->cs[0], (uint32_t*)e->cs[1], W, H));
+  }
+  // right-view initial disparities when checking consistency at an init level
+  const int16_t* dinit_r = nullptr;
+  if (!st && dinit && e->opt.do_lr_check) {
+    cudaMemsetAsync(e->key, 0, N * sizeof(unsigned), e->stream);
+    dim3 g((W + 127) / 128, H);
+    st = SGM_LAUNCH(e, e->stream, "right_init_scatter",
+                    sgm::k_right_init_scatter<<<g, 128, 0, e->stream>>>(dinit, e->key, W, H));
+    if (!st)
+      st = SGM_LAUNCH(e, e->stream, "right_init_decode",
+                      sgm::k_right_init_decode<<<(unsigned)((N + 255) / 256), 256, 0, e->stream>>>(e->key, e->init_tmp, (int)N));
+    if (!st) {
+      dim3 db(32, 8), dg((W + 31) / 32, (H + 7) / 8);
+      st = SGM_LAUNCH(e, e->stream, "dilation_init",
+                      sgm::k_dilation<int16_t><<<dg, db, 0, e->stream>>>(e->init_tmp, e->init[1], W, H, 2));
+    }
+    dinit_r = e->init[1];
+  }
+  // cost + four paths + WTA, both views
+  if (!st) {
+    const bool w64 = e->opt.cs_type == 1;
+    if (dinit) {
+      st = w64 ? launch_init<uint64_t>(e, (const uint64_t*)e->cs[0], (const uint64_t*)e->cs[1], dinit, dinit_r, e->wta)
+               : launch_init<uint32_t>(e, (const uint32_t*)e->cs[0], (const uint32_t*)e->cs[1], dinit, dinit_r, e->wta);
+    } else {
+      switch (e->D) {
+        case 32: st = w64 ? launch_plain<1, uint64_t>(e, (uint64_t*)e->cs[0], (uint64_t*)e->cs[1], e->wta)
+                          : launch_plain<1, uint32_t>(e, (uint32_t*)e->cs[0], (uint32_t*)e->cs[1], e->wta); break;
+        case 64: st = w64 ? launch_plain<2, uint64_t>(e, (uint64_t*)e->cs[0], (uint64_t*)e->cs[1], e->wta)
+                          : launch_plain<2, uint32_t>(e, (uint32_t*)e->cs[0], (uint32_t*)e->cs[1], e->wta); break;
+        case 128: st = w64 ? launch_plain<4, uint64_t>(e, (uint64_t*)e->cs[0], (uint64_t*)e->cs[1], e->wta)
+                           : launch_plain<4, uint32_t>(e, (uint32_t*)e->cs[0], (uint32_t*)e->cs[1], e->wta); break;
+        default: st = w64 ? launch_plain<8, uint64_t>(e, (uint64_t*)e->cs[0], (uint64_t*)e->cs[1], e->wta)
+                          : launch_plain<8, uint32_t>(e, (uint32_t*)e->cs[0], (uint32_t*)e->cs[1], e->wta); break;
+      }
+    }
+  }
+  // left-right check + median, then optional dilation and small-region removal
+  const bool lr = e->opt.do_lr_check, med = e->opt.do_median_filter;
+  const bool dil = e->opt.morphology_type == 2;
+  const bool peaks = e->opt.do_remove_peaks;
+  float* cur = e->wta;  // view 0
+  if (!st && lr && dout_r) {
+    cudaMemcpyAsync(dout_r, e->wta + N, N * sizeof(float), cudaMemcpyDeviceToDevice, e->stream);
+  }
+  if (!st && (lr || med)) {
+    float* dst = (!dil) ? dout : e->post;
+    dim3 b(32, 8), g((W + 31) / 32, (H + 7) / 8);
+    float* marks = lr ? dout_r : nullptr;
+    if (lr && med)
+      st = SGM_LAUNCH(e, e->stream, "lr_median", sgm::k_lr_median<true, true><<<g, b, 0, e->stream>>>(
+                                                     e->wta, e->wta + N, marks, dst, W, H, e->opt.lr_threshold));
+    else if (lr)
+      st = SGM_LAUNCH(e, e->stream, "lr_median", sgm::k_lr_median<true, false><<<g, b, 0, e->stream>>>(
+                                                     e->wta, e->wta + N, marks, dst, W, H, e->opt.lr_threshold));
+    else
+      st = SGM_LAUNCH(e, e->stream, "lr_median", sgm::k_lr_median<false, true><<<g, b, 0, e->stream>>>(
+                                                     e->wta, nullptr, nullptr, dst, W, H, 0.0f));
+    cur = dst;
+  }
+  if (!st && dil) {
+    const int s2 = std::min(W, H);
+    const int wnd = s2 < 360 ? 3 : (s2 < 720 ? 5 : 7);
+    dim3 b(32, 8), g((W + 31) / 32, (H + 7) / 8);
+    st = SGM_LAUNCH(e, e->stream, "dilation", sgm::k_dilation<float><<<g, b, 0, e->stream>>>(cur, dout, W, H, (wnd - 1) / 2));
+    cur = dout;
+  }
+  if (!st && cur != dout) {
+    cudaMemcpyAsync(dout, cur, N * sizeof(float), cudaMemcpyDeviceToDevice, e->stream);
+    cur = dout;
+  }
+  if (!st && peaks) {
+    const int strips = e->ext.peaks_strips > 0 ? e->ext.peaks_strips : default_peaks_strips();
+    const int tiles = H / strips;
+    if (tiles > 0) {
+      const int rows = strips * tiles;
+      const unsigned nb = (unsigned)((N + 255) / 256);
+      st = SGM_LAUNCH(e, e->stream, "cc_init", sgm::k_cc_init<<<nb, 256, 0, e->stream>>>(dout, e->label, e->count, W, H, rows));
+      if (!st)
+        st = SGM_LAUNCH(e, e->stream, "cc_union", sgm::k_cc_union<<<nb, 256, 0, e->stream>>>(
+                                                      dout, e->label, W, H, tiles, rows, e->ext.peaks_abs_mode));
+      if (!st)
+        st = SGM_LAUNCH(e, e->stream, "cc_count", sgm::k_cc_count<<<nb, 256, 0, e->stream>>>(e->label, e->count, (int)N));
+      if (!st)
+        st = SGM_LAUNCH(e, e->stream, "cc_filter", sgm::k_cc_filter<<<nb, 256, 0, e->stream>>>(
+                                                       dout, e->label, e->count, W, H, tiles, e->opt.peaks_ratio_threshold));
+    }
+  }
+  e->stream = saved;
+  return st;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------
+// Pyramid matcher
+// ------------------------------------------------------------------------------------------
+struct sgm_pyramid {
+  bool ready = false;
+  int W = 0, H = 0, layers = 0;
+  std::vector<sgm_engine*> lv;
+  std::vector<uint8_t*> imgs_l, imgs_r;  // decimated images per level (level 0 unused)
+  std::vector<float*> disp;              // per-level output (level 0 unused)
+  std::vector<int16_t*> init;            // initial disparity per level (coarsest unused)
+  uint8_t* in_l = nullptr;
+  uint8_t* in_r = nullptr;
+  float* out = nullptr;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  int64_t launches = 0;
+
+  void free_all() {
+    for (auto* e : lv) {
+      if (e) { e->free_all(); delete e; }
+    }
+    lv.clear();
+    for (auto* p : imgs_l) if (p) cudaFree(p);
+    for (auto* p : imgs_r) if (p) cudaFree(p);
+    for (auto* p : disp) if (p) cudaFree(p);
+    for (auto* p : init) if (p) cudaFree(p);
+    imgs_l.clear(); imgs_r.clear(); disp.clear(); init.clear();
+    if (in_l) cudaFree(in_l);
+    if (in_r) cudaFree(in_r);
+    if (out) cudaFree(out);
+    in_l = in_r = nullptr;
+    out = nullptr;
+    if (stream) cudaStreamDestroy(stream);
+    stream = nullptr;
+    ready = false;
+  }
+};
+
+namespace {
+
+// SetSgmParameters (FasterStereoCuda.cpp:169-199) with the optional census/penalty override,
+// and the disparity-range rules of HierSgmCudaImpl::Init (:264-288).
+void level_options(const sgm_pyr_option1_t* o, const sgm_level_override_t* ov, int level, int layers,
+                   sgm_option_t* so, int* dmin_out, int* drange_out) {
+  memset(so, 0, sizeof(*so));
+  so->p1 = ov ? ov->p1 : 8;
+  so->p2_init = ov ? ov->p2 : 32;
+  so->p2_max = 64;
+  so->cs_type = ov ? ov->cs_type : 0;
+  so->num_paths = 4;
+  so->unique_threshold = level == 0 ? 0.95f : 1.0f;
+  so->lr_threshold = 1.0f;
+  so->do_median_filter = true;
+  so->post_filter_type = 0;
+  so->using_constant_p2 = true;
+  if (layers <= 1) {
+    so->do_lr_check = o->do_lr_check;
+    so->do_remove_peaks = o->do_rm_peaks;
+    so->peaks_ratio_threshold = 0.0005f;
+    so->morphology_type = 0;
+  } else if (layers <= 2) {
+    so->do_lr_check = level == 0 ? false : o->do_lr_check;
+    so->do_remove_peaks = level == 0 ? false : o->do_rm_peaks;
+    so->peaks_ratio_threshold = level == 0 ? 0.0005f : 0.001f;
+    so->morphology_type = level < layers - 1 ? 0 : 2;
+  } else {
+    so->do_lr_check = level < layers - 1 ? false : o->do_lr_check;
+    so->do_remove_peaks = level < layers - 1 ? false : o->do_rm_peaks;
+    so->peaks_ratio_threshold = level < layers - 1 ? 0.0005f : 0.005f;
+    so->morphology_type = level < layers - 1 ? 0 : 2;
+  }
+  const int scale = 1 << level;
+  if (level == layers - 1) {
+    int dmin = o->min_disp / scale, dmax = o->max_disp / scale;
+    int range = dmax - dmin;
+    int k = 6;
+    while ((1 << k) < range) ++k;
+    range = 1 << k;
+    if (range > 2 * o->width) range /= 2;
+    if (dmin >= o->width) {
+      dmin = o->width - range;
+      if (dmin < -o->width) dmin = -o->width;
+    }
+    *dmin_out = dmin;
+    *drange_out = range;
+  } else {
+    *dmin_out = 0;
+    *drange_out = sgm::kLevelRange;
+  }
+}
+
+int pyr_enqueue(sgm_pyramid* p, const uint8_t* dl, const uint8_t* dr, float* dout, cudaStream_t s) {
+  const int L = p->layers;
+  int st = SGM_OK;
+  for (int n = 1; n < L && !st; ++n) {
+    sgm_engine* e = p->lv[n];
+    dim3 g((e->W + 127) / 128, e->H);
+    prof_start(s);
+    sgm::k_decimate<<<g, 128, 0, s>>>(dl, dr, p->imgs_l[n], p->imgs_r[n], p->W, e->W, e->H, n);
+    prof_end("decimate");
+    p->launches++;
+    if (cudaGetLastError() != cudaSuccess) st = SGM_ERR_CUDA;
+  }
+  for (int n = L - 1; n >= 0 && !st; --n) {
+    sgm_engine* e = p->lv[n];
+    const uint8_t* il = n == 0 ? dl : p->imgs_l[n];
+    const uint8_t* ir = n == 0 ? dr : p->imgs_r[n];
+    float* o = n == 0 ? dout : p->disp[n];
+    const int64_t before = e->launches;
+    st = engine_enqueue(e, il, ir, n < L - 1 ? p->init[n] : nullptr, o, nullptr, s);
+    p->launches += e->launches - before;
+    if (st) {
+      p->err = e->err;
+      break;
+    }
+    if (n > 0) {
+      sgm_engine* f = p->lv[n - 1];
+      dim3 g((f->W + 127) / 128, f->H);
+      prof_start(s);
+      sgm::k_init_next_level<<<g, 128, 0, s>>>(p->disp[n], (long)e->W * e->H, p->init[n - 1], f->W, f->H);
+      prof_end("init_next_level");
+      p->launches++;
+      if (cudaGetLastError() != cudaSuccess) st = SGM_ERR_CUDA;
+    }
+  }
+  return st;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------
+// C ABI
+// ------------------------------------------------------------------------------------------
+extern "C" {
+
+int sgm_create(sgm_handle_t* out) {
+  if (!out) return SGM_ERR_ARG;
+  *out = new (std::nothrow) sgm_engine();
+  return *out ? SGM_OK : SGM_ERR_NOMEM;
+}
+
+int sgm_destroy(sgm_handle_t h) {
+  if (!h) return SGM_ERR_ARG;
+  h->free_all();
+  delete h;
+  return SGM_OK;
+}
+
+int sgm_init(sgm_handle_t h, int32_t width, int32_t height, int32_t min_disparity, int32_t disp_range,
+             const sgm_option_t* option, int32_t print_log) {
+  if (!h || !option) return SGM_ERR_ARG;
+  const int st = engine_init(h, width, height, min_disparity, disp_range, option, print_log != 0);
+  if (st) h->free_all();
+  return st;
+}
+
+int sgm_set_ext_options(sgm_handle_t h, const sgm_ext_options_t* ext) {
+  if (!h || !ext) return SGM_ERR_ARG;
+  if (ext->tie_rule < 0 || ext->tie_rule > 3 || ext->init_tie_rule < 0 || ext->init_tie_rule > 3 ||
+      ext->peaks_abs_mode < 0 || ext->peaks_abs_mode > 1) {
+    set_error(&h->err, "extended option out of range");
+    return SGM_ERR_ARG;
+  }
+  h->ext = *ext;
+  return SGM_OK;
+}
+
+int sgm_get_ext_options(sgm_handle_t h, sgm_ext_options_t* ext) {
+  if (!h || !ext) return SGM_ERR_ARG;
+  *ext = h->ext;
+  return SGM_OK;
+}
+
+int sgm_match(sgm_handle_t h, const uint8_t* img_left, const uint8_t* img_right, float* disp_left,
+              float* disp_right, const int16_t* init_disp_left, const sgm_roi_t* roi_left,
+              const sgm_roi_t* roi_right) {
+  if (!h) return SGM_ERR_ARG;
+  if (!img_left || !img_right || !disp_left) {
+    set_error(&h->err, "null image or output pointer");
+    return SGM_ERR_ARG;
+  }
+  if (!h->ready) {
+    set_error(&h->err, "matcher not initialised");
+    return SGM_ERR_STATE;
+  }
+  if (roi_left || roi_right) {
+    set_error(&h->err, "ROI matching is not supported");
+    return SGM_ERR_UNSUPPORTED;
+  }
+  const size_t N = h->npix();
+  h->launches = 0;
+  SGM_CUDA_TRY(h, cudaMemcpyAsync(h->img[0], img_left, N, cudaMemcpyHostToDevice, h->stream));
+  SGM_CUDA_TRY(h, cudaMemcpyAsync(h->img[1], img_right, N, cudaMemcpyHostToDevice, h->stream));
+  if (init_disp_left)
+    SGM_CUDA_TRY(h, cudaMemcpyAsync(h->init[0], init_disp_left, N * sizeof(int16_t), cudaMemcpyHostToDevice, h->stream));
+  int st = engine_enqueue(h, h->img[0], h->img[1], init_disp_left ? h->init[0] : nullptr, h->out,
+                          (disp_right && h->opt.do_lr_check) ? h->dr_out : nullptr, h->stream);
+  if (st) return st;
+  SGM_CUDA_TRY(h, cudaMemcpyAsync(disp_left, h->out, N * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+  if (disp_right && h->opt.do_lr_check)
+    SGM_CUDA_TRY(h, cudaMemcpyAsync(disp_right, h->dr_out, N * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+  SGM_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  if (disp_right && !h->opt.do_lr_check)
+    for (size_t i = 0; i < N; ++i) disp_right[i] = sgm::kInvalidFloat;
+  return SGM_OK;
+}
+
+int sgm_match_device(sgm_handle_t h, const uint8_t* d_left, const uint8_t* d_right, float* d_disp_left,
+                     float* d_disp_right, const int16_t* d_init_disp_left, void* stream) {
+  if (!h) return SGM_ERR_ARG;
+  if (!d_left || !d_right || !d_disp_left) {
+    set_error(&h->err, "null device pointer");
+    return SGM_ERR_ARG;
+  }
+  if (d_disp_right && !h->opt.do_lr_check) {
+    set_error(&h->err, "a right disparity map needs the left-right check");
+    return SGM_ERR_ARG;
+  }
+  h->launches = 0;
+  return engine_enqueue(h, d_left, d_right, d_init_disp_left, d_disp_left, d_disp_right, (cudaStream_t)stream);
+}
+
+int sgm_release(sgm_handle_t h) {
+  if (!h) return SGM_ERR_ARG;
+  h->free_all();
+  return SGM_OK;
+}
+
+int sgm_set_min_disparity(sgm_handle_t h, int32_t min_disparity) {
+  if (!h) return SGM_ERR_ARG;
+  h->M = min_disparity;
+  return SGM_OK;
+}
+
+int32_t sgm_get_disparity_range(sgm_handle_t h) { return h ? h->D : 0; }
+
+void sgm_roi_from_disp_map(const float* disp, int32_t width, int32_t height, sgm_roi_t* roi) {
+  // StereoCudaImpl::GetRoiFromDispMap (StereoCudaImpl.cpp:585-628), same scan order
+  if (!disp || !roi) return;
+  const int size = width * height;
+  int n = 0;
+  for (n = 0; n < size; n++)
+    if (disp[n] != sgm::kInvalidFloat) break;
+  roi->y = n / width;
+  const int size0 = roi->y * width;
+  for (n = size - 1; n > size0; n--)
+    if (disp[n] != sgm::kInvalidFloat) break;
+  roi->h = n / width - roi->y + 1;
+  bool done = false;
+  for (int j = 0; j < width && !done; j++)
+    for (int i = 0; i < height; i++)
+      if (disp[i * width + j] != sgm::kInvalidFloat) { roi->x = j; done = true; break; }
+  done = false;
+  for (int j = width - 1; j > roi->x && !done; j--)
+    for (int i = 0; i < height; i++)
+      if (disp[i * width + j] != sgm::kInvalidFloat) { roi->w = j - roi->x + 1; done = true; break; }
+}
+
+float sgm_invalid_float(void) { return sgm::kInvalidFloat; }
+int16_t sgm_invalid_short(void) { return sgm::kInvalidShort; }
+int16_t sgm_level_range(void) { return (int16_t)sgm::kLevelRange; }
+
+int sgm_malloc_page_locked(void** ptr, size_t size) {
+  if (!ptr) return SGM_ERR_ARG;
+  return cudaHostAlloc(ptr, size, cudaHostAllocDefault) == cudaSuccess ? SGM_OK : SGM_ERR_NOMEM;
+}
+
+int sgm_free_page_locked(void* ptr) {
+  if (!ptr) return SGM_ERR_ARG;
+  return cudaFreeHost(ptr) == cudaSuccess ? SGM_OK : SGM_ERR_CUDA;
+}
+
+const char* sgm_last_error(sgm_handle_t h) { return h ? h->err.c_str() : g_last_error.c_str(); }
+
+int64_t sgm_kernel_launches(sgm_handle_t h) { return h ? h->launches : 0; }
+
+int sgm_debug_read(sgm_handle_t h, int32_t which, int32_t view, void* dst, size_t bytes) {
+  if (!h || !dst || view < 0 || view > 1) return SGM_ERR_ARG;
+  if (!h->ready) return SGM_ERR_STATE;
+  const size_t N = h->npix(), V = h->vol();
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) return SGM_ERR_CUDA;
+  if (which == 0 || which == 1) {
+    if (bytes != N * 8) return SGM_ERR_ARG;
+    const int wb = h->census_bytes();
+    std::vector<uint8_t> tmp(N * wb);
+    if (cudaMemcpy(tmp.data(), h->cs[which], N * wb, cudaMemcpyDeviceToHost) != cudaSuccess) return SGM_ERR_CUDA;
+    uint64_t* out = static_cast<uint64_t*>(dst);
+    for (size_t i = 0; i < N; ++i) {
+      uint64_t v = 0;
+      memcpy(&v, tmp.data() + i * wb, wb);
+      out[i] = v;
+    }
+    return SGM_OK;
+  }
+  const uint8_t* src = nullptr;
+  size_t n = V;
+  switch (which) {
+    case 2: src = h->cost + view * V; break;
+    case 3: src = h->lr + view * V; break;
+    case 4: src = h->rl + view * V; break;
+    case 5: src = h->bt + view * V; break;
+    case 6: src = reinterpret_cast<const uint8_t*>(h->wta + view * N); n = N * sizeof(float); break;
+    default: return SGM_ERR_ARG;
+  }
+  if (bytes != n) return SGM_ERR_ARG;
+  return cudaMemcpy(dst, src, n, cudaMemcpyDeviceToHost) == cudaSuccess ? SGM_OK : SGM_ERR_CUDA;
+}
+
+int sgm_profile_enable(int32_t enable) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  g_prof.collect();
+  g_prof.stats.clear();
+  g_prof.on = enable != 0;
+  return SGM_OK;
+}
+
+int sgm_profile_read(char* buf, size_t cap) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  g_prof.collect();
+  std::string js = "{";
+  for (size_t i = 0; i < g_prof.stats.size(); ++i) {
+    char item[256];
+    snprintf(item, sizeof(item), "%s\"%s\": {\"launches\": %lld, \"ms\": %.6f}", i ? ", " : "",
+             g_prof.stats[i].name.c_str(), (long long)g_prof.stats[i].launches, g_prof.stats[i].ms);
+    js += item;
+  }
+  js += "}";
+  if (!buf || cap < js.size() + 1) return (int)(js.size() + 1);
+  memcpy(buf, js.c_str(), js.size() + 1);
+  return SGM_OK;
+}
+
+int sgm_pyr_create(sgm_pyr_handle_t* out) {
+  if (!out) return SGM_ERR_ARG;
+  *out = new (std::nothrow) sgm_pyramid();
+  return *out ? SGM_OK : SGM_ERR_NOMEM;
+}
+
+int sgm_pyr_destroy(sgm_pyr_handle_t h) {
+  if (!h) return SGM_ERR_ARG;
+  h->free_all();
+  delete h;
+  return SGM_OK;
+}
+
+int sgm_pyr_init(sgm_pyr_handle_t h, const sgm_pyr_option1_t* o, const sgm_level_override_t* ov,
+                 const sgm_ext_options_t* ext) {
+  if (!h || !o) return SGM_ERR_ARG;
+  h->free_all();
+  if (o->width <= 0 || o->height <= 0) {
+    set_error(&h->err, "image size error");
+    return SGM_ERR_ARG;
+  }
+  const int L = std::max(1, o->num_layers);
+  if ((o->width >> (L - 1)) < 8 || (o->height >> (L - 1)) < 8) {
+    set_error(&h->err, "too many layers for a %dx%d image", o->width, o->height);
+    return SGM_ERR_ARG;
+  }
+  h->W = o->width;
+  h->H = o->height;
+  h->layers = L;
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return SGM_ERR_CUDA;
+  h->lv.assign(L, nullptr);
+  h->imgs_l.assign(L, nullptr);
+  h->imgs_r.assign(L, nullptr);
+  h->disp.assign(L, nullptr);
+  h->init.assign(L, nullptr);
+  for (int i = 0; i < L; ++i) {
+    sgm_option_t so;
+    int dmin = 0, dr = 0;
+    level_options(o, ov, i, L, &so, &dmin, &dr);
+    h->lv[i] = new sgm_engine();
+    if (ext) h->lv[i]->ext = *ext;
+    const int w = o->width >> i, hh = o->height >> i;
+    int st = engine_init(h->lv[i], w, hh, dmin, dr, &so, false);
+    if (st) {
+      h->err = h->lv[i]->err;
+      h->free_all();
+      return st;
+    }
+    const size_t n = (size_t)w * hh;
+    if (i > 0) {
+      if (cudaMalloc(&h->imgs_l[i], n) || cudaMalloc(&h->imgs_r[i], n) || cudaMalloc(&h->disp[i], n * sizeof(float))) {
+        h->free_all();
+        return SGM_ERR_NOMEM;
+      }
+    }
+    if (i < L - 1 && cudaMalloc(&h->init[i], n * sizeof(int16_t))) {
+      h->free_all();
+      return SGM_ERR_NOMEM;
+    }
+  }
+  const size_t N = (size_t)o->width * o->height;
+  if (cudaMalloc(&h->in_l, N) || cudaMalloc(&h->in_r, N) || cudaMalloc(&h->out, N * sizeof(float))) {
+    h->free_all();
+    return SGM_ERR_NOMEM;
+  }
+  h->ready = true;
+  return SGM_OK;
+}
+
+int sgm_pyr_match(sgm_pyr_handle_t h, const uint8_t* img_left, const uint8_t* img_right, float* disp) {
+  if (!h) return SGM_ERR_ARG;
+  if (!h->ready) return SGM_ERR_STATE;
+  if (!img_left || !img_right || !disp) return SGM_ERR_ARG;
+  const size_t N = (size_t)h->W * h->H;
+  h->launches = 0;
+  if (cudaMemcpyAsync(h->in_l, img_left, N, cudaMemcpyHostToDevice, h->stream) ||
+      cudaMemcpyAsync(h->in_r, img_right, N, cudaMemcpyHostToDevice, h->stream))
+    return SGM_ERR_CUDA;
+  int st = pyr_enqueue(h, h->in_l, h->in_r, h->out, h->stream);
+  if (st) return st;
+  if (cudaMemcpyAsync(disp, h->out, N * sizeof(float), cudaMemcpyDeviceToHost, h->stream)) return SGM_ERR_CUDA;
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
+    set_error(&h->err, "pyramid match failed: %s", cudaGetErrorString(cudaGetLastError()));
+    return SGM_ERR_CUDA;
+  }
+  return SGM_OK;
+}
+
+int sgm_pyr_match_device(sgm_pyr_handle_t h, const uint8_t* d_left, const uint8_t* d_right, float* d_disp,
+                         void* stream) {
+  if (!h) return SGM_ERR_ARG;
+  if (!h->ready) return SGM_ERR_STATE;
+  if (!d_left || !d_right || !d_disp) return SGM_ERR_ARG;
+  h->launches = 0;
+  return pyr_enqueue(h, d_left, d_right, d_disp, stream ? (cudaStream_t)stream : h->stream);
+}
+
+int sgm_pyr_release(sgm_pyr_handle_t h) {
+  if (!h) return SGM_ERR_ARG;
+  h->free_all();
+  return SGM_OK;
+}
+
+int sgm_pyr_level_info(sgm_pyr_handle_t h, int32_t level, int32_t* width, int32_t* height, int32_t* min_disp,
+                       int32_t* disp_range) {
+  if (!h || !h->ready || level < 0 || level >= h->layers) return SGM_ERR_ARG;
+  const sgm_engine* e = h->lv[level];
+  if (width) *width = e->W;
+  if (height) *height = e->H;
+  if (min_disp) *min_disp = e->M;
+  if (disp_range) *disp_range = e->D;
+  return SGM_OK;
+}
+
+int64_t sgm_pyr_kernel_launches(sgm_pyr_handle_t h) { return h ? h->launches : 0; }
+
+}  // extern "C"

@@ -1,0 +1,728 @@
+// SGM stereo kernels for sm_100a.
+//
+// Data layout in HBM (dense, no pitch):
+//   images        u8   [H][W]                 per view
+//   census        u32/u64 [H][W]              per view (5x5 -> u32, 9x7 -> u64)
+//   volumes       u8   [view][H][W][D]        cost, left->right, right->left, bottom->top path costs
+//   disparity     f32  [view][H][W]
+// Views: 0 = left image matched against the right one, 1 = right image against the left
+// (the second view exists only when the left-right check is on).
+//
+// Warp mapping of the path scans: one warp owns one scanline; lane l holds the K = D/32
+// contiguous disparities d = l*K + j, so the d-1 / d+1 neighbours cross lanes only at j = 0
+// and j = K-1 (two shuffles per step), and the per-step minimum is one REDUX (__reduce_min_sync).
+#pragma once
+#include "sgm_common.cuh"
+
+namespace sgm {
+
+// ---------------------------------------------------------------------------------------------
+// Census transform (reference SgmStereoCuda/cusgm_cc.cu:30-106). Both views in one launch
+// (blockIdx.z). Left border value 0, right border value 0xFFFFFFFF (zero-extended).
+// ---------------------------------------------------------------------------------------------
+template <typename Word, int CSW, int CSH>
+__global__ void __launch_bounds__(128) k_census(const uint8_t* __restrict__ img_l, const uint8_t* __restrict__ img_r,
+                                                Word* __restrict__ cs_l, Word* __restrict__ cs_r, int W, int H) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  const bool right = blockIdx.z == 1;
+  if (x >= W) return;
+  const uint8_t* img = right ? img_r : img_l;
+  Word v = 0;
+  if (x < CSW || x >= W - CSW || y < CSH || y >= H - CSH) {
+    v = right ? (Word)0xFFFFFFFFu : (Word)0;
+  } else {
+    const uint8_t c = __ldg(img + (size_t)y * W + x);
+#pragma unroll
+    for (int dy = -CSH; dy <= CSH; ++dy) {
+      const uint8_t* row = img + (size_t)(y + dy) * W + x;
+#pragma unroll
+      for (int dx = -CSW; dx <= CSW; ++dx) v = (Word)((v << 1) | (Word)(__ldg(row + dx) < c));
+    }
+  }
+  (right ? cs_r : cs_l)[(size_t)y * W + x] = v;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Recurrence step shared by every plain scan (reference cusgm_ca.cu:1517-1564 and its 32/128
+// twins): L_p(d) = C_p(d) + min(L_q(d), L_q(d-1)+P1, L_q(d+1)+P1, m_q+P2) - m_q, uint32,
+// with 127 as the candidate beyond d = 0 and d = D-1. Returns the new warp-wide minimum.
+// ---------------------------------------------------------------------------------------------
+template <int K>
+__device__ __forceinline__ uint32_t plain_step(uint32_t (&L)[K], const uint32_t (&c)[K], uint32_t m, uint32_t p1,
+                                               uint32_t p2, int lane) {
+  const uint32_t left_nb = __shfl_up_sync(kFull, L[K - 1], 1);
+  const uint32_t right_nb = __shfl_down_sync(kFull, L[0], 1);
+  const uint32_t l4 = m + p2;
+  uint32_t nl[K];
+  uint32_t mn = 0xFFFFFFFFu;
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    const uint32_t a = j > 0 ? L[j - 1] + p1 : (lane > 0 ? left_nb + p1 : kInvalidCost);
+    const uint32_t b = j < K - 1 ? L[j + 1] + p1 : (lane < 31 ? right_nb + p1 : kInvalidCost);
+    const uint32_t t = min(min(min(L[j], a), b), l4);
+    nl[j] = c[j] + (t - m);
+    mn = min(mn, nl[j]);
+  }
+#pragma unroll
+  for (int j = 0; j < K; ++j) L[j] = nl[j];
+  return __reduce_min_sync(kFull, mn);
+}
+
+template <int K>
+__device__ __forceinline__ void store_u8(uint8_t* p, const uint32_t (&v)[K]) {
+  if constexpr (K == 1) {
+    *p = (uint8_t)v[0];
+  } else if constexpr (K == 2) {
+    *reinterpret_cast<uint16_t*>(p) = (uint16_t)((v[0] & 0xFFu) | ((v[1] & 0xFFu) << 8));
+  } else if constexpr (K == 4) {
+    *reinterpret_cast<uint32_t*>(p) = (v[0] & 0xFFu) | ((v[1] & 0xFFu) << 8) | ((v[2] & 0xFFu) << 16) | (v[3] << 24);
+  } else {
+    uint2 w;
+    w.x = (v[0] & 0xFFu) | ((v[1] & 0xFFu) << 8) | ((v[2] & 0xFFu) << 16) | (v[3] << 24);
+    w.y = (v[4] & 0xFFu) | ((v[5] & 0xFFu) << 8) | ((v[6] & 0xFFu) << 16) | (v[7] << 24);
+    *reinterpret_cast<uint2*>(p) = w;
+  }
+}
+
+template <int K>
+__device__ __forceinline__ void load_u8(const uint8_t* p, uint32_t (&v)[K]) {
+  if constexpr (K == 1) {
+    v[0] = __ldg(p);
+  } else if constexpr (K == 2) {
+    const uint32_t w = __ldg(reinterpret_cast<const uint16_t*>(p));
+    v[0] = w & 0xFFu;
+    v[1] = w >> 8;
+  } else if constexpr (K == 4) {
+    const uint32_t w = __ldg(reinterpret_cast<const uint32_t*>(p));
+#pragma unroll
+    for (int j = 0; j < 4; ++j) v[j] = (w >> (8 * j)) & 0xFFu;
+  } else {
+    const uint2 w = __ldg(reinterpret_cast<const uint2*>(p));
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      v[j] = (w.x >> (8 * j)) & 0xFFu;
+      v[4 + j] = (w.y >> (8 * j)) & 0xFFu;
+    }
+  }
+}
+
+struct PlainParams {
+  int W, H;
+  int min_d;   // minimum disparity
+  int x0;      // first column of every scan, max(0, min_d)
+  uint32_t p1, p2;
+  size_t vstride;  // elements between the views of a volume (H*W*D)
+};
+
+// ---------------------------------------------------------------------------------------------
+// Horizontal scans (left->right and right->left) of the plain path, with the Hamming cost
+// computed on the fly from census rows staged in shared memory.
+// Reference: Kernel_CostCompute cusgm_cc.cu:118-172/238-293 and
+// Kernel_Aggregate_Horizontal_Warpfor{32,64,128} cusgm_ca.cu:1343-1770.
+// One CTA = R rows x 2 directions (2R warps). The left->right warp also stores the cost volume.
+// View 0: C(x,d) = popc(cl[x] ^ cr[x-min_d-d]); view 1: C(x,d) = popc(cr[x] ^ cl[x+min_d+d]);
+// an out-of-range partner index reads element 0 of the partner row. With 5x5 census the
+// reference's right-to-left cost kernel leaves the last pixel of every D-pixel block holding
+// the left-to-right cost (cusgm_cc.cu:288); view 1 reproduces that.
+// ---------------------------------------------------------------------------------------------
+template <int K, typename Word>
+__global__ void __launch_bounds__(256) k_hpaths_plain(const Word* __restrict__ cs_l, const Word* __restrict__ cs_r,
+                                                      uint8_t* __restrict__ cost, uint8_t* __restrict__ lr,
+                                                      uint8_t* __restrict__ rl, PlainParams P) {
+  constexpr int D = 32 * K;
+  const int view = blockIdx.y;
+  const int lane = threadIdx.x;
+  const int wid = threadIdx.y;
+  const int R = blockDim.y >> 1;
+  const int row = wid >> 1;
+  const int dir = wid & 1;
+  const int y = blockIdx.x * R + row;
+  const int W = P.W;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Word* own = reinterpret_cast<Word*>(smem_raw) + (size_t)row * 2 * W;
+  Word* oth = own + W;
+  if (y < P.H) {
+    const Word* g_own = (view == 0 ? cs_l : cs_r) + (size_t)y * W;
+    const Word* g_oth = (view == 0 ? cs_r : cs_l) + (size_t)y * W;
+    for (int i = dir * 32 + lane; i < W; i += 64) {
+      own[i] = g_own[i];
+      oth[i] = g_oth[i];
+    }
+  }
+  __syncthreads();
+  if (y >= P.H) return;
+  const int x0 = P.x0;
+  const int len = W - x0;
+  if (len <= 0) return;
+  const size_t vo = (size_t)view * P.vstride;
+  uint8_t* out = (dir == 0 ? lr : rl) + vo;
+  uint8_t* cvol = cost + vo;
+  const int dbase = lane * K;
+  const bool stale5 = (view == 1) && (sizeof(Word) == 4);
+  uint32_t L[K];
+  uint32_t m = 0;
+  for (int s = 0; s < len; ++s) {
+    const int x = dir == 0 ? x0 + s : W - 1 - s;
+    uint32_t c[K];
+    bool lr_cost = false;
+    if (stale5) {
+      const int blk = x0 + ((x - x0) / D) * D;
+      const int iend = min(D, W - blk);
+      lr_cost = (x == blk + iend - 1);
+    }
+    if (!lr_cost) {
+      const Word a = own[x];
+#pragma unroll
+      for (int j = 0; j < K; ++j) {
+        const int d = dbase + j;
+        const int pos = view == 0 ? x - P.min_d - d : x + P.min_d + d;
+        c[j] = popc_word((Word)(a ^ ((pos >= 0 && pos < W) ? oth[pos] : oth[0])));
+      }
+    } else {  // view 1, 5x5: left-to-right cost of this pixel (own = right census, oth = left census)
+      const Word a = oth[x];
+#pragma unroll
+      for (int j = 0; j < K; ++j) {
+        const int pos = x - P.min_d - (dbase + j);
+        c[j] = popc_word((Word)(a ^ ((pos >= 0 && pos < W) ? own[pos] : own[0])));
+      }
+    }
+    const size_t off = ((size_t)y * W + x) * D + dbase;
+    if (s == 0) {
+      uint32_t mn = 0xFFFFFFFFu;
+#pragma unroll
+      for (int j = 0; j < K; ++j) {
+        L[j] = c[j];
+        mn = min(mn, c[j]);
+      }
+      m = __reduce_min_sync(kFull, mn);
+    } else {
+      m = plain_step<K>(L, c, m, P.p1, P.p2, lane);
+    }
+    store_u8<K>(out + off, L);
+    if (dir == 0) store_u8<K>(cvol + off, c);
+  }
+}
+
+struct WtaParams {
+  float uniqueness;
+  int tie_rule;
+  int rows;        // rows the reference's WTA launch covers
+  int dmax_excl;   // d* must be < dmax_excl (D for the warp kernels, D-1 for the generic one)
+  size_t dstride;  // elements between the views of the disparity maps (H*W)
+};
+
+// Winner-take-all + uniqueness + subpixel on the summed path costs of one pixel.
+// Reference Kernel_ComputeDisparityByWTA_Warpfor{32,64,128} cusgm_ca.cu:3514-3809 and the
+// generic kernel :3149-3232. Returns the disparity (valid in every lane).
+template <int K>
+__device__ __forceinline__ float wta_pixel(const uint32_t (&S)[K], int lane, int min_d_or_base, const WtaParams& Q,
+                                           int dmin_excl) {
+  constexpr int D = 32 * K;
+  uint32_t lm = S[0];
+#pragma unroll
+  for (int j = 1; j < K; ++j) lm = min(lm, S[j]);
+  const uint32_t m = __reduce_min_sync(kFull, lm);
+  uint32_t bal[K];
+#pragma unroll
+  for (int j = 0; j < K; ++j) bal[j] = __ballot_sync(kFull, S[j] == m);
+  const int ds = pick_tie<K>(bal, Q.tie_rule);
+  // neighbours of d*: S(d*-1) and S(d*+1) live in lanes (d*-1)/K and (d*+1)/K
+  const int dl = ds - 1 < 0 ? 0 : ds - 1;
+  const int dr = ds + 1 >= D ? D - 1 : ds + 1;
+  uint32_t vl = S[0], vr = S[0];
+#pragma unroll
+  for (int j = 1; j < K; ++j) {
+    if ((dl % K) == j) vl = S[j];
+    if ((dr % K) == j) vr = S[j];
+  }
+  const uint32_t s1 = __shfl_sync(kFull, vl, dl / K);
+  const uint32_t s3 = __shfl_sync(kFull, vr, dr / K);
+  if (ds <= dmin_excl || ds >= Q.dmax_excl) return kInvalidFloat;
+  const float c1 = (float)s1;
+  const float c2 = (float)m;
+  const float c3 = (ds + 1 < D) ? (float)s3 : (float)ds;
+  const float d12 = __fsub_rn(c1, c2), d32 = __fsub_rn(c3, c2);
+  const float uq = d12 < d32 ? d12 : d32;
+  if (uq <= __fmul_rn(c2, __fsub_rn(1.0f, Q.uniqueness))) return kInvalidFloat;
+  return __fadd_rn((float)(ds + min_d_or_base), subpix_bias(c1, c2, c3));
+}
+
+// ---------------------------------------------------------------------------------------------
+// Vertical scans (bottom->top, then top->bottom) fused with the 4-path sum and the WTA.
+// Reference Kernel_Aggregate_Vertical_Warpfor{32,64,128} cusgm_ca.cu:1410-1888 and the WTA
+// kernels above. One warp per column; 8 columns per CTA. Columns left of x0 are INVALID.
+// ---------------------------------------------------------------------------------------------
+template <int K>
+__global__ void __launch_bounds__(256) k_vpaths_wta_plain(const uint8_t* __restrict__ cost,
+                                                          const uint8_t* __restrict__ lr,
+                                                          const uint8_t* __restrict__ rl, uint8_t* __restrict__ bt,
+                                                          float* __restrict__ disp, PlainParams P, WtaParams Q) {
+  constexpr int D = 32 * K;
+  const int view = blockIdx.y;
+  const int lane = threadIdx.x;
+  const int x = blockIdx.x * blockDim.y + threadIdx.y;
+  const int W = P.W, H = P.H;
+  if (x >= W) return;
+  float* dout = disp + (size_t)view * Q.dstride;
+  if (x < P.x0) {
+    for (int y = lane; y < H; y += 32) dout[(size_t)y * W + x] = kInvalidFloat;
+    return;
+  }
+  const size_t vo = (size_t)view * P.vstride;
+  const uint8_t* cv = cost + vo;
+  uint8_t* btv = bt + vo;
+  const int dbase = lane * K;
+  uint32_t L[K], c[K];
+  uint32_t m = 0;
+  // bottom -> top
+  for (int s = 0; s < H; ++s) {
+    const int y = H - 1 - s;
+    const size_t off = ((size_t)y * W + x) * D + dbase;
+    load_u8<K>(cv + off, c);
+    if (s == 0) {
+      uint32_t mn = 0xFFFFFFFFu;
+#pragma unroll
+      for (int j = 0; j < K; ++j) { L[j] = c[j]; mn = min(mn, c[j]); }
+      m = __reduce_min_sync(kFull, mn);
+    } else {
+      m = plain_step<K>(L, c, m, P.p1, P.p2, lane);
+    }
+    store_u8<K>(btv + off, L);
+  }
+  __syncwarp();
+  // top -> bottom, summing the four paths and selecting the disparity
+  const uint8_t* lrv = lr + vo;
+  const uint8_t* rlv = rl + vo;
+  const bool col_ok = x >= 5 && x <= W - 5;
+  for (int y = 0; y < H; ++y) {
+    const size_t off = ((size_t)y * W + x) * D + dbase;
+    load_u8<K>(cv + off, c);
+    if (y == 0) {
+      uint32_t mn = 0xFFFFFFFFu;
+#pragma unroll
+      for (int j = 0; j < K; ++j) { L[j] = c[j]; mn = min(mn, c[j]); }
+      m = __reduce_min_sync(kFull, mn);
+    } else {
+      m = plain_step<K>(L, c, m, P.p1, P.p2, lane);
+    }
+    float dv = kInvalidFloat;
+    if (col_ok && y >= 5 && y <= H - 5 && y < Q.rows) {
+      uint32_t a[K], b[K], e[K], S[K];
+      load_u8<K>(btv + off, a);
+      load_u8<K>(lrv + off, b);
+      load_u8<K>(rlv + off, e);
+#pragma unroll
+      for (int j = 0; j < K; ++j) S[j] = (L[j] & 0xFFu) + a[j] + b[j] + e[j];
+      dv = wta_pixel<K>(S, lane, P.min_d, Q, 0);
+    }
+    if (lane == 0) dout[(size_t)y * W + x] = dv;
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Initial-disparity (pyramid) levels, D = 32: cost with CostAdjust and the per-pixel offset,
+// recurrence realigned by base - last_base (reference cusgm_cc.cu:173-237/294-360,
+// cusgm_ca.cu:1181-1338). All arithmetic uint32 as in the reference.
+// ---------------------------------------------------------------------------------------------
+struct InitParams {
+  int W, H, x0;
+  uint32_t p1;
+  int32_t p1s, p2s, p2_div0;
+  uint32_t invalid_cost;  // 0xFF (9x7) or 127 (5x5)
+  size_t vstride;
+};
+
+// One realigned step. Returns the new minimum; L is replaced.
+__device__ __forceinline__ uint32_t init_step(uint32_t& L, uint32_t c, uint32_t m, int base, int last_base, int lane,
+                                              const InitParams& P) {
+  const int i1 = lane + base - 1 - last_base;
+  const int i2 = lane + base + 1 - last_base;
+  const uint32_t v1 = __shfl_sync(kFull, L, i1 & 31);
+  const uint32_t v2 = __shfl_sync(kFull, L, i2 & 31);
+  const uint32_t a = (i1 >= 0 && i1 < kLevelRange) ? v1 + P.p1 : kInvalidCost;
+  const uint32_t b = (i2 >= 0 && i2 < kLevelRange) ? v2 + P.p1 : kInvalidCost;
+  const int div = abs(last_base - base + 1);
+  const int32_t q = div != 0 ? P.p2s / div : P.p2_div0;
+  const uint32_t l4 = m + (uint32_t)(P.p1s > q ? P.p1s : q);
+  const uint32_t t = min(min(min(L, a), b), l4);
+  L = c + (t - m);
+  return __reduce_min_sync(kFull, L);
+}
+
+template <typename Word>
+__device__ __forceinline__ uint32_t init_cost(const Word* own, const Word* oth, int x, int d, int base, int W,
+                                              int view, uint32_t invalid_cost) {
+  if (view == 0) {
+    const int pos = x - d - base;
+    return (pos > 0 && pos < W) ? ((popc_word((Word)(own[x] ^ oth[pos])) + cost_adjust(d)) & 0xFFu) : invalid_cost;
+  }
+  const int pos = x + d + base;
+  return (popc_word((Word)(own[x] ^ ((pos > 0 && pos < W) ? oth[pos] : oth[0]))) + cost_adjust(d)) & 0xFFu;
+}
+
+template <typename Word>
+__global__ void __launch_bounds__(256) k_hpaths_init(const Word* __restrict__ cs_l, const Word* __restrict__ cs_r,
+                                                     const int16_t* __restrict__ init_l,
+                                                     const int16_t* __restrict__ init_r, uint8_t* __restrict__ cost,
+                                                     uint8_t* __restrict__ lr, uint8_t* __restrict__ rl, InitParams P) {
+  constexpr int D = kLevelRange;
+  const int view = blockIdx.y;
+  const int lane = threadIdx.x;
+  const int wid = threadIdx.y;
+  const int R = blockDim.y >> 1;
+  const int row = wid >> 1;
+  const int dir = wid & 1;
+  const int y = blockIdx.x * R + row;
+  const int W = P.W;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Word* own = reinterpret_cast<Word*>(smem_raw) + (size_t)row * 2 * W;
+  Word* oth = own + W;
+  int16_t* ibase = reinterpret_cast<int16_t*>(reinterpret_cast<Word*>(smem_raw) + (size_t)R * 2 * W) + (size_t)row * W;
+  if (y < P.H) {
+    const Word* g_own = (view == 0 ? cs_l : cs_r) + (size_t)y * W;
+    const Word* g_oth = (view == 0 ? cs_r : cs_l) + (size_t)y * W;
+    const int16_t* g_init = (view == 0 ? init_l : init_r) + (size_t)y * W;
+    for (int i = dir * 32 + lane; i < W; i += 64) {
+      own[i] = g_own[i];
+      oth[i] = g_oth[i];
+      ibase[i] = g_init[i];
+    }
+  }
+  __syncthreads();
+  if (y >= P.H) return;
+  const int len = W - P.x0;
+  if (len <= 0) return;
+  const size_t vo = (size_t)view * P.vstride;
+  uint8_t* out = (dir == 0 ? lr : rl) + vo;
+  uint8_t* cvol = cost + vo;
+  uint32_t L = 0, m = 0;
+  int last_base = 0;
+  for (int s = 0; s < len; ++s) {
+    const int x = dir == 0 ? P.x0 + s : W - 1 - s;
+    const int base = ibase[x];
+    const uint32_t c = init_cost<Word>(own, oth, x, lane, base, W, view, P.invalid_cost);
+    const size_t off = ((size_t)y * W + x) * D + lane;
+    if (dir == 0) cvol[off] = (uint8_t)c;
+    if (s == 0) {
+      L = c;
+      m = __reduce_min_sync(kFull, c);
+      last_base = base;
+      out[off] = (uint8_t)L;
+      continue;
+    }
+    if (base == kInvalidShort) {
+      m = kInvalidCost;
+      continue;
+    }
+    m = init_step(L, c, m, base, last_base, lane, P);
+    last_base = base;
+    out[off] = (uint8_t)L;
+  }
+}
+
+// Vertical scans + WTA at initial-disparity levels (reference cusgm_ca.cu:1263-1338 and
+// Kernel_ComputeDisparityByWTA_Warpfor32 with init, :3425-3512). Both vertical scans start
+// last_base from row 0 (:1291). disp = d* + base + bias; d* <= 1 or d* >= 31 -> INVALID.
+__global__ void __launch_bounds__(256) k_vpaths_wta_init(const uint8_t* __restrict__ cost,
+                                                         const uint8_t* __restrict__ lr,
+                                                         const uint8_t* __restrict__ rl,
+                                                         const int16_t* __restrict__ init_l,
+                                                         const int16_t* __restrict__ init_r, uint8_t* __restrict__ bt,
+                                                         float* __restrict__ disp, InitParams P, WtaParams Q) {
+  constexpr int D = kLevelRange;
+  const int view = blockIdx.y;
+  const int lane = threadIdx.x;
+  const int x = blockIdx.x * blockDim.y + threadIdx.y;
+  const int W = P.W, H = P.H;
+  if (x >= W) return;
+  float* dout = disp + (size_t)view * Q.dstride;
+  if (x < P.x0) {
+    for (int y = lane; y < H; y += 32) dout[(size_t)y * W + x] = kInvalidFloat;
+    return;
+  }
+  const int16_t* ib = view == 0 ? init_l : init_r;
+  const size_t vo = (size_t)view * P.vstride;
+  const uint8_t* cv = cost + vo;
+  uint8_t* btv = bt + vo;
+  uint32_t L = 0, m = 0;
+  int last_base = ib[x];  // row 0 for both directions
+  for (int s = 0; s < H; ++s) {
+    const int y = H - 1 - s;
+    const size_t off = ((size_t)y * W + x) * D + lane;
+    const uint32_t c = cv[off];
+    if (s == 0) {
+      L = c;
+      m = __reduce_min_sync(kFull, c);
+      btv[off] = (uint8_t)L;
+      continue;
+    }
+    const int base = ib[(size_t)y * W + x];
+    if (base == kInvalidShort) { m = kInvalidCost; continue; }
+    m = init_step(L, c, m, base, last_base, lane, P);
+    last_base = base;
+    btv[off] = (uint8_t)L;
+  }
+  __syncwarp();
+  const uint8_t* lrv = lr + vo;
+  const uint8_t* rlv = rl + vo;
+  const bool col_ok = x >= 5 && x <= W - 5;
+  last_base = ib[x];
+  for (int y = 0; y < H; ++y) {
+    const size_t off = ((size_t)y * W + x) * D + lane;
+    const uint32_t c = cv[off];
+    const int base = ib[(size_t)y * W + x];
+    bool skipped = false;
+    if (y == 0) {
+      L = c;
+      m = __reduce_min_sync(kFull, c);
+    } else if (base == kInvalidShort) {
+      m = kInvalidCost;
+      skipped = true;
+    } else {
+      m = init_step(L, c, m, base, last_base, lane, P);
+      last_base = base;
+    }
+    float dv = kInvalidFloat;
+    if (col_ok && y >= 5 && y <= H - 5 && y < Q.rows && base != kInvalidShort && !skipped) {
+      uint32_t S[1];
+      S[0] = (L & 0xFFu) + btv[off] + lrv[off] + rlv[off];
+      dv = wta_pixel<1>(S, lane, base, Q, 1);
+    }
+    if (lane == 0) dout[(size_t)y * W + x] = dv;
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Left-right check (reference Kernel_LRCheck cusgm_ca.cu:3873-3898) and 3x3 median
+// (cusgm_df.cu:16-75, launch :346-355), fused: a 32x8 output tile stages the LR-checked
+// left map with a one-pixel halo in shared memory, then takes the median. The right map
+// is read from a snapshot; failed pixels mark INVALID in dr_out (idempotent stores).
+// Median rows 1..ylim (ylim = min(H-2, 2*ceil((W-2)/2))) and columns 1..W-2.
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ float lr_value(float dl, int x, const float* __restrict__ dr_row, float* dr_out_row, int W,
+                                          float thr) {
+  if (dl == kInvalidFloat) return dl;
+  const float xrf = __fsub_rn((float)x, dl);
+  const int xr = xrf > 0.0f ? (int)__dadd_rn((double)xrf, 0.5) : (int)__dsub_rn((double)xrf, 0.5);
+  if (xr < 0 || xr >= W) return kInvalidFloat;
+  const float dr = dr_row[xr];
+  if (fabsf(__fsub_rn(dl, dr)) > thr) {
+    if (dr_out_row) dr_out_row[xr] = kInvalidFloat;
+    return kInvalidFloat;
+  }
+  return __fdiv_rn(__fadd_rn(dl, dr), 2.0f);
+}
+
+__device__ __forceinline__ void cswap(float& a, float& b) {
+  const float lo = fminf(a, b), hi = fmaxf(a, b);
+  a = lo;
+  b = hi;
+}
+
+__device__ __forceinline__ float median9(float a0, float a1, float a2, float a3, float a4, float a5, float a6,
+                                         float a7, float a8) {
+  // 19 compare-exchanges selecting the middle of 9 (Paeth's median-of-9 network);
+  // disparity values are never NaN, so min/max equal the reference's compare-and-swap.
+  cswap(a1, a2); cswap(a4, a5); cswap(a7, a8);
+  cswap(a0, a1); cswap(a3, a4); cswap(a6, a7);
+  cswap(a1, a2); cswap(a4, a5); cswap(a7, a8);
+  cswap(a0, a3); cswap(a5, a8); cswap(a4, a7);
+  cswap(a3, a6); cswap(a1, a4); cswap(a2, a5);
+  cswap(a4, a7); cswap(a4, a2); cswap(a6, a4);
+  cswap(a4, a2);
+  return a4;
+}
+
+template <bool DoLR, bool DoMedian>
+__global__ void __launch_bounds__(256) k_lr_median(const float* __restrict__ dl, const float* __restrict__ dr,
+                                                   float* __restrict__ dr_out, float* __restrict__ out, int W, int H,
+                                                   float thr) {
+  __shared__ float tile[10][34];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int bx = blockIdx.x * 32, by = blockIdx.y * 8;
+  for (int i = ty * 32 + tx; i < 10 * 34; i += 256) {
+    const int ly = i / 34, lx = i - ly * 34;
+    const int gx = bx + lx - 1, gy = by + ly - 1;
+    float v = kInvalidFloat;
+    if (gx >= 0 && gx < W && gy >= 0 && gy < H) {
+      v = dl[(size_t)gy * W + gx];
+      if (DoLR) {
+        const bool own = lx >= 1 && lx <= 32 && ly >= 1 && ly <= 8;  // marks only from the tile's own pixels
+        v = lr_value(v, gx, dr + (size_t)gy * W, (own && dr_out) ? dr_out + (size_t)gy * W : nullptr, W, thr);
+      }
+    }
+    tile[ly][lx] = v;
+  }
+  __syncthreads();
+  const int x = bx + tx, y = by + ty;
+  if (x >= W || y >= H) return;
+  float v = tile[ty + 1][tx + 1];
+  if (DoMedian) {
+    int ylim = 2 * ((W - 1) / 2);
+    ylim = ylim > H - 2 ? H - 2 : ylim;
+    if (x >= 1 && x <= W - 2 && y >= 1 && y <= ylim) {
+      v = median9(tile[ty][tx], tile[ty][tx + 1], tile[ty][tx + 2], tile[ty + 1][tx], tile[ty + 1][tx + 1],
+                  tile[ty + 1][tx + 2], tile[ty + 2][tx], tile[ty + 2][tx + 1], tile[ty + 2][tx + 2]);
+    }
+  }
+  out[(size_t)y * W + x] = v;
+}
+
+// Dilation of INVALID pixels (reference Kernel_Dilation, cusgm_df.cu:197-222).
+template <typename T>
+__global__ void __launch_bounds__(256) k_dilation(const T* __restrict__ in, T* __restrict__ out, int W, int H,
+                                                  int wth) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= W || y >= H) return;
+  T v = in[(size_t)y * W + x];
+  if ((float)v == kInvalidFloat || (float)v == (float)kInvalidShort) {
+    if (x > wth && x < W - wth && y > wth && y < H - wth) {
+      for (int dx = -wth; dx <= wth; ++dx)
+        for (int dy = -wth; dy <= wth; ++dy) {
+          const T u = in[(size_t)(y + dy) * W + x + dx];
+          if (u > v) v = u;
+        }
+    }
+  }
+  out[(size_t)y * W + x] = v;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Small-region removal (reference StereoCudaImpl.cpp:32-125, 463-498) as connected-component
+// labelling: union-find over 4-neighbours within a strip, roots = smallest pixel index.
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ bool peaks_adjacent(float a, float b, int abs_mode) {
+  const float d = __fsub_rn(a, b);
+  if (abs_mode == kPeaksAbsFloat) return fabsf(d) <= 1.0f;
+  const int t = (int)d;  // truncation toward zero, as int abs((int)x) in the g++ build
+  return (t < 0 ? -t : t) <= 1;
+}
+
+// Root of p. Reads go to L2 (ld.global.cg): parents are rewritten by atomics from other SMs.
+__device__ __forceinline__ int cc_find(const int* label, int p) {
+  int q = __ldcg(label + p);
+  while (q != p) {
+    p = q;
+    q = __ldcg(label + p);
+  }
+  return p;
+}
+
+__global__ void k_cc_init(const float* __restrict__ disp, int* __restrict__ label, int* __restrict__ count, int W,
+                          int H, int rows) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= W * H) return;
+  const int y = i / W;
+  label[i] = (y < rows && disp[i] != kInvalidFloat) ? i : -1;
+  count[i] = 0;
+}
+
+__global__ void k_cc_union(const float* __restrict__ disp, int* label, int W, int H, int tiles,
+                           int rows, int abs_mode) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= W * H) return;
+  const int y = i / W, x = i - y * W;
+  if (y >= rows || label[i] < 0) return;
+  const float v = disp[i];
+  // right and down neighbours (the down one only inside the same strip)
+  for (int n = 0; n < 2; ++n) {
+    int q;
+    if (n == 0) {
+      if (x + 1 >= W) continue;
+      q = i + 1;
+    } else {
+      if (y + 1 >= rows || (y + 1) / tiles != y / tiles) continue;
+      q = i + W;
+    }
+    if (disp[q] == kInvalidFloat || !peaks_adjacent(disp[q], v, abs_mode)) continue;
+    int a = i, b = q;
+    while (true) {
+      a = cc_find(label, a);
+      b = cc_find(label, b);
+      if (a == b) break;
+      if (a > b) { const int t = a; a = b; b = t; }
+      const int old = atomicMin(&label[b], a);
+      if (old == b) break;
+      b = old;
+    }
+  }
+}
+
+__global__ void k_cc_count(int* label, int* __restrict__ count, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || label[i] < 0) return;
+  const int r = cc_find(label, i);
+  label[i] = r;
+  atomicAdd(&count[r], 1);
+}
+
+__global__ void k_cc_filter(float* __restrict__ disp, const int* __restrict__ label, const int* __restrict__ count,
+                            int W, int H, int tiles, float ratio) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= W * H || label[i] < 0) return;
+  // every processed strip has exactly `tiles` rows, so the threshold is the same for all of them
+  const int threshold = (int)__fmul_rn((float)(W * tiles), ratio);
+  if (count[label[i]] < threshold) disp[i] = kInvalidFloat;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Pyramid helpers (reference FasterStereoCuda.cpp:114-166, cusgm_util.cu:47-59).
+// ---------------------------------------------------------------------------------------------
+// Level image = full-resolution image sampled at (x << shift, y << shift); both views.
+__global__ void k_decimate(const uint8_t* __restrict__ full_l, const uint8_t* __restrict__ full_r,
+                           uint8_t* __restrict__ lvl_l, uint8_t* __restrict__ lvl_r, int W0, int w, int h,
+                           int shift) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= w || y >= h) return;
+  const size_t src = ((size_t)y << shift) * W0 + ((size_t)x << shift);
+  lvl_l[(size_t)y * w + x] = full_l[src];
+  lvl_r[(size_t)y * w + x] = full_r[src];
+}
+
+// Initial disparity of the next finer level: even rows (except the last) from cur at the flat
+// index (y/2)*(width/2) + x/2 (INVALID past the end of cur); odd rows and the last row copy the
+// row above.
+__global__ void k_init_next_level(const float* __restrict__ cur, long ncur, int16_t* __restrict__ next, int width,
+                                  int height) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= width || y >= height) return;
+  int ys = y;
+  if (y % 2 == 1 || y == height - 1) ys = y - 1;
+  if (ys % 2 == 1) ys -= 1;  // last row with an even index copies an odd row, whose source is one more up
+  if (ys < 0) {
+    next[(size_t)y * width + x] = kInvalidShort;
+    return;
+  }
+  const long idx = (long)(ys >> 1) * (width >> 1) + (x >> 1);
+  const float d = idx < ncur ? cur[idx] : kInvalidFloat;
+  next[(size_t)y * width + x] =
+      d != kInvalidFloat ? (int16_t)(int)__fsub_rn(__fmul_rn(2.0f, d), (float)(kLevelRange >> 1)) : kInvalidShort;
+}
+
+// Right-view initial disparities: cleared to INVALID, then a scatter in which the largest
+// source x wins for every target (the reference's concurrent scatter made deterministic).
+__global__ void k_right_init_scatter(const int16_t* __restrict__ init_l, unsigned* __restrict__ key, int W, int H) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= W) return;
+  const int16_t xl = (int16_t)x;
+  const int16_t il = (int16_t)(init_l[(size_t)y * W + x] + (kLevelRange >> 1));
+  const int t = xl - il;
+  if (t > 0 && t < W) {
+    const int16_t val = (int16_t)(il - (kLevelRange >> 1));
+    atomicMax(&key[(size_t)y * W + t], ((unsigned)(x + 1) << 16) | (uint16_t)val);
+  }
+}
+
+__global__ void k_right_init_decode(const unsigned* __restrict__ key, int16_t* __restrict__ out, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const unsigned k = key[i];
+  out[i] = k == 0 ? kInvalidShort : (int16_t)(uint16_t)(k & 0xFFFFu);
+}
+
+}  // namespace sgm

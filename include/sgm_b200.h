@@ -1,0 +1,170 @@
+/*
+ * sgm_b200.h -- C ABI of the B200 semi-global-matching stereo engine.
+ *
+ * Drop-in boundary for the stereo path of ethan-li-coding/FasterStereoCuda.
+ * Every entry point below names the reference interface it replaces
+ * (paths are relative to the reference project). Plain pointers and sizes
+ * only; no C++ or torch types cross this boundary.
+ *
+ * Status codes: 0 = success, negative = failure (see sgm_status_t).
+ * Threading: one handle is one matcher; calls on a handle must not overlap.
+ * Invalid disparity value: -999999.0f. Invalid initial disparity: -32768.
+ */
+#ifndef SGM_B200_H_
+#define SGM_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+#ifndef __cplusplus
+#include <stdbool.h>
+#endif
+
+#if defined(_WIN32)
+#define SGM_API __declspec(dllexport)
+#else
+#define SGM_API __attribute__((visibility("default")))
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  SGM_OK = 0,
+  SGM_ERR_ARG = -1,         /* bad argument (size, range, null pointer, option combination) */
+  SGM_ERR_STATE = -2,       /* handle not initialised / already released */
+  SGM_ERR_CUDA = -3,        /* CUDA runtime error (message in sgm_last_error) */
+  SGM_ERR_UNSUPPORTED = -4, /* valid in the reference API but not supported by this engine */
+  SGM_ERR_NOMEM = -5        /* device or host allocation failed */
+} sgm_status_t;
+
+/* Same member order, types and layout as the reference's CuSGMOption
+ * (SgmStereoCuda/sgm_types.h:21-65), so a CuSGMOption* may be passed directly. */
+typedef struct sgm_option_s {
+  int32_t p1;
+  int32_t p2_init;
+  int32_t p2_max;
+  int32_t cs_type;        /* 0 = census 5x5, 1 = census 9x7 */
+  int32_t num_paths;
+  bool do_median_filter;
+  bool do_lr_check;
+  float lr_threshold;
+  float unique_threshold;
+  bool using_constant_p2;
+  bool do_remove_peaks;
+  float peaks_ratio_threshold;
+  int32_t post_filter_type; /* 0 = none (only value supported) */
+  int32_t morphology_type;  /* 0 = none, 2 = dilation */
+} sgm_option_t;
+
+/* Same layout as StereoROI_T (SgmStereoCuda/sgm_types.h:89-92). */
+typedef struct sgm_roi_s {
+  int32_t x, y, w, h;
+} sgm_roi_t;
+
+/* Choices the reference leaves to thread scheduling or to its compiler; fixed here. */
+typedef struct sgm_ext_options_s {
+  int32_t tie_rule;       /* WTA tie break, plain path: 0 lowest d, 1 highest d, 2 highest lane, 3 lowest lane */
+  int32_t init_tie_rule;  /* the same at initial-disparity (pyramid) levels */
+  int32_t peaks_strips;   /* strips of small-region removal; <= 0: hardware threads * 3 / 4 */
+  int32_t peaks_abs_mode; /* region test: 0 |(int)(a-b)| <= 1 (g++ build), 1 |a-b| <= 1.0f (MSVC build) */
+  int32_t p2_div0;        /* P2 / 0 at initial-disparity levels */
+} sgm_ext_options_t;
+
+typedef struct sgm_engine* sgm_handle_t;
+
+/* StereoCuda::StereoCuda() -- SgmStereoCuda/StereoCuda.cpp:4-7 */
+SGM_API int sgm_create(sgm_handle_t* out);
+/* StereoCuda::~StereoCuda() -- SgmStereoCuda/StereoCuda.cpp:9-16 */
+SGM_API int sgm_destroy(sgm_handle_t h);
+/* StereoCuda::Init -- SgmStereoCuda/StereoCuda.h:31, StereoCudaImpl.cpp:128-261.
+ * Allocates every device buffer for (width, height, min_disparity, disp_range). */
+SGM_API int sgm_init(sgm_handle_t h, int32_t width, int32_t height, int32_t min_disparity, int32_t disp_range,
+                     const sgm_option_t* option, int32_t print_log);
+/* No counterpart in the reference: sets the rules in sgm_ext_options_t (before or after init). */
+SGM_API int sgm_set_ext_options(sgm_handle_t h, const sgm_ext_options_t* ext);
+SGM_API int sgm_get_ext_options(sgm_handle_t h, sgm_ext_options_t* ext);
+/* StereoCuda::Match -- SgmStereoCuda/StereoCuda.h:44, StereoCudaImpl.cpp:507-546.
+ * Host buffers of width*height elements. disp_right, init_disp_left, roi_* may be NULL.
+ * Returns after the disparity has been copied back (synchronous, like the reference). */
+SGM_API int sgm_match(sgm_handle_t h, const uint8_t* img_left, const uint8_t* img_right, float* disp_left,
+                      float* disp_right, const int16_t* init_disp_left, const sgm_roi_t* roi_left,
+                      const sgm_roi_t* roi_right);
+/* No counterpart in the reference: the same match on device-resident buffers
+ * (dense width*height arrays), enqueued on `stream` (a cudaStream_t, NULL = the
+ * handle's own stream) without synchronising. */
+SGM_API int sgm_match_device(sgm_handle_t h, const uint8_t* d_left, const uint8_t* d_right, float* d_disp_left,
+                             float* d_disp_right, const int16_t* d_init_disp_left, void* stream);
+/* StereoCuda::Release -- SgmStereoCuda/StereoCuda.h:75, StereoCudaImpl.cpp:281-332 */
+SGM_API int sgm_release(sgm_handle_t h);
+/* StereoCuda::SetMinDisparity / GetDispartyRange -- SgmStereoCuda/StereoCuda.h:71-72 */
+SGM_API int sgm_set_min_disparity(sgm_handle_t h, int32_t min_disparity);
+SGM_API int32_t sgm_get_disparity_range(sgm_handle_t h);
+/* StereoCuda::GetRoiFromDispMap -- SgmStereoCuda/StereoCudaImpl.cpp:585-628 */
+SGM_API void sgm_roi_from_disp_map(const float* disp, int32_t width, int32_t height, sgm_roi_t* roi);
+/* StereoCuda::get_invad_float / get_invad_short / get_level_range -- StereoCuda.h:87-91 */
+SGM_API float sgm_invalid_float(void);
+SGM_API int16_t sgm_invalid_short(void);
+SGM_API int16_t sgm_level_range(void);
+/* StereoCuda::MallocPageLockedPtr / FreePageLockedPtr -- StereoCuda.h:94-97 */
+SGM_API int sgm_malloc_page_locked(void** ptr, size_t size);
+SGM_API int sgm_free_page_locked(void* ptr);
+/* No counterpart in the reference: message of the last failure on h (NULL h: process-wide). */
+SGM_API const char* sgm_last_error(sgm_handle_t h);
+/* No counterpart in the reference: number of kernel launches issued by the last match on h. */
+SGM_API int64_t sgm_kernel_launches(sgm_handle_t h);
+
+/* No counterpart in the reference: copies an internal stage buffer of the last match to host
+ * memory, for stage-by-stage parity tests. `which`: 0/1 census left/right (uint64 per pixel,
+ * 5x5 zero-extended), 2 cost, 3 left->right, 4 right->left, 5 bottom->top path costs
+ * (uint8 [H][W][D]) and 6 the WTA disparity (float [H][W]) of view `view` (0 left, 1 right).
+ * `bytes` must equal the buffer size. Synchronises the handle's stream. */
+SGM_API int sgm_debug_read(sgm_handle_t h, int32_t which, int32_t view, void* dst, size_t bytes);
+
+/* No counterpart in the reference: per-kernel timing with CUDA events recorded on the launching
+ * stream around every launch of every handle in the process. Enabling resets the counters. */
+SGM_API int sgm_profile_enable(int32_t enable);
+/* Writes {"kernel": {"launches": n, "ms": total}, ...} into buf; returns 0, or the size needed
+ * (including the terminating NUL) when cap is too small. Synchronises on the recorded events. */
+SGM_API int sgm_profile_read(char* buf, size_t cap);
+
+/* ---------------- pyramid matcher (FasterStereoCuda) ---------------- */
+
+/* Same layout as FasterStereoCuda::StereoOption1 (FasterStereoCuda/FasterStereoCuda.h:39-51). */
+typedef struct sgm_pyr_option1_s {
+  int32_t width, height, min_disp, max_disp, num_layers;
+  bool do_lr_check, do_rm_peaks, do_smooth;
+} sgm_pyr_option1_t;
+
+/* No counterpart in the reference: replaces the census type and penalties that
+ * SetSgmParameters (FasterStereoCuda.cpp:169-199) hard-codes for every level. */
+typedef struct sgm_level_override_s {
+  int32_t cs_type, p1, p2;
+} sgm_level_override_t;
+
+typedef struct sgm_pyramid* sgm_pyr_handle_t;
+
+/* FasterStereoCuda::FasterStereoCuda / ~FasterStereoCuda -- FasterStereoCuda.cpp:693-703 */
+SGM_API int sgm_pyr_create(sgm_pyr_handle_t* out);
+SGM_API int sgm_pyr_destroy(sgm_pyr_handle_t h);
+/* FasterStereoCuda::Init -- FasterStereoCuda.h:95, HierSgmCudaImpl::Init FasterStereoCuda.cpp:201-295.
+ * override may be NULL (reference per-level parameters). */
+SGM_API int sgm_pyr_init(sgm_pyr_handle_t h, const sgm_pyr_option1_t* option, const sgm_level_override_t* override_,
+                         const sgm_ext_options_t* ext);
+/* FasterStereoCuda::Match -- FasterStereoCuda.h:114, HierSgmCudaImpl::Match FasterStereoCuda.cpp:408-529.
+ * All levels run on the device; no host round trip between levels. */
+SGM_API int sgm_pyr_match(sgm_pyr_handle_t h, const uint8_t* img_left, const uint8_t* img_right, float* disp);
+/* No counterpart in the reference: device-resident variant, enqueued on `stream` without synchronising. */
+SGM_API int sgm_pyr_match_device(sgm_pyr_handle_t h, const uint8_t* d_left, const uint8_t* d_right, float* d_disp,
+                                 void* stream);
+/* FasterStereoCuda::Release -- FasterStereoCuda.h:105 */
+SGM_API int sgm_pyr_release(sgm_pyr_handle_t h);
+/* No counterpart in the reference: level geometry chosen by init (for tests and tools). */
+SGM_API int sgm_pyr_level_info(sgm_pyr_handle_t h, int32_t level, int32_t* width, int32_t* height,
+                               int32_t* min_disp, int32_t* disp_range);
+SGM_API int64_t sgm_pyr_kernel_launches(sgm_pyr_handle_t h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

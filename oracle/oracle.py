@@ -1,0 +1,227 @@
+"""ctypes binding of the C oracle (oracle/sgm_oracle.c) -- test infrastructure only.
+
+Every function returns numpy arrays in the dense layouts described in sgm_oracle.h.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field, fields
+from pathlib import Path
+
+import numpy as np
+
+_LIB = Path(__file__).resolve().parent / "_build" / "liborc.so"
+_lib = None
+
+INVALID_FLOAT = np.float32(-999999.0)
+INVALID_SHORT = np.int16(-32768)
+
+
+class _Cfg(C.Structure):
+    _fields_ = [(n, t) for n, t in [
+        ("width", C.c_int32), ("height", C.c_int32), ("min_disp", C.c_int32), ("disp_range", C.c_int32),
+        ("cs_type", C.c_int32), ("p1", C.c_int32), ("p2", C.c_int32), ("uniqueness", C.c_float),
+        ("do_lr_check", C.c_int32), ("lr_threshold", C.c_float), ("do_median", C.c_int32),
+        ("morphology_dilation", C.c_int32), ("do_remove_peaks", C.c_int32), ("peaks_ratio", C.c_float),
+        ("peaks_strips", C.c_int32), ("peaks_abs_mode", C.c_int32), ("tie_rule", C.c_int32),
+        ("init_tie_rule", C.c_int32), ("p2_div0", C.c_int32), ("threads", C.c_int32)]]
+
+
+class _PyrCfg(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in (
+        "width", "height", "min_disp", "max_disp", "num_layers", "do_lr_check", "do_rm_peaks", "do_smooth",
+        "override_enable", "cs_type", "p1", "p2", "peaks_strips", "peaks_abs_mode", "tie_rule", "init_tie_rule",
+        "p2_div0", "threads")]
+
+
+@dataclass
+class Config:
+    """One matching level (mirrors orc_config_t)."""
+    width: int
+    height: int
+    min_disp: int = 0
+    disp_range: int = 64
+    cs_type: int = 1
+    p1: int = 10
+    p2: int = 150
+    uniqueness: float = 0.95
+    do_lr_check: int = 1
+    lr_threshold: float = 1.0
+    do_median: int = 1
+    morphology_dilation: int = 0
+    do_remove_peaks: int = 0
+    peaks_ratio: float = 0.0005
+    peaks_strips: int = 6
+    peaks_abs_mode: int = 0
+    tie_rule: int = 0
+    init_tie_rule: int = 0
+    p2_div0: int = -1
+    threads: int = 0
+
+    def c(self) -> _Cfg:
+        s = _Cfg()
+        for f in fields(self):
+            setattr(s, f.name, getattr(self, f.name))
+        return s
+
+
+@dataclass
+class PyrConfig:
+    width: int
+    height: int
+    min_disp: int = 0
+    max_disp: int = 64
+    num_layers: int = 3
+    do_lr_check: int = 1
+    do_rm_peaks: int = 1
+    do_smooth: int = 0
+    override_enable: int = 1
+    cs_type: int = 1
+    p1: int = 10
+    p2: int = 150
+    peaks_strips: int = 6
+    peaks_abs_mode: int = 0
+    tie_rule: int = 0
+    init_tie_rule: int = 0
+    p2_div0: int = -1
+    threads: int = 0
+
+    def c(self) -> _PyrCfg:
+        s = _PyrCfg()
+        for f in fields(self):
+            setattr(s, f.name, int(getattr(self, f.name)))
+        return s
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not _LIB.exists():
+            from fasterstereocuda_b200.build import build_oracle
+            build_oracle()
+        _lib = C.CDLL(str(_LIB))
+        vp, i32 = C.c_void_p, C.c_int32
+        _lib.orc_match_dump.argtypes = [C.POINTER(_Cfg), vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+        _lib.orc_match_dump.restype = i32
+        _lib.orc_pyr_match.argtypes = [C.POINTER(_PyrCfg), vp, vp, vp]
+        _lib.orc_pyr_match.restype = i32
+        _lib.orc_pyr_level_config.argtypes = [C.POINTER(_PyrCfg), i32, C.POINTER(_Cfg)]
+        _lib.orc_pyr_level_config.restype = i32
+        _lib.orc_census.argtypes = [vp, i32, i32, i32, i32, vp]
+        _lib.orc_remove_peaks.argtypes = [vp, i32, i32, i32, C.c_float, i32]
+        _lib.orc_remove_peaks.restype = i32
+        _lib.orc_remove_peaks_strip.argtypes = [vp, i32, i32, i32, i32]
+        _lib.orc_remove_peaks_strip.restype = i32
+        _lib.orc_zoom_half.argtypes = [vp, i32, i32, vp]
+        _lib.orc_init_next_level.argtypes = [vp, i32, i32, vp, i32, i32]
+        _lib.orc_median3x3.argtypes = [vp, vp, i32, i32]
+        _lib.orc_dilation.argtypes = [vp, vp, i32, i32, i32]
+        _lib.orc_lr_check.argtypes = [vp, vp, vp, i32, i32, C.c_float]
+        _lib.orc_cost_adjust.argtypes = [i32]
+        _lib.orc_cost_adjust.restype = C.c_uint8
+        _lib.orc_set_threads.argtypes = [i32]
+        _lib.orc_max_threads.restype = i32
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+def match(cfg: Config, left: np.ndarray, right: np.ndarray, init: np.ndarray | None = None,
+          dump: bool = False, want_right: bool = False) -> dict:
+    """StereoCuda::Match restated. Returns a dict with 'disp' (and stage buffers when dump)."""
+    W, H, D = cfg.width, cfg.height, cfg.disp_range
+    left = np.ascontiguousarray(left, np.uint8)
+    right = np.ascontiguousarray(right, np.uint8)
+    out = {"disp": np.empty((H, W), np.float32)}
+    if want_right:
+        out["disp_r"] = np.empty((H, W), np.float32)
+    if dump:
+        out.update(census_l=np.empty((H, W), np.uint64), census_r=np.empty((H, W), np.uint64),
+                   cost=np.empty((H, W, D), np.uint8), paths=np.empty((4, H, W, D), np.uint8),
+                   wta_l=np.empty((H, W), np.float32), wta_r=np.empty((H, W), np.float32))
+    g = out.get
+    init_c = None if init is None else np.ascontiguousarray(init, np.int16)
+    rc = lib().orc_match_dump(C.byref(cfg.c()), _p(left), _p(right), _p(init_c), _p(g("census_l")),
+                              _p(g("census_r")), _p(g("cost")), _p(g("paths")), _p(g("wta_l")), _p(g("wta_r")),
+                              _p(out["disp"]), _p(g("disp_r")))
+    if rc != 0:
+        raise RuntimeError(f"oracle match failed ({rc})")
+    return out
+
+
+def pyr_match(pc: PyrConfig, left: np.ndarray, right: np.ndarray) -> np.ndarray:
+    disp = np.empty((pc.height, pc.width), np.float32)
+    rc = lib().orc_pyr_match(C.byref(pc.c()), _p(np.ascontiguousarray(left, np.uint8)),
+                             _p(np.ascontiguousarray(right, np.uint8)), _p(disp))
+    if rc != 0:
+        raise RuntimeError(f"oracle pyramid match failed ({rc})")
+    return disp
+
+
+def pyr_level_config(pc: PyrConfig, level: int) -> Config:
+    c = _Cfg()
+    if lib().orc_pyr_level_config(C.byref(pc.c()), level, C.byref(c)) != 0:
+        raise IndexError(level)
+    return Config(**{f.name: getattr(c, f.name) for f in fields(Config)})
+
+
+def census(img: np.ndarray, cs_type: int, is_right: bool) -> np.ndarray:
+    img = np.ascontiguousarray(img, np.uint8)
+    out = np.empty(img.shape, np.uint64)
+    lib().orc_census(_p(img), img.shape[1], img.shape[0], cs_type, int(is_right), _p(out))
+    return out
+
+
+def remove_peaks(disp: np.ndarray, strips: int, ratio: float, abs_mode: int = 0) -> tuple[np.ndarray, int]:
+    d = np.ascontiguousarray(disp, np.float32).copy()
+    n = lib().orc_remove_peaks(_p(d), d.shape[1], d.shape[0], strips, ratio, abs_mode)
+    return d, n
+
+
+def remove_peaks_strip(disp: np.ndarray, threshold: int, abs_mode: int = 0) -> tuple[np.ndarray, int]:
+    d = np.ascontiguousarray(disp, np.float32).copy()
+    n = lib().orc_remove_peaks_strip(_p(d), d.shape[1], d.shape[0], threshold, abs_mode)
+    return d, n
+
+
+def zoom_half(img: np.ndarray) -> np.ndarray:
+    img = np.ascontiguousarray(img, np.uint8)
+    h, w = img.shape
+    out = np.empty((h // 2, w // 2), np.uint8)
+    lib().orc_zoom_half(_p(img), w, h, _p(out))
+    return out
+
+
+def init_next_level(cur: np.ndarray, width: int, height: int) -> np.ndarray:
+    cur = np.ascontiguousarray(cur, np.float32)
+    out = np.empty((height, width), np.int16)
+    lib().orc_init_next_level(_p(cur), cur.shape[1], cur.shape[0], _p(out), width, height)
+    return out
+
+
+def median3x3(d: np.ndarray) -> np.ndarray:
+    d = np.ascontiguousarray(d, np.float32)
+    out = np.empty_like(d)
+    lib().orc_median3x3(_p(d), _p(out), d.shape[1], d.shape[0])
+    return out
+
+
+def dilation(d: np.ndarray, wnd: int) -> np.ndarray:
+    d = np.ascontiguousarray(d, np.float32)
+    out = np.empty_like(d)
+    lib().orc_dilation(_p(d), _p(out), d.shape[1], d.shape[0], wnd)
+    return out
+
+
+def cost_adjust(d: int) -> int:
+    return lib().orc_cost_adjust(d)
+
+
+def set_threads(n: int) -> None:
+    lib().orc_set_threads(n)
+
+
+def max_threads() -> int:
+    return lib().orc_max_threads()

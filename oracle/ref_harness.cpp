@@ -1,0 +1,234 @@
+// Reference dump harness -- TEST INFRASTRUCTURE ONLY.
+//
+// Compiled by oracle/build_ref.sh against the reference's own headers and linked with the
+// reference built from its sources (oracle/_ref/libsgmref.so). It drives the reference's
+// classes exactly as StereoCudaImpl::Match does and copies every stage buffer out, so the
+// oracle can be checked against the reference itself. Access to the reference's private
+// members comes from compiling this file with -Dprivate=public.
+//
+// Safety: the reference writes up to 3 floats past the end of each disparity row (WTA grid
+// rounding) and reads one float past it (LR check, x == width); the initial-disparity WTA
+// reads up to 3 int16 past each row. ref_match_dump() refuses a case unless the pitched
+// allocations leave that much padding, and it refuses the kernels that index shared memory
+// past their allocation (D = 32 without initial disparities, D = 128, D = 256).
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+#include "StereoCudaImpl.h"
+#include "cusgm_ca.cuh"
+#include "cusgm_cc.cuh"
+#include "cusgm_df.h"
+#include "FasterStereoCuda.h"
+
+// Reference host functions (StereoCudaImpl.cpp:32, FasterStereoCuda.cpp:114 and :138).
+sint32 RemovePeaks(float32* disp_map, sint32* segid, sint32 w, sint32 h, sint32 threshold);
+void Zoom(const unsigned char* src, unsigned char* dst, int w_src, int h_src, int scale_x, int scale_y);
+int ComputeInitDispInNextLevel(float* cur, short* next, int width, int height);
+
+extern "C" {
+
+struct ref_case_t {
+  int32_t width, height, min_disp, disp_range;
+  int32_t cs_type, p1, p2;
+  float uniqueness;
+  int32_t do_lr_check;
+  float lr_threshold;
+  int32_t do_median;
+  int32_t morphology;  // 0 none, 2 dilation
+  int32_t do_remove_peaks;
+  float peaks_ratio;
+};
+
+int ref_remove_peaks(float* disp, int32_t* segid, int w, int h, int threshold) {
+  memset(segid, 0, sizeof(int32_t) * (size_t)w * h);
+  return RemovePeaks(disp, segid, w, h, threshold);
+}
+
+void ref_zoom_half(const uint8_t* src, uint8_t* dst, int w, int h) { Zoom(src, dst, w, h, 2, 2); }
+
+int ref_init_next_level(float* cur, int16_t* next, int width, int height) {
+  return ComputeInitDispInNextLevel(cur, next, width, height);
+}
+
+int ref_hardware_threads_peaks(void) {
+  // the strip count StereoCudaImpl::Init derives (StereoCudaImpl.cpp:234)
+  return (int)(std::thread::hardware_concurrency() * 3 / 4);
+}
+
+static const char* g_msg = "";
+const char* ref_last_message(void) { return g_msg; }
+
+static bool padding_ok(size_t pitch, size_t row_bytes, size_t extra) { return pitch >= row_bytes + extra; }
+
+static void copy_pitched_volume(const cudaPitchedPtr& p, int W, int H, int D, uint8_t* out) {
+  // cudaMalloc3D layout of the reference: (pitch, ceil(W/ppp), H), ppp = pitch / D pixels per pitch row
+  const int ppp = (int)(p.pitch / D);
+  const size_t slice = p.pitch * p.ysize;
+  std::vector<uint8_t> host(slice * H);
+  cudaMemcpy(host.data(), p.ptr, host.size(), cudaMemcpyDeviceToHost);
+  for (int y = 0; y < H; ++y)
+    for (int x = 0; x < W; ++x) {
+      const uint8_t* src = host.data() + y * slice + (size_t)(x / ppp) * p.pitch + (size_t)(x % ppp) * D;
+      memcpy(out + ((size_t)y * W + x) * D, src, D);
+    }
+}
+
+static void clear_pitched_volume(const cudaPitchedPtr& p, int H) { cudaMemset(p.ptr, 0, p.pitch * p.ysize * H); }
+
+static CuSGMOption make_option(const ref_case_t* c, bool lr, bool median, bool peaks, int morph) {
+  CuSGMOption o;
+  o.p1 = c->p1;
+  o.p2_init = c->p2;
+  o.p2_max = 64;
+  o.cs_type = c->cs_type ? CuSGMOption::CS_9x7 : CuSGMOption::CS_5x5;
+  o.num_paths = 4;
+  o.do_median_filter = median;
+  o.do_lr_check = lr;
+  o.lr_threshold = c->lr_threshold;
+  o.unique_threshold = c->uniqueness;
+  o.using_constant_p2 = true;
+  o.do_remove_peaks = peaks;
+  o.peaks_ratio_threshold = c->peaks_ratio;
+  o.post_filter_type = CuSGMOption::PF_NONE;
+  o.morphology_type = morph == 2 ? CuSGMOption::MP_DILATION : CuSGMOption::MP_NONE;
+  return o;
+}
+
+static int check_case(const ref_case_t* c, bool with_init) {
+  if (c->width < 16 || c->height < 16) { g_msg = "size too small"; return -1; }
+  if (!(c->disp_range == 64 || (c->disp_range == 32 && with_init))) {
+    g_msg = "only D=64, or D=32 with initial disparities, are run (other widths index shared memory out of range)";
+    return -1;
+  }
+  if (with_init && c->min_disp > 0) { g_msg = "initial disparities need min_disp <= 0"; return -1; }
+  return 0;
+}
+
+// Stage dumps of one case. Any output pointer may be NULL.
+//   run A (LR, median, peaks off): census_l/census_r, cost_lr, paths_lr, wta_l
+//   run B (LR on, median off):     cost_rl, paths_rl, lr_l (left after LR), lr_r (right after marks)
+//   run C (the case's options):    disp_l, disp_r
+int ref_match_dump(const ref_case_t* c, const uint8_t* left, const uint8_t* right, const int16_t* init,
+                   uint64_t* census_l, uint64_t* census_r, uint8_t* cost_lr, uint8_t* paths_lr, float* wta_l,
+                   uint8_t* cost_rl, uint8_t* paths_rl, float* lr_l, float* lr_r, float* disp_l, float* disp_r) {
+  if (check_case(c, init != nullptr)) return -1;
+  const int W = c->width, H = c->height, D = c->disp_range;
+  std::vector<uint8_t> L(left, left + (size_t)W * H), R(right, right + (size_t)W * H);
+  std::vector<int16_t> I;
+  if (init) I.assign(init, init + (size_t)W * H);
+  std::vector<float> tmp_l((size_t)W * H), tmp_r((size_t)W * H);
+  for (int run = 0; run < 3; ++run) {
+    const bool lr = run == 0 ? false : (run == 1 ? true : c->do_lr_check != 0);
+    const bool median = run == 2 ? c->do_median != 0 : false;
+    const bool peaks = run == 2 ? c->do_remove_peaks != 0 : false;
+    const int morph = run == 2 ? c->morphology : 0;
+    StereoCudaImpl impl;
+    if (!impl.Init(W, H, c->min_disp, D, make_option(c, lr, median, peaks, morph), false)) {
+      g_msg = "reference Init failed";
+      return -2;
+    }
+    const size_t dp = impl.aggregator_->dp_psize_;
+    const size_t wta_extra = 4 * sizeof(float);  // up to 3 floats written past a row, 1 read
+    if (!padding_ok(dp, (size_t)W * sizeof(float), wta_extra) ||
+        (init && !padding_ok(impl.idp_psize_, (size_t)W * sizeof(int16_t), 3 * sizeof(int16_t)))) {
+      g_msg = "pitch padding too small for the reference's row overrun";
+      impl.Release();
+      return -3;
+    }
+    // known contents for everything the reference leaves unwritten
+    clear_pitched_volume(*impl.computor_->cost_, H);
+    for (int k = 0; k < 4; ++k) clear_pitched_volume(impl.aggregator_->cost_aggr_dir_[k], H);
+    cudaMemset(impl.aggregator_->disp_map_, 0, dp * H);
+    cudaMemset(impl.aggregator_->disp_map_r_, 0, dp * H);
+    cudaDeviceSynchronize();
+    const bool ok = impl.Match(L.data(), R.data(), tmp_l.data(), tmp_r.data(), init ? I.data() : nullptr);
+    if (cudaDeviceSynchronize() != cudaSuccess || !ok) {
+      g_msg = "reference Match failed";
+      impl.Release();
+      return -4;
+    }
+    if (run == 0) {
+      const size_t cs = impl.computor_->cs_psize_;
+      const int bytes = c->cs_type ? 8 : 4;
+      std::vector<uint8_t> buf(cs * H);
+      for (int view = 0; view < 2; ++view) {
+        uint64_t* dst = view == 0 ? census_l : census_r;
+        if (!dst) continue;
+        cudaMemcpy(buf.data(), view == 0 ? impl.computor_->census_left_ : impl.computor_->census_right_, buf.size(),
+                   cudaMemcpyDeviceToHost);
+        for (int y = 0; y < H; ++y)
+          for (int x = 0; x < W; ++x) {
+            uint64_t v = 0;
+            memcpy(&v, buf.data() + y * cs + (size_t)x * bytes, bytes);
+            dst[(size_t)y * W + x] = v;
+          }
+      }
+      if (cost_lr) copy_pitched_volume(*impl.computor_->cost_, W, H, D, cost_lr);
+      if (paths_lr)
+        for (int k = 0; k < 4; ++k)
+          copy_pitched_volume(impl.aggregator_->cost_aggr_dir_[k], W, H, D, paths_lr + (size_t)k * W * H * D);
+      if (wta_l) memcpy(wta_l, tmp_l.data(), sizeof(float) * W * H);
+    } else if (run == 1) {
+      if (cost_rl) copy_pitched_volume(*impl.computor_->cost_, W, H, D, cost_rl);
+      if (paths_rl)
+        for (int k = 0; k < 4; ++k)
+          copy_pitched_volume(impl.aggregator_->cost_aggr_dir_[k], W, H, D, paths_rl + (size_t)k * W * H * D);
+      if (lr_l) memcpy(lr_l, tmp_l.data(), sizeof(float) * W * H);
+      if (lr_r) memcpy(lr_r, tmp_r.data(), sizeof(float) * W * H);
+    } else {
+      if (disp_l) memcpy(disp_l, tmp_l.data(), sizeof(float) * W * H);
+      if (disp_r) memcpy(disp_r, tmp_r.data(), sizeof(float) * W * H);
+    }
+    impl.Release();
+  }
+  return 0;
+}
+
+// FasterStereoCuda::Match through the reference's public API (per-level options as the
+// reference hard-codes them). Returns 0 on success.
+int ref_pyr_match(int width, int height, int min_disp, int max_disp, int layers, int lr, int peaks,
+                  const uint8_t* left, const uint8_t* right, float* disp) {
+  FasterStereoCuda s;
+  FasterStereoCuda::StereoOption1 o;
+  o.width = width;
+  o.height = height;
+  o.min_disp = min_disp;
+  o.max_disp = max_disp;
+  o.num_layers = layers;
+  o.do_lr_check = lr != 0;
+  o.do_rm_peaks = peaks != 0;
+  o.do_smooth = false;
+  if (!s.Init(o)) { g_msg = "FasterStereoCuda::Init failed"; return -2; }
+  const bool ok = s.Match(left, right, disp);
+  s.Release();
+  if (!ok || cudaDeviceSynchronize() != cudaSuccess) { g_msg = "FasterStereoCuda::Match failed"; return -4; }
+  return 0;
+}
+
+// Wall time of n StereoCuda::Match calls on one pair (host buffers in and out), in ms per call.
+double ref_time_match(const ref_case_t* c, const uint8_t* left, const uint8_t* right, int warmup, int n) {
+  if (check_case(c, false)) return -1.0;
+  StereoCudaImpl impl;
+  if (!impl.Init(c->width, c->height, c->min_disp, c->disp_range,
+                 make_option(c, c->do_lr_check != 0, c->do_median != 0, c->do_remove_peaks != 0, c->morphology),
+                 false))
+    return -2.0;
+  std::vector<uint8_t> L(left, left + (size_t)c->width * c->height), R(right, right + (size_t)c->width * c->height);
+  std::vector<float> d((size_t)c->width * c->height);
+  for (int i = 0; i < warmup; ++i) impl.Match(L.data(), R.data(), d.data());
+  cudaDeviceSynchronize();
+  const auto t0 = std::chrono::steady_clock::now();
+  for (int i = 0; i < n; ++i) impl.Match(L.data(), R.data(), d.data());
+  cudaDeviceSynchronize();
+  const auto t1 = std::chrono::steady_clock::now();
+  impl.Release();
+  return std::chrono::duration<double, std::milli>(t1 - t0).count() / n;
+}
+
+}  // extern "C"

@@ -1,0 +1,308 @@
+"""Generates the golden fixtures that pin the oracle to the reference itself.
+
+The reference (ethan-li-coding/FasterStereoCuda) ships no tests or golden vectors, so the
+fixtures come from running the reference's own code, built from its sources by
+oracle/build_ref.sh into oracle/_ref/libsgmref.so:
+
+  python tests/golden/make_golden.py host
+      CPU only: the reference's host functions (RemovePeaks, Zoom,
+      ComputeInitDispInNextLevel) on seeded inputs -> tests/golden/host_ops.npz
+
+  python tests/golden/make_golden.py refdump --out DIR
+      on a CUDA machine: the reference's stage buffers (census, cost, four path volumes,
+      WTA, left-right check, filtered output) for the cases below -> DIR/<case>.npz
+
+  python tests/golden/make_golden.py finalize DIR
+      compares the dumps with the oracle, prints the agreement, and writes the compact
+      fixtures tests/golden/ref_<case>.npz (inputs, reference maps, volume digests).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import hashlib
+import json
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+from fasterstereocuda_b200 import scenes  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+
+GOLDEN = Path(__file__).resolve().parent
+REF_LIB = ROOT / "oracle" / "_ref" / "libsgmref.so"
+INV = np.float32(-999999.0)
+
+
+class RefCase(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("min_disp", C.c_int32), ("disp_range", C.c_int32),
+                ("cs_type", C.c_int32), ("p1", C.c_int32), ("p2", C.c_int32), ("uniqueness", C.c_float),
+                ("do_lr_check", C.c_int32), ("lr_threshold", C.c_float), ("do_median", C.c_int32),
+                ("morphology", C.c_int32), ("do_remove_peaks", C.c_int32), ("peaks_ratio", C.c_float)]
+
+
+def ref_lib():
+    lib = C.CDLL(str(REF_LIB))
+    vp = C.c_void_p
+    lib.ref_match_dump.argtypes = [C.POINTER(RefCase)] + [vp] * 14
+    lib.ref_match_dump.restype = C.c_int
+    lib.ref_pyr_match.argtypes = [C.c_int] * 7 + [vp, vp, vp]
+    lib.ref_pyr_match.restype = C.c_int
+    lib.ref_remove_peaks.argtypes = [vp, vp, C.c_int, C.c_int, C.c_int]
+    lib.ref_remove_peaks.restype = C.c_int
+    lib.ref_zoom_half.argtypes = [vp, vp, C.c_int, C.c_int]
+    lib.ref_init_next_level.argtypes = [vp, vp, C.c_int, C.c_int]
+    lib.ref_init_next_level.restype = C.c_int
+    lib.ref_hardware_threads_peaks.restype = C.c_int
+    lib.ref_last_message.restype = C.c_char_p
+    lib.ref_time_match.argtypes = [C.POINTER(RefCase), vp, vp, C.c_int, C.c_int]
+    lib.ref_time_match.restype = C.c_double
+    return lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+# ----------------------------------------------------------------------------- cases
+def _init_from_coarse(left, right, cs_type, p1, p2):
+    """Initial disparity of a D=32 level: the oracle's matching of the half-resolution pair,
+    propagated with the next-level rule (as the pyramid does)."""
+    h, w = left.shape
+    lh, rh = O.zoom_half(left), O.zoom_half(right)
+    cfg = O.Config(width=w // 2, height=h // 2, disp_range=64, cs_type=cs_type, p1=p1, p2=p2, uniqueness=1.0,
+                   do_lr_check=1, do_median=1, morphology_dilation=1)
+    coarse = O.match(cfg, lh, rh)["disp"]
+    return O.init_next_level(coarse, w, h)
+
+
+def cases():
+    """name -> (RefCase fields, left, right, init or None, dump volumes)"""
+    out = {}
+    base = dict(min_disp=0, disp_range=64, cs_type=1, p1=10, p2=150, uniqueness=0.95, do_lr_check=1,
+                lr_threshold=1.0, do_median=1, morphology=0, do_remove_peaks=0, peaks_ratio=0.0005)
+    L, R, _ = scenes.planar_pair(11, 162, 120)
+    out["c9x7"] = (dict(base, width=162, height=120), L, R, None, True)
+    L, R, _ = scenes.planar_pair(12, 162, 120)
+    out["c5x5"] = (dict(base, width=162, height=120, cs_type=0, p1=8, p2=32), L, R, None, True)
+    L, R, _ = scenes.planar_pair(13, 130, 100, dmin=0.0, dmax=50.0)
+    out["negmin"] = (dict(base, width=130, height=100, min_disp=-4), L, R, None, True)
+    L, R, _ = scenes.planar_pair(14, 162, 120)
+    init = _init_from_coarse(L, R, 1, 10, 150)
+    out["init9x7"] = (dict(base, width=162, height=120, disp_range=32, uniqueness=1.0, do_lr_check=0), L, R, init,
+                      True)
+    L, R, _ = scenes.planar_pair(15, 162, 120)
+    init = _init_from_coarse(L, R, 0, 8, 32)
+    out["init5x5"] = (dict(base, width=162, height=120, disp_range=32, cs_type=0, p1=8, p2=32, do_lr_check=0), L, R,
+                      init, True)
+    L, R, _ = scenes.cone_like(16)
+    out["cfg0"] = (dict(base, width=450, height=375), L, R, None, False)
+    out["cfg0_peaks"] = (dict(base, width=450, height=375, do_lr_check=0, do_remove_peaks=1, peaks_ratio=0.0005), L,
+                         R, None, False)
+    L, R, _ = scenes.kitti_like(17, 621, 187)
+    out["kitti_half"] = (dict(base, width=621, height=187, morphology=2, do_remove_peaks=1, peaks_ratio=0.005), L, R,
+                         None, False)
+    return out
+
+
+PYR_CASES = {"pyr_kitti": (17, 1242, 375, 0, 64, 3), "pyr_cone": (16, 450, 375, 0, 64, 2)}
+
+
+# ----------------------------------------------------------------------------- host ops
+def make_host():
+    lib = ref_lib()
+    rng = np.random.Generator(np.random.PCG64(7))
+    fx = {}
+    # small-region removal: piecewise-constant maps with noise, INVALID holes, one strip each
+    for k, (w, h) in enumerate([(64, 32), (97, 41), (128, 16)]):
+        blocks = rng.integers(0, 12, size=(h // 4 + 1, w // 4 + 1)).astype(np.float32)
+        d = np.kron(blocks, np.ones((4, 4), np.float32))[:h, :w] * 1.7
+        d += rng.normal(0, 0.45, size=d.shape).astype(np.float32)
+        d[rng.random(d.shape) < 0.1] = INV
+        for thr in (3, 11, 40):
+            out = d.copy()
+            seg = np.zeros(d.shape, np.int32)
+            n = lib.ref_remove_peaks(_p(out), _p(seg), w, h, thr)
+            fx[f"peaks_{k}_{thr}_in"] = d
+            fx[f"peaks_{k}_{thr}_out"] = out
+            fx[f"peaks_{k}_{thr}_n"] = np.int32(n)
+    # decimation
+    for k, (w, h) in enumerate([(31, 17), (64, 48), (101, 77)]):
+        img = rng.integers(0, 256, size=(h, w), dtype=np.uint8)
+        out = np.zeros((h // 2, w // 2), np.uint8)
+        lib.ref_zoom_half(_p(img), _p(out), w, h)
+        fx[f"zoom_{k}_in"], fx[f"zoom_{k}_out"] = img, out
+    # next-level initial disparity (odd and even sizes); one spare INVALID after the coarse map
+    # absorbs the reference's read past the end for odd widths
+    for k, (w, h) in enumerate([(64, 48), (65, 48), (63, 47), (621, 187)]):
+        cur = rng.uniform(0, 30, size=(h // 2, w // 2)).astype(np.float32)
+        cur[rng.random(cur.shape) < 0.15] = INV
+        buf = np.concatenate([cur.reshape(-1), [INV]]).astype(np.float32)
+        nxt = np.zeros((h, w), np.int16)
+        lib.ref_init_next_level(_p(buf), _p(nxt), w, h)
+        fx[f"initnext_{k}_in"], fx[f"initnext_{k}_out"] = cur, nxt
+        fx[f"initnext_{k}_size"] = np.array([w, h], np.int32)
+    np.savez_compressed(GOLDEN / "host_ops.npz", **fx)
+    print("wrote", GOLDEN / "host_ops.npz", len(fx), "arrays")
+
+
+# ----------------------------------------------------------------------------- reference dumps
+def refdump(out_dir: Path, only=None):
+    lib = ref_lib()
+    out_dir.mkdir(parents=True, exist_ok=True)
+    meta = {"peaks_strips": lib.ref_hardware_threads_peaks()}
+    for name, (f, L, R, init, vols) in cases().items():
+        if only and name not in only:
+            continue
+        c = RefCase(**f)
+        W, H, D = f["width"], f["height"], f["disp_range"]
+        arr = {}
+        if vols:
+            arr.update(census_l=np.zeros((H, W), np.uint64), census_r=np.zeros((H, W), np.uint64),
+                       cost_lr=np.zeros((H, W, D), np.uint8), paths_lr=np.zeros((4, H, W, D), np.uint8),
+                       cost_rl=np.zeros((H, W, D), np.uint8), paths_rl=np.zeros((4, H, W, D), np.uint8))
+        arr.update(wta_l=np.zeros((H, W), np.float32), lr_l=np.zeros((H, W), np.float32),
+                   lr_r=np.zeros((H, W), np.float32), disp_l=np.zeros((H, W), np.float32),
+                   disp_r=np.zeros((H, W), np.float32))
+        g = arr.get
+        rc = lib.ref_match_dump(C.byref(c), _p(L), _p(R), _p(init), _p(g("census_l")), _p(g("census_r")),
+                                _p(g("cost_lr")), _p(g("paths_lr")), _p(g("wta_l")), _p(g("cost_rl")),
+                                _p(g("paths_rl")), _p(g("lr_l")), _p(g("lr_r")), _p(g("disp_l")), _p(g("disp_r")))
+        print(name, "rc", rc, lib.ref_last_message().decode(), flush=True)
+        if rc != 0:
+            continue
+        extra = {} if init is None else {"init": init}
+        np.savez_compressed(out_dir / f"{name}.npz", left=L, right=R, case=np.array(json.dumps(f)), **extra, **arr)
+    for name, (seed, w, h, dmin, dmax, layers) in PYR_CASES.items():
+        if only and name not in only:
+            continue
+        if name == "pyr_kitti":
+            L, R, _ = scenes.kitti_like(seed, w, h)
+        else:
+            L, R, _ = scenes.cone_like(seed)
+        disp = np.zeros((h, w), np.float32)
+        rc = lib.ref_pyr_match(w, h, dmin, dmax, layers, 1, 1, _p(L), _p(R), _p(disp))
+        print(name, "rc", rc, lib.ref_last_message().decode(), flush=True)
+        if rc == 0:
+            np.savez_compressed(out_dir / f"{name}.npz", left=L, right=R, disp=disp,
+                                case=np.array(json.dumps(dict(width=w, height=h, min_disp=dmin, max_disp=dmax,
+                                                              num_layers=layers))))
+    (out_dir / "meta.json").write_text(json.dumps(meta))
+    print("meta", meta)
+
+
+def digest(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def _eq(a, b):
+    return np.asarray(a).view(np.uint8).reshape(-1).tobytes() == np.asarray(b).view(np.uint8).reshape(-1).tobytes()
+
+
+def path_first_pixel_mask(W, H, x0):
+    """[4][H][W] mask of the first pixel of every path (never stored by the reference)."""
+    m = np.zeros((4, H, W), bool)
+    m[0, 0, x0:] = True
+    m[2, H - 1, x0:] = True
+    m[1, :, x0] = True
+    m[3, :, W - 1] = True
+    return m
+
+
+def finalize(dump_dir: Path, write: bool = True):
+    meta = json.loads((dump_dir / "meta.json").read_text())
+    report = {}
+    for f in sorted(dump_dir.glob("*.npz")):
+        z = dict(np.load(f))
+        name = f.stem
+        case = json.loads(str(z["case"]))
+        if name.startswith("pyr_"):
+            pc = O.PyrConfig(width=case["width"], height=case["height"], min_disp=case["min_disp"],
+                             max_disp=case["max_disp"], num_layers=case["num_layers"], override_enable=0,
+                             peaks_strips=meta["peaks_strips"])
+            d = O.pyr_match(pc, z["left"], z["right"])
+            same = (d.view(np.uint32) == z["disp"].view(np.uint32))
+            report[name] = {"disp_equal": float(same.mean())}
+            if write:
+                np.savez_compressed(GOLDEN / f"ref_{name}.npz", left=z["left"], right=z["right"], disp=z["disp"],
+                                    case=z["case"], peaks_strips=np.int32(meta["peaks_strips"]))
+            continue
+        W, H, D = case["width"], case["height"], case["disp_range"]
+        init = z.get("init")
+        cfg = O.Config(width=W, height=H, min_disp=case["min_disp"], disp_range=D, cs_type=case["cs_type"],
+                       p1=case["p1"], p2=case["p2"], uniqueness=case["uniqueness"], do_lr_check=0, do_median=0,
+                       peaks_strips=meta["peaks_strips"])
+        r = {}
+        a = O.match(cfg, z["left"], z["right"], init, dump=True)
+        x0 = max(0, case["min_disp"])
+        if "census_l" in z:
+            r["census_l"] = _eq(a["census_l"], z["census_l"])
+            r["census_r"] = _eq(a["census_r"], z["census_r"])
+            cm = np.zeros((H, W), bool)
+            cm[:, x0:] = True
+            r["cost_lr"] = float((a["cost"] == z["cost_lr"])[cm].mean())
+            fm = path_first_pixel_mask(W, H, x0)
+            valid = np.broadcast_to(cm, (4, H, W)) & ~fm
+            if init is not None:
+                valid = valid & (np.broadcast_to(init != -32768, (4, H, W)))
+            pe = (a["paths"] == z["paths_lr"]).all(-1)
+            r["paths_lr"] = [float(pe[k][valid[k]].mean()) for k in range(4)]
+        # WTA: equality per tie rule, and on pixels without ties
+        best = None
+        for rule in range(4):
+            c2 = O.Config(**{**cfg.__dict__, "tie_rule": rule, "init_tie_rule": rule})
+            w = O.match(c2, z["left"], z["right"], init)["disp"]
+            eq = float((w.view(np.uint32) == z["wta_l"].view(np.uint32)).mean())
+            r[f"wta_rule{rule}"] = eq
+            if best is None or eq > best[1]:
+                best = (rule, eq)
+        r["wta_best_rule"] = best[0]
+        # full options under the best rule
+        cf = O.Config(**{**cfg.__dict__, "do_lr_check": case["do_lr_check"], "do_median": case["do_median"],
+                         "morphology_dilation": int(case["morphology"] == 2),
+                         "do_remove_peaks": case["do_remove_peaks"], "peaks_ratio": case["peaks_ratio"],
+                         "tie_rule": best[0], "init_tie_rule": best[0]})
+        full = O.match(cf, z["left"], z["right"], init, want_right=True)
+        rows = slice(0, H - 1) if H % 2 else slice(0, H)  # the reference never writes the last odd row
+        r["disp_equal"] = float((full["disp"][rows].view(np.uint32) == z["disp_l"][rows].view(np.uint32)).mean())
+        report[name] = r
+        if write:
+            keep = {k: z[k] for k in ("left", "right", "wta_l", "lr_l", "lr_r", "disp_l", "disp_r", "case") if k in z}
+            if init is not None:
+                keep["init"] = init
+            if "census_l" in z:
+                keep["census_l"], keep["census_r"] = z["census_l"], z["census_r"]
+                keep["digest_cost_lr"] = np.array(digest(np.where(cm[..., None], z["cost_lr"], 0)))
+            keep["peaks_strips"] = np.int32(meta["peaks_strips"])
+            np.savez_compressed(GOLDEN / f"ref_{name}.npz", **keep)
+    print(json.dumps(report, indent=1))
+    if write:
+        (GOLDEN / "ref_agreement.json").write_text(json.dumps(report, indent=1))
+    return report
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    sub.add_parser("host")
+    d = sub.add_parser("refdump")
+    d.add_argument("--out", required=True)
+    d.add_argument("--only", nargs="*")
+    f = sub.add_parser("finalize")
+    f.add_argument("dir")
+    f.add_argument("--no-write", action="store_true")
+    a = ap.parse_args()
+    if a.cmd == "host":
+        make_host()
+    elif a.cmd == "refdump":
+        refdump(Path(a.out), a.only)
+    else:
+        finalize(Path(a.dir), not a.no_write)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,85 @@
+"""The C ABI library loads and exports every entry point include/*.h declares (no GPU needed)."""
+import ctypes as C
+import re
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def declared_symbols():
+    names = set()
+    for h in (ROOT / "include").glob("*.h"):
+        text = h.read_text()
+        for m in re.finditer(r"SGM_API\s+[\w\s\*]+?\b(sgm_\w+)\s*\(", text):
+            names.add(m.group(1))
+    return names
+
+
+def test_library_exports_all_declared_symbols(engine_lib):
+    lib_path = ROOT / "fasterstereocuda_b200" / "_lib" / "libsgmb200.so"
+    out = subprocess.run(["nm", "-D", "--defined-only", str(lib_path)], capture_output=True, text=True, check=True)
+    exported = {line.split()[-1] for line in out.stdout.splitlines() if line.strip()}
+    declared = declared_symbols()
+    assert len(declared) >= 25
+    missing = sorted(declared - exported)
+    assert not missing, f"declared but not exported: {missing}"
+    # only the C ABI and the C++ drop-in classes are visible
+    extra = sorted(s for s in exported if s.startswith("sgm_") and s not in declared)
+    assert not extra, f"exported but not declared: {extra}"
+
+
+def test_struct_layouts_match_reference(engine_lib):
+    import fasterstereocuda_b200 as fsc
+    # CuSGMOption (sgm_types.h:21-65): 5 ints, 2 bools, 2 floats, 2 bools, float, 2 enums
+    assert C.sizeof(fsc.CuSGMOption) == 48
+    assert fsc.CuSGMOption.lr_threshold.offset == 24
+    assert fsc.CuSGMOption.using_constant_p2.offset == 32
+    assert fsc.CuSGMOption.peaks_ratio_threshold.offset == 36
+    assert fsc.CuSGMOption.morphology_type.offset == 44
+    assert C.sizeof(fsc.StereoROI) == 16
+    assert C.sizeof(fsc.StereoOption1) == 24
+
+
+def test_reference_defaults():
+    import fasterstereocuda_b200 as fsc
+    o = fsc.CuSGMOption()
+    assert (o.p1, o.p2_init, o.cs_type, o.do_lr_check, o.unique_threshold) == (8, 32, 0, False, 0.0)
+    s = fsc.StereoOption1()
+    assert (s.num_layers, s.do_lr_check, s.do_rm_peaks, s.do_smooth) == (1, True, True, False)
+
+
+def test_constants(engine_lib):
+    import fasterstereocuda_b200 as fsc
+    assert fsc.StereoCuda.get_invad_float() == -999999.0
+    assert fsc.StereoCuda.get_invad_short() == -32768
+    assert fsc.StereoCuda.get_level_range() == 32
+
+
+def test_argument_errors_without_device(engine_lib):
+    """Validation happens before any CUDA call, so these run without a GPU."""
+    import fasterstereocuda_b200 as fsc
+    s = fsc.StereoCuda()
+    opt = fsc.CuSGMOption(cs_type=1, p1=10, p2_init=150)
+    assert not s.Init(0, 10, 0, 64, opt) and s.status == -1
+    assert not s.Init(10, 10, 0, 0, opt) and s.status == -1
+    assert not s.Init(100, 100, 0, 96, opt) and s.status == -4      # not 32/64/128/256
+    assert not s.Init(100, 100, 0, 64, fsc.CuSGMOption(p1=-1)) and s.status == -1
+    assert not s.Init(100, 100, 0, 64, fsc.CuSGMOption(post_filter_type=1)) and s.status == -4
+    img = np.zeros((10, 10), np.uint8)
+    d = np.zeros((10, 10), np.float32)
+    s.width = s.height = 10
+    assert not s.Match(img, img, d) and s.status == -2                 # not initialised
+    assert "not initialised" in s.last_error()
+
+
+def test_roi_from_disp_map(engine_lib):
+    import fasterstereocuda_b200 as fsc
+    d = np.full((20, 30), -999999.0, np.float32)
+    d[5:12, 7:19] = 3.0
+    roi = fsc.StereoROI()
+    fsc.StereoCuda.GetRoiFromDispMap(d, 30, 20, roi)
+    assert (roi.x, roi.y, roi.w, roi.h) == (7, 5, 12, 7)

@@ -1,0 +1,200 @@
+"""CUDA engine vs oracle, bit-exact, stage by stage (runs on a B200).
+
+Every case goes through the C ABI (StereoCuda.Init / Match, FasterStereoCuda.Init / Match).
+Integer stages (census, cost, path volumes) and float disparities are compared bit for bit.
+"""
+import numpy as np
+import pytest
+
+from fasterstereocuda_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+INV = np.float32(-999999.0)
+STRIPS = 6
+
+
+def bits(a):
+    return np.ascontiguousarray(a).view(np.uint8)
+
+
+def assert_same(name, got, exp, mask=None):
+    g, e = np.asarray(got), np.asarray(exp)
+    assert g.shape == e.shape, (name, g.shape, e.shape)
+    if g.dtype == np.float32:
+        neq = g.view(np.uint32) != e.view(np.uint32)
+    else:
+        neq = g != e
+    if neq.ndim == 3 and mask is not None and mask.ndim == 2:
+        neq = neq.any(-1)
+    if mask is not None:
+        neq = neq & mask
+    n = int(neq.sum())
+    if n:
+        idx = np.argwhere(neq)[:5]
+        detail = [(tuple(int(v) for v in i), g[tuple(i)].tolist() if g.ndim <= 2 else None,
+                   e[tuple(i)].tolist() if e.ndim <= 2 else None) for i in idx]
+        pytest.fail(f"{name}: {n} mismatches, first {detail}")
+
+
+def make_engine(fsc, W, H, M, D, cs, p1, p2, u, lr, med, peaks=0, ratio=0.0005, morph=0, tie=0):
+    s = fsc.StereoCuda()
+    opt = fsc.CuSGMOption(p1=p1, p2_init=p2, cs_type=cs, num_paths=4, do_median_filter=bool(med),
+                          do_lr_check=bool(lr), lr_threshold=1.0, unique_threshold=u, using_constant_p2=True,
+                          do_remove_peaks=bool(peaks), peaks_ratio_threshold=ratio, morphology_type=morph)
+    assert s.Init(W, H, M, D, opt), s.last_error()
+    assert s.set_ext_options(fsc.ExtOptions(tie_rule=tie, init_tie_rule=tie, peaks_strips=STRIPS, peaks_abs_mode=0))
+    return s
+
+
+CASES = {
+    # name: (W, H, M, D, cs, p1, p2, uniq, lr, median, peaks, morph, seed)
+    "d64_9x7_lr_med": (162, 120, 0, 64, 1, 10, 150, 0.95, 1, 1, 0, 0, 11),
+    "d64_5x5_lr_med": (162, 120, 0, 64, 0, 8, 32, 0.95, 1, 1, 0, 0, 12),
+    "d32_plain": (150, 90, 0, 32, 1, 10, 150, 0.95, 1, 1, 0, 0, 13),
+    "d128": (300, 96, 0, 128, 1, 10, 150, 0.95, 1, 1, 0, 0, 14),
+    "d256_generic": (400, 64, 0, 256, 1, 10, 150, 0.95, 1, 0, 0, 0, 15),
+    "neg_min_disp": (130, 100, -4, 64, 1, 10, 150, 0.95, 1, 1, 0, 0, 16),
+    "pos_min_disp": (130, 100, 8, 64, 1, 10, 150, 0.95, 1, 1, 0, 0, 17),
+    "odd_size": (131, 77, 0, 64, 1, 10, 150, 0.9, 1, 1, 0, 0, 18),
+    "no_lr_no_median": (162, 120, 0, 64, 1, 10, 150, 0.95, 0, 0, 0, 0, 19),
+    "big_penalty": (162, 120, 0, 64, 1, 10, 230, 0.95, 1, 1, 0, 0, 20),
+    "peaks": (200, 150, 0, 64, 1, 10, 150, 0.95, 0, 1, 1, 0, 21),
+    "dilation_peaks": (200, 150, 0, 64, 0, 8, 32, 1.0, 1, 1, 1, 2, 22),
+    "cfg0_450x375": (450, 375, 0, 64, 1, 10, 150, 0.95, 1, 1, 0, 0, 23),
+}
+
+
+@pytest.mark.parametrize("name", list(CASES))
+@pytest.mark.parametrize("tie", [0, 2])
+def test_plain_parity(engine_lib, oracle_mod, name, tie):
+    import fasterstereocuda_b200 as fsc
+    O = oracle_mod
+    W, H, M, D, cs, p1, p2, u, lr, med, peaks, morph, seed = CASES[name]
+    if tie and name not in ("d64_9x7_lr_med", "d128", "d32_plain", "d256_generic"):
+        pytest.skip("tie rule variants on a subset")
+    L, R, _ = scenes.planar_pair(seed, W, H, dmin=2.0, dmax=min(60.0, D - 4.0))
+    ratio = 0.005 if peaks else 0.0005
+    s = make_engine(fsc, W, H, M, D, cs, p1, p2, u, lr, med, peaks, ratio, morph, tie)
+    disp = np.empty((H, W), np.float32)
+    disp_r = np.empty((H, W), np.float32)
+    assert s.Match(L, R, disp, disp_r), s.last_error()
+    cfg = O.Config(width=W, height=H, min_disp=M, disp_range=D, cs_type=cs, p1=p1, p2=p2, uniqueness=u,
+                   do_lr_check=lr, do_median=med, do_remove_peaks=peaks, peaks_ratio=ratio,
+                   morphology_dilation=int(morph == 2), peaks_strips=STRIPS, tie_rule=tie, init_tie_rule=tie)
+    ref = O.match(cfg, L, R, dump=True, want_right=True)
+    x0 = max(0, M)
+    colmask = np.zeros((H, W), bool)
+    colmask[:, x0:] = True
+    assert_same("census_l", s.debug_read("census_l"), ref["census_l"])
+    assert_same("census_r", s.debug_read("census_r"), ref["census_r"])
+    assert_same("cost", s.debug_read("cost"), ref["cost"], colmask)
+    assert_same("path L->R", s.debug_read("lr"), ref["paths"][1], colmask)
+    assert_same("path R->L", s.debug_read("rl"), ref["paths"][3], colmask)
+    assert_same("path B->T", s.debug_read("bt"), ref["paths"][2], colmask)
+    assert_same("wta left", s.debug_read("wta", 0), ref["wta_l"])
+    if lr:
+        assert_same("wta right", s.debug_read("wta", 1), ref["wta_r"])
+        assert_same("disp right", disp_r, ref["disp_r"])
+    assert_same("disp left", disp, ref["disp"])
+    assert s.kernel_launches() >= 3
+
+
+def _init_for(O, L, R, cs, p1, p2):
+    h, w = L.shape
+    cfg = O.Config(width=w // 2, height=h // 2, disp_range=64, cs_type=cs, p1=p1, p2=p2, uniqueness=1.0,
+                   do_lr_check=1, do_median=1, morphology_dilation=1)
+    coarse = O.match(cfg, O.zoom_half(L), O.zoom_half(R))["disp"]
+    return O.init_next_level(coarse, w, h)
+
+
+@pytest.mark.parametrize("cs,p1,p2,lr,u", [(1, 10, 150, 0, 1.0), (0, 8, 32, 0, 0.95), (1, 10, 150, 1, 0.95),
+                                           (0, 8, 32, 1, 1.0)])
+def test_init_disparity_parity(engine_lib, oracle_mod, cs, p1, p2, lr, u):
+    import fasterstereocuda_b200 as fsc
+    O = oracle_mod
+    W, H = 162, 121
+    L, R, _ = scenes.planar_pair(31 + cs, W, H)
+    init = _init_for(O, L, R, cs, p1, p2)
+    s = make_engine(fsc, W, H, 0, 32, cs, p1, p2, u, lr, 1)
+    disp = np.empty((H, W), np.float32)
+    assert s.Match(L, R, disp, None, init), s.last_error()
+    cfg = O.Config(width=W, height=H, disp_range=32, cs_type=cs, p1=p1, p2=p2, uniqueness=u, do_lr_check=lr,
+                   do_median=1, peaks_strips=STRIPS)
+    ref = O.match(cfg, L, R, init, dump=True, want_right=True)
+    valid = init != -32768
+    assert_same("cost", s.debug_read("cost"), ref["cost"])
+    assert_same("path L->R", s.debug_read("lr"), ref["paths"][1], valid)
+    assert_same("path R->L", s.debug_read("rl"), ref["paths"][3], valid)
+    assert_same("path B->T", s.debug_read("bt"), ref["paths"][2], valid)
+    assert_same("wta left", s.debug_read("wta", 0), ref["wta_l"])
+    if lr:
+        assert_same("wta right", s.debug_read("wta", 1), ref["wta_r"])
+    assert_same("disp left", disp, ref["disp"])
+
+
+@pytest.mark.parametrize("override", [True, False])
+@pytest.mark.parametrize("size,layers", [((1242, 375), 3), ((450, 375), 2), ((640, 480), 4)])
+def test_pyramid_parity(engine_lib, oracle_mod, override, size, layers):
+    import fasterstereocuda_b200 as fsc
+    O = oracle_mod
+    W, H = size
+    L, R, _ = scenes.kitti_like(41, W, H)
+    p = fsc.FasterStereoCuda()
+    opt = fsc.StereoOption1(width=W, height=H, min_disp=0, max_disp=64, num_layers=layers, do_lr_check=True,
+                            do_rm_peaks=True)
+    ov = fsc.LevelOverride(cs_type=1, p1=10, p2=150) if override else None
+    assert p.Init(opt, ov, fsc.ExtOptions(peaks_strips=STRIPS)), p.last_error()
+    disp = np.empty((H, W), np.float32)
+    assert p.Match(L, R, disp)
+    pc = O.PyrConfig(width=W, height=H, min_disp=0, max_disp=64, num_layers=layers, override_enable=int(override),
+                     cs_type=1 if override else 0, p1=10 if override else 8, p2=150 if override else 32,
+                     peaks_strips=STRIPS)
+    ref = O.pyr_match(pc, L, R)
+    assert_same("pyramid disp", disp, ref)
+    for lvl in range(layers):
+        w, h, m, d = p.level_info(lvl)
+        c = O.pyr_level_config(pc, lvl)
+        assert (w, h, m, d) == (c.width, c.height, c.min_disp, c.disp_range)
+
+
+def test_device_api_matches_host_api(engine_lib, oracle_mod):
+    import torch
+    import fasterstereocuda_b200 as fsc
+    W, H = 320, 200
+    L, R, _ = scenes.planar_pair(51, W, H)
+    s = make_engine(fsc, W, H, 0, 64, 1, 10, 150, 0.95, 1, 1)
+    host = np.empty((H, W), np.float32)
+    assert s.Match(L, R, host)
+    dl, dr = torch.from_numpy(L).cuda(), torch.from_numpy(R).cuda()
+    out = torch.empty((H, W), dtype=torch.float32, device="cuda")
+    out_r = torch.empty((H, W), dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    assert s.match_device(dl, dr, out, out_r, None, stream), s.last_error()
+    torch.cuda.synchronize()
+    assert_same("device api", out.cpu().numpy(), host)
+
+
+def test_repeated_matches_are_identical(engine_lib):
+    import fasterstereocuda_b200 as fsc
+    W, H = 256, 160
+    L, R, _ = scenes.planar_pair(52, W, H)
+    s = make_engine(fsc, W, H, 0, 64, 1, 10, 150, 0.95, 1, 1, 1, 0.001)
+    a = np.empty((H, W), np.float32)
+    b = np.empty((H, W), np.float32)
+    assert s.Match(L, R, a) and s.Match(L, R, b)
+    assert_same("repeat", a, b)
+
+
+def test_errors_on_device(engine_lib):
+    import fasterstereocuda_b200 as fsc
+    W, H = 128, 96
+    s = make_engine(fsc, W, H, 0, 64, 1, 10, 150, 0.95, 0, 1)
+    img = np.zeros((H, W), np.uint8)
+    out = np.empty((H, W), np.float32)
+    init = np.zeros((H, W), np.int16)
+    assert not s.Match(img, img, out, None, init) and s.status == -4   # init needs D=32
+    roi = fsc.StereoROI(0, 0, 10, 10)
+    assert not s.Match(img, img, out, None, None, roi) and s.status == -4
+    s.Release()
+    assert not s.Match(img, img, out) and s.status == -2
