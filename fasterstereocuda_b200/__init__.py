@@ -63,12 +63,12 @@ class ExtOptions(C.Structure):
     """Rules the reference leaves to thread scheduling or its compiler (sgm_ext_options_t)."""
     _fields_ = [("tie_rule", C.c_int32), ("init_tie_rule", C.c_int32), ("peaks_strips", C.c_int32),
                 ("peaks_abs_mode", C.c_int32), ("p2_div0", C.c_int32)]
-    TIE_LOWEST, TIE_HIGHEST, TIE_LANE_HIGH, TIE_LANE_LOW = 0, 1, 2, 3
+    TIE_LOWEST, TIE_HIGHEST, TIE_LANE_HIGH, TIE_LANE_LOW, TIE_REF_B200 = 0, 1, 2, 3, 4
     PEAKS_ABS_INT, PEAKS_ABS_FLOAT = 0, 1
 
     def __init__(self, **kw):
         super().__init__()
-        self.tie_rule = self.init_tie_rule = 0
+        self.tie_rule = self.init_tie_rule = 4
         self.peaks_strips = 0
         self.peaks_abs_mode = 0
         self.p2_div0 = -1

@@ -11,7 +11,13 @@ constexpr uint32_t kInvalidCost = 127;         // out-of-range neighbour candida
 constexpr int kLevelRange = 32;                // disparity range of every non-coarsest pyramid level
 constexpr unsigned kFull = 0xFFFFFFFFu;
 
-enum TieRule : int { kTieLowest = 0, kTieHighest = 1, kTieLaneHigh = 2, kTieLaneLow = 3 };
+// kTieRefB200: what the reference build does on a B200 (measured from its dumps):
+//   D=64 plain -- lanes t with S(t)==m store t, lanes with only S(t+32)==m store t+32; the lowest
+//   lane wins within a store and the later store wins; the store order is t then t+32 on even rows
+//   and t+32 then t on odd rows (the two rows of one WTA block compile differently).
+//   other plain D -- lowest d. Initial-disparity levels -- every tied lane stores its own result:
+//   a valid disparity wins over INVALID, the lowest lane among valid ones.
+enum TieRule : int { kTieLowest = 0, kTieHighest = 1, kTieLaneHigh = 2, kTieLaneLow = 3, kTieRefB200 = 4 };
 enum PeaksAbs : int { kPeaksAbsInt = 0, kPeaksAbsFloat = 1 };
 
 __device__ __forceinline__ uint32_t popc_word(uint64_t v) { return __popcll(v); }
@@ -50,10 +56,11 @@ __device__ __forceinline__ uint32_t spread8(uint32_t v) {
 // Tie-break over a warp whose lane l holds disparities d = l*K + j (j < K).
 // bal[j] has bit l set when S(l*K + j) equals the minimum. Returns the chosen d.
 template <int K>
-__device__ __forceinline__ int pick_tie(const uint32_t (&bal)[K], int rule) {
+__device__ __forceinline__ int pick_tie(const uint32_t (&bal)[K], int rule, int y) {
   uint32_t any = 0;
 #pragma unroll
   for (int j = 0; j < K; ++j) any |= bal[j];
+  if (rule == kTieRefB200 && K != 2) rule = kTieLowest;
   if (rule == kTieLowest || rule == kTieHighest) {
     const int lane = rule == kTieLowest ? __ffs(any) - 1 : 31 - __clz(any);
     int best = -1;
@@ -90,6 +97,11 @@ __device__ __forceinline__ int pick_tie(const uint32_t (&bal)[K], int rule) {
       for (int j = 0; j < K; ++j) acc |= spread8(bal[j] >> (4 * w)) << j;
       word[w] = acc;
     }
+  }
+  if (rule == kTieRefB200) {  // K == 2 only (D = 64)
+    const uint32_t A = word[0], B = word[K - 1] & ~word[0];
+    if ((y & 1) == 0) return B ? (__ffs(B) - 1 + 32) : (__ffs(A) - 1);
+    return A ? (__ffs(A) - 1) : (__ffs(B) - 1 + 32);
   }
   uint32_t ref_any = 0;
 #pragma unroll

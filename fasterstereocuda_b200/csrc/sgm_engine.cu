@@ -43,8 +43,8 @@ int default_peaks_strips() {
 
 sgm_ext_options_t default_ext() {
   sgm_ext_options_t e;
-  e.tie_rule = sgm::kTieLowest;
-  e.init_tie_rule = sgm::kTieLowest;
+  e.tie_rule = sgm::kTieRefB200;
+  e.init_tie_rule = sgm::kTieRefB200;
   e.peaks_strips = 0;
   e.peaks_abs_mode = sgm::kPeaksAbsInt;
   e.p2_div0 = -1;
@@ -136,6 +136,8 @@ struct sgm_engine {
   sgm_option_t opt{};
   sgm_ext_options_t ext = default_ext();
   bool print_log = false;
+  bool has_cam = false;
+  sgm_camera_t cam{};
   cudaStream_t stream = nullptr;
   std::string err;
   int64_t launches = 0;
@@ -458,6 +460,14 @@ int engine_enqueue(sgm_engine* e, const uint8_t* dl_img, const uint8_t* dr_img, 
 
 }  // namespace
 
+namespace {
+int enqueue_depth(sgm_engine* e, const float* disp, float* depth, const sgm_camera_t& c, cudaStream_t s) {
+  const int n = (int)e->npix();
+  return SGM_LAUNCH(e, s, "depth", sgm::k_depth<<<(n + 255) / 256, 256, 0, s>>>(
+                                       disp, depth, n, c.baseline * c.focus, c.x0_right - c.x0_left));
+}
+}  // namespace
+
 // ------------------------------------------------------------------------------------------
 // Pyramid matcher
 // ------------------------------------------------------------------------------------------
@@ -474,8 +484,14 @@ struct sgm_pyramid {
   cudaStream_t stream = nullptr;
   std::string err;
   int64_t launches = 0;
+  bool depth_mode = false;
+  sgm_camera_t cam0{};
+  float* disp0 = nullptr;  // finest-level disparity in depth mode
 
   void free_all() {
+    if (disp0) cudaFree(disp0);
+    disp0 = nullptr;
+    depth_mode = false;
     for (auto* e : lv) {
       if (e) { e->free_all(); delete e; }
     }
@@ -567,7 +583,9 @@ int pyr_enqueue(sgm_pyramid* p, const uint8_t* dl, const uint8_t* dr, float* dou
     const uint8_t* ir = n == 0 ? dr : p->imgs_r[n];
     float* o = n == 0 ? dout : p->disp[n];
     const int64_t before = e->launches;
+    if (n == 0 && p->depth_mode) o = p->disp0;
     st = engine_enqueue(e, il, ir, n < L - 1 ? p->init[n] : nullptr, o, nullptr, s);
+    if (!st && n == 0 && p->depth_mode) st = enqueue_depth(e, p->disp0, dout, p->cam0, s);
     p->launches += e->launches - before;
     if (st) {
       p->err = e->err;
@@ -616,7 +634,7 @@ int sgm_init(sgm_handle_t h, int32_t width, int32_t height, int32_t min_disparit
 
 int sgm_set_ext_options(sgm_handle_t h, const sgm_ext_options_t* ext) {
   if (!h || !ext) return SGM_ERR_ARG;
-  if (ext->tie_rule < 0 || ext->tie_rule > 3 || ext->init_tie_rule < 0 || ext->init_tie_rule > 3 ||
+  if (ext->tie_rule < 0 || ext->tie_rule > 4 || ext->init_tie_rule < 0 || ext->init_tie_rule > 4 ||
       ext->peaks_abs_mode < 0 || ext->peaks_abs_mode > 1) {
     set_error(&h->err, "extended option out of range");
     return SGM_ERR_ARG;
@@ -678,6 +696,42 @@ int sgm_match_device(sgm_handle_t h, const uint8_t* d_left, const uint8_t* d_rig
   }
   h->launches = 0;
   return engine_enqueue(h, d_left, d_right, d_init_disp_left, d_disp_left, d_disp_right, (cudaStream_t)stream);
+}
+
+int sgm_init2(sgm_handle_t h, int32_t width, int32_t height, int32_t min_disparity, int32_t disp_range,
+              const sgm_option_t* option, const sgm_camera_t* camera, int32_t print_log) {
+  if (!h || !option || !camera) return SGM_ERR_ARG;
+  const int st = sgm_init(h, width, height, min_disparity, disp_range, option, print_log);
+  if (st) return st;
+  h->cam = *camera;
+  h->has_cam = true;
+  return SGM_OK;
+}
+
+int sgm_match2(sgm_handle_t h, const uint8_t* img_left, const uint8_t* img_right, float* depth_left,
+               const int16_t* init_disp_left, const sgm_roi_t* roi_left, const sgm_roi_t* roi_right) {
+  if (!h) return SGM_ERR_ARG;
+  if (!h->has_cam) {
+    set_error(&h->err, "Match2 needs Init2 (camera parameters)");
+    return SGM_ERR_STATE;
+  }
+  if (!img_left || !img_right || !depth_left) return SGM_ERR_ARG;
+  if (roi_left || roi_right) {
+    set_error(&h->err, "ROI matching is not supported");
+    return SGM_ERR_UNSUPPORTED;
+  }
+  const size_t N = h->npix();
+  h->launches = 0;
+  SGM_CUDA_TRY(h, cudaMemcpyAsync(h->img[0], img_left, N, cudaMemcpyHostToDevice, h->stream));
+  SGM_CUDA_TRY(h, cudaMemcpyAsync(h->img[1], img_right, N, cudaMemcpyHostToDevice, h->stream));
+  if (init_disp_left)
+    SGM_CUDA_TRY(h, cudaMemcpyAsync(h->init[0], init_disp_left, N * sizeof(int16_t), cudaMemcpyHostToDevice, h->stream));
+  int st = engine_enqueue(h, h->img[0], h->img[1], init_disp_left ? h->init[0] : nullptr, h->out, nullptr, h->stream);
+  if (!st) st = enqueue_depth(h, h->out, h->post2, h->cam, h->stream);
+  if (st) return st;
+  SGM_CUDA_TRY(h, cudaMemcpyAsync(depth_left, h->post2, N * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+  SGM_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return SGM_OK;
 }
 
 int sgm_release(sgm_handle_t h) {
@@ -885,6 +939,77 @@ int sgm_pyr_match_device(sgm_pyr_handle_t h, const uint8_t* d_left, const uint8_
   if (!d_left || !d_right || !d_disp) return SGM_ERR_ARG;
   h->launches = 0;
   return pyr_enqueue(h, d_left, d_right, d_disp, stream ? (cudaStream_t)stream : h->stream);
+}
+
+int sgm_pyr_init2(sgm_pyr_handle_t h, const sgm_pyr_option2_t* o, const sgm_level_override_t* ov,
+                  const sgm_ext_options_t* ext) {
+  if (!h || !o) return SGM_ERR_ARG;
+  if (!(o->min_depth > 0.0f) || !(o->max_depth > o->min_depth)) {
+    set_error(&h->err, "depth range must satisfy 0 < min_depth < max_depth");
+    return SGM_ERR_ARG;
+  }
+  // HierSgmCudaImpl::Init2 (FasterStereoCuda.cpp:339-399): disparity range of the coarsest level from
+  // the depth range seen by the camera scaled to that level; the finer levels search 32 disparities.
+  const int L = std::max(1, o->num_layers);
+  const int scale = 1 << (L - 1);
+  const double x0l = o->epi.x0_left / scale, x0r = o->epi.x0_right / scale, f = o->epi.focus / scale;
+  double dmin = o->epi.baseline * f / o->max_depth - x0r + x0l;
+  const double dmax = o->epi.baseline * f / o->min_depth - x0r + x0l;
+  double range = dmax - dmin;
+  int k = 6;
+  while (std::pow(2.0, k) < range && k < 30) ++k;
+  range = std::pow(2.0, k);
+  if (range > 2.0 * o->width) range /= 2;
+  if (dmin >= o->width) {
+    dmin = o->width - range;
+    if (dmin < -o->width) dmin = -o->width;
+  }
+  // express the coarsest range as the min/max pair the disparity initialisation understands
+  sgm_pyr_option1_t o1;
+  o1.width = o->width;
+  o1.height = o->height;
+  o1.num_layers = L;
+  o1.do_lr_check = o->do_lr_check;
+  o1.do_rm_peaks = o->do_rm_peaks;
+  o1.do_smooth = o->do_smooth;
+  o1.min_disp = (int)std::floor(dmin) * scale;
+  o1.max_disp = o1.min_disp + (int)range * scale;
+  int st = sgm_pyr_init(h, &o1, ov, ext);
+  if (st) return st;
+  sgm_engine* c = h->lv[L - 1];
+  if (c->M != (int)std::floor(dmin) || c->D != (int)range) {
+    // fall back to setting the coarsest level directly when the integer round trip differs
+    sgm_option_t so = c->opt;
+    sgm_ext_options_t ex = c->ext;
+    st = engine_init(c, c->W, c->H, (int)std::floor(dmin), (int)range, &so, false);
+    c->ext = ex;
+    if (st) {
+      h->err = c->err;
+      h->free_all();
+      return st;
+    }
+  }
+  h->cam0.x0_left = o->epi.x0_left;
+  h->cam0.y0_left = o->epi.y0_left;
+  h->cam0.x0_right = o->epi.x0_right;
+  h->cam0.y0_right = o->epi.y0_right;
+  h->cam0.focus = o->epi.focus;
+  h->cam0.baseline = o->epi.baseline;
+  if (cudaMalloc(&h->disp0, (size_t)o->width * o->height * sizeof(float)) != cudaSuccess) {
+    h->free_all();
+    return SGM_ERR_NOMEM;
+  }
+  h->depth_mode = true;
+  return SGM_OK;
+}
+
+int sgm_pyr_match2(sgm_pyr_handle_t h, const uint8_t* img_left, const uint8_t* img_right, float* depth) {
+  if (!h) return SGM_ERR_ARG;
+  if (!h->ready || !h->depth_mode) {
+    set_error(&h->err, "Match2 needs Init2");
+    return SGM_ERR_STATE;
+  }
+  return sgm_pyr_match(h, img_left, img_right, depth);
 }
 
 int sgm_pyr_release(sgm_pyr_handle_t h) {

@@ -217,7 +217,7 @@ struct WtaParams {
 // generic kernel :3149-3232. Returns the disparity (valid in every lane).
 template <int K>
 __device__ __forceinline__ float wta_pixel(const uint32_t (&S)[K], int lane, int min_d_or_base, const WtaParams& Q,
-                                           int dmin_excl) {
+                                           int dmin_excl, int y) {
   constexpr int D = 32 * K;
   uint32_t lm = S[0];
 #pragma unroll
@@ -226,7 +226,7 @@ __device__ __forceinline__ float wta_pixel(const uint32_t (&S)[K], int lane, int
   uint32_t bal[K];
 #pragma unroll
   for (int j = 0; j < K; ++j) bal[j] = __ballot_sync(kFull, S[j] == m);
-  const int ds = pick_tie<K>(bal, Q.tie_rule);
+  const int ds = pick_tie<K>(bal, Q.tie_rule, y);
   // neighbours of d*: S(d*-1) and S(d*+1) live in lanes (d*-1)/K and (d*+1)/K
   const int dl = ds - 1 < 0 ? 0 : ds - 1;
   const int dr = ds + 1 >= D ? D - 1 : ds + 1;
@@ -246,6 +246,24 @@ __device__ __forceinline__ float wta_pixel(const uint32_t (&S)[K], int lane, int
   const float uq = d12 < d32 ? d12 : d32;
   if (uq <= __fmul_rn(c2, __fsub_rn(1.0f, Q.uniqueness))) return kInvalidFloat;
   return __fadd_rn((float)(ds + min_d_or_base), subpix_bias(c1, c2, c3));
+}
+
+// WTA at an initial-disparity level under the reference's measured behaviour (every tied lane
+// stores its own result, cusgm_ca.cu:3488-3509): the lowest tied lane with a valid disparity wins.
+__device__ __forceinline__ float wta_pixel_init_ref(uint32_t S, int lane, int base, const WtaParams& Q) {
+  const uint32_t m = __reduce_min_sync(kFull, S);
+  const uint32_t c1u = __shfl_up_sync(kFull, S, 1);
+  const uint32_t c3u = __shfl_down_sync(kFull, S, 1);
+  float v = kInvalidFloat;
+  if (S == m && lane > 1 && lane < kLevelRange - 1) {
+    const float c1 = (float)c1u, c2 = (float)m, c3 = (float)c3u;
+    const float d12 = __fsub_rn(c1, c2), d32 = __fsub_rn(c3, c2);
+    const float uq = d12 < d32 ? d12 : d32;
+    if (!(uq <= __fmul_rn(c2, __fsub_rn(1.0f, Q.uniqueness))))
+      v = __fadd_rn((float)(lane + base), subpix_bias(c1, c2, c3));
+  }
+  const uint32_t ok = __ballot_sync(kFull, v != kInvalidFloat);
+  return __shfl_sync(kFull, v, ok ? __ffs(ok) - 1 : 0);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -314,7 +332,7 @@ __global__ void __launch_bounds__(256) k_vpaths_wta_plain(const uint8_t* __restr
       load_u8<K>(rlv + off, e);
 #pragma unroll
       for (int j = 0; j < K; ++j) S[j] = (L[j] & 0xFFu) + a[j] + b[j] + e[j];
-      dv = wta_pixel<K>(S, lane, P.min_d, Q, 0);
+      dv = wta_pixel<K>(S, lane, P.min_d, Q, 0, y);
     }
     if (lane == 0) dout[(size_t)y * W + x] = dv;
   }
@@ -487,7 +505,7 @@ __global__ void __launch_bounds__(256) k_vpaths_wta_init(const uint8_t* __restri
     if (col_ok && y >= 5 && y <= H - 5 && y < Q.rows && base != kInvalidShort && !skipped) {
       uint32_t S[1];
       S[0] = (L & 0xFFu) + btv[off] + lrv[off] + rlv[off];
-      dv = wta_pixel<1>(S, lane, base, Q, 1);
+      dv = Q.tie_rule == kTieRefB200 ? wta_pixel_init_ref(S[0], lane, base, Q) : wta_pixel<1>(S, lane, base, Q, 1, y);
     }
     if (lane == 0) dout[(size_t)y * W + x] = dv;
   }
@@ -723,6 +741,15 @@ __global__ void k_right_init_decode(const unsigned* __restrict__ key, int16_t* _
   if (i >= n) return;
   const unsigned k = key[i];
   out[i] = k == 0 ? kInvalidShort : (int16_t)(uint16_t)(k & 0xFFFFu);
+}
+
+// Disparity -> depth (reference Kernel_ComputeDepth, cusgm_util.cu:7-34):
+// depth = baseline*focus / (d + x0_right - x0_left) in double, INVALID kept.
+__global__ void k_depth(const float* __restrict__ disp, float* __restrict__ depth, int n, double f1, double f2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float d = disp[i];
+  depth[i] = d == kInvalidFloat ? kInvalidFloat : (float)__ddiv_rn(f1, __dadd_rn((double)d, f2));
 }
 
 }  // namespace sgm

@@ -64,12 +64,21 @@ typedef struct sgm_roi_s {
 
 /* Choices the reference leaves to thread scheduling or to its compiler; fixed here. */
 typedef struct sgm_ext_options_s {
-  int32_t tie_rule;       /* WTA tie break, plain path: 0 lowest d, 1 highest d, 2 highest lane, 3 lowest lane */
-  int32_t init_tie_rule;  /* the same at initial-disparity (pyramid) levels */
+  int32_t tie_rule;       /* WTA tie break, plain path: 0 lowest d, 1 highest d, 2 highest lane, 3 lowest lane,
+                             4 (default) the reference build's behaviour measured on a B200 */
+  int32_t init_tie_rule;  /* the same at initial-disparity (pyramid) levels (default 4) */
   int32_t peaks_strips;   /* strips of small-region removal; <= 0: hardware threads * 3 / 4 */
   int32_t peaks_abs_mode; /* region test: 0 |(int)(a-b)| <= 1 (g++ build), 1 |a-b| <= 1.0f (MSVC build) */
   int32_t p2_div0;        /* P2 / 0 at initial-disparity levels */
 } sgm_ext_options_t;
+
+/* Same layout as CamParam_T (SgmStereoCuda/sgm_types.h:70-84). */
+typedef struct sgm_camera_s {
+  double x0_left, y0_left;
+  double x0_right, y0_right;
+  double focus;
+  double baseline;
+} sgm_camera_t;
 
 typedef struct sgm_engine* sgm_handle_t;
 
@@ -95,6 +104,14 @@ SGM_API int sgm_match(sgm_handle_t h, const uint8_t* img_left, const uint8_t* im
  * handle's own stream) without synchronising. */
 SGM_API int sgm_match_device(sgm_handle_t h, const uint8_t* d_left, const uint8_t* d_right, float* d_disp_left,
                              float* d_disp_right, const int16_t* d_init_disp_left, void* stream);
+/* StereoCuda::Init2 -- SgmStereoCuda/StereoCuda.h:57, StereoCudaImpl.cpp:263-278: Init plus the
+ * camera used by sgm_match2. */
+SGM_API int sgm_init2(sgm_handle_t h, int32_t width, int32_t height, int32_t min_disparity, int32_t disp_range,
+                      const sgm_option_t* option, const sgm_camera_t* camera, int32_t print_log);
+/* StereoCuda::Match2 -- SgmStereoCuda/StereoCuda.h:69, StereoCudaImpl.cpp:548-583: match, then
+ * depth = baseline*focus / (d + x0_right - x0_left) in double, INVALID kept (cusgm_util.cu:7-34). */
+SGM_API int sgm_match2(sgm_handle_t h, const uint8_t* img_left, const uint8_t* img_right, float* depth_left,
+                       const int16_t* init_disp_left, const sgm_roi_t* roi_left, const sgm_roi_t* roi_right);
 /* StereoCuda::Release -- SgmStereoCuda/StereoCuda.h:75, StereoCudaImpl.cpp:281-332 */
 SGM_API int sgm_release(sgm_handle_t h);
 /* StereoCuda::SetMinDisparity / GetDispartyRange -- SgmStereoCuda/StereoCuda.h:71-72 */
@@ -142,6 +159,23 @@ typedef struct sgm_level_override_s {
   int32_t cs_type, p1, p2;
 } sgm_level_override_t;
 
+/* Same layout as FasterStereoCuda::EpipolarStereoParam and StereoOption2
+ * (FasterStereoCuda/FasterStereoCuda.h:28-69). */
+typedef struct sgm_epipolar_s {
+  double x0_left, y0_left;
+  double x0_right, y0_right;
+  double baseline;
+  double focus;
+} sgm_epipolar_t;
+
+typedef struct sgm_pyr_option2_s {
+  int32_t width, height;
+  float min_depth, max_depth;
+  int32_t num_layers;
+  bool do_lr_check, do_rm_peaks, do_smooth;
+  sgm_epipolar_t epi;
+} sgm_pyr_option2_t;
+
 typedef struct sgm_pyramid* sgm_pyr_handle_t;
 
 /* FasterStereoCuda::FasterStereoCuda / ~FasterStereoCuda -- FasterStereoCuda.cpp:693-703 */
@@ -157,6 +191,12 @@ SGM_API int sgm_pyr_match(sgm_pyr_handle_t h, const uint8_t* img_left, const uin
 /* No counterpart in the reference: device-resident variant, enqueued on `stream` without synchronising. */
 SGM_API int sgm_pyr_match_device(sgm_pyr_handle_t h, const uint8_t* d_left, const uint8_t* d_right, float* d_disp,
                                  void* stream);
+/* FasterStereoCuda::Init2 -- FasterStereoCuda.h:102, HierSgmCudaImpl::Init2 FasterStereoCuda.cpp:297-406:
+ * the coarsest disparity range comes from the depth range and the scaled camera. */
+SGM_API int sgm_pyr_init2(sgm_pyr_handle_t h, const sgm_pyr_option2_t* option, const sgm_level_override_t* override_,
+                          const sgm_ext_options_t* ext);
+/* FasterStereoCuda::Match2 -- FasterStereoCuda.h:123, FasterStereoCuda.cpp:531-635: depth of the finest level. */
+SGM_API int sgm_pyr_match2(sgm_pyr_handle_t h, const uint8_t* img_left, const uint8_t* img_right, float* depth);
 /* FasterStereoCuda::Release -- FasterStereoCuda.h:105 */
 SGM_API int sgm_pyr_release(sgm_pyr_handle_t h);
 /* No counterpart in the reference: level geometry chosen by init (for tests and tools). */

@@ -53,8 +53,8 @@ class Config:
     peaks_ratio: float = 0.0005
     peaks_strips: int = 6
     peaks_abs_mode: int = 0
-    tie_rule: int = 0
-    init_tie_rule: int = 0
+    tie_rule: int = 4
+    init_tie_rule: int = 4
     p2_div0: int = -1
     threads: int = 0
 
@@ -81,8 +81,8 @@ class PyrConfig:
     p2: int = 150
     peaks_strips: int = 6
     peaks_abs_mode: int = 0
-    tie_rule: int = 0
-    init_tie_rule: int = 0
+    tie_rule: int = 4
+    init_tie_rule: int = 4
     p2_div0: int = -1
     threads: int = 0
 
@@ -101,7 +101,7 @@ def lib():
             build_oracle()
         _lib = C.CDLL(str(_LIB))
         vp, i32 = C.c_void_p, C.c_int32
-        _lib.orc_match_dump.argtypes = [C.POINTER(_Cfg), vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+        _lib.orc_match_dump.argtypes = [C.POINTER(_Cfg)] + [vp] * 13
         _lib.orc_match_dump.restype = i32
         _lib.orc_pyr_match.argtypes = [C.POINTER(_PyrCfg), vp, vp, vp]
         _lib.orc_pyr_match.restype = i32
@@ -141,11 +141,13 @@ def match(cfg: Config, left: np.ndarray, right: np.ndarray, init: np.ndarray | N
         out.update(census_l=np.empty((H, W), np.uint64), census_r=np.empty((H, W), np.uint64),
                    cost=np.empty((H, W, D), np.uint8), paths=np.empty((4, H, W, D), np.uint8),
                    wta_l=np.empty((H, W), np.float32), wta_r=np.empty((H, W), np.float32))
+        if cfg.do_lr_check:
+            out.update(cost_rl=np.zeros((H, W, D), np.uint8), paths_rl=np.zeros((4, H, W, D), np.uint8))
     g = out.get
     init_c = None if init is None else np.ascontiguousarray(init, np.int16)
     rc = lib().orc_match_dump(C.byref(cfg.c()), _p(left), _p(right), _p(init_c), _p(g("census_l")),
-                              _p(g("census_r")), _p(g("cost")), _p(g("paths")), _p(g("wta_l")), _p(g("wta_r")),
-                              _p(out["disp"]), _p(g("disp_r")))
+                              _p(g("census_r")), _p(g("cost")), _p(g("paths")), _p(g("wta_l")), _p(g("cost_rl")),
+                              _p(g("paths_rl")), _p(g("wta_r")), _p(out["disp"]), _p(g("disp_r")))
     if rc != 0:
         raise RuntimeError(f"oracle match failed ({rc})")
     return out

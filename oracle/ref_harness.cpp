@@ -192,9 +192,13 @@ int ref_match_dump(const ref_case_t* c, const uint8_t* left, const uint8_t* righ
 
 // FasterStereoCuda::Match through the reference's public API (per-level options as the
 // reference hard-codes them). Returns 0 on success.
+// The matcher is deliberately never released: HierSgmCudaImpl::Release (FasterStereoCuda.cpp:
+// 641-679) frees each level's pinned disparity buffer before releasing that level's StereoCuda,
+// whose teardown (ThreadBase::WaitForTerminate, common/thread.h) wakes the small-region worker
+// threads once more on the freed buffer -- a host-side use-after-free that crashed the process.
 int ref_pyr_match(int width, int height, int min_disp, int max_disp, int layers, int lr, int peaks,
                   const uint8_t* left, const uint8_t* right, float* disp) {
-  FasterStereoCuda s;
+  FasterStereoCuda& s = *new FasterStereoCuda;  // leaked on purpose, see above
   FasterStereoCuda::StereoOption1 o;
   o.width = width;
   o.height = height;
@@ -206,7 +210,6 @@ int ref_pyr_match(int width, int height, int min_disp, int max_disp, int layers,
   o.do_smooth = false;
   if (!s.Init(o)) { g_msg = "FasterStereoCuda::Init failed"; return -2; }
   const bool ok = s.Match(left, right, disp);
-  s.Release();
   if (!ok || cudaDeviceSynchronize() != cudaSuccess) { g_msg = "FasterStereoCuda::Match failed"; return -4; }
   return 0;
 }
@@ -228,6 +231,31 @@ double ref_time_match(const ref_case_t* c, const uint8_t* left, const uint8_t* r
   cudaDeviceSynchronize();
   const auto t1 = std::chrono::steady_clock::now();
   impl.Release();
+  return std::chrono::duration<double, std::milli>(t1 - t0).count() / n;
+}
+
+// Wall time of n FasterStereoCuda::Match calls (host buffers in and out), ms per call.
+// The matcher is leaked for the reason given at ref_pyr_match.
+double ref_time_pyr(int width, int height, int min_disp, int max_disp, int layers, int lr, int peaks,
+                    const uint8_t* left, const uint8_t* right, int warmup, int n) {
+  FasterStereoCuda& s = *new FasterStereoCuda;
+  FasterStereoCuda::StereoOption1 o;
+  o.width = width;
+  o.height = height;
+  o.min_disp = min_disp;
+  o.max_disp = max_disp;
+  o.num_layers = layers;
+  o.do_lr_check = lr != 0;
+  o.do_rm_peaks = peaks != 0;
+  o.do_smooth = false;
+  if (!s.Init(o)) return -2.0;
+  std::vector<float> d((size_t)width * height);
+  for (int i = 0; i < warmup; ++i) s.Match(left, right, d.data());
+  cudaDeviceSynchronize();
+  const auto t0 = std::chrono::steady_clock::now();
+  for (int i = 0; i < n; ++i) s.Match(left, right, d.data());
+  cudaDeviceSynchronize();
+  const auto t1 = std::chrono::steady_clock::now();
   return std::chrono::duration<double, std::milli>(t1 - t0).count() / n;
 }
 

@@ -260,8 +260,25 @@ static inline float subpix_bias(float c1, float c0, float c2) {
   return (c1 - c2 + den) / (2.0f * den);
 }
 
-static int pick_tie(const uint32_t* S, int D, uint32_t m, int rule) {
+/* y: image row (the measured reference rule depends on its parity). */
+static int pick_tie(const uint32_t* S, int D, uint32_t m, int rule, int y) {
   int best = -1;
+  if (rule == ORC_TIE_REF_B200) {
+    /* Warpfor64 (cusgm_ca.cu:3666-3675): lanes t with S(t)==m store t, lanes with only
+     * S(t+32)==m store t+32; within one store the lowest lane wins; the later of the two
+     * stores wins, and the compiled order differs between the two rows of a WTA block:
+     * on even rows the t+32 store is later, on odd rows the t store. Other D: lowest d. */
+    if (D != 64) rule = ORC_TIE_LOWEST;
+    else {
+      int a = -1, b = -1;
+      for (int t = 0; t < 32; ++t) {
+        if (S[t] == m) { if (a < 0) a = t; }
+        else if (S[t + 32] == m) { if (b < 0) b = t + 32; }
+      }
+      if (y % 2 == 0) return b >= 0 ? b : a;
+      return a >= 0 ? a : b;
+    }
+  }
   switch (rule) {
     case ORC_TIE_HIGHEST:
       for (int d = D - 1; d >= 0; --d) if (S[d] == m) return d;
@@ -312,7 +329,7 @@ void orc_wta_plain(const uint8_t* const paths[4], int W, int H, int x0, int min_
           S[d] = (uint32_t)paths[0][off + d] + paths[1][off + d] + paths[2][off + d] + paths[3][off + d];
           m = umin(m, S[d]);
         }
-        const int ds = pick_tie(S, D, m, tie_rule);
+        const int ds = pick_tie(S, D, m, tie_rule, y);
         if (ds <= 0 || ds >= (warp_kernel ? D : D - 1)) continue;
         const float c1 = (float)S[ds - 1];
         const float c2 = (float)m;
@@ -325,6 +342,18 @@ void orc_wta_plain(const uint8_t* const paths[4], int W, int H, int x0, int min_
     }
     free(S);
   }
+}
+
+/* Output of one winning candidate d at an init-disparity level (cusgm_ca.cu:3488-3509). */
+static float init_candidate(const uint32_t* S, int D, int ds, int base, float ut) {
+  if (ds <= 1 || ds >= D - 1) return ORC_INVALID_FLOAT;
+  const float c1 = (float)S[ds - 1];
+  const float c2 = (float)S[ds];
+  const float c3 = (float)S[ds + 1];
+  const float d12 = c1 - c2, d32 = c3 - c2;
+  const float uniq = d12 < d32 ? d12 : d32;
+  if (uniq <= c2 * ut) return ORC_INVALID_FLOAT;
+  return (float)(ds + base) + subpix_bias(c1, c2, c3);
 }
 
 /* WTA at init-disparity levels. cusgm_ca.cu:3425-3512 (launched with 4 lines, :4073-4077).
@@ -353,15 +382,19 @@ void orc_wta_init(const uint8_t* const paths[4], const int16_t* init, int W, int
           S[d] = (uint32_t)paths[0][off + d] + paths[1][off + d] + paths[2][off + d] + paths[3][off + d];
           m = umin(m, S[d]);
         }
-        const int ds = pick_tie(S, D, m, tie_rule);
-        if (ds <= 1 || ds >= D - 1) continue;
-        const float c1 = (float)S[ds - 1];
-        const float c2 = (float)m;
-        const float c3 = (float)S[ds + 1];
-        const float d12 = c1 - c2, d32 = c3 - c2;
-        const float uniq = d12 < d32 ? d12 : d32;
-        if (uniq <= c2 * ut) continue;
-        *out = (float)(ds + base) + subpix_bias(c1, c2, c3);
+        if (tie_rule == ORC_TIE_REF_B200) {
+          /* every tied lane stores its own result (cusgm_ca.cu:3488-3509); measured on a B200:
+           * a valid disparity wins over INVALID, and the lowest lane wins among valid ones */
+          for (int d = 0; d < D; ++d) {
+            if (S[d] != m) continue;
+            const float v = init_candidate(S, D, d, base, ut);
+            if (v != ORC_INVALID_FLOAT) { *out = v; break; }
+          }
+          continue;
+        }
+        const int ds = pick_tie(S, D, m, tie_rule, y);
+        *out = init_candidate(S, D, ds, base, ut);
+        continue;
       }
     }
     free(S);
@@ -622,7 +655,7 @@ static int run_view(const orc_config_t* c, const uint64_t* cl, const uint64_t* c
  * filter :448-461, D2H then small-region removal :463-498). */
 int orc_match_dump(const orc_config_t* c, const uint8_t* left, const uint8_t* right, const int16_t* init,
                    uint64_t* census_l, uint64_t* census_r, uint8_t* cost_lr, uint8_t* paths_lr, float* wta_l,
-                   float* wta_r, float* disp_l, float* disp_r) {
+                   uint8_t* cost_rl, uint8_t* paths_rl, float* wta_r, float* disp_l, float* disp_r) {
   const int W = c->width, H = c->height, D = c->disp_range;
   if (W <= 0 || H <= 0 || D <= 0 || !left || !right || !disp_l) return -1;
   const size_t N = (size_t)W * H, V = N * D;
@@ -649,7 +682,7 @@ int orc_match_dump(const orc_config_t* c, const uint8_t* left, const uint8_t* ri
       right_init(init, init_r, W, H);
     }
     /* right view: census roles swapped, same cost buffer (stale 5x5 pixels keep L->R cost) */
-    run_view(c, cr, cl, init_r, 0, cost, paths, dr, NULL, NULL);
+    run_view(c, cr, cl, init_r, 0, cost, paths, dr, cost_rl, paths_rl);
     if (wta_r) memcpy(wta_r, dr, sizeof(float) * N);
     memcpy(tmp, dr, sizeof(float) * N);
     orc_lr_check(dl, tmp, dr, W, H, c->lr_threshold);
@@ -677,7 +710,7 @@ done:
 
 int orc_match(const orc_config_t* cfg, const uint8_t* left, const uint8_t* right, const int16_t* init,
               float* disp_l, float* disp_r) {
-  return orc_match_dump(cfg, left, right, init, NULL, NULL, NULL, NULL, NULL, NULL, disp_l, disp_r);
+  return orc_match_dump(cfg, left, right, init, NULL, NULL, NULL, NULL, NULL, NULL, NULL, NULL, disp_l, disp_r);
 }
 
 /* Per-level options and disparity ranges: SetSgmParameters (FasterStereoCuda.cpp:169-199)

@@ -37,7 +37,8 @@ enum {
   ORC_TIE_LOWEST = 0,     /* smallest d */
   ORC_TIE_HIGHEST = 1,    /* largest d */
   ORC_TIE_LANE_HIGH = 2,  /* warp mapping d = lane + 32*j: highest lane wins, lowest j within it */
-  ORC_TIE_LANE_LOW = 3    /* warp mapping d = lane + 32*j: lowest lane wins, lowest j within it */
+  ORC_TIE_LANE_LOW = 3,   /* warp mapping d = lane + 32*j: lowest lane wins, lowest j within it */
+  ORC_TIE_REF_B200 = 4    /* the reference build's behaviour measured on a B200 (see orc_wta_plain/init) */
 };
 
 /* Region-growing neighbour test used by small-region removal. */
@@ -96,10 +97,11 @@ int orc_match(const orc_config_t* cfg, const uint8_t* left, const uint8_t* right
               float* disp_l, float* disp_r);
 
 /* Stage dump variant used by tests: any output pointer may be NULL.
- * cost_lr / paths_lr[4] are [H][W][D]; wta_l is the left WTA map before LR/median. */
+ * cost_* are [H][W][D], paths_* [4][H][W][D] (left view: *_lr, right view: *_rl, the latter
+ * only computed with the LR check); wta_* are the WTA maps before LR/median. */
 int orc_match_dump(const orc_config_t* cfg, const uint8_t* left, const uint8_t* right, const int16_t* init,
-                   uint64_t* census_l, uint64_t* census_r, uint8_t* cost_lr, uint8_t* paths_lr /*4*H*W*D*/,
-                   float* wta_l, float* wta_r, float* disp_l, float* disp_r);
+                   uint64_t* census_l, uint64_t* census_r, uint8_t* cost_lr, uint8_t* paths_lr, float* wta_l,
+                   uint8_t* cost_rl, uint8_t* paths_rl, float* wta_r, float* disp_l, float* disp_r);
 
 /* ---- pyramid (FasterStereoCuda::Match) ---- */
 typedef struct {

@@ -213,6 +213,31 @@ def path_first_pixel_mask(W, H, x0):
     return m
 
 
+def _race_free_lr(O, wta_l, wta_r, thr):
+    """Pixels whose LR result is the same whether the right map is read before or after every
+    invalidation (the reference reads it while other threads invalidate it)."""
+    a = wta_l.copy()
+    marks = wta_r.copy()
+    O.lib().orc_lr_check(a.ctypes.data, wta_r.ctypes.data, marks.ctypes.data, a.shape[1], a.shape[0], C.c_float(thr))
+    b = wta_l.copy()
+    O.lib().orc_lr_check(b.ctypes.data, marks.ctypes.data, None, b.shape[1], b.shape[0], C.c_float(thr))
+    return a.view(np.uint32) == b.view(np.uint32), a
+
+
+def _race_free_median(O, inp):
+    """Pixels whose median is the same when neighbouring blocks of the reference's in-place
+    median (30x2 outputs per block) have already written their filtered values."""
+    H, W = inp.shape
+    snap = O.median3x3(inp)
+    mixed = inp.copy()
+    ys, xs = np.mgrid[0:H, 0:W]
+    # a block writes rows 2by+1..2by+2 and columns 30bx+1..30bx+30; its halo rows/columns belong to others
+    boundary_rows = (ys % 2 == 0) | (ys % 2 == 1)
+    mixed[boundary_rows] = snap[boundary_rows]
+    alt = O.median3x3(mixed)
+    return snap.view(np.uint32) == alt.view(np.uint32), snap
+
+
 def finalize(dump_dir: Path, write: bool = True):
     meta = json.loads((dump_dir / "meta.json").read_text())
     report = {}
@@ -226,62 +251,77 @@ def finalize(dump_dir: Path, write: bool = True):
                              peaks_strips=meta["peaks_strips"])
             d = O.pyr_match(pc, z["left"], z["right"])
             same = (d.view(np.uint32) == z["disp"].view(np.uint32))
-            report[name] = {"disp_equal": float(same.mean())}
+            report[name] = {"disp_equal": float(same[:case["height"] - 1].mean())}
             if write:
                 np.savez_compressed(GOLDEN / f"ref_{name}.npz", left=z["left"], right=z["right"], disp=z["disp"],
                                     case=z["case"], peaks_strips=np.int32(meta["peaks_strips"]))
             continue
         W, H, D = case["width"], case["height"], case["disp_range"]
         init = z.get("init")
-        cfg = O.Config(width=W, height=H, min_disp=case["min_disp"], disp_range=D, cs_type=case["cs_type"],
-                       p1=case["p1"], p2=case["p2"], uniqueness=case["uniqueness"], do_lr_check=0, do_median=0,
-                       peaks_strips=meta["peaks_strips"])
-        r = {}
-        a = O.match(cfg, z["left"], z["right"], init, dump=True)
         x0 = max(0, case["min_disp"])
+        cfg = O.Config(width=W, height=H, min_disp=case["min_disp"], disp_range=D, cs_type=case["cs_type"],
+                       p1=case["p1"], p2=case["p2"], uniqueness=case["uniqueness"], do_lr_check=1, do_median=0,
+                       peaks_strips=meta["peaks_strips"], tie_rule=4, init_tie_rule=4)
+        r = {}
+        a = O.match(cfg, z["left"], z["right"], init, dump=True, want_right=True)
+        written = np.zeros((H, W), bool)
+        written[:(H // 4) * 4 if init is not None else (H // 2) * 2, x0:] = True
         if "census_l" in z:
             r["census_l"] = _eq(a["census_l"], z["census_l"])
             r["census_r"] = _eq(a["census_r"], z["census_r"])
             cm = np.zeros((H, W), bool)
             cm[:, x0:] = True
-            r["cost_lr"] = float((a["cost"] == z["cost_lr"])[cm].mean())
             fm = path_first_pixel_mask(W, H, x0)
             valid = np.broadcast_to(cm, (4, H, W)) & ~fm
             if init is not None:
-                valid = valid & (np.broadcast_to(init != -32768, (4, H, W)))
-            pe = (a["paths"] == z["paths_lr"]).all(-1)
-            r["paths_lr"] = [float(pe[k][valid[k]].mean()) for k in range(4)]
-        # WTA: equality per tie rule, and on pixels without ties
-        best = None
-        for rule in range(4):
-            c2 = O.Config(**{**cfg.__dict__, "tie_rule": rule, "init_tie_rule": rule})
-            w = O.match(c2, z["left"], z["right"], init)["disp"]
-            eq = float((w.view(np.uint32) == z["wta_l"].view(np.uint32)).mean())
-            r[f"wta_rule{rule}"] = eq
-            if best is None or eq > best[1]:
-                best = (rule, eq)
-        r["wta_best_rule"] = best[0]
-        # full options under the best rule
+                valid = valid & np.broadcast_to(init != -32768, (4, H, W))
+            for tag, ours_c, ours_p in (("lr", a["cost"], a["paths"]), ("rl", a.get("cost_rl"), a.get("paths_rl"))):
+                if ours_c is None or ("cost_" + tag) not in z:
+                    continue
+                if tag == "rl" and init is not None:
+                    continue  # right view of an init level: right initial disparities differ by design
+                r["cost_" + tag] = float((ours_c == z["cost_" + tag]).all(-1)[cm].mean())
+                pe = (ours_p == z["paths_" + tag]).all(-1)
+                r["paths_" + tag] = [float(pe[k][valid[k]].mean()) for k in range(4)]
+        r["wta_written"] = float((a["wta_l"].view(np.uint32) == z["wta_l"].view(np.uint32))[written].mean())
+        # LR stage (run B: LR on, median off) -- only on plain levels (init levels have no LR in the pyramid)
+        if init is None:
+            rf, lr_ours = _race_free_lr(O, a["wta_l"], a["wta_r"], case["lr_threshold"])
+            eq = lr_ours.view(np.uint32) == z["lr_l"].view(np.uint32)
+            r["lr_all"] = float(eq[written].mean())
+            r["lr_race_free"] = float(eq[written & rf].mean())
+            r["lr_race_free_frac"] = float(rf[written].mean())
+            r["lr_right_all"] = float((a["disp_r"].view(np.uint32) == z["lr_r"].view(np.uint32))[written].mean())
+        # full options
         cf = O.Config(**{**cfg.__dict__, "do_lr_check": case["do_lr_check"], "do_median": case["do_median"],
                          "morphology_dilation": int(case["morphology"] == 2),
-                         "do_remove_peaks": case["do_remove_peaks"], "peaks_ratio": case["peaks_ratio"],
-                         "tie_rule": best[0], "init_tie_rule": best[0]})
-        full = O.match(cf, z["left"], z["right"], init, want_right=True)
-        rows = slice(0, H - 1) if H % 2 else slice(0, H)  # the reference never writes the last odd row
-        r["disp_equal"] = float((full["disp"][rows].view(np.uint32) == z["disp_l"][rows].view(np.uint32)).mean())
+                         "do_remove_peaks": case["do_remove_peaks"], "peaks_ratio": case["peaks_ratio"]})
+        full = O.match(cf, z["left"], z["right"], init)["disp"]
+        rows = np.zeros((H, W), bool)
+        rows[:H - 1 if H % 2 else H] = True  # the reference never writes the last odd row
+        eq = full.view(np.uint32) == z["disp_l"].view(np.uint32)
+        r["disp_all"] = float(eq[rows].mean())
+        if case["do_median"] and not case["do_remove_peaks"] and case["morphology"] == 0:
+            pre = z["lr_l"] if case["do_lr_check"] else z["wta_l"]
+            mf, _ = _race_free_median(O, pre)
+            mf[-2:] = False
+            r["disp_median_race_free"] = float(eq[rows & mf].mean())
+            r["median_race_free_frac"] = float(mf[rows].mean())
         report[name] = r
         if write:
-            keep = {k: z[k] for k in ("left", "right", "wta_l", "lr_l", "lr_r", "disp_l", "disp_r", "case") if k in z}
+            keep = {k: z[k] for k in ("left", "right", "wta_l", "lr_l", "lr_r", "disp_l", "case") if k in z}
             if init is not None:
                 keep["init"] = init
             if "census_l" in z:
-                keep["census_l"], keep["census_r"] = z["census_l"], z["census_r"]
+                keep["digest_census"] = np.array(digest(np.stack([z["census_l"], z["census_r"]])))
                 keep["digest_cost_lr"] = np.array(digest(np.where(cm[..., None], z["cost_lr"], 0)))
+                pz = np.where(valid[..., None], z["paths_lr"], 0)
+                keep["digest_paths_lr"] = np.array(digest(pz))
             keep["peaks_strips"] = np.int32(meta["peaks_strips"])
             np.savez_compressed(GOLDEN / f"ref_{name}.npz", **keep)
     print(json.dumps(report, indent=1))
     if write:
-        (GOLDEN / "ref_agreement.json").write_text(json.dumps(report, indent=1))
+        (GOLDEN / "ref_agreement.json").write_text(json.dumps(report, indent=1) + "\n")
     return report
 
 

@@ -83,3 +83,14 @@ def test_roi_from_disp_map(engine_lib):
     roi = fsc.StereoROI()
     fsc.StereoCuda.GetRoiFromDispMap(d, 30, 20, roi)
     assert (roi.x, roi.y, roi.w, roi.h) == (7, 5, 12, 7)
+
+
+def test_cxx_classes_export_the_reference_symbols(engine_lib):
+    """StereoCuda / FasterStereoCuda export exactly the mangled names of the reference's classes
+    (list taken from the reference built from its sources), so reference-linked code relinks."""
+    want = set((ROOT / "tests" / "golden" / "reference_cxx_symbols.txt").read_text().split())
+    lib_path = ROOT / "fasterstereocuda_b200" / "_lib" / "libsgmb200.so"
+    out = subprocess.run(["nm", "-D", "--defined-only", str(lib_path)], capture_output=True, text=True, check=True)
+    have = {l.split()[-1] for l in out.stdout.splitlines() if "10StereoCuda" in l or "16FasterStereoCuda" in l}
+    assert len(want) == 28
+    assert want == have, (sorted(want - have), sorted(have - want))

@@ -37,7 +37,7 @@ def assert_same(name, got, exp, mask=None):
         pytest.fail(f"{name}: {n} mismatches, first {detail}")
 
 
-def make_engine(fsc, W, H, M, D, cs, p1, p2, u, lr, med, peaks=0, ratio=0.0005, morph=0, tie=0):
+def make_engine(fsc, W, H, M, D, cs, p1, p2, u, lr, med, peaks=0, ratio=0.0005, morph=0, tie=4):
     s = fsc.StereoCuda()
     opt = fsc.CuSGMOption(p1=p1, p2_init=p2, cs_type=cs, num_paths=4, do_median_filter=bool(med),
                           do_lr_check=bool(lr), lr_threshold=1.0, unique_threshold=u, using_constant_p2=True,
@@ -66,12 +66,12 @@ CASES = {
 
 
 @pytest.mark.parametrize("name", list(CASES))
-@pytest.mark.parametrize("tie", [0, 2])
+@pytest.mark.parametrize("tie", [4, 0, 2])
 def test_plain_parity(engine_lib, oracle_mod, name, tie):
     import fasterstereocuda_b200 as fsc
     O = oracle_mod
     W, H, M, D, cs, p1, p2, u, lr, med, peaks, morph, seed = CASES[name]
-    if tie and name not in ("d64_9x7_lr_med", "d128", "d32_plain", "d256_generic"):
+    if tie != 4 and name not in ("d64_9x7_lr_med", "d128", "d32_plain", "d256_generic"):
         pytest.skip("tie rule variants on a subset")
     L, R, _ = scenes.planar_pair(seed, W, H, dmin=2.0, dmax=min(60.0, D - 4.0))
     ratio = 0.005 if peaks else 0.0005
@@ -108,19 +108,20 @@ def _init_for(O, L, R, cs, p1, p2):
     return O.init_next_level(coarse, w, h)
 
 
+@pytest.mark.parametrize("tie", [4, 0])
 @pytest.mark.parametrize("cs,p1,p2,lr,u", [(1, 10, 150, 0, 1.0), (0, 8, 32, 0, 0.95), (1, 10, 150, 1, 0.95),
                                            (0, 8, 32, 1, 1.0)])
-def test_init_disparity_parity(engine_lib, oracle_mod, cs, p1, p2, lr, u):
+def test_init_disparity_parity(engine_lib, oracle_mod, cs, p1, p2, lr, u, tie):
     import fasterstereocuda_b200 as fsc
     O = oracle_mod
     W, H = 162, 121
     L, R, _ = scenes.planar_pair(31 + cs, W, H)
     init = _init_for(O, L, R, cs, p1, p2)
-    s = make_engine(fsc, W, H, 0, 32, cs, p1, p2, u, lr, 1)
+    s = make_engine(fsc, W, H, 0, 32, cs, p1, p2, u, lr, 1, tie=tie)
     disp = np.empty((H, W), np.float32)
     assert s.Match(L, R, disp, None, init), s.last_error()
     cfg = O.Config(width=W, height=H, disp_range=32, cs_type=cs, p1=p1, p2=p2, uniqueness=u, do_lr_check=lr,
-                   do_median=1, peaks_strips=STRIPS)
+                   do_median=1, peaks_strips=STRIPS, tie_rule=tie, init_tie_rule=tie)
     ref = O.match(cfg, L, R, init, dump=True, want_right=True)
     valid = init != -32768
     assert_same("cost", s.debug_read("cost"), ref["cost"])
