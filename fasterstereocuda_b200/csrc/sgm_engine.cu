@@ -128,6 +128,8 @@ void dfree(T*& p) {
 
 }  // namespace
 
+void sgm_set_process_error(const char* msg) { set_error(nullptr, "%s", msg); }
+
 // One matching level (the state of one StereoCuda instance).
 struct sgm_engine {
   bool ready = false;
@@ -155,6 +157,11 @@ struct sgm_engine {
   unsigned* key = nullptr;
   int* label = nullptr;
   int* count = nullptr;
+  bool own_volumes = true;  // false: cost/lr/rl/bt belong to a batch arena
+  int tune_rows = 0;        // rows per CTA of the row kernels (0: default)
+  int tune_cols = 0;        // columns per CTA of the column kernels (0: default)
+  int tune_bt_smem = 0;     // 1: keep bottom->top path costs in shared memory when they fit
+  bool bt_stored = true;    // the last match wrote the bottom->top volume to global memory
 
   int nviews() const { return opt.do_lr_check ? 2 : 1; }
   size_t npix() const { return (size_t)W * H; }
@@ -168,7 +175,10 @@ struct sgm_engine {
       if (cs[i]) cudaFree(cs[i]);
       cs[i] = nullptr;
     }
-    dfree(cost); dfree(lr); dfree(rl); dfree(bt);
+    if (own_volumes) {
+      dfree(cost); dfree(lr); dfree(rl); dfree(bt);
+    }
+    cost = lr = rl = bt = nullptr;
     dfree(wta); dfree(post); dfree(post2); dfree(dr_out); dfree(out);
     dfree(init_tmp); dfree(key); dfree(label); dfree(count);
     if (stream) cudaStreamDestroy(stream);
@@ -236,8 +246,10 @@ int validate(sgm_engine* e, int W, int H, int D, const sgm_option_t* o) {
   return SGM_OK;
 }
 
-int engine_init(sgm_engine* e, int W, int H, int M, int D, const sgm_option_t* o, bool log) {
+// volumes == false: the cost and path volumes are supplied later (batch arena).
+int engine_init(sgm_engine* e, int W, int H, int M, int D, const sgm_option_t* o, bool log, bool volumes = true) {
   if (e->ready) e->free_all();
+  e->own_volumes = volumes;
   const int v = validate(e, W, H, D, o);
   if (v != SGM_OK) return v;
   SGM_CUDA_TRY(e, cudaGetDevice(&e->dev));
@@ -252,10 +264,12 @@ int engine_init(sgm_engine* e, int W, int H, int M, int D, const sgm_option_t* o
     SGM_CUDA_TRY(e, cudaMalloc(&e->cs[i], N * 8));
     SGM_CUDA_TRY(e, dalloc(&e->init[i], N));
   }
-  SGM_CUDA_TRY(e, dalloc(&e->cost, V));
-  SGM_CUDA_TRY(e, dalloc(&e->lr, V));
-  SGM_CUDA_TRY(e, dalloc(&e->rl, V));
-  SGM_CUDA_TRY(e, dalloc(&e->bt, V));
+  if (volumes) {
+    SGM_CUDA_TRY(e, dalloc(&e->cost, V));
+    SGM_CUDA_TRY(e, dalloc(&e->lr, V));
+    SGM_CUDA_TRY(e, dalloc(&e->rl, V));
+    SGM_CUDA_TRY(e, dalloc(&e->bt, V));
+  }
   SGM_CUDA_TRY(e, dalloc(&e->wta, 2 * N));
   SGM_CUDA_TRY(e, dalloc(&e->post, N));
   SGM_CUDA_TRY(e, dalloc(&e->post2, N));
@@ -268,6 +282,30 @@ int engine_init(sgm_engine* e, int W, int H, int M, int D, const sgm_option_t* o
   e->ready = true;
   if (log) printf("sgm-b200: init %dx%d, disparities %d..%d, census %s\n", W, H, M, M + D, o->cs_type ? "9x7" : "5x5");
   return SGM_OK;
+}
+
+// Columns per CTA of the vertical kernels and whether the bottom->top path costs of those
+// columns fit in shared memory (H*C*D bytes, at most 100 KB so two CTAs share an SM).
+void vertical_shape(int H, int D, int* C, int* bt_smem, size_t* smem, int max_cols = 0, int use_smem = 0) {
+  const size_t per_col = (size_t)H * D;
+  const size_t budget = 100 * 1024;
+  int c = max_cols > 0 ? max_cols : 8;
+  if (!use_smem) {
+    *C = c;
+    *bt_smem = 0;
+    *smem = 0;
+    return;
+  }
+  while (c > 2 && per_col * c > budget) c >>= 1;
+  if (per_col * c <= budget) {
+    *C = c;
+    *bt_smem = 1;
+    *smem = per_col * c;
+  } else {
+    *C = 8;
+    *bt_smem = 0;
+    *smem = 0;
+  }
 }
 
 int rows_per_cta(int W, int word_bytes, bool with_init) {
@@ -284,13 +322,9 @@ int launch_plain(sgm_engine* e, const Word* csl, const Word* csr, float* wta) {
   P.p1 = (uint32_t)e->opt.p1; P.p2 = (uint32_t)e->opt.p2_init;
   P.vstride = e->vol();
   const int nv = e->nviews();
-  const int R = rows_per_cta(e->W, sizeof(Word), false);
-  const size_t smem = (size_t)R * 2 * e->W * sizeof(Word);
-  if (smem > 227 * 1024) {
-    set_error(&e->err, "image width %d too large for the row kernel", e->W);
-    return SGM_ERR_UNSUPPORTED;
-  }
-  auto hk = sgm::k_hpaths_plain<K, Word>;
+  const int R = e->tune_rows > 0 ? e->tune_rows : 4;
+  const size_t smem = (size_t)2 * R * sgm::hpaths2_warp_smem<K, Word>();
+  auto hk = sgm::k_hpaths_plain2<K, Word>;
   SGM_CUDA_TRY(e, cudaFuncSetAttribute(hk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 hg((e->H + R - 1) / R, nv), hb(32, 2 * R);
   int st = SGM_LAUNCH(e, e->stream, "hpaths_plain", hk<<<hg, hb, smem, e->stream>>>(csl, csr, e->cost, e->lr, e->rl, P));
@@ -302,9 +336,15 @@ int launch_plain(sgm_engine* e, const Word* csl, const Word* csr, float* wta) {
   Q.rows = warp_kernel ? (e->H / 2) * 2 : e->H;
   Q.dmax_excl = warp_kernel ? 32 * K : 32 * K - 1;
   Q.dstride = e->npix();
-  dim3 vg((e->W + 7) / 8, nv), vb(32, 8);
+  int C = 8, bt_smem = 0;
+  size_t vsmem = 0;
+  vertical_shape(e->H, 32 * K, &C, &bt_smem, &vsmem, e->tune_cols, e->tune_bt_smem);
+  e->bt_stored = !bt_smem;
+  auto vk = sgm::k_vpaths_wta_plain2<K, 8>;
+  if (vsmem) SGM_CUDA_TRY(e, cudaFuncSetAttribute(vk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vsmem));
+  dim3 vg((e->W + C - 1) / C, nv), vb(32, C);
   return SGM_LAUNCH(e, e->stream, "vpaths_wta_plain",
-                    sgm::k_vpaths_wta_plain<K><<<vg, vb, 0, e->stream>>>(e->cost, e->lr, e->rl, e->bt, wta, P, Q));
+                    vk<<<vg, vb, vsmem, e->stream>>>(e->cost, e->lr, e->rl, e->bt, wta, P, Q, bt_smem));
 }
 
 template <typename Word>
@@ -315,13 +355,15 @@ int launch_init(sgm_engine* e, const Word* csl, const Word* csr, const int16_t* 
   P.invalid_cost = e->opt.cs_type == 1 ? 0xFFu : sgm::kInvalidCost;
   P.vstride = e->vol();
   const int nv = e->nviews();
-  const int R = rows_per_cta(e->W, sizeof(Word), true);
-  const size_t smem = (size_t)R * e->W * (2 * sizeof(Word) + 2);
-  if (smem > 227 * 1024) {
+  int R = 4;
+  const size_t row_bytes = ((size_t)e->W * (2 * sizeof(Word) + 2) + 15) & ~size_t(15);  // as in the kernel
+  while (R > 1 && R * row_bytes > 120 * 1024) R >>= 1;
+  const size_t smem = R * row_bytes + (size_t)2 * R * sgm::hinit2_warp_smem();
+  if (smem > 220 * 1024) {
     set_error(&e->err, "image width %d too large for the row kernel", e->W);
     return SGM_ERR_UNSUPPORTED;
   }
-  auto hk = sgm::k_hpaths_init<Word>;
+  auto hk = sgm::k_hpaths_init2<Word>;
   SGM_CUDA_TRY(e, cudaFuncSetAttribute(hk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 hg((e->H + R - 1) / R, nv), hb(32, 2 * R);
   int st = SGM_LAUNCH(e, e->stream, "hpaths_init", hk<<<hg, hb, smem, e->stream>>>(csl, csr, il, ir, e->cost, e->lr, e->rl, P));
@@ -332,9 +374,15 @@ int launch_init(sgm_engine* e, const Word* csl, const Word* csr, const int16_t* 
   Q.rows = (e->H / 4) * 4;
   Q.dmax_excl = sgm::kLevelRange - 1;
   Q.dstride = e->npix();
-  dim3 vg((e->W + 7) / 8, nv), vb(32, 8);
+  int C = 8, bt_smem = 0;
+  size_t vsmem = 0;
+  vertical_shape(e->H, sgm::kLevelRange, &C, &bt_smem, &vsmem, e->tune_cols, e->tune_bt_smem);
+  e->bt_stored = !bt_smem;
+  auto vk = sgm::k_vpaths_wta_init2<8>;
+  if (vsmem) SGM_CUDA_TRY(e, cudaFuncSetAttribute(vk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vsmem));
+  dim3 vg((e->W + C - 1) / C, nv), vb(32, C);
   return SGM_LAUNCH(e, e->stream, "vpaths_wta_init",
-                    sgm::k_vpaths_wta_init<<<vg, vb, 0, e->stream>>>(e->cost, e->lr, e->rl, il, ir, e->bt, wta, P, Q));
+                    vk<<<vg, vb, vsmem, e->stream>>>(e->cost, e->lr, e->rl, il, ir, e->bt, wta, P, Q, bt_smem));
 }
 
 // Enqueues one full match of this level on s. Inputs/outputs are dense device arrays.
@@ -812,7 +860,13 @@ int sgm_debug_read(sgm_handle_t h, int32_t which, int32_t view, void* dst, size_
     case 2: src = h->cost + view * V; break;
     case 3: src = h->lr + view * V; break;
     case 4: src = h->rl + view * V; break;
-    case 5: src = h->bt + view * V; break;
+    case 5:
+      if (!h->bt_stored) {
+        set_error(&h->err, "the last match kept the bottom->top path costs in shared memory");
+        return SGM_ERR_STATE;
+      }
+      src = h->bt + view * V;
+      break;
     case 6: src = reinterpret_cast<const uint8_t*>(h->wta + view * N); n = N * sizeof(float); break;
     default: return SGM_ERR_ARG;
   }

@@ -85,6 +85,30 @@ __device__ __forceinline__ void store_u8(uint8_t* p, const uint32_t (&v)[K]) {
   }
 }
 
+// K bytes read through L2 (ld.global.cg): for data other warps of the same kernel write
+// (adjacent columns share cache lines, so the read-only path could hold a stale line).
+template <int K>
+__device__ __forceinline__ void load_u8_cg(const uint8_t* p, uint32_t (&v)[K]) {
+  if constexpr (K == 1) {
+    v[0] = __ldcg(p);
+  } else if constexpr (K == 2) {
+    const uint32_t w = __ldcg(reinterpret_cast<const uint16_t*>(p));
+    v[0] = w & 0xFFu;
+    v[1] = w >> 8;
+  } else if constexpr (K == 4) {
+    const uint32_t w = __ldcg(reinterpret_cast<const uint32_t*>(p));
+#pragma unroll
+    for (int j = 0; j < 4; ++j) v[j] = (w >> (8 * j)) & 0xFFu;
+  } else {
+    const uint2 w = __ldcg(reinterpret_cast<const uint2*>(p));
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      v[j] = (w.x >> (8 * j)) & 0xFFu;
+      v[4 + j] = (w.y >> (8 * j)) & 0xFFu;
+    }
+  }
+}
+
 template <int K>
 __device__ __forceinline__ void load_u8(const uint8_t* p, uint32_t (&v)[K]) {
   if constexpr (K == 1) {
@@ -201,6 +225,138 @@ __global__ void __launch_bounds__(256) k_hpaths_plain(const Word* __restrict__ c
     }
     store_u8<K>(out + off, L);
     if (dir == 0) store_u8<K>(cvol + off, c);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Horizontal scans, second form. Each warp walks its row in chunks of 32 pixels:
+//   1. the census words the chunk needs (32 own words and the D+31 partner words, out-of-range
+//      partners replaced by element 0 of the row) are staged in the warp's shared window;
+//   2. every lane computes the D costs of one pixel of the chunk (off the serial chain);
+//   3. the 32 recurrence steps read their costs from shared memory;
+//   4. the chunk's path costs (and, for the left-to-right warp, its costs) leave with coalesced
+//      16-byte stores.
+// Same results as k_hpaths_plain (reference kernels listed there). Shared memory per warp:
+// window (D+64 words) + cost chunk (32 x (D+4) bytes) + path chunk (32 x D bytes).
+// ---------------------------------------------------------------------------------------------
+template <int K, typename Word>
+__host__ __device__ constexpr size_t hpaths2_warp_smem() {
+  return (size_t)(32 * K + 64) * sizeof(Word) + 32 * (32 * K + 4) + 32 * (32 * K);
+}
+
+template <int K, typename Word>
+__global__ void __launch_bounds__(256) k_hpaths_plain2(const Word* __restrict__ cs_l, const Word* __restrict__ cs_r,
+                                                       uint8_t* __restrict__ cost, uint8_t* __restrict__ lr,
+                                                       uint8_t* __restrict__ rl, PlainParams P) {
+  constexpr int D = 32 * K;
+  constexpr int CST = D + 4;  // padded row stride of the cost chunk (bank-conflict free prologue)
+  const int view = blockIdx.y;
+  const int lane = threadIdx.x;
+  const int wid = threadIdx.y;
+  const int R = blockDim.y >> 1;
+  const int y = blockIdx.x * R + (wid >> 1);
+  const int dir = wid & 1;
+  const int W = P.W;
+  if (y >= P.H) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  unsigned char* base = smem_raw + (size_t)wid * hpaths2_warp_smem<K, Word>();
+  Word* win = reinterpret_cast<Word*>(base);                   // [D + 64]: own[32], partner[D + 31]
+  uint8_t* cbuf = base + (size_t)(D + 64) * sizeof(Word);      // [32][CST]
+  uint8_t* pbuf = cbuf + 32 * CST;                             // [32][D]
+  const int x0 = P.x0;
+  const int len = W - x0;
+  if (len <= 0) return;
+  const size_t vo = (size_t)view * P.vstride;
+  const Word* g_own = (view == 0 ? cs_l : cs_r) + (size_t)y * W;
+  const Word* g_oth = (view == 0 ? cs_r : cs_l) + (size_t)y * W;
+  const Word oth0 = g_oth[0];
+  uint8_t* out = (dir == 0 ? lr : rl) + vo + (size_t)y * W * D;
+  uint8_t* cout = cost + vo + (size_t)y * W * D;
+  const bool stale5 = (view == 1) && (sizeof(Word) == 4);
+  const Word own0 = g_own[0];
+  uint32_t L[K];
+  uint32_t m = 0;
+  const int nchunks = (len + 31) >> 5;
+  for (int c = 0; c < nchunks; ++c) {
+    const int s0 = c << 5;
+    const int n = min(32, len - s0);
+    const int xa = dir == 0 ? x0 + s0 : W - (s0 + n);  // lowest pixel of the chunk
+    // 1. census window
+    const int ws = view == 0 ? xa - P.min_d - (D - 1) : xa + P.min_d;
+    __syncwarp();
+    for (int i = lane; i < D + 31; i += 32) {
+      const int pos = ws + i;
+      win[32 + i] = (pos >= 0 && pos < W) ? g_oth[pos] : oth0;
+    }
+    win[lane] = lane < n ? g_own[xa + lane] : (Word)0;
+    __syncwarp();
+    // 2. costs of pixel xa + lane for every d
+    if (lane < n) {
+      const int x = xa + lane;
+      const Word a = win[lane];
+      bool lr_cost = false;
+      if (stale5) {
+        const int blk = x0 + ((x - x0) / D) * D;
+        lr_cost = (x == blk + min(D, W - blk) - 1);
+      }
+      uint32_t* crow = reinterpret_cast<uint32_t*>(cbuf + lane * CST);
+#pragma unroll 4
+      for (int d4 = 0; d4 < D; d4 += 4) {
+        uint32_t packed = 0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int d = d4 + q;
+          Word partner;
+          if (!lr_cost) {
+            // view 0: pos = x - min_d - d -> window index (x - xa) + (D - 1) - d
+            // view 1: pos = x + min_d + d -> window index (x - xa) + d
+            partner = win[32 + (view == 0 ? lane + (D - 1) - d : lane + d)];
+          } else {  // 5x5 right view: this pixel keeps its left-to-right cost
+            const int pos = x - P.min_d - d;
+            partner = (pos >= 0 && pos < W) ? g_own[pos] : own0;
+          }
+          const Word own_word = lr_cost ? g_oth[x] : a;
+          packed |= popc_word((Word)(own_word ^ partner)) << (8 * q);
+        }
+        crow[d4 >> 2] = packed;
+      }
+    }
+    __syncwarp();
+    // 3. recurrence over the chunk
+    for (int i = 0; i < n; ++i) {
+      const int s = s0 + i;
+      const int px = dir == 0 ? i : n - 1 - i;  // buffer row of this step's pixel
+      const uint8_t* cr = cbuf + px * CST + lane * K;
+      uint32_t cv[K];
+#pragma unroll
+      for (int j = 0; j < K; ++j) cv[j] = cr[j];
+      if (s == 0) {
+        uint32_t mn = 0xFFFFFFFFu;
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+          L[j] = cv[j];
+          mn = min(mn, cv[j]);
+        }
+        m = __reduce_min_sync(kFull, mn);
+      } else {
+        m = plain_step<K>(L, cv, m, P.p1, P.p2, lane);
+      }
+      store_u8<K>(pbuf + px * D + lane * K, L);
+    }
+    __syncwarp();
+    // 4. write the chunk: n pixels x D bytes contiguous in both volumes
+    const int bytes = n * D;
+    uint8_t* og = out + (size_t)xa * D;
+    for (int b = lane * 16; b < bytes; b += 32 * 16)
+      *reinterpret_cast<uint4*>(og + b) = *reinterpret_cast<const uint4*>(pbuf + b);
+    if (dir == 0) {  // costs: 4-byte words (the padded chunk rows are only 4-byte aligned)
+      uint32_t* cg = reinterpret_cast<uint32_t*>(cout + (size_t)xa * D);
+      const uint32_t* cb = reinterpret_cast<const uint32_t*>(cbuf);
+      for (int w = lane; w < bytes / 4; w += 32) {
+        const int row = w / (D / 4), col = w - row * (D / 4);
+        cg[w] = cb[row * (CST / 4) + col];
+      }
+    }
   }
 }
 
@@ -327,7 +483,7 @@ __global__ void __launch_bounds__(256) k_vpaths_wta_plain(const uint8_t* __restr
     float dv = kInvalidFloat;
     if (col_ok && y >= 5 && y <= H - 5 && y < Q.rows) {
       uint32_t a[K], b[K], e[K], S[K];
-      load_u8<K>(btv + off, a);
+      load_u8_cg<K>(btv + off, a);
       load_u8<K>(lrv + off, b);
       load_u8<K>(rlv + off, e);
 #pragma unroll
@@ -335,6 +491,170 @@ __global__ void __launch_bounds__(256) k_vpaths_wta_plain(const uint8_t* __restr
       dv = wta_pixel<K>(S, lane, P.min_d, Q, 0, y);
     }
     if (lane == 0) dout[(size_t)y * W + x] = dv;
+  }
+}
+
+// Packed K bytes of one lane (K disparities) as loaded from a [..][D] u8 volume.
+template <int K> struct PackOf { using T = uint32_t; };
+template <> struct PackOf<8> { using T = uint2; };
+
+template <int K>
+__device__ __forceinline__ typename PackOf<K>::T ld_pack_cg(const uint8_t* p) {
+  if constexpr (K == 1) return __ldcg(p);
+  else if constexpr (K == 2) return __ldcg(reinterpret_cast<const uint16_t*>(p));
+  else if constexpr (K == 4) return __ldcg(reinterpret_cast<const uint32_t*>(p));
+  else return __ldcg(reinterpret_cast<const uint2*>(p));
+}
+
+template <int K>
+__device__ __forceinline__ typename PackOf<K>::T ld_pack(const uint8_t* p) {
+  if constexpr (K == 1) return __ldg(p);
+  else if constexpr (K == 2) return __ldg(reinterpret_cast<const uint16_t*>(p));
+  else if constexpr (K == 4) return __ldg(reinterpret_cast<const uint32_t*>(p));
+  else return __ldg(reinterpret_cast<const uint2*>(p));
+}
+
+// The same K bytes read from shared memory with an access of exactly their size (the address
+// is aligned to K bytes only).
+template <int K>
+__device__ __forceinline__ typename PackOf<K>::T ld_pack_shared(const uint8_t* p) {
+  if constexpr (K == 1) return *p;
+  else if constexpr (K == 2) return *reinterpret_cast<const uint16_t*>(p);
+  else if constexpr (K == 4) return *reinterpret_cast<const uint32_t*>(p);
+  else return *reinterpret_cast<const uint2*>(p);
+}
+
+template <int K>
+__device__ __forceinline__ void unpack(const typename PackOf<K>::T& w, uint32_t (&v)[K]) {
+  if constexpr (K == 8) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      v[j] = (w.x >> (8 * j)) & 0xFFu;
+      v[4 + j] = (w.y >> (8 * j)) & 0xFFu;
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < K; ++j) v[j] = (w >> (8 * j)) & 0xFFu;
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Vertical scans + WTA, second form: the per-row loads of the serial chain come from a
+// PF-deep register ring filled PF rows ahead, and the bottom->top path costs of the CTA's
+// columns stay in shared memory (bt_smem) when H*C*D fits, so the top->bottom pass reads them
+// without a global round trip. One warp per column, C = blockDim.y columns per CTA.
+// Same results as k_vpaths_wta_plain (reference kernels listed there).
+// ---------------------------------------------------------------------------------------------
+template <int K, int PF>
+__global__ void __launch_bounds__(256) k_vpaths_wta_plain2(const uint8_t* __restrict__ cost,
+                                                           const uint8_t* __restrict__ lr,
+                                                           const uint8_t* __restrict__ rl, uint8_t* __restrict__ bt,
+                                                           float* __restrict__ disp, PlainParams P, WtaParams Q,
+                                                           int bt_smem) {
+  using Pk = typename PackOf<K>::T;
+  constexpr int D = 32 * K;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int view = blockIdx.y;
+  const int lane = threadIdx.x;
+  const int x = blockIdx.x * blockDim.y + threadIdx.y;
+  const int W = P.W, H = P.H;
+  if (x >= W) return;
+  float* dout = disp + (size_t)view * Q.dstride;
+  if (x < P.x0) {
+    for (int y = lane; y < H; y += 32) dout[(size_t)y * W + x] = kInvalidFloat;
+    return;
+  }
+  const size_t vo = (size_t)view * P.vstride;
+  const uint8_t* cv = cost + vo + (size_t)x * D + lane * K;
+  const uint8_t* lrv = lr + vo + (size_t)x * D + lane * K;
+  const uint8_t* rlv = rl + vo + (size_t)x * D + lane * K;
+  const size_t rs = (size_t)W * D;  // row stride of a volume
+  uint8_t* btp;
+  size_t bts;
+  if (bt_smem) {
+    btp = smem_raw + (size_t)threadIdx.y * H * D + lane * K;
+    bts = D;
+  } else {
+    btp = bt + vo + (size_t)x * D + lane * K;
+    bts = rs;
+  }
+  uint32_t L[K], c[K];
+  uint32_t m = 0;
+  // bottom -> top
+  Pk ring[PF];
+#pragma unroll
+  for (int i = 0; i < PF; ++i) {
+    const int y = H - 1 - i;
+    if (y >= 0) ring[i] = ld_pack<K>(cv + (size_t)y * rs);
+  }
+  for (int s0 = 0; s0 < H; s0 += PF) {
+#pragma unroll
+    for (int i = 0; i < PF; ++i) {
+      const int s = s0 + i;
+      if (s < H) {
+        const int y = H - 1 - s;
+        unpack<K>(ring[i], c);
+        if (s + PF < H) ring[i] = ld_pack<K>(cv + (size_t)(y - PF) * rs);
+        if (s == 0) {
+          uint32_t mn = 0xFFFFFFFFu;
+#pragma unroll
+          for (int j = 0; j < K; ++j) { L[j] = c[j]; mn = min(mn, c[j]); }
+          m = __reduce_min_sync(kFull, mn);
+        } else {
+          m = plain_step<K>(L, c, m, P.p1, P.p2, lane);
+        }
+        store_u8<K>(btp + (size_t)y * bts, L);
+      }
+    }
+  }
+  __syncwarp();
+  // top -> bottom + sum + WTA (the bottom->top costs join the ring when they live in global memory)
+  Pk rc[PF], ra[PF], rb[PF], re[PF];
+#pragma unroll
+  for (int i = 0; i < PF; ++i) {
+    if (i < H) {
+      rc[i] = ld_pack<K>(cv + (size_t)i * rs);
+      ra[i] = ld_pack<K>(lrv + (size_t)i * rs);
+      rb[i] = ld_pack<K>(rlv + (size_t)i * rs);
+      if (!bt_smem) re[i] = ld_pack_cg<K>(btp + (size_t)i * bts);
+    }
+  }
+  const bool col_ok = x >= 5 && x <= W - 5;
+  for (int y0 = 0; y0 < H; y0 += PF) {
+#pragma unroll
+    for (int i = 0; i < PF; ++i) {
+      const int y = y0 + i;
+      if (y < H) {
+        uint32_t a[K], b[K], e[K];
+        unpack<K>(rc[i], c);
+        unpack<K>(ra[i], a);
+        unpack<K>(rb[i], b);
+        if (!bt_smem) unpack<K>(re[i], e);
+        if (y + PF < H) {
+          rc[i] = ld_pack<K>(cv + (size_t)(y + PF) * rs);
+          ra[i] = ld_pack<K>(lrv + (size_t)(y + PF) * rs);
+          rb[i] = ld_pack<K>(rlv + (size_t)(y + PF) * rs);
+          if (!bt_smem) re[i] = ld_pack_cg<K>(btp + (size_t)(y + PF) * bts);
+        }
+        if (y == 0) {
+          uint32_t mn = 0xFFFFFFFFu;
+#pragma unroll
+          for (int j = 0; j < K; ++j) { L[j] = c[j]; mn = min(mn, c[j]); }
+          m = __reduce_min_sync(kFull, mn);
+        } else {
+          m = plain_step<K>(L, c, m, P.p1, P.p2, lane);
+        }
+        float dv = kInvalidFloat;
+        if (col_ok && y >= 5 && y <= H - 5 && y < Q.rows) {
+          uint32_t S[K];
+          if (bt_smem) unpack<K>(ld_pack_shared<K>(btp + (size_t)y * bts), e);
+#pragma unroll
+          for (int j = 0; j < K; ++j) S[j] = (L[j] & 0xFFu) + e[j] + a[j] + b[j];
+          dv = wta_pixel<K>(S, lane, P.min_d, Q, 0, y);
+        }
+        if (lane == 0) dout[(size_t)y * W + x] = dv;
+      }
+    }
   }
 }
 
@@ -351,18 +671,30 @@ struct InitParams {
   size_t vstride;
 };
 
+// max(P1, P2 / k) for k = |last_base - base + 1|; k < kP2Tab from a shared-memory table.
+constexpr int kP2Tab = 64;
+__device__ __forceinline__ void fill_p2_table(uint32_t* tab, const InitParams& P, int tid, int nthreads) {
+  for (int k = tid; k < kP2Tab; k += nthreads) {
+    const int32_t q = k ? P.p2s / k : P.p2_div0;
+    tab[k] = (uint32_t)(P.p1s > q ? P.p1s : q);
+  }
+}
+__device__ __forceinline__ uint32_t p2_term(const uint32_t* tab, int k, const InitParams& P) {
+  if (k < kP2Tab) return tab[k];
+  const int32_t q = P.p2s / k;
+  return (uint32_t)(P.p1s > q ? P.p1s : q);
+}
+
 // One realigned step. Returns the new minimum; L is replaced.
 __device__ __forceinline__ uint32_t init_step(uint32_t& L, uint32_t c, uint32_t m, int base, int last_base, int lane,
-                                              const InitParams& P) {
+                                              const InitParams& P, const uint32_t* p2tab) {
   const int i1 = lane + base - 1 - last_base;
   const int i2 = lane + base + 1 - last_base;
   const uint32_t v1 = __shfl_sync(kFull, L, i1 & 31);
   const uint32_t v2 = __shfl_sync(kFull, L, i2 & 31);
   const uint32_t a = (i1 >= 0 && i1 < kLevelRange) ? v1 + P.p1 : kInvalidCost;
   const uint32_t b = (i2 >= 0 && i2 < kLevelRange) ? v2 + P.p1 : kInvalidCost;
-  const int div = abs(last_base - base + 1);
-  const int32_t q = div != 0 ? P.p2s / div : P.p2_div0;
-  const uint32_t l4 = m + (uint32_t)(P.p1s > q ? P.p1s : q);
+  const uint32_t l4 = m + p2_term(p2tab, abs(last_base - base + 1), P);
   const uint32_t t = min(min(min(L, a), b), l4);
   L = c + (t - m);
   return __reduce_min_sync(kFull, L);
@@ -370,13 +702,13 @@ __device__ __forceinline__ uint32_t init_step(uint32_t& L, uint32_t c, uint32_t 
 
 template <typename Word>
 __device__ __forceinline__ uint32_t init_cost(const Word* own, const Word* oth, int x, int d, int base, int W,
-                                              int view, uint32_t invalid_cost) {
+                                              int view, uint32_t invalid_cost, uint32_t adj) {
   if (view == 0) {
     const int pos = x - d - base;
-    return (pos > 0 && pos < W) ? ((popc_word((Word)(own[x] ^ oth[pos])) + cost_adjust(d)) & 0xFFu) : invalid_cost;
+    return (pos > 0 && pos < W) ? ((popc_word((Word)(own[x] ^ oth[pos])) + adj) & 0xFFu) : invalid_cost;
   }
   const int pos = x + d + base;
-  return (popc_word((Word)(own[x] ^ ((pos > 0 && pos < W) ? oth[pos] : oth[0]))) + cost_adjust(d)) & 0xFFu;
+  return (popc_word((Word)(own[x] ^ ((pos > 0 && pos < W) ? oth[pos] : oth[0]))) + adj) & 0xFFu;
 }
 
 template <typename Word>
@@ -397,6 +729,8 @@ __global__ void __launch_bounds__(256) k_hpaths_init(const Word* __restrict__ cs
   Word* own = reinterpret_cast<Word*>(smem_raw) + (size_t)row * 2 * W;
   Word* oth = own + W;
   int16_t* ibase = reinterpret_cast<int16_t*>(reinterpret_cast<Word*>(smem_raw) + (size_t)R * 2 * W) + (size_t)row * W;
+  __shared__ uint32_t p2tab[kP2Tab];
+  fill_p2_table(p2tab, P, threadIdx.y * 32 + lane, blockDim.x * blockDim.y);
   if (y < P.H) {
     const Word* g_own = (view == 0 ? cs_l : cs_r) + (size_t)y * W;
     const Word* g_oth = (view == 0 ? cs_r : cs_l) + (size_t)y * W;
@@ -416,10 +750,11 @@ __global__ void __launch_bounds__(256) k_hpaths_init(const Word* __restrict__ cs
   uint8_t* cvol = cost + vo;
   uint32_t L = 0, m = 0;
   int last_base = 0;
+  const uint32_t adj = cost_adjust(lane);
   for (int s = 0; s < len; ++s) {
     const int x = dir == 0 ? P.x0 + s : W - 1 - s;
     const int base = ibase[x];
-    const uint32_t c = init_cost<Word>(own, oth, x, lane, base, W, view, P.invalid_cost);
+    const uint32_t c = init_cost<Word>(own, oth, x, lane, base, W, view, P.invalid_cost, adj);
     const size_t off = ((size_t)y * W + x) * D + lane;
     if (dir == 0) cvol[off] = (uint8_t)c;
     if (s == 0) {
@@ -433,16 +768,124 @@ __global__ void __launch_bounds__(256) k_hpaths_init(const Word* __restrict__ cs
       m = kInvalidCost;
       continue;
     }
-    m = init_step(L, c, m, base, last_base, lane, P);
+    m = init_step(L, c, m, base, last_base, lane, P, p2tab);
     last_base = base;
     out[off] = (uint8_t)L;
+  }
+}
+
+// Horizontal scans at initial-disparity levels, second form: as k_hpaths_init, with the costs of
+// 32 pixels computed per chunk by a prologue (lane = pixel) and the chunk's path costs and costs
+// written with coalesced stores. Census rows and bases of the CTA's rows are staged whole (each
+// pixel's partner window depends on its own base). Pixels skipped for an INVALID base leave
+// unspecified bytes in the path volumes; nothing reads them (the WTA rejects those pixels first).
+constexpr int kInitCst = kLevelRange + 4;  // padded cost-chunk row stride
+__host__ __device__ constexpr size_t hinit2_warp_smem() { return 32 * kInitCst + 32 * kLevelRange; }
+
+template <typename Word>
+__global__ void __launch_bounds__(256) k_hpaths_init2(const Word* __restrict__ cs_l, const Word* __restrict__ cs_r,
+                                                      const int16_t* __restrict__ init_l,
+                                                      const int16_t* __restrict__ init_r, uint8_t* __restrict__ cost,
+                                                      uint8_t* __restrict__ lr, uint8_t* __restrict__ rl,
+                                                      InitParams P) {
+  constexpr int D = kLevelRange;
+  const int view = blockIdx.y;
+  const int lane = threadIdx.x;
+  const int wid = threadIdx.y;
+  const int R = blockDim.y >> 1;
+  const int row = wid >> 1;
+  const int dir = wid & 1;
+  const int y = blockIdx.x * R + row;
+  const int W = P.W;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ uint32_t p2tab[kP2Tab];
+  fill_p2_table(p2tab, P, wid * 32 + lane, blockDim.x * blockDim.y);
+  // each staged row (own words, partner words, bases) starts on a 16-byte boundary
+  const size_t row_bytes = ((size_t)W * (2 * sizeof(Word) + 2) + 15) & ~size_t(15);
+  const size_t rows_bytes = (size_t)R * row_bytes;
+  Word* own = reinterpret_cast<Word*>(smem_raw + (size_t)row * row_bytes);
+  Word* oth = own + W;
+  int16_t* ibase = reinterpret_cast<int16_t*>(oth + W);
+  uint8_t* cbuf = smem_raw + rows_bytes + (size_t)wid * hinit2_warp_smem();
+  uint8_t* pbuf = cbuf + 32 * kInitCst;
+  if (y < P.H) {
+    const Word* g_own = (view == 0 ? cs_l : cs_r) + (size_t)y * W;
+    const Word* g_oth = (view == 0 ? cs_r : cs_l) + (size_t)y * W;
+    const int16_t* g_init = (view == 0 ? init_l : init_r) + (size_t)y * W;
+    for (int i = dir * 32 + lane; i < W; i += 64) {
+      own[i] = g_own[i];
+      oth[i] = g_oth[i];
+      ibase[i] = g_init[i];
+    }
+  }
+  __syncthreads();
+  if (y >= P.H) return;
+  const int len = W - P.x0;
+  if (len <= 0) return;
+  const size_t vo = (size_t)view * P.vstride;
+  uint8_t* out = (dir == 0 ? lr : rl) + vo + (size_t)y * W * D;
+  uint8_t* cout = cost + vo + (size_t)y * W * D;
+  uint32_t L = 0, m = 0;
+  int last_base = 0;
+  const int nchunks = (len + 31) >> 5;
+  for (int c = 0; c < nchunks; ++c) {
+    const int s0 = c << 5;
+    const int n = min(32, len - s0);
+    const int xa = dir == 0 ? P.x0 + s0 : W - (s0 + n);
+    __syncwarp();
+    if (lane < n) {  // costs of pixel xa + lane
+      const int x = xa + lane;
+      const int bx = ibase[x];
+      uint32_t* crow = reinterpret_cast<uint32_t*>(cbuf + lane * kInitCst);
+#pragma unroll
+      for (int d4 = 0; d4 < D; d4 += 4) {
+        uint32_t packed = 0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          packed |= init_cost<Word>(own, oth, x, d4 + q, bx, W, view, P.invalid_cost, cost_adjust(d4 + q)) << (8 * q);
+        crow[d4 >> 2] = packed;
+      }
+    }
+    __syncwarp();
+    for (int i = 0; i < n; ++i) {
+      const int s = s0 + i;
+      const int px = dir == 0 ? i : n - 1 - i;
+      const int x = xa + px;
+      const int base = ibase[x];
+      const uint32_t cv = cbuf[px * kInitCst + lane];
+      if (s == 0) {
+        L = cv;
+        m = __reduce_min_sync(kFull, cv);
+        last_base = base;
+      } else if (base == kInvalidShort) {
+        m = kInvalidCost;
+        continue;
+      } else {
+        m = init_step(L, cv, m, base, last_base, lane, P, p2tab);
+        last_base = base;
+      }
+      pbuf[px * D + lane] = (uint8_t)L;
+    }
+    __syncwarp();
+    const int bytes = n * D;
+    uint8_t* og = out + (size_t)xa * D;
+    for (int b = lane * 16; b < bytes; b += 32 * 16)
+      *reinterpret_cast<uint4*>(og + b) = *reinterpret_cast<const uint4*>(pbuf + b);
+    if (dir == 0) {
+      uint32_t* cg = reinterpret_cast<uint32_t*>(cout + (size_t)xa * D);
+      const uint32_t* cb = reinterpret_cast<const uint32_t*>(cbuf);
+      for (int w = lane; w < bytes / 4; w += 32) {
+        const int r2 = w / (D / 4), col = w - r2 * (D / 4);
+        cg[w] = cb[r2 * (kInitCst / 4) + col];
+      }
+    }
   }
 }
 
 // Vertical scans + WTA at initial-disparity levels (reference cusgm_ca.cu:1263-1338 and
 // Kernel_ComputeDisparityByWTA_Warpfor32 with init, :3425-3512). Both vertical scans start
 // last_base from row 0 (:1291). disp = d* + base + bias; d* <= 1 or d* >= 31 -> INVALID.
-__global__ void __launch_bounds__(256) k_vpaths_wta_init(const uint8_t* __restrict__ cost,
+static __global__ void __launch_bounds__(256) k_vpaths_wta_init(const uint8_t* __restrict__ cost,
                                                          const uint8_t* __restrict__ lr,
                                                          const uint8_t* __restrict__ rl,
                                                          const int16_t* __restrict__ init_l,
@@ -459,6 +902,12 @@ __global__ void __launch_bounds__(256) k_vpaths_wta_init(const uint8_t* __restri
     for (int y = lane; y < H; y += 32) dout[(size_t)y * W + x] = kInvalidFloat;
     return;
   }
+  __shared__ uint32_t p2tab[kP2Tab];
+  for (int k = lane; k < kP2Tab; k += 32) {
+    const int32_t q = k ? P.p2s / k : P.p2_div0;
+    p2tab[k] = (uint32_t)(P.p1s > q ? P.p1s : q);
+  }
+  __syncwarp();
   const int16_t* ib = view == 0 ? init_l : init_r;
   const size_t vo = (size_t)view * P.vstride;
   const uint8_t* cv = cost + vo;
@@ -477,7 +926,7 @@ __global__ void __launch_bounds__(256) k_vpaths_wta_init(const uint8_t* __restri
     }
     const int base = ib[(size_t)y * W + x];
     if (base == kInvalidShort) { m = kInvalidCost; continue; }
-    m = init_step(L, c, m, base, last_base, lane, P);
+    m = init_step(L, c, m, base, last_base, lane, P, p2tab);
     last_base = base;
     btv[off] = (uint8_t)L;
   }
@@ -498,16 +947,147 @@ __global__ void __launch_bounds__(256) k_vpaths_wta_init(const uint8_t* __restri
       m = kInvalidCost;
       skipped = true;
     } else {
-      m = init_step(L, c, m, base, last_base, lane, P);
+      m = init_step(L, c, m, base, last_base, lane, P, p2tab);
       last_base = base;
     }
     float dv = kInvalidFloat;
     if (col_ok && y >= 5 && y <= H - 5 && y < Q.rows && base != kInvalidShort && !skipped) {
       uint32_t S[1];
-      S[0] = (L & 0xFFu) + btv[off] + lrv[off] + rlv[off];
+      S[0] = (L & 0xFFu) + __ldcg(btv + off) + lrv[off] + rlv[off];
       dv = Q.tie_rule == kTieRefB200 ? wta_pixel_init_ref(S[0], lane, base, Q) : wta_pixel<1>(S, lane, base, Q, 1, y);
     }
     if (lane == 0) dout[(size_t)y * W + x] = dv;
+  }
+}
+
+// Vertical scans + WTA at initial-disparity levels, second form (prefetch ring, bottom->top
+// path costs in shared memory); same results as k_vpaths_wta_init.
+template <int PF>
+__global__ void __launch_bounds__(256) k_vpaths_wta_init2(const uint8_t* __restrict__ cost,
+                                                          const uint8_t* __restrict__ lr,
+                                                          const uint8_t* __restrict__ rl,
+                                                          const int16_t* __restrict__ init_l,
+                                                          const int16_t* __restrict__ init_r,
+                                                          uint8_t* __restrict__ bt, float* __restrict__ disp,
+                                                          InitParams P, WtaParams Q, int bt_smem) {
+  constexpr int D = kLevelRange;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ uint32_t p2tab[kP2Tab];
+  fill_p2_table(p2tab, P, threadIdx.y * 32 + threadIdx.x, blockDim.x * blockDim.y);
+  __syncthreads();
+  const int view = blockIdx.y;
+  const int lane = threadIdx.x;
+  const int x = blockIdx.x * blockDim.y + threadIdx.y;
+  const int W = P.W, H = P.H;
+  if (x >= W) return;
+  float* dout = disp + (size_t)view * Q.dstride;
+  if (x < P.x0) {
+    for (int y = lane; y < H; y += 32) dout[(size_t)y * W + x] = kInvalidFloat;
+    return;
+  }
+  const int16_t* ib = (view == 0 ? init_l : init_r) + x;
+  const size_t vo = (size_t)view * P.vstride;
+  const size_t rs = (size_t)W * D;
+  const uint8_t* cv = cost + vo + (size_t)x * D + lane;
+  const uint8_t* lrv = lr + vo + (size_t)x * D + lane;
+  const uint8_t* rlv = rl + vo + (size_t)x * D + lane;
+  uint8_t* btp;
+  size_t bts;
+  if (bt_smem) {
+    btp = smem_raw + (size_t)threadIdx.y * H * D + lane;
+    bts = D;
+  } else {
+    btp = bt + vo + (size_t)x * D + lane;
+    bts = rs;
+  }
+  uint32_t L = 0, m = 0;
+  int last_base = ib[0];  // row 0 for both directions
+  uint32_t rc[PF];
+  int rbase[PF];
+#pragma unroll
+  for (int i = 0; i < PF; ++i) {
+    const int y = H - 1 - i;
+    if (y >= 0) {
+      rc[i] = __ldg(cv + (size_t)y * rs);
+      rbase[i] = ib[(size_t)y * W];
+    }
+  }
+  for (int s0 = 0; s0 < H; s0 += PF) {
+#pragma unroll
+    for (int i = 0; i < PF; ++i) {
+      const int s = s0 + i;
+      if (s < H) {
+        const int y = H - 1 - s;
+        const uint32_t c = rc[i];
+        const int base = rbase[i];
+        if (s + PF < H) {
+          rc[i] = __ldg(cv + (size_t)(y - PF) * rs);
+          rbase[i] = ib[(size_t)(y - PF) * W];
+        }
+        if (s == 0) {
+          L = c;
+          m = __reduce_min_sync(kFull, c);
+          btp[(size_t)y * bts] = (uint8_t)L;
+        } else if (base == kInvalidShort) {
+          m = kInvalidCost;
+        } else {
+          m = init_step(L, c, m, base, last_base, lane, P, p2tab);
+          last_base = base;
+          btp[(size_t)y * bts] = (uint8_t)L;
+        }
+      }
+    }
+  }
+  __syncwarp();
+  const bool col_ok = x >= 5 && x <= W - 5;
+  last_base = ib[0];
+  uint32_t ra[PF], rb[PF], re[PF];
+#pragma unroll
+  for (int i = 0; i < PF; ++i) {
+    if (i < H) {
+      rc[i] = __ldg(cv + (size_t)i * rs);
+      ra[i] = __ldg(lrv + (size_t)i * rs);
+      rb[i] = __ldg(rlv + (size_t)i * rs);
+      re[i] = bt_smem ? 0u : (uint32_t)__ldcg(btp + (size_t)i * bts);
+      rbase[i] = ib[(size_t)i * W];
+    }
+  }
+  for (int y0 = 0; y0 < H; y0 += PF) {
+#pragma unroll
+    for (int i = 0; i < PF; ++i) {
+      const int y = y0 + i;
+      if (y < H) {
+        const uint32_t c = rc[i], a = ra[i], b = rb[i];
+        const uint32_t e = bt_smem ? (uint32_t)btp[(size_t)y * bts] : re[i];
+        const int base = rbase[i];
+        if (y + PF < H) {
+          rc[i] = __ldg(cv + (size_t)(y + PF) * rs);
+          ra[i] = __ldg(lrv + (size_t)(y + PF) * rs);
+          rb[i] = __ldg(rlv + (size_t)(y + PF) * rs);
+          if (!bt_smem) re[i] = __ldcg(btp + (size_t)(y + PF) * bts);
+          rbase[i] = ib[(size_t)(y + PF) * W];
+        }
+        bool skipped = false;
+        if (y == 0) {
+          L = c;
+          m = __reduce_min_sync(kFull, c);
+        } else if (base == kInvalidShort) {
+          m = kInvalidCost;
+          skipped = true;
+        } else {
+          m = init_step(L, c, m, base, last_base, lane, P, p2tab);
+          last_base = base;
+        }
+        float dv = kInvalidFloat;
+        if (col_ok && y >= 5 && y <= H - 5 && y < Q.rows && base != kInvalidShort && !skipped) {
+          uint32_t S[1];
+          S[0] = (L & 0xFFu) + e + a + b;
+          dv = Q.tie_rule == kTieRefB200 ? wta_pixel_init_ref(S[0], lane, base, Q)
+                                         : wta_pixel<1>(S, lane, base, Q, 1, y);
+        }
+        if (lane == 0) dout[(size_t)y * W + x] = dv;
+      }
+    }
   }
 }
 
@@ -628,7 +1208,7 @@ __device__ __forceinline__ int cc_find(const int* label, int p) {
   return p;
 }
 
-__global__ void k_cc_init(const float* __restrict__ disp, int* __restrict__ label, int* __restrict__ count, int W,
+static __global__ void k_cc_init(const float* __restrict__ disp, int* __restrict__ label, int* __restrict__ count, int W,
                           int H, int rows) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= W * H) return;
@@ -637,7 +1217,7 @@ __global__ void k_cc_init(const float* __restrict__ disp, int* __restrict__ labe
   count[i] = 0;
 }
 
-__global__ void k_cc_union(const float* __restrict__ disp, int* label, int W, int H, int tiles,
+static __global__ void k_cc_union(const float* __restrict__ disp, int* label, int W, int H, int tiles,
                            int rows, int abs_mode) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= W * H) return;
@@ -668,7 +1248,7 @@ __global__ void k_cc_union(const float* __restrict__ disp, int* label, int W, in
   }
 }
 
-__global__ void k_cc_count(int* label, int* __restrict__ count, int n) {
+static __global__ void k_cc_count(int* label, int* __restrict__ count, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || label[i] < 0) return;
   const int r = cc_find(label, i);
@@ -676,7 +1256,7 @@ __global__ void k_cc_count(int* label, int* __restrict__ count, int n) {
   atomicAdd(&count[r], 1);
 }
 
-__global__ void k_cc_filter(float* __restrict__ disp, const int* __restrict__ label, const int* __restrict__ count,
+static __global__ void k_cc_filter(float* __restrict__ disp, const int* __restrict__ label, const int* __restrict__ count,
                             int W, int H, int tiles, float ratio) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= W * H || label[i] < 0) return;
@@ -689,7 +1269,7 @@ __global__ void k_cc_filter(float* __restrict__ disp, const int* __restrict__ la
 // Pyramid helpers (reference FasterStereoCuda.cpp:114-166, cusgm_util.cu:47-59).
 // ---------------------------------------------------------------------------------------------
 // Level image = full-resolution image sampled at (x << shift, y << shift); both views.
-__global__ void k_decimate(const uint8_t* __restrict__ full_l, const uint8_t* __restrict__ full_r,
+static __global__ void k_decimate(const uint8_t* __restrict__ full_l, const uint8_t* __restrict__ full_r,
                            uint8_t* __restrict__ lvl_l, uint8_t* __restrict__ lvl_r, int W0, int w, int h,
                            int shift) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -703,7 +1283,7 @@ __global__ void k_decimate(const uint8_t* __restrict__ full_l, const uint8_t* __
 // Initial disparity of the next finer level: even rows (except the last) from cur at the flat
 // index (y/2)*(width/2) + x/2 (INVALID past the end of cur); odd rows and the last row copy the
 // row above.
-__global__ void k_init_next_level(const float* __restrict__ cur, long ncur, int16_t* __restrict__ next, int width,
+static __global__ void k_init_next_level(const float* __restrict__ cur, long ncur, int16_t* __restrict__ next, int width,
                                   int height) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y;
@@ -723,7 +1303,7 @@ __global__ void k_init_next_level(const float* __restrict__ cur, long ncur, int1
 
 // Right-view initial disparities: cleared to INVALID, then a scatter in which the largest
 // source x wins for every target (the reference's concurrent scatter made deterministic).
-__global__ void k_right_init_scatter(const int16_t* __restrict__ init_l, unsigned* __restrict__ key, int W, int H) {
+static __global__ void k_right_init_scatter(const int16_t* __restrict__ init_l, unsigned* __restrict__ key, int W, int H) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y;
   if (x >= W) return;
@@ -736,7 +1316,7 @@ __global__ void k_right_init_scatter(const int16_t* __restrict__ init_l, unsigne
   }
 }
 
-__global__ void k_right_init_decode(const unsigned* __restrict__ key, int16_t* __restrict__ out, int n) {
+static __global__ void k_right_init_decode(const unsigned* __restrict__ key, int16_t* __restrict__ out, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const unsigned k = key[i];
@@ -745,7 +1325,7 @@ __global__ void k_right_init_decode(const unsigned* __restrict__ key, int16_t* _
 
 // Disparity -> depth (reference Kernel_ComputeDepth, cusgm_util.cu:7-34):
 // depth = baseline*focus / (d + x0_right - x0_left) in double, INVALID kept.
-__global__ void k_depth(const float* __restrict__ disp, float* __restrict__ depth, int n, double f1, double f2) {
+static __global__ void k_depth(const float* __restrict__ disp, float* __restrict__ depth, int n, double f1, double f2) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float d = disp[i];

@@ -26,7 +26,9 @@
 #include "cusgm_df.h"
 #include "FasterStereoCuda.h"
 
-// Reference host functions (StereoCudaImpl.cpp:32, FasterStereoCuda.cpp:114 and :138).
+// Reference host functions (StereoCudaImpl.cpp:32, FasterStereoCuda.cpp:114, :138 and :169).
+void SetSgmParameters(const bool& do_lr_check, const bool& do_rm_peaks, const bool& do_smooth, CuSGMOption& sgm_param,
+                      int layer_id, int num_layers);
 sint32 RemovePeaks(float32* disp_map, sint32* segid, sint32 w, sint32 h, sint32 threshold);
 void Zoom(const unsigned char* src, unsigned char* dst, int w_src, int h_src, int scale_x, int scale_y);
 int ComputeInitDispInNextLevel(float* cur, short* next, int width, int height);
@@ -232,6 +234,73 @@ double ref_time_match(const ref_case_t* c, const uint8_t* left, const uint8_t* r
   const auto t1 = std::chrono::steady_clock::now();
   impl.Release();
   return std::chrono::duration<double, std::milli>(t1 - t0).count() / n;
+}
+
+// The pyramid of FasterStereoCuda::Match (HierSgmCudaImpl::Init :201-295 and Match :408-529)
+// driven level by level with the reference's own pieces -- SetSgmParameters, StereoCudaImpl,
+// Zoom, ComputeInitDispInNextLevel -- so that every level's output can be dumped.
+// disp_levels receives the levels' disparity maps concatenated (coarsest first), init_levels the
+// initial disparities handed to the finer levels (next-coarsest first).
+int ref_pyr_levels(int width, int height, int min_disp, int max_disp, int layers, int lr, int peaks,
+                   const uint8_t* left, const uint8_t* right, float* disp_levels, int16_t* init_levels) {
+  const int L = layers < 1 ? 1 : layers;
+  std::vector<int> w(L), h(L);
+  std::vector<std::vector<uint8_t>> bl(L), br(L);
+  std::vector<std::vector<float>> disp(L);
+  std::vector<std::vector<int16_t>> init(L);
+  std::vector<StereoCudaImpl*> st(L, nullptr);
+  for (int i = 0; i < L; ++i) {
+    const int scale = 1 << i;
+    w[i] = width / scale;
+    h[i] = height / scale;
+    bl[i].resize((size_t)w[i] * h[i]);
+    br[i].resize((size_t)w[i] * h[i]);
+    disp[i].resize((size_t)w[i] * h[i]);
+    init[i].resize((size_t)w[i] * h[i]);
+    CuSGMOption param;
+    SetSgmParameters(lr != 0, peaks != 0, false, param, i, L);
+    if (!param.using_constant_p2) { param.p1 = 10; param.p2_init = 150; }
+    int dmin = min_disp / scale, dmax = max_disp / scale, range = 32;
+    if (i == L - 1) {
+      range = dmax - dmin;
+      int k = 6;
+      while ((1 << k) < range) k++;
+      range = 1 << k;
+      if (range > 2 * width) range /= 2;
+      if (dmin >= width) { dmin = width - range; if (dmin < -width) dmin = -width; }
+    } else {
+      dmin = 0;
+    }
+    st[i] = new StereoCudaImpl;  // released below only after its output buffer is copied
+    if (!st[i]->Init(w[i], h[i], dmin, range, param, false)) { g_msg = "level Init failed"; return -2; }
+  }
+  memcpy(bl[0].data(), left, (size_t)w[0] * h[0]);
+  memcpy(br[0].data(), right, (size_t)w[0] * h[0]);
+  for (int i = 1; i < L; ++i) {
+    Zoom(bl[i - 1].data(), bl[i].data(), w[i - 1], h[i - 1], 2, 2);
+    Zoom(br[i - 1].data(), br[i].data(), w[i - 1], h[i - 1], 2, 2);
+  }
+  size_t doff = 0, ioff = 0;
+  for (int n = L - 1; n >= 0; --n) {
+    if (!st[n]->Match(bl[n].data(), br[n].data(), disp[n].data(), nullptr, n < L - 1 ? init[n].data() : nullptr)) {
+      g_msg = "level Match failed";
+      return -4;
+    }
+    memcpy(disp_levels + doff, disp[n].data(), sizeof(float) * w[n] * h[n]);
+    doff += (size_t)w[n] * h[n];
+    if (n > 0) {
+      // one spare INVALID after the coarse map for the reference's read past its end (odd widths)
+      std::vector<float> cur(disp[n]);
+      cur.push_back(INVALID_VALUE);
+      ComputeInitDispInNextLevel(cur.data(), init[n - 1].data(), w[n - 1], h[n - 1]);
+      memcpy(init_levels + ioff, init[n - 1].data(), sizeof(int16_t) * w[n - 1] * h[n - 1]);
+      ioff += (size_t)w[n - 1] * h[n - 1];
+    }
+  }
+  cudaDeviceSynchronize();
+  // the levels' small-region workers still point at disp[]: release them while it is alive
+  for (int i = 0; i < L; ++i) { st[i]->Release(); delete st[i]; }
+  return 0;
 }
 
 // Wall time of n FasterStereoCuda::Match calls (host buffers in and out), ms per call.

@@ -61,6 +61,8 @@ def ref_lib():
     lib.ref_last_message.restype = C.c_char_p
     lib.ref_time_match.argtypes = [C.POINTER(RefCase), vp, vp, C.c_int, C.c_int]
     lib.ref_time_match.restype = C.c_double
+    lib.ref_pyr_levels.argtypes = [C.c_int] * 7 + [vp, vp, vp, vp]
+    lib.ref_pyr_levels.restype = C.c_int
     return lib
 
 
@@ -106,10 +108,16 @@ def cases():
     L, R, _ = scenes.kitti_like(17, 621, 187)
     out["kitti_half"] = (dict(base, width=621, height=187, morphology=2, do_remove_peaks=1, peaks_ratio=0.005), L, R,
                          None, False)
+    # deterministic filter stages: no LR check, no median (their races stay out)
+    out["dil_only"] = (dict(base, width=621, height=187, do_lr_check=0, do_median=0, morphology=2), L, R, None, False)
+    out["peaks_only"] = (dict(base, width=621, height=187, do_lr_check=0, do_median=0, do_remove_peaks=1,
+                              peaks_ratio=0.005), L, R, None, False)
     return out
 
 
-PYR_CASES = {"pyr_kitti": (17, 1242, 375, 0, 64, 3), "pyr_cone": (16, 450, 375, 0, 64, 2)}
+# name: (seed, width, height, min_disp, max_disp, layers, lr check, small-region removal)
+PYR_CASES = {"pyr_kitti": (17, 1242, 375, 0, 64, 3, 1, 1), "pyr_cone": (16, 450, 375, 0, 64, 2, 1, 1),
+             "pyr_kitti_nolr": (18, 1242, 375, 0, 64, 3, 0, 1)}
 
 
 # ----------------------------------------------------------------------------- host ops
@@ -177,20 +185,31 @@ def refdump(out_dir: Path, only=None):
             continue
         extra = {} if init is None else {"init": init}
         np.savez_compressed(out_dir / f"{name}.npz", left=L, right=R, case=np.array(json.dumps(f)), **extra, **arr)
-    for name, (seed, w, h, dmin, dmax, layers) in PYR_CASES.items():
+    for name, (seed, w, h, dmin, dmax, layers, lr, pk) in PYR_CASES.items():
         if only and name not in only:
             continue
-        if name == "pyr_kitti":
+        if name.startswith("pyr_kitti"):
             L, R, _ = scenes.kitti_like(seed, w, h)
         else:
             L, R, _ = scenes.cone_like(seed)
+        assert L.shape == (h, w) and R.shape == (h, w), (name, L.shape)
         disp = np.zeros((h, w), np.float32)
-        rc = lib.ref_pyr_match(w, h, dmin, dmax, layers, 1, 1, _p(L), _p(R), _p(disp))
+        rc = lib.ref_pyr_match(w, h, dmin, dmax, layers, lr, pk, _p(L), _p(R), _p(disp))
         print(name, "rc", rc, lib.ref_last_message().decode(), flush=True)
         if rc == 0:
             np.savez_compressed(out_dir / f"{name}.npz", left=L, right=R, disp=disp,
                                 case=np.array(json.dumps(dict(width=w, height=h, min_disp=dmin, max_disp=dmax,
-                                                              num_layers=layers))))
+                                                              num_layers=layers, lr=lr, peaks=pk))))
+        n_d = sum((w >> i) * (h >> i) for i in range(layers))
+        n_i = sum((w >> i) * (h >> i) for i in range(layers - 1))
+        dl = np.zeros(n_d, np.float32)
+        il = np.zeros(max(n_i, 1), np.int16)
+        rc = lib.ref_pyr_levels(w, h, dmin, dmax, layers, lr, pk, _p(L), _p(R), _p(dl), _p(il))
+        print(name, "levels rc", rc, lib.ref_last_message().decode(), flush=True)
+        if rc == 0:
+            np.savez_compressed(out_dir / f"levels_{name}.npz", left=L, right=R, disp_levels=dl, init_levels=il,
+                                case=np.array(json.dumps(dict(width=w, height=h, min_disp=dmin, max_disp=dmax,
+                                                              num_layers=layers, lr=lr, peaks=pk))))
     (out_dir / "meta.json").write_text(json.dumps(meta))
     print("meta", meta)
 
@@ -238,6 +257,36 @@ def _race_free_median(O, inp):
     return snap.view(np.uint32) == alt.view(np.uint32), snap
 
 
+def _levels_report(z, case, meta):
+    """Per level: the oracle's level output given the reference's own input to that level (the
+    previous level's initial disparity computed by the reference), so races do not cascade."""
+    W, H, layers = case["width"], case["height"], case["num_layers"]
+    pc = O.PyrConfig(width=W, height=H, min_disp=case["min_disp"], max_disp=case["max_disp"], num_layers=layers,
+                     override_enable=0, peaks_strips=meta["peaks_strips"], do_lr_check=case.get("lr", 1),
+                     do_rm_peaks=case.get("peaks", 1))
+    imgs = [(z["left"], z["right"])]
+    for i in range(1, layers):
+        imgs.append((O.zoom_half(imgs[-1][0]), O.zoom_half(imgs[-1][1])))
+    out, doff, ioff = {}, 0, 0
+    init = None
+    for n in range(layers - 1, -1, -1):
+        c = O.pyr_level_config(pc, n)
+        w, h = c.width, c.height
+        ref_d = z["disp_levels"][doff:doff + w * h].reshape(h, w)
+        doff += w * h
+        ours = O.match(c, imgs[n][0], imgs[n][1], init)["disp"]
+        rows = slice(0, h - 1) if h % 2 else slice(0, h)
+        out[f"level{n}"] = float((ours[rows].view(np.uint32) == ref_d[rows].view(np.uint32)).mean())
+        if n > 0:
+            wn, hn = W >> (n - 1), H >> (n - 1)
+            ref_init = z["init_levels"][ioff:ioff + wn * hn].reshape(hn, wn)
+            ioff += wn * hn
+            mine = O.init_next_level(ref_d, wn, hn)
+            out[f"init{n - 1}"] = float((mine == ref_init).mean())
+            init = ref_init
+    return out
+
+
 def finalize(dump_dir: Path, write: bool = True):
     meta = json.loads((dump_dir / "meta.json").read_text())
     report = {}
@@ -245,10 +294,16 @@ def finalize(dump_dir: Path, write: bool = True):
         z = dict(np.load(f))
         name = f.stem
         case = json.loads(str(z["case"]))
+        if name.startswith("levels_"):
+            report[name] = _levels_report(z, case, meta)
+            if write:
+                np.savez_compressed(GOLDEN / f"ref_{name}.npz", **z, peaks_strips=np.int32(meta["peaks_strips"]))
+            continue
         if name.startswith("pyr_"):
             pc = O.PyrConfig(width=case["width"], height=case["height"], min_disp=case["min_disp"],
                              max_disp=case["max_disp"], num_layers=case["num_layers"], override_enable=0,
-                             peaks_strips=meta["peaks_strips"])
+                             peaks_strips=meta["peaks_strips"], do_lr_check=case.get("lr", 1),
+                             do_rm_peaks=case.get("peaks", 1))
             d = O.pyr_match(pc, z["left"], z["right"])
             same = (d.view(np.uint32) == z["disp"].view(np.uint32))
             report[name] = {"disp_equal": float(same[:case["height"] - 1].mean())}
