@@ -24,7 +24,7 @@ ORACLE_DIR = ROOT / "oracle"
 ORACLE_LIB = ORACLE_DIR / "_build" / "liborc.so"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-ENGINE_SOURCES = ["sgm_engine.cu", "stereo_cuda.cpp", "float_sgm.cu", "sgm_batch.cu"]
+ENGINE_SOURCES = ["sgm_engine.cu", "stereo_cuda.cpp", "sgm_noalloc.cu", "float_sgm.cu", "sgm_batch.cu"]
 
 
 def _nvcc() -> str:
