@@ -48,6 +48,9 @@ def parse():
     ap.add_argument("--pool", type=int, default=160, help="distinct input pairs resident in HBM")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="budget of the CPU baseline sample")
     ap.add_argument("--no-extras", action="store_true", help="skip the CPU baseline and extra workloads")
+    ap.add_argument("--tuning", default="", help="kernel variants row_kernel,rows_per_cta,col_kernel,cols_per_cta,"
+                                                 "bt_smem (default: the engine's)")
+    ap.add_argument("--profile-pairs", type=int, default=16, help="pairs of the serialised per-kernel timing pass")
     return ap.parse_args()
 
 
@@ -132,6 +135,8 @@ def alg_bytes(kernel, W, H, D, nviews, census_bytes):
         return nviews * (2 * V + 4 * n)
     if kernel == "census":
         return 2 * n + 2 * census_bytes * n
+    if kernel == "cost":
+        return nviews * (V + 2 * census_bytes * n)
     if kernel == "lr_median":
         return 12 * n
     return 0
@@ -214,6 +219,8 @@ def run_ours(a, rank, world, local_rank):
                                                           unique_threshold=0.95, using_constant_p2=True))
         if not ok:
             raise RuntimeError(f"matcher init failed: {m.last_error()}")
+        if a.tuning and not m.set_tuning(fsc.Tuning(*[int(v) for v in a.tuning.split(",")])):
+            raise RuntimeError(f"tuning rejected: {m.last_error()}")
         return m
 
     def run_one(m, L, R, out, stream):
@@ -295,54 +302,57 @@ def run_ours(a, rank, world, local_rank):
     ms = max_over_ranks(t0.elapsed_time(t1))
     value = a.steps * a.batch * world / (ms / 1e3)
 
-    # second pass of the same steps with per-kernel CUDA events (roofline of the dominant kernel)
+    # per-kernel CUDA events over a serialised pass (one matcher, one stream, one pair at a time),
+    # so each launch's duration is its own: the roofline of the dominant kernel comes from here
     fsc.profile_enable(True)
-    for _ in range(a.steps):
-        step()
+    for j in range(a.profile_pairs):
+        i = j % len(dL)
+        run_one(matchers[0], dL[i], dR[i], outs[0], main.cuda_stream)
     torch.cuda.synchronize()
     prof = fsc.profile_read()
     fsc.profile_enable(False)
 
-    # e2e: the host-buffer API (synchronous, like the reference's Match), pinned host memory
+    # e2e: the host-buffer API (synchronous Match, like the reference's), pinned host memory, one
+    # host thread per matcher (the reference API is per object; ctypes releases the GIL)
+    from concurrent.futures import ThreadPoolExecutor
     e2e_steps = max(1, min(a.steps, 5))
     hostL = [torch.from_numpy(L).pin_memory().numpy() for L, _ in pool[:a.batch]]
     hostR = [torch.from_numpy(R).pin_memory().numpy() for _, R in pool[:a.batch]]
     hostO = [torch.empty((H_, W_), dtype=torch.float32).pin_memory().numpy() for _ in range(a.batch)]
-    m0 = matchers[0]
 
-    def host_call(i):
-        if a.workload == "pyramid":
-            ok = m0.Match(hostL[i], hostR[i], hostO[i])
-        else:
-            ok = m0.Match(hostL[i], hostR[i], hostO[i])
-        if not ok:
-            raise RuntimeError(m0.last_error())
+    def host_worker(k):
+        m = matchers[k]
+        for b in range(k, a.batch, S):
+            if not m.Match(hostL[b], hostR[b], hostO[b]):
+                raise RuntimeError(m.last_error())
 
-    host_call(0)
-    barrier()
-    te = time.perf_counter()
-    for _ in range(e2e_steps):
-        for b in range(a.batch):
-            host_call(b)
-    te = max_over_ranks(time.perf_counter() - te)
+    with ThreadPoolExecutor(max_workers=S) as ex:
+        list(ex.map(host_worker, range(S)))  # warm-up
+        barrier()
+        te = time.perf_counter()
+        for _ in range(e2e_steps):
+            list(ex.map(host_worker, range(S)))
+        te = max_over_ranks(time.perf_counter() - te)
     e2e_value = e2e_steps * a.batch * world / te
 
     if rank != 0:
         return 0
     hbm_peak, peak_kind = peaks()
     # per-kernel algorithmic bytes over the profiled pass
+    # (kind, w, h, D, views) of each level a pair goes through
     levels = []
     if a.workload == "pyramid":
         for lv in range(LAYERS):
             w, h, mn, d = matchers[0].level_info(lv)
-            levels.append((w, h, d, 2 if lv == LAYERS - 1 else 1))
+            levels.append(("plain", w, h, d, 2) if lv == LAYERS - 1 else ("init", w, h, d, 1))
     else:
-        levels.append((W_, H_, DMAX, 2))
+        levels.append(("plain", W_, H_, DMAX, 2))
     per_call_bytes = {}
     for k in prof:
-        per_call_bytes[k] = sum(alg_bytes(k, w, h, d, nv, 8) for (w, h, d, nv) in levels)
+        per_call_bytes[k] = sum(alg_bytes(k, w, h, d, nv, 8) for (kind, w, h, d, nv) in levels
+                                if not k.startswith(("hpaths", "vpaths")) or k.endswith(kind))
     dom = max(prof, key=lambda k: prof[k]["ms"]) if prof else None
-    calls = a.steps * a.batch
+    calls = a.profile_pairs
     roofline = None
     if dom:
         total_ms = prof[dom]["ms"]
@@ -351,29 +361,204 @@ def run_ours(a, rank, world, local_rank):
         roofline = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
                     "frac": ach / hbm_peak, "traffic": None, "peak_kind": peak_kind,
                     "avg_launch_us": total_ms / prof[dom]["launches"] * 1e3,
-                    "alg_bytes_per_launch": per_call_bytes.get(dom, 0) / max(1, prof[dom]["launches"] // calls)}
-    kernels = {k: {"launches": v["launches"], "ms": round(v["ms"], 4),
-                   "share": round(v["ms"] / sum(x["ms"] for x in prof.values()), 4)} for k, v in prof.items()}
+                    "alg_bytes_per_launch": per_call_bytes.get(dom, 0) / max(1, prof[dom]["launches"] // calls),
+                    "timing": f"CUDA events around each launch, serialised pass of {calls} pairs on one stream"}
+    tot_ms = sum(x["ms"] for x in prof.values()) or 1.0
+    kernels = {k: {"launches": v["launches"], "avg_us": round(v["ms"] / max(1, v["launches"]) * 1e3, 2),
+                   "share": round(v["ms"] / tot_ms, 4)} for k, v in prof.items()}
 
     cpu = None
+    extras = None
     if not a.no_extras:
         cpu = cpu_baseline(a, pool)
+        extras = extra_batches(pool)
+        extras["float_sgm"] = extra_float_sgm()
+        extras["large_pyramid"] = extra_large_pyramid()
     clocks = clk.summary()
     line = {"metric": metric_name(a.workload), "value": value, "unit": "pairs/s", "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u8/u32 (f32 subpixel)",
             "data": "synthetic seeded KITTI-like pairs",
-            "config": dict(workload_config(a, a.batch), streams=S,
+            "config": dict(workload_config(a, a.batch), streams=S, tuning=a.tuning or "default",
                            l2=f"inputs larger than L2: rotating pool of {len(dL)} distinct pairs "
                               f"({pool_bytes / 2**20:.0f} MiB) per GPU"),
             "e2e": {"value": e2e_value, "unit": "pairs/s",
                     "h2d_bytes_per_step": a.batch * 2 * W_ * H_, "d2h_bytes_per_step": a.batch * 4 * W_ * H_,
-                    "api": "FasterStereoCuda.Match (host buffers, synchronous)" if a.workload == "pyramid"
-                    else "StereoCuda.Match (host buffers, synchronous)"},
+                    "api": ("FasterStereoCuda.Match" if a.workload == "pyramid" else "StereoCuda.Match")
+                    + f" (host buffers, synchronous), {S} host threads with one matcher each"},
             "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
-            "bit_exact_vs_oracle": bit_exact, "kernels": kernels}
+            "bit_exact_vs_oracle": bit_exact, "kernels": kernels, "extras": extras}
     print(json.dumps(line), flush=True)
     return 0
+
+
+# ------------------------------------------------------------------------------------ extras
+def _dev_copy(dst_addr, src_tensor):
+    from cuda.bindings import runtime as rt
+    (err,) = rt.cudaMemcpy(dst_addr, src_tensor.data_ptr(), src_tensor.numel() * src_tensor.element_size(),
+                           rt.cudaMemcpyKind.cudaMemcpyDeviceToDevice)
+    if err != rt.cudaError_t.cudaSuccess:
+        raise RuntimeError(f"cudaMemcpy failed: {err}")
+
+
+def _read_dev(addr, h, w):
+    import torch
+    from cuda.bindings import runtime as rt
+    out = torch.empty((h, w), dtype=torch.float32, device="cuda")
+    (err,) = rt.cudaMemcpy(out.data_ptr(), addr, h * w * 4, rt.cudaMemcpyKind.cudaMemcpyDeviceToDevice)
+    if err != rt.cudaError_t.cudaSuccess:
+        raise RuntimeError(f"cudaMemcpy failed: {err}")
+    return out
+
+
+def batch_vs_loop(pairs, images, runs, warmup):
+    """One batch graph over `pairs` vs a loop of per-pair StereoCuda.match_device calls on one
+    stream (the plain path), same inputs resident in HBM, device-timed; outputs compared bit for bit."""
+    import torch
+    import fasterstereocuda_b200 as fsc
+    opt = fsc.CuSGMOption(p1=10, p2_init=150, cs_type=1, num_paths=4, do_median_filter=True, do_lr_check=True,
+                          lr_threshold=1.0, unique_threshold=0.95, using_constant_p2=True)
+    b = fsc.StereoBatch()
+    t = time.perf_counter()
+    if not b.Init(pairs, opt):
+        raise RuntimeError(b.last_error())
+    init_s = time.perf_counter() - t
+    dev = [(torch.from_numpy(L).cuda(), torch.from_numpy(R).cuda()) for L, R in images]
+    for i, (dl, dr) in enumerate(dev):
+        al, ar, _ = b.buffers(i)
+        _dev_copy(al, dl)
+        _dev_copy(ar, dr)
+    torch.cuda.synchronize()
+    main = torch.cuda.Stream()  # a real stream handle: NULL would mean the batch's own stream
+    for _ in range(warmup):
+        b.run(main.cuda_stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(main)
+    for _ in range(runs):
+        b.run(main.cuda_stream)
+    e1.record(main)
+    torch.cuda.synchronize()
+    batch_ms = e0.elapsed_time(e1) / runs
+    # plain per-pair loop: one matcher per distinct shape, pairs matched one after another
+    engines, outs = {}, []
+    for (w, h, m, d) in pairs:
+        if (w, h, m, d) not in engines:
+            s = fsc.StereoCuda()
+            if not s.Init(w, h, m, d, opt):
+                raise RuntimeError(s.last_error())
+            engines[(w, h, m, d)] = s
+        outs.append(torch.empty((h, w), dtype=torch.float32, device="cuda"))
+
+    def loop():
+        for i, p in enumerate(pairs):
+            if not engines[p].match_device(dev[i][0], dev[i][1], outs[i], None, None, main.cuda_stream):
+                raise RuntimeError(engines[p].last_error())
+    for _ in range(warmup):
+        loop()
+    torch.cuda.synchronize()
+    e0.record(main)
+    for _ in range(runs):
+        loop()
+    e1.record(main)
+    torch.cuda.synchronize()
+    loop_ms = e0.elapsed_time(e1) / runs
+    same = all(torch.equal(_read_dev(b.buffers(i)[2], p[1], p[0]).view(torch.int32), outs[i].view(torch.int32))
+               for i, p in enumerate(pairs))
+    info = b.info()
+    return {"pairs": len(pairs), "batch_pairs_per_s": len(pairs) / (batch_ms / 1e3),
+            "loop_pairs_per_s": len(pairs) / (loop_ms / 1e3), "speedup": loop_ms / batch_ms,
+            "batch_ms": batch_ms, "loop_ms": loop_ms, "bit_exact_vs_per_pair": bool(same),
+            "kernels_per_graph": info["kernels_per_run"], "arena_gib": info["arena_bytes"] / 2**30,
+            "init_s": init_s, "buckets": b.buckets()}
+
+
+def extra_batches(pool):
+    from fasterstereocuda_b200 import scenes
+    out = {}
+    n = 32
+    out["batch_1242x375x64"] = batch_vs_loop([(W_, H_, 0, DMAX)] * n, [pool[i % len(pool)] for i in range(n)],
+                                             runs=5, warmup=2)
+    specs = scenes.batch_specs()
+    imgs = [scenes.planar_pair(seed, w, h, dmin=2.0, dmax=60.0)[:2] for (w, h, d, seed) in specs]
+    out["batch64_uneven"] = batch_vs_loop([(w, h, 0, d) for (w, h, d, _) in specs], imgs, runs=3, warmup=1)
+    out["batch64_uneven"]["workload"] = ("64 pairs, widths 320..1920, heights 240..1080 (multiples of 32), "
+                                         "D in {64,128}, seeded planar scenes, census 9x7, LR + median")
+    return out
+
+
+def extra_float_sgm():
+    """Differentiable float32 SGM: forward + backward of 4 x 1242x375 x 64 (device-timed)."""
+    import torch
+    from fasterstereocuda_b200.float_sgm import float_sgm
+    B, H, W, D = 4, H_, W_, DMAX
+    g = torch.Generator(device="cuda").manual_seed(0)
+    cost = (torch.randint(0, 64, (B, H, W, D), generator=g, device="cuda").float()
+            + torch.rand((B, H, W, D), generator=g, device="cuda") * 0.5).requires_grad_()
+    p1 = torch.full((B, H, W), 10.0, device="cuda", requires_grad=True)
+    p2 = torch.full((B, H, W), 150.0, device="cuda", requires_grad=True)
+    w = torch.randn((B, H, W), generator=g, device="cuda")
+
+    def step():
+        cost.grad = p1.grad = p2.grad = None
+        (float_sgm(cost, p1, p2) * w).sum().backward()
+    for _ in range(3):
+        step()
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    torch.cuda.synchronize()
+    n = 5
+    e0.record()
+    for _ in range(n):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    fwd = []
+    with torch.no_grad():
+        for _ in range(n):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            float_sgm(cost, p1, p2)
+            b.record()
+            torch.cuda.synchronize()
+            fwd.append(a.elapsed_time(b))
+    return {"workload": "float32 SGM 4 x 1242x375, D=64, 4 paths + soft-argmin", "fwd_bwd_ms": e0.elapsed_time(e1) / n,
+            "fwd_ms": statistics.median(fwd)}
+
+
+def extra_large_pyramid():
+    """4800x3409, disparities 0..256, 4-level pyramid, census 9x7, P1=10, P2=150 (fractal scene):
+    device time per pair and the matcher's device memory."""
+    import torch
+    import fasterstereocuda_b200 as fsc
+    from fasterstereocuda_b200 import scenes
+    from cuda.bindings import runtime as rt
+    W, H = 4800, 3409
+    L, R, _ = scenes.building_like(2, W, H)
+    torch.cuda.synchronize()
+    free0 = rt.cudaMemGetInfo()[1]
+    p = fsc.FasterStereoCuda()
+    if not p.Init(fsc.StereoOption1(width=W, height=H, min_disp=0, max_disp=256, num_layers=4),
+                  fsc.LevelOverride(1, 10, 150), fsc.ExtOptions()):
+        raise RuntimeError(p.last_error())
+    torch.cuda.synchronize()
+    used = free0 - rt.cudaMemGetInfo()[1]
+    dl, dr = torch.from_numpy(L).cuda(), torch.from_numpy(R).cuda()
+    out = torch.empty((H, W), dtype=torch.float32, device="cuda")
+    s = torch.cuda.Stream()
+    for _ in range(2):
+        p.match_device(dl, dr, out, s.cuda_stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n = 5
+    e0.record(s)
+    for _ in range(n):
+        if not p.match_device(dl, dr, out, s.cuda_stream):
+            raise RuntimeError(p.last_error())
+    e1.record(s)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / n
+    return {"workload": "4800x3409, D=256, 4-level pyramid, census 9x7, P1=10 P2=150, fractal scene",
+            "ms_per_pair": ms, "pairs_per_s": 1e3 / ms, "matcher_device_gib": used / 2**30,
+            "levels": [p.level_info(i) for i in range(4)]}
 
 
 def cpu_baseline(a, pool):

@@ -97,6 +97,30 @@ class LevelOverride(C.Structure):
     _fields_ = [("cs_type", C.c_int32), ("p1", C.c_int32), ("p2", C.c_int32)]
 
 
+class Tuning(C.Structure):
+    """Kernel variants and launch shapes (sgm_tuning_t); every setting gives the same result."""
+    _fields_ = [("row_kernel", C.c_int32), ("rows_per_cta", C.c_int32), ("col_kernel", C.c_int32),
+                ("cols_per_cta", C.c_int32), ("bt_smem", C.c_int32), ("row_lanes", C.c_int32),
+                ("col_lanes", C.c_int32)]
+
+
+class BatchPair(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("min_disparity", C.c_int32),
+                ("disp_range", C.c_int32)]
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [("pairs", C.c_int32), ("buckets", C.c_int32), ("arena_bytes", C.c_uint64),
+                ("kernels_per_run", C.c_int64)]
+
+
+class BatchBucket(C.Structure):
+    _fields_ = [("disp_range", C.c_int32), ("width_class", C.c_int32), ("pairs", C.c_int32),
+                ("rows_lanes", C.c_int32), ("rows_warps_per_cta", C.c_int32), ("rows_ctas", C.c_int32),
+                ("cols_lanes", C.c_int32), ("cols_warps_per_cta", C.c_int32), ("cols_prefetch", C.c_int32),
+                ("cols_ctas", C.c_int32)]
+
+
 def load_library(path: Optional[os.PathLike] = None):
     """Loads the engine library (raises if it is missing: there is no fallback)."""
     global _lib
@@ -112,6 +136,8 @@ def load_library(path: Optional[os.PathLike] = None):
         "sgm_init": (i32, [vp, i32, i32, i32, i32, C.POINTER(CuSGMOption), i32]),
         "sgm_set_ext_options": (i32, [vp, C.POINTER(ExtOptions)]),
         "sgm_get_ext_options": (i32, [vp, C.POINTER(ExtOptions)]),
+        "sgm_set_tuning": (i32, [vp, C.POINTER(Tuning)]), "sgm_get_tuning": (i32, [vp, C.POINTER(Tuning)]),
+        "sgm_pyr_set_tuning": (i32, [vp, i32, C.POINTER(Tuning)]),
         "sgm_match": (i32, [vp, vp, vp, vp, vp, vp, C.POINTER(StereoROI), C.POINTER(StereoROI)]),
         "sgm_match_device": (i32, [vp, vp, vp, vp, vp, vp, vp]),
         "sgm_release": (i32, [vp]), "sgm_set_min_disparity": (i32, [vp, i32]),
@@ -128,6 +154,15 @@ def load_library(path: Optional[os.PathLike] = None):
         "sgm_pyr_kernel_launches": (i64, [vp]),
         "sgm_debug_read": (i32, [vp, i32, i32, vp, C.c_size_t]),
         "sgm_profile_enable": (i32, [i32]), "sgm_profile_read": (i32, [C.c_char_p, C.c_size_t]),
+        "sgm_batch_create": (i32, [C.POINTER(vp)]), "sgm_batch_destroy": (i32, [vp]),
+        "sgm_batch_last_error": (C.c_char_p, [vp]),
+        "sgm_batch_init": (i32, [vp, C.POINTER(BatchPair), i32, C.POINTER(CuSGMOption), C.POINTER(ExtOptions)]),
+        "sgm_batch_autotune": (i32, [vp]),
+        "sgm_batch_pair_buffers": (i32, [vp, i32, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]),
+        "sgm_batch_run": (i32, [vp, vp]),
+        "sgm_batch_match": (i32, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]),
+        "sgm_batch_info": (i32, [vp, C.POINTER(BatchInfo)]),
+        "sgm_batch_bucket": (i32, [vp, i32, C.POINTER(BatchBucket)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -190,6 +225,10 @@ class StereoCuda:
 
     def set_ext_options(self, ext: ExtOptions) -> bool:
         self.status = self._lib.sgm_set_ext_options(self._h, C.byref(ext))
+        return self.status == 0
+
+    def set_tuning(self, tuning: Tuning) -> bool:
+        self.status = self._lib.sgm_set_tuning(self._h, C.byref(tuning))
         return self.status == 0
 
     def Init(self, width: int, height: int, min_disparity: int, disp_range: int, sgm_option: CuSGMOption,
@@ -298,6 +337,11 @@ class FasterStereoCuda:
             self.width, self.height = option.width, option.height
         return self.status == 0
 
+    def set_tuning(self, tuning: Tuning, level: int = -1) -> bool:
+        """After Init: tuning of one level, or of every level (-1)."""
+        self.status = self._lib.sgm_pyr_set_tuning(self._h, level, C.byref(tuning))
+        return self.status == 0
+
     def Match(self, bytes_left, bytes_right, disparity_data) -> bool:
         n = self.width * self.height
         for a, t in ((bytes_left, np.uint8), (bytes_right, np.uint8), (disparity_data, np.float32)):
@@ -333,3 +377,79 @@ class FasterStereoCuda:
     @staticmethod
     def FreePageLockedPtr(ptr: int) -> bool:
         return load_library().sgm_free_page_locked(C.c_void_p(ptr)) == 0
+
+
+class StereoBatch:
+    """Many pairs of different sizes / disparity ranges matched by one CUDA graph launch
+    (sgm_batch_*). Each pair's disparity equals StereoCuda's for the same pair and options."""
+
+    def __init__(self):
+        self._lib = load_library()
+        h = C.c_void_p()
+        st = self._lib.sgm_batch_create(C.byref(h))
+        if st != 0:
+            raise RuntimeError(f"sgm_batch_create failed ({st})")
+        self._h = h
+        self.status = 0
+        self.shapes = []
+
+    def __del__(self):
+        h, self._h = getattr(self, "_h", None), None
+        if h:
+            self._lib.sgm_batch_destroy(h)
+
+    def last_error(self) -> str:
+        return (self._lib.sgm_batch_last_error(self._h) or b"").decode()
+
+    def Init(self, pairs, sgm_option: CuSGMOption, ext: Optional[ExtOptions] = None) -> bool:
+        """pairs: sequence of (width, height, min_disparity, disp_range)."""
+        arr = (BatchPair * len(pairs))(*[BatchPair(*p) for p in pairs])
+        self.status = self._lib.sgm_batch_init(self._h, arr, len(pairs), C.byref(sgm_option),
+                                               C.byref(ext) if ext is not None else None)
+        if self.status == 0:
+            self.shapes = [(p[1], p[0]) for p in pairs]
+        return self.status == 0
+
+    def autotune(self) -> bool:
+        self.status = self._lib.sgm_batch_autotune(self._h)
+        return self.status == 0
+
+    def buffers(self, i: int):
+        """(d_left, d_right, d_disp) device addresses of pair i inside the batch arena."""
+        a, b, c = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        self.status = self._lib.sgm_batch_pair_buffers(self._h, i, C.byref(a), C.byref(b), C.byref(c))
+        if self.status != 0:
+            raise RuntimeError(self.last_error())
+        return a.value, b.value, c.value
+
+    def run(self, stream: int = 0) -> bool:
+        self.status = self._lib.sgm_batch_run(self._h, C.c_void_p(stream) if stream else None)
+        return self.status == 0
+
+    def Match(self, lefts, rights, disps) -> bool:
+        n = len(self.shapes)
+        for i, (L, R, O) in enumerate(zip(lefts, rights, disps)):
+            h, w = self.shapes[i]
+            for a, dt in ((L, np.uint8), (R, np.uint8), (O, np.float32)):
+                if a.dtype != dt or a.shape != (h, w) or not a.flags["C_CONTIGUOUS"]:
+                    raise ValueError(f"pair {i}: expected C-contiguous {dt.__name__} array of shape {(h, w)}")
+        pl = (C.c_void_p * n)(*[L.ctypes.data for L in lefts])
+        pr = (C.c_void_p * n)(*[R.ctypes.data for R in rights])
+        po = (C.c_void_p * n)(*[O.ctypes.data for O in disps])
+        self.status = self._lib.sgm_batch_match(self._h, pl, pr, po)
+        return self.status == 0
+
+    def info(self) -> dict:
+        i = BatchInfo()
+        if self._lib.sgm_batch_info(self._h, C.byref(i)) != 0:
+            raise RuntimeError(self.last_error())
+        return {f: getattr(i, f) for f, _ in BatchInfo._fields_}
+
+    def buckets(self) -> list:
+        out = []
+        for k in range(self.info()["buckets"]):
+            b = BatchBucket()
+            if self._lib.sgm_batch_bucket(self._h, k, C.byref(b)) != 0:
+                raise RuntimeError(self.last_error())
+            out.append({f: getattr(b, f) for f, _ in BatchBucket._fields_})
+        return out

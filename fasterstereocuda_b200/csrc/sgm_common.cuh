@@ -3,6 +3,10 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <mutex>
+#include <set>
+#include <utility>
+
 namespace sgm {
 
 constexpr float kInvalidFloat = -999999.0f;    // output invalid value (StereoCuda::get_invad_float)
@@ -112,6 +116,30 @@ __device__ __forceinline__ int pick_tie(const uint32_t (&bal)[K], int rule, int 
   for (int w = 0; w < K; ++w)
     if (best < 0 && ((word[w] >> t) & 1u)) best = w;
   return t + 32 * best;
+}
+
+// Lets kernel `fn` launch with as much dynamic shared memory as the device allows. The limit is a
+// per-function attribute shared by every launcher in the process (other matchers, other host
+// threads), so it is always raised to the device maximum instead of being set to the size of one
+// launch, which could undercut a concurrent launch that needs more.
+// Done once per (function, device); later calls are a set lookup.
+template <typename F>
+inline cudaError_t allow_max_dynamic_smem(F* fn) {
+  static std::mutex mu;
+  static std::set<std::pair<const void*, int>> done;
+  int dev = 0, optin = 0;
+  cudaError_t st = cudaGetDevice(&dev);
+  if (st != cudaSuccess) return st;
+  const void* f = reinterpret_cast<const void*>(fn);
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.count({f, dev})) return cudaSuccess;
+  st = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaFuncAttributes fa{};
+  if (st == cudaSuccess) st = cudaFuncGetAttributes(&fa, f);
+  if (st == cudaSuccess)
+    st = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+  if (st == cudaSuccess) done.insert({f, dev});
+  return st;
 }
 
 // Parabola through (d-1,c1), (d,c0), (d+1,c2); the reference's SubPixBias.

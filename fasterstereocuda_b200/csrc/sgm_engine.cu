@@ -19,7 +19,7 @@
 #include <vector>
 
 #include "../../include/sgm_b200.h"
-#include "sgm_kernels.cuh"
+#include "sgm_kernels3.cuh"
 
 namespace {
 
@@ -161,6 +161,10 @@ struct sgm_engine {
   int tune_rows = 0;        // rows per CTA of the row kernels (0: default)
   int tune_cols = 0;        // columns per CTA of the column kernels (0: default)
   int tune_bt_smem = 0;     // 1: keep bottom->top path costs in shared memory when they fit
+  int tune_row_kernel = 0;  // 0: 3 when exact else 2; 1 whole-row census, 2 chunked, 3 u16x2 per scanline
+  int tune_col_kernel = 0;  // 0: 3 when exact else 1; 1 plain loads, 2 prefetch ring, 3 u16x2 per column
+  int tune_row_lanes = 0;   // variant 3: lanes per scanline (0: default)
+  int tune_col_lanes = 0;
   bool bt_stored = true;    // the last match wrote the bottom->top volume to global memory
 
   int nviews() const { return opt.do_lr_check ? 2 : 1; }
@@ -315,6 +319,66 @@ int rows_per_cta(int W, int word_bytes, bool with_init) {
   return R;
 }
 
+// Thread-per-scanline kernels (variant 3): G lanes per scanline, prefetch depth by slice size.
+template <int K, int G>
+constexpr int pf3() {
+  return 32 * K / G >= 64 ? 2 : (32 * K / G >= 32 ? 4 : 8);
+}
+// the column kernel keeps four volumes in its prefetch ring
+template <int K, int G>
+constexpr int pf3v() {
+  return 32 * K / G >= 32 ? 1 : (32 * K / G >= 16 ? 2 : 4);
+}
+template <int K>
+constexpr bool lanes_ok(int G) {
+  return (G == 1 || G == 2 || G == 4 || G == 8) && !(K == 4 && (G == 1 || G == 8)) && K <= 4;
+}
+constexpr int kDefaultRowLanes = 8, kDefaultColLanes = 4;
+
+template <int K>
+int launch_rows3(sgm_engine* e, int G, const sgm::PlainParams& P, int nv) {
+  if (!lanes_ok<K>(G)) G = kDefaultRowLanes;
+  const long threads = (long)nv * 2 * e->H * G;
+  const int blocks = (int)((threads + 127) / 128);
+  cudaStream_t s = e->stream;
+  auto go = [&](auto kern) {
+    return SGM_LAUNCH(e, s, "hpaths_plain", kern<<<blocks, 128, 0, s>>>(e->cost, e->lr, e->rl, P, nv));
+  };
+  if constexpr (K == 4) {
+    return G == 2 ? go(sgm::k_hpaths3<K, 2, pf3<K, 2>()>) : go(sgm::k_hpaths3<K, 4, pf3<K, 4>()>);
+  } else {
+    switch (G) {
+      case 1: return go(sgm::k_hpaths3<K, 1, pf3<K, 1>()>);
+      case 4: return go(sgm::k_hpaths3<K, 4, pf3<K, 4>()>);
+      case 8: return go(sgm::k_hpaths3<K, 8, pf3<K, 8>()>);
+      default: return go(sgm::k_hpaths3<K, 2, pf3<K, 2>()>);
+    }
+  }
+}
+
+template <int K>
+int launch_cols3(sgm_engine* e, int G, const sgm::PlainParams& P, const sgm::WtaParams& Q, float* wta, int nv) {
+  if (!lanes_ok<K>(G)) G = kDefaultColLanes;
+  const long threads = (long)e->W * G;
+  dim3 grid((unsigned)((threads + 127) / 128), nv);
+  const size_t smem = (size_t)(128 / G) * sgm::vpaths3_col_smem<K>();
+  cudaStream_t s = e->stream;
+  auto go = [&](auto kern) {
+    return SGM_LAUNCH(e, s, "vpaths_wta_plain",
+                      kern<<<grid, 128, smem, s>>>(e->cost, e->lr, e->rl, e->bt, wta, P, Q));
+  };
+  if constexpr (K == 4) {
+    return G == 2 ? go(sgm::k_vpaths3<K, 2, pf3v<K, 2>()>) : go(sgm::k_vpaths3<K, 4, pf3v<K, 4>()>);
+  } else {
+    switch (G) {
+      case 1: return go(sgm::k_vpaths3<K, 1, pf3v<K, 1>()>);
+      case 2: return go(sgm::k_vpaths3<K, 2, pf3v<K, 2>()>);
+      case 8: return go(sgm::k_vpaths3<K, 8, pf3v<K, 8>()>);
+      default: return go(sgm::k_vpaths3<K, 4, pf3v<K, 4>()>);
+    }
+  }
+}
+
 template <int K, typename Word>
 int launch_plain(sgm_engine* e, const Word* csl, const Word* csr, float* wta) {
   sgm::PlainParams P;
@@ -322,12 +386,35 @@ int launch_plain(sgm_engine* e, const Word* csl, const Word* csr, float* wta) {
   P.p1 = (uint32_t)e->opt.p1; P.p2 = (uint32_t)e->opt.p2_init;
   P.vstride = e->vol();
   const int nv = e->nviews();
-  const int R = e->tune_rows > 0 ? e->tune_rows : 4;
-  const size_t smem = (size_t)2 * R * sgm::hpaths2_warp_smem<K, Word>();
-  auto hk = sgm::k_hpaths_plain2<K, Word>;
-  SGM_CUDA_TRY(e, cudaFuncSetAttribute(hk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  dim3 hg((e->H + R - 1) / R, nv), hb(32, 2 * R);
-  int st = SGM_LAUNCH(e, e->stream, "hpaths_plain", hk<<<hg, hb, smem, e->stream>>>(csl, csr, e->cost, e->lr, e->rl, P));
+  // thread-per-scanline kernels: exact for 16-bit path costs and the min(x + P1, L) form
+  const bool v3_ok = K <= 4 && e->opt.p1 <= (int)sgm::kMaxPenalty16 && e->opt.p2_init <= (int)sgm::kMaxPenalty16 &&
+                     e->opt.p2_init >= e->opt.p1 &&
+                     (e->ext.tie_rule == sgm::kTieLowest || e->ext.tie_rule == sgm::kTieRefB200);
+  int st;
+  if ((e->tune_row_kernel == 3 || e->tune_row_kernel == 0) && v3_ok) {
+    dim3 cg((e->W + 127) / 128, e->H, nv);
+    st = SGM_LAUNCH(e, e->stream, "cost", sgm::k_cost3<K, Word><<<cg, 128, 0, e->stream>>>(csl, csr, e->cost, P));
+    if (st) return st;
+    st = launch_rows3<K>(e, e->tune_row_lanes, P, nv);
+  } else if (e->tune_row_kernel == 1) {  // whole census rows of R scanlines in shared memory
+    const int R = e->tune_rows > 0 ? e->tune_rows : rows_per_cta(e->W, sizeof(Word), false);
+    const size_t smem = (size_t)R * 2 * e->W * sizeof(Word);
+    if (smem > 227 * 1024) {
+      set_error(&e->err, "image width %d too large for the whole-row kernel", e->W);
+      return SGM_ERR_UNSUPPORTED;
+    }
+    auto hk = sgm::k_hpaths_plain<K, Word>;
+    SGM_CUDA_TRY(e, sgm::allow_max_dynamic_smem(hk));
+    dim3 hg((e->H + R - 1) / R, nv), hb(32, 2 * R);
+    st = SGM_LAUNCH(e, e->stream, "hpaths_plain", hk<<<hg, hb, smem, e->stream>>>(csl, csr, e->cost, e->lr, e->rl, P));
+  } else {
+    const int R = e->tune_rows > 0 ? e->tune_rows : 4;
+    const size_t smem = (size_t)2 * R * sgm::hpaths2_warp_smem<K, Word>();
+    auto hk = sgm::k_hpaths_plain2<K, Word>;
+    SGM_CUDA_TRY(e, sgm::allow_max_dynamic_smem(hk));
+    dim3 hg((e->H + R - 1) / R, nv), hb(32, 2 * R);
+    st = SGM_LAUNCH(e, e->stream, "hpaths_plain", hk<<<hg, hb, smem, e->stream>>>(csl, csr, e->cost, e->lr, e->rl, P));
+  }
   if (st) return st;
   sgm::WtaParams Q;
   Q.uniqueness = e->opt.unique_threshold;
@@ -338,13 +425,63 @@ int launch_plain(sgm_engine* e, const Word* csl, const Word* csr, float* wta) {
   Q.dstride = e->npix();
   int C = 8, bt_smem = 0;
   size_t vsmem = 0;
+  if ((e->tune_col_kernel == 3 || e->tune_col_kernel == 0) && v3_ok) {
+    e->bt_stored = true;
+    return launch_cols3<K>(e, e->tune_col_lanes, P, Q, wta, nv);
+  }
+  if (e->tune_col_kernel != 2) {
+    C = e->tune_cols > 0 ? e->tune_cols : 8;
+    e->bt_stored = true;
+    dim3 vg((e->W + C - 1) / C, nv), vb(32, C);
+    return SGM_LAUNCH(e, e->stream, "vpaths_wta_plain",
+                      sgm::k_vpaths_wta_plain<K><<<vg, vb, 0, e->stream>>>(e->cost, e->lr, e->rl, e->bt, wta, P, Q));
+  }
   vertical_shape(e->H, 32 * K, &C, &bt_smem, &vsmem, e->tune_cols, e->tune_bt_smem);
   e->bt_stored = !bt_smem;
   auto vk = sgm::k_vpaths_wta_plain2<K, 8>;
-  if (vsmem) SGM_CUDA_TRY(e, cudaFuncSetAttribute(vk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vsmem));
+  if (vsmem) SGM_CUDA_TRY(e, sgm::allow_max_dynamic_smem(vk));
   dim3 vg((e->W + C - 1) / C, nv), vb(32, C);
   return SGM_LAUNCH(e, e->stream, "vpaths_wta_plain",
                     vk<<<vg, vb, vsmem, e->stream>>>(e->cost, e->lr, e->rl, e->bt, wta, P, Q, bt_smem));
+}
+
+// Initial-disparity levels, thread-per-scanline kernels (uint32 per disparity): G = 2, 4 or 8.
+constexpr int kDefaultInitRowLanes = 8, kDefaultInitColLanes = 8;
+
+template <typename Word>
+int launch_init3(sgm_engine* e, const Word* csl, const Word* csr, const int16_t* il, const int16_t* ir, float* wta,
+                 const sgm::InitParams& P, const sgm::WtaParams& Q, bool rows3, bool cols3) {
+  const int nv = e->nviews();
+  cudaStream_t s = e->stream;
+  int st = SGM_OK;
+  if (rows3) {
+    const size_t csmem = (size_t)e->W * sizeof(Word);
+    auto ck = sgm::k_cost3_init<Word>;
+    SGM_CUDA_TRY(e, sgm::allow_max_dynamic_smem(ck));
+    st = SGM_LAUNCH(e, s, "cost", ck<<<dim3(e->H, nv), 256, csmem, s>>>(csl, csr, il, ir, e->cost, P));
+    if (st) return st;
+    int G = e->tune_row_lanes;
+    if (G != 2 && G != 4 && G != 8) G = kDefaultInitRowLanes;
+    const long threads = (long)nv * 2 * e->H * G;
+    const int blocks = (int)((threads + 127) / 128);
+    auto go = [&](auto kern) {
+      return SGM_LAUNCH(e, s, "hpaths_init", kern<<<blocks, 128, 0, s>>>(e->cost, il, ir, e->lr, e->rl, P, nv));
+    };
+    st = G == 2 ? go(sgm::k_hpaths3_init<2, 4>) : G == 8 ? go(sgm::k_hpaths3_init<8, 8>) : go(sgm::k_hpaths3_init<4, 8>);
+    if (st) return st;
+  }
+  if (cols3) {
+    int G = e->tune_col_lanes;
+    if (G != 2 && G != 4 && G != 8) G = kDefaultInitColLanes;
+    e->bt_stored = true;
+    dim3 grid((unsigned)(((long)e->W * G + 127) / 128), nv);
+    auto go = [&](auto kern) {
+      return SGM_LAUNCH(e, s, "vpaths_wta_init",
+                        kern<<<grid, 128, 0, s>>>(e->cost, e->lr, e->rl, il, ir, e->bt, wta, P, Q));
+    };
+    st = G == 2 ? go(sgm::k_vpaths3_init<2, 2>) : G == 8 ? go(sgm::k_vpaths3_init<8, 4>) : go(sgm::k_vpaths3_init<4, 4>);
+  }
+  return st;
 }
 
 template <typename Word>
@@ -355,18 +492,46 @@ int launch_init(sgm_engine* e, const Word* csl, const Word* csr, const int16_t* 
   P.invalid_cost = e->opt.cs_type == 1 ? 0xFFu : sgm::kInvalidCost;
   P.vstride = e->vol();
   const int nv = e->nviews();
-  int R = 4;
-  const size_t row_bytes = ((size_t)e->W * (2 * sizeof(Word) + 2) + 15) & ~size_t(15);  // as in the kernel
-  while (R > 1 && R * row_bytes > 120 * 1024) R >>= 1;
-  const size_t smem = R * row_bytes + (size_t)2 * R * sgm::hinit2_warp_smem();
-  if (smem > 220 * 1024) {
-    set_error(&e->err, "image width %d too large for the row kernel", e->W);
-    return SGM_ERR_UNSUPPORTED;
+  sgm::WtaParams Q3;
+  Q3.uniqueness = e->opt.unique_threshold;
+  Q3.tie_rule = e->ext.init_tie_rule;
+  Q3.rows = (e->H / 4) * 4;
+  Q3.dmax_excl = sgm::kLevelRange - 1;
+  Q3.dstride = e->npix();
+  // thread-per-scanline kernels: uint32 arithmetic (exact for any penalties); WTA rules 0 and 4
+  const bool v3_ok = e->ext.init_tie_rule == sgm::kTieLowest || e->ext.init_tie_rule == sgm::kTieRefB200;
+  const bool rows3 = v3_ok && (e->tune_row_kernel == 0 || e->tune_row_kernel == 3);
+  const bool cols3 = v3_ok && (e->tune_col_kernel == 0 || e->tune_col_kernel == 3);
+  int st;
+  if (rows3) {
+    st = launch_init3<Word>(e, csl, csr, il, ir, wta, P, Q3, true, false);
+  } else if (e->tune_row_kernel == 1) {  // whole census rows of R scanlines in shared memory
+    const int R = e->tune_rows > 0 ? e->tune_rows : rows_per_cta(e->W, sizeof(Word), true);
+    const size_t smem = (size_t)R * e->W * (2 * sizeof(Word) + 2);
+    if (smem > 227 * 1024) {
+      set_error(&e->err, "image width %d too large for the whole-row kernel", e->W);
+      return SGM_ERR_UNSUPPORTED;
+    }
+    auto hk = sgm::k_hpaths_init<Word>;
+    SGM_CUDA_TRY(e, sgm::allow_max_dynamic_smem(hk));
+    dim3 hg((e->H + R - 1) / R, nv), hb(32, 2 * R);
+    st = SGM_LAUNCH(e, e->stream, "hpaths_init",
+                    hk<<<hg, hb, smem, e->stream>>>(csl, csr, il, ir, e->cost, e->lr, e->rl, P));
+  } else {
+    int R = e->tune_rows > 0 ? e->tune_rows : 4;
+    const size_t row_bytes = ((size_t)e->W * (2 * sizeof(Word) + 2) + 15) & ~size_t(15);  // as in the kernel
+    while (R > 1 && R * row_bytes > 120 * 1024) R >>= 1;
+    const size_t smem = R * row_bytes + (size_t)2 * R * sgm::hinit2_warp_smem();
+    if (smem > 220 * 1024) {
+      set_error(&e->err, "image width %d too large for the row kernel", e->W);
+      return SGM_ERR_UNSUPPORTED;
+    }
+    auto hk = sgm::k_hpaths_init2<Word>;
+    SGM_CUDA_TRY(e, sgm::allow_max_dynamic_smem(hk));
+    dim3 hg((e->H + R - 1) / R, nv), hb(32, 2 * R);
+    st = SGM_LAUNCH(e, e->stream, "hpaths_init",
+                    hk<<<hg, hb, smem, e->stream>>>(csl, csr, il, ir, e->cost, e->lr, e->rl, P));
   }
-  auto hk = sgm::k_hpaths_init2<Word>;
-  SGM_CUDA_TRY(e, cudaFuncSetAttribute(hk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  dim3 hg((e->H + R - 1) / R, nv), hb(32, 2 * R);
-  int st = SGM_LAUNCH(e, e->stream, "hpaths_init", hk<<<hg, hb, smem, e->stream>>>(csl, csr, il, ir, e->cost, e->lr, e->rl, P));
   if (st) return st;
   sgm::WtaParams Q;
   Q.uniqueness = e->opt.unique_threshold;
@@ -376,10 +541,18 @@ int launch_init(sgm_engine* e, const Word* csl, const Word* csr, const int16_t* 
   Q.dstride = e->npix();
   int C = 8, bt_smem = 0;
   size_t vsmem = 0;
+  if (cols3) return launch_init3<Word>(e, csl, csr, il, ir, wta, P, Q3, false, true);
+  if (e->tune_col_kernel != 2) {
+    C = e->tune_cols > 0 ? e->tune_cols : 8;
+    e->bt_stored = true;
+    dim3 vg((e->W + C - 1) / C, nv), vb(32, C);
+    return SGM_LAUNCH(e, e->stream, "vpaths_wta_init",
+                      sgm::k_vpaths_wta_init<<<vg, vb, 0, e->stream>>>(e->cost, e->lr, e->rl, il, ir, e->bt, wta, P, Q));
+  }
   vertical_shape(e->H, sgm::kLevelRange, &C, &bt_smem, &vsmem, e->tune_cols, e->tune_bt_smem);
   e->bt_stored = !bt_smem;
   auto vk = sgm::k_vpaths_wta_init2<8>;
-  if (vsmem) SGM_CUDA_TRY(e, cudaFuncSetAttribute(vk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vsmem));
+  if (vsmem) SGM_CUDA_TRY(e, sgm::allow_max_dynamic_smem(vk));
   dim3 vg((e->W + C - 1) / C, nv), vb(32, C);
   return SGM_LAUNCH(e, e->stream, "vpaths_wta_init",
                     vk<<<vg, vb, vsmem, e->stream>>>(e->cost, e->lr, e->rl, il, ir, e->bt, wta, P, Q, bt_smem));
@@ -491,10 +664,11 @@ int engine_enqueue(sgm_engine* e, const uint8_t* dl_img, const uint8_t* dr_img, 
     if (tiles > 0) {
       const int rows = strips * tiles;
       const unsigned nb = (unsigned)((N + 255) / 256);
-      st = SGM_LAUNCH(e, e->stream, "cc_init", sgm::k_cc_init<<<nb, 256, 0, e->stream>>>(dout, e->label, e->count, W, H, rows));
-      if (!st)
-        st = SGM_LAUNCH(e, e->stream, "cc_union", sgm::k_cc_union<<<nb, 256, 0, e->stream>>>(
-                                                      dout, e->label, W, H, tiles, rows, e->ext.peaks_abs_mode));
+      st = SGM_LAUNCH(e, e->stream, "cc_rows", sgm::k_cc_rows<<<(H + 7) / 8, dim3(32, 8), 0, e->stream>>>(
+                                                   dout, e->label, e->count, W, H, rows, e->ext.peaks_abs_mode));
+      if (!st && tiles > 1)
+        st = SGM_LAUNCH(e, e->stream, "cc_vert", sgm::k_cc_vert<<<nb, 256, 0, e->stream>>>(
+                                                     dout, e->label, W, H, tiles, rows, e->ext.peaks_abs_mode));
       if (!st)
         st = SGM_LAUNCH(e, e->stream, "cc_count", sgm::k_cc_count<<<nb, 256, 0, e->stream>>>(e->label, e->count, (int)N));
       if (!st)
@@ -694,6 +868,47 @@ int sgm_set_ext_options(sgm_handle_t h, const sgm_ext_options_t* ext) {
 int sgm_get_ext_options(sgm_handle_t h, sgm_ext_options_t* ext) {
   if (!h || !ext) return SGM_ERR_ARG;
   *ext = h->ext;
+  return SGM_OK;
+}
+
+namespace {
+bool tuning_ok(const sgm_tuning_t* t) {
+  const int r = t->rows_per_cta, c = t->cols_per_cta;
+  return t->row_kernel >= 0 && t->row_kernel <= 3 && t->col_kernel >= 0 && t->col_kernel <= 3 &&
+         (r == 0 || r == 1 || r == 2 || r == 4) && c >= 0 && c <= 8 && (t->bt_smem == 0 || t->bt_smem == 1) &&
+         (t->row_lanes == 0 || t->row_lanes == 1 || t->row_lanes == 2 || t->row_lanes == 4 || t->row_lanes == 8) &&
+         (t->col_lanes == 0 || t->col_lanes == 1 || t->col_lanes == 2 || t->col_lanes == 4 || t->col_lanes == 8);
+}
+void apply_tuning(sgm_engine* e, const sgm_tuning_t* t) {
+  e->tune_row_kernel = t->row_kernel;
+  e->tune_rows = t->rows_per_cta;
+  e->tune_col_kernel = t->col_kernel;
+  e->tune_cols = t->cols_per_cta;
+  e->tune_bt_smem = t->bt_smem;
+  e->tune_row_lanes = t->row_lanes;
+  e->tune_col_lanes = t->col_lanes;
+}
+}  // namespace
+
+int sgm_set_tuning(sgm_handle_t h, const sgm_tuning_t* t) {
+  if (!h || !t) return SGM_ERR_ARG;
+  if (!tuning_ok(t)) {
+    set_error(&h->err, "tuning out of range (kernels 0-3, rows per CTA 0/1/2/4, columns per CTA 0-8, bt_smem 0/1)");
+    return SGM_ERR_ARG;
+  }
+  apply_tuning(h, t);
+  return SGM_OK;
+}
+
+int sgm_get_tuning(sgm_handle_t h, sgm_tuning_t* t) {
+  if (!h || !t) return SGM_ERR_ARG;
+  t->row_kernel = h->tune_row_kernel;
+  t->rows_per_cta = h->tune_rows;
+  t->col_kernel = h->tune_col_kernel;
+  t->cols_per_cta = h->tune_cols;
+  t->bt_smem = h->tune_bt_smem;
+  t->row_lanes = h->tune_row_lanes;
+  t->col_lanes = h->tune_col_lanes;
   return SGM_OK;
 }
 
@@ -1084,5 +1299,20 @@ int sgm_pyr_level_info(sgm_pyr_handle_t h, int32_t level, int32_t* width, int32_
 }
 
 int64_t sgm_pyr_kernel_launches(sgm_pyr_handle_t h) { return h ? h->launches : 0; }
+
+int sgm_pyr_set_tuning(sgm_pyr_handle_t h, int32_t level, const sgm_tuning_t* t) {
+  if (!h || !t) return SGM_ERR_ARG;
+  if (!h->ready || level < -1 || level >= h->layers) {
+    h->err = "tuning: matcher not initialised or level out of range";
+    return SGM_ERR_ARG;
+  }
+  if (!tuning_ok(t)) {
+    h->err = "tuning out of range (kernels 0-3, rows per CTA 0/1/2/4, columns per CTA 0-8, bt_smem 0/1)";
+    return SGM_ERR_ARG;
+  }
+  for (int i = 0; i < h->layers; ++i)
+    if (level < 0 || level == i) apply_tuning(h->lv[i], t);
+  return SGM_OK;
+}
 
 }  // extern "C"

@@ -21,13 +21,7 @@ namespace sgm {
 // (blockIdx.z). Left border value 0, right border value 0xFFFFFFFF (zero-extended).
 // ---------------------------------------------------------------------------------------------
 template <typename Word, int CSW, int CSH>
-__global__ void __launch_bounds__(128) k_census(const uint8_t* __restrict__ img_l, const uint8_t* __restrict__ img_r,
-                                                Word* __restrict__ cs_l, Word* __restrict__ cs_r, int W, int H) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y;
-  const bool right = blockIdx.z == 1;
-  if (x >= W) return;
-  const uint8_t* img = right ? img_r : img_l;
+__device__ __forceinline__ Word census_value(const uint8_t* __restrict__ img, int x, int y, int W, int H, bool right) {
   Word v = 0;
   if (x < CSW || x >= W - CSW || y < CSH || y >= H - CSH) {
     v = right ? (Word)0xFFFFFFFFu : (Word)0;
@@ -40,7 +34,17 @@ __global__ void __launch_bounds__(128) k_census(const uint8_t* __restrict__ img_
       for (int dx = -CSW; dx <= CSW; ++dx) v = (Word)((v << 1) | (Word)(__ldg(row + dx) < c));
     }
   }
-  (right ? cs_r : cs_l)[(size_t)y * W + x] = v;
+  return v;
+}
+
+template <typename Word, int CSW, int CSH>
+__global__ void __launch_bounds__(128) k_census(const uint8_t* __restrict__ img_l, const uint8_t* __restrict__ img_r,
+                                                Word* __restrict__ cs_l, Word* __restrict__ cs_r, int W, int H) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  const bool right = blockIdx.z == 1;
+  if (x >= W) return;
+  (right ? cs_r : cs_l)[(size_t)y * W + x] = census_value<Word, CSW, CSH>(right ? img_r : img_l, x, y, W, H, right);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -244,22 +248,17 @@ __host__ __device__ constexpr size_t hpaths2_warp_smem() {
   return (size_t)(32 * K + 64) * sizeof(Word) + 32 * (32 * K + 4) + 32 * (32 * K);
 }
 
+// One scanline (view, y) in one direction (dir 0: left->right, 1: right->left), by one warp;
+// `base` is the warp's hpaths2_warp_smem<K, Word>() bytes of shared memory (16-byte aligned).
 template <int K, typename Word>
-__global__ void __launch_bounds__(256) k_hpaths_plain2(const Word* __restrict__ cs_l, const Word* __restrict__ cs_r,
-                                                       uint8_t* __restrict__ cost, uint8_t* __restrict__ lr,
-                                                       uint8_t* __restrict__ rl, PlainParams P) {
+__device__ __forceinline__ void hpaths2_warp(const Word* __restrict__ cs_l, const Word* __restrict__ cs_r,
+                                             uint8_t* __restrict__ cost, uint8_t* __restrict__ lr,
+                                             uint8_t* __restrict__ rl, const PlainParams& P, int view, int y, int dir,
+                                             unsigned char* base) {
   constexpr int D = 32 * K;
   constexpr int CST = D + 4;  // padded row stride of the cost chunk (bank-conflict free prologue)
-  const int view = blockIdx.y;
-  const int lane = threadIdx.x;
-  const int wid = threadIdx.y;
-  const int R = blockDim.y >> 1;
-  const int y = blockIdx.x * R + (wid >> 1);
-  const int dir = wid & 1;
+  const int lane = threadIdx.x & 31;
   const int W = P.W;
-  if (y >= P.H) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  unsigned char* base = smem_raw + (size_t)wid * hpaths2_warp_smem<K, Word>();
   Word* win = reinterpret_cast<Word*>(base);                   // [D + 64]: own[32], partner[D + 31]
   uint8_t* cbuf = base + (size_t)(D + 64) * sizeof(Word);      // [32][CST]
   uint8_t* pbuf = cbuf + 32 * CST;                             // [32][D]
@@ -358,6 +357,20 @@ __global__ void __launch_bounds__(256) k_hpaths_plain2(const Word* __restrict__ 
       }
     }
   }
+  __syncwarp();
+}
+
+template <int K, typename Word>
+__global__ void __launch_bounds__(256) k_hpaths_plain2(const Word* __restrict__ cs_l, const Word* __restrict__ cs_r,
+                                                       uint8_t* __restrict__ cost, uint8_t* __restrict__ lr,
+                                                       uint8_t* __restrict__ rl, PlainParams P) {
+  const int wid = threadIdx.y;
+  const int R = blockDim.y >> 1;
+  const int y = blockIdx.x * R + (wid >> 1);
+  if (y >= P.H) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  hpaths2_warp<K, Word>(cs_l, cs_r, cost, lr, rl, P, blockIdx.y, y, wid & 1,
+                        smem_raw + (size_t)wid * hpaths2_warp_smem<K, Word>());
 }
 
 struct WtaParams {
@@ -428,16 +441,13 @@ __device__ __forceinline__ float wta_pixel_init_ref(uint32_t S, int lane, int ba
 // kernels above. One warp per column; 8 columns per CTA. Columns left of x0 are INVALID.
 // ---------------------------------------------------------------------------------------------
 template <int K>
-__global__ void __launch_bounds__(256) k_vpaths_wta_plain(const uint8_t* __restrict__ cost,
-                                                          const uint8_t* __restrict__ lr,
-                                                          const uint8_t* __restrict__ rl, uint8_t* __restrict__ bt,
-                                                          float* __restrict__ disp, PlainParams P, WtaParams Q) {
+__device__ __forceinline__ void vpaths1_warp(const uint8_t* __restrict__ cost, const uint8_t* __restrict__ lr,
+                                             const uint8_t* __restrict__ rl, uint8_t* __restrict__ bt,
+                                             float* __restrict__ disp, const PlainParams& P, const WtaParams& Q,
+                                             int view, int x) {
   constexpr int D = 32 * K;
-  const int view = blockIdx.y;
-  const int lane = threadIdx.x;
-  const int x = blockIdx.x * blockDim.y + threadIdx.y;
+  const int lane = threadIdx.x & 31;
   const int W = P.W, H = P.H;
-  if (x >= W) return;
   float* dout = disp + (size_t)view * Q.dstride;
   if (x < P.x0) {
     for (int y = lane; y < H; y += 32) dout[(size_t)y * W + x] = kInvalidFloat;
@@ -492,6 +502,17 @@ __global__ void __launch_bounds__(256) k_vpaths_wta_plain(const uint8_t* __restr
     }
     if (lane == 0) dout[(size_t)y * W + x] = dv;
   }
+  __syncwarp();
+}
+
+template <int K>
+__global__ void __launch_bounds__(256) k_vpaths_wta_plain(const uint8_t* __restrict__ cost,
+                                                          const uint8_t* __restrict__ lr,
+                                                          const uint8_t* __restrict__ rl, uint8_t* __restrict__ bt,
+                                                          float* __restrict__ disp, PlainParams P, WtaParams Q) {
+  const int x = blockIdx.x * blockDim.y + threadIdx.y;
+  if (x >= P.W) return;
+  vpaths1_warp<K>(cost, lr, rl, bt, disp, P, Q, blockIdx.y, x);
 }
 
 // Packed K bytes of one lane (K disparities) as loaded from a [..][D] u8 volume.
@@ -545,20 +566,18 @@ __device__ __forceinline__ void unpack(const typename PackOf<K>::T& w, uint32_t 
 // without a global round trip. One warp per column, C = blockDim.y columns per CTA.
 // Same results as k_vpaths_wta_plain (reference kernels listed there).
 // ---------------------------------------------------------------------------------------------
+// One column (view, x) by one warp. bt_col: this column's H x D bytes of shared memory for the
+// bottom->top path costs, or nullptr to keep them in the global volume bt.
 template <int K, int PF>
-__global__ void __launch_bounds__(256) k_vpaths_wta_plain2(const uint8_t* __restrict__ cost,
-                                                           const uint8_t* __restrict__ lr,
-                                                           const uint8_t* __restrict__ rl, uint8_t* __restrict__ bt,
-                                                           float* __restrict__ disp, PlainParams P, WtaParams Q,
-                                                           int bt_smem) {
+__device__ __forceinline__ void vpaths2_warp(const uint8_t* __restrict__ cost, const uint8_t* __restrict__ lr,
+                                             const uint8_t* __restrict__ rl, uint8_t* __restrict__ bt,
+                                             float* __restrict__ disp, const PlainParams& P, const WtaParams& Q,
+                                             int view, int x, uint8_t* bt_col) {
   using Pk = typename PackOf<K>::T;
   constexpr int D = 32 * K;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int view = blockIdx.y;
-  const int lane = threadIdx.x;
-  const int x = blockIdx.x * blockDim.y + threadIdx.y;
+  const int lane = threadIdx.x & 31;
   const int W = P.W, H = P.H;
-  if (x >= W) return;
+  const bool bt_smem = bt_col != nullptr;
   float* dout = disp + (size_t)view * Q.dstride;
   if (x < P.x0) {
     for (int y = lane; y < H; y += 32) dout[(size_t)y * W + x] = kInvalidFloat;
@@ -572,7 +591,7 @@ __global__ void __launch_bounds__(256) k_vpaths_wta_plain2(const uint8_t* __rest
   uint8_t* btp;
   size_t bts;
   if (bt_smem) {
-    btp = smem_raw + (size_t)threadIdx.y * H * D + lane * K;
+    btp = bt_col + lane * K;
     bts = D;
   } else {
     btp = bt + vo + (size_t)x * D + lane * K;
@@ -656,6 +675,19 @@ __global__ void __launch_bounds__(256) k_vpaths_wta_plain2(const uint8_t* __rest
       }
     }
   }
+}
+
+template <int K, int PF>
+__global__ void __launch_bounds__(256) k_vpaths_wta_plain2(const uint8_t* __restrict__ cost,
+                                                           const uint8_t* __restrict__ lr,
+                                                           const uint8_t* __restrict__ rl, uint8_t* __restrict__ bt,
+                                                           float* __restrict__ disp, PlainParams P, WtaParams Q,
+                                                           int bt_smem) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int x = blockIdx.x * blockDim.y + threadIdx.y;
+  if (x >= P.W) return;
+  vpaths2_warp<K, PF>(cost, lr, rl, bt, disp, P, Q, blockIdx.y, x,
+                      bt_smem ? smem_raw + (size_t)threadIdx.y * P.H * (32 * K) : nullptr);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1132,13 +1164,12 @@ __device__ __forceinline__ float median9(float a0, float a1, float a2, float a3,
   return a4;
 }
 
+// One 32x8 output tile at (bx, by) by a 32x8 block; every thread of the block calls it.
 template <bool DoLR, bool DoMedian>
-__global__ void __launch_bounds__(256) k_lr_median(const float* __restrict__ dl, const float* __restrict__ dr,
-                                                   float* __restrict__ dr_out, float* __restrict__ out, int W, int H,
-                                                   float thr) {
-  __shared__ float tile[10][34];
+__device__ __forceinline__ void lr_median_tile(const float* __restrict__ dl, const float* __restrict__ dr,
+                                               float* __restrict__ dr_out, float* __restrict__ out, int W, int H,
+                                               float thr, int bx, int by, float (*tile)[34]) {
   const int tx = threadIdx.x, ty = threadIdx.y;
-  const int bx = blockIdx.x * 32, by = blockIdx.y * 8;
   for (int i = ty * 32 + tx; i < 10 * 34; i += 256) {
     const int ly = i / 34, lx = i - ly * 34;
     const int gx = bx + lx - 1, gy = by + ly - 1;
@@ -1165,6 +1196,14 @@ __global__ void __launch_bounds__(256) k_lr_median(const float* __restrict__ dl,
     }
   }
   out[(size_t)y * W + x] = v;
+}
+
+template <bool DoLR, bool DoMedian>
+__global__ void __launch_bounds__(256) k_lr_median(const float* __restrict__ dl, const float* __restrict__ dr,
+                                                   float* __restrict__ dr_out, float* __restrict__ out, int W, int H,
+                                                   float thr) {
+  __shared__ float tile[10][34];
+  lr_median_tile<DoLR, DoMedian>(dl, dr, dr_out, out, W, H, thr, blockIdx.x * 32, blockIdx.y * 8, tile);
 }
 
 // Dilation of INVALID pixels (reference Kernel_Dilation, cusgm_df.cu:197-222).
@@ -1208,43 +1247,65 @@ __device__ __forceinline__ int cc_find(const int* label, int p) {
   return p;
 }
 
-static __global__ void k_cc_init(const float* __restrict__ disp, int* __restrict__ label, int* __restrict__ count, int W,
-                          int H, int rows) {
+// Row pass: label[i] = first pixel of i's horizontal run of connected pixels (its provisional
+// root), -1 for INVALID pixels and rows >= `rows`; zeroes count. One warp per row, 32 pixels per
+// step: run starts by ballot, the run of the previous step carried across.
+static __global__ void k_cc_rows(const float* __restrict__ disp, int* __restrict__ label, int* __restrict__ count,
+                                 int W, int H, int rows, int abs_mode) {
+  const int y = blockIdx.x * blockDim.y + threadIdx.y;
+  if (y >= H) return;
+  const int lane = threadIdx.x;
+  const float* drow = disp + (size_t)y * W;
+  int* lrow = label + (size_t)y * W;
+  int* crow = count + (size_t)y * W;
+  int carry = -1;
+  float prev_v = kInvalidFloat;
+  bool prev_valid = false;
+  for (int x0 = 0; x0 < W; x0 += 32) {
+    const int x = x0 + lane;
+    const bool in = x < W;
+    const float v = in ? drow[x] : kInvalidFloat;
+    const bool valid = in && y < rows && v != kInvalidFloat;
+    float lv = __shfl_up_sync(kFull, v, 1);
+    bool lvalid = __shfl_up_sync(kFull, (int)valid, 1) != 0;
+    if (lane == 0) {
+      lv = prev_v;
+      lvalid = prev_valid;
+    }
+    const bool conn = valid && lvalid && peaks_adjacent(v, lv, abs_mode);
+    const unsigned brk = __ballot_sync(kFull, !conn);
+    const unsigned upto = brk & (0xFFFFFFFFu >> (31 - lane));
+    const int start = upto ? x0 + (31 - __clz(upto)) : carry;
+    if (in) {
+      lrow[x] = valid ? y * W + start : -1;
+      crow[x] = 0;
+    }
+    carry = __shfl_sync(kFull, start, 31);
+    prev_v = __shfl_sync(kFull, v, 31);
+    prev_valid = __shfl_sync(kFull, (int)valid, 31) != 0;
+  }
+}
+
+// Vertical pass: unions pixel i with the pixel below it (same strip) when both are valid and
+// adjacent; roots are the smallest pixel index (atomicMin hooks the larger root).
+static __global__ void k_cc_vert(const float* __restrict__ disp, int* label, int W, int H, int tiles, int rows,
+                                 int abs_mode) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= W * H) return;
   const int y = i / W;
-  label[i] = (y < rows && disp[i] != kInvalidFloat) ? i : -1;
-  count[i] = 0;
-}
-
-static __global__ void k_cc_union(const float* __restrict__ disp, int* label, int W, int H, int tiles,
-                           int rows, int abs_mode) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= W * H) return;
-  const int y = i / W, x = i - y * W;
-  if (y >= rows || label[i] < 0) return;
-  const float v = disp[i];
-  // right and down neighbours (the down one only inside the same strip)
-  for (int n = 0; n < 2; ++n) {
-    int q;
-    if (n == 0) {
-      if (x + 1 >= W) continue;
-      q = i + 1;
-    } else {
-      if (y + 1 >= rows || (y + 1) / tiles != y / tiles) continue;
-      q = i + W;
-    }
-    if (disp[q] == kInvalidFloat || !peaks_adjacent(disp[q], v, abs_mode)) continue;
-    int a = i, b = q;
-    while (true) {
-      a = cc_find(label, a);
-      b = cc_find(label, b);
-      if (a == b) break;
-      if (a > b) { const int t = a; a = b; b = t; }
-      const int old = atomicMin(&label[b], a);
-      if (old == b) break;
-      b = old;
-    }
+  if (y + 1 >= rows || (y + 1) / tiles != y / tiles) return;
+  const int q = i + W;
+  const float v = disp[i], w = disp[q];
+  if (v == kInvalidFloat || w == kInvalidFloat || !peaks_adjacent(w, v, abs_mode)) return;
+  int a = i, b = q;
+  while (true) {
+    a = cc_find(label, a);
+    b = cc_find(label, b);
+    if (a == b) break;
+    if (a > b) { const int t = a; a = b; b = t; }
+    const int old = atomicMin(&label[b], a);
+    if (old == b) break;
+    b = old;
   }
 }
 

@@ -1,0 +1,890 @@
+// SGM kernels with one thread per scanline (sm_100a).
+//
+// A thread owns one path (a row in one direction, or a column) and keeps all D path costs of
+// its current pixel in registers, two disparities per 32-bit word (u16x2: L(2k) in the low
+// half, L(2k+1) in the high half). One recurrence step is then, per word,
+//   x = min3(L(d-1), L(d+1), m + P2 - P1)      __vimin3_u16x2
+//   t = min(x + P1, L(d))                      __viaddmin_u16x2
+//   L'(d) = t + C(d) - m                       one 3-input add
+// with the d-1 / d+1 words formed by byte permutes inside the thread: no shuffles, no warp
+// reductions, and the minimum over d is a tree of SIMD minima. A scanline may also be split over
+// G = 2, 4 or 8 neighbouring lanes (each holding D/G disparities; two shuffles carry the
+// boundary words and a butterfly the minimum), trading instructions for parallelism. The WTA
+// runs in the scanline's threads (keys S << 6 | d, sums kept in shared memory). Neighbouring
+// scanlines sit in neighbouring lanes, so the column kernel's loads of one row are contiguous.
+//
+// Exactness: the reference's recurrence is uint32; here every value is held in 16 bits, which
+// is exact while L <= 255 + P2 and m + P2 < 65536, i.e. for P1, P2 <= 16383 (checked on the
+// host), and the min(x + P1, ...) form needs P2 >= P1 (host falls back otherwise).
+// Results equal k_hpaths_plain / k_vpaths_wta_plain (reference kernels cited there).
+#pragma once
+#include "sgm_kernels.cuh"
+
+namespace sgm {
+
+constexpr uint32_t kMaxPenalty16 = 16383;
+
+__device__ __forceinline__ uint32_t rep16(uint32_t v) { return v * 0x10001u; }
+__device__ __forceinline__ uint32_t min16x2(uint32_t a, uint32_t b) { return __vimin3_u16x2(a, b, b); }
+__device__ __forceinline__ uint32_t hmin16(uint32_t w) { return min(w & 0xFFFFu, w >> 16); }
+
+// Bytes (b0 b1 b2 b3) of v -> u16x2 words (b0, b1) and (b2, b3).
+__device__ __forceinline__ uint32_t widen_lo(uint32_t v) { return __byte_perm(v, 0u, 0x4140); }
+__device__ __forceinline__ uint32_t widen_hi(uint32_t v) { return __byte_perm(v, 0u, 0x4342); }
+// Low bytes of the four halves of (w0, w1) -> one 32-bit word of u8 path costs.
+__device__ __forceinline__ uint32_t narrow(uint32_t w0, uint32_t w1) { return __byte_perm(w0, w1, 0x6420); }
+
+// Raw per-thread slices: NR 32-bit words (4*NR bytes, 4-, 8- or 16*n-byte aligned).
+template <int NR>
+__device__ __forceinline__ void ld_slice(const uint8_t* __restrict__ p, uint32_t (&r)[NR]) {
+  if constexpr (NR == 1) {
+    r[0] = __ldcg(reinterpret_cast<const unsigned int*>(p));
+  } else if constexpr (NR == 2) {
+    const uint2 q = __ldcg(reinterpret_cast<const uint2*>(p));
+    r[0] = q.x; r[1] = q.y;
+  } else {
+#pragma unroll
+    for (int v = 0; v < NR / 4; ++v) {
+      const uint4 q = __ldcg(reinterpret_cast<const uint4*>(p) + v);
+      r[4 * v] = q.x; r[4 * v + 1] = q.y; r[4 * v + 2] = q.z; r[4 * v + 3] = q.w;
+    }
+  }
+}
+
+template <int NR>
+__device__ __forceinline__ void st_slice(uint8_t* __restrict__ p, const uint32_t (&r)[NR]) {
+  if constexpr (NR == 1) {
+    *reinterpret_cast<uint32_t*>(p) = r[0];
+  } else if constexpr (NR == 2) {
+    *reinterpret_cast<uint2*>(p) = make_uint2(r[0], r[1]);
+  } else {
+#pragma unroll
+    for (int v = 0; v < NR / 4; ++v)
+      reinterpret_cast<uint4*>(p)[v] = make_uint4(r[4 * v], r[4 * v + 1], r[4 * v + 2], r[4 * v + 3]);
+  }
+}
+
+// bytes -> u16x2 words (NT = 2*NR) and back (low bytes)
+template <int NR>
+__device__ __forceinline__ void widen_slice(const uint32_t (&r)[NR], uint32_t (&w)[2 * NR]) {
+#pragma unroll
+  for (int i = 0; i < NR; ++i) {
+    w[2 * i] = widen_lo(r[i]);
+    w[2 * i + 1] = widen_hi(r[i]);
+  }
+}
+template <int NR>
+__device__ __forceinline__ void narrow_slice(const uint32_t (&w)[2 * NR], uint32_t (&r)[NR]) {
+#pragma unroll
+  for (int i = 0; i < NR; ++i) r[i] = narrow(w[2 * i], w[2 * i + 1]);
+}
+
+// Minimum over the u16x2 words (a log-depth tree), then over the G threads of the scanline.
+template <int NT, int G>
+__device__ __forceinline__ uint32_t group_min16(const uint32_t (&v)[NT]) {
+  uint32_t t[NT];
+#pragma unroll
+  for (int k = 0; k < NT; ++k) t[k] = v[k];
+#pragma unroll
+  for (int st = 1; st < NT; st *= 2) {
+#pragma unroll
+    for (int k = 0; k + st < NT; k += 2 * st) t[k] = min16x2(t[k], t[k + st]);
+  }
+  uint32_t r = hmin16(t[0]);
+#pragma unroll
+  for (int o = 1; o < G; o *= 2) r = min(r, __shfl_xor_sync(kFull, r, o, G));
+  return r;
+}
+
+template <int G>
+__device__ __forceinline__ uint32_t group_min(uint32_t r) {
+#pragma unroll
+  for (int o = 1; o < G; o *= 2) r = min(r, __shfl_xor_sync(kFull, r, o, G));
+  return r;
+}
+
+// First pixel of a path: L = C. Returns m = min_d C(d) over the scanline's G threads.
+template <int NT, int G>
+__device__ __forceinline__ uint32_t first_g(uint32_t (&L)[NT], const uint32_t (&c)[NT]) {
+#pragma unroll
+  for (int k = 0; k < NT; ++k) L[k] = c[k];
+  return group_min16<NT, G>(c);
+}
+
+// One recurrence step of a scanline held by G threads (thread g owns words g*NT .. g*NT+NT-1);
+// returns the new minimum. p1x2 = rep16(P1), p2m1 = P2 - P1. Every lane of the warp calls it.
+template <int NT, int G>
+__device__ __forceinline__ uint32_t step_g(uint32_t (&L)[NT], const uint32_t (&c)[NT], uint32_t m, uint32_t p1x2,
+                                          uint32_t p2m1, int g) {
+  uint32_t left_nb = 0, right_nb = 0;
+  if constexpr (G > 1) {
+    left_nb = __shfl_up_sync(kFull, L[NT - 1], 1, G);
+    right_nb = __shfl_down_sync(kFull, L[0], 1, G);
+  }
+  const bool first = g == 0, last = g == G - 1;
+  const uint32_t l4 = rep16(m + p2m1);
+  const uint32_t mm = rep16(m);
+  uint32_t nl[NT];
+#pragma unroll
+  for (int k = 0; k < NT; ++k) {
+    uint32_t lw, rw;
+    if (k > 0) lw = __byte_perm(L[k - 1], L[k], 0x5432);
+    else lw = first ? ((L[0] << 16) | 0xFFFFu) : __byte_perm(left_nb, L[0], 0x5432);
+    if (k < NT - 1) rw = __byte_perm(L[k], L[k + 1], 0x5432);
+    else rw = last ? ((L[k] >> 16) | 0xFFFF0000u) : __byte_perm(L[k], right_nb, 0x5432);
+    const uint32_t x = __vimin3_u16x2(lw, rw, l4);
+    uint32_t t = __viaddmin_u16x2(x, p1x2, L[k]);
+    if (k == 0 && first) t = min16x2(t, 0xFFFF0000u | kInvalidCost);            // d = 0: left candidate 127
+    if (k == NT - 1 && last) t = min16x2(t, (kInvalidCost << 16) | 0xFFFFu);    // d = D-1: right candidate 127
+    nl[k] = t + c[k] - mm;
+  }
+#pragma unroll
+  for (int k = 0; k < NT; ++k) L[k] = nl[k];
+  return group_min16<NT, G>(nl);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Cost volume of both views (reference Kernel_CostCompute cusgm_cc.cu:118-172 / 238-293):
+// view 0: C(x,d) = popc(cl[x] ^ cr[x-min_d-d]), view 1: C(x,d) = popc(cr[x] ^ cl[x+min_d+d]),
+// an out-of-range partner index reads element 0 of the partner row; with 5x5 census the last
+// pixel of every D-pixel block of view 1 keeps its view-0 cost (cusgm_cc.cu:288).
+// One thread per pixel, 128 pixels of one row per CTA, partner words staged in shared memory.
+// Columns x < max(0, min_d) are not written (no path reads them).
+// ---------------------------------------------------------------------------------------------
+// 128 pixels [bx, bx + 128) of row y, view `view`, by a 128-thread block (every thread calls it).
+template <int K, typename Word>
+__device__ __forceinline__ void cost3_block(const Word* __restrict__ cs_l, const Word* __restrict__ cs_r,
+                                            uint8_t* __restrict__ cost, const PlainParams& P, int view, int y, int bx,
+                                            Word* win) {
+  constexpr int D = 32 * K;
+  const int W = P.W;
+  const Word* own = (view == 0 ? cs_l : cs_r) + (size_t)y * W;
+  const Word* oth = (view == 0 ? cs_r : cs_l) + (size_t)y * W;
+  const Word oth0 = oth[0];
+  // view 0: window index i <-> partner position bx - min_d - (D-1) + i;
+  // view 1: i <-> bx + min_d + i
+  const int ws = view == 0 ? bx - P.min_d - (D - 1) : bx + P.min_d;
+  for (int i = threadIdx.x; i < 128 + D - 1; i += 128) {
+    const int pos = ws + i;
+    win[i] = (pos >= 0 && pos < W) ? oth[pos] : oth0;
+  }
+  __syncthreads();
+  const int x = bx + threadIdx.x;
+  if (x >= W || x < P.x0) return;
+  const Word a = own[x];
+  bool lr_cost = false;
+  if (view == 1 && sizeof(Word) == 4) {
+    const int blk = P.x0 + ((x - P.x0) / D) * D;
+    lr_cost = (x == blk + min(D, W - blk) - 1);
+  }
+  uint8_t* out = cost + (size_t)view * P.vstride + ((size_t)y * W + x) * D;
+  if (!lr_cost) {
+#pragma unroll
+    for (int v = 0; v < D / 16; ++v) {
+      uint32_t q[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        uint32_t packed = 0;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          const int d = 16 * v + 4 * j + b;
+          const Word p = win[view == 0 ? threadIdx.x + (D - 1) - d : threadIdx.x + d];
+          packed |= popc_word((Word)(a ^ p)) << (8 * b);
+        }
+        q[j] = packed;
+      }
+      reinterpret_cast<uint4*>(out)[v] = make_uint4(q[0], q[1], q[2], q[3]);
+    }
+  } else {  // 5x5 right view: this pixel keeps its left-to-right cost
+    const Word* g_own = cs_r + (size_t)y * W;
+    const Word own0 = g_own[0];
+    const Word l = cs_l[(size_t)y * W + x];
+    for (int v = 0; v < D / 16; ++v) {
+      uint32_t q[4];
+      for (int j = 0; j < 4; ++j) {
+        uint32_t packed = 0;
+        for (int b = 0; b < 4; ++b) {
+          const int d = 16 * v + 4 * j + b;
+          const int pos = x - P.min_d - d;
+          const Word p = (pos >= 0 && pos < W) ? g_own[pos] : own0;
+          packed |= popc_word((Word)(l ^ p)) << (8 * b);
+        }
+        q[j] = packed;
+      }
+      reinterpret_cast<uint4*>(out)[v] = make_uint4(q[0], q[1], q[2], q[3]);
+    }
+  }
+}
+
+template <int K, typename Word>
+__global__ void __launch_bounds__(128) k_cost3(const Word* __restrict__ cs_l, const Word* __restrict__ cs_r,
+                                               uint8_t* __restrict__ cost, PlainParams P) {
+  __shared__ Word win[128 + 32 * K];
+  cost3_block<K, Word>(cs_l, cs_r, cost, P, blockIdx.z, blockIdx.y, blockIdx.x * 128, win);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Horizontal paths, G threads per scanline (view, direction, row): scanline index i -> group
+// i / H (view = group >> 1, dir = group & 1), y = i % H. Reads the cost volume, writes the
+// left-to-right (dir 0) or right-to-left (dir 1) path volume; the cost of step s + PF is loaded
+// at step s. Same results as the lane-per-disparity row kernels (reference
+// Kernel_Aggregate_Horizontal_Warpfor*, cusgm_ca.cu:1343-1770).
+// ---------------------------------------------------------------------------------------------
+// Scanline i (lane g of its G lanes); every lane of the warp calls it with the same trip count.
+// i >= nviews*2*H: the lane follows the last scanline without storing (the shuffles need it).
+template <int K, int G, int PF>
+__device__ __forceinline__ void hpaths3_lane(const uint8_t* __restrict__ cost, uint8_t* __restrict__ lr,
+                                             uint8_t* __restrict__ rl, const PlainParams& P, int nviews, int i,
+                                             int g) {
+  constexpr int D = 32 * K, NT = D / 2 / G, NR = NT / 2, SB = D / G;  // SB: bytes per thread slice
+  const int H = P.H, W = P.W;
+  const int nscan = nviews * 2 * H;
+  const bool valid = i < nscan;
+  if (!valid) i = nscan - 1;
+  const int grp = i / H;
+  const int y = i - grp * H;
+  const int view = grp >> 1, dir = grp & 1;
+  const int x0 = P.x0;
+  const int len = W - x0;
+  if (len <= 0) return;  // uniform over the grid
+  const size_t vo = (size_t)view * P.vstride + (size_t)y * W * D + (size_t)g * SB;
+  const uint8_t* crow = cost + vo;
+  uint8_t* orow = (dir == 0 ? lr : rl) + vo;
+  const uint32_t p1x2 = rep16(P.p1), p2m1 = P.p2 - P.p1;
+  const int xs = dir == 0 ? x0 : W - 1;
+  const int dx = dir == 0 ? 1 : -1;
+  uint32_t L[NT], c[NT], out[NR];
+  uint32_t ring[PF][NR];
+#pragma unroll
+  for (int j = 0; j < PF; ++j)
+    if (j < len) ld_slice<NR>(crow + (size_t)(xs + j * dx) * D, ring[j]);
+  uint32_t m = 0;
+  for (int s0 = 0; s0 < len; s0 += PF) {
+#pragma unroll
+    for (int j = 0; j < PF; ++j) {
+      const int s = s0 + j;
+      if (s < len) {
+        const int x = xs + s * dx;
+        widen_slice<NR>(ring[j], c);
+        if (s + PF < len) ld_slice<NR>(crow + (size_t)(x + PF * dx) * D, ring[j]);
+        m = s == 0 ? first_g<NT, G>(L, c) : step_g<NT, G>(L, c, m, p1x2, p2m1, g);
+        narrow_slice<NR>(L, out);
+        if (valid) st_slice<NR>(orow + (size_t)x * D, out);
+      }
+    }
+  }
+}
+
+template <int K, int G, int PF>
+__global__ void __launch_bounds__(128) k_hpaths3(const uint8_t* __restrict__ cost, uint8_t* __restrict__ lr,
+                                                 uint8_t* __restrict__ rl, PlainParams P, int nviews) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  hpaths3_lane<K, G, PF>(cost, lr, rl, P, nviews, t / G, threadIdx.x % G);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Vertical paths + 4-path sum + WTA, G threads per column: a bottom-to-top pass storing its path
+// costs, then top-to-bottom summing the four u8 path costs and selecting the disparity inside
+// the column's threads. Same results as k_vpaths_wta_plain (reference
+// Kernel_Aggregate_Vertical_Warpfor*, cusgm_ca.cu:1410-1888, WTA cusgm_ca.cu:3514-3809).
+// Shared memory: D/2 + 1 words per column (the sums, read back for S(d*-1), S(d*+1) and the
+// reference tie rule), i.e. vpaths3_col_smem<K>() bytes per column.
+// ---------------------------------------------------------------------------------------------
+template <int K>
+__host__ __device__ constexpr size_t vpaths3_col_smem() { return (size_t)(16 * K + 1) * 4; }
+
+// Column xc of view `view` (lane g of its G lanes); colS: this column's D/2 + 1 words of shared
+// memory. Every lane of the warp calls it (same H); xc >= W: the lane follows column W-1 without
+// storing.
+template <int K, int G, int PF>
+__device__ __forceinline__ void vpaths3_lane(const uint8_t* __restrict__ cost, const uint8_t* __restrict__ lr,
+                                             const uint8_t* __restrict__ rl, uint8_t* __restrict__ bt,
+                                             float* __restrict__ disp, const PlainParams& P, const WtaParams& Q,
+                                             int view, int xc, int g, uint32_t* colS) {
+  constexpr int D = 32 * K, NW = D / 2, NT = NW / G, NR = NT / 2, SB = D / G;
+  uint32_t* myS = colS + g * NT;
+  const int W = P.W, H = P.H;
+  const bool valid = xc < W;
+  const int x = valid ? xc : W - 1;            // idle lanes follow the last column, without stores
+  const bool computed = valid && x >= P.x0;    // columns left of x0 are INVALID
+  const bool col_ok = computed && x >= 5 && x <= W - 5;
+  float* dout = disp + (size_t)view * Q.dstride + x;
+  const size_t vo = (size_t)view * P.vstride + (size_t)x * D + (size_t)g * SB;
+  const size_t rs = (size_t)W * D;
+  const uint8_t* cv = cost + vo;
+  uint8_t* btv = bt + vo;
+  const uint32_t p1x2 = rep16(P.p1), p2m1 = P.p2 - P.p1;
+  uint32_t L[NT], c[NT], out[NR];
+  uint32_t ring[PF][NR];
+  uint32_t m = 0;
+  // bottom -> top
+#pragma unroll
+  for (int j = 0; j < PF; ++j)
+    if (j < H) ld_slice<NR>(cv + (size_t)(H - 1 - j) * rs, ring[j]);
+  for (int s0 = 0; s0 < H; s0 += PF) {
+#pragma unroll
+    for (int j = 0; j < PF; ++j) {
+      const int s = s0 + j;
+      if (s < H) {
+        const int y = H - 1 - s;
+        widen_slice<NR>(ring[j], c);
+        if (s + PF < H) ld_slice<NR>(cv + (size_t)(y - PF) * rs, ring[j]);
+        m = s == 0 ? first_g<NT, G>(L, c) : step_g<NT, G>(L, c, m, p1x2, p2m1, g);
+        narrow_slice<NR>(L, out);
+        if (computed) st_slice<NR>(btv + (size_t)y * rs, out);
+      }
+    }
+  }
+  // top -> bottom + sum + WTA; the other three paths of row y + PF are loaded at row y
+  const uint8_t* lrv = lr + vo;
+  const uint8_t* rlv = rl + vo;
+  uint32_t ra[PF][NR], rb[PF][NR], re[PF][NR];
+#pragma unroll
+  for (int j = 0; j < PF; ++j) {
+    if (j < H) {
+      ld_slice<NR>(cv + (size_t)j * rs, ring[j]);
+      ld_slice<NR>(btv + (size_t)j * rs, ra[j]);
+      ld_slice<NR>(lrv + (size_t)j * rs, rb[j]);
+      ld_slice<NR>(rlv + (size_t)j * rs, re[j]);
+    }
+  }
+  for (int y0 = 0; y0 < H; y0 += PF) {
+#pragma unroll
+    for (int j = 0; j < PF; ++j) {
+      const int y = y0 + j;
+      if (y < H) {
+        uint32_t wa[NT], wb[NT], we[NT];
+        widen_slice<NR>(ring[j], c);
+        widen_slice<NR>(ra[j], wa);
+        widen_slice<NR>(rb[j], wb);
+        widen_slice<NR>(re[j], we);
+        if (y + PF < H) {
+          const size_t o = (size_t)(y + PF) * rs;
+          ld_slice<NR>(cv + o, ring[j]);
+          ld_slice<NR>(btv + o, ra[j]);
+          ld_slice<NR>(lrv + o, rb[j]);
+          ld_slice<NR>(rlv + o, re[j]);
+        }
+        m = y == 0 ? first_g<NT, G>(L, c) : step_g<NT, G>(L, c, m, p1x2, p2m1, g);
+        if (y >= 5 && y <= H - 5 && y < Q.rows) {  // uniform over the warp
+          // S = the four u8 path costs summed (< 1024). Keys S << 6 | (d mod 64) per block of
+          // disparities: D = 32 one block; D = 64: d < 32 (A) and d >= 32 (B), the reference's two
+          // stores; D = 128: d < 64 and d >= 64.
+          constexpr int SPLIT = D == 32 ? 64 : (D == 64 ? 32 : 64);  // first d of the second block
+          uint32_t acc0 = 0xFFFFFFFFu, acc1 = 0xFFFFFFFFu;
+#pragma unroll
+          for (int k = 0; k < NT; ++k) {
+            const uint32_t sk = (L[k] & 0x00FF00FFu) + wa[k] + wb[k] + we[k];
+            myS[k] = sk;
+            const uint32_t d0 = (uint32_t)(2 * (g * NT + k));
+            const uint32_t key = sk * 64u + ((d0 & 63u) | (((d0 + 1u) & 63u) << 16));
+            if ((int)d0 < SPLIT) acc0 = min16x2(acc0, key);
+            else acc1 = min16x2(acc1, key);
+          }
+          const uint32_t k0 = group_min<G>(hmin16(acc0)), k1 = group_min<G>(hmin16(acc1));
+          __syncwarp();
+          uint32_t sm;
+          int ds;
+          if constexpr (D == 32) {
+            sm = k0 >> 6;
+            ds = (int)(k0 & 63);
+          } else if constexpr (D == 64) {
+            const uint32_t SA = k0 >> 6, SB2 = k1 >> 6;
+            sm = min(SA, SB2);
+            ds = (int)(min(k0, k1) & 63);  // lowest d among the minima
+            if (Q.tie_rule == kTieRefB200) {
+              // A non-empty: odd rows take A; even rows take B = {t : S(t+32) == m, S(t) != m}
+              // when non-empty (computed by every lane; the shuffles must not diverge)
+              const uint32_t mm = rep16(sm);
+              uint32_t ax = 0xFFFFFFFFu;
+#pragma unroll
+              for (int k = 0; k < NT; ++k) {
+                const int w = g * NT + k;  // word index; B words are 16..31
+                if (w >= 16) {
+                  const uint32_t z = colS[w - 16] - mm + 0x7FFF7FFFu;  // half >= 0x8000 iff S(t) != m
+                  const uint32_t eq = ~z & 0x80008000u;               // bit 15 of a half iff S(t) == m
+                  const uint32_t hx = myS[k] + (eq >> 5);              // excluded lanes get + 1024
+                  const uint32_t t0 = (uint32_t)(2 * (w - 16));
+                  ax = min16x2(ax, hx * 32u + (t0 | ((t0 + 1u) << 16)));
+                }
+              }
+              const uint32_t kx = group_min<G>(hmin16(ax));
+              if (SA == sm) {
+                ds = (int)(k0 & 63);
+                if ((y & 1) == 0 && (kx >> 5) == sm) ds = 32 + (int)(kx & 31);
+              }
+            }
+          } else {
+            const uint32_t s0 = k0 >> 6, s1 = k1 >> 6;
+            sm = min(s0, s1);
+            ds = s0 <= s1 ? (int)(k0 & 63) : 64 + (int)(k1 & 63);
+          }
+          float dv = kInvalidFloat;
+          if (col_ok && ds > 0 && ds < Q.dmax_excl) {
+            const uint32_t w1 = colS[(ds - 1) >> 1];
+            const float c1 = (float)(((ds - 1) & 1) ? (w1 >> 16) : (w1 & 0xFFFFu));
+            const float c2 = (float)sm;
+            float c3;
+            if (ds + 1 < D) {
+              const uint32_t w3 = colS[(ds + 1) >> 1];
+              c3 = (float)(((ds + 1) & 1) ? (w3 >> 16) : (w3 & 0xFFFFu));
+            } else {
+              c3 = (float)ds;
+            }
+            const float d12 = __fsub_rn(c1, c2), d32 = __fsub_rn(c3, c2);
+            const float uq = d12 < d32 ? d12 : d32;
+            if (!(uq <= __fmul_rn(c2, __fsub_rn(1.0f, Q.uniqueness))))
+              dv = __fadd_rn((float)(ds + P.min_d), subpix_bias(c1, c2, c3));
+          }
+          __syncwarp();
+          if (valid && g == 0) dout[(size_t)y * W] = dv;
+        } else if (valid && g == 0) {
+          dout[(size_t)y * W] = kInvalidFloat;
+        }
+      }
+    }
+  }
+}
+
+template <int K, int G, int PF>
+__global__ void __launch_bounds__(128) k_vpaths3(const uint8_t* __restrict__ cost, const uint8_t* __restrict__ lr,
+                                                 const uint8_t* __restrict__ rl, uint8_t* __restrict__ bt,
+                                                 float* __restrict__ disp, PlainParams P, WtaParams Q) {
+  extern __shared__ uint32_t s_sum[];
+  vpaths3_lane<K, G, PF>(cost, lr, rl, bt, disp, P, Q, blockIdx.y, (blockIdx.x * blockDim.x + threadIdx.x) / G,
+                         threadIdx.x % G, s_sum + (threadIdx.x / G) * (16 * K + 1));
+}
+
+}  // namespace sgm
+
+namespace sgm {
+
+// =============================================================================================
+// Initial-disparity levels (D = 32) with one thread (or G lanes) per scanline.
+//
+// The realigned recurrence (reference cusgm_ca.cu:1181-1338): with s = base - last_base,
+//   L'(d) = C(d) + min(L(d), L(d+s-1)+P1, L(d+s+1)+P1, m+P2') - m        (uint32)
+// where an index outside [0, 32) gives the candidate 127 and P2' = max(P1, P2/|last_base-base+1|).
+// After a pixel with an INVALID base the reference sets m = 127 whatever the path costs are, so
+// t - m wraps and later steps see wrapped values: these kernels keep one uint32 per disparity
+// (no 16-bit packing) so that the wraparound is the reference's. The shifted neighbours come from
+// the scanline's old costs written to a shared-memory row padded with 127 - P1 (127 after + P1,
+// modulo 2^32 for any P1); shifts beyond +-33 read padding only.
+// =============================================================================================
+constexpr int kIPad = 34;                      // padding words on each side of a scanline row
+constexpr int kIRow = kIPad + 32 + kIPad + 1;  // words per scanline row (odd: fewer bank conflicts)
+
+template <int ND>
+__device__ __forceinline__ void unpack_bytes(const uint32_t (&r)[ND / 4], uint32_t (&c)[ND]) {
+#pragma unroll
+  for (int j = 0; j < ND; ++j) c[j] = (r[j >> 2] >> (8 * (j & 3))) & 0xFFu;
+}
+template <int ND>
+__device__ __forceinline__ void pack_bytes(const uint32_t (&L)[ND], uint32_t (&r)[ND / 4]) {
+#pragma unroll
+  for (int i = 0; i < ND / 4; ++i)
+    r[i] = (L[4 * i] & 0xFFu) | ((L[4 * i + 1] & 0xFFu) << 8) | ((L[4 * i + 2] & 0xFFu) << 16) | (L[4 * i + 3] << 24);
+}
+
+template <int ND, int G>
+__device__ __forceinline__ uint32_t group_min32(const uint32_t (&v)[ND]) {
+  uint32_t t[ND];
+#pragma unroll
+  for (int k = 0; k < ND; ++k) t[k] = v[k];
+#pragma unroll
+  for (int st = 1; st < ND; st *= 2) {
+#pragma unroll
+    for (int k = 0; k + st < ND; k += 2 * st) t[k] = min(t[k], t[k + st]);
+  }
+  return group_min<G>(t[0]);
+}
+
+// P2' for k = |last_base - base + 1| (table for k < kP2Tab).
+__device__ __forceinline__ uint32_t p2_prime(const uint32_t* tab, int k, const InitParams& P) {
+  return p2_term(tab, k, P);
+}
+
+// One realigned step of the scanline held by G lanes (lane g owns d = g*ND .. g*ND+ND-1); every
+// lane of the warp calls it. `row`: this scanline's kIRow words (padding already written).
+template <int ND, int G>
+__device__ __forceinline__ uint32_t init_step32(uint32_t (&L)[ND], const uint32_t (&c)[ND], uint32_t m, int s,
+                                                uint32_t p2t, uint32_t p1, uint32_t* row, int g) {
+#pragma unroll
+  for (int j = 0; j < ND; ++j) row[kIPad + g * ND + j] = L[j];
+  __syncwarp();
+  const int sc = s < -33 ? -33 : (s > 33 ? 33 : s);
+  const uint32_t* src = row + kIPad + g * ND + sc - 1;  // src[j] = old L(g*ND + j + s - 1)
+  uint32_t w[ND + 2];
+#pragma unroll
+  for (int j = 0; j < ND + 2; ++j) w[j] = src[j];
+  __syncwarp();
+  const uint32_t l4 = m + p2t;
+  uint32_t nl[ND];
+#pragma unroll
+  for (int j = 0; j < ND; ++j) {
+    const uint32_t t = min(__vimin3_u32(L[j], w[j] + p1, w[j + 2] + p1), l4);
+    nl[j] = c[j] + (t - m);
+  }
+#pragma unroll
+  for (int j = 0; j < ND; ++j) L[j] = nl[j];
+  return group_min32<ND, G>(nl);
+}
+
+// Cost volume of an initial-disparity level (reference cusgm_cc.cu:173-237 / 294-360):
+// view 0: pos = x - d - base, C = (popc(own ^ oth[pos]) + CostAdjust(d)) & 0xFF for 0 < pos < W,
+// else the invalid cost; view 1: pos = x + d + base, partner oth[pos] for 0 < pos < W else oth[0].
+// One CTA per (row, view); the partner row's census words in shared memory (W words).
+template <typename Word>
+__global__ void __launch_bounds__(256) k_cost3_init(const Word* __restrict__ cs_l, const Word* __restrict__ cs_r,
+                                                    const int16_t* __restrict__ init_l,
+                                                    const int16_t* __restrict__ init_r, uint8_t* __restrict__ cost,
+                                                    InitParams P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Word* oth_s = reinterpret_cast<Word*>(smem_raw);
+  const int y = blockIdx.x, view = blockIdx.y;
+  const int W = P.W;
+  const Word* own = (view == 0 ? cs_l : cs_r) + (size_t)y * W;
+  const Word* oth = (view == 0 ? cs_r : cs_l) + (size_t)y * W;
+  const int16_t* ib = (view == 0 ? init_l : init_r) + (size_t)y * W;
+  for (int i = threadIdx.x; i < W; i += blockDim.x) oth_s[i] = oth[i];
+  __syncthreads();
+  uint8_t* crow = cost + (size_t)view * P.vstride + (size_t)y * W * kLevelRange;
+  for (int x = P.x0 + threadIdx.x; x < W; x += blockDim.x) {
+    const int base = ib[x];
+    const Word a = own[x];
+    uint32_t q[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      uint32_t packed = 0;
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const int d = 4 * i + b;
+        uint32_t v;
+        if (view == 0) {
+          const int pos = x - d - base;
+          v = (pos > 0 && pos < W) ? ((popc_word((Word)(a ^ oth_s[pos])) + cost_adjust(d)) & 0xFFu) : P.invalid_cost;
+        } else {
+          const int pos = x + d + base;
+          v = (popc_word((Word)(a ^ ((pos > 0 && pos < W) ? oth_s[pos] : oth_s[0]))) + cost_adjust(d)) & 0xFFu;
+        }
+        packed |= v << (8 * b);
+      }
+      q[i] = packed;
+    }
+    uint4* o = reinterpret_cast<uint4*>(crow + (size_t)x * kLevelRange);
+    o[0] = make_uint4(q[0], q[1], q[2], q[3]);
+    o[1] = make_uint4(q[4], q[5], q[6], q[7]);
+  }
+}
+
+// Horizontal paths of an initial-disparity level, G lanes per scanline (view, dir, y) with the
+// scanline index as in hpaths3_lane. INVALID bases are skipped (m := 127, L and last_base kept);
+// the first pixel sets last_base whatever its base.
+template <int G, int PF>
+__device__ __forceinline__ void hpaths3_init_lane(const uint8_t* __restrict__ cost,
+                                                  const int16_t* __restrict__ init_l,
+                                                  const int16_t* __restrict__ init_r, uint8_t* __restrict__ lr,
+                                                  uint8_t* __restrict__ rl, const InitParams& P, int nviews, int i,
+                                                  int g, uint32_t* row, const uint32_t* p2tab) {
+  constexpr int ND = kLevelRange / G, NR = ND / 4;
+  const int H = P.H, W = P.W;
+  const int nscan = nviews * 2 * H;
+  const bool valid = i < nscan;
+  if (!valid) i = nscan - 1;
+  const int grp = i / H;
+  const int y = i - grp * H;
+  const int view = grp >> 1, dir = grp & 1;
+  const int len = W - P.x0;
+  if (len <= 0) return;
+  const size_t vo = (size_t)view * P.vstride + (size_t)y * W * kLevelRange + (size_t)g * ND;
+  const uint8_t* crow = cost + vo;
+  uint8_t* orow = (dir == 0 ? lr : rl) + vo;
+  const int16_t* ib = (view == 0 ? init_l : init_r) + (size_t)y * W;
+  const int xs = dir == 0 ? P.x0 : W - 1;
+  const int dx = dir == 0 ? 1 : -1;
+  uint32_t L[ND], c[ND], out[NR];
+  uint32_t ring[PF][NR];
+  int rbase[PF];
+#pragma unroll
+  for (int j = 0; j < PF; ++j) {
+    if (j < len) {
+      ld_slice<NR>(crow + (size_t)(xs + j * dx) * kLevelRange, ring[j]);
+      rbase[j] = ib[xs + j * dx];
+    }
+  }
+  uint32_t m = 0;
+  int last_base = 0;
+  for (int s0 = 0; s0 < len; s0 += PF) {
+#pragma unroll
+    for (int j = 0; j < PF; ++j) {
+      const int s = s0 + j;
+      if (s < len) {
+        const int x = xs + s * dx;
+        unpack_bytes<ND>(ring[j], c);
+        const int base = rbase[j];
+        if (s + PF < len) {
+          ld_slice<NR>(crow + (size_t)(x + PF * dx) * kLevelRange, ring[j]);
+          rbase[j] = ib[x + PF * dx];
+        }
+        if (s == 0) {
+#pragma unroll
+          for (int k = 0; k < ND; ++k) L[k] = c[k];
+          m = group_min32<ND, G>(c);
+          last_base = base;
+        } else {
+          // computed by every lane (the exchange and the minimum are warp-wide); kept only for
+          // a valid base
+          uint32_t Lk[ND];
+#pragma unroll
+          for (int k = 0; k < ND; ++k) Lk[k] = L[k];
+          const int kk = abs(last_base - base + 1);
+          const uint32_t mn = init_step32<ND, G>(Lk, c, m, base - last_base, p2_prime(p2tab, kk, P), P.p1, row, g);
+          if (base != kInvalidShort) {
+#pragma unroll
+            for (int k = 0; k < ND; ++k) L[k] = Lk[k];
+            m = mn;
+            last_base = base;
+          } else {
+            m = kInvalidCost;
+          }
+        }
+        pack_bytes<ND>(L, out);
+        if (valid) st_slice<NR>(orow + (size_t)x * kLevelRange, out);
+      }
+    }
+  }
+}
+
+template <int G, int PF>
+__global__ void __launch_bounds__(128) k_hpaths3_init(const uint8_t* __restrict__ cost,
+                                                      const int16_t* __restrict__ init_l,
+                                                      const int16_t* __restrict__ init_r, uint8_t* __restrict__ lr,
+                                                      uint8_t* __restrict__ rl, InitParams P, int nviews) {
+  __shared__ uint32_t p2tab[kP2Tab];
+  __shared__ uint32_t rows[(128 / G) * kIRow];
+  fill_p2_table(p2tab, P, threadIdx.x, blockDim.x);
+  uint32_t* row = rows + (threadIdx.x / G) * kIRow;
+  const uint32_t pad = kInvalidCost - P.p1;
+  for (int k = threadIdx.x % G; k < kIPad; k += G) {
+    row[k] = pad;
+    row[kIPad + 32 + k] = pad;
+  }
+  __syncthreads();
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  hpaths3_init_lane<G, PF>(cost, init_l, init_r, lr, rl, P, nviews, t / G, threadIdx.x % G, row, p2tab);
+}
+
+// Vertical paths + sum + WTA of an initial-disparity level, G lanes per column. last_base starts
+// from row 0's base in both directions (reference behaviour). WTA (reference
+// Kernel_ComputeDisparityByWTA for initial disparities): d in [2, 30]; tie rule kTieRefB200 =
+// the lowest tied d whose uniqueness test passes (every tied lane writes its own result, a valid
+// one wins), kTieLowest = the lowest tied d, then tested.
+template <int G, int PF>
+__device__ __forceinline__ void vpaths3_init_lane(const uint8_t* __restrict__ cost, const uint8_t* __restrict__ lr,
+                                                  const uint8_t* __restrict__ rl, const int16_t* __restrict__ init_l,
+                                                  const int16_t* __restrict__ init_r, uint8_t* __restrict__ bt,
+                                                  float* __restrict__ disp, const InitParams& P, const WtaParams& Q,
+                                                  int view, int xc, int g, uint32_t* row, uint32_t* colS,
+                                                  const uint32_t* p2tab) {
+  constexpr int ND = kLevelRange / G, NR = ND / 4;
+  const int W = P.W, H = P.H;
+  const bool valid = xc < W;
+  const int x = valid ? xc : W - 1;
+  const bool computed = valid && x >= P.x0;
+  const bool col_ok = computed && x >= 5 && x <= W - 5;
+  float* dout = disp + (size_t)view * Q.dstride + x;
+  const int16_t* ib = (view == 0 ? init_l : init_r) + x;
+  const size_t vo = (size_t)view * P.vstride + (size_t)x * kLevelRange + (size_t)g * ND;
+  const size_t rs = (size_t)W * kLevelRange;
+  const uint8_t* cv = cost + vo;
+  uint8_t* btv = bt + vo;
+  uint32_t L[ND], c[ND], out[NR];
+  uint32_t ring[PF][NR];
+  int rbase[PF];
+  uint32_t m = 0;
+  const int base0 = ib[0];
+  int last_base = base0;
+  // bottom -> top
+#pragma unroll
+  for (int j = 0; j < PF; ++j) {
+    if (j < H) {
+      ld_slice<NR>(cv + (size_t)(H - 1 - j) * rs, ring[j]);
+      rbase[j] = ib[(size_t)(H - 1 - j) * W];
+    }
+  }
+  for (int s0 = 0; s0 < H; s0 += PF) {
+#pragma unroll
+    for (int j = 0; j < PF; ++j) {
+      const int s = s0 + j;
+      if (s < H) {
+        const int y = H - 1 - s;
+        unpack_bytes<ND>(ring[j], c);
+        const int base = rbase[j];
+        if (s + PF < H) {
+          ld_slice<NR>(cv + (size_t)(y - PF) * rs, ring[j]);
+          rbase[j] = ib[(size_t)(y - PF) * W];
+        }
+        bool store = true;
+        if (s == 0) {
+#pragma unroll
+          for (int k = 0; k < ND; ++k) L[k] = c[k];
+          m = group_min32<ND, G>(c);
+        } else {
+          uint32_t Lk[ND];
+#pragma unroll
+          for (int k = 0; k < ND; ++k) Lk[k] = L[k];
+          const uint32_t mn = init_step32<ND, G>(Lk, c, m, base - last_base,
+                                                 p2_prime(p2tab, abs(last_base - base + 1), P), P.p1, row, g);
+          if (base != kInvalidShort) {
+#pragma unroll
+            for (int k = 0; k < ND; ++k) L[k] = Lk[k];
+            m = mn;
+            last_base = base;
+          } else {
+            m = kInvalidCost;
+            store = false;
+          }
+        }
+        if (store && computed) {
+          pack_bytes<ND>(L, out);
+          st_slice<NR>(btv + (size_t)y * rs, out);
+        }
+      }
+    }
+  }
+  // top -> bottom + sum + WTA
+  const uint8_t* lrv = lr + vo;
+  const uint8_t* rlv = rl + vo;
+  last_base = base0;
+  uint32_t ra[PF][NR], rb[PF][NR], re[PF][NR];
+#pragma unroll
+  for (int j = 0; j < PF; ++j) {
+    if (j < H) {
+      const size_t o = (size_t)j * rs;
+      ld_slice<NR>(cv + o, ring[j]);
+      ld_slice<NR>(btv + o, ra[j]);
+      ld_slice<NR>(lrv + o, rb[j]);
+      ld_slice<NR>(rlv + o, re[j]);
+      rbase[j] = ib[(size_t)j * W];
+    }
+  }
+  for (int y0 = 0; y0 < H; y0 += PF) {
+#pragma unroll
+    for (int j = 0; j < PF; ++j) {
+      const int y = y0 + j;
+      if (y < H) {
+        uint32_t a[ND], b[ND], e[ND];
+        unpack_bytes<ND>(ring[j], c);
+        unpack_bytes<ND>(ra[j], a);
+        unpack_bytes<ND>(rb[j], b);
+        unpack_bytes<ND>(re[j], e);
+        const int base = rbase[j];
+        if (y + PF < H) {
+          const size_t o = (size_t)(y + PF) * rs;
+          ld_slice<NR>(cv + o, ring[j]);
+          ld_slice<NR>(btv + o, ra[j]);
+          ld_slice<NR>(lrv + o, rb[j]);
+          ld_slice<NR>(rlv + o, re[j]);
+          rbase[j] = ib[(size_t)(y + PF) * W];
+        }
+        bool skipped = false;
+        if (y == 0) {
+#pragma unroll
+          for (int k = 0; k < ND; ++k) L[k] = c[k];
+          m = group_min32<ND, G>(c);
+        } else {
+          uint32_t Lk[ND];
+#pragma unroll
+          for (int k = 0; k < ND; ++k) Lk[k] = L[k];
+          const uint32_t mn = init_step32<ND, G>(Lk, c, m, base - last_base,
+                                                 p2_prime(p2tab, abs(last_base - base + 1), P), P.p1, row, g);
+          if (base != kInvalidShort) {
+#pragma unroll
+            for (int k = 0; k < ND; ++k) L[k] = Lk[k];
+            m = mn;
+            last_base = base;
+          } else {
+            m = kInvalidCost;
+            skipped = true;
+          }
+        }
+        if (y >= 5 && y <= H - 5 && y < Q.rows) {  // uniform over the warp
+          uint32_t S[ND];
+          uint32_t lm = 0xFFFFFFFFu;
+#pragma unroll
+          for (int k = 0; k < ND; ++k) {
+            S[k] = (L[k] & 0xFFu) + a[k] + b[k] + e[k];
+            colS[g * ND + k] = S[k];
+            lm = min(lm, S[k]);
+          }
+          const uint32_t sm = group_min<G>(lm);
+          __syncwarp();
+          // lowest candidate d of this lane (and, for the reference rule, its uniqueness test)
+          int best = 64;
+          float bestv = kInvalidFloat;
+#pragma unroll
+          for (int k = 0; k < ND; ++k) {
+            const int d = g * ND + k;
+            if (S[k] == sm && best == 64) {
+              float v = kInvalidFloat;
+              if (d > 1 && d < kLevelRange - 1) {
+                const float c1 = (float)colS[d - 1], c2 = (float)sm, c3 = (float)colS[d + 1];
+                const float d12 = __fsub_rn(c1, c2), d32 = __fsub_rn(c3, c2);
+                const float uq = d12 < d32 ? d12 : d32;
+                if (!(uq <= __fmul_rn(c2, __fsub_rn(1.0f, Q.uniqueness))))
+                  v = __fadd_rn((float)(d + base), subpix_bias(c1, c2, c3));
+              }
+              if (Q.tie_rule == kTieRefB200) {
+                if (v != kInvalidFloat) { best = d; bestv = v; }
+              } else {
+                best = d;
+                bestv = v;
+              }
+            }
+          }
+          // group: the lane holding the lowest such d wins
+          int win = best;
+#pragma unroll
+          for (int o = 1; o < G; o *= 2) win = min(win, __shfl_xor_sync(kFull, win, o, G));
+          float dv = kInvalidFloat;
+          const uint32_t has = __ballot_sync(kFull, best == win && win < 64);
+          const int lane = threadIdx.x & 31;
+          const int gl = lane - g;  // first lane of this group
+          const uint32_t gmask = (G == 32 ? 0xFFFFFFFFu : ((1u << G) - 1u)) << gl;
+          const uint32_t mine = has & gmask;
+          const float vv = __shfl_sync(kFull, bestv, mine ? __ffs(mine) - 1 : lane);
+          if (mine) dv = vv;
+          if (!(col_ok && base != kInvalidShort && !skipped)) dv = kInvalidFloat;
+          __syncwarp();
+          if (valid && g == 0) dout[(size_t)y * W] = dv;
+        } else if (valid && g == 0) {
+          dout[(size_t)y * W] = kInvalidFloat;
+        }
+      }
+    }
+  }
+}
+
+template <int G, int PF>
+__global__ void __launch_bounds__(128) k_vpaths3_init(const uint8_t* __restrict__ cost,
+                                                      const uint8_t* __restrict__ lr, const uint8_t* __restrict__ rl,
+                                                      const int16_t* __restrict__ init_l,
+                                                      const int16_t* __restrict__ init_r, uint8_t* __restrict__ bt,
+                                                      float* __restrict__ disp, InitParams P, WtaParams Q) {
+  __shared__ uint32_t p2tab[kP2Tab];
+  __shared__ uint32_t rows[(128 / G) * kIRow];
+  __shared__ uint32_t sums[(128 / G) * 33];
+  fill_p2_table(p2tab, P, threadIdx.x, blockDim.x);
+  uint32_t* row = rows + (threadIdx.x / G) * kIRow;
+  const uint32_t pad = kInvalidCost - P.p1;
+  for (int k = threadIdx.x % G; k < kIPad; k += G) {
+    row[k] = pad;
+    row[kIPad + 32 + k] = pad;
+  }
+  __syncthreads();
+  const int xc = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+  vpaths3_init_lane<G, PF>(cost, lr, rl, init_l, init_r, bt, disp, P, Q, blockIdx.y, xc, threadIdx.x % G, row,
+                           sums + (threadIdx.x / G) * 33, p2tab);
+}
+
+}  // namespace sgm

@@ -100,7 +100,7 @@ int run(const uint8_t* dl, const uint8_t* dr, float* dout, int W, int H, int M, 
   const size_t hsmem = (size_t)R * 2 * W * sizeof(Word);
   if (hsmem > 227 * 1024) return fail(SGM_ERR_UNSUPPORTED, "image width %d too large", W);
   auto hk = sgm::k_hpaths_plain<K, Word>;
-  cudaFuncSetAttribute(hk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem);
+  sgm::allow_max_dynamic_smem(hk);
   hk<<<dim3((H + R - 1) / R, nv), dim3(32, 2 * R), hsmem, s>>>(cs[0], cs[1], cost, lr, rl, P);
   sgm::WtaParams Q;
   Q.uniqueness = o->unique_threshold;

@@ -93,6 +93,27 @@ SGM_API int sgm_init(sgm_handle_t h, int32_t width, int32_t height, int32_t min_
 /* No counterpart in the reference: sets the rules in sgm_ext_options_t (before or after init). */
 SGM_API int sgm_set_ext_options(sgm_handle_t h, const sgm_ext_options_t* ext);
 SGM_API int sgm_get_ext_options(sgm_handle_t h, sgm_ext_options_t* ext);
+
+/* No counterpart in the reference. Kernel variants and launch shapes; results do not depend on
+ * them (every variant is bit-exact), only speed does. 0 everywhere = defaults. */
+typedef struct sgm_tuning_t {
+  int32_t row_kernel;   /* horizontal scans: 1 = whole census rows in shared memory,
+                           2 = census window and 32-pixel cost chunks in shared memory,
+                           3 = cost-volume kernel + row_lanes lanes per scanline (u16x2 SIMD);
+                           0 (default) = 3 where it is exact (see below), else 2 */
+  int32_t rows_per_cta; /* scanlines per CTA of the horizontal scans: 0 (default), 1, 2 or 4 */
+  int32_t col_kernel;   /* vertical scans + WTA: 1 = one warp per column, plain loads, 2 = the same with
+                           an 8-row prefetch ring, 3 = col_lanes lanes per column (u16x2 SIMD, WTA in
+                           the lanes); 0 (default) = 3 where it is exact, else 1. Variant 3 is exact
+                           for D <= 128, P1 <= P2 <= 16383 and tie rule 0 or 4 (else 2 / 1 run) */
+  int32_t cols_per_cta; /* columns (one warp each) per CTA of the vertical scans: 0 (default) .. 8 */
+  int32_t bt_smem;      /* 1: keep bottom-to-top path costs in shared memory when they fit */
+  int32_t row_lanes;    /* variant 3: lanes per scanline of the horizontal scans, 1/2/4/8 (0: 8) */
+  int32_t col_lanes;    /* variant 3: lanes per column of the vertical scans, 1/2/4/8 (0: 4);
+                           D = 128 takes 2 or 4 (default 4) */
+} sgm_tuning_t;
+SGM_API int sgm_set_tuning(sgm_handle_t h, const sgm_tuning_t* t);
+SGM_API int sgm_get_tuning(sgm_handle_t h, sgm_tuning_t* t);
 /* StereoCuda::Match -- SgmStereoCuda/StereoCuda.h:44, StereoCudaImpl.cpp:507-546.
  * Host buffers of width*height elements. disp_right, init_disp_left, roi_* may be NULL.
  * Returns after the disparity has been copied back (synchronous, like the reference). */
@@ -164,6 +185,51 @@ SGM_API int sgm_profile_read(char* buf, size_t cap);
 SGM_API int sgm_match_noalloc(const uint8_t* d_left, const uint8_t* d_right, float* d_disp_left, int32_t width,
                               int32_t height, int32_t min_disparity, int32_t disp_range, const sgm_option_t* option,
                               void* stream);
+
+/* ---------------- batched matching (many pairs, one graph launch) ---------------- */
+
+/* No counterpart in the reference, which matches one pair per StereoCuda::Match call. A batch
+ * holds pairs of different sizes and disparity ranges (D = 32, 64 or 128) under one option set
+ * (census, penalties, uniqueness, LR check, median; no small-region removal, morphology, post
+ * filters or initial disparities). sgm_batch_init allocates one device arena for all pairs,
+ * picks launch shapes per (D, width class) bucket by timing candidates (cached per process) and
+ * captures the whole batch into one CUDA graph. Each pair's result is bit-identical to
+ * sgm_match_device on that pair. */
+typedef struct sgm_batch* sgm_batch_t;
+typedef struct sgm_batch_pair_t {
+  int32_t width, height, min_disparity, disp_range;
+} sgm_batch_pair_t;
+typedef struct sgm_batch_info_t {
+  int32_t pairs, buckets;
+  uint64_t arena_bytes;     /* device memory of the batch */
+  int64_t kernels_per_run;  /* kernel launches inside one graph launch */
+} sgm_batch_info_t;
+typedef struct sgm_batch_bucket_t {
+  int32_t disp_range, width_class, pairs;  /* width class 0: <= 640, 1: <= 1280, 2: wider */
+  int32_t rows_lanes;                      /* 0: one warp per scanline; G: G lanes per scanline (u16x2) */
+  int32_t rows_warps_per_cta, rows_ctas;   /* persistent row-scan kernel shape */
+  int32_t cols_lanes;                      /* 0: one warp per column; G: G lanes per column (u16x2) */
+  int32_t cols_warps_per_cta, cols_prefetch, cols_ctas;  /* prefetch (one warp per column): 0 plain, 4/8 ring */
+} sgm_batch_bucket_t;
+SGM_API int sgm_batch_create(sgm_batch_t* out);
+SGM_API int sgm_batch_destroy(sgm_batch_t b);
+SGM_API const char* sgm_batch_last_error(sgm_batch_t b);
+/* ext may be NULL (default rules). */
+SGM_API int sgm_batch_init(sgm_batch_t b, const sgm_batch_pair_t* pairs, int32_t count, const sgm_option_t* option,
+                           const sgm_ext_options_t* ext);
+/* Re-times every bucket's candidates (ignoring the cache) and re-captures the graph. */
+SGM_API int sgm_batch_autotune(sgm_batch_t b);
+/* Device buffers of pair `index` inside the arena: width*height uint8 images to fill before
+ * sgm_batch_run, width*height float disparities to read after it. */
+SGM_API int sgm_batch_pair_buffers(sgm_batch_t b, int32_t index, uint8_t** d_left, uint8_t** d_right,
+                                   float** d_disp);
+/* One graph launch matching every pair, enqueued on `stream` (NULL: the batch's own stream). */
+SGM_API int sgm_batch_run(sgm_batch_t b, void* stream);
+/* Host buffers (arrays of `count` pointers): copies in, runs, copies out, synchronises. */
+SGM_API int sgm_batch_match(sgm_batch_t b, const uint8_t* const* left, const uint8_t* const* right,
+                            float* const* disp);
+SGM_API int sgm_batch_info(sgm_batch_t b, sgm_batch_info_t* info);
+SGM_API int sgm_batch_bucket(sgm_batch_t b, int32_t index, sgm_batch_bucket_t* bucket);
 
 /* ---------------- differentiable float32 SGM (training harness) ---------------- */
 
@@ -241,6 +307,9 @@ SGM_API int sgm_pyr_release(sgm_pyr_handle_t h);
 SGM_API int sgm_pyr_level_info(sgm_pyr_handle_t h, int32_t level, int32_t* width, int32_t* height,
                                int32_t* min_disp, int32_t* disp_range);
 SGM_API int64_t sgm_pyr_kernel_launches(sgm_pyr_handle_t h);
+/* No counterpart in the reference. Tuning of one level (level >= 0) or of every level (-1),
+ * after sgm_pyr_init. */
+SGM_API int sgm_pyr_set_tuning(sgm_pyr_handle_t h, int32_t level, const sgm_tuning_t* t);
 
 #ifdef __cplusplus
 }

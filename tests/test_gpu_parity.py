@@ -76,9 +76,17 @@ CASES = {
 }
 
 
+SCANLINE = {"warp": (2, 0, 1, 0, 0, 0, 0), "scanline_g1": (3, 0, 3, 0, 0, 1, 1),
+            "scanline_g8": (3, 0, 3, 0, 0, 8, 8)}
+
+
 @pytest.mark.parametrize("name", list(CASES))
 @pytest.mark.parametrize("tie", [4, 0, 2])
-def test_plain_parity(engine_lib, oracle_mod, name, tie):
+@pytest.mark.parametrize("variant", ["default", "warp", "scanline_g1", "scanline_g8"])
+def test_plain_parity(engine_lib, oracle_mod, name, tie, variant):
+    """Every stage against the oracle. 'default' runs the u16x2 scanline kernels where they are
+    exact (else the warp kernels), 'warp' the lane-per-disparity kernels, 'scanline_g*' the
+    scanline kernels with one and eight lanes per scanline."""
     import fasterstereocuda_b200 as fsc
     O = oracle_mod
     W, H, M, D, cs, p1, p2, u, lr, med, peaks, morph, seed = CASES[name]
@@ -87,6 +95,10 @@ def test_plain_parity(engine_lib, oracle_mod, name, tie):
     L, R, _ = scenes.planar_pair(seed, W, H, dmin=2.0, dmax=min(60.0, D - 4.0))
     ratio = 0.005 if peaks else 0.0005
     s = make_engine(fsc, W, H, M, D, cs, p1, p2, u, lr, med, peaks, ratio, morph, tie)
+    if variant != "default":
+        if tie != 4 and variant != "warp":
+            pytest.skip("tie rule variants with the default lane split only")
+        assert s.set_tuning(fsc.Tuning(*SCANLINE[variant])), s.last_error()
     disp = np.empty((H, W), np.float32)
     disp_r = np.empty((H, W), np.float32)
     assert s.Match(L, R, disp, disp_r), s.last_error()
@@ -232,3 +244,71 @@ def test_errors_on_device(engine_lib):
     assert not s.Match(img, img, out, None, None, roi) and s.status == -4
     s.Release()
     assert not s.Match(img, img, out) and s.status == -2
+
+
+TUNINGS = [(1, 0, 1, 0, 0), (1, 2, 1, 4, 0), (2, 1, 2, 8, 1), (2, 2, 2, 2, 0), (2, 4, 2, 1, 1), (1, 4, 2, 8, 0),
+           (3, 0, 3, 0, 0), (3, 0, 1, 0, 0), (2, 0, 3, 0, 0), (3, 0, 3, 0, 0, 2, 2), (3, 0, 3, 0, 0, 4, 8),
+           (3, 0, 3, 0, 0, 8, 1)]
+
+
+@pytest.mark.parametrize("tuning", TUNINGS)
+@pytest.mark.parametrize("kind", ["plain64", "plain128_5x5", "init32"])
+def test_tuning_variants_are_bit_exact(engine_lib, oracle_mod, tuning, kind):
+    """Every kernel variant / launch shape the tuner may pick gives the oracle's result."""
+    import fasterstereocuda_b200 as fsc
+    O = oracle_mod
+    W, H = 203, 131
+    L, R, _ = scenes.planar_pair(61, W, H)
+    t = fsc.Tuning(*tuning)
+    disp = np.empty((H, W), np.float32)
+    if kind == "init32":
+        init = _init_for(O, L, R, 1, 10, 150)
+        s = make_engine(fsc, W, H, 0, 32, 1, 10, 150, 0.95, 1, 1)
+        assert s.set_tuning(t), s.last_error()
+        assert s.Match(L, R, disp, None, init), s.last_error()
+        ref = O.match(O.Config(width=W, height=H, disp_range=32, do_lr_check=1, do_median=1, peaks_strips=STRIPS),
+                      L, R, init)
+    else:
+        D, cs, p1, p2 = (64, 1, 10, 150) if kind == "plain64" else (128, 0, 8, 32)
+        s = make_engine(fsc, W, H, -2, D, cs, p1, p2, 0.95, 1, 1)
+        assert s.set_tuning(t), s.last_error()
+        assert s.Match(L, R, disp), s.last_error()
+        ref = O.match(O.Config(width=W, height=H, min_disp=-2, disp_range=D, cs_type=cs, p1=p1, p2=p2,
+                               do_lr_check=1, do_median=1, peaks_strips=STRIPS), L, R)
+    assert_same(f"disp {kind} {tuning}", disp, ref["disp"])
+
+
+def test_pyramid_tuning_is_bit_exact(engine_lib, oracle_mod):
+    import fasterstereocuda_b200 as fsc
+    O = oracle_mod
+    W, H = 640, 360
+    L, R, _ = scenes.kitti_like(43, W, H)
+    p = fsc.FasterStereoCuda()
+    assert p.Init(fsc.StereoOption1(width=W, height=H, min_disp=0, max_disp=64, num_layers=3),
+                  fsc.LevelOverride(1, 10, 150), fsc.ExtOptions(peaks_strips=STRIPS)), p.last_error()
+    pc = O.PyrConfig(width=W, height=H, max_disp=64, num_layers=3, override_enable=1, cs_type=1, p1=10, p2=150,
+                     peaks_strips=STRIPS)
+    ref = O.pyr_match(pc, L, R)
+    for t in TUNINGS[:3]:
+        assert p.set_tuning(fsc.Tuning(*t)), p.last_error()
+        disp = np.empty((H, W), np.float32)
+        assert p.Match(L, R, disp)
+        assert_same(f"pyramid {t}", disp, ref)
+
+
+def test_large_pyramid_4800x3409_d256(engine_lib, oracle_mod):
+    """The large configuration: 4800x3409, disparities 0..256, 4 levels (coarsest 600x426 at
+    D=64, three 32-disparity levels), census 9x7, P1=10, P2=150, fractal texture, 40 planes."""
+    import fasterstereocuda_b200 as fsc
+    O = oracle_mod
+    W, H = 4800, 3409
+    L, R, _ = scenes.building_like(2, W, H)
+    p = fsc.FasterStereoCuda()
+    assert p.Init(fsc.StereoOption1(width=W, height=H, min_disp=0, max_disp=256, num_layers=4),
+                  fsc.LevelOverride(1, 10, 150), fsc.ExtOptions(peaks_strips=STRIPS)), p.last_error()
+    disp = np.empty((H, W), np.float32)
+    assert p.Match(L, R, disp), p.last_error()
+    pc = O.PyrConfig(width=W, height=H, max_disp=256, num_layers=4, override_enable=1, cs_type=1, p1=10, p2=150,
+                     peaks_strips=STRIPS)
+    assert_same("large pyramid", disp, O.pyr_match(pc, L, R))
+    assert (disp != INV).mean() > 0.5
