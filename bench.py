@@ -31,6 +31,9 @@ import numpy as np
 
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
+# one hardware work queue per matcher stream (the runtime's default of 8 serialises streams
+# beyond the eighth); must be set before CUDA initialises
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 W_, H_, DMAX = 1242, 375, 64
 LAYERS = 3
@@ -43,13 +46,13 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["pyramid", "plain"], default="pyramid")
-    ap.add_argument("--batch", type=int, default=32, help="pairs per step")
-    ap.add_argument("--streams", type=int, default=8, help="matchers (one CUDA stream each) per GPU")
+    ap.add_argument("--batch", type=int, default=64, help="pairs per step")
+    ap.add_argument("--streams", type=int, default=32, help="matchers (one CUDA stream each) per GPU")
     ap.add_argument("--pool", type=int, default=160, help="distinct input pairs resident in HBM")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="budget of the CPU baseline sample")
     ap.add_argument("--no-extras", action="store_true", help="skip the CPU baseline and extra workloads")
     ap.add_argument("--tuning", default="", help="kernel variants row_kernel,rows_per_cta,col_kernel,cols_per_cta,"
-                                                 "bt_smem (default: the engine's)")
+                                                 "bt_smem,row_lanes,col_lanes (default: autotuned lane split)")
     ap.add_argument("--profile-pairs", type=int, default=16, help="pairs of the serialised per-kernel timing pass")
     return ap.parse_args()
 
@@ -142,6 +145,12 @@ def alg_bytes(kernel, W, H, D, nviews, census_bytes):
     return 0
 
 
+# DRAM bytes per voxel (W*H*D*views of the launch) measured by ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum) for the default kernels at 1242x375x64; profiles/scanline_kernels_1242x375x64.md.
+NCU_DRAM_BYTES_PER_VOXEL = {"hpaths_plain": 2.79, "vpaths_wta_plain": 5.34, "hpaths_init": 1.07,
+                            "vpaths_wta_init": 3.23}
+
+
 # ------------------------------------------------------------------------------------ reference arm
 def run_reference(a, rank, world):
     if rank != 0:
@@ -223,6 +232,11 @@ def run_ours(a, rank, world, local_rank):
             raise RuntimeError(f"tuning rejected: {m.last_error()}")
         return m
 
+    def apply_tuning(t):
+        for m in matchers:
+            if not m.set_tuning(fsc.Tuning(*t)):
+                raise RuntimeError(f"tuning rejected: {m.last_error()}")
+
     def run_one(m, L, R, out, stream):
         if a.workload == "pyramid":
             ok = m.match_device(L, R, out, stream)
@@ -284,6 +298,24 @@ def run_ours(a, rank, world, local_rank):
             exp = O.match(O.Config(width=W_, height=H_, disp_range=DMAX), *pool[0])["disp"]
         bit_exact = bool(np.array_equal(outs[0].cpu().numpy().view(np.uint32), exp.view(np.uint32)))
 
+    # autotune: the lane split of the scanline kernels that is fastest at this concurrency
+    # (every split gives the same disparities); two untimed steps per candidate
+    tuning = a.tuning or None
+    if not a.tuning:
+        best = None
+        for lanes in ((8, 8), (8, 4), (4, 4), (4, 2), (2, 2)):
+            apply_tuning((0, 0, 0, 0, 0) + lanes)
+            step()
+            torch.cuda.synchronize()
+            t0c = time.perf_counter()
+            for _ in range(2):
+                step()
+            torch.cuda.synchronize()
+            dt = max_over_ranks(time.perf_counter() - t0c)
+            if best is None or dt < best[0]:
+                best = (dt, lanes)
+        apply_tuning((0, 0, 0, 0, 0) + best[1])
+        tuning = "autotuned row_lanes,col_lanes = %d,%d" % best[1]
     for _ in range(a.warmup):
         step()
     torch.cuda.synchronize()
@@ -347,10 +379,12 @@ def run_ours(a, rank, world, local_rank):
             levels.append(("plain", w, h, d, 2) if lv == LAYERS - 1 else ("init", w, h, d, 1))
     else:
         levels.append(("plain", W_, H_, DMAX, 2))
-    per_call_bytes = {}
+    per_call_bytes, per_call_voxels = {}, {}
     for k in prof:
-        per_call_bytes[k] = sum(alg_bytes(k, w, h, d, nv, 8) for (kind, w, h, d, nv) in levels
-                                if not k.startswith(("hpaths", "vpaths")) or k.endswith(kind))
+        mine = [(w, h, d, nv) for (kind, w, h, d, nv) in levels
+                if not k.startswith(("hpaths", "vpaths")) or k.endswith(kind)]
+        per_call_bytes[k] = sum(alg_bytes(k, w, h, d, nv, 8) for (w, h, d, nv) in mine)
+        per_call_voxels[k] = sum(w * h * d * nv for (w, h, d, nv) in mine)
     dom = max(prof, key=lambda k: prof[k]["ms"]) if prof else None
     calls = a.profile_pairs
     roofline = None
@@ -358,8 +392,12 @@ def run_ours(a, rank, world, local_rank):
         total_ms = prof[dom]["ms"]
         byts = per_call_bytes.get(dom, 0) * calls
         ach = byts / (total_ms / 1e3) / 1e9 if total_ms > 0 else 0.0
+        per_launch = max(1, prof[dom]["launches"] // calls)
+        bpv = NCU_DRAM_BYTES_PER_VOXEL.get(dom)
+        traffic = bpv * per_call_voxels.get(dom, 0) / per_launch if bpv else None
         roofline = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
-                    "frac": ach / hbm_peak, "traffic": None, "peak_kind": peak_kind,
+                    "frac": ach / hbm_peak, "traffic": traffic, "peak_kind": peak_kind,
+                    "traffic_source": "ncu DRAM bytes per voxel of this kernel x voxels per launch",
                     "avg_launch_us": total_ms / prof[dom]["launches"] * 1e3,
                     "alg_bytes_per_launch": per_call_bytes.get(dom, 0) / max(1, prof[dom]["launches"] // calls),
                     "timing": f"CUDA events around each launch, serialised pass of {calls} pairs on one stream"}
@@ -379,7 +417,7 @@ def run_ours(a, rank, world, local_rank):
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u8/u32 (f32 subpixel)",
             "data": "synthetic seeded KITTI-like pairs",
-            "config": dict(workload_config(a, a.batch), streams=S, tuning=a.tuning or "default",
+            "config": dict(workload_config(a, a.batch), streams=S, tuning=tuning,
                            l2=f"inputs larger than L2: rotating pool of {len(dL)} distinct pairs "
                               f"({pool_bytes / 2**20:.0f} MiB) per GPU"),
             "e2e": {"value": e2e_value, "unit": "pairs/s",
