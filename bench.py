@@ -511,6 +511,64 @@ def batch_vs_loop(pairs, images, runs, warmup):
             "init_s": init_s, "buckets": b.buckets()}
 
 
+def batch_pyramid_vs_loop(images, runs, warmup, streams=None):
+    """64 pyramid pairs (1242x375, disparities 0..64, 3 layers, census 9x7, P1=10, P2=150, LR +
+    median + removal) as one graph launch vs a loop of FasterStereoCuda.match_device on one
+    stream; outputs compared bit for bit."""
+    import torch
+    import fasterstereocuda_b200 as fsc
+    n = len(images)
+    opt = fsc.StereoOption1(num_layers=LAYERS, do_lr_check=True, do_rm_peaks=True)
+    ov = fsc.LevelOverride(1, 10, 150)
+    b = fsc.StereoBatchPyramid()
+    t = time.perf_counter()
+    if not b.Init([(W_, H_, 0, DMAX)] * n, opt, ov, fsc.ExtOptions()):
+        raise RuntimeError(b.last_error())
+    init_s = time.perf_counter() - t
+    dev = [(torch.from_numpy(L).cuda(), torch.from_numpy(R).cuda()) for L, R in images]
+    for i, (dl, dr) in enumerate(dev):
+        al, ar, _ = b.buffers(i)
+        _dev_copy(al, dl)
+        _dev_copy(ar, dr)
+    torch.cuda.synchronize()
+    main = torch.cuda.Stream()
+    for _ in range(warmup):
+        b.run(main.cuda_stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(main)
+    for _ in range(runs):
+        b.run(main.cuda_stream)
+    e1.record(main)
+    torch.cuda.synchronize()
+    batch_ms = e0.elapsed_time(e1) / runs
+    m = fsc.FasterStereoCuda()
+    if not m.Init(fsc.StereoOption1(width=W_, height=H_, min_disp=0, max_disp=DMAX, num_layers=LAYERS,
+                                    do_lr_check=True, do_rm_peaks=True), ov, fsc.ExtOptions()):
+        raise RuntimeError(m.last_error())
+    outs = [torch.empty((H_, W_), dtype=torch.float32, device="cuda") for _ in range(n)]
+
+    def loop():
+        for i in range(n):
+            if not m.match_device(dev[i][0], dev[i][1], outs[i], main.cuda_stream):
+                raise RuntimeError(m.last_error())
+    for _ in range(warmup):
+        loop()
+    torch.cuda.synchronize()
+    e0.record(main)
+    for _ in range(runs):
+        loop()
+    e1.record(main)
+    torch.cuda.synchronize()
+    loop_ms = e0.elapsed_time(e1) / runs
+    same = all(torch.equal(_read_dev(b.buffers(i)[2], H_, W_).view(torch.int32), outs[i].view(torch.int32))
+               for i in range(n))
+    info = b.info()
+    return {"pairs": n, "batch_pairs_per_s": n / (batch_ms / 1e3), "loop_pairs_per_s": n / (loop_ms / 1e3),
+            "speedup": loop_ms / batch_ms, "batch_ms": batch_ms, "loop_ms": loop_ms, "bit_exact_vs_per_pair": bool(same),
+            "kernels_per_graph": info["kernels_per_run"], "arena_gib": info["arena_bytes"] / 2**30, "init_s": init_s}
+
+
 def extra_batches(pool):
     from fasterstereocuda_b200 import scenes
     out = {}
@@ -520,6 +578,8 @@ def extra_batches(pool):
     specs = scenes.batch_specs()
     imgs = [scenes.planar_pair(seed, w, h, dmin=2.0, dmax=60.0)[:2] for (w, h, d, seed) in specs]
     out["batch64_uneven"] = batch_vs_loop([(w, h, 0, d) for (w, h, d, _) in specs], imgs, runs=3, warmup=1)
+    out["batch_pyramid_1242x375x64"] = batch_pyramid_vs_loop([pool[i % len(pool)] for i in range(64)], runs=5,
+                                                             warmup=2)
     out["batch64_uneven"]["workload"] = ("64 pairs, widths 320..1920, heights 240..1080 (multiples of 32), "
                                          "D in {64,128}, seeded planar scenes, census 9x7, LR + median")
     return out

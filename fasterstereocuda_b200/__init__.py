@@ -163,6 +163,14 @@ def load_library(path: Optional[os.PathLike] = None):
         "sgm_batch_match": (i32, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]),
         "sgm_batch_info": (i32, [vp, C.POINTER(BatchInfo)]),
         "sgm_batch_bucket": (i32, [vp, i32, C.POINTER(BatchBucket)]),
+        "sgm_batch_pyr_create": (i32, [C.POINTER(vp)]), "sgm_batch_pyr_destroy": (i32, [vp]),
+        "sgm_batch_pyr_last_error": (C.c_char_p, [vp]),
+        "sgm_batch_pyr_init": (i32, [vp, C.POINTER(BatchPair), i32, C.POINTER(StereoOption1),
+                                     C.POINTER(LevelOverride), C.POINTER(ExtOptions)]),
+        "sgm_batch_pyr_pair_buffers": (i32, [vp, i32, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]),
+        "sgm_batch_pyr_run": (i32, [vp, vp]),
+        "sgm_batch_pyr_match": (i32, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]),
+        "sgm_batch_pyr_info": (i32, [vp, C.POINTER(BatchInfo)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -453,3 +461,67 @@ class StereoBatch:
                 raise RuntimeError(self.last_error())
             out.append({f: getattr(b, f) for f, _ in BatchBucket._fields_})
         return out
+
+
+class StereoBatchPyramid:
+    """Many pyramid pairs (FasterStereoCuda semantics) of different sizes in one CUDA graph
+    launch (sgm_batch_pyr_*). Each pair's disparity equals FasterStereoCuda's for that pair."""
+
+    def __init__(self):
+        self._lib = load_library()
+        h = C.c_void_p()
+        st = self._lib.sgm_batch_pyr_create(C.byref(h))
+        if st != 0:
+            raise RuntimeError(f"sgm_batch_pyr_create failed ({st})")
+        self._h = h
+        self.status = 0
+        self.shapes = []
+
+    def __del__(self):
+        h, self._h = getattr(self, "_h", None), None
+        if h:
+            self._lib.sgm_batch_pyr_destroy(h)
+
+    def last_error(self) -> str:
+        return (self._lib.sgm_batch_pyr_last_error(self._h) or b"").decode()
+
+    def Init(self, pairs, option: StereoOption1, override: Optional[LevelOverride] = None,
+             ext: Optional[ExtOptions] = None) -> bool:
+        """pairs: sequence of (width, height, min_disp, max_disp); option: layers, LR, removal."""
+        arr = (BatchPair * len(pairs))(*[BatchPair(w, h, mn, mx - mn) for (w, h, mn, mx) in pairs])
+        self.status = self._lib.sgm_batch_pyr_init(self._h, arr, len(pairs), C.byref(option),
+                                                   C.byref(override) if override is not None else None,
+                                                   C.byref(ext) if ext is not None else None)
+        if self.status == 0:
+            self.shapes = [(p[1], p[0]) for p in pairs]
+        return self.status == 0
+
+    def buffers(self, i: int):
+        a, b, c = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        self.status = self._lib.sgm_batch_pyr_pair_buffers(self._h, i, C.byref(a), C.byref(b), C.byref(c))
+        if self.status != 0:
+            raise RuntimeError(self.last_error())
+        return a.value, b.value, c.value
+
+    def run(self, stream: int = 0) -> bool:
+        self.status = self._lib.sgm_batch_pyr_run(self._h, C.c_void_p(stream) if stream else None)
+        return self.status == 0
+
+    def Match(self, lefts, rights, disps) -> bool:
+        n = len(self.shapes)
+        for i, (L, R, O) in enumerate(zip(lefts, rights, disps)):
+            h, w = self.shapes[i]
+            for a, dt in ((L, np.uint8), (R, np.uint8), (O, np.float32)):
+                if a.dtype != dt or a.shape != (h, w) or not a.flags["C_CONTIGUOUS"]:
+                    raise ValueError(f"pair {i}: expected C-contiguous {dt.__name__} array of shape {(h, w)}")
+        pl = (C.c_void_p * n)(*[L.ctypes.data for L in lefts])
+        pr = (C.c_void_p * n)(*[R.ctypes.data for R in rights])
+        po = (C.c_void_p * n)(*[O.ctypes.data for O in disps])
+        self.status = self._lib.sgm_batch_pyr_match(self._h, pl, pr, po)
+        return self.status == 0
+
+    def info(self) -> dict:
+        i = BatchInfo()
+        if self._lib.sgm_batch_pyr_info(self._h, C.byref(i)) != 0:
+            raise RuntimeError(self.last_error())
+        return {f: getattr(i, f) for f, _ in BatchInfo._fields_}

@@ -31,181 +31,14 @@
 #include <vector>
 
 #include "../../include/sgm_b200.h"
-#include "sgm_kernels3.cuh"
+#include "sgm_batch_kernels.cuh"
+#include "sgm_levels.h"
 
 void sgm_set_process_error(const char* msg);
 
 namespace {
 
-struct BatchPair {
-  const uint8_t* img_l;
-  const uint8_t* img_r;
-  void* cs_l;
-  void* cs_r;
-  uint8_t* cost;
-  uint8_t* lr;
-  uint8_t* rl;
-  uint8_t* bt;
-  float* wta;  // [2][H][W]
-  float* out;  // [H][W]
-  sgm::PlainParams P;
-  sgm::WtaParams Q;
-  int nv;  // views (2 with the LR check)
-};
-
-// Largest b in [0, n) with prefix[b] <= item (prefix ascending, prefix[0] = 0).
-__device__ __forceinline__ int find_pair(const int* __restrict__ prefix, int n, int item) {
-  int lo = 0, hi = n - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (__ldg(prefix + mid) <= item) lo = mid;
-    else hi = mid - 1;
-  }
-  return lo;
-}
-
-template <typename Word, int CSW, int CSH>
-__global__ void __launch_bounds__(256) kb_census(const BatchPair* __restrict__ pairs, const int* __restrict__ prefix,
-                                                 int n) {
-  const int item = blockIdx.x * blockDim.y + threadIdx.y;
-  if (item >= __ldg(prefix + n)) return;
-  const int b = find_pair(prefix, n, item);
-  const BatchPair d = pairs[b];
-  const int W = d.P.W, H = d.P.H;
-  const int local = item - __ldg(prefix + b);
-  const int view = local / H;
-  const int y = local - view * H;
-  const uint8_t* img = view ? d.img_r : d.img_l;
-  Word* out = static_cast<Word*>(view ? d.cs_r : d.cs_l) + (size_t)y * W;
-  for (int x = threadIdx.x; x < W; x += 32) out[x] = sgm::census_value<Word, CSW, CSH>(img, x, y, W, H, view == 1);
-}
-
-template <int K, typename Word>
-__global__ void __launch_bounds__(256) kb_rows(const BatchPair* __restrict__ pairs, const int* __restrict__ ids,
-                                               const int* __restrict__ prefix, int n, int* __restrict__ queue) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  unsigned char* base = smem_raw + (size_t)threadIdx.y * sgm::hpaths2_warp_smem<K, Word>();
-  const int total = __ldg(prefix + n);
-  for (;;) {
-    int item = 0;
-    if (threadIdx.x == 0) item = atomicAdd(queue, 1);
-    item = __shfl_sync(sgm::kFull, item, 0);
-    if (item >= total) break;
-    const int b = find_pair(prefix, n, item);
-    const BatchPair d = pairs[__ldg(ids + b)];
-    const int local = item - __ldg(prefix + b);
-    const int per_view = 2 * d.P.H;
-    const int view = local / per_view;
-    const int rem = local - view * per_view;
-    sgm::hpaths2_warp<K, Word>(static_cast<const Word*>(d.cs_l), static_cast<const Word*>(d.cs_r), d.cost, d.lr,
-                               d.rl, d.P, view, rem >> 1, rem & 1, base);
-  }
-}
-
-template <int K, int PF>
-__global__ void __launch_bounds__(256) kb_cols(const BatchPair* __restrict__ pairs, const int* __restrict__ ids,
-                                               const int* __restrict__ prefix, int n, int* __restrict__ queue) {
-  const int total = __ldg(prefix + n);
-  for (;;) {
-    int item = 0;
-    if (threadIdx.x == 0) item = atomicAdd(queue, 1);
-    item = __shfl_sync(sgm::kFull, item, 0);
-    if (item >= total) break;
-    const int b = find_pair(prefix, n, item);
-    const BatchPair d = pairs[__ldg(ids + b)];
-    const int local = item - __ldg(prefix + b);
-    const int view = local / d.P.W;
-    const int x = local - view * d.P.W;
-    if constexpr (PF == 0)
-      sgm::vpaths1_warp<K>(d.cost, d.lr, d.rl, d.bt, d.wta, d.P, d.Q, view, x);
-    else
-      sgm::vpaths2_warp<K, PF>(d.cost, d.lr, d.rl, d.bt, d.wta, d.P, d.Q, view, x, nullptr);
-  }
-}
-
-template <int K, typename Word>
-__global__ void __launch_bounds__(128) kb_cost3(const BatchPair* __restrict__ pairs, const int* __restrict__ ids,
-                                                const int* __restrict__ prefix, int n) {
-  __shared__ Word win[128 + 32 * K];
-  const int item = blockIdx.x;
-  const int b = find_pair(prefix, n, item);
-  const BatchPair d = pairs[__ldg(ids + b)];
-  const int local = item - __ldg(prefix + b);
-  const int segs = (d.P.W + 127) / 128;
-  const int row = local / segs;  // view * H + y
-  const int seg = local - row * segs;
-  const int view = row / d.P.H;
-  sgm::cost3_block<K, Word>(static_cast<const Word*>(d.cs_l), static_cast<const Word*>(d.cs_r), d.cost, d.P, view,
-                            row - view * d.P.H, seg * 128, win);
-}
-
-// Items of 32/G scanlines (pair, first scanline); lanes beyond the pair's scanlines idle.
-template <int K, int G, int PF>
-__global__ void __launch_bounds__(256) kb_rows3(const BatchPair* __restrict__ pairs, const int* __restrict__ ids,
-                                                const int* __restrict__ prefix, int n, int* __restrict__ queue) {
-  constexpr int S = 32 / G;
-  const int lane = threadIdx.x;
-  const int total = __ldg(prefix + n);
-  for (;;) {
-    int item = 0;
-    if (lane == 0) item = atomicAdd(queue, 1);
-    item = __shfl_sync(sgm::kFull, item, 0);
-    if (item >= total) break;
-    const int b = find_pair(prefix, n, item);
-    const BatchPair d = pairs[__ldg(ids + b)];
-    const int local = item - __ldg(prefix + b);
-    sgm::hpaths3_lane<K, G, PF>(d.cost, d.lr, d.rl, d.P, d.nv, local * S + lane / G, lane % G);
-  }
-}
-
-template <int K, int G, int PF>
-__global__ void __launch_bounds__(256) kb_cols3(const BatchPair* __restrict__ pairs, const int* __restrict__ ids,
-                                                const int* __restrict__ prefix, int n, int* __restrict__ queue) {
-  constexpr int S = 32 / G;
-  extern __shared__ uint32_t s_sum[];
-  const int lane = threadIdx.x;
-  uint32_t* colS = s_sum + ((size_t)threadIdx.y * S + lane / G) * (16 * K + 1);
-  const int total = __ldg(prefix + n);
-  for (;;) {
-    int item = 0;
-    if (lane == 0) item = atomicAdd(queue, 1);
-    item = __shfl_sync(sgm::kFull, item, 0);
-    if (item >= total) break;
-    const int b = find_pair(prefix, n, item);
-    const BatchPair d = pairs[__ldg(ids + b)];
-    const int local = item - __ldg(prefix + b);
-    const int per_view = (d.P.W + S - 1) / S;
-    const int view = local / per_view;
-    const int grp = local - view * per_view;
-    sgm::vpaths3_lane<K, G, PF>(d.cost, d.lr, d.rl, d.bt, d.wta, d.P, d.Q, view, grp * S + lane / G, lane % G, colS);
-    __syncwarp();
-  }
-}
-
-template <bool LR, bool MED>
-__global__ void __launch_bounds__(256) kb_lr_median(const BatchPair* __restrict__ pairs,
-                                                    const int* __restrict__ prefix, int n, float thr) {
-  __shared__ float tile[10][34];
-  const int item = blockIdx.x;
-  const int b = find_pair(prefix, n, item);
-  const BatchPair d = pairs[b];
-  const int local = item - __ldg(prefix + b);
-  const int tiles_x = (d.P.W + 31) / 32;
-  const int ty = local / tiles_x;
-  const int tx = local - ty * tiles_x;
-  sgm::lr_median_tile<LR, MED>(d.wta, d.wta + d.Q.dstride, nullptr, d.out, d.P.W, d.P.H, thr, tx * 32, ty * 8, tile);
-}
-
-// Deterministic noise for the autotuner's timing runs (overwritten by the caller's images).
-__global__ void kb_fill_noise(uint8_t* p, size_t n, uint32_t seed) {
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    uint32_t h = (uint32_t)i * 2654435761u ^ seed;
-    h ^= h >> 15;
-    h *= 2246822519u;
-    h ^= h >> 13;
-    p[i] = (uint8_t)(h >> 24);
-  }
-}
+using namespace sgm::batch;
 
 size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
 
@@ -868,6 +701,685 @@ int sgm_batch_bucket(sgm_batch_t b, int32_t index, sgm_batch_bucket_t* out) {
   out->cols_warps_per_cta = k.tune.cols_warps;
   out->cols_prefetch = k.tune.cols_pf;
   out->cols_ctas = k.cols_blocks;
+  return SGM_OK;
+}
+
+}  // extern "C"
+
+// =============================================================================================
+// Batched pyramid: every pair's full pyramid (reference FasterStereoCuda::Match,
+// FasterStereoCuda.cpp:408-529) in one graph. The coarsest level of all pairs is a single-level
+// batch (its buckets and autotuned kernels above), followed by its dilation and small-region
+// removal; each finer 32-disparity level runs census, cost, the uint32 scanline scans (per width
+// class bucket, lane split autotuned) and the median for all pairs, then hands its map to the
+// next level as initial disparities.
+// =============================================================================================
+struct sgm_batch_pyr {
+  struct Bucket {
+    int wclass = 0;
+    std::vector<int> members;
+    int ids = 0, cost_prefix = 0, cost_items = 0, max_w = 0;
+    int rows_prefix[5] = {}, rows_items[5] = {}, cols_prefix[5] = {}, cols_items[5] = {};
+    int rows_lanes = 8, cols_lanes = 8, rows_blocks = 0, cols_blocks = 0;
+  };
+  struct Level {  // a 32-disparity level (index n < layers - 1)
+    int n = 0;
+    sgm_option_t opt{};
+    std::vector<BatchPair> hdesc;
+    BatchPair* ddesc = nullptr;
+    int census_prefix = 0, census_items = 0, tile_prefix = 0, tile_items = 0;
+    int row_prefix = 0, row_items = 0, pix_prefix = 0, pix_items = 0;
+    std::vector<Bucket> buckets;
+    int queue0 = 0;
+  };
+  bool ready = false;
+  int dev = 0, nsm = 148, layers = 1, word = 8;
+  cudaStream_t stream = nullptr;
+  std::vector<cudaStream_t> side;
+  std::vector<cudaEvent_t> ev;
+  std::vector<sgm_batch_pair_t> pairs;
+  sgm_ext_options_t ext{};
+  sgm_option_t copt{};  // coarsest level options (dilation / removal applied here)
+  sgm_batch* coarse = nullptr;
+  std::vector<Level> lv;
+  int c_tile_prefix = 0, c_tile_items = 0, c_row_prefix = 0, c_row_items = 0, c_pix_prefix = 0, c_pix_items = 0;
+  std::vector<int> dec_prefix, dec_items;  // per level >= 1: rows of the level (decimation)
+  unsigned char* arena = nullptr;
+  size_t arena_bytes = 0;
+  int* dtab = nullptr;
+  int* queues = nullptr;
+  int nqueues = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int64_t graph_kernels = 0;
+  std::string err;
+
+  void free_all() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+    if (coarse) {
+      coarse->free_all();
+      delete coarse;
+    }
+    coarse = nullptr;
+    for (auto& L : lv)
+      if (L.ddesc) cudaFree(L.ddesc);
+    lv.clear();
+    if (arena) cudaFree(arena);
+    if (dtab) cudaFree(dtab);
+    if (queues) cudaFree(queues);
+    arena = nullptr;
+    dtab = nullptr;
+    queues = nullptr;
+    for (auto s : side) cudaStreamDestroy(s);
+    side.clear();
+    for (auto e : ev) cudaEventDestroy(e);
+    ev.clear();
+    if (stream) cudaStreamDestroy(stream);
+    stream = nullptr;
+    pairs.clear();
+    dec_prefix.clear();
+    dec_items.clear();
+    ready = false;
+  }
+};
+
+namespace {
+
+int perr(sgm_batch_pyr* p, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  p->err = buf;
+  return code;
+}
+
+#define PTRY(p, expr)                                                                         \
+  do {                                                                                        \
+    cudaError_t _st = (expr);                                                                 \
+    if (_st != cudaSuccess)                                                                   \
+      return perr(p, _st == cudaErrorMemoryAllocation ? SGM_ERR_NOMEM : SGM_ERR_CUDA, "%s failed: %s", #expr, \
+                  cudaGetErrorString(_st));                                                   \
+  } while (0)
+
+using PBucket = sgm_batch_pyr::Bucket;
+using PLevel = sgm_batch_pyr::Level;
+
+template <typename F>
+int psize_grid(sgm_batch_pyr* p, F* fn, int threads, int items, int warps, int* blocks) {
+  PTRY(p, sgm::allow_max_dynamic_smem(fn));
+  int occ = 0;
+  PTRY(p, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, threads, 0));
+  *blocks = std::max(1, std::min(p->nsm * std::max(occ, 1), (items + warps - 1) / warps));
+  return SGM_OK;
+}
+
+int init_rows(sgm_batch_pyr* p, PLevel& L, PBucket& k, cudaStream_t s, int* queue, bool prepare) {
+  const int G = k.rows_lanes, li = lanes_index(G), n = (int)k.members.size();
+  const int* ids = p->dtab + k.ids;
+  const int* pre = p->dtab + k.rows_prefix[li];
+  auto go = [&](auto fn) -> int {
+    if (prepare) return psize_grid(p, fn, 128, k.rows_items[li], 4, &k.rows_blocks);
+    fn<<<k.rows_blocks, 128, 0, s>>>(L.ddesc, ids, pre, n, queue);
+    PTRY(p, cudaGetLastError());
+    return SGM_OK;
+  };
+  return G == 2 ? go(kb_rows3_init<2, 4>) : G == 4 ? go(kb_rows3_init<4, 8>) : go(kb_rows3_init<8, 8>);
+}
+
+int init_cols(sgm_batch_pyr* p, PLevel& L, PBucket& k, cudaStream_t s, int* queue, bool prepare) {
+  const int G = k.cols_lanes, li = lanes_index(G), n = (int)k.members.size();
+  const int* ids = p->dtab + k.ids;
+  const int* pre = p->dtab + k.cols_prefix[li];
+  auto go = [&](auto fn) -> int {
+    if (prepare) return psize_grid(p, fn, 128, k.cols_items[li], 4, &k.cols_blocks);
+    fn<<<k.cols_blocks, 128, 0, s>>>(L.ddesc, ids, pre, n, queue);
+    PTRY(p, cudaGetLastError());
+    return SGM_OK;
+  };
+  return G == 2 ? go(kb_cols3_init<2, 2>) : G == 4 ? go(kb_cols3_init<4, 4>) : go(kb_cols3_init<8, 4>);
+}
+
+int init_cost(sgm_batch_pyr* p, PLevel& L, PBucket& k, cudaStream_t s) {
+  const size_t smem = (size_t)k.max_w * p->word;
+  const int n = (int)k.members.size();
+  if (p->word == 8) {
+    PTRY(p, sgm::allow_max_dynamic_smem(kb_cost3_init<uint64_t>));
+    kb_cost3_init<uint64_t><<<k.cost_items, 256, smem, s>>>(L.ddesc, p->dtab + k.ids, p->dtab + k.cost_prefix, n);
+  } else {
+    PTRY(p, sgm::allow_max_dynamic_smem(kb_cost3_init<uint32_t>));
+    kb_cost3_init<uint32_t><<<k.cost_items, 256, smem, s>>>(L.ddesc, p->dtab + k.ids, p->dtab + k.cost_prefix, n);
+  }
+  PTRY(p, cudaGetLastError());
+  return SGM_OK;
+}
+
+// Median (and LR when set) of one level into post (dilation next) or out.
+int level_post(sgm_batch_pyr* p, const BatchPair* d, const int* tpre, int tiles, int n, const sgm_option_t& o,
+               cudaStream_t s) {
+  const dim3 blk(32, 8);
+  const float thr = o.lr_threshold;
+  if (o.do_lr_check && o.do_median_filter) kb_lr_median<true, true><<<tiles, blk, 0, s>>>(d, tpre, n, thr);
+  else if (o.do_lr_check) kb_lr_median<true, false><<<tiles, blk, 0, s>>>(d, tpre, n, thr);
+  else if (o.do_median_filter) kb_lr_median<false, true><<<tiles, blk, 0, s>>>(d, tpre, n, thr);
+  else kb_lr_median<false, false><<<tiles, blk, 0, s>>>(d, tpre, n, thr);
+  PTRY(p, cudaGetLastError());
+  return SGM_OK;
+}
+
+// Dilation and small-region removal of one level, when its options ask for them.
+int level_filters(sgm_batch_pyr* p, const BatchPair* d, const sgm_option_t& o, int tpre, int tiles, int rpre, int rows,
+                  int ppre, int pix, int n, cudaStream_t s, int64_t* kernels) {
+  if (o.morphology_type == 2) {
+    kb_dilation<<<tiles, dim3(32, 8), 0, s>>>(d, p->dtab + tpre, n);
+    (*kernels)++;
+  }
+  if (o.do_remove_peaks) {
+    const int am = p->ext.peaks_abs_mode;
+    kb_cc_rows<<<(rows + 7) / 8, dim3(32, 8), 0, s>>>(d, p->dtab + rpre, n, am);
+    kb_cc_vert<<<(pix + 255) / 256, 256, 0, s>>>(d, p->dtab + ppre, n, am);
+    kb_cc_count<<<(pix + 255) / 256, 256, 0, s>>>(d, p->dtab + ppre, n);
+    kb_cc_filter<<<(pix + 255) / 256, 256, 0, s>>>(d, p->dtab + ppre, n, o.peaks_ratio_threshold);
+    (*kernels) += 4;
+  }
+  PTRY(p, cudaGetLastError());
+  return SGM_OK;
+}
+
+int level_census(sgm_batch_pyr* p, const BatchPair* d, int cpre, int citems, int n, cudaStream_t s) {
+  const int blocks = (citems + 7) / 8;
+  if (p->word == 8) kb_census<uint64_t, 4, 3><<<blocks, dim3(32, 8), 0, s>>>(d, p->dtab + cpre, n);
+  else kb_census<uint32_t, 2, 2><<<blocks, dim3(32, 8), 0, s>>>(d, p->dtab + cpre, n);
+  PTRY(p, cudaGetLastError());
+  return SGM_OK;
+}
+
+// Lane splits of each 32-disparity bucket, timed on this batch's shapes (noise images, zero
+// initial disparities); every split gives the same result.
+int pyr_autotune(sgm_batch_pyr* p) {
+  const int npairs = (int)p->pairs.size();
+  for (auto& L : p->lv) {
+    int st0 = level_census(p, L.ddesc, L.census_prefix, L.census_items, npairs, p->stream);
+    if (st0) return st0;
+    for (size_t bi = 0; bi < L.buckets.size(); ++bi) {
+      auto& k = L.buckets[bi];
+      int* q = p->queues + L.queue0 + 2 * bi;
+      int st = init_cost(p, L, k, p->stream);
+      if (st) return st;
+      float best = 1e30f;
+      int bg = 8;
+      for (int G : {2, 4, 8}) {
+        k.rows_lanes = G;
+        st = init_rows(p, L, k, nullptr, nullptr, true);
+        if (st) return st;
+        cudaEvent_t e0, e1;
+        PTRY(p, cudaEventCreate(&e0));
+        PTRY(p, cudaEventCreate(&e1));
+        for (int r = 0; r < 2 && !st; ++r) {
+          if (r == 1) cudaEventRecord(e0, p->stream);
+          cudaMemsetAsync(q, 0, 2 * sizeof(int), p->stream);
+          st = init_rows(p, L, k, p->stream, q, false);
+        }
+        cudaEventRecord(e1, p->stream);
+        float ms = 0;
+        if (!st && cudaEventSynchronize(e1) == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (st) return st;
+        if (ms < best) { best = ms; bg = G; }
+      }
+      k.rows_lanes = bg;
+      best = 1e30f;
+      bg = 8;
+      for (int G : {2, 4, 8}) {
+        k.cols_lanes = G;
+        st = init_cols(p, L, k, nullptr, nullptr, true);
+        if (st) return st;
+        cudaEvent_t e0, e1;
+        PTRY(p, cudaEventCreate(&e0));
+        PTRY(p, cudaEventCreate(&e1));
+        for (int r = 0; r < 2 && !st; ++r) {
+          if (r == 1) cudaEventRecord(e0, p->stream);
+          cudaMemsetAsync(q + 1, 0, sizeof(int), p->stream);
+          st = init_cols(p, L, k, p->stream, q + 1, false);
+        }
+        cudaEventRecord(e1, p->stream);
+        float ms = 0;
+        if (!st && cudaEventSynchronize(e1) == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (st) return st;
+        if (ms < best) { best = ms; bg = G; }
+      }
+      k.cols_lanes = bg;
+      st = init_rows(p, L, k, nullptr, nullptr, true);
+      if (!st) st = init_cols(p, L, k, nullptr, nullptr, true);
+      if (st) return st;
+    }
+  }
+  return SGM_OK;
+}
+
+}  // namespace
+
+namespace {
+
+// census -> per-bucket [cost, rows, cols] -> LR/median of the coarsest level (the single-level
+// batch's stages), then its dilation and small-region removal; then, for every finer level, the
+// next-level initial disparities, census, per-bucket [cost, rows, cols], median.
+int pyr_capture(sgm_batch_pyr* p) {
+  if (p->exec) cudaGraphExecDestroy(p->exec);
+  if (p->graph) cudaGraphDestroy(p->graph);
+  p->exec = nullptr;
+  p->graph = nullptr;
+  cudaStream_t s = p->stream;
+  sgm_batch* c = p->coarse;
+  const int n = (int)p->pairs.size();
+  const int Lc = p->layers - 1;
+  PTRY(p, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  int st = SGM_OK;
+  int64_t kernels = 0;
+  int evi = 0;
+  auto fork_join = [&](int nb, auto body) {
+    cudaEventRecord(p->ev[evi], s);
+    const int fork = evi++;
+    for (int i = 0; i < nb && !st; ++i) {
+      cudaStream_t t = p->side[i];
+      cudaStreamWaitEvent(t, p->ev[fork], 0);
+      st = body(i, t);
+      cudaEventRecord(p->ev[evi], t);
+      cudaStreamWaitEvent(s, p->ev[evi], 0);
+      ++evi;
+    }
+  };
+  if (cudaMemsetAsync(c->queues, 0, c->nqueues * sizeof(int), s) != cudaSuccess ||
+      (p->nqueues && cudaMemsetAsync(p->queues, 0, p->nqueues * sizeof(int), s) != cudaSuccess))
+    st = perr(p, SGM_ERR_CUDA, "queue reset failed");
+  // level images from the full-resolution images
+  for (int lvl = 1; lvl < p->layers && !st; ++lvl) {
+    const BatchPair* dst = lvl == Lc ? c->ddesc : p->lv[lvl].ddesc;
+    kb_decimate<<<p->dec_items[lvl], 128, 0, s>>>(dst, p->lv[0].ddesc, p->dtab + p->dec_prefix[lvl], n, lvl);
+    kernels++;
+    if (cudaGetLastError() != cudaSuccess) st = perr(p, SGM_ERR_CUDA, "decimation launch failed");
+  }
+  // coarsest level
+  if (!st) { st = launch_census(c, s); kernels++; }
+  if (!st)
+    fork_join((int)c->buckets.size(), [&](int i, cudaStream_t t) {
+      int r = launch_rows(c, c->buckets[i], t, c->queues + 2 * i);
+      if (!r) r = launch_cols(c, c->buckets[i], t, c->queues + 2 * i + 1);
+      kernels += c->buckets[i].tune.rows_lanes ? 3 : 2;
+      return r;
+    });
+  if (!st) { st = launch_post(c, s); kernels++; }
+  if (!st)
+    st = level_filters(p, c->ddesc, p->copt, p->c_tile_prefix, p->c_tile_items, p->c_row_prefix, p->c_row_items,
+                       p->c_pix_prefix, p->c_pix_items, n, s, &kernels);
+  // finer levels
+  for (int lvl = Lc - 1; lvl >= 0 && !st; --lvl) {
+    PLevel& L = p->lv[lvl];
+    const BatchPair* above = lvl == Lc - 1 ? c->ddesc : p->lv[lvl + 1].ddesc;
+    kb_init_next<<<(L.pix_items + 255) / 256, 256, 0, s>>>(L.ddesc, above, p->dtab + L.pix_prefix, n);
+    kernels++;
+    if (cudaGetLastError() != cudaSuccess) st = perr(p, SGM_ERR_CUDA, "initial-disparity launch failed");
+    if (!st) { st = level_census(p, L.ddesc, L.census_prefix, L.census_items, n, s); kernels++; }
+    if (!st)
+      fork_join((int)L.buckets.size(), [&](int i, cudaStream_t t) {
+        int* q = p->queues + L.queue0 + 2 * i;
+        int r = init_cost(p, L, L.buckets[i], t);
+        if (!r) r = init_rows(p, L, L.buckets[i], t, q, false);
+        if (!r) r = init_cols(p, L, L.buckets[i], t, q + 1, false);
+        kernels += 3;
+        return r;
+      });
+    if (!st) { st = level_post(p, L.ddesc, p->dtab + L.tile_prefix, L.tile_items, n, L.opt, s); kernels++; }
+    if (!st)
+      st = level_filters(p, L.ddesc, L.opt, L.tile_prefix, L.tile_items, L.row_prefix, L.row_items, L.pix_prefix,
+                         L.pix_items, n, s, &kernels);
+  }
+  cudaGraph_t g = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(s, &g);
+  if (st) {
+    if (g) cudaGraphDestroy(g);
+    return st;
+  }
+  if (ce != cudaSuccess) return perr(p, SGM_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
+  p->graph = g;
+  PTRY(p, cudaGraphInstantiate(&p->exec, g, 0));
+  p->graph_kernels = kernels;
+  return SGM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sgm_batch_pyr_create(sgm_batch_pyr_t* out) {
+  if (!out) return SGM_ERR_ARG;
+  *out = new sgm_batch_pyr();
+  return SGM_OK;
+}
+
+int sgm_batch_pyr_destroy(sgm_batch_pyr_t p) {
+  if (!p) return SGM_ERR_ARG;
+  p->free_all();
+  delete p;
+  return SGM_OK;
+}
+
+const char* sgm_batch_pyr_last_error(sgm_batch_pyr_t p) { return p ? p->err.c_str() : ""; }
+
+int sgm_batch_pyr_init(sgm_batch_pyr_t p, const sgm_batch_pair_t* pairs, int32_t count,
+                       const sgm_pyr_option1_t* option, const sgm_level_override_t* ov, const sgm_ext_options_t* ext) {
+  if (!p) return SGM_ERR_ARG;
+  if (!pairs || !option || count <= 0) return perr(p, SGM_ERR_ARG, "empty batch or null argument");
+  if (count > 4096) return perr(p, SGM_ERR_ARG, "at most 4096 pairs per batch (got %d)", count);
+  if (option->do_smooth) return perr(p, SGM_ERR_UNSUPPORTED, "post filters are not supported");
+  const int layers = std::max(1, option->num_layers);
+  sgm_ext_options_t ex{};
+  ex.tie_rule = ex.init_tie_rule = sgm::kTieRefB200;
+  ex.p2_div0 = -1;
+  if (ext) ex = *ext;
+  if (layers > 1 && ex.init_tie_rule != sgm::kTieLowest && ex.init_tie_rule != sgm::kTieRefB200)
+    return perr(p, SGM_ERR_UNSUPPORTED, "batched pyramids support initial-disparity tie rules 0 and 4");
+  for (int i = 0; i < count; ++i) {
+    if (pairs[i].width <= 0 || pairs[i].height <= 0 || pairs[i].disp_range <= 0)
+      return perr(p, SGM_ERR_ARG, "pair %d: size or disparity range error", i);
+    if ((pairs[i].width >> (layers - 1)) < 8 || (pairs[i].height >> (layers - 1)) < 8)
+      return perr(p, SGM_ERR_ARG, "pair %d: too many layers for a %dx%d image", i, pairs[i].width, pairs[i].height);
+  }
+  p->free_all();
+  p->pairs.assign(pairs, pairs + count);
+  p->layers = layers;
+  p->ext = ex;
+  PTRY(p, cudaGetDevice(&p->dev));
+  PTRY(p, cudaDeviceGetAttribute(&p->nsm, cudaDevAttrMultiProcessorCount, p->dev));
+  PTRY(p, cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+  const int Lc = layers - 1;
+  auto o1_of = [&](int i) {
+    sgm_pyr_option1_t o = *option;
+    o.width = pairs[i].width;
+    o.height = pairs[i].height;
+    o.min_disp = pairs[i].min_disparity;
+    o.max_disp = pairs[i].min_disparity + pairs[i].disp_range;
+    return o;
+  };
+  // coarsest level: a single-level batch without its dilation / removal (applied here)
+  std::vector<sgm_batch_pair_t> cp(count);
+  sgm_option_t copt{};
+  for (int i = 0; i < count; ++i) {
+    const sgm_pyr_option1_t o = o1_of(i);
+    int dmin = 0, dr = 0;
+    level_options(&o, ov, Lc, layers, &copt, &dmin, &dr);
+    cp[i] = {pairs[i].width >> Lc, pairs[i].height >> Lc, dmin, dr};
+  }
+  p->copt = copt;
+  p->word = copt.cs_type == 1 ? 8 : 4;
+  sgm_option_t cbatch = copt;
+  cbatch.do_remove_peaks = false;
+  cbatch.morphology_type = 0;
+  p->coarse = new sgm_batch();
+  int st = sgm_batch_init(p->coarse, cp.data(), count, &cbatch, &ex);
+  if (st) return perr(p, st, "coarsest level: %s", p->coarse->err.c_str());
+  // finer levels: arena
+  p->lv.resize(Lc);
+  struct Sz { size_t img, cs, vol, n4, n2; };
+  size_t total = 0;
+  std::vector<std::vector<size_t>> off(Lc, std::vector<size_t>(count));
+  const bool cdil = copt.morphology_type == 2, cpeaks = copt.do_remove_peaks;
+  for (int lvl = 0; lvl < Lc; ++lvl) {
+    int dmin = 0, dr = 0;
+    const sgm_pyr_option1_t o0 = o1_of(0);
+    level_options(&o0, ov, lvl, layers, &p->lv[lvl].opt, &dmin, &dr);
+    p->lv[lvl].n = lvl;
+    const sgm_option_t& lo = p->lv[lvl].opt;
+    if (lo.do_lr_check) return perr(p, SGM_ERR_UNSUPPORTED, "LR check at an initial-disparity level");
+    for (int i = 0; i < count; ++i) {
+      const size_t N = (size_t)(pairs[i].width >> lvl) * (pairs[i].height >> lvl);
+      off[lvl][i] = total;
+      total += 2 * align256(N) + 2 * align256(N * p->word) + 4 * align256(N * sgm::kLevelRange) +
+               3 * align256(N * 4) + align256(N * 2) + (lo.do_remove_peaks ? 2 * align256(N * 4) : 0);
+    }
+  }
+  std::vector<size_t> coff(count);
+  for (int i = 0; i < count; ++i) {
+    const size_t N = (size_t)cp[i].width * cp[i].height;
+    coff[i] = total;
+    total += (cdil ? align256(N * 4) : 0) + (cpeaks ? 2 * align256(N * 4) : 0);
+  }
+  p->arena_bytes = total + p->coarse->arena_bytes;
+  if (total) PTRY(p, cudaMalloc(&p->arena, total));
+  // coarsest-level descriptors: post-processing buffers
+  int strips = ex.peaks_strips > 0 ? ex.peaks_strips : default_peaks_strips();
+  for (int i = 0; i < count; ++i) {
+    BatchPair& d = p->coarse->hdesc[i];
+    unsigned char* q = p->arena + coff[i];
+    const size_t N = (size_t)cp[i].width * cp[i].height;
+    if (cdil) {
+      d.post = reinterpret_cast<float*>(q);
+      q += align256(N * 4);
+      const int s2 = std::min(cp[i].width, cp[i].height);
+      d.dil_wth = ((s2 < 360 ? 3 : (s2 < 720 ? 5 : 7)) - 1) / 2;
+    }
+    if (cpeaks) {
+      d.label = reinterpret_cast<int*>(q);
+      q += align256(N * 4);
+      d.count = reinterpret_cast<int*>(q);
+      d.peaks_tiles = cp[i].height / strips;
+      d.peaks_rows = strips * d.peaks_tiles;
+    }
+  }
+  PTRY(p, cudaMemcpy(p->coarse->ddesc, p->coarse->hdesc.data(), sizeof(BatchPair) * count, cudaMemcpyHostToDevice));
+  // finer-level descriptors
+  for (int lvl = 0; lvl < Lc; ++lvl) {
+    PLevel& L = p->lv[lvl];
+    const sgm_option_t& lo = L.opt;
+    L.hdesc.assign(count, BatchPair{});
+    for (int i = 0; i < count; ++i) {
+      const int w = pairs[i].width >> lvl, h = pairs[i].height >> lvl;
+      const size_t N = (size_t)w * h;
+      unsigned char* q = p->arena + off[lvl][i];
+      BatchPair& d = L.hdesc[i];
+      d.img_l = q; q += align256(N);
+      d.img_r = q; q += align256(N);
+      d.cs_l = q; q += align256(N * p->word);
+      d.cs_r = q; q += align256(N * p->word);
+      d.cost = q; q += align256(N * sgm::kLevelRange);
+      d.lr = q; q += align256(N * sgm::kLevelRange);
+      d.rl = q; q += align256(N * sgm::kLevelRange);
+      d.bt = q; q += align256(N * sgm::kLevelRange);
+      d.wta = reinterpret_cast<float*>(q); q += align256(N * 4);
+      d.post = nullptr;
+      float* post = reinterpret_cast<float*>(q); q += align256(N * 4);
+      d.out = reinterpret_cast<float*>(q); q += align256(N * 4);
+      d.init = reinterpret_cast<const int16_t*>(q); q += align256(N * 2);
+      if (lo.morphology_type == 2) {
+        d.post = post;
+        const int s2 = std::min(w, h);
+        d.dil_wth = ((s2 < 360 ? 3 : (s2 < 720 ? 5 : 7)) - 1) / 2;
+      }
+      if (lo.do_remove_peaks) {
+        d.label = reinterpret_cast<int*>(q); q += align256(N * 4);
+        d.count = reinterpret_cast<int*>(q);
+        d.peaks_tiles = h / strips;
+        d.peaks_rows = strips * d.peaks_tiles;
+      }
+      d.P.W = w; d.P.H = h; d.P.min_d = 0; d.P.x0 = 0;
+      d.P.p1 = (uint32_t)lo.p1; d.P.p2 = (uint32_t)lo.p2_init;
+      d.P.vstride = N * sgm::kLevelRange;
+      d.Q.uniqueness = lo.unique_threshold;
+      d.Q.tie_rule = ex.init_tie_rule;
+      d.Q.rows = (h / 4) * 4;
+      d.Q.dmax_excl = sgm::kLevelRange - 1;
+      d.Q.dstride = N;
+      d.nv = 1;
+      d.IP.W = w; d.IP.H = h; d.IP.x0 = 0;
+      d.IP.p1 = (uint32_t)lo.p1; d.IP.p1s = lo.p1; d.IP.p2s = lo.p2_init; d.IP.p2_div0 = ex.p2_div0;
+      d.IP.invalid_cost = lo.cs_type == 1 ? 0xFFu : sgm::kInvalidCost;
+      d.IP.vstride = N * sgm::kLevelRange;
+    }
+    PTRY(p, cudaMalloc(&L.ddesc, sizeof(BatchPair) * count));
+    PTRY(p, cudaMemcpy(L.ddesc, L.hdesc.data(), sizeof(BatchPair) * count, cudaMemcpyHostToDevice));
+  }
+  // item tables
+  std::vector<int> tab;
+  auto prefix_of = [&](const std::vector<int>& ids, auto per) {
+    const int at = (int)tab.size();
+    int acc = 0;
+    for (int id : ids) { tab.push_back(acc); acc += per(id); }
+    tab.push_back(acc);
+    return std::make_pair(at, acc);
+  };
+  std::vector<int> all(count);
+  for (int i = 0; i < count; ++i) all[i] = i;
+  auto tiles_of = [](int w, int h) { return ((w + 31) / 32) * ((h + 7) / 8); };
+  {
+    auto t = prefix_of(all, [&](int i) { return tiles_of(cp[i].width, cp[i].height); });
+    p->c_tile_prefix = t.first; p->c_tile_items = t.second;
+    auto r = prefix_of(all, [&](int i) { return cp[i].height; });
+    p->c_row_prefix = r.first; p->c_row_items = r.second;
+    auto x = prefix_of(all, [&](int i) { return cp[i].width * cp[i].height; });
+    p->c_pix_prefix = x.first; p->c_pix_items = x.second;
+  }
+  p->dec_prefix.assign(layers, 0);
+  p->dec_items.assign(layers, 0);
+  for (int lvl = 1; lvl < layers; ++lvl) {
+    auto r = prefix_of(all, [&](int i) { return pairs[i].height >> lvl; });
+    p->dec_prefix[lvl] = r.first; p->dec_items[lvl] = r.second;
+  }
+  int nq = 0;
+  for (int lvl = 0; lvl < Lc; ++lvl) {
+    PLevel& L = p->lv[lvl];
+    auto hw = [&](int i) { return std::make_pair(pairs[i].width >> lvl, pairs[i].height >> lvl); };
+    auto c = prefix_of(all, [&](int i) { return 2 * hw(i).second; });
+    L.census_prefix = c.first; L.census_items = c.second;
+    auto t = prefix_of(all, [&](int i) { return tiles_of(hw(i).first, hw(i).second); });
+    L.tile_prefix = t.first; L.tile_items = t.second;
+    auto r = prefix_of(all, [&](int i) { return hw(i).second; });
+    L.row_prefix = r.first; L.row_items = r.second;
+    auto x = prefix_of(all, [&](int i) { return hw(i).first * hw(i).second; });
+    L.pix_prefix = x.first; L.pix_items = x.second;
+    std::map<int, std::vector<int>> groups;
+    for (int i = 0; i < count; ++i) groups[width_class(hw(i).first)].push_back(i);
+    for (auto& gr : groups) {
+      PBucket k;
+      k.wclass = gr.first;
+      k.members = gr.second;
+      std::stable_sort(k.members.begin(), k.members.end(),
+                       [&](int a, int b2) { return hw(a).first * 2 + hw(a).second > hw(b2).first * 2 + hw(b2).second; });
+      k.ids = (int)tab.size();
+      tab.insert(tab.end(), k.members.begin(), k.members.end());
+      for (int i : k.members) k.max_w = std::max(k.max_w, hw(i).first);
+      auto cc = prefix_of(k.members, [&](int i) { return hw(i).second; });
+      k.cost_prefix = cc.first; k.cost_items = cc.second;
+      for (int li = 1; li < 5; ++li) {
+        const int per = 32 >> (li - 1);
+        auto rp = prefix_of(k.members, [&](int i) { return (2 * hw(i).second + per - 1) / per; });
+        k.rows_prefix[li] = rp.first; k.rows_items[li] = rp.second;
+        auto vp = prefix_of(k.members, [&](int i) { return (hw(i).first + per - 1) / per; });
+        k.cols_prefix[li] = vp.first; k.cols_items[li] = vp.second;
+      }
+      L.buckets.push_back(k);
+    }
+    L.queue0 = nq;
+    nq += 2 * (int)L.buckets.size();
+  }
+  PTRY(p, cudaMalloc(&p->dtab, tab.size() * sizeof(int)));
+  PTRY(p, cudaMemcpy(p->dtab, tab.data(), tab.size() * sizeof(int), cudaMemcpyHostToDevice));
+  p->nqueues = nq;
+  if (nq) PTRY(p, cudaMalloc(&p->queues, nq * sizeof(int)));
+  size_t nside = p->coarse->buckets.size();
+  int nev = 1 + (int)p->coarse->buckets.size();
+  for (auto& L : p->lv) {
+    nside = std::max(nside, L.buckets.size());
+    nev += 1 + (int)L.buckets.size();
+  }
+  for (size_t i = 0; i < nside; ++i) {
+    cudaStream_t t;
+    PTRY(p, cudaStreamCreateWithFlags(&t, cudaStreamNonBlocking));
+    p->side.push_back(t);
+  }
+  for (int i = 0; i < nev; ++i) {
+    cudaEvent_t e;
+    PTRY(p, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    p->ev.push_back(e);
+  }
+  // tune the 32-disparity levels on noise images with zero initial disparities, then capture
+  for (int lvl = 0; lvl < Lc; ++lvl)
+    for (int i = 0; i < count; ++i) {
+      const size_t N = (size_t)(pairs[i].width >> lvl) * (pairs[i].height >> lvl);
+      BatchPair& d = p->lv[lvl].hdesc[i];
+      kb_fill_noise<<<64, 256, 0, p->stream>>>(const_cast<uint8_t*>(d.img_l), N, 31u + 2u * i);
+      kb_fill_noise<<<64, 256, 0, p->stream>>>(const_cast<uint8_t*>(d.img_r), N, 32u + 2u * i);
+      PTRY(p, cudaMemsetAsync(const_cast<int16_t*>(d.init), 0, N * 2, p->stream));
+    }
+  PTRY(p, cudaGetLastError());
+  st = pyr_autotune(p);
+  if (st) return st;
+  st = pyr_capture(p);
+  if (st) return st;
+  PTRY(p, cudaStreamSynchronize(p->stream));
+  p->ready = true;
+  return SGM_OK;
+}
+
+int sgm_batch_pyr_pair_buffers(sgm_batch_pyr_t p, int32_t index, uint8_t** d_left, uint8_t** d_right,
+                               float** d_disp) {
+  if (!p || !p->ready) return p ? perr(p, SGM_ERR_STATE, "batch not initialised") : SGM_ERR_ARG;
+  if (index < 0 || index >= (int)p->pairs.size()) return perr(p, SGM_ERR_ARG, "pair index %d out of range", index);
+  const BatchPair& d = p->layers > 1 ? p->lv[0].hdesc[index] : p->coarse->hdesc[index];
+  if (d_left) *d_left = const_cast<uint8_t*>(d.img_l);
+  if (d_right) *d_right = const_cast<uint8_t*>(d.img_r);
+  if (d_disp) *d_disp = d.out;
+  return SGM_OK;
+}
+
+int sgm_batch_pyr_run(sgm_batch_pyr_t p, void* stream) {
+  if (!p || !p->ready) return p ? perr(p, SGM_ERR_STATE, "batch not initialised") : SGM_ERR_ARG;
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : p->stream;
+  const cudaError_t ce = cudaGraphLaunch(p->exec, s);
+  if (ce != cudaSuccess) return perr(p, SGM_ERR_CUDA, "graph launch failed: %s", cudaGetErrorString(ce));
+  return SGM_OK;
+}
+
+int sgm_batch_pyr_match(sgm_batch_pyr_t p, const uint8_t* const* left, const uint8_t* const* right,
+                        float* const* disp) {
+  if (!p || !p->ready) return p ? perr(p, SGM_ERR_STATE, "batch not initialised") : SGM_ERR_ARG;
+  if (!left || !right || !disp) return perr(p, SGM_ERR_ARG, "null pointer argument");
+  const int n = (int)p->pairs.size();
+  cudaStream_t s = p->stream;
+  for (int i = 0; i < n; ++i) {
+    if (!left[i] || !right[i] || !disp[i]) return perr(p, SGM_ERR_ARG, "pair %d: null buffer", i);
+    uint8_t *dl, *dr;
+    sgm_batch_pyr_pair_buffers(p, i, &dl, &dr, nullptr);
+    const size_t N = (size_t)p->pairs[i].width * p->pairs[i].height;
+    PTRY(p, cudaMemcpyAsync(dl, left[i], N, cudaMemcpyHostToDevice, s));
+    PTRY(p, cudaMemcpyAsync(dr, right[i], N, cudaMemcpyHostToDevice, s));
+  }
+  int st = sgm_batch_pyr_run(p, s);
+  if (st) return st;
+  for (int i = 0; i < n; ++i) {
+    float* dd;
+    sgm_batch_pyr_pair_buffers(p, i, nullptr, nullptr, &dd);
+    const size_t N = (size_t)p->pairs[i].width * p->pairs[i].height;
+    PTRY(p, cudaMemcpyAsync(disp[i], dd, N * sizeof(float), cudaMemcpyDeviceToHost, s));
+  }
+  PTRY(p, cudaStreamSynchronize(s));
+  return SGM_OK;
+}
+
+int sgm_batch_pyr_info(sgm_batch_pyr_t p, sgm_batch_info_t* info) {
+  if (!p || !info) return SGM_ERR_ARG;
+  if (!p->ready) return perr(p, SGM_ERR_STATE, "batch not initialised");
+  info->pairs = (int32_t)p->pairs.size();
+  info->buckets = (int32_t)p->coarse->buckets.size();
+  for (auto& L : p->lv) info->buckets += (int32_t)L.buckets.size();
+  info->arena_bytes = p->arena_bytes;
+  info->kernels_per_run = p->graph_kernels;
   return SGM_OK;
 }
 

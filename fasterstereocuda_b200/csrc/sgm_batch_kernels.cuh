@@ -1,0 +1,354 @@
+// Batched kernels: the single-pair device bodies (sgm_kernels.cuh, sgm_kernels3.cuh) applied to a
+// table of pairs. Every kernel maps its block or warp item to (pair, item within the pair) with a
+// prefix table over the pairs, so one launch covers pairs of different sizes; the scan kernels
+// are persistent and take warp items from an atomic queue.
+#pragma once
+#include "sgm_kernels3.cuh"
+
+namespace sgm {
+namespace batch {
+
+struct BatchPair {
+  const uint8_t* img_l;
+  const uint8_t* img_r;
+  void* cs_l;
+  void* cs_r;
+  uint8_t* cost;
+  uint8_t* lr;
+  uint8_t* rl;
+  uint8_t* bt;
+  float* wta;  // [2][H][W]
+  float* out;  // [H][W]
+  sgm::PlainParams P;
+  sgm::WtaParams Q;
+  int nv;  // views (2 with the LR check)
+  // pyramid levels (zero / null in single-level batches)
+  float* post;           // LR/median output when a dilation follows (the dilation writes `out`)
+  int* label;            // small-region removal: labels and component sizes [H][W]
+  int* count;
+  int peaks_tiles;       // strip height; strips cover rows [0, peaks_rows)
+  int peaks_rows;
+  int dil_wth;           // dilation half window
+  const int16_t* init;   // initial disparities of a 32-disparity level [H][W]
+  sgm::InitParams IP;    // that level's recurrence parameters
+};
+
+// Largest b in [0, n) with prefix[b] <= item (prefix ascending, prefix[0] = 0).
+__device__ __forceinline__ int find_pair(const int* __restrict__ prefix, int n, int item) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(prefix + mid) <= item) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <typename Word, int CSW, int CSH>
+__global__ void __launch_bounds__(256) kb_census(const BatchPair* __restrict__ pairs, const int* __restrict__ prefix,
+                                                 int n) {
+  const int item = blockIdx.x * blockDim.y + threadIdx.y;
+  if (item >= __ldg(prefix + n)) return;
+  const int b = find_pair(prefix, n, item);
+  const BatchPair d = pairs[b];
+  const int W = d.P.W, H = d.P.H;
+  const int local = item - __ldg(prefix + b);
+  const int view = local / H;
+  const int y = local - view * H;
+  const uint8_t* img = view ? d.img_r : d.img_l;
+  Word* out = static_cast<Word*>(view ? d.cs_r : d.cs_l) + (size_t)y * W;
+  for (int x = threadIdx.x; x < W; x += 32) out[x] = sgm::census_value<Word, CSW, CSH>(img, x, y, W, H, view == 1);
+}
+
+template <int K, typename Word>
+__global__ void __launch_bounds__(256) kb_rows(const BatchPair* __restrict__ pairs, const int* __restrict__ ids,
+                                               const int* __restrict__ prefix, int n, int* __restrict__ queue) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  unsigned char* base = smem_raw + (size_t)threadIdx.y * sgm::hpaths2_warp_smem<K, Word>();
+  const int total = __ldg(prefix + n);
+  for (;;) {
+    int item = 0;
+    if (threadIdx.x == 0) item = atomicAdd(queue, 1);
+    item = __shfl_sync(sgm::kFull, item, 0);
+    if (item >= total) break;
+    const int b = find_pair(prefix, n, item);
+    const BatchPair d = pairs[__ldg(ids + b)];
+    const int local = item - __ldg(prefix + b);
+    const int per_view = 2 * d.P.H;
+    const int view = local / per_view;
+    const int rem = local - view * per_view;
+    sgm::hpaths2_warp<K, Word>(static_cast<const Word*>(d.cs_l), static_cast<const Word*>(d.cs_r), d.cost, d.lr,
+                               d.rl, d.P, view, rem >> 1, rem & 1, base);
+  }
+}
+
+template <int K, int PF>
+__global__ void __launch_bounds__(256) kb_cols(const BatchPair* __restrict__ pairs, const int* __restrict__ ids,
+                                               const int* __restrict__ prefix, int n, int* __restrict__ queue) {
+  const int total = __ldg(prefix + n);
+  for (;;) {
+    int item = 0;
+    if (threadIdx.x == 0) item = atomicAdd(queue, 1);
+    item = __shfl_sync(sgm::kFull, item, 0);
+    if (item >= total) break;
+    const int b = find_pair(prefix, n, item);
+    const BatchPair d = pairs[__ldg(ids + b)];
+    const int local = item - __ldg(prefix + b);
+    const int view = local / d.P.W;
+    const int x = local - view * d.P.W;
+    if constexpr (PF == 0)
+      sgm::vpaths1_warp<K>(d.cost, d.lr, d.rl, d.bt, d.wta, d.P, d.Q, view, x);
+    else
+      sgm::vpaths2_warp<K, PF>(d.cost, d.lr, d.rl, d.bt, d.wta, d.P, d.Q, view, x, nullptr);
+  }
+}
+
+template <int K, typename Word>
+__global__ void __launch_bounds__(128) kb_cost3(const BatchPair* __restrict__ pairs, const int* __restrict__ ids,
+                                                const int* __restrict__ prefix, int n) {
+  __shared__ Word win[128 + 32 * K];
+  const int item = blockIdx.x;
+  const int b = find_pair(prefix, n, item);
+  const BatchPair d = pairs[__ldg(ids + b)];
+  const int local = item - __ldg(prefix + b);
+  const int segs = (d.P.W + 127) / 128;
+  const int row = local / segs;  // view * H + y
+  const int seg = local - row * segs;
+  const int view = row / d.P.H;
+  sgm::cost3_block<K, Word>(static_cast<const Word*>(d.cs_l), static_cast<const Word*>(d.cs_r), d.cost, d.P, view,
+                            row - view * d.P.H, seg * 128, win);
+}
+
+// Items of 32/G scanlines (pair, first scanline); lanes beyond the pair's scanlines idle.
+template <int K, int G, int PF>
+__global__ void __launch_bounds__(256) kb_rows3(const BatchPair* __restrict__ pairs, const int* __restrict__ ids,
+                                                const int* __restrict__ prefix, int n, int* __restrict__ queue) {
+  constexpr int S = 32 / G;
+  const int lane = threadIdx.x;
+  const int total = __ldg(prefix + n);
+  for (;;) {
+    int item = 0;
+    if (lane == 0) item = atomicAdd(queue, 1);
+    item = __shfl_sync(sgm::kFull, item, 0);
+    if (item >= total) break;
+    const int b = find_pair(prefix, n, item);
+    const BatchPair d = pairs[__ldg(ids + b)];
+    const int local = item - __ldg(prefix + b);
+    sgm::hpaths3_lane<K, G, PF>(d.cost, d.lr, d.rl, d.P, d.nv, local * S + lane / G, lane % G);
+  }
+}
+
+template <int K, int G, int PF>
+__global__ void __launch_bounds__(256) kb_cols3(const BatchPair* __restrict__ pairs, const int* __restrict__ ids,
+                                                const int* __restrict__ prefix, int n, int* __restrict__ queue) {
+  constexpr int S = 32 / G;
+  extern __shared__ uint32_t s_sum[];
+  const int lane = threadIdx.x;
+  uint32_t* colS = s_sum + ((size_t)threadIdx.y * S + lane / G) * (16 * K + 1);
+  const int total = __ldg(prefix + n);
+  for (;;) {
+    int item = 0;
+    if (lane == 0) item = atomicAdd(queue, 1);
+    item = __shfl_sync(sgm::kFull, item, 0);
+    if (item >= total) break;
+    const int b = find_pair(prefix, n, item);
+    const BatchPair d = pairs[__ldg(ids + b)];
+    const int local = item - __ldg(prefix + b);
+    const int per_view = (d.P.W + S - 1) / S;
+    const int view = local / per_view;
+    const int grp = local - view * per_view;
+    sgm::vpaths3_lane<K, G, PF>(d.cost, d.lr, d.rl, d.bt, d.wta, d.P, d.Q, view, grp * S + lane / G, lane % G, colS);
+    __syncwarp();
+  }
+}
+
+template <bool LR, bool MED>
+__global__ void __launch_bounds__(256) kb_lr_median(const BatchPair* __restrict__ pairs,
+                                                    const int* __restrict__ prefix, int n, float thr) {
+  __shared__ float tile[10][34];
+  const int item = blockIdx.x;
+  const int b = find_pair(prefix, n, item);
+  const BatchPair d = pairs[b];
+  const int local = item - __ldg(prefix + b);
+  const int tiles_x = (d.P.W + 31) / 32;
+  const int ty = local / tiles_x;
+  const int tx = local - ty * tiles_x;
+  sgm::lr_median_tile<LR, MED>(d.wta, d.wta + d.Q.dstride, nullptr, d.post ? d.post : d.out, d.P.W, d.P.H, thr,
+                               tx * 32, ty * 8, tile);
+}
+
+// Deterministic noise for the autotuner's timing runs (overwritten by the caller's images).
+static __global__ void kb_fill_noise(uint8_t* p, size_t n, uint32_t seed) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    uint32_t h = (uint32_t)i * 2654435761u ^ seed;
+    h ^= h >> 15;
+    h *= 2246822519u;
+    h ^= h >> 13;
+    p[i] = (uint8_t)(h >> 24);
+  }
+}
+
+
+// ------------------------------------------------------------------ pyramid levels
+// Level images sampled from the full-resolution images (pair order shared by lv and l0); one
+// block per level row.
+static __global__ void kb_decimate(const BatchPair* __restrict__ lv, const BatchPair* __restrict__ l0,
+                                   const int* __restrict__ rprefix, int n, int shift) {
+  const int item = blockIdx.x;
+  const int b = find_pair(rprefix, n, item);
+  const int y = item - __ldg(rprefix + b);
+  const int w = lv[b].P.W, W0 = l0[b].P.W;
+  uint8_t* dl = const_cast<uint8_t*>(lv[b].img_l);
+  uint8_t* dr = const_cast<uint8_t*>(lv[b].img_r);
+  const uint8_t* sl = l0[b].img_l;
+  const uint8_t* sr = l0[b].img_r;
+  for (int x = threadIdx.x; x < w; x += blockDim.x) sgm::decimate_px(sl, sr, dl, dr, W0, w, shift, x, y);
+}
+
+// Dilation post -> out, one block per 32x8 tile.
+static __global__ void __launch_bounds__(256) kb_dilation(const BatchPair* __restrict__ pairs,
+                                                          const int* __restrict__ tprefix, int n) {
+  const int item = blockIdx.x;
+  const int b = find_pair(tprefix, n, item);
+  const BatchPair d = pairs[b];
+  const int local = item - __ldg(tprefix + b);
+  const int tiles_x = (d.P.W + 31) / 32;
+  const int ty = local / tiles_x, tx = local - ty * tiles_x;
+  const int x = tx * 32 + threadIdx.x, y = ty * 8 + threadIdx.y;
+  if (x < d.P.W && y < d.P.H) sgm::dilation_px<float>(d.post, d.out, d.P.W, d.P.H, d.dil_wth, x, y);
+}
+
+// Small-region removal on `out`: row runs (one warp per row), vertical unions, sizes, filter.
+static __global__ void __launch_bounds__(256) kb_cc_rows(const BatchPair* __restrict__ pairs,
+                                                         const int* __restrict__ rprefix, int n, int abs_mode) {
+  const int item = blockIdx.x * blockDim.y + threadIdx.y;
+  if (item >= __ldg(rprefix + n)) return;
+  const int b = find_pair(rprefix, n, item);
+  const BatchPair d = pairs[b];
+  sgm::cc_rows_warp(d.out, d.label, d.count, d.P.W, d.P.H, d.peaks_rows, abs_mode, item - __ldg(rprefix + b));
+}
+
+static __global__ void __launch_bounds__(256) kb_cc_vert(const BatchPair* __restrict__ pairs,
+                                                         const int* __restrict__ pprefix, int n, int abs_mode) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= __ldg(pprefix + n)) return;
+  const int b = find_pair(pprefix, n, i);
+  const BatchPair d = pairs[b];
+  if (d.peaks_tiles > 1)
+    sgm::cc_vert_px(d.out, d.label, d.P.W, d.P.H, d.peaks_tiles, d.peaks_rows, abs_mode, i - __ldg(pprefix + b));
+}
+
+static __global__ void __launch_bounds__(256) kb_cc_count(const BatchPair* __restrict__ pairs,
+                                                          const int* __restrict__ pprefix, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= __ldg(pprefix + n)) return;
+  const int b = find_pair(pprefix, n, i);
+  sgm::cc_count_px(pairs[b].label, pairs[b].count, i - __ldg(pprefix + b));
+}
+
+static __global__ void __launch_bounds__(256) kb_cc_filter(const BatchPair* __restrict__ pairs,
+                                                           const int* __restrict__ pprefix, int n, float ratio) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= __ldg(pprefix + n)) return;
+  const int b = find_pair(pprefix, n, i);
+  const BatchPair d = pairs[b];
+  if (d.peaks_tiles > 0) sgm::cc_filter_px(d.out, d.label, d.count, d.P.W, d.peaks_tiles, ratio, i - __ldg(pprefix + b));
+}
+
+// Initial disparities of the finer level `next` from the coarser level's `out`.
+static __global__ void __launch_bounds__(256) kb_init_next(const BatchPair* __restrict__ next,
+                                                           const BatchPair* __restrict__ cur,
+                                                           const int* __restrict__ pprefix, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= __ldg(pprefix + n)) return;
+  const int b = find_pair(pprefix, n, i);
+  const int local = i - __ldg(pprefix + b);
+  const int w = next[b].P.W, h = next[b].P.H;
+  const int y = local / w;
+  sgm::init_next_px(cur[b].out, (long)cur[b].P.W * cur[b].P.H, const_cast<int16_t*>(next[b].init), w, h, local - y * w,
+                    y);
+}
+
+// Cost volume of a 32-disparity level: one block per (pair, view, row); `ids` gives the pair order.
+template <typename Word>
+__global__ void __launch_bounds__(256) kb_cost3_init(const BatchPair* __restrict__ pairs, const int* __restrict__ ids,
+                                                     const int* __restrict__ rprefix, int n) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int item = blockIdx.x;
+  const int b = find_pair(rprefix, n, item);
+  const BatchPair d = pairs[__ldg(ids + b)];
+  const int local = item - __ldg(rprefix + b);
+  const int view = local / d.P.H;
+  sgm::cost3_init_row<Word>(static_cast<const Word*>(d.cs_l), static_cast<const Word*>(d.cs_r), d.init, d.init, d.cost,
+                            d.IP, local - view * d.P.H, view, reinterpret_cast<Word*>(smem_raw));
+}
+
+// Shared-memory set-up of the 32-disparity scan kernels (penalties are the same for every pair
+// of a level): the P2' table and the padding of every scanline row.
+template <int G>
+__device__ __forceinline__ void init_scan_smem(uint32_t* p2tab, uint32_t* rows, const sgm::InitParams& P) {
+  sgm::fill_p2_table(p2tab, P, threadIdx.x, blockDim.x);
+  uint32_t* row = rows + (threadIdx.x / G) * sgm::kIRow;
+  const uint32_t pad = sgm::kInvalidCost - P.p1;
+  for (int k = threadIdx.x % G; k < sgm::kIPad; k += G) {
+    row[k] = pad;
+    row[sgm::kIPad + 32 + k] = pad;
+  }
+  __syncthreads();
+}
+
+// Persistent scans of 32-disparity levels, 128-thread blocks; items of 32/G scanlines / columns.
+template <int G, int PF>
+__global__ void __launch_bounds__(128) kb_rows3_init(const BatchPair* __restrict__ pairs, const int* __restrict__ ids,
+                                                     const int* __restrict__ prefix, int n, int* __restrict__ queue) {
+  constexpr int S = 32 / G;
+  __shared__ uint32_t p2tab[sgm::kP2Tab];
+  __shared__ uint32_t rows[(128 / G) * sgm::kIRow];
+  init_scan_smem<G>(p2tab, rows, pairs[__ldg(ids)].IP);
+  uint32_t* row = rows + (threadIdx.x / G) * sgm::kIRow;
+  const int lane = threadIdx.x & 31;
+  const int total = __ldg(prefix + n);
+  for (;;) {
+    int item = 0;
+    if (lane == 0) item = atomicAdd(queue, 1);
+    item = __shfl_sync(sgm::kFull, item, 0);
+    if (item >= total) break;
+    const int b = find_pair(prefix, n, item);
+    const BatchPair d = pairs[__ldg(ids + b)];
+    const int local = item - __ldg(prefix + b);
+    sgm::hpaths3_init_lane<G, PF>(d.cost, d.init, d.init, d.lr, d.rl, d.IP, d.nv, local * S + lane / G, lane % G, row,
+                                  p2tab);
+  }
+}
+
+template <int G, int PF>
+__global__ void __launch_bounds__(128) kb_cols3_init(const BatchPair* __restrict__ pairs, const int* __restrict__ ids,
+                                                     const int* __restrict__ prefix, int n, int* __restrict__ queue) {
+  constexpr int S = 32 / G;
+  __shared__ uint32_t p2tab[sgm::kP2Tab];
+  __shared__ uint32_t rows[(128 / G) * sgm::kIRow];
+  __shared__ uint32_t sums[(128 / G) * 33];
+  init_scan_smem<G>(p2tab, rows, pairs[__ldg(ids)].IP);
+  uint32_t* row = rows + (threadIdx.x / G) * sgm::kIRow;
+  uint32_t* colS = sums + (threadIdx.x / G) * 33;
+  const int lane = threadIdx.x & 31;
+  const int total = __ldg(prefix + n);
+  for (;;) {
+    int item = 0;
+    if (lane == 0) item = atomicAdd(queue, 1);
+    item = __shfl_sync(sgm::kFull, item, 0);
+    if (item >= total) break;
+    const int b = find_pair(prefix, n, item);
+    const BatchPair d = pairs[__ldg(ids + b)];
+    const int local = item - __ldg(prefix + b);
+    const int per_view = (d.P.W + S - 1) / S;
+    const int view = local / per_view;
+    const int grp = local - view * per_view;
+    sgm::vpaths3_init_lane<G, PF>(d.cost, d.lr, d.rl, d.init, d.init, d.bt, d.wta, d.IP, d.Q, view, grp * S + lane / G,
+                                  lane % G, row, colS, p2tab);
+    __syncwarp();
+  }
+}
+
+}  // namespace batch
+}  // namespace sgm

@@ -1208,11 +1208,8 @@ __global__ void __launch_bounds__(256) k_lr_median(const float* __restrict__ dl,
 
 // Dilation of INVALID pixels (reference Kernel_Dilation, cusgm_df.cu:197-222).
 template <typename T>
-__global__ void __launch_bounds__(256) k_dilation(const T* __restrict__ in, T* __restrict__ out, int W, int H,
-                                                  int wth) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  if (x >= W || y >= H) return;
+__device__ __forceinline__ void dilation_px(const T* __restrict__ in, T* __restrict__ out, int W, int H, int wth,
+                                            int x, int y) {
   T v = in[(size_t)y * W + x];
   if ((float)v == kInvalidFloat || (float)v == (float)kInvalidShort) {
     if (x > wth && x < W - wth && y > wth && y < H - wth) {
@@ -1224,6 +1221,15 @@ __global__ void __launch_bounds__(256) k_dilation(const T* __restrict__ in, T* _
     }
   }
   out[(size_t)y * W + x] = v;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_dilation(const T* __restrict__ in, T* __restrict__ out, int W, int H,
+                                                  int wth) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= W || y >= H) return;
+  dilation_px<T>(in, out, W, H, wth, x, y);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1250,11 +1256,9 @@ __device__ __forceinline__ int cc_find(const int* label, int p) {
 // Row pass: label[i] = first pixel of i's horizontal run of connected pixels (its provisional
 // root), -1 for INVALID pixels and rows >= `rows`; zeroes count. One warp per row, 32 pixels per
 // step: run starts by ballot, the run of the previous step carried across.
-static __global__ void k_cc_rows(const float* __restrict__ disp, int* __restrict__ label, int* __restrict__ count,
-                                 int W, int H, int rows, int abs_mode) {
-  const int y = blockIdx.x * blockDim.y + threadIdx.y;
-  if (y >= H) return;
-  const int lane = threadIdx.x;
+__device__ __forceinline__ void cc_rows_warp(const float* __restrict__ disp, int* __restrict__ label,
+                                             int* __restrict__ count, int W, int H, int rows, int abs_mode, int y) {
+  const int lane = threadIdx.x & 31;
   const float* drow = disp + (size_t)y * W;
   int* lrow = label + (size_t)y * W;
   int* crow = count + (size_t)y * W;
@@ -1286,12 +1290,17 @@ static __global__ void k_cc_rows(const float* __restrict__ disp, int* __restrict
   }
 }
 
+static __global__ void k_cc_rows(const float* __restrict__ disp, int* __restrict__ label, int* __restrict__ count,
+                                 int W, int H, int rows, int abs_mode) {
+  const int y = blockIdx.x * blockDim.y + threadIdx.y;
+  if (y >= H) return;
+  cc_rows_warp(disp, label, count, W, H, rows, abs_mode, y);
+}
+
 // Vertical pass: unions pixel i with the pixel below it (same strip) when both are valid and
 // adjacent; roots are the smallest pixel index (atomicMin hooks the larger root).
-static __global__ void k_cc_vert(const float* __restrict__ disp, int* label, int W, int H, int tiles, int rows,
-                                 int abs_mode) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= W * H) return;
+__device__ __forceinline__ void cc_vert_px(const float* __restrict__ disp, int* label, int W, int H, int tiles,
+                                           int rows, int abs_mode, int i) {
   const int y = i / W;
   if (y + 1 >= rows || (y + 1) / tiles != y / tiles) return;
   const int q = i + W;
@@ -1309,46 +1318,65 @@ static __global__ void k_cc_vert(const float* __restrict__ disp, int* label, int
   }
 }
 
-static __global__ void k_cc_count(int* label, int* __restrict__ count, int n) {
+static __global__ void k_cc_vert(const float* __restrict__ disp, int* label, int W, int H, int tiles, int rows,
+                                 int abs_mode) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n || label[i] < 0) return;
+  if (i >= W * H) return;
+  cc_vert_px(disp, label, W, H, tiles, rows, abs_mode, i);
+}
+
+__device__ __forceinline__ void cc_count_px(int* label, int* __restrict__ count, int i) {
+  if (label[i] < 0) return;
   const int r = cc_find(label, i);
   label[i] = r;
   atomicAdd(&count[r], 1);
 }
 
-static __global__ void k_cc_filter(float* __restrict__ disp, const int* __restrict__ label, const int* __restrict__ count,
-                            int W, int H, int tiles, float ratio) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= W * H || label[i] < 0) return;
-  // every processed strip has exactly `tiles` rows, so the threshold is the same for all of them
+// every processed strip has exactly `tiles` rows, so the threshold is the same for all of them
+__device__ __forceinline__ void cc_filter_px(float* __restrict__ disp, const int* __restrict__ label,
+                                             const int* __restrict__ count, int W, int tiles, float ratio, int i) {
+  if (label[i] < 0) return;
   const int threshold = (int)__fmul_rn((float)(W * tiles), ratio);
   if (count[label[i]] < threshold) disp[i] = kInvalidFloat;
+}
+
+static __global__ void k_cc_count(int* label, int* __restrict__ count, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  cc_count_px(label, count, i);
+}
+static __global__ void k_cc_filter(float* __restrict__ disp, const int* __restrict__ label, const int* __restrict__ count,
+                                   int W, int H, int tiles, float ratio) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= W * H) return;
+  cc_filter_px(disp, label, count, W, tiles, ratio, i);
 }
 
 // ---------------------------------------------------------------------------------------------
 // Pyramid helpers (reference FasterStereoCuda.cpp:114-166, cusgm_util.cu:47-59).
 // ---------------------------------------------------------------------------------------------
 // Level image = full-resolution image sampled at (x << shift, y << shift); both views.
-static __global__ void k_decimate(const uint8_t* __restrict__ full_l, const uint8_t* __restrict__ full_r,
-                           uint8_t* __restrict__ lvl_l, uint8_t* __restrict__ lvl_r, int W0, int w, int h,
-                           int shift) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y;
-  if (x >= w || y >= h) return;
+__device__ __forceinline__ void decimate_px(const uint8_t* __restrict__ full_l, const uint8_t* __restrict__ full_r,
+                                            uint8_t* __restrict__ lvl_l, uint8_t* __restrict__ lvl_r, int W0, int w,
+                                            int shift, int x, int y) {
   const size_t src = ((size_t)y << shift) * W0 + ((size_t)x << shift);
   lvl_l[(size_t)y * w + x] = full_l[src];
   lvl_r[(size_t)y * w + x] = full_r[src];
+}
+static __global__ void k_decimate(const uint8_t* __restrict__ full_l, const uint8_t* __restrict__ full_r,
+                                  uint8_t* __restrict__ lvl_l, uint8_t* __restrict__ lvl_r, int W0, int w, int h,
+                                  int shift) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= w || y >= h) return;
+  decimate_px(full_l, full_r, lvl_l, lvl_r, W0, w, shift, x, y);
 }
 
 // Initial disparity of the next finer level: even rows (except the last) from cur at the flat
 // index (y/2)*(width/2) + x/2 (INVALID past the end of cur); odd rows and the last row copy the
 // row above.
-static __global__ void k_init_next_level(const float* __restrict__ cur, long ncur, int16_t* __restrict__ next, int width,
-                                  int height) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y;
-  if (x >= width || y >= height) return;
+__device__ __forceinline__ void init_next_px(const float* __restrict__ cur, long ncur, int16_t* __restrict__ next,
+                                             int width, int height, int x, int y) {
   int ys = y;
   if (y % 2 == 1 || y == height - 1) ys = y - 1;
   if (ys % 2 == 1) ys -= 1;  // last row with an even index copies an odd row, whose source is one more up
@@ -1360,6 +1388,13 @@ static __global__ void k_init_next_level(const float* __restrict__ cur, long ncu
   const float d = idx < ncur ? cur[idx] : kInvalidFloat;
   next[(size_t)y * width + x] =
       d != kInvalidFloat ? (int16_t)(int)__fsub_rn(__fmul_rn(2.0f, d), (float)(kLevelRange >> 1)) : kInvalidShort;
+}
+static __global__ void k_init_next_level(const float* __restrict__ cur, long ncur, int16_t* __restrict__ next, int width,
+                                         int height) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= width || y >= height) return;
+  init_next_px(cur, ncur, next, width, height, x, y);
 }
 
 // Right-view initial disparities: cleared to INVALID, then a scatter in which the largest

@@ -534,14 +534,12 @@ __device__ __forceinline__ uint32_t init_step32(uint32_t (&L)[ND], const uint32_
 // view 0: pos = x - d - base, C = (popc(own ^ oth[pos]) + CostAdjust(d)) & 0xFF for 0 < pos < W,
 // else the invalid cost; view 1: pos = x + d + base, partner oth[pos] for 0 < pos < W else oth[0].
 // One CTA per (row, view); the partner row's census words in shared memory (W words).
+// Row y of view `view` by one block (every thread calls it); oth_s: W words of shared memory.
 template <typename Word>
-__global__ void __launch_bounds__(256) k_cost3_init(const Word* __restrict__ cs_l, const Word* __restrict__ cs_r,
-                                                    const int16_t* __restrict__ init_l,
-                                                    const int16_t* __restrict__ init_r, uint8_t* __restrict__ cost,
-                                                    InitParams P) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  Word* oth_s = reinterpret_cast<Word*>(smem_raw);
-  const int y = blockIdx.x, view = blockIdx.y;
+__device__ __forceinline__ void cost3_init_row(const Word* __restrict__ cs_l, const Word* __restrict__ cs_r,
+                                               const int16_t* __restrict__ init_l, const int16_t* __restrict__ init_r,
+                                               uint8_t* __restrict__ cost, const InitParams& P, int y, int view,
+                                               Word* oth_s) {
   const int W = P.W;
   const Word* own = (view == 0 ? cs_l : cs_r) + (size_t)y * W;
   const Word* oth = (view == 0 ? cs_r : cs_l) + (size_t)y * W;
@@ -575,6 +573,15 @@ __global__ void __launch_bounds__(256) k_cost3_init(const Word* __restrict__ cs_
     o[0] = make_uint4(q[0], q[1], q[2], q[3]);
     o[1] = make_uint4(q[4], q[5], q[6], q[7]);
   }
+}
+
+template <typename Word>
+__global__ void __launch_bounds__(256) k_cost3_init(const Word* __restrict__ cs_l, const Word* __restrict__ cs_r,
+                                                    const int16_t* __restrict__ init_l,
+                                                    const int16_t* __restrict__ init_r, uint8_t* __restrict__ cost,
+                                                    InitParams P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cost3_init_row<Word>(cs_l, cs_r, init_l, init_r, cost, P, blockIdx.x, blockIdx.y, reinterpret_cast<Word*>(smem_raw));
 }
 
 // Horizontal paths of an initial-disparity level, G lanes per scanline (view, dir, y) with the

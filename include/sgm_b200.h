@@ -311,6 +311,31 @@ SGM_API int64_t sgm_pyr_kernel_launches(sgm_pyr_handle_t h);
  * after sgm_pyr_init. */
 SGM_API int sgm_pyr_set_tuning(sgm_pyr_handle_t h, int32_t level, const sgm_tuning_t* t);
 
+/* ---------------- batched pyramids ---------------- */
+
+/* No counterpart in the reference. Batched pyramids: every pair's FasterStereoCuda::Match
+ * (FasterStereoCuda.cpp:408-529: decimation, coarsest level with LR / dilation / small-region
+ * removal per SetSgmParameters, then 32-disparity levels driven by the coarser map) for many
+ * pairs of different sizes in one CUDA graph. pairs[i]: full-resolution width, height,
+ * min_disparity and disp_range = max_disp - min_disp; option: num_layers, do_lr_check,
+ * do_rm_peaks (do_smooth unsupported; its width/height/disparity fields are ignored); override
+ * and ext as for sgm_pyr_init (ext may be NULL). Each pair's result is bit-identical to
+ * sgm_pyr_match_device on that pair. */
+typedef struct sgm_batch_pyr* sgm_batch_pyr_t;
+SGM_API int sgm_batch_pyr_create(sgm_batch_pyr_t* out);
+SGM_API int sgm_batch_pyr_destroy(sgm_batch_pyr_t p);
+SGM_API const char* sgm_batch_pyr_last_error(sgm_batch_pyr_t p);
+SGM_API int sgm_batch_pyr_init(sgm_batch_pyr_t p, const sgm_batch_pair_t* pairs, int32_t count,
+                               const sgm_pyr_option1_t* option, const sgm_level_override_t* level_override,
+                               const sgm_ext_options_t* ext);
+/* Full-resolution input images and final disparity of pair `index` (device, dense). */
+SGM_API int sgm_batch_pyr_pair_buffers(sgm_batch_pyr_t p, int32_t index, uint8_t** d_left, uint8_t** d_right,
+                                       float** d_disp);
+SGM_API int sgm_batch_pyr_run(sgm_batch_pyr_t p, void* stream);
+SGM_API int sgm_batch_pyr_match(sgm_batch_pyr_t p, const uint8_t* const* left, const uint8_t* const* right,
+                                float* const* disp);
+SGM_API int sgm_batch_pyr_info(sgm_batch_pyr_t p, sgm_batch_info_t* info);
+
 #ifdef __cplusplus
 }
 #endif

@@ -130,3 +130,47 @@ def test_batch_of_uneven_full_size_pairs_equals_per_pair_engine(engine_lib):
     buckets = b.buckets()
     assert sum(k["pairs"] for k in buckets) == 12
     assert all(k["rows_ctas"] > 0 and k["cols_ctas"] > 0 for k in buckets)
+
+
+PYR_PAIRS = [(640, 360, 0, 64), (450, 375, 0, 64), (1242, 375, 0, 64), (800, 600, 0, 64), (320, 256, 0, 64)]
+
+
+def test_batch_pyramid_rejects_before_any_device_call(engine_lib):
+    import fasterstereocuda_b200 as fsc
+    b = fsc.StereoBatchPyramid()
+    opt = fsc.StereoOption1(num_layers=3, do_lr_check=True, do_rm_peaks=True)
+    assert not b.Init([(64, 24, 0, 64)], opt) and b.status == -1 and "too many layers" in b.last_error()
+    opt.do_smooth = True
+    assert not b.Init([(640, 360, 0, 64)], opt) and b.status == -4
+    assert not b.Init([], fsc.StereoOption1(num_layers=3)) and b.status == -1
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("layers,override", [(3, True), (3, False), (2, True), (1, True)])
+def test_batch_pyramid_equals_per_pair_pyramid(engine_lib, oracle_mod, layers, override):
+    import fasterstereocuda_b200 as fsc
+    O = oracle_mod
+    opt = fsc.StereoOption1(num_layers=layers, do_lr_check=True, do_rm_peaks=True)
+    ov = fsc.LevelOverride(1, 10, 150) if override else None
+    ext = fsc.ExtOptions(peaks_strips=STRIPS)
+    b = fsc.StereoBatchPyramid()
+    assert b.Init(PYR_PAIRS, opt, ov, ext), b.last_error()
+    imgs = [scenes.kitti_like(500 + i, w, h)[:2] for i, (w, h, _, _) in enumerate(PYR_PAIRS)]
+    outs = [np.full((h, w), 7.0, np.float32) for (w, h, _, _) in PYR_PAIRS]
+    for rnd in range(2):  # two graph launches in a row
+        assert b.Match([L for L, _ in imgs], [R for _, R in imgs], outs), b.last_error()
+        for i, ((w, h, mn, mx), (L, R)) in enumerate(zip(PYR_PAIRS, imgs)):
+            p = fsc.FasterStereoCuda()
+            assert p.Init(fsc.StereoOption1(width=w, height=h, min_disp=mn, max_disp=mx, num_layers=layers,
+                                            do_lr_check=True, do_rm_peaks=True), ov, ext), p.last_error()
+            exp = np.empty((h, w), np.float32)
+            assert p.Match(L, R, exp)
+            assert np.array_equal(outs[i].view(np.uint32), exp.view(np.uint32)), (rnd, i, int((outs[i] != exp).sum()))
+    # one pair against the oracle as well
+    w, h, mn, mx = PYR_PAIRS[1]
+    pc = O.PyrConfig(width=w, height=h, min_disp=mn, max_disp=mx, num_layers=layers, override_enable=int(override),
+                     cs_type=1 if override else 0, p1=10 if override else 8, p2=150 if override else 32,
+                     peaks_strips=STRIPS)
+    ref = O.pyr_match(pc, *imgs[1])
+    assert np.array_equal(outs[1].view(np.uint32), ref.view(np.uint32))
+    assert b.info()["pairs"] == len(PYR_PAIRS)
