@@ -162,6 +162,16 @@ struct sgm_engine {
   int tune_row_lanes = 0;   // variant 3: lanes per scanline (0: default)
   int tune_col_lanes = 0;
   bool bt_stored = true;    // the last match wrote the bottom->top volume to global memory
+  // img[0], img[1] -> out captured as a CUDA graph after a first direct run (matches without
+  // initial disparities or a right map); later matches copy in, launch it, copy out.
+  cudaGraphExec_t gexec = nullptr;
+  int direct_runs = 0;
+  int64_t graph_launches = 0;
+  void drop_graph() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    gexec = nullptr;
+    direct_runs = 0;
+  }
 
   int nviews() const { return opt.do_lr_check ? 2 : 1; }
   size_t npix() const { return (size_t)W * H; }
@@ -169,6 +179,7 @@ struct sgm_engine {
   int census_bytes() const { return opt.cs_type == 1 ? 8 : 4; }
 
   void free_all() {
+    drop_graph();
     for (int i = 0; i < 2; ++i) {
       dfree(img[i]);
       dfree(init[i]);
@@ -258,7 +269,7 @@ int engine_init(sgm_engine* e, int W, int H, int M, int D, const sgm_option_t* o
   e->print_log = log;
   SGM_CUDA_TRY(e, cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
   const size_t N = e->npix();
-  const size_t V = e->vol() * 2;  // room for both views whatever the options
+  const size_t V = e->vol() * e->nviews();  // the right view's volumes only with the LR check
   for (int i = 0; i < 2; ++i) {
     SGM_CUDA_TRY(e, dalloc(&e->img[i], N));
     SGM_CUDA_TRY(e, cudaMalloc(&e->cs[i], N * 8));
@@ -679,6 +690,51 @@ int engine_enqueue(sgm_engine* e, const uint8_t* dl_img, const uint8_t* dr_img, 
 }  // namespace
 
 namespace {
+// A match without initial disparities or a right map on stream s (0: the matcher's own). Without
+// profiling, the second and later calls replay a CUDA graph of the match on the matcher's own
+// buffers, with device-to-device copies around it when the caller's buffers differ.
+int engine_run(sgm_engine* e, const uint8_t* dl, const uint8_t* dr, float* dout, cudaStream_t s) {
+  if (!s) s = e->stream;
+  if (g_prof.on) {
+    e->drop_graph();
+    return engine_enqueue(e, dl, dr, nullptr, dout, nullptr, s);
+  }
+  if (!e->gexec && e->direct_runs == 0) {
+    e->direct_runs++;
+    return engine_enqueue(e, dl, dr, nullptr, dout, nullptr, s);
+  }
+  const size_t N = e->npix();
+  if (!e->gexec) {
+    if (cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      set_error(&e->err, "graph capture could not start");
+      return SGM_ERR_CUDA;
+    }
+    e->launches = 0;
+    const int st = engine_enqueue(e, e->img[0], e->img[1], nullptr, e->out, nullptr, e->stream);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
+    if (st || ce != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      if (!st) set_error(&e->err, "graph capture failed: %s", cudaGetErrorString(ce));
+      return st ? st : SGM_ERR_CUDA;
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&e->gexec, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) {
+      e->gexec = nullptr;
+      set_error(&e->err, "graph instantiation failed: %s", cudaGetErrorString(ie));
+      return SGM_ERR_CUDA;
+    }
+    e->graph_launches = e->launches;
+  }
+  if (dl != e->img[0]) SGM_CUDA_TRY(e, cudaMemcpyAsync(e->img[0], dl, N, cudaMemcpyDeviceToDevice, s));
+  if (dr != e->img[1]) SGM_CUDA_TRY(e, cudaMemcpyAsync(e->img[1], dr, N, cudaMemcpyDeviceToDevice, s));
+  SGM_CUDA_TRY(e, cudaGraphLaunch(e->gexec, s));
+  if (dout != e->out) SGM_CUDA_TRY(e, cudaMemcpyAsync(dout, e->out, N * sizeof(float), cudaMemcpyDeviceToDevice, s));
+  e->launches = e->graph_launches;
+  return SGM_OK;
+}
+
 int enqueue_depth(sgm_engine* e, const float* disp, float* depth, const sgm_camera_t& c, cudaStream_t s) {
   const int n = (int)e->npix();
   return SGM_LAUNCH(e, s, "depth", sgm::k_depth<<<(n + 255) / 256, 256, 0, s>>>(
@@ -705,8 +761,20 @@ struct sgm_pyramid {
   bool depth_mode = false;
   sgm_camera_t cam0{};
   float* disp0 = nullptr;  // finest-level disparity in depth mode
+  // The whole pyramid (in_l, in_r -> out) captured once as a CUDA graph after a first direct run;
+  // later matches copy in, launch it, copy out.
+  cudaGraphExec_t gexec = nullptr;
+  int direct_runs = 0;
+  int64_t graph_launches = 0;  // kernels inside the graph
+
+  void drop_graph() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    gexec = nullptr;
+    direct_runs = 0;
+  }
 
   void free_all() {
+    drop_graph();
     if (disp0) cudaFree(disp0);
     disp0 = nullptr;
     depth_mode = false;
@@ -774,6 +842,54 @@ int pyr_enqueue(sgm_pyramid* p, const uint8_t* dl, const uint8_t* dr, float* dou
   return st;
 }
 
+// One pyramid match on stream s. Without profiling, the second and later calls replay a CUDA
+// graph of the whole pyramid on the matcher's own buffers (one launch instead of one per
+// kernel), with device-to-device copies around it when the caller's buffers differ.
+int pyr_run(sgm_pyramid* p, const uint8_t* dl, const uint8_t* dr, float* dout, cudaStream_t s) {
+  if (g_prof.on) {
+    p->drop_graph();
+    return pyr_enqueue(p, dl, dr, dout, s);
+  }
+  if (!p->gexec && p->direct_runs == 0) {
+    p->direct_runs++;
+    return pyr_enqueue(p, dl, dr, dout, s);
+  }
+  const size_t N = (size_t)p->W * p->H;
+  if (!p->gexec) {
+    if (cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      p->err = "graph capture could not start";
+      return SGM_ERR_CUDA;
+    }
+    p->launches = 0;
+    const int st = pyr_enqueue(p, p->in_l, p->in_r, p->out, p->stream);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(p->stream, &g);
+    if (st || ce != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      if (!st) p->err = std::string("graph capture failed: ") + cudaGetErrorString(ce);
+      return st ? st : SGM_ERR_CUDA;
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&p->gexec, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) {
+      p->gexec = nullptr;
+      p->err = std::string("graph instantiation failed: ") + cudaGetErrorString(ie);
+      return SGM_ERR_CUDA;
+    }
+    p->graph_launches = p->launches;
+  }
+  if (dl != p->in_l && cudaMemcpyAsync(p->in_l, dl, N, cudaMemcpyDeviceToDevice, s) != cudaSuccess) return SGM_ERR_CUDA;
+  if (dr != p->in_r && cudaMemcpyAsync(p->in_r, dr, N, cudaMemcpyDeviceToDevice, s) != cudaSuccess) return SGM_ERR_CUDA;
+  if (cudaGraphLaunch(p->gexec, s) != cudaSuccess) {
+    p->err = "graph launch failed";
+    return SGM_ERR_CUDA;
+  }
+  if (dout != p->out && cudaMemcpyAsync(dout, p->out, N * sizeof(float), cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+    return SGM_ERR_CUDA;
+  p->launches = p->graph_launches;
+  return SGM_OK;
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------------------------------
@@ -810,6 +926,7 @@ int sgm_set_ext_options(sgm_handle_t h, const sgm_ext_options_t* ext) {
     return SGM_ERR_ARG;
   }
   h->ext = *ext;
+  h->drop_graph();
   return SGM_OK;
 }
 
@@ -845,6 +962,7 @@ int sgm_set_tuning(sgm_handle_t h, const sgm_tuning_t* t) {
     return SGM_ERR_ARG;
   }
   apply_tuning(h, t);
+  h->drop_graph();
   return SGM_OK;
 }
 
@@ -882,8 +1000,11 @@ int sgm_match(sgm_handle_t h, const uint8_t* img_left, const uint8_t* img_right,
   SGM_CUDA_TRY(h, cudaMemcpyAsync(h->img[1], img_right, N, cudaMemcpyHostToDevice, h->stream));
   if (init_disp_left)
     SGM_CUDA_TRY(h, cudaMemcpyAsync(h->init[0], init_disp_left, N * sizeof(int16_t), cudaMemcpyHostToDevice, h->stream));
-  int st = engine_enqueue(h, h->img[0], h->img[1], init_disp_left ? h->init[0] : nullptr, h->out,
-                          (disp_right && h->opt.do_lr_check) ? h->dr_out : nullptr, h->stream);
+  const bool right = disp_right && h->opt.do_lr_check;
+  int st = (!init_disp_left && !right)
+               ? engine_run(h, h->img[0], h->img[1], h->out, h->stream)
+               : engine_enqueue(h, h->img[0], h->img[1], init_disp_left ? h->init[0] : nullptr, h->out,
+                                right ? h->dr_out : nullptr, h->stream);
   if (st) return st;
   SGM_CUDA_TRY(h, cudaMemcpyAsync(disp_left, h->out, N * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
   if (disp_right && h->opt.do_lr_check)
@@ -906,6 +1027,7 @@ int sgm_match_device(sgm_handle_t h, const uint8_t* d_left, const uint8_t* d_rig
     return SGM_ERR_ARG;
   }
   h->launches = 0;
+  if (!d_init_disp_left && !d_disp_right) return engine_run(h, d_left, d_right, d_disp_left, (cudaStream_t)stream);
   return engine_enqueue(h, d_left, d_right, d_init_disp_left, d_disp_left, d_disp_right, (cudaStream_t)stream);
 }
 
@@ -954,6 +1076,7 @@ int sgm_release(sgm_handle_t h) {
 int sgm_set_min_disparity(sgm_handle_t h, int32_t min_disparity) {
   if (!h) return SGM_ERR_ARG;
   h->M = min_disparity;
+  h->drop_graph();  // kernel parameters are part of the graph
   return SGM_OK;
 }
 
@@ -1019,6 +1142,10 @@ int sgm_debug_read(sgm_handle_t h, int32_t which, int32_t view, void* dst, size_
   }
   const uint8_t* src = nullptr;
   size_t n = V;
+  if (which >= 2 && which <= 5 && view >= h->nviews()) {
+    set_error(&h->err, "no right-view volumes without the left-right check");
+    return SGM_ERR_ARG;
+  }
   switch (which) {
     case 2: src = h->cost + view * V; break;
     case 3: src = h->lr + view * V; break;
@@ -1139,7 +1266,7 @@ int sgm_pyr_match(sgm_pyr_handle_t h, const uint8_t* img_left, const uint8_t* im
   if (cudaMemcpyAsync(h->in_l, img_left, N, cudaMemcpyHostToDevice, h->stream) ||
       cudaMemcpyAsync(h->in_r, img_right, N, cudaMemcpyHostToDevice, h->stream))
     return SGM_ERR_CUDA;
-  int st = pyr_enqueue(h, h->in_l, h->in_r, h->out, h->stream);
+  int st = pyr_run(h, h->in_l, h->in_r, h->out, h->stream);
   if (st) return st;
   if (cudaMemcpyAsync(disp, h->out, N * sizeof(float), cudaMemcpyDeviceToHost, h->stream)) return SGM_ERR_CUDA;
   if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
@@ -1155,7 +1282,7 @@ int sgm_pyr_match_device(sgm_pyr_handle_t h, const uint8_t* d_left, const uint8_
   if (!h->ready) return SGM_ERR_STATE;
   if (!d_left || !d_right || !d_disp) return SGM_ERR_ARG;
   h->launches = 0;
-  return pyr_enqueue(h, d_left, d_right, d_disp, stream ? (cudaStream_t)stream : h->stream);
+  return pyr_run(h, d_left, d_right, d_disp, stream ? (cudaStream_t)stream : h->stream);
 }
 
 int sgm_pyr_init2(sgm_pyr_handle_t h, const sgm_pyr_option2_t* o, const sgm_level_override_t* ov,
@@ -1260,6 +1387,7 @@ int sgm_pyr_set_tuning(sgm_pyr_handle_t h, int32_t level, const sgm_tuning_t* t)
   }
   for (int i = 0; i < h->layers; ++i)
     if (level < 0 || level == i) apply_tuning(h->lv[i], t);
+  h->drop_graph();
   return SGM_OK;
 }
 

@@ -312,3 +312,44 @@ def test_large_pyramid_4800x3409_d256(engine_lib, oracle_mod):
                      peaks_strips=STRIPS)
     assert_same("large pyramid", disp, O.pyr_match(pc, L, R))
     assert (disp != INV).mean() > 0.5
+
+
+def test_graph_replay_over_successive_matches(engine_lib, oracle_mod):
+    """The first match runs kernel by kernel, later ones replay a captured CUDA graph (with
+    copies in and out for caller buffers); a tuning change drops the graph. Every result must
+    equal the oracle, for both matchers and both entry points."""
+    import torch
+    import fasterstereocuda_b200 as fsc
+    O = oracle_mod
+    W, H = 320, 200
+    s = make_engine(fsc, W, H, 0, 64, 1, 10, 150, 0.95, 1, 1)
+    cfg = O.Config(width=W, height=H, disp_range=64, peaks_strips=STRIPS)
+    p = fsc.FasterStereoCuda()
+    assert p.Init(fsc.StereoOption1(width=W, height=H, min_disp=0, max_disp=64, num_layers=2),
+                  fsc.LevelOverride(1, 10, 150), fsc.ExtOptions(peaks_strips=STRIPS)), p.last_error()
+    pc = O.PyrConfig(width=W, height=H, max_disp=64, num_layers=2, override_enable=1, cs_type=1, p1=10, p2=150,
+                     peaks_strips=STRIPS)
+    stream = torch.cuda.current_stream().cuda_stream
+    for k in range(5):
+        L, R, _ = scenes.planar_pair(70 + k, W, H)
+        if k == 3:
+            assert s.set_tuning(fsc.Tuning(3, 0, 3, 0, 0, 4, 2)) and p.set_tuning(fsc.Tuning(0, 0, 0, 0, 0, 2, 4))
+        out = np.empty((H, W), np.float32)
+        if k % 2 == 0:
+            assert s.Match(L, R, out), s.last_error()
+        else:
+            dout = torch.empty((H, W), dtype=torch.float32, device="cuda")
+            assert s.match_device(torch.from_numpy(L).cuda(), torch.from_numpy(R).cuda(), dout, None, None, stream)
+            torch.cuda.synchronize()
+            out = dout.cpu().numpy()
+        assert_same(f"plain match {k}", out, O.match(cfg, L, R)["disp"])
+        pout = np.empty((H, W), np.float32)
+        if k % 2 == 1:
+            assert p.Match(L, R, pout), p.last_error()
+        else:
+            dout = torch.empty((H, W), dtype=torch.float32, device="cuda")
+            assert p.match_device(torch.from_numpy(L).cuda(), torch.from_numpy(R).cuda(), dout, stream)
+            torch.cuda.synchronize()
+            pout = dout.cpu().numpy()
+        assert_same(f"pyramid match {k}", pout, O.pyr_match(pc, L, R))
+    assert s.kernel_launches() > 0 and p.kernel_launches() > 0
