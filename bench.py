@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--tuning", default="", help="kernel variants row_kernel,rows_per_cta,col_kernel,cols_per_cta,"
                                                  "bt_smem,row_lanes,col_lanes (default: autotuned lane split)")
     ap.add_argument("--profile-pairs", type=int, default=16, help="pairs of the serialised per-kernel timing pass")
+    ap.add_argument("--e2e-threads", type=int, default=64, help="host threads (one matcher each) of the e2e pass")
     return ap.parse_args()
 
 
@@ -301,6 +302,7 @@ def run_ours(a, rank, world, local_rank):
     # autotune: the lane split of the scanline kernels that is fastest at this concurrency
     # (every split gives the same disparities); two untimed steps per candidate
     tuning = a.tuning or None
+    chosen = None  # tuning applied to matchers made later (None: make_matcher's own)
     if not a.tuning:
         best = None
         for lanes in ((8, 8), (8, 4), (4, 4), (4, 2), (2, 2)):
@@ -314,7 +316,8 @@ def run_ours(a, rank, world, local_rank):
             dt = max_over_ranks(time.perf_counter() - t0c)
             if best is None or dt < best[0]:
                 best = (dt, lanes)
-        apply_tuning((0, 0, 0, 0, 0) + best[1])
+        chosen = (0, 0, 0, 0, 0) + best[1]
+        apply_tuning(chosen)
         tuning = "autotuned row_lanes,col_lanes = %d,%d" % best[1]
     for _ in range(a.warmup):
         step()
@@ -346,27 +349,36 @@ def run_ours(a, rank, world, local_rank):
 
     # e2e: the host-buffer API (synchronous Match, like the reference's), pinned host memory, one
     # host thread per matcher (the reference API is per object; ctypes releases the GIL)
+    # each host thread matches its share of e2e_steps * batch pairs in one loop
     from concurrent.futures import ThreadPoolExecutor
     e2e_steps = max(1, min(a.steps, 5))
+    E = max(S, a.e2e_threads)
+    e2e_matchers = matchers + [make_matcher() for _ in range(E - S)]
+    if chosen is not None:
+        for m in e2e_matchers[S:]:
+            if not m.set_tuning(fsc.Tuning(*chosen)):
+                raise RuntimeError(f"tuning rejected: {m.last_error()}")
     hostL = [torch.from_numpy(L).pin_memory().numpy() for L, _ in pool[:a.batch]]
     hostR = [torch.from_numpy(R).pin_memory().numpy() for _, R in pool[:a.batch]]
-    hostO = [torch.empty((H_, W_), dtype=torch.float32).pin_memory().numpy() for _ in range(a.batch)]
+    hostO = [[torch.empty((H_, W_), dtype=torch.float32).pin_memory().numpy() for _ in range(2)] for _ in range(E)]
+    total_pairs = e2e_steps * a.batch
 
-    def host_worker(k):
-        m = matchers[k]
-        for b in range(k, a.batch, S):
-            if not m.Match(hostL[b], hostR[b], hostO[b]):
+    def host_worker(k, count):
+        m = e2e_matchers[k]
+        for j, b in enumerate(range(k, count, E)):
+            i = b % a.batch
+            if not m.Match(hostL[i], hostR[i], hostO[k][j % 2]):
                 raise RuntimeError(m.last_error())
 
-    with ThreadPoolExecutor(max_workers=S) as ex:
-        list(ex.map(host_worker, range(S)))  # warm-up
+    with ThreadPoolExecutor(max_workers=E) as ex:
+        list(ex.map(lambda k: host_worker(k, 2 * E), range(E)))  # warm-up (direct run, graph capture)
         barrier()
         te = time.perf_counter()
-        for _ in range(e2e_steps):
-            list(ex.map(host_worker, range(S)))
+        list(ex.map(lambda k: host_worker(k, total_pairs), range(E)))
         te = max_over_ranks(time.perf_counter() - te)
-    e2e_value = e2e_steps * a.batch * world / te
+    e2e_value = total_pairs * world / te
 
+    clk_summary = clk.summary()
     if rank != 0:
         return 0
     hbm_peak, peak_kind = peaks()
@@ -401,6 +413,17 @@ def run_ours(a, rank, world, local_rank):
                     "avg_launch_us": total_ms / prof[dom]["launches"] * 1e3,
                     "alg_bytes_per_launch": per_call_bytes.get(dom, 0) / max(1, prof[dom]["launches"] // calls),
                     "timing": f"CUDA events around each launch, serialised pass of {calls} pairs on one stream"}
+    if roofline is not None:
+        # the path is integer-ALU bound: algorithmic int ops per view 34*W*H*D + 248*W*H (xor+popc,
+        # 7 per path step x 4 paths, 3 adds, 1 min per voxel; census per pixel), over all levels,
+        # against the nominal INT32 rate of the measured SM clock (148 SMs x 128 lanes)
+        ops = sum(nv * (34 * w * h * d + 248 * w * h) for (kind, w, h, d, nv) in levels)
+        clk = (clk_summary or {}).get("sm_mhz") or 1965.0
+        peak = 148 * 128 * clk * 1e6
+        roofline["alu"] = {"ops_alg_per_pair": ops, "achieved_tops": ops * value / 1e12 / world,
+                           "int32_peak_tops": peak / 1e12, "frac": ops * value / world / peak,
+                           "peak_kind": "nominal: 148 SMs x 128 INT32 lanes x median SM clock under load",
+                           "per": "GPU"}
     tot_ms = sum(x["ms"] for x in prof.values()) or 1.0
     kernels = {k: {"launches": v["launches"], "avg_us": round(v["ms"] / max(1, v["launches"]) * 1e3, 2),
                    "share": round(v["ms"] / tot_ms, 4)} for k, v in prof.items()}
@@ -412,7 +435,7 @@ def run_ours(a, rank, world, local_rank):
         extras = extra_batches(pool)
         extras["float_sgm"] = extra_float_sgm()
         extras["large_pyramid"] = extra_large_pyramid()
-    clocks = clk.summary()
+    clocks = clk_summary
     line = {"metric": metric_name(a.workload), "value": value, "unit": "pairs/s", "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u8/u32 (f32 subpixel)",
@@ -423,7 +446,7 @@ def run_ours(a, rank, world, local_rank):
             "e2e": {"value": e2e_value, "unit": "pairs/s",
                     "h2d_bytes_per_step": a.batch * 2 * W_ * H_, "d2h_bytes_per_step": a.batch * 4 * W_ * H_,
                     "api": ("FasterStereoCuda.Match" if a.workload == "pyramid" else "StereoCuda.Match")
-                    + f" (host buffers, synchronous), {S} host threads with one matcher each"},
+                    + f" (host buffers, synchronous), {E} host threads with one matcher each"},
             "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
             "bit_exact_vs_oracle": bit_exact, "kernels": kernels, "extras": extras}
     print(json.dumps(line), flush=True)

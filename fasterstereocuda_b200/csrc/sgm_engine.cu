@@ -167,6 +167,7 @@ struct sgm_engine {
   cudaGraphExec_t gexec = nullptr;
   int direct_runs = 0;
   int64_t graph_launches = 0;
+  cudaEvent_t done = nullptr;  // blocking-sync event of the synchronous host API
   void drop_graph() {
     if (gexec) cudaGraphExecDestroy(gexec);
     gexec = nullptr;
@@ -180,6 +181,8 @@ struct sgm_engine {
 
   void free_all() {
     drop_graph();
+    if (done) cudaEventDestroy(done);
+    done = nullptr;
     for (int i = 0; i < 2; ++i) {
       dfree(img[i]);
       dfree(init[i]);
@@ -199,6 +202,18 @@ struct sgm_engine {
 };
 
 namespace {
+
+// Waits for everything enqueued on s so far without spinning a CPU core (a blocking-sync event):
+// callers that run many matchers from many host threads keep their cores for the other threads.
+// `ev` is the matcher's own event, created on first use on its device.
+cudaError_t wait_stream(cudaStream_t s, cudaEvent_t* ev) {
+  if (!*ev) {
+    const cudaError_t st = cudaEventCreateWithFlags(ev, cudaEventBlockingSync | cudaEventDisableTiming);
+    if (st != cudaSuccess) return st;
+  }
+  const cudaError_t st = cudaEventRecord(*ev, s);
+  return st != cudaSuccess ? st : cudaEventSynchronize(*ev);
+}
 
 #define SGM_CUDA_TRY(e, expr)                                                          \
   do {                                                                                 \
@@ -766,6 +781,7 @@ struct sgm_pyramid {
   cudaGraphExec_t gexec = nullptr;
   int direct_runs = 0;
   int64_t graph_launches = 0;  // kernels inside the graph
+  cudaEvent_t done = nullptr;  // blocking-sync event of the synchronous host API
 
   void drop_graph() {
     if (gexec) cudaGraphExecDestroy(gexec);
@@ -775,6 +791,8 @@ struct sgm_pyramid {
 
   void free_all() {
     drop_graph();
+    if (done) cudaEventDestroy(done);
+    done = nullptr;
     if (disp0) cudaFree(disp0);
     disp0 = nullptr;
     depth_mode = false;
@@ -1009,7 +1027,7 @@ int sgm_match(sgm_handle_t h, const uint8_t* img_left, const uint8_t* img_right,
   SGM_CUDA_TRY(h, cudaMemcpyAsync(disp_left, h->out, N * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
   if (disp_right && h->opt.do_lr_check)
     SGM_CUDA_TRY(h, cudaMemcpyAsync(disp_right, h->dr_out, N * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
-  SGM_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  SGM_CUDA_TRY(h, wait_stream(h->stream, &h->done));
   if (disp_right && !h->opt.do_lr_check)
     for (size_t i = 0; i < N; ++i) disp_right[i] = sgm::kInvalidFloat;
   return SGM_OK;
@@ -1063,7 +1081,7 @@ int sgm_match2(sgm_handle_t h, const uint8_t* img_left, const uint8_t* img_right
   if (!st) st = enqueue_depth(h, h->out, h->post2, h->cam, h->stream);
   if (st) return st;
   SGM_CUDA_TRY(h, cudaMemcpyAsync(depth_left, h->post2, N * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
-  SGM_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  SGM_CUDA_TRY(h, wait_stream(h->stream, &h->done));
   return SGM_OK;
 }
 
@@ -1269,7 +1287,7 @@ int sgm_pyr_match(sgm_pyr_handle_t h, const uint8_t* img_left, const uint8_t* im
   int st = pyr_run(h, h->in_l, h->in_r, h->out, h->stream);
   if (st) return st;
   if (cudaMemcpyAsync(disp, h->out, N * sizeof(float), cudaMemcpyDeviceToHost, h->stream)) return SGM_ERR_CUDA;
-  if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
+  if (wait_stream(h->stream, &h->done) != cudaSuccess) {
     set_error(&h->err, "pyramid match failed: %s", cudaGetErrorString(cudaGetLastError()));
     return SGM_ERR_CUDA;
   }
