@@ -54,7 +54,7 @@ def parse():
     ap.add_argument("--tuning", default="", help="kernel variants row_kernel,rows_per_cta,col_kernel,cols_per_cta,"
                                                  "bt_smem,row_lanes,col_lanes (default: autotuned lane split)")
     ap.add_argument("--profile-pairs", type=int, default=16, help="pairs of the serialised per-kernel timing pass")
-    ap.add_argument("--e2e-threads", type=int, default=64, help="host threads (one matcher each) of the e2e pass")
+    ap.add_argument("--e2e-threads", type=int, default=96, help="host threads (one matcher each) of the e2e pass")
     return ap.parse_args()
 
 
@@ -233,10 +233,15 @@ def run_ours(a, rank, world, local_rank):
             raise RuntimeError(f"tuning rejected: {m.last_error()}")
         return m
 
-    def apply_tuning(t):
-        for m in matchers:
+    def apply_tuning(t, init_t=None, ms=None):
+        """t for every level; init_t (pyramid) for the 32-disparity levels below the coarsest."""
+        for m in (matchers if ms is None else ms):
             if not m.set_tuning(fsc.Tuning(*t)):
                 raise RuntimeError(f"tuning rejected: {m.last_error()}")
+            if init_t is not None:
+                for lv in range(LAYERS - 1):
+                    if not m.set_tuning(fsc.Tuning(*init_t), lv):
+                        raise RuntimeError(f"tuning rejected: {m.last_error()}")
 
     def run_one(m, L, R, out, stream):
         if a.workload == "pyramid":
@@ -302,23 +307,28 @@ def run_ours(a, rank, world, local_rank):
     # autotune: the lane split of the scanline kernels that is fastest at this concurrency
     # (every split gives the same disparities); two untimed steps per candidate
     tuning = a.tuning or None
-    chosen = None  # tuning applied to matchers made later (None: make_matcher's own)
+    chosen, chosen_init = None, None  # tunings applied to matchers made later
     if not a.tuning:
-        best = None
-        for lanes in ((8, 8), (8, 4), (4, 4), (4, 2), (2, 2)):
-            apply_tuning((0, 0, 0, 0, 0) + lanes)
+        def timed(t, init_t=None):
+            apply_tuning(t, init_t)
             step()
             torch.cuda.synchronize()
             t0c = time.perf_counter()
             for _ in range(2):
                 step()
             torch.cuda.synchronize()
-            dt = max_over_ranks(time.perf_counter() - t0c)
-            if best is None or dt < best[0]:
-                best = (dt, lanes)
+            return max_over_ranks(time.perf_counter() - t0c)
+        best = min(((timed((0, 0, 0, 0, 0) + lanes), lanes) for lanes in ((8, 8), (8, 4), (4, 4), (4, 2), (2, 2))),
+                   key=lambda r: r[0])
         chosen = (0, 0, 0, 0, 0) + best[1]
-        apply_tuning(chosen)
         tuning = "autotuned row_lanes,col_lanes = %d,%d" % best[1]
+        if a.workload == "pyramid":  # then the 32-disparity levels on their own
+            best_i = min(((timed(chosen, (0, 0, 0, 0, 0) + lanes), lanes) for lanes in ((8, 8), (4, 4), (2, 2))),
+                         key=lambda r: r[0])
+            if best_i[0] < best[0]:
+                chosen_init = (0, 0, 0, 0, 0) + best_i[1]
+                tuning += "; 32-disparity levels %d,%d" % best_i[1]
+        apply_tuning(chosen, chosen_init)
     for _ in range(a.warmup):
         step()
     torch.cuda.synchronize()
@@ -355,9 +365,7 @@ def run_ours(a, rank, world, local_rank):
     E = max(S, a.e2e_threads)
     e2e_matchers = matchers + [make_matcher() for _ in range(E - S)]
     if chosen is not None:
-        for m in e2e_matchers[S:]:
-            if not m.set_tuning(fsc.Tuning(*chosen)):
-                raise RuntimeError(f"tuning rejected: {m.last_error()}")
+        apply_tuning(chosen, chosen_init, e2e_matchers[S:])
     hostL = [torch.from_numpy(L).pin_memory().numpy() for L, _ in pool[:a.batch]]
     hostR = [torch.from_numpy(R).pin_memory().numpy() for _, R in pool[:a.batch]]
     hostO = [[torch.empty((H_, W_), dtype=torch.float32).pin_memory().numpy() for _ in range(2)] for _ in range(E)]

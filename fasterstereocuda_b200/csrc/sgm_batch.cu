@@ -874,6 +874,10 @@ int level_post(sgm_batch_pyr* p, const BatchPair* d, const int* tpre, int tiles,
 // Dilation and small-region removal of one level, when its options ask for them.
 int level_filters(sgm_batch_pyr* p, const BatchPair* d, const sgm_option_t& o, int tpre, int tiles, int rpre, int rows,
                   int ppre, int pix, int n, cudaStream_t s, int64_t* kernels) {
+  if (o.post_filter_type == 1) {  // the LR/median stage wrote `post`
+    kb_gauss<<<tiles, dim3(32, 8), 0, s>>>(d, p->dtab + tpre, n);
+    (*kernels)++;
+  }
   if (o.morphology_type == 2) {
     kb_dilation<<<tiles, dim3(32, 8), 0, s>>>(d, p->dtab + tpre, n);
     (*kernels)++;
@@ -1078,7 +1082,7 @@ int sgm_batch_pyr_init(sgm_batch_pyr_t p, const sgm_batch_pair_t* pairs, int32_t
   if (!p) return SGM_ERR_ARG;
   if (!pairs || !option || count <= 0) return perr(p, SGM_ERR_ARG, "empty batch or null argument");
   if (count > 4096) return perr(p, SGM_ERR_ARG, "at most 4096 pairs per batch (got %d)", count);
-  if (option->do_smooth) return perr(p, SGM_ERR_UNSUPPORTED, "post filters are not supported");
+
   const int layers = std::max(1, option->num_layers);
   sgm_ext_options_t ex{};
   ex.tie_rule = ex.init_tie_rule = sgm::kTieRefB200;
@@ -1119,9 +1123,10 @@ int sgm_batch_pyr_init(sgm_batch_pyr_t p, const sgm_batch_pair_t* pairs, int32_t
   }
   p->copt = copt;
   p->word = copt.cs_type == 1 ? 8 : 4;
-  sgm_option_t cbatch = copt;
+  sgm_option_t cbatch = copt;  // the parent applies smoothing, dilation and removal
   cbatch.do_remove_peaks = false;
   cbatch.morphology_type = 0;
+  cbatch.post_filter_type = 0;
   p->coarse = new sgm_batch();
   int st = sgm_batch_init(p->coarse, cp.data(), count, &cbatch, &ex);
   if (st) return perr(p, st, "coarsest level: %s", p->coarse->err.c_str());
@@ -1138,6 +1143,8 @@ int sgm_batch_pyr_init(sgm_batch_pyr_t p, const sgm_batch_pair_t* pairs, int32_t
     p->lv[lvl].n = lvl;
     const sgm_option_t& lo = p->lv[lvl].opt;
     if (lo.do_lr_check) return perr(p, SGM_ERR_UNSUPPORTED, "LR check at an initial-disparity level");
+    if (lo.post_filter_type == 1 && lo.morphology_type == 2)
+      return perr(p, SGM_ERR_UNSUPPORTED, "smoothing and dilation at the same level");
     for (int i = 0; i < count; ++i) {
       const size_t N = (size_t)(pairs[i].width >> lvl) * (pairs[i].height >> lvl);
       off[lvl][i] = total;
@@ -1145,11 +1152,13 @@ int sgm_batch_pyr_init(sgm_batch_pyr_t p, const sgm_batch_pair_t* pairs, int32_t
                3 * align256(N * 4) + align256(N * 2) + (lo.do_remove_peaks ? 2 * align256(N * 4) : 0);
     }
   }
+  const bool cpf = copt.post_filter_type == 1;
+  if (cpf && cdil) return perr(p, SGM_ERR_UNSUPPORTED, "smoothing and dilation at the same level");
   std::vector<size_t> coff(count);
   for (int i = 0; i < count; ++i) {
     const size_t N = (size_t)cp[i].width * cp[i].height;
     coff[i] = total;
-    total += (cdil ? align256(N * 4) : 0) + (cpeaks ? 2 * align256(N * 4) : 0);
+    total += (cdil || cpf ? align256(N * 4) : 0) + (cpeaks ? 2 * align256(N * 4) : 0);
   }
   p->arena_bytes = total + p->coarse->arena_bytes;
   if (total) PTRY(p, cudaMalloc(&p->arena, total));
@@ -1159,7 +1168,7 @@ int sgm_batch_pyr_init(sgm_batch_pyr_t p, const sgm_batch_pair_t* pairs, int32_t
     BatchPair& d = p->coarse->hdesc[i];
     unsigned char* q = p->arena + coff[i];
     const size_t N = (size_t)cp[i].width * cp[i].height;
-    if (cdil) {
+    if (cdil || cpf) {
       d.post = reinterpret_cast<float*>(q);
       q += align256(N * 4);
       const int s2 = std::min(cp[i].width, cp[i].height);
@@ -1197,7 +1206,7 @@ int sgm_batch_pyr_init(sgm_batch_pyr_t p, const sgm_batch_pair_t* pairs, int32_t
       float* post = reinterpret_cast<float*>(q); q += align256(N * 4);
       d.out = reinterpret_cast<float*>(q); q += align256(N * 4);
       d.init = reinterpret_cast<const int16_t*>(q); q += align256(N * 2);
-      if (lo.morphology_type == 2) {
+      if (lo.morphology_type == 2 || lo.post_filter_type == 1) {
         d.post = post;
         const int s2 = std::min(w, h);
         d.dil_wth = ((s2 < 360 ? 3 : (s2 < 720 ? 5 : 7)) - 1) / 2;

@@ -218,6 +218,19 @@ static __global__ void __launch_bounds__(256) kb_dilation(const BatchPair* __res
   if (x < d.P.W && y < d.P.H) sgm::dilation_px<float>(d.post, d.out, d.P.W, d.P.H, d.dil_wth, x, y);
 }
 
+// Gauss smoothing post -> out (the pyramid's finest level with do_smooth), one block per tile.
+static __global__ void __launch_bounds__(256) kb_gauss(const BatchPair* __restrict__ pairs,
+                                                       const int* __restrict__ tprefix, int n) {
+  const int item = blockIdx.x;
+  const int b = find_pair(tprefix, n, item);
+  const BatchPair d = pairs[b];
+  const int local = item - __ldg(tprefix + b);
+  const int tiles_x = (d.P.W + 31) / 32;
+  const int ty = local / tiles_x, tx = local - ty * tiles_x;
+  const int x = tx * 32 + threadIdx.x, y = ty * 8 + threadIdx.y;
+  if (x < d.P.W && y < d.P.H) sgm::gauss_px(d.post, d.out, d.P.W, d.P.H, 1.5f, 2.0f, x, y);
+}
+
 // Small-region removal on `out`: row runs (one warp per row), vertical unions, sizes, filter.
 static __global__ void __launch_bounds__(256) kb_cc_rows(const BatchPair* __restrict__ pairs,
                                                          const int* __restrict__ rprefix, int n, int abs_mode) {

@@ -257,13 +257,14 @@ int validate(sgm_engine* e, int W, int H, int D, const sgm_option_t* o) {
     set_error(&e->err, "negative penalties (p1=%d p2=%d)", o->p1, o->p2_init);
     return SGM_ERR_ARG;
   }
-  if (o->post_filter_type != 0) {
-    set_error(&e->err, "post filter type %d unsupported", o->post_filter_type);
-    return SGM_ERR_UNSUPPORTED;
+  if (o->post_filter_type < 0 || o->post_filter_type > 2) {
+    set_error(&e->err, "post filter type %d invalid (0 none, 1 Gauss, 2 bilateral)", o->post_filter_type);
+    return SGM_ERR_ARG;
   }
-  if (o->morphology_type != 0 && o->morphology_type != 2) {
-    set_error(&e->err, "morphology type %d unsupported (none or dilation)", o->morphology_type);
-    return SGM_ERR_UNSUPPORTED;
+  if (o->morphology_type < 0 || o->morphology_type > 4) {
+    set_error(&e->err, "morphology type %d invalid (0 none, 1 erosion, 2 dilation, 3 open, 4 close)",
+              o->morphology_type);
+    return SGM_ERR_ARG;
   }
   if ((size_t)W * H > (size_t)INT32_MAX / 2) {
     set_error(&e->err, "image too large");
@@ -646,35 +647,57 @@ int engine_enqueue(sgm_engine* e, const uint8_t* dl_img, const uint8_t* dr_img, 
       }
     }
   }
-  // left-right check + median, then optional dilation and small-region removal
+  // left-right check + median, post filter, morphology (reference DisparityFilter::Filter,
+  // cusgm_df.cu:275-339), then small-region removal. The reference's OPEN and CLOSE run both
+  // of their steps from the same input into the same output, so OPEN leaves the dilation and
+  // CLOSE the erosion (cusgm_df.cu:311-322); so do these.
   const bool lr = e->opt.do_lr_check, med = e->opt.do_median_filter;
-  const bool dil = e->opt.morphology_type == 2;
+  const int pf = e->opt.post_filter_type;
+  const int mp = e->opt.morphology_type;
+  const int morph = mp == 3 ? 2 : (mp == 4 ? 1 : mp);  // 1 erosion, 2 dilation
   const bool peaks = e->opt.do_remove_peaks;
+  const int nstages = (lr || med ? 1 : 0) + (pf ? 1 : 0) + (morph ? 1 : 0);
+  int stage = 0;
+  float* spare[2] = {e->post, e->post2};
+  // the last stage writes dout; the others alternate between the two spare maps
+  auto next_out = [&]() { return ++stage == nstages ? dout : spare[stage & 1]; };
   float* cur = e->wta;  // view 0
   if (!st && lr && dout_r) {
     cudaMemcpyAsync(dout_r, e->wta + N, N * sizeof(float), cudaMemcpyDeviceToDevice, e->stream);
   }
+  const dim3 fb(32, 8), fg((W + 31) / 32, (H + 7) / 8);
   if (!st && (lr || med)) {
-    float* dst = (!dil) ? dout : e->post;
-    dim3 b(32, 8), g((W + 31) / 32, (H + 7) / 8);
+    float* dst = next_out();
     float* marks = lr ? dout_r : nullptr;
     if (lr && med)
-      st = SGM_LAUNCH(e, e->stream, "lr_median", sgm::k_lr_median<true, true><<<g, b, 0, e->stream>>>(
+      st = SGM_LAUNCH(e, e->stream, "lr_median", sgm::k_lr_median<true, true><<<fg, fb, 0, e->stream>>>(
                                                      e->wta, e->wta + N, marks, dst, W, H, e->opt.lr_threshold));
     else if (lr)
-      st = SGM_LAUNCH(e, e->stream, "lr_median", sgm::k_lr_median<true, false><<<g, b, 0, e->stream>>>(
+      st = SGM_LAUNCH(e, e->stream, "lr_median", sgm::k_lr_median<true, false><<<fg, fb, 0, e->stream>>>(
                                                      e->wta, e->wta + N, marks, dst, W, H, e->opt.lr_threshold));
     else
-      st = SGM_LAUNCH(e, e->stream, "lr_median", sgm::k_lr_median<false, true><<<g, b, 0, e->stream>>>(
+      st = SGM_LAUNCH(e, e->stream, "lr_median", sgm::k_lr_median<false, true><<<fg, fb, 0, e->stream>>>(
                                                      e->wta, nullptr, nullptr, dst, W, H, 0.0f));
     cur = dst;
   }
-  if (!st && dil) {
+  if (!st && pf) {
+    float* dst = next_out();
+    if (pf == 1)
+      st = SGM_LAUNCH(e, e->stream, "gauss", sgm::k_gauss_filter<<<fg, fb, 0, e->stream>>>(cur, dst, W, H, 1.5f, 2.0f));
+    else
+      st = SGM_LAUNCH(e, e->stream, "bilateral", sgm::k_bilateral_filter<<<fg, fb, 0, e->stream>>>(
+                                                     dl_img, cur, dst, W, H, 2.5f, 10.0f));
+    cur = dst;
+  }
+  if (!st && morph) {
+    float* dst = next_out();
     const int s2 = std::min(W, H);
     const int wnd = s2 < 360 ? 3 : (s2 < 720 ? 5 : 7);
-    dim3 b(32, 8), g((W + 31) / 32, (H + 7) / 8);
-    st = SGM_LAUNCH(e, e->stream, "dilation", sgm::k_dilation<float><<<g, b, 0, e->stream>>>(cur, dout, W, H, (wnd - 1) / 2));
-    cur = dout;
+    if (morph == 2)
+      st = SGM_LAUNCH(e, e->stream, "dilation", sgm::k_dilation<float><<<fg, fb, 0, e->stream>>>(cur, dst, W, H, (wnd - 1) / 2));
+    else
+      st = SGM_LAUNCH(e, e->stream, "erosion", sgm::k_erosion<<<fg, fb, 0, e->stream>>>(cur, dst, W, H, (wnd - 1) / 2));
+    cur = dst;
   }
   if (!st && cur != dout) {
     cudaMemcpyAsync(dout, cur, N * sizeof(float), cudaMemcpyDeviceToDevice, e->stream);

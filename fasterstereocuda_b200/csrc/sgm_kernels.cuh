@@ -1223,6 +1223,100 @@ __device__ __forceinline__ void dilation_px(const T* __restrict__ in, T* __restr
   out[(size_t)y * W + x] = v;
 }
 
+// Erosion (reference Kernel_Erosion, cusgm_df.cu:165-195): an interior pixel whose window
+// holds an INVALID value becomes INVALID, every other pixel keeps its value.
+__device__ __forceinline__ void erosion_px(const float* __restrict__ in, float* __restrict__ out, int W, int H,
+                                           int wth, int x, int y) {
+  const float v = in[(size_t)y * W + x];
+  float mn = v;
+  if (x > wth && x < W - wth && y > wth && y < H - wth) {
+    for (int dx = -wth; dx <= wth; ++dx)
+      for (int dy = -wth; dy <= wth; ++dy) {
+        const float u = in[(size_t)(y + dy) * W + x + dx];
+        if (u < mn) mn = u;
+      }
+  }
+  out[(size_t)y * W + x] = mn == kInvalidFloat ? mn : v;
+}
+
+static __global__ void __launch_bounds__(256) k_erosion(const float* __restrict__ in, float* __restrict__ out, int W,
+                                                        int H, int wth) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= W || y >= H) return;
+  erosion_px(in, out, W, H, wth, x, y);
+}
+
+// Range-limited Gaussian smoothing of the disparity (reference Kernel_GaussFilter,
+// cusgm_df.cu:93-121, called with sigmaD 1.5 and sigmaR 2.0): weights exp(-(dx^2+dy^2)/(2 sD^2))
+// over a (2*ceil(2 sD)+1)^2 window of valid neighbours within sR of the centre.
+__device__ __forceinline__ void gauss_px(const float* __restrict__ in, float* __restrict__ out, int W, int H,
+                                         float sigma_d, float sigma_r, int x, int y) {
+  const int r = (int)ceil(2.0 * sigma_d);
+  float result = kInvalidFloat;
+  float sum = 0.0f, sum_w = 0.0f;
+  const float c = in[(size_t)y * W + x];
+  if (c != kInvalidFloat) {
+    for (int m = x - r; m <= x + r; ++m)
+      for (int n = y - r; n <= y + r; ++n)
+        if (m >= 0 && n >= 0 && m < W && n < H) {
+          const float v = in[(size_t)n * W + m];
+          if (v != kInvalidFloat && fabsf(c - v) < sigma_r) {
+            const int dx = m - x, dy = n - y;
+            const float w = expf(-((dx * dx + dy * dy) / (2.0f * sigma_d * sigma_d)));
+            sum_w += w;
+            sum += w * v;
+          }
+        }
+  }
+  if (sum_w > 0.0f) result = sum / sum_w;
+  out[(size_t)y * W + x] = result;
+}
+
+static __global__ void __launch_bounds__(256) k_gauss_filter(const float* __restrict__ in, float* __restrict__ out,
+                                                             int W, int H, float sigma_d, float sigma_r) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= W || y >= H) return;
+  gauss_px(in, out, W, H, sigma_d, sigma_r, x, y);
+}
+
+// Bilateral smoothing guided by the left image (reference Kernel_BilateralFilter,
+// cusgm_df.cu:123-162, called with sigmaD 2.5 and sigmaR 10.0): the spatial weight times
+// exp(-g^2/(2 sR^2)) of the grey difference g (evaluated in double, as there), for valid
+// neighbours with |g| < sR.
+static __global__ void __launch_bounds__(256) k_bilateral_filter(const uint8_t* __restrict__ img,
+                                                                 const float* __restrict__ in, float* __restrict__ out,
+                                                                 int W, int H, float sigma_d, float sigma_r) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= W || y >= H) return;
+  const int r = (int)ceil(2.0 * sigma_d);
+  float result = kInvalidFloat;
+  float sum = 0.0f, sum_w = 0.0f;
+  const float c = in[(size_t)y * W + x];
+  const uint8_t gc = img[(size_t)y * W + x];
+  if (c != kInvalidFloat) {
+    for (int m = x - r; m <= x + r; ++m)
+      for (int n = y - r; n <= y + r; ++n)
+        if (m >= 0 && n >= 0 && m < W && n < H) {
+          const float v = in[(size_t)n * W + m];
+          const uint8_t g = img[(size_t)n * W + m];
+          if (v != kInvalidFloat && fabsf(float(g - gc)) < sigma_r) {
+            const int dx = m - x, dy = n - y;
+            const float dist = (float)(g - gc);
+            const float wd = expf(-((dx * dx + dy * dy) / (2.0f * sigma_d * sigma_d)));
+            const float wr = (float)exp(-(dist * dist) / (2.0 * sigma_r * sigma_r));
+            const float w = wd * wr;
+            sum_w += w;
+            sum += w * v;
+          }
+        }
+    if (sum_w > 0.0f) result = sum / sum_w;
+  }
+  out[(size_t)y * W + x] = result;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) k_dilation(const T* __restrict__ in, T* __restrict__ out, int W, int H,
                                                   int wth) {

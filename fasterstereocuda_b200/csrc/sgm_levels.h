@@ -28,7 +28,7 @@ inline void level_options(const sgm_pyr_option1_t* o, const sgm_level_override_t
   so->unique_threshold = level == 0 ? 0.95f : 1.0f;
   so->lr_threshold = 1.0f;
   so->do_median_filter = true;
-  so->post_filter_type = 0;
+  so->post_filter_type = (level == 0 && o->do_smooth) ? 1 : 0;  // Gauss at the finest level
   so->using_constant_p2 = true;
   if (layers <= 1) {
     so->do_lr_check = o->do_lr_check;

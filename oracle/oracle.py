@@ -24,7 +24,8 @@ class _Cfg(C.Structure):
         ("do_lr_check", C.c_int32), ("lr_threshold", C.c_float), ("do_median", C.c_int32),
         ("morphology_dilation", C.c_int32), ("do_remove_peaks", C.c_int32), ("peaks_ratio", C.c_float),
         ("peaks_strips", C.c_int32), ("peaks_abs_mode", C.c_int32), ("tie_rule", C.c_int32),
-        ("init_tie_rule", C.c_int32), ("p2_div0", C.c_int32), ("threads", C.c_int32)]]
+        ("init_tie_rule", C.c_int32), ("p2_div0", C.c_int32), ("threads", C.c_int32),
+        ("post_filter", C.c_int32), ("morphology", C.c_int32)]]
 
 
 class _PyrCfg(C.Structure):
@@ -57,6 +58,8 @@ class Config:
     init_tie_rule: int = 4
     p2_div0: int = -1
     threads: int = 0
+    post_filter: int = 0
+    morphology: int = 0
 
     def c(self) -> _Cfg:
         s = _Cfg()

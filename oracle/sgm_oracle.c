@@ -462,6 +462,90 @@ void orc_median3x3(const float* in, float* out, int W, int H) {
   }
 }
 
+/* Erosion. cusgm_df.cu:165-195: an interior pixel (wth < x < W-wth, wth < y < H-wth) whose
+ * window holds an INVALID value becomes INVALID; every other pixel is copied. */
+void orc_erosion(const float* in, float* out, int W, int H, int wnd) {
+  const int wth = (wnd - 1) / 2;
+#pragma omp parallel for num_threads(nthreads()) schedule(static)
+  for (int y = 0; y < H; ++y) {
+    for (int x = 0; x < W; ++x) {
+      const float v = in[(size_t)y * W + x];
+      float mn = v;
+      if (x > wth && x < W - wth && y > wth && y < H - wth) {
+        for (int dx = -wth; dx <= wth; ++dx)
+          for (int dy = -wth; dy <= wth; ++dy) {
+            const float u = in[(size_t)(y + dy) * W + x + dx];
+            if (u < mn) mn = u;
+          }
+      }
+      out[(size_t)y * W + x] = mn == ORC_INVALID_FLOAT ? mn : v;
+    }
+  }
+}
+
+/* Range-limited Gaussian smoothing. cusgm_df.cu:93-121 (sigma_d 1.5, sigma_r 2.0 at :294):
+ * over a (2*ceil(2 sd)+1)^2 window (columns outer, rows inner), valid neighbours within sr of a
+ * valid centre weigh expf(-(dx^2+dy^2)/(2 sd^2)); INVALID when no weight. */
+void orc_gauss(const float* in, float* out, int W, int H, float sigma_d, float sigma_r) {
+  const int r = (int)ceil(2.0 * sigma_d);
+#pragma omp parallel for num_threads(nthreads()) schedule(static)
+  for (int y = 0; y < H; ++y) {
+    for (int x = 0; x < W; ++x) {
+      float result = ORC_INVALID_FLOAT, sum = 0.0f, sum_w = 0.0f;
+      const float c = in[(size_t)y * W + x];
+      if (c != ORC_INVALID_FLOAT) {
+        for (int m = x - r; m <= x + r; ++m)
+          for (int n = y - r; n <= y + r; ++n)
+            if (m >= 0 && n >= 0 && m < W && n < H) {
+              const float v = in[(size_t)n * W + m];
+              if (v != ORC_INVALID_FLOAT && fabsf(c - v) < sigma_r) {
+                const int dx = m - x, dy = n - y;
+                const float w = expf(-((float)(dx * dx + dy * dy) / (2.0f * sigma_d * sigma_d)));
+                sum_w += w;
+                sum = fmaf(w, v, sum);
+              }
+            }
+      }
+      if (sum_w > 0.0f) result = sum / sum_w;
+      out[(size_t)y * W + x] = result;
+    }
+  }
+}
+
+/* Bilateral smoothing guided by the left image. cusgm_df.cu:123-162 (sigma_d 2.5, sigma_r 10.0
+ * at :298): spatial weight times exp(-g^2/(2 sr^2)) of the grey difference g (in double) for
+ * valid neighbours with |g| < sr. */
+void orc_bilateral(const uint8_t* img, const float* in, float* out, int W, int H, float sigma_d, float sigma_r) {
+  const int r = (int)ceil(2.0 * sigma_d);
+#pragma omp parallel for num_threads(nthreads()) schedule(static)
+  for (int y = 0; y < H; ++y) {
+    for (int x = 0; x < W; ++x) {
+      float result = ORC_INVALID_FLOAT, sum = 0.0f, sum_w = 0.0f;
+      const float c = in[(size_t)y * W + x];
+      const int gc = img[(size_t)y * W + x];
+      if (c != ORC_INVALID_FLOAT) {
+        for (int m = x - r; m <= x + r; ++m)
+          for (int n = y - r; n <= y + r; ++n)
+            if (m >= 0 && n >= 0 && m < W && n < H) {
+              const float v = in[(size_t)n * W + m];
+              const int g = img[(size_t)n * W + m];
+              if (v != ORC_INVALID_FLOAT && fabsf((float)(g - gc)) < sigma_r) {
+                const int dx = m - x, dy = n - y;
+                const float dist = (float)(g - gc);
+                const float wd = expf(-((float)(dx * dx + dy * dy) / (2.0f * sigma_d * sigma_d)));
+                const float wr = (float)exp(-(double)(dist * dist) / (2.0 * sigma_r * sigma_r));
+                const float w = wd * wr;
+                sum_w += w;
+                sum = fmaf(w, v, sum);
+              }
+            }
+        if (sum_w > 0.0f) result = sum / sum_w;
+      }
+      out[(size_t)y * W + x] = result;
+    }
+  }
+}
+
 /* Dilation of INVALID pixels. cusgm_df.cu:197-222; window size rule :302-303.
  * An INVALID (or -32768) pixel with wth < x < W-wth and wth < y < H-wth takes the max
  * over its window; every other pixel is copied. */
@@ -694,11 +778,23 @@ int orc_match_dump(const orc_config_t* c, const uint8_t* left, const uint8_t* ri
     orc_median3x3(dl, tmp, W, H);
     memcpy(dl, tmp, sizeof(float) * N);
   }
-  if (c->morphology_dilation) {
-    const int s = W < H ? W : H;
-    const int wnd = s < 360 ? 3 : (s < 720 ? 5 : 7);
-    orc_dilation(dl, tmp, W, H, wnd);
+  if (c->post_filter == 1 || c->post_filter == 2) {
+    if (c->post_filter == 1) orc_gauss(dl, tmp, W, H, 1.5f, 2.0f);
+    else orc_bilateral(left, dl, tmp, W, H, 2.5f, 10.0f);
     memcpy(dl, tmp, sizeof(float) * N);
+  }
+  {
+    /* cusgm_df.cu:301-338: OPEN and CLOSE run both steps from the same input into the same
+     * output, leaving the dilation (OPEN) or the erosion (CLOSE) */
+    const int mp = c->morphology ? c->morphology : (c->morphology_dilation ? 2 : 0);
+    const int op = mp == 3 ? 2 : (mp == 4 ? 1 : mp);
+    if (op) {
+      const int s = W < H ? W : H;
+      const int wnd = s < 360 ? 3 : (s < 720 ? 5 : 7);
+      if (op == 2) orc_dilation(dl, tmp, W, H, wnd);
+      else orc_erosion(dl, tmp, W, H, wnd);
+      memcpy(dl, tmp, sizeof(float) * N);
+    }
   }
   if (c->do_remove_peaks) orc_remove_peaks(dl, W, H, c->peaks_strips, c->peaks_ratio, c->peaks_abs_mode);
   memcpy(disp_l, dl, sizeof(float) * N);
@@ -729,6 +825,8 @@ int orc_pyr_level_config(const orc_pyr_config_t* pc, int level, orc_config_t* o)
   o->uniqueness = level == 0 ? 0.95f : 1.0f;
   o->lr_threshold = 1.0f;
   o->do_median = 1;
+  o->post_filter = (level == 0 && pc->do_smooth) ? 1 : 0;
+  o->morphology = 0;
   if (layers <= 1) {
     o->do_lr_check = pc->do_lr_check;
     o->do_remove_peaks = pc->do_rm_peaks;

@@ -65,6 +65,8 @@ typedef struct {
   int32_t init_tie_rule;    /* init-disparity WTA tie rule */
   int32_t p2_div0;          /* value of P2 / 0 at init-disparity levels */
   int32_t threads;          /* OpenMP threads, <= 0: runtime default */
+  int32_t post_filter;      /* 0 none, 1 Gauss, 2 bilateral (after the median) */
+  int32_t morphology;       /* 0: as morphology_dilation; 1 erosion, 2 dilation, 3 open, 4 close */
 } orc_config_t;
 
 /* ---- stages ---- */
@@ -85,6 +87,9 @@ void orc_wta_init(const uint8_t* const paths[4], const int16_t* init, int W, int
 void orc_lr_check(float* disp_l, const float* disp_r_snapshot, float* disp_r_out, int W, int H, float threshold);
 void orc_median3x3(const float* in, float* out, int W, int H);
 void orc_dilation(const float* in, float* out, int W, int H, int wnd);
+void orc_erosion(const float* in, float* out, int W, int H, int wnd);
+void orc_gauss(const float* in, float* out, int W, int H, float sigma_d, float sigma_r);
+void orc_bilateral(const uint8_t* img, const float* in, float* out, int W, int H, float sigma_d, float sigma_r);
 int orc_remove_peaks(float* disp, int W, int H, int strips, float ratio, int abs_mode);
 int orc_remove_peaks_strip(float* disp, int w, int h, int threshold, int abs_mode);
 void orc_zoom_half(const uint8_t* src, int w_src, int h_src, uint8_t* dst);

@@ -68,7 +68,8 @@ def test_argument_errors_without_device(engine_lib):
     assert not s.Init(10, 10, 0, 0, opt) and s.status == -1
     assert not s.Init(100, 100, 0, 96, opt) and s.status == -4      # not 32/64/128/256
     assert not s.Init(100, 100, 0, 64, fsc.CuSGMOption(p1=-1)) and s.status == -1
-    assert not s.Init(100, 100, 0, 64, fsc.CuSGMOption(post_filter_type=1)) and s.status == -4
+    assert not s.Init(100, 100, 0, 64, fsc.CuSGMOption(post_filter_type=3)) and s.status == -1
+    assert not s.Init(100, 100, 0, 64, fsc.CuSGMOption(morphology_type=5)) and s.status == -1
     img = np.zeros((10, 10), np.uint8)
     d = np.zeros((10, 10), np.float32)
     s.width = s.height = 10

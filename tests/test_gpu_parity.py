@@ -353,3 +353,51 @@ def test_graph_replay_over_successive_matches(engine_lib, oracle_mod):
             pout = dout.cpu().numpy()
         assert_same(f"pyramid match {k}", pout, O.pyr_match(pc, L, R))
     assert s.kernel_launches() > 0 and p.kernel_launches() > 0
+
+
+@pytest.mark.parametrize("pf", [0, 1, 2])
+@pytest.mark.parametrize("morph", [0, 1, 2, 3, 4])
+def test_post_filters_and_morphology(engine_lib, oracle_mod, pf, morph):
+    """Gauss / bilateral post filters and erosion / dilation / open / close after the median
+    (reference DisparityFilter::Filter). Without a post filter the maps are bit-exact; the
+    filters weight by exp(), whose last bit may differ between CUDA and the host's libm, so
+    there INVALID masks must be identical and values within 1e-4 px."""
+    import fasterstereocuda_b200 as fsc
+    O = oracle_mod
+    W, H = 220, 150
+    L, R, _ = scenes.planar_pair(90 + pf + 3 * morph, W, H)
+    s = fsc.StereoCuda()
+    opt = fsc.CuSGMOption(p1=10, p2_init=150, cs_type=1, num_paths=4, do_median_filter=True, do_lr_check=True,
+                          lr_threshold=1.0, unique_threshold=0.95, using_constant_p2=True, post_filter_type=pf,
+                          morphology_type=morph)
+    assert s.Init(W, H, 0, 64, opt), s.last_error()
+    assert s.set_ext_options(fsc.ExtOptions(peaks_strips=STRIPS))
+    disp = np.empty((H, W), np.float32)
+    assert s.Match(L, R, disp), s.last_error()
+    ref = O.match(O.Config(width=W, height=H, disp_range=64, post_filter=pf, morphology=morph, peaks_strips=STRIPS),
+                  L, R)["disp"]
+    if pf == 0:
+        assert_same(f"pf0 morph{morph}", disp, ref)
+    else:
+        assert np.array_equal(disp == INV, ref == INV), int(((disp == INV) != (ref == INV)).sum())
+        ok = disp != INV
+        assert np.abs(disp[ok] - ref[ok]).max() <= 1e-4, np.abs(disp[ok] - ref[ok]).max()
+    assert (disp != INV).mean() > 0.3
+
+
+def test_pyramid_smoothing(engine_lib, oracle_mod):
+    """do_smooth: Gauss filter at the finest pyramid level (reference SetSgmParameters)."""
+    import fasterstereocuda_b200 as fsc
+    O = oracle_mod
+    W, H = 450, 375
+    L, R, _ = scenes.cone_like(16)
+    p = fsc.FasterStereoCuda()
+    assert p.Init(fsc.StereoOption1(width=W, height=H, min_disp=0, max_disp=64, num_layers=2, do_smooth=True),
+                  None, fsc.ExtOptions(peaks_strips=STRIPS)), p.last_error()
+    disp = np.empty((H, W), np.float32)
+    assert p.Match(L, R, disp), p.last_error()
+    ref = O.pyr_match(O.PyrConfig(width=W, height=H, max_disp=64, num_layers=2, do_smooth=1, override_enable=0,
+                                  peaks_strips=STRIPS), L, R)
+    assert np.array_equal(disp == INV, ref == INV)
+    ok = disp != INV
+    assert np.abs(disp[ok] - ref[ok]).max() <= 1e-4
