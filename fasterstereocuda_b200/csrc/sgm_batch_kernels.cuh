@@ -301,12 +301,7 @@ __global__ void __launch_bounds__(256) kb_cost3_init(const BatchPair* __restrict
 template <int G>
 __device__ __forceinline__ void init_scan_smem(uint32_t* p2tab, uint32_t* rows, const sgm::InitParams& P) {
   sgm::fill_p2_table(p2tab, P, threadIdx.x, blockDim.x);
-  uint32_t* row = rows + (threadIdx.x / G) * sgm::kIRow;
-  const uint32_t pad = sgm::kInvalidCost - P.p1;
-  for (int k = threadIdx.x % G; k < sgm::kIPad; k += G) {
-    row[k] = pad;
-    row[sgm::kIPad + 32 + k] = pad;
-  }
+  sgm::init_row_pad<G>(rows + (threadIdx.x / G) * sgm::kIRow, P.p1, true, threadIdx.x % G);
   __syncthreads();
 }
 

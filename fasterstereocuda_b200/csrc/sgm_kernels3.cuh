@@ -465,25 +465,45 @@ namespace sgm {
 // The realigned recurrence (reference cusgm_ca.cu:1181-1338): with s = base - last_base,
 //   L'(d) = C(d) + min(L(d), L(d+s-1)+P1, L(d+s+1)+P1, m+P2') - m        (uint32)
 // where an index outside [0, 32) gives the candidate 127 and P2' = max(P1, P2/|last_base-base+1|).
-// After a pixel with an INVALID base the reference sets m = 127 whatever the path costs are, so
-// t - m wraps and later steps see wrapped values: these kernels keep one uint32 per disparity
-// (no 16-bit packing) so that the wraparound is the reference's. The shifted neighbours come from
-// the scanline's old costs written to a shared-memory row padded with 127 - P1 (127 after + P1,
-// modulo 2^32 for any P1); shifts beyond +-33 read padding only.
+// After a pixel with an INVALID base the reference sets m = 127 whatever the path costs are, and
+// a realignment by more than the range makes every neighbour candidate 127, so t - m can wrap and
+// later steps see wrapped values.
+//
+// 16-bit form. Read every uint32 value v of the reference as the signed integer r with
+// v = r mod 2^32. While every value compared in a step has r in [-2^15, 2^15), the unsigned order
+// of v equals that of r mod 2^16 and sums agree modulo 2^16 (so in the stored low byte): the
+// recurrence can run on u16x2 words (two disparities per word, wrapping SIMD adds). With P1 >= 0,
+// every P2' <= kNarrowP2 and C <= 255:
+//   m >= 0: the candidate m + P2' is non-negative, so t is in [0, m + P2'] and L' in [-m, 255+P2'];
+//   m <  0: m is the least of values that are all negative, so every L is in [m, -1]; t is the
+//           least non-negative candidate (<= max(127, P2')) or a negative >= m, and L' is in
+//           [0, 382 + P2' + |m|].
+// A step that starts from |m| <= kNarrowM therefore compares values below 382 + 2*kNarrowP2 +
+// kNarrowM < 2^15. The kernels run a scanline in 16 bits while |m| <= kNarrowM after each step
+// (the sign-extended 16-bit minimum is exact) and otherwise continue it in 32 bits from the
+// sign-extended state, which is exact too. The switch is needed: realignments beyond the range
+// alternating with cost-255 pixels can grow |m| by up to 255 every two steps.
+// The shifted neighbours come from the scanline's old costs written to a shared-memory row padded
+// with 127 - P1 (127 after + P1, modulo 2^16 or 2^32 for any P1); shifts beyond +-33 read padding
+// only. 32-bit layout: kIPad words, 32 words, kIPad words. 16-bit layout (the first kIRow16 words
+// of the same row): 17 words (34 halves), 16 words, 18 words.
 // =============================================================================================
 constexpr int kIPad = 34;                      // padding words on each side of a scanline row
 constexpr int kIRow = kIPad + 32 + kIPad + 1;  // words per scanline row (odd: fewer bank conflicts)
 
+// byte j of the slice -> word j (one byte permute each)
 template <int ND>
 __device__ __forceinline__ void unpack_bytes(const uint32_t (&r)[ND / 4], uint32_t (&c)[ND]) {
 #pragma unroll
-  for (int j = 0; j < ND; ++j) c[j] = (r[j >> 2] >> (8 * (j & 3))) & 0xFFu;
+  for (int j = 0; j < ND; ++j) c[j] = __byte_perm(r[j >> 2], 0u, 0x4440u | (unsigned)(j & 3));
 }
+// low bytes of four words -> one word (three byte permutes)
 template <int ND>
 __device__ __forceinline__ void pack_bytes(const uint32_t (&L)[ND], uint32_t (&r)[ND / 4]) {
 #pragma unroll
   for (int i = 0; i < ND / 4; ++i)
-    r[i] = (L[4 * i] & 0xFFu) | ((L[4 * i + 1] & 0xFFu) << 8) | ((L[4 * i + 2] & 0xFFu) << 16) | (L[4 * i + 3] << 24);
+    r[i] = __byte_perm(__byte_perm(L[4 * i], L[4 * i + 1], 0x0040u), __byte_perm(L[4 * i + 2], L[4 * i + 3], 0x0040u),
+                       0x5410u);
 }
 
 template <int ND, int G>
@@ -528,6 +548,224 @@ __device__ __forceinline__ uint32_t init_step32(uint32_t (&L)[ND], const uint32_
 #pragma unroll
   for (int j = 0; j < ND; ++j) L[j] = nl[j];
   return group_min32<ND, G>(nl);
+}
+
+constexpr int kINPad = 17;                         // 16-bit layout: padding words on the left
+constexpr int kIRow16 = kINPad + 16 + kINPad + 1;  // 51 words; the last one is read at odd shifts
+constexpr int32_t kNarrowP2 = 8191, kNarrowM = 8192;
+
+// Penalties that keep a 16-bit step exact (P2' = max(P1, P2 / k) or max(P1, p2_div0)).
+__device__ __forceinline__ bool init_narrow_ok(const InitParams& P) {
+  return P.p1s >= 0 && P.p1s <= kNarrowP2 && P.p2s <= kNarrowP2 && P.p2_div0 <= kNarrowP2;
+}
+__device__ __forceinline__ uint32_t sext16(uint32_t v) { return (uint32_t)(int32_t)(int16_t)(uint16_t)v; }
+__device__ __forceinline__ bool narrow_m_ok(uint32_t m) {
+  return (int32_t)m <= kNarrowM && (int32_t)m >= -kNarrowM;
+}
+
+// Padding of one scanline row for the 16-bit or the 32-bit layout, by the scanline's G lanes.
+template <int G>
+__device__ __forceinline__ void init_row_pad(uint32_t* row, uint32_t p1, bool narrow16, int g) {
+  const uint32_t pad = kInvalidCost - p1;
+  if (narrow16) {
+    const uint32_t w = rep16(pad & 0xFFFFu);
+    for (int k = g; k < kINPad; k += G) row[k] = w;
+    for (int k = g; k < kINPad + 1; k += G) row[kINPad + 16 + k] = w;
+  } else {
+    for (int k = g; k < kIPad; k += G) {
+      row[k] = pad;
+      row[kIPad + 32 + k] = pad;
+    }
+  }
+}
+
+// One realigned step in 16 bits: L[0 .. ND/2) are this lane's u16x2 words (d = g*ND + 2k in the
+// low half), r its ND raw cost bytes; writes the new words to nl and returns the new minimum,
+// sign-extended. Every lane of the warp calls it. Requires |m| <= kNarrowM and p2t <= kNarrowP2.
+template <int ND, int G>
+__device__ __forceinline__ uint32_t init_step16(const uint32_t (&L)[ND], uint32_t (&nl)[ND / 2],
+                                                const uint32_t (&r)[ND / 4], uint32_t m, int s, uint32_t p2t,
+                                                uint32_t p1, uint32_t* row, int g) {
+  constexpr int NW = ND / 2;
+#pragma unroll
+  for (int k = 0; k < NW; ++k) row[kINPad + g * NW + k] = L[k];
+  __syncwarp();
+  const int sc = s < -33 ? -33 : (s > 33 ? 33 : s);
+  const int o = 2 * kINPad + g * ND + sc - 1;  // half index of old L(g*ND + s - 1), in [0, 98 - ND]
+  const uint32_t* src = row + (o >> 1);
+  const uint32_t sel = (o & 1) ? 0x5432u : 0x3210u;
+  uint32_t wd[NW + 2];
+#pragma unroll
+  for (int k = 0; k < NW + 2; ++k) wd[k] = src[k];
+  __syncwarp();
+  const uint32_t l4 = rep16((m + p2t) & 0xFFFFu);
+  const uint32_t p1x2 = rep16(p1 & 0xFFFFu);
+  const uint32_t mm = rep16(m & 0xFFFFu);
+  uint32_t a[NW + 1];  // min(old L(d + s - 1) + P1, m + P2') for the word's two d
+#pragma unroll
+  for (int k = 0; k < NW + 1; ++k) a[k] = __vminu2(__vadd2(__byte_perm(wd[k], wd[k + 1], sel), p1x2), l4);
+#pragma unroll
+  for (int k = 0; k < NW; ++k) {
+    const uint32_t t = __vimin3_u16x2(L[k], a[k], a[k + 1]);
+    const uint32_t c2 = (k & 1) ? widen_hi(r[k >> 1]) : widen_lo(r[k >> 1]);
+    nl[k] = __vadd2(c2, __vsub2(t, mm));
+  }
+  return sext16(group_min16<NW, G>(nl));
+}
+
+// 16-bit words -> one uint32 per disparity (in place, sign-extended: exact, see above).
+template <int ND>
+__device__ __forceinline__ void widen_state(uint32_t (&L)[ND]) {
+#pragma unroll
+  for (int k = ND / 2 - 1; k >= 0; --k) {
+    const uint32_t w = L[k];
+    L[2 * k + 1] = sext16(w >> 16);
+    L[2 * k] = sext16(w & 0xFFFFu);
+  }
+}
+
+// Stored path costs (low bytes) of the state, in either form.
+template <int ND>
+__device__ __forceinline__ void pack_state(const uint32_t (&L)[ND], bool wide, uint32_t (&out)[ND / 4]) {
+  if (wide) {
+    pack_bytes<ND>(L, out);
+  } else {
+#pragma unroll
+    for (int i = 0; i < ND / 4; ++i) out[i] = narrow(L[2 * i], L[2 * i + 1]);
+  }
+}
+
+// First pixel of a scanline: L = C. Returns min C over the scanline.
+template <int ND, int G>
+__device__ __forceinline__ uint32_t init_first(uint32_t (&L)[ND], const uint32_t (&r)[ND / 4], bool wide) {
+  if (wide) {
+    uint32_t c[ND];
+    unpack_bytes<ND>(r, c);
+#pragma unroll
+    for (int k = 0; k < ND; ++k) L[k] = c[k];
+    return group_min32<ND, G>(c);
+  }
+  uint32_t w[ND / 2];
+  widen_slice<ND / 4>(r, w);
+#pragma unroll
+  for (int k = 0; k < ND / 2; ++k) L[k] = w[k];
+  return group_min16<ND / 2, G>(w);
+}
+
+// One step of a scanline; keeps the result only for a valid base (else m = 127, L unchanged).
+// 16-bit form (L[0 .. ND/2) are u16x2 words):
+template <int ND, int G>
+__device__ __forceinline__ void init_advance16(uint32_t (&L)[ND], const uint32_t (&r)[ND / 4], uint32_t& m,
+                                               int& last_base, int base, const InitParams& P,
+                                               const uint32_t* p2tab, uint32_t* row, int g) {
+  uint32_t nl[ND / 2];
+  const uint32_t mn = init_step16<ND, G>(L, nl, r, m, base - last_base, p2_prime(p2tab, abs(last_base - base + 1), P),
+                                         P.p1, row, g);
+  if (base != kInvalidShort) {
+#pragma unroll
+    for (int k = 0; k < ND / 2; ++k) L[k] = nl[k];
+    m = mn;
+    last_base = base;
+  } else {
+    m = kInvalidCost;
+  }
+}
+// 32-bit form (one uint32 per disparity; the row holds the 32-bit padding):
+template <int ND, int G>
+__device__ __forceinline__ void init_advance32(uint32_t (&L)[ND], const uint32_t (&r)[ND / 4], uint32_t& m,
+                                               int& last_base, int base, const InitParams& P,
+                                               const uint32_t* p2tab, uint32_t* row, int g) {
+  uint32_t c[ND], Lk[ND];
+  unpack_bytes<ND>(r, c);
+#pragma unroll
+  for (int k = 0; k < ND; ++k) Lk[k] = L[k];
+  const uint32_t mn = init_step32<ND, G>(Lk, c, m, base - last_base, p2_prime(p2tab, abs(last_base - base + 1), P),
+                                         P.p1, row, g);
+  if (base != kInvalidShort) {
+#pragma unroll
+    for (int k = 0; k < ND; ++k) L[k] = Lk[k];
+    m = mn;
+    last_base = base;
+  } else {
+    m = kInvalidCost;
+  }
+}
+
+// Between scanlines the row holds the 16-bit padding. A scanline that continues in 32 bits
+// (from step `from`; 0: from its first pixel) widens its state and switches the padding, and
+// switches it back at its end. Warp-uniform.
+template <int ND, int G>
+__device__ __forceinline__ void init_go_wide(uint32_t (&L)[ND], int from, const InitParams& P, uint32_t* row,
+                                             int g) {
+  if (from > 0) widen_state<ND>(L);
+  __syncwarp();
+  init_row_pad<G>(row, P.p1, false, g);
+  __syncwarp();
+}
+template <int G>
+__device__ __forceinline__ void init_go_narrow(const InitParams& P, uint32_t* row, int g) {
+  __syncwarp();
+  init_row_pad<G>(row, P.p1, true, g);
+  __syncwarp();
+}
+
+// WTA of one pixel of an initial-disparity level from the u16x2 sums of its four paths
+// (reference Kernel_ComputeDisparityByWTA for initial disparities). ok: the pixel may be valid.
+template <int ND, int G>
+__device__ __forceinline__ void init_wta_pixel(const uint32_t (&S2)[ND / 2], uint32_t* colS, int g, int base,
+                                               bool ok, const WtaParams& Q, bool store, float* dst) {
+  constexpr int NW = ND / 2;
+#pragma unroll
+  for (int k = 0; k < NW; ++k) colS[g * NW + k] = S2[k];
+  const uint32_t sm = group_min16<NW, G>(S2);
+  __syncwarp();
+  const uint32_t sm2 = rep16(sm);
+  // lowest candidate d of this lane (and, for the reference rule, its uniqueness test)
+  int best = 64;
+  float bestv = kInvalidFloat;
+#pragma unroll
+  for (int k = 0; k < NW; ++k) {
+    const uint32_t eq = __vcmpeq2(S2[k], sm2);
+    if (eq != 0u && best == 64) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int d = g * ND + 2 * k + h;
+        if (((eq >> (16 * h)) & 1u) && best == 64) {
+          float v = kInvalidFloat;
+          if (d > 1 && d < kLevelRange - 1) {
+            const uint32_t w1 = colS[(d - 1) >> 1], w3 = colS[(d + 1) >> 1];
+            const float c1 = (float)((d - 1) & 1 ? w1 >> 16 : w1 & 0xFFFFu), c2 = (float)sm,
+                        c3 = (float)((d + 1) & 1 ? w3 >> 16 : w3 & 0xFFFFu);
+            const float d12 = __fsub_rn(c1, c2), d32 = __fsub_rn(c3, c2);
+            const float uq = d12 < d32 ? d12 : d32;
+            if (!(uq <= __fmul_rn(c2, __fsub_rn(1.0f, Q.uniqueness))))
+              v = __fadd_rn((float)(d + base), subpix_bias(c1, c2, c3));
+          }
+          if (Q.tie_rule == kTieRefB200) {
+            if (v != kInvalidFloat) { best = d; bestv = v; }
+          } else {
+            best = d;
+            bestv = v;
+          }
+        }
+      }
+    }
+  }
+  // group: the lane holding the lowest such d wins
+  int win = best;
+#pragma unroll
+  for (int o = 1; o < G; o *= 2) win = min(win, __shfl_xor_sync(kFull, win, o, G));
+  float dv = kInvalidFloat;
+  const uint32_t has = __ballot_sync(kFull, best == win && win < 64);
+  const int lane = threadIdx.x & 31;
+  const int gl = lane - g;  // first lane of this group
+  const uint32_t gmask = (G == 32 ? 0xFFFFFFFFu : ((1u << G) - 1u)) << gl;
+  const uint32_t mine = has & gmask;
+  const float vv = __shfl_sync(kFull, bestv, mine ? __ffs(mine) - 1 : lane);
+  if (mine) dv = vv;
+  if (!ok) dv = kInvalidFloat;
+  __syncwarp();
+  if (store && g == 0) *dst = dv;
 }
 
 // Cost volume of an initial-disparity level (reference cusgm_cc.cu:173-237 / 294-360):
@@ -609,56 +847,67 @@ __device__ __forceinline__ void hpaths3_init_lane(const uint8_t* __restrict__ co
   const int16_t* ib = (view == 0 ? init_l : init_r) + (size_t)y * W;
   const int xs = dir == 0 ? P.x0 : W - 1;
   const int dx = dir == 0 ? 1 : -1;
-  uint32_t L[ND], c[ND], out[NR];
-  uint32_t ring[PF][NR];
-  int rbase[PF];
-#pragma unroll
-  for (int j = 0; j < PF; ++j) {
-    if (j < len) {
-      ld_slice<NR>(crow + (size_t)(xs + j * dx) * kLevelRange, ring[j]);
-      rbase[j] = ib[xs + j * dx];
-    }
-  }
+  uint32_t L[ND], out[NR];
   uint32_t m = 0;
   int last_base = 0;
-  for (int s0 = 0; s0 < len; s0 += PF) {
+  // 16-bit steps with a PF-deep prefetch ring up to s_wide, 32-bit steps (plain loads) after it
+  int s_wide = init_narrow_ok(P) ? len : 0;
+  if (s_wide > 0) {
+    uint32_t ring[PF][NR];
+    int rbase[PF];
 #pragma unroll
     for (int j = 0; j < PF; ++j) {
-      const int s = s0 + j;
-      if (s < len) {
-        const int x = xs + s * dx;
-        unpack_bytes<ND>(ring[j], c);
-        const int base = rbase[j];
-        if (s + PF < len) {
-          ld_slice<NR>(crow + (size_t)(x + PF * dx) * kLevelRange, ring[j]);
-          rbase[j] = ib[x + PF * dx];
-        }
-        if (s == 0) {
-#pragma unroll
-          for (int k = 0; k < ND; ++k) L[k] = c[k];
-          m = group_min32<ND, G>(c);
-          last_base = base;
-        } else {
-          // computed by every lane (the exchange and the minimum are warp-wide); kept only for
-          // a valid base
-          uint32_t Lk[ND];
-#pragma unroll
-          for (int k = 0; k < ND; ++k) Lk[k] = L[k];
-          const int kk = abs(last_base - base + 1);
-          const uint32_t mn = init_step32<ND, G>(Lk, c, m, base - last_base, p2_prime(p2tab, kk, P), P.p1, row, g);
-          if (base != kInvalidShort) {
-#pragma unroll
-            for (int k = 0; k < ND; ++k) L[k] = Lk[k];
-            m = mn;
-            last_base = base;
-          } else {
-            m = kInvalidCost;
-          }
-        }
-        pack_bytes<ND>(L, out);
-        if (valid) st_slice<NR>(orow + (size_t)x * kLevelRange, out);
+      if (j < len) {
+        ld_slice<NR>(crow + (size_t)(xs + j * dx) * kLevelRange, ring[j]);
+        rbase[j] = ib[xs + j * dx];
       }
     }
+    for (int s0 = 0; s0 < s_wide; s0 += PF) {
+#pragma unroll
+      for (int j = 0; j < PF; ++j) {
+        const int s = s0 + j;
+        if (s < s_wide) {
+          const int x = xs + s * dx;
+          uint32_t r[NR];
+#pragma unroll
+          for (int k = 0; k < NR; ++k) r[k] = ring[j][k];
+          const int base = rbase[j];
+          if (s + PF < len) {
+            ld_slice<NR>(crow + (size_t)(x + PF * dx) * kLevelRange, ring[j]);
+            rbase[j] = ib[x + PF * dx];
+          }
+          if (s == 0) {
+            m = init_first<ND, G>(L, r, false);
+            last_base = base;
+          } else {
+            // every lane steps (the exchange and the minimum are warp-wide); kept for a valid base
+            init_advance16<ND, G>(L, r, m, last_base, base, P, p2tab, row, g);
+          }
+#pragma unroll
+          for (int i = 0; i < NR; ++i) out[i] = narrow(L[2 * i], L[2 * i + 1]);
+          if (valid) st_slice<NR>(orow + (size_t)x * kLevelRange, out);
+          if (__any_sync(kFull, !narrow_m_ok(m))) s_wide = s + 1;
+        }
+      }
+    }
+  }
+  if (s_wide < len) {
+    init_go_wide<ND, G>(L, s_wide, P, row, g);
+    for (int s = s_wide; s < len; ++s) {
+      const int x = xs + s * dx;
+      uint32_t r[NR];
+      ld_slice<NR>(crow + (size_t)x * kLevelRange, r);
+      const int base = ib[x];
+      if (s == 0) {
+        m = init_first<ND, G>(L, r, true);
+        last_base = base;
+      } else {
+        init_advance32<ND, G>(L, r, m, last_base, base, P, p2tab, row, g);
+      }
+      pack_bytes<ND>(L, out);
+      if (valid) st_slice<NR>(orow + (size_t)x * kLevelRange, out);
+    }
+    init_go_narrow<G>(P, row, g);
   }
 }
 
@@ -671,11 +920,7 @@ __global__ void __launch_bounds__(128) k_hpaths3_init(const uint8_t* __restrict_
   __shared__ uint32_t rows[(128 / G) * kIRow];
   fill_p2_table(p2tab, P, threadIdx.x, blockDim.x);
   uint32_t* row = rows + (threadIdx.x / G) * kIRow;
-  const uint32_t pad = kInvalidCost - P.p1;
-  for (int k = threadIdx.x % G; k < kIPad; k += G) {
-    row[k] = pad;
-    row[kIPad + 32 + k] = pad;
-  }
+  init_row_pad<G>(row, P.p1, true, threadIdx.x % G);
   __syncthreads();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   hpaths3_init_lane<G, PF>(cost, init_l, init_r, lr, rl, P, nviews, t / G, threadIdx.x % G, row, p2tab);
@@ -693,7 +938,7 @@ __device__ __forceinline__ void vpaths3_init_lane(const uint8_t* __restrict__ co
                                                   float* __restrict__ disp, const InitParams& P, const WtaParams& Q,
                                                   int view, int xc, int g, uint32_t* row, uint32_t* colS,
                                                   const uint32_t* p2tab) {
-  constexpr int ND = kLevelRange / G, NR = ND / 4;
+  constexpr int ND = kLevelRange / G, NR = ND / 4, NW = ND / 2;
   const int W = P.W, H = P.H;
   const bool valid = xc < W;
   const int x = valid ? xc : W - 1;
@@ -705,170 +950,153 @@ __device__ __forceinline__ void vpaths3_init_lane(const uint8_t* __restrict__ co
   const size_t rs = (size_t)W * kLevelRange;
   const uint8_t* cv = cost + vo;
   uint8_t* btv = bt + vo;
-  uint32_t L[ND], c[ND], out[NR];
-  uint32_t ring[PF][NR];
-  int rbase[PF];
+  const bool narrow_ok = init_narrow_ok(P);
+  uint32_t L[ND], out[NR];
   uint32_t m = 0;
   const int base0 = ib[0];
   int last_base = base0;
-  // bottom -> top
-#pragma unroll
-  for (int j = 0; j < PF; ++j) {
-    if (j < H) {
-      ld_slice<NR>(cv + (size_t)(H - 1 - j) * rs, ring[j]);
-      rbase[j] = ib[(size_t)(H - 1 - j) * W];
-    }
-  }
-  for (int s0 = 0; s0 < H; s0 += PF) {
+  // bottom -> top: 16-bit steps with a prefetch ring up to s_wide, then 32-bit steps
+  int s_wide = narrow_ok ? H : 0;
+  if (s_wide > 0) {
+    uint32_t ring[PF][NR];
+    int rbase[PF];
 #pragma unroll
     for (int j = 0; j < PF; ++j) {
-      const int s = s0 + j;
-      if (s < H) {
-        const int y = H - 1 - s;
-        unpack_bytes<ND>(ring[j], c);
-        const int base = rbase[j];
-        if (s + PF < H) {
-          ld_slice<NR>(cv + (size_t)(y - PF) * rs, ring[j]);
-          rbase[j] = ib[(size_t)(y - PF) * W];
-        }
-        bool store = true;
-        if (s == 0) {
+      if (j < H) {
+        ld_slice<NR>(cv + (size_t)(H - 1 - j) * rs, ring[j]);
+        rbase[j] = ib[(size_t)(H - 1 - j) * W];
+      }
+    }
+    for (int s0 = 0; s0 < s_wide; s0 += PF) {
 #pragma unroll
-          for (int k = 0; k < ND; ++k) L[k] = c[k];
-          m = group_min32<ND, G>(c);
-        } else {
-          uint32_t Lk[ND];
+      for (int j = 0; j < PF; ++j) {
+        const int s = s0 + j;
+        if (s < s_wide) {
+          const int y = H - 1 - s;
+          uint32_t r[NR];
 #pragma unroll
-          for (int k = 0; k < ND; ++k) Lk[k] = L[k];
-          const uint32_t mn = init_step32<ND, G>(Lk, c, m, base - last_base,
-                                                 p2_prime(p2tab, abs(last_base - base + 1), P), P.p1, row, g);
-          if (base != kInvalidShort) {
-#pragma unroll
-            for (int k = 0; k < ND; ++k) L[k] = Lk[k];
-            m = mn;
-            last_base = base;
-          } else {
-            m = kInvalidCost;
-            store = false;
+          for (int k = 0; k < NR; ++k) r[k] = ring[j][k];
+          const int base = rbase[j];
+          if (s + PF < H) {
+            ld_slice<NR>(cv + (size_t)(y - PF) * rs, ring[j]);
+            rbase[j] = ib[(size_t)(y - PF) * W];
           }
-        }
-        if (store && computed) {
-          pack_bytes<ND>(L, out);
-          st_slice<NR>(btv + (size_t)y * rs, out);
+          if (s == 0) m = init_first<ND, G>(L, r, false);
+          else init_advance16<ND, G>(L, r, m, last_base, base, P, p2tab, row, g);
+          if ((s == 0 || base != kInvalidShort) && computed) {
+#pragma unroll
+            for (int i = 0; i < NR; ++i) out[i] = narrow(L[2 * i], L[2 * i + 1]);
+            st_slice<NR>(btv + (size_t)y * rs, out);
+          }
+          if (__any_sync(kFull, !narrow_m_ok(m))) s_wide = s + 1;
         }
       }
     }
   }
-  // top -> bottom + sum + WTA
+  if (s_wide < H) {
+    init_go_wide<ND, G>(L, s_wide, P, row, g);
+    for (int s = s_wide; s < H; ++s) {
+      const int y = H - 1 - s;
+      uint32_t r[NR];
+      ld_slice<NR>(cv + (size_t)y * rs, r);
+      const int base = ib[(size_t)y * W];
+      if (s == 0) m = init_first<ND, G>(L, r, true);
+      else init_advance32<ND, G>(L, r, m, last_base, base, P, p2tab, row, g);
+      if ((s == 0 || base != kInvalidShort) && computed) {
+        pack_bytes<ND>(L, out);
+        st_slice<NR>(btv + (size_t)y * rs, out);
+      }
+    }
+    init_go_narrow<G>(P, row, g);
+  }
+  // top -> bottom + sum + WTA (a new scanline)
   const uint8_t* lrv = lr + vo;
   const uint8_t* rlv = rl + vo;
   last_base = base0;
-  uint32_t ra[PF][NR], rb[PF][NR], re[PF][NR];
-#pragma unroll
-  for (int j = 0; j < PF; ++j) {
-    if (j < H) {
-      const size_t o = (size_t)j * rs;
-      ld_slice<NR>(cv + o, ring[j]);
-      ld_slice<NR>(btv + o, ra[j]);
-      ld_slice<NR>(lrv + o, rb[j]);
-      ld_slice<NR>(rlv + o, re[j]);
-      rbase[j] = ib[(size_t)j * W];
-    }
-  }
-  for (int y0 = 0; y0 < H; y0 += PF) {
+  int y_wide = narrow_ok ? H : 0;
+  if (y_wide > 0) {
+    uint32_t ring[PF][NR], ra[PF][NR], rb[PF][NR], re[PF][NR];
+    int rbase[PF];
 #pragma unroll
     for (int j = 0; j < PF; ++j) {
-      const int y = y0 + j;
-      if (y < H) {
-        uint32_t a[ND], b[ND], e[ND];
-        unpack_bytes<ND>(ring[j], c);
-        unpack_bytes<ND>(ra[j], a);
-        unpack_bytes<ND>(rb[j], b);
-        unpack_bytes<ND>(re[j], e);
-        const int base = rbase[j];
-        if (y + PF < H) {
-          const size_t o = (size_t)(y + PF) * rs;
-          ld_slice<NR>(cv + o, ring[j]);
-          ld_slice<NR>(btv + o, ra[j]);
-          ld_slice<NR>(lrv + o, rb[j]);
-          ld_slice<NR>(rlv + o, re[j]);
-          rbase[j] = ib[(size_t)(y + PF) * W];
-        }
-        bool skipped = false;
-        if (y == 0) {
+      if (j < H) {
+        const size_t o = (size_t)j * rs;
+        ld_slice<NR>(cv + o, ring[j]);
+        ld_slice<NR>(btv + o, ra[j]);
+        ld_slice<NR>(lrv + o, rb[j]);
+        ld_slice<NR>(rlv + o, re[j]);
+        rbase[j] = ib[(size_t)j * W];
+      }
+    }
+    for (int y0 = 0; y0 < y_wide; y0 += PF) {
 #pragma unroll
-          for (int k = 0; k < ND; ++k) L[k] = c[k];
-          m = group_min32<ND, G>(c);
-        } else {
-          uint32_t Lk[ND];
+      for (int j = 0; j < PF; ++j) {
+        const int y = y0 + j;
+        if (y < y_wide) {
+          uint32_t r[NR], S2[NW];
 #pragma unroll
-          for (int k = 0; k < ND; ++k) Lk[k] = L[k];
-          const uint32_t mn = init_step32<ND, G>(Lk, c, m, base - last_base,
-                                                 p2_prime(p2tab, abs(last_base - base + 1), P), P.p1, row, g);
-          if (base != kInvalidShort) {
-#pragma unroll
-            for (int k = 0; k < ND; ++k) L[k] = Lk[k];
-            m = mn;
-            last_base = base;
-          } else {
-            m = kInvalidCost;
-            skipped = true;
+          for (int k = 0; k < NR; ++k) {
+            r[k] = ring[j][k];
+            // sums of the three stored paths, two disparities per word (each half <= 765)
+            S2[2 * k] = widen_lo(ra[j][k]) + widen_lo(rb[j][k]) + widen_lo(re[j][k]);
+            S2[2 * k + 1] = widen_hi(ra[j][k]) + widen_hi(rb[j][k]) + widen_hi(re[j][k]);
           }
-        }
-        if (y >= 5 && y <= H - 5 && y < Q.rows) {  // uniform over the warp
-          uint32_t S[ND];
-          uint32_t lm = 0xFFFFFFFFu;
-#pragma unroll
-          for (int k = 0; k < ND; ++k) {
-            S[k] = (L[k] & 0xFFu) + a[k] + b[k] + e[k];
-            colS[g * ND + k] = S[k];
-            lm = min(lm, S[k]);
+          const int base = rbase[j];
+          if (y + PF < H) {
+            const size_t o = (size_t)(y + PF) * rs;
+            ld_slice<NR>(cv + o, ring[j]);
+            ld_slice<NR>(btv + o, ra[j]);
+            ld_slice<NR>(lrv + o, rb[j]);
+            ld_slice<NR>(rlv + o, re[j]);
+            rbase[j] = ib[(size_t)(y + PF) * W];
           }
-          const uint32_t sm = group_min<G>(lm);
-          __syncwarp();
-          // lowest candidate d of this lane (and, for the reference rule, its uniqueness test)
-          int best = 64;
-          float bestv = kInvalidFloat;
+          if (y == 0) m = init_first<ND, G>(L, r, false);
+          else init_advance16<ND, G>(L, r, m, last_base, base, P, p2tab, row, g);
+          const bool skipped = y > 0 && base == kInvalidShort;
+          if (y >= 5 && y <= H - 5 && y < Q.rows) {  // uniform over the warp
 #pragma unroll
-          for (int k = 0; k < ND; ++k) {
-            const int d = g * ND + k;
-            if (S[k] == sm && best == 64) {
-              float v = kInvalidFloat;
-              if (d > 1 && d < kLevelRange - 1) {
-                const float c1 = (float)colS[d - 1], c2 = (float)sm, c3 = (float)colS[d + 1];
-                const float d12 = __fsub_rn(c1, c2), d32 = __fsub_rn(c3, c2);
-                const float uq = d12 < d32 ? d12 : d32;
-                if (!(uq <= __fmul_rn(c2, __fsub_rn(1.0f, Q.uniqueness))))
-                  v = __fadd_rn((float)(d + base), subpix_bias(c1, c2, c3));
-              }
-              if (Q.tie_rule == kTieRefB200) {
-                if (v != kInvalidFloat) { best = d; bestv = v; }
-              } else {
-                best = d;
-                bestv = v;
-              }
-            }
+            for (int k = 0; k < NW; ++k) S2[k] += L[k] & 0x00FF00FFu;  // + this path (<= 1020 per half)
+            init_wta_pixel<ND, G>(S2, colS, g, base, col_ok && base != kInvalidShort && !skipped, Q, valid,
+                                  dout + (size_t)y * W);
+          } else if (valid && g == 0) {
+            dout[(size_t)y * W] = kInvalidFloat;
           }
-          // group: the lane holding the lowest such d wins
-          int win = best;
-#pragma unroll
-          for (int o = 1; o < G; o *= 2) win = min(win, __shfl_xor_sync(kFull, win, o, G));
-          float dv = kInvalidFloat;
-          const uint32_t has = __ballot_sync(kFull, best == win && win < 64);
-          const int lane = threadIdx.x & 31;
-          const int gl = lane - g;  // first lane of this group
-          const uint32_t gmask = (G == 32 ? 0xFFFFFFFFu : ((1u << G) - 1u)) << gl;
-          const uint32_t mine = has & gmask;
-          const float vv = __shfl_sync(kFull, bestv, mine ? __ffs(mine) - 1 : lane);
-          if (mine) dv = vv;
-          if (!(col_ok && base != kInvalidShort && !skipped)) dv = kInvalidFloat;
-          __syncwarp();
-          if (valid && g == 0) dout[(size_t)y * W] = dv;
-        } else if (valid && g == 0) {
-          dout[(size_t)y * W] = kInvalidFloat;
+          if (__any_sync(kFull, !narrow_m_ok(m))) y_wide = y + 1;
         }
       }
     }
+  }
+  if (y_wide < H) {
+    init_go_wide<ND, G>(L, y_wide, P, row, g);
+    for (int y = y_wide; y < H; ++y) {
+      const size_t o = (size_t)y * rs;
+      uint32_t r[NR], S2[NW];
+      ld_slice<NR>(cv + o, r);
+      {
+        uint32_t qa[NR], qb[NR], qe[NR];
+        ld_slice<NR>(btv + o, qa);
+        ld_slice<NR>(lrv + o, qb);
+        ld_slice<NR>(rlv + o, qe);
+#pragma unroll
+        for (int k = 0; k < NR; ++k) {
+          S2[2 * k] = widen_lo(qa[k]) + widen_lo(qb[k]) + widen_lo(qe[k]);
+          S2[2 * k + 1] = widen_hi(qa[k]) + widen_hi(qb[k]) + widen_hi(qe[k]);
+        }
+      }
+      const int base = ib[(size_t)y * W];
+      if (y == 0) m = init_first<ND, G>(L, r, true);
+      else init_advance32<ND, G>(L, r, m, last_base, base, P, p2tab, row, g);
+      const bool skipped = y > 0 && base == kInvalidShort;
+      if (y >= 5 && y <= H - 5 && y < Q.rows) {
+#pragma unroll
+        for (int k = 0; k < NW; ++k) S2[k] += (L[2 * k] & 0xFFu) | ((L[2 * k + 1] & 0xFFu) << 16);
+        init_wta_pixel<ND, G>(S2, colS, g, base, col_ok && base != kInvalidShort && !skipped, Q, valid,
+                              dout + (size_t)y * W);
+      } else if (valid && g == 0) {
+        dout[(size_t)y * W] = kInvalidFloat;
+      }
+    }
+    init_go_narrow<G>(P, row, g);
   }
 }
 
@@ -883,11 +1111,7 @@ __global__ void __launch_bounds__(128) k_vpaths3_init(const uint8_t* __restrict_
   __shared__ uint32_t sums[(128 / G) * 33];
   fill_p2_table(p2tab, P, threadIdx.x, blockDim.x);
   uint32_t* row = rows + (threadIdx.x / G) * kIRow;
-  const uint32_t pad = kInvalidCost - P.p1;
-  for (int k = threadIdx.x % G; k < kIPad; k += G) {
-    row[k] = pad;
-    row[kIPad + 32 + k] = pad;
-  }
+  init_row_pad<G>(row, P.p1, true, threadIdx.x % G);
   __syncthreads();
   const int xc = (blockIdx.x * blockDim.x + threadIdx.x) / G;
   vpaths3_init_lane<G, PF>(cost, lr, rl, init_l, init_r, bt, disp, P, Q, blockIdx.y, xc, threadIdx.x % G, row,
