@@ -85,10 +85,12 @@ __device__ __forceinline__ uint32_t group_min16(const uint32_t (&v)[NT]) {
   uint32_t t[NT];
 #pragma unroll
   for (int k = 0; k < NT; ++k) t[k] = v[k];
+  // ternary tree of 3-input SIMD minima
 #pragma unroll
-  for (int st = 1; st < NT; st *= 2) {
+  for (int st = 1; st < NT; st *= 3) {
 #pragma unroll
-    for (int k = 0; k + st < NT; k += 2 * st) t[k] = min16x2(t[k], t[k + st]);
+    for (int k = 0; k + st < NT; k += 3 * st)
+      t[k] = k + 2 * st < NT ? __vimin3_u16x2(t[k], t[k + st], t[k + 2 * st]) : min16x2(t[k], t[k + st]);
   }
   uint32_t r = hmin16(t[0]);
 #pragma unroll
@@ -598,17 +600,20 @@ __device__ __forceinline__ uint32_t init_step16(const uint32_t (&L)[ND], uint32_
 #pragma unroll
   for (int k = 0; k < NW + 2; ++k) wd[k] = src[k];
   __syncwarp();
+  // __viaddmin_u16x2(a, b, c) = min((a + b) mod 2^16, c) per half; with c = 0xFFFF it is the
+  // wrapping add (the wrap of the add is what the exactness argument needs; the wrapping tests
+  // of these kernels reach it)
   const uint32_t l4 = rep16((m + p2t) & 0xFFFFu);
   const uint32_t p1x2 = rep16(p1 & 0xFFFFu);
-  const uint32_t mm = rep16(m & 0xFFFFu);
+  const uint32_t negm = rep16((0u - m) & 0xFFFFu);
   uint32_t a[NW + 1];  // min(old L(d + s - 1) + P1, m + P2') for the word's two d
 #pragma unroll
-  for (int k = 0; k < NW + 1; ++k) a[k] = __vminu2(__vadd2(__byte_perm(wd[k], wd[k + 1], sel), p1x2), l4);
+  for (int k = 0; k < NW + 1; ++k) a[k] = __viaddmin_u16x2(__byte_perm(wd[k], wd[k + 1], sel), p1x2, l4);
 #pragma unroll
   for (int k = 0; k < NW; ++k) {
-    const uint32_t t = __vimin3_u16x2(L[k], a[k], a[k + 1]);
     const uint32_t c2 = (k & 1) ? widen_hi(r[k >> 1]) : widen_lo(r[k >> 1]);
-    nl[k] = __vadd2(c2, __vsub2(t, mm));
+    const uint32_t cm = __viaddmin_u16x2(c2, negm, 0xFFFFFFFFu);  // C - m
+    nl[k] = __viaddmin_u16x2(__vimin3_u16x2(L[k], a[k], a[k + 1]), cm, 0xFFFFFFFFu);
   }
   return sext16(group_min16<NW, G>(nl));
 }
@@ -711,58 +716,44 @@ __device__ __forceinline__ void init_go_narrow(const InitParams& P, uint32_t* ro
 
 // WTA of one pixel of an initial-disparity level from the u16x2 sums of its four paths
 // (reference Kernel_ComputeDisparityByWTA for initial disparities). ok: the pixel may be valid.
+// Keys S*32 + d (S <= 1020) fit 16 bits: their minimum is the lowest d of least S. Rule
+// kTieRefB200: the lowest tied d whose uniqueness test passes; kTieLowest: the lowest tied d.
+__device__ __forceinline__ float init_candidate(const uint32_t* colS, int d, uint32_t sm, int base,
+                                                const WtaParams& Q) {
+  if (d <= 1 || d >= kLevelRange - 1) return kInvalidFloat;
+  const uint32_t w1 = colS[(d - 1) >> 1], w3 = colS[(d + 1) >> 1];
+  const float c1 = (float)((d - 1) & 1 ? w1 >> 16 : w1 & 0xFFFFu), c2 = (float)sm,
+              c3 = (float)((d + 1) & 1 ? w3 >> 16 : w3 & 0xFFFFu);
+  const float d12 = __fsub_rn(c1, c2), d32 = __fsub_rn(c3, c2);
+  const float uq = d12 < d32 ? d12 : d32;
+  if (uq <= __fmul_rn(c2, __fsub_rn(1.0f, Q.uniqueness))) return kInvalidFloat;
+  return __fadd_rn((float)(d + base), subpix_bias(c1, c2, c3));
+}
 template <int ND, int G>
 __device__ __forceinline__ void init_wta_pixel(const uint32_t (&S2)[ND / 2], uint32_t* colS, int g, int base,
                                                bool ok, const WtaParams& Q, bool store, float* dst) {
   constexpr int NW = ND / 2;
-#pragma unroll
-  for (int k = 0; k < NW; ++k) colS[g * NW + k] = S2[k];
-  const uint32_t sm = group_min16<NW, G>(S2);
-  __syncwarp();
-  const uint32_t sm2 = rep16(sm);
-  // lowest candidate d of this lane (and, for the reference rule, its uniqueness test)
-  int best = 64;
-  float bestv = kInvalidFloat;
+  const uint32_t d0 = (uint32_t)(g * ND) * 0x10001u + 0x10000u;  // (d, d + 1) of word 0
+  uint32_t key[NW];
 #pragma unroll
   for (int k = 0; k < NW; ++k) {
-    const uint32_t eq = __vcmpeq2(S2[k], sm2);
-    if (eq != 0u && best == 64) {
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int d = g * ND + 2 * k + h;
-        if (((eq >> (16 * h)) & 1u) && best == 64) {
-          float v = kInvalidFloat;
-          if (d > 1 && d < kLevelRange - 1) {
-            const uint32_t w1 = colS[(d - 1) >> 1], w3 = colS[(d + 1) >> 1];
-            const float c1 = (float)((d - 1) & 1 ? w1 >> 16 : w1 & 0xFFFFu), c2 = (float)sm,
-                        c3 = (float)((d + 1) & 1 ? w3 >> 16 : w3 & 0xFFFFu);
-            const float d12 = __fsub_rn(c1, c2), d32 = __fsub_rn(c3, c2);
-            const float uq = d12 < d32 ? d12 : d32;
-            if (!(uq <= __fmul_rn(c2, __fsub_rn(1.0f, Q.uniqueness))))
-              v = __fadd_rn((float)(d + base), subpix_bias(c1, c2, c3));
-          }
-          if (Q.tie_rule == kTieRefB200) {
-            if (v != kInvalidFloat) { best = d; bestv = v; }
-          } else {
-            best = d;
-            bestv = v;
-          }
-        }
+    colS[g * NW + k] = S2[k];
+    key[k] = (S2[k] << 5) + d0 + (uint32_t)(2 * k) * 0x10001u;
+  }
+  const uint32_t kmin = group_min16<NW, G>(key);
+  __syncwarp();
+  const uint32_t sm = kmin >> 5;
+  const int ds = (int)(kmin & 31u);
+  float dv = init_candidate(colS, ds, sm, base, Q);  // the same in every lane of the group
+  if (dv == kInvalidFloat && Q.tie_rule == kTieRefB200) {
+    for (int d = ds + 1; d < kLevelRange - 1; ++d) {  // rare: a later tied d that passes
+      const uint32_t w = colS[d >> 1];
+      if (((d & 1) ? w >> 16 : w & 0xFFFFu) == sm) {
+        dv = init_candidate(colS, d, sm, base, Q);
+        if (dv != kInvalidFloat) break;
       }
     }
   }
-  // group: the lane holding the lowest such d wins
-  int win = best;
-#pragma unroll
-  for (int o = 1; o < G; o *= 2) win = min(win, __shfl_xor_sync(kFull, win, o, G));
-  float dv = kInvalidFloat;
-  const uint32_t has = __ballot_sync(kFull, best == win && win < 64);
-  const int lane = threadIdx.x & 31;
-  const int gl = lane - g;  // first lane of this group
-  const uint32_t gmask = (G == 32 ? 0xFFFFFFFFu : ((1u << G) - 1u)) << gl;
-  const uint32_t mine = has & gmask;
-  const float vv = __shfl_sync(kFull, bestv, mine ? __ffs(mine) - 1 : lane);
-  if (mine) dv = vv;
   if (!ok) dv = kInvalidFloat;
   __syncwarp();
   if (store && g == 0) *dst = dv;
