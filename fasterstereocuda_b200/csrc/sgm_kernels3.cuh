@@ -374,14 +374,39 @@ __device__ __forceinline__ void vpaths3_lane(const uint8_t* __restrict__ cost, c
           // stores; D = 128: d < 64 and d >= 64.
           constexpr int SPLIT = D == 32 ? 64 : (D == 64 ? 32 : 64);  // first d of the second block
           uint32_t acc0 = 0xFFFFFFFFu, acc1 = 0xFFFFFFFFu;
+          if constexpr (G > 1) {
+            // every d of this lane lies in one block: one tree of SIMD minima
+            uint32_t key[NT];
+            const uint32_t dl = (uint32_t)((g * SB) & 63) * 0x10001u + 0x10000u;  // (d, d+1) mod 64 of word 0
 #pragma unroll
-          for (int k = 0; k < NT; ++k) {
-            const uint32_t sk = (L[k] & 0x00FF00FFu) + wa[k] + wb[k] + we[k];
-            myS[k] = sk;
-            const uint32_t d0 = (uint32_t)(2 * (g * NT + k));
-            const uint32_t key = sk * 64u + ((d0 & 63u) | (((d0 + 1u) & 63u) << 16));
-            if ((int)d0 < SPLIT) acc0 = min16x2(acc0, key);
-            else acc1 = min16x2(acc1, key);
+            for (int k = 0; k < NT; ++k) {
+              const uint32_t sk = (L[k] & 0x00FF00FFu) + wa[k] + wb[k] + we[k];
+              myS[k] = sk;
+              key[k] = sk * 64u + dl + (uint32_t)(2 * k) * 0x10001u;
+            }
+            uint32_t t = key[0];
+            if constexpr (NT > 1) {
+#pragma unroll
+              for (int st = 1; st < NT; st *= 3) {
+#pragma unroll
+                for (int k = 0; k + st < NT; k += 3 * st)
+                  key[k] = k + 2 * st < NT ? __vimin3_u16x2(key[k], key[k + st], key[k + 2 * st])
+                                           : min16x2(key[k], key[k + st]);
+              }
+              t = key[0];
+            }
+            if (g * SB < SPLIT) acc0 = t;
+            else acc1 = t;
+          } else {
+#pragma unroll
+            for (int k = 0; k < NT; ++k) {
+              const uint32_t sk = (L[k] & 0x00FF00FFu) + wa[k] + wb[k] + we[k];
+              myS[k] = sk;
+              const uint32_t d0 = (uint32_t)(2 * (g * NT + k));
+              const uint32_t key = sk * 64u + ((d0 & 63u) | (((d0 + 1u) & 63u) << 16));
+              if ((int)d0 < SPLIT) acc0 = min16x2(acc0, key);
+              else acc1 = min16x2(acc1, key);
+            }
           }
           const uint32_t k0 = group_min<G>(hmin16(acc0)), k1 = group_min<G>(hmin16(acc1));
           __syncwarp();
@@ -394,9 +419,10 @@ __device__ __forceinline__ void vpaths3_lane(const uint8_t* __restrict__ cost, c
             const uint32_t SA = k0 >> 6, SB2 = k1 >> 6;
             sm = min(SA, SB2);
             ds = (int)(min(k0, k1) & 63);  // lowest d among the minima
-            if (Q.tie_rule == kTieRefB200) {
-              // A non-empty: odd rows take A; even rows take B = {t : S(t+32) == m, S(t) != m}
-              // when non-empty (computed by every lane; the shuffles must not diverge)
+            // A non-empty: odd rows take A; even rows take B = {t : S(t+32) == m, S(t) != m}
+            // when non-empty, which needs the minimum in both blocks (rare); computed by every
+            // lane of a warp where one column needs it (the shuffles must not diverge)
+            if (Q.tie_rule == kTieRefB200 && (y & 1) == 0 && __any_sync(kFull, SA == SB2)) {
               const uint32_t mm = rep16(sm);
               uint32_t ax = 0xFFFFFFFFu;
 #pragma unroll
@@ -480,9 +506,11 @@ namespace sgm {
 //   m <  0: m is the least of values that are all negative, so every L is in [m, -1]; t is the
 //           least non-negative candidate (<= max(127, P2')) or a negative >= m, and L' is in
 //           [0, 382 + P2' + |m|].
-// A step that starts from |m| <= kNarrowM therefore compares values below 382 + 2*kNarrowP2 +
-// kNarrowM < 2^15. The kernels run a scanline in 16 bits while |m| <= kNarrowM after each step
-// (the sign-extended 16-bit minimum is exact) and otherwise continue it in 32 bits from the
+// So |m| grows by at most 382 + P2max per step, and a step that starts from |m| = M compares
+// values below M + 382 + 2*P2max. The kernels check |m| <= kNarrowM once per block of up to
+// kNarrowBlock steps: a block that starts there stays below kNarrowM + 8*(382 + P2max) + P2max
+// = 29671 < 2^15 for P2max = kNarrowP2 = 2047. A scanline runs in 16 bits while the check
+// holds (the sign-extended 16-bit minimum is exact) and otherwise continues in 32 bits from the
 // sign-extended state, which is exact too. The switch is needed: realignments beyond the range
 // alternating with cost-255 pixels can grow |m| by up to 255 every two steps.
 // The shifted neighbours come from the scanline's old costs written to a shared-memory row padded
@@ -554,7 +582,8 @@ __device__ __forceinline__ uint32_t init_step32(uint32_t (&L)[ND], const uint32_
 
 constexpr int kINPad = 17;                         // 16-bit layout: padding words on the left
 constexpr int kIRow16 = kINPad + 16 + kINPad + 1;  // 51 words; the last one is read at odd shifts
-constexpr int32_t kNarrowP2 = 8191, kNarrowM = 8192;
+constexpr int32_t kNarrowP2 = 2047, kNarrowM = 8192;
+constexpr int kNarrowBlock = 8;  // steps between two checks of |m| (the prefetch depth)
 
 // Penalties that keep a 16-bit step exact (P2' = max(P1, P2 / k) or max(P1, p2_div0)).
 __device__ __forceinline__ bool init_narrow_ok(const InitParams& P) {
@@ -583,7 +612,8 @@ __device__ __forceinline__ void init_row_pad(uint32_t* row, uint32_t p1, bool na
 
 // One realigned step in 16 bits: L[0 .. ND/2) are this lane's u16x2 words (d = g*ND + 2k in the
 // low half), r its ND raw cost bytes; writes the new words to nl and returns the new minimum,
-// sign-extended. Every lane of the warp calls it. Requires |m| <= kNarrowM and p2t <= kNarrowP2.
+// sign-extended. Every lane of the warp calls it. Requires p2t <= kNarrowP2 and |m| within the
+// bound of its block (see above).
 template <int ND, int G>
 __device__ __forceinline__ uint32_t init_step16(const uint32_t (&L)[ND], uint32_t (&nl)[ND / 2],
                                                 const uint32_t (&r)[ND / 4], uint32_t m, int s, uint32_t p2t,
@@ -745,12 +775,22 @@ __device__ __forceinline__ void init_wta_pixel(const uint32_t (&S2)[ND / 2], uin
   const uint32_t sm = kmin >> 5;
   const int ds = (int)(kmin & 31u);
   float dv = init_candidate(colS, ds, sm, base, Q);  // the same in every lane of the group
-  if (dv == kInvalidFloat && Q.tie_rule == kTieRefB200) {
-    for (int d = ds + 1; d < kLevelRange - 1; ++d) {  // rare: a later tied d that passes
-      const uint32_t w = colS[d >> 1];
-      if (((d & 1) ? w >> 16 : w & 0xFFFFu) == sm) {
-        dv = init_candidate(colS, d, sm, base, Q);
-        if (dv != kInvalidFloat) break;
+  if (Q.tie_rule == kTieRefB200) {
+    // while the candidate fails: the next tied d, i.e. the least key above kcur and below
+    // (sm + 1) * 32 (keys <= kcur wrap to >= 2^15 in key - kcur - 1)
+    const uint32_t lim = (sm + 1u) << 5;
+    uint32_t kcur = kmin;
+    for (;;) {
+      const bool need = dv == kInvalidFloat && kcur + 1u < lim;
+      if (!__any_sync(kFull, need)) break;
+      const uint32_t neg = rep16((0u - (kcur + 1u)) & 0xFFFFu);
+      uint32_t u[NW];
+#pragma unroll
+      for (int k = 0; k < NW; ++k) u[k] = __viaddmin_u16x2(key[k], neg, 0xFFFFFFFFu);
+      const uint32_t nk = group_min16<NW, G>(u) + kcur + 1u;
+      if (need) {
+        kcur = nk < lim ? nk : lim;
+        if (nk < lim) dv = init_candidate(colS, (int)(nk & 31u), sm, base, Q);
       }
     }
   }
@@ -843,6 +883,7 @@ __device__ __forceinline__ void hpaths3_init_lane(const uint8_t* __restrict__ co
   int last_base = 0;
   // 16-bit steps with a PF-deep prefetch ring up to s_wide, 32-bit steps (plain loads) after it
   int s_wide = init_narrow_ok(P) ? len : 0;
+  static_assert(PF <= kNarrowBlock, "the 16-bit bound holds for kNarrowBlock steps");
   if (s_wide > 0) {
     uint32_t ring[PF][NR];
     int rbase[PF];
@@ -877,9 +918,9 @@ __device__ __forceinline__ void hpaths3_init_lane(const uint8_t* __restrict__ co
 #pragma unroll
           for (int i = 0; i < NR; ++i) out[i] = narrow(L[2 * i], L[2 * i + 1]);
           if (valid) st_slice<NR>(orow + (size_t)x * kLevelRange, out);
-          if (__any_sync(kFull, !narrow_m_ok(m))) s_wide = s + 1;
         }
       }
+      if (__any_sync(kFull, !narrow_m_ok(m))) s_wide = min(len, s0 + PF);  // 32 bits after this block
     }
   }
   if (s_wide < len) {
@@ -948,6 +989,7 @@ __device__ __forceinline__ void vpaths3_init_lane(const uint8_t* __restrict__ co
   int last_base = base0;
   // bottom -> top: 16-bit steps with a prefetch ring up to s_wide, then 32-bit steps
   int s_wide = narrow_ok ? H : 0;
+  static_assert(PF <= kNarrowBlock, "the 16-bit bound holds for kNarrowBlock steps");
   if (s_wide > 0) {
     uint32_t ring[PF][NR];
     int rbase[PF];
@@ -979,9 +1021,9 @@ __device__ __forceinline__ void vpaths3_init_lane(const uint8_t* __restrict__ co
             for (int i = 0; i < NR; ++i) out[i] = narrow(L[2 * i], L[2 * i + 1]);
             st_slice<NR>(btv + (size_t)y * rs, out);
           }
-          if (__any_sync(kFull, !narrow_m_ok(m))) s_wide = s + 1;
         }
       }
+      if (__any_sync(kFull, !narrow_m_ok(m))) s_wide = min(H, s0 + PF);
     }
   }
   if (s_wide < H) {
@@ -1052,9 +1094,9 @@ __device__ __forceinline__ void vpaths3_init_lane(const uint8_t* __restrict__ co
           } else if (valid && g == 0) {
             dout[(size_t)y * W] = kInvalidFloat;
           }
-          if (__any_sync(kFull, !narrow_m_ok(m))) y_wide = y + 1;
         }
       }
+      if (__any_sync(kFull, !narrow_m_ok(m))) y_wide = min(H, y0 + PF);
     }
   }
   if (y_wide < H) {

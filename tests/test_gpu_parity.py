@@ -161,6 +161,38 @@ def test_init_disparity_parity(engine_lib, oracle_mod, cs, p1, p2, lr, u, tie):
     assert_same("disp left", disp, ref["disp"])
 
 
+def _blocky_pair(seed, W, H, shift=5):
+    """Piecewise-constant 8x8 blocks of four grey levels: flat patches give equal costs over
+    many disparities, so the WTA meets ties whose first candidate fails the uniqueness test."""
+    rng = np.random.default_rng(seed)
+    blocks = rng.integers(0, 4, ((H + 7) // 8, (W + 7) // 8 + 2)) * 60
+    img = np.repeat(np.repeat(blocks, 8, 0), 8, 1).astype(np.uint8)
+    L = np.ascontiguousarray(img[:H, 8:8 + W])
+    R = np.ascontiguousarray(img[:H, 8 + shift:8 + shift + W])
+    return L, R
+
+
+@pytest.mark.parametrize("lanes", [(2, 2), (8, 8)])
+@pytest.mark.parametrize("tie", [4, 0])
+def test_init_disparity_ties_low_texture(engine_lib, oracle_mod, tie, lanes):
+    import fasterstereocuda_b200 as fsc
+    O = oracle_mod
+    W, H = 200, 96
+    L, R = _blocky_pair(7, W, H)
+    init = np.full((H, W), 3, np.int16)
+    init[:, ::17] = 9
+    s = make_engine(fsc, W, H, 0, 32, 1, 10, 150, 0.95, 1, 1, tie=tie)
+    assert s.set_tuning(fsc.Tuning(3, 0, 3, 0, 0, *lanes)), s.last_error()
+    disp = np.empty((H, W), np.float32)
+    assert s.Match(L, R, disp, None, init), s.last_error()
+    cfg = O.Config(width=W, height=H, disp_range=32, cs_type=1, p1=10, p2=150, uniqueness=0.95, do_lr_check=1,
+                   do_median=1, peaks_strips=STRIPS, tie_rule=tie, init_tie_rule=tie)
+    ref = O.match(cfg, L, R, init, dump=True, want_right=True)
+    assert_same("wta left", s.debug_read("wta", 0), ref["wta_l"])
+    assert_same("wta right", s.debug_read("wta", 1), ref["wta_r"])
+    assert_same("disp left", disp, ref["disp"])
+
+
 def test_init_disparity_tall_global_bt(engine_lib, oracle_mod):
     """32-disparity level taller than the shared-memory budget of the vertical kernel."""
     import fasterstereocuda_b200 as fsc

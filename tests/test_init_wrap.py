@@ -3,8 +3,9 @@
 After a realignment beyond the disparity range every neighbour candidate is 127, so when the
 previous minimum m exceeds 127 + C all new path costs wrap below zero; alternating such pixels
 with invalid-cost (255) pixels grows |m| by up to 255 every two steps. The CUDA kernels run the
-recurrence in 16 bits while |m| <= 8192 and continue a scanline in 32 bits beyond that; these
-cases drive |m| far past 2^15, so a 16-bit-only form would differ from the oracle.
+recurrence in 16 bits while |m| <= 8192 at the end of every block of up to 8 steps and continue
+a scanline in 32 bits beyond that; these cases drive |m| far past 2^15, so a 16-bit-only form
+would differ from the oracle.
 """
 import numpy as np
 import pytest
@@ -82,13 +83,52 @@ def test_alternating_realignment_drives_minimum_past_16_bits(oracle_mod):
     assert min(ms) < -(1 << 15)
 
 
+def test_minimum_grows_at_most_382_plus_p2_per_step():
+    """The bound behind the 16-bit form: per step |m| and every |L| grow by at most 382 + P2'
+    over the |m| the step started from, on random scanlines with random realignments, INVALID
+    bases and cost 255 pixels."""
+    rng = np.random.default_rng(11)
+    for trial in range(40):
+        n = 60
+        p1 = int(rng.integers(0, 40))
+        p2 = int(rng.integers(p1, 2048))
+        cost = rng.integers(0, 118, (n, 32))
+        cost[rng.random(n) < 0.3] = 255
+        bases = rng.choice([0, 1, -1, 3, 40, -40, 2000], size=n).astype(np.int64)
+        bases[rng.random(n) < 0.1] = -32768
+        bases[0] = 0
+        Lq = [int(c) for c in cost[0]]
+        m, last = min(Lq), 0
+        for s in range(1, n):
+            base = int(bases[s])
+            if base == -32768:
+                m = 127
+                continue
+            div = abs(last - base + 1)
+            q = int(p2 / div) if div else -1
+            p2p = max(p1, q)
+            ms = m - M32 if m >= 1 << 31 else m
+            Lp = []
+            for d in range(32):
+                i1, i2 = d + base - 1 - last, d + base + 1 - last
+                a = (Lq[i1] + p1) % M32 if 0 <= i1 < 32 else 127
+                b = (Lq[i2] + p1) % M32 if 0 <= i2 < 32 else 127
+                Lp.append((int(cost[s][d]) + min(Lq[d], a, b, (m + p2p) % M32) - m) % M32)
+            signed = [v - M32 if v >= 1 << 31 else v for v in Lp]
+            assert max(abs(v) for v in signed) <= abs(ms) + 382 + p2p, (trial, s)
+            Lq, m, last = Lp, min(Lp), base
+            m_new = m - M32 if m >= 1 << 31 else m
+            assert abs(m_new) <= abs(ms) + 382 + p2p, (trial, s)
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("lanes", [(2, 2), (4, 4), (8, 8)])
-@pytest.mark.parametrize("p1,p2", [(10, 150), (10, 9000)])
+@pytest.mark.parametrize("p1,p2", [(10, 150), (10, 2047), (10, 9000)])
 @pytest.mark.parametrize("kind", ["cols", "rows", "random"])
 def test_wrapping_paths_match_oracle(engine_lib, oracle_mod, kind, p1, p2, lanes):
     """Path volumes and disparities bit-exact on the wrapping cases, for every lane split of the
-    scanline kernels; P2 = 9000 runs them in 32 bits from the first pixel."""
+    scanline kernels; P2 = 2047 is the largest penalty of the 16-bit form, P2 = 9000 runs them in
+    32 bits from the first pixel."""
     import fasterstereocuda_b200 as fsc
     O = oracle_mod
     W, H = {"cols": (720, 40), "rows": (48, 600), "random": (300, 200)}[kind]
