@@ -55,6 +55,9 @@ def parse():
                                                  "bt_smem,row_lanes,col_lanes (default: autotuned lane split)")
     ap.add_argument("--profile-pairs", type=int, default=16, help="pairs of the serialised per-kernel timing pass")
     ap.add_argument("--e2e-threads", type=int, default=96, help="host threads (one matcher each) of the e2e pass")
+    ap.add_argument("--extra", choices=["batch_pyramid", "batch", "batch_uneven", "float_sgm", "large_pyramid"],
+                    default="", help="run one extra workload alone and print its JSON (e.g. for a profiler)")
+    ap.add_argument("--extra-pairs", type=int, default=64, help="pairs of the --extra batch workloads")
     return ap.parse_args()
 
 
@@ -710,6 +713,29 @@ def cpu_baseline(a, pool):
             "sample": f"{n} pairs of the same workload in {dt:.1f} s (oracle/ C restatement, OpenMP)"}
 
 
+def run_extra(a):
+    """One extra workload on its own (single GPU), with a small pool of distinct pairs."""
+    from fasterstereocuda_b200 import scenes
+    n = a.extra_pairs
+    if a.extra == "float_sgm":
+        out = extra_float_sgm()
+    elif a.extra == "large_pyramid":
+        out = extra_large_pyramid()
+    elif a.extra == "batch_uneven":
+        specs = scenes.batch_specs()[:n]
+        imgs = [scenes.planar_pair(seed, w, h, dmin=2.0, dmax=60.0)[:2] for (w, h, d, seed) in specs]
+        out = batch_vs_loop([(w, h, 0, d) for (w, h, d, _) in specs], imgs, runs=3, warmup=1)
+    else:
+        pool = make_pool(min(n, 16))
+        imgs = [pool[i % len(pool)] for i in range(n)]
+        if a.extra == "batch":
+            out = batch_vs_loop([(W_, H_, 0, DMAX)] * n, imgs, runs=5, warmup=2)
+        else:
+            out = batch_pyramid_vs_loop(imgs, runs=5, warmup=2)
+    print(json.dumps({"extra": a.extra, **out}), flush=True)
+    return 0
+
+
 def main():
     a = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -717,6 +743,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if a.impl == "reference":
         return run_reference(a, rank, world)
+    if a.extra:
+        return run_extra(a)
     if world > 1:
         import datetime
         import torch

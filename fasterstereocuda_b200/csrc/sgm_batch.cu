@@ -828,7 +828,7 @@ int init_rows(sgm_batch_pyr* p, PLevel& L, PBucket& k, cudaStream_t s, int* queu
     PTRY(p, cudaGetLastError());
     return SGM_OK;
   };
-  return G == 2 ? go(kb_rows3_init<2, 4>) : G == 4 ? go(kb_rows3_init<4, 8>) : go(kb_rows3_init<8, 8>);
+  return G == 2 ? go(kb_rows3_init<2, 8>) : G == 4 ? go(kb_rows3_init<4, 8>) : go(kb_rows3_init<8, 8>);
 }
 
 int init_cols(sgm_batch_pyr* p, PLevel& L, PBucket& k, cudaStream_t s, int* queue, bool prepare) {

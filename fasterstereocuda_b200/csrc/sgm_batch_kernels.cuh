@@ -301,7 +301,7 @@ __global__ void __launch_bounds__(256) kb_cost3_init(const BatchPair* __restrict
 template <int G>
 __device__ __forceinline__ void init_scan_smem(uint32_t* p2tab, uint32_t* rows, const sgm::InitParams& P) {
   sgm::fill_p2_table(p2tab, P, threadIdx.x, blockDim.x);
-  sgm::init_row_pad<G>(rows + (threadIdx.x / G) * sgm::kIRow, P.p1, true, threadIdx.x % G);
+  sgm::init_row_pad<G>(rows + threadIdx.x / G, P.p1, true, threadIdx.x % G);
   __syncthreads();
 }
 
@@ -311,9 +311,9 @@ __global__ void __launch_bounds__(128) kb_rows3_init(const BatchPair* __restrict
                                                      const int* __restrict__ prefix, int n, int* __restrict__ queue) {
   constexpr int S = 32 / G;
   __shared__ uint32_t p2tab[sgm::kP2Tab];
-  __shared__ uint32_t rows[(128 / G) * sgm::kIRow];
+  __shared__ uint32_t rows[sgm::init_rs<G>() * sgm::kIRow];
   init_scan_smem<G>(p2tab, rows, pairs[__ldg(ids)].IP);
-  uint32_t* row = rows + (threadIdx.x / G) * sgm::kIRow;
+  uint32_t* row = rows + threadIdx.x / G;
   const int lane = threadIdx.x & 31;
   const int total = __ldg(prefix + n);
   for (;;) {
@@ -334,11 +334,11 @@ __global__ void __launch_bounds__(128) kb_cols3_init(const BatchPair* __restrict
                                                      const int* __restrict__ prefix, int n, int* __restrict__ queue) {
   constexpr int S = 32 / G;
   __shared__ uint32_t p2tab[sgm::kP2Tab];
-  __shared__ uint32_t rows[(128 / G) * sgm::kIRow];
-  __shared__ uint32_t sums[(128 / G) * 33];
+  __shared__ uint32_t rows[sgm::init_rs<G>() * sgm::kIRow];
+  __shared__ uint32_t sums[sgm::init_rs<G>() * (sgm::kLevelRange / 2)];
   init_scan_smem<G>(p2tab, rows, pairs[__ldg(ids)].IP);
-  uint32_t* row = rows + (threadIdx.x / G) * sgm::kIRow;
-  uint32_t* colS = sums + (threadIdx.x / G) * 33;
+  uint32_t* row = rows + threadIdx.x / G;
+  uint32_t* colS = sums + threadIdx.x / G;
   const int lane = threadIdx.x & 31;
   const int total = __ldg(prefix + n);
   for (;;) {

@@ -490,7 +490,7 @@ int launch_init3(sgm_engine* e, const Word* csl, const Word* csr, const int16_t*
     auto go = [&](auto kern) {
       return SGM_LAUNCH(e, s, "hpaths_init", kern<<<blocks, 128, 0, s>>>(e->cost, il, ir, e->lr, e->rl, P, nv));
     };
-    st = G == 2 ? go(sgm::k_hpaths3_init<2, 4>) : G == 8 ? go(sgm::k_hpaths3_init<8, 8>) : go(sgm::k_hpaths3_init<4, 8>);
+    st = G == 2 ? go(sgm::k_hpaths3_init<2, 8>) : G == 8 ? go(sgm::k_hpaths3_init<8, 8>) : go(sgm::k_hpaths3_init<4, 8>);
     if (st) return st;
   }
   if (cols3) {

@@ -64,6 +64,25 @@ __device__ __forceinline__ void st_slice(uint8_t* __restrict__ p, const uint32_t
   }
 }
 
+// Bulk prefetch of `bytes` (a multiple of 16, 16-byte aligned, inside one allocation) into L2.
+__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// A row scan reads one short slice per row and step, so its loads of one DRAM page are spread
+// over many steps. Every 16 steps the scanline's first lane prefetches the row's next 16 pixels
+// (steps s0 + 16 .. s0 + 31, clamped to the scanline) into L2 in one request.
+template <int BYTES_PER_PX>
+__device__ __forceinline__ void prefetch_row_ahead(const uint8_t* row, int xs, int dx, int s0, int len, int g) {
+  if (g == 0 && (s0 & 15) == 0) {
+    const int a = s0 + 16, n = min(16, len - a);
+    if (n > 0) {
+      const int x_lo = dx > 0 ? xs + a : xs - a - (n - 1);
+      prefetch_l2(row + (size_t)x_lo * BYTES_PER_PX, (uint32_t)(n * BYTES_PER_PX));
+    }
+  }
+}
+
 // bytes -> u16x2 words (NT = 2*NR) and back (low bytes)
 template <int NR>
 __device__ __forceinline__ void widen_slice(const uint32_t (&r)[NR], uint32_t (&w)[2 * NR]) {
@@ -261,7 +280,9 @@ __device__ __forceinline__ void hpaths3_lane(const uint8_t* __restrict__ cost, u
   for (int j = 0; j < PF; ++j)
     if (j < len) ld_slice<NR>(crow + (size_t)(xs + j * dx) * D, ring[j]);
   uint32_t m = 0;
+  static_assert(16 % PF == 0, "blocks of PF steps start every 16 steps");
   for (int s0 = 0; s0 < len; s0 += PF) {
+    prefetch_row_ahead<D>(crow - (size_t)g * SB, xs, dx, s0, len, g);
 #pragma unroll
     for (int j = 0; j < PF; ++j) {
       const int s = s0 + j;
@@ -554,19 +575,26 @@ __device__ __forceinline__ uint32_t p2_prime(const uint32_t* tab, int k, const I
   return p2_term(tab, k, P);
 }
 
+// Shared-memory rows of a 128-thread block are stored scanline-minor: word w of the scanline
+// at row[w * init_rs<G>()]. The stride 128/G + 2 is twice an odd number, so the G lanes of the
+// 32/G scanlines of a warp that access the same word index (the same shift) hit 32 different
+// banks.
+template <int G>
+__host__ __device__ constexpr int init_rs() { return 128 / G + 2; }
+
 // One realigned step of the scanline held by G lanes (lane g owns d = g*ND .. g*ND+ND-1); every
 // lane of the warp calls it. `row`: this scanline's kIRow words (padding already written).
 template <int ND, int G>
 __device__ __forceinline__ uint32_t init_step32(uint32_t (&L)[ND], const uint32_t (&c)[ND], uint32_t m, int s,
                                                 uint32_t p2t, uint32_t p1, uint32_t* row, int g) {
 #pragma unroll
-  for (int j = 0; j < ND; ++j) row[kIPad + g * ND + j] = L[j];
+  for (int j = 0; j < ND; ++j) row[(kIPad + g * ND + j) * init_rs<G>()] = L[j];
   __syncwarp();
   const int sc = s < -33 ? -33 : (s > 33 ? 33 : s);
-  const uint32_t* src = row + kIPad + g * ND + sc - 1;  // src[j] = old L(g*ND + j + s - 1)
+  const uint32_t* src = row + (kIPad + g * ND + sc - 1) * init_rs<G>();  // word j: old L(g*ND + j + s - 1)
   uint32_t w[ND + 2];
 #pragma unroll
-  for (int j = 0; j < ND + 2; ++j) w[j] = src[j];
+  for (int j = 0; j < ND + 2; ++j) w[j] = src[j * init_rs<G>()];
   __syncwarp();
   const uint32_t l4 = m + p2t;
   uint32_t nl[ND];
@@ -600,12 +628,12 @@ __device__ __forceinline__ void init_row_pad(uint32_t* row, uint32_t p1, bool na
   const uint32_t pad = kInvalidCost - p1;
   if (narrow16) {
     const uint32_t w = rep16(pad & 0xFFFFu);
-    for (int k = g; k < kINPad; k += G) row[k] = w;
-    for (int k = g; k < kINPad + 1; k += G) row[kINPad + 16 + k] = w;
+    for (int k = g; k < kINPad; k += G) row[k * init_rs<G>()] = w;
+    for (int k = g; k < kINPad + 1; k += G) row[(kINPad + 16 + k) * init_rs<G>()] = w;
   } else {
     for (int k = g; k < kIPad; k += G) {
-      row[k] = pad;
-      row[kIPad + 32 + k] = pad;
+      row[k * init_rs<G>()] = pad;
+      row[(kIPad + 32 + k) * init_rs<G>()] = pad;
     }
   }
 }
@@ -620,15 +648,15 @@ __device__ __forceinline__ uint32_t init_step16(const uint32_t (&L)[ND], uint32_
                                                 uint32_t p1, uint32_t* row, int g) {
   constexpr int NW = ND / 2;
 #pragma unroll
-  for (int k = 0; k < NW; ++k) row[kINPad + g * NW + k] = L[k];
+  for (int k = 0; k < NW; ++k) row[(kINPad + g * NW + k) * init_rs<G>()] = L[k];
   __syncwarp();
   const int sc = s < -33 ? -33 : (s > 33 ? 33 : s);
   const int o = 2 * kINPad + g * ND + sc - 1;  // half index of old L(g*ND + s - 1), in [0, 98 - ND]
-  const uint32_t* src = row + (o >> 1);
+  const uint32_t* src = row + (o >> 1) * init_rs<G>();
   const uint32_t sel = (o & 1) ? 0x5432u : 0x3210u;
   uint32_t wd[NW + 2];
 #pragma unroll
-  for (int k = 0; k < NW + 2; ++k) wd[k] = src[k];
+  for (int k = 0; k < NW + 2; ++k) wd[k] = src[k * init_rs<G>()];
   __syncwarp();
   // __viaddmin_u16x2(a, b, c) = min((a + b) mod 2^16, c) per half; with c = 0xFFFF it is the
   // wrapping add (the wrap of the add is what the exactness argument needs; the wrapping tests
@@ -748,10 +776,11 @@ __device__ __forceinline__ void init_go_narrow(const InitParams& P, uint32_t* ro
 // (reference Kernel_ComputeDisparityByWTA for initial disparities). ok: the pixel may be valid.
 // Keys S*32 + d (S <= 1020) fit 16 bits: their minimum is the lowest d of least S. Rule
 // kTieRefB200: the lowest tied d whose uniqueness test passes; kTieLowest: the lowest tied d.
+template <int G>
 __device__ __forceinline__ float init_candidate(const uint32_t* colS, int d, uint32_t sm, int base,
                                                 const WtaParams& Q) {
   if (d <= 1 || d >= kLevelRange - 1) return kInvalidFloat;
-  const uint32_t w1 = colS[(d - 1) >> 1], w3 = colS[(d + 1) >> 1];
+  const uint32_t w1 = colS[((d - 1) >> 1) * init_rs<G>()], w3 = colS[((d + 1) >> 1) * init_rs<G>()];
   const float c1 = (float)((d - 1) & 1 ? w1 >> 16 : w1 & 0xFFFFu), c2 = (float)sm,
               c3 = (float)((d + 1) & 1 ? w3 >> 16 : w3 & 0xFFFFu);
   const float d12 = __fsub_rn(c1, c2), d32 = __fsub_rn(c3, c2);
@@ -767,14 +796,14 @@ __device__ __forceinline__ void init_wta_pixel(const uint32_t (&S2)[ND / 2], uin
   uint32_t key[NW];
 #pragma unroll
   for (int k = 0; k < NW; ++k) {
-    colS[g * NW + k] = S2[k];
+    colS[(g * NW + k) * init_rs<G>()] = S2[k];
     key[k] = (S2[k] << 5) + d0 + (uint32_t)(2 * k) * 0x10001u;
   }
   const uint32_t kmin = group_min16<NW, G>(key);
   __syncwarp();
   const uint32_t sm = kmin >> 5;
   const int ds = (int)(kmin & 31u);
-  float dv = init_candidate(colS, ds, sm, base, Q);  // the same in every lane of the group
+  float dv = init_candidate<G>(colS, ds, sm, base, Q);  // the same in every lane of the group
   if (Q.tie_rule == kTieRefB200) {
     // while the candidate fails: the next tied d, i.e. the least key above kcur and below
     // (sm + 1) * 32 (keys <= kcur wrap to >= 2^15 in key - kcur - 1)
@@ -790,7 +819,7 @@ __device__ __forceinline__ void init_wta_pixel(const uint32_t (&S2)[ND / 2], uin
       const uint32_t nk = group_min16<NW, G>(u) + kcur + 1u;
       if (need) {
         kcur = nk < lim ? nk : lim;
-        if (nk < lim) dv = init_candidate(colS, (int)(nk & 31u), sm, base, Q);
+        if (nk < lim) dv = init_candidate<G>(colS, (int)(nk & 31u), sm, base, Q);
       }
     }
   }
@@ -884,6 +913,7 @@ __device__ __forceinline__ void hpaths3_init_lane(const uint8_t* __restrict__ co
   // 16-bit steps with a PF-deep prefetch ring up to s_wide, 32-bit steps (plain loads) after it
   int s_wide = init_narrow_ok(P) ? len : 0;
   static_assert(PF <= kNarrowBlock, "the 16-bit bound holds for kNarrowBlock steps");
+  static_assert(16 % PF == 0, "blocks of PF steps start every 16 steps");
   if (s_wide > 0) {
     uint32_t ring[PF][NR];
     int rbase[PF];
@@ -895,6 +925,7 @@ __device__ __forceinline__ void hpaths3_init_lane(const uint8_t* __restrict__ co
       }
     }
     for (int s0 = 0; s0 < s_wide; s0 += PF) {
+      prefetch_row_ahead<kLevelRange>(crow - (size_t)g * ND, xs, dx, s0, len, g);
 #pragma unroll
       for (int j = 0; j < PF; ++j) {
         const int s = s0 + j;
@@ -949,9 +980,9 @@ __global__ void __launch_bounds__(128) k_hpaths3_init(const uint8_t* __restrict_
                                                       const int16_t* __restrict__ init_r, uint8_t* __restrict__ lr,
                                                       uint8_t* __restrict__ rl, InitParams P, int nviews) {
   __shared__ uint32_t p2tab[kP2Tab];
-  __shared__ uint32_t rows[(128 / G) * kIRow];
+  __shared__ uint32_t rows[init_rs<G>() * kIRow];
   fill_p2_table(p2tab, P, threadIdx.x, blockDim.x);
-  uint32_t* row = rows + (threadIdx.x / G) * kIRow;
+  uint32_t* row = rows + threadIdx.x / G;
   init_row_pad<G>(row, P.p1, true, threadIdx.x % G);
   __syncthreads();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1140,15 +1171,15 @@ __global__ void __launch_bounds__(128) k_vpaths3_init(const uint8_t* __restrict_
                                                       const int16_t* __restrict__ init_r, uint8_t* __restrict__ bt,
                                                       float* __restrict__ disp, InitParams P, WtaParams Q) {
   __shared__ uint32_t p2tab[kP2Tab];
-  __shared__ uint32_t rows[(128 / G) * kIRow];
-  __shared__ uint32_t sums[(128 / G) * 33];
+  __shared__ uint32_t rows[init_rs<G>() * kIRow];
+  __shared__ uint32_t sums[init_rs<G>() * (kLevelRange / 2)];
   fill_p2_table(p2tab, P, threadIdx.x, blockDim.x);
-  uint32_t* row = rows + (threadIdx.x / G) * kIRow;
+  uint32_t* row = rows + threadIdx.x / G;
   init_row_pad<G>(row, P.p1, true, threadIdx.x % G);
   __syncthreads();
   const int xc = (blockIdx.x * blockDim.x + threadIdx.x) / G;
   vpaths3_init_lane<G, PF>(cost, lr, rl, init_l, init_r, bt, disp, P, Q, blockIdx.y, xc, threadIdx.x % G, row,
-                           sums + (threadIdx.x / G) * 33, p2tab);
+                           sums + threadIdx.x / G, p2tab);
 }
 
 }  // namespace sgm
