@@ -150,9 +150,10 @@ def alg_bytes(kernel, W, H, D, nviews, census_bytes):
 
 
 # DRAM bytes per voxel (W*H*D*views of the launch) measured by ncu (dram__bytes_read.sum +
-# dram__bytes_write.sum) for the default kernels at 1242x375x64; profiles/scanline_kernels_1242x375x64.md.
-NCU_DRAM_BYTES_PER_VOXEL = {"hpaths_plain": 2.79, "vpaths_wta_plain": 5.34, "hpaths_init": 1.07,
-                            "vpaths_wta_init": 3.23}
+# dram__bytes_write.sum) for the default kernels at 1242x375x64, one pair per launch: the plain
+# kernels on the single-level workload, the 32-disparity kernels on the pyramid's finest level.
+NCU_DRAM_BYTES_PER_VOXEL = {"hpaths_plain": 2.82, "vpaths_wta_plain": 5.35, "hpaths_init": 1.07,
+                            "vpaths_wta_init": 3.29}
 
 
 # ------------------------------------------------------------------------------------ reference arm

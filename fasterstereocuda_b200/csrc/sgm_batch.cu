@@ -841,7 +841,7 @@ int init_cols(sgm_batch_pyr* p, PLevel& L, PBucket& k, cudaStream_t s, int* queu
     PTRY(p, cudaGetLastError());
     return SGM_OK;
   };
-  return G == 2 ? go(kb_cols3_init<2, 2>) : G == 4 ? go(kb_cols3_init<4, 4>) : go(kb_cols3_init<8, 4>);
+  return G == 2 ? go(kb_cols3_init<2, 1>) : G == 4 ? go(kb_cols3_init<4, 4>) : go(kb_cols3_init<8, 4>);
 }
 
 int init_cost(sgm_batch_pyr* p, PLevel& L, PBucket& k, cudaStream_t s) {

@@ -502,7 +502,7 @@ int launch_init3(sgm_engine* e, const Word* csl, const Word* csr, const int16_t*
       return SGM_LAUNCH(e, s, "vpaths_wta_init",
                         kern<<<grid, 128, 0, s>>>(e->cost, e->lr, e->rl, il, ir, e->bt, wta, P, Q));
     };
-    st = G == 2 ? go(sgm::k_vpaths3_init<2, 2>) : G == 8 ? go(sgm::k_vpaths3_init<8, 4>) : go(sgm::k_vpaths3_init<4, 4>);
+    st = G == 2 ? go(sgm::k_vpaths3_init<2, 1>) : G == 8 ? go(sgm::k_vpaths3_init<8, 4>) : go(sgm::k_vpaths3_init<4, 4>);
   }
   return st;
 }

@@ -71,11 +71,11 @@ __device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
 
 // A row scan reads one short slice per row and step, so its loads of one DRAM page are spread
 // over many steps. Every 16 steps the scanline's first lane prefetches the row's next 16 pixels
-// (steps s0 + 16 .. s0 + 31, clamped to the scanline) into L2 in one request.
+// (steps s0 + 8 .. s0 + 23, clamped to the scanline) into L2 in one request.
 template <int BYTES_PER_PX>
 __device__ __forceinline__ void prefetch_row_ahead(const uint8_t* row, int xs, int dx, int s0, int len, int g) {
   if (g == 0 && (s0 & 15) == 0) {
-    const int a = s0 + 16, n = min(16, len - a);
+    const int a = s0 + 8, n = min(16, len - a);
     if (n > 0) {
       const int x_lo = dx > 0 ? xs + a : xs - a - (n - 1);
       prefetch_l2(row + (size_t)x_lo * BYTES_PER_PX, (uint32_t)(n * BYTES_PER_PX));
