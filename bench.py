@@ -432,8 +432,11 @@ def run_ours(a, rank, world, local_rank):
         ops = sum(nv * (34 * w * h * d + 248 * w * h) for (kind, w, h, d, nv) in levels)
         clk = (clk_summary or {}).get("sm_mhz") or 1965.0
         peak = 148 * 128 * clk * 1e6
+        # the scans execute their recurrence on packed 16x2 words (two disparities per
+        # instruction): frac_packed16x2 is against twice the INT32 rate
         roofline["alu"] = {"ops_alg_per_pair": ops, "achieved_tops": ops * value / 1e12 / world,
                            "int32_peak_tops": peak / 1e12, "frac": ops * value / world / peak,
+                           "frac_packed16x2": ops * value / world / (2 * peak),
                            "peak_kind": "nominal: 148 SMs x 128 INT32 lanes x median SM clock under load",
                            "per": "GPU"}
     tot_ms = sum(x["ms"] for x in prof.values()) or 1.0
