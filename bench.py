@@ -42,7 +42,7 @@ LAYERS = 3
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["pyramid", "plain"], default="pyramid")
@@ -87,7 +87,8 @@ def make_pool(n_distinct, seed=100):
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms while the timed region runs."""
+    """nvidia-smi clocks / throttle reasons sampled every 50 ms while the timed region runs (the
+    region starts once the sampler has written its first line)."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
@@ -102,8 +103,12 @@ class ClockSampler:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            t = time.perf_counter()
+            while time.perf_counter() - t < 5.0 and os.path.getsize(self.path) == 0 and self.proc.poll() is None:
+                time.sleep(0.01)
+            self.skip = os.path.getsize(self.path)  # lines written before the timed region
         except Exception:
             self.proc = None
         return self
@@ -119,8 +124,11 @@ class ClockSampler:
     def summary(self):
         if not self.path or not os.path.exists(self.path):
             return None
-        rows = [l.split(",") for l in open(self.path).read().splitlines() if l.count(",") >= 8]
+        with open(self.path) as f:
+            data = f.read()
         os.remove(self.path)
+        timed = data[getattr(self, "skip", 0):]
+        rows = [l.split(",") for l in (timed if timed.strip() else data).splitlines() if l.count(",") >= 8]
         if not rows:
             return None
         sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]

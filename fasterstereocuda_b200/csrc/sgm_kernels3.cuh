@@ -299,7 +299,10 @@ __device__ __forceinline__ void hpaths3_lane(const uint8_t* __restrict__ cost, u
 }
 
 template <int K, int G, int PF>
-__global__ void __launch_bounds__(128) k_hpaths3(const uint8_t* __restrict__ cost, uint8_t* __restrict__ lr,
+// five CTAs per SM (at most 96 registers) where a lane holds at most 32 disparities and G >= 2:
+// many concurrent pairs are occupancy-bound (plain 1242x375x64: +5 % pairs/s over the
+// unconstrained 113-128 registers); wider slices would spill
+__global__ void __launch_bounds__(128, (G >= 2 && 32 * K / G <= 32) ? 5 : 1) k_hpaths3(const uint8_t* __restrict__ cost, uint8_t* __restrict__ lr,
                                                  uint8_t* __restrict__ rl, PlainParams P, int nviews) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   hpaths3_lane<K, G, PF>(cost, lr, rl, P, nviews, t / G, threadIdx.x % G);
@@ -496,7 +499,10 @@ __device__ __forceinline__ void vpaths3_lane(const uint8_t* __restrict__ cost, c
 }
 
 template <int K, int G, int PF>
-__global__ void __launch_bounds__(128) k_vpaths3(const uint8_t* __restrict__ cost, const uint8_t* __restrict__ lr,
+// five CTAs per SM (at most 96 registers) where a lane holds at most 32 disparities and G >= 2:
+// many concurrent pairs are occupancy-bound (plain 1242x375x64: +5 % pairs/s over the
+// unconstrained 113-128 registers); wider slices would spill
+__global__ void __launch_bounds__(128, (G >= 2 && 32 * K / G <= 32) ? 5 : 1) k_vpaths3(const uint8_t* __restrict__ cost, const uint8_t* __restrict__ lr,
                                                  const uint8_t* __restrict__ rl, uint8_t* __restrict__ bt,
                                                  float* __restrict__ disp, PlainParams P, WtaParams Q) {
   extern __shared__ uint32_t s_sum[];
