@@ -298,12 +298,12 @@ int prepare_bucket(sgm_batch* b, sgm_batch::Bucket& k) {
 }
 
 int launch_census(sgm_batch* b, cudaStream_t s) {
-  const int blocks = (b->census_items + 7) / 8;
+  const int blocks = b->census_items;  // one block per (pair, view, row block)
   const int n = (int)b->pairs.size();
   if (b->word == 8)
-    kb_census<uint64_t, 4, 3><<<blocks, dim3(32, 8), 0, s>>>(b->ddesc, b->dtab + b->census_prefix, n);
+    kb_census4<uint64_t, 4, 3><<<blocks, 128, 0, s>>>(b->ddesc, b->dtab + b->census_prefix, n);
   else
-    kb_census<uint32_t, 2, 2><<<blocks, dim3(32, 8), 0, s>>>(b->ddesc, b->dtab + b->census_prefix, n);
+    kb_census4<uint32_t, 2, 2><<<blocks, 128, 0, s>>>(b->ddesc, b->dtab + b->census_prefix, n);
   BTRY(b, cudaGetLastError());
   return SGM_OK;
 }
@@ -564,7 +564,7 @@ int sgm_batch_init(sgm_batch_t b, const sgm_batch_pair_t* pairs, int32_t count, 
   };
   std::vector<int> all(count);
   for (int i = 0; i < count; ++i) all[i] = i;
-  auto cp = prefix_of(all, [&](int i) { return 2 * pairs[i].height; });
+  auto cp = prefix_of(all, [&](int i) { return 2 * ((pairs[i].height + sgm::kCensusRows - 1) / sgm::kCensusRows); });
   b->census_prefix = cp.first; b->census_items = cp.second;
   auto tp = prefix_of(all, [&](int i) { return ((pairs[i].width + 31) / 32) * ((pairs[i].height + 7) / 8); });
   b->tile_prefix = tp.first; b->tile_items = tp.second;
@@ -895,9 +895,9 @@ int level_filters(sgm_batch_pyr* p, const BatchPair* d, const sgm_option_t& o, i
 }
 
 int level_census(sgm_batch_pyr* p, const BatchPair* d, int cpre, int citems, int n, cudaStream_t s) {
-  const int blocks = (citems + 7) / 8;
-  if (p->word == 8) kb_census<uint64_t, 4, 3><<<blocks, dim3(32, 8), 0, s>>>(d, p->dtab + cpre, n);
-  else kb_census<uint32_t, 2, 2><<<blocks, dim3(32, 8), 0, s>>>(d, p->dtab + cpre, n);
+  const int blocks = citems;  // one block per (pair, view, row block)
+  if (p->word == 8) kb_census4<uint64_t, 4, 3><<<blocks, 128, 0, s>>>(d, p->dtab + cpre, n);
+  else kb_census4<uint32_t, 2, 2><<<blocks, 128, 0, s>>>(d, p->dtab + cpre, n);
   PTRY(p, cudaGetLastError());
   return SGM_OK;
 }
@@ -1264,7 +1264,7 @@ int sgm_batch_pyr_init(sgm_batch_pyr_t p, const sgm_batch_pair_t* pairs, int32_t
   for (int lvl = 0; lvl < Lc; ++lvl) {
     PLevel& L = p->lv[lvl];
     auto hw = [&](int i) { return std::make_pair(pairs[i].width >> lvl, pairs[i].height >> lvl); };
-    auto c = prefix_of(all, [&](int i) { return 2 * hw(i).second; });
+    auto c = prefix_of(all, [&](int i) { return 2 * ((hw(i).second + sgm::kCensusRows - 1) / sgm::kCensusRows); });
     L.census_prefix = c.first; L.census_items = c.second;
     auto t = prefix_of(all, [&](int i) { return tiles_of(hw(i).first, hw(i).second); });
     L.tile_prefix = t.first; L.tile_items = t.second;

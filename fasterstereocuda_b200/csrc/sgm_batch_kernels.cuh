@@ -44,6 +44,26 @@ __device__ __forceinline__ int find_pair(const int* __restrict__ prefix, int n, 
   return lo;
 }
 
+// Census by tiles of kCensusRows rows (sgm::census4_tile): item = (pair, view, row block), the
+// block walks the row block's 512-pixel tiles.
+template <typename Word, int CSW, int CSH>
+__global__ void __launch_bounds__(128, 4) kb_census4(const BatchPair* __restrict__ pairs, const int* __restrict__ prefix,
+                                                  int n) {
+  constexpr int RY = sgm::kCensusRows;
+  __shared__ uint32_t tile[sgm::census4_tile_words<CSH, RY>()];
+  const int item = blockIdx.x;
+  const int b = find_pair(prefix, n, item);
+  const BatchPair& d = pairs[b];
+  const int W = d.P.W, H = d.P.H;
+  const int nrb = (H + RY - 1) / RY;
+  const int local = item - __ldg(prefix + b);
+  const int view = local / nrb;
+  const int by = (local - view * nrb) * RY;
+  const uint8_t* img = view ? d.img_r : d.img_l;
+  Word* out = static_cast<Word*>(view ? d.cs_r : d.cs_l);
+  for (int bx = 0; bx < W; bx += 512) sgm::census4_tile<Word, CSW, CSH, RY>(img, out, W, H, view == 1, bx, by, tile);
+}
+
 template <typename Word, int CSW, int CSH>
 __global__ void __launch_bounds__(256) kb_census(const BatchPair* __restrict__ pairs, const int* __restrict__ prefix,
                                                  int n) {

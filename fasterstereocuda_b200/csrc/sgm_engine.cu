@@ -603,12 +603,13 @@ int engine_enqueue(sgm_engine* e, const uint8_t* dl_img, const uint8_t* dr_img, 
   int st = SGM_OK;
   // census of both images
   {
-    dim3 g((W + 127) / 128, H, 2), b(128);
+    constexpr int RY = sgm::kCensusRows;
+    dim3 g((W + 511) / 512, (H + RY - 1) / RY, 2), b(128);
     if (e->opt.cs_type == 1)
-      st = SGM_LAUNCH(e, e->stream, "census", sgm::k_census<uint64_t, 4, 3><<<g, b, 0, e->stream>>>(
+      st = SGM_LAUNCH(e, e->stream, "census", sgm::k_census4<uint64_t, 4, 3, RY><<<g, b, 0, e->stream>>>(
                                                   dl_img, dr_img, (uint64_t*)e->cs[0], (uint64_t*)e->cs[1], W, H));
     else
-      st = SGM_LAUNCH(e, e->stream, "census", sgm::k_census<uint32_t, 2, 2><<<g, b, 0, e->stream>>>(
+      st = SGM_LAUNCH(e, e->stream, "census", sgm::k_census4<uint32_t, 2, 2, RY><<<g, b, 0, e->stream>>>(
                                                   dl_img, dr_img, (uint32_t*)e->cs[0], (uint32_t*)e->cs[1], W, H));
   }
   // right-view initial disparities when checking consistency at an init level

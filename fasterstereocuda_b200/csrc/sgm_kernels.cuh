@@ -47,6 +47,101 @@ __global__ void __launch_bounds__(128) k_census(const uint8_t* __restrict__ img_
   (right ? cs_r : cs_l)[(size_t)y * W + x] = census_value<Word, CSW, CSH>(right ? img_r : img_l, x, y, W, H, right);
 }
 
+// Census of 4 consecutive pixels per thread with byte-parallel compares (same values as
+// census_value). A 128-thread block covers 512 pixels of RY rows; the rows y-CSH .. y+RY-1+CSH,
+// columns x0-4 .. x0+515 are staged in shared memory (`tile`, census4_tile_words<CSH, RY>()
+// words). For each window offset the thread compares the 4-byte window of its pixels' neighbours
+// with their 4 centres at once:
+//   a < c (unsigned, per byte)  <=>  top bit of (~a & c) | (~(a ^ c) & ~((a | 0x80) - (c & 0x7f)))
+// (the subtraction cannot borrow across bytes), and collects offset k's bit of pixel p in byte p
+// of word k / 8 at bit 7 - k % 8; a byte transpose then yields each pixel's MSB-first word.
+constexpr int kCensus4Stride = 131;  // words per staged row (130 used)
+constexpr int kCensusRows = 8;      // output rows per block (RY)
+template <int CSH, int RY>
+__host__ __device__ constexpr int census4_tile_words() { return (RY + 2 * CSH) * kCensus4Stride; }
+
+template <typename Word, int CSW, int CSH, int RY>
+__device__ __forceinline__ void census4_tile(const uint8_t* __restrict__ img, Word* __restrict__ cs, int W, int H,
+                                             bool right, int bx, int by, uint32_t* tile) {
+  static_assert(CSW <= 4, "the window spans x0-4 .. x0+7");
+  constexpr int TR = RY + 2 * CSH, NC = 2 * CSW + 1, NB = (2 * CSH + 1) * NC, NG = (NB + 7) / 8;
+  static_assert(NG == (int)sizeof(Word) || NG == 4 || NG == 8, "census word of NB bits");
+  // stage: word w of row r holds pixels bx - 4 + 4w .. +3 of image row by + r - CSH (0 outside);
+  // the first barrier lets a block call this for several tiles in a row
+  __syncthreads();
+  for (int i = threadIdx.x; i < TR * 130; i += 128) {
+    const int r = i / 130, w = i - r * 130;
+    const int yy = by + r - CSH, xx = bx - 4 + 4 * w;
+    uint32_t v = 0;
+    if (yy >= 0 && yy < H) {
+      const uint8_t* row = img + (size_t)yy * W;
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (xx + j >= 0 && xx + j < W) v |= (uint32_t)__ldg(row + xx + j) << (8 * j);
+    }
+    tile[r * kCensus4Stride + w] = v;
+  }
+  __syncthreads();
+  const int t = threadIdx.x, x0 = bx + 4 * t;
+  if (x0 >= W) return;
+  const uint32_t* tw = tile + t;
+#pragma unroll 1
+  for (int oy = 0; oy < RY; ++oy) {
+    const int y = by + oy;
+    if (y >= H) break;
+    const uint32_t c = tw[(oy + CSH) * kCensus4Stride + 1], c7 = c & 0x7F7F7F7Fu;
+    uint32_t acc[NG];
+#pragma unroll
+    for (int g = 0; g < NG; ++g) acc[g] = 0;
+#pragma unroll
+    for (int dy = 0; dy <= 2 * CSH; ++dy) {
+#pragma unroll
+      for (int dx = -CSW; dx <= CSW; ++dx) {
+        const int k = dy * NC + dx + CSW, s = 4 + dx;
+        const uint32_t* w = tw + (oy + dy) * kCensus4Stride;  // shared: words x0-4, x0, x0+4
+        uint32_t a;
+        if (s == 0) a = w[0];
+        else if (s == 4) a = w[1];
+        else if (s == 8) a = w[2];  // the compiler loads each of the row's 3 words once
+        else if (s < 4) a = __byte_perm(w[0], w[1], (uint32_t)(s | (s + 1) << 4 | (s + 2) << 8 | (s + 3) << 12));
+        else a = __byte_perm(w[1], w[2], (uint32_t)((s - 4) | (s - 3) << 4 | (s - 2) << 8 | (s - 1) << 12));
+        const uint32_t d = (a | 0x80808080u) - c7;
+        const uint32_t lt = (~a & c) | (~(a ^ c) & ~d);  // top bit of each byte: a < c
+        acc[k >> 3] |= (lt >> (k & 7)) & (0x80808080u >> (k & 7));
+      }
+    }
+    Word* out = cs + (size_t)y * W;
+    const bool row_border = y < CSH || y >= H - CSH;
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+      const int x = x0 + p;
+      if (x >= W) break;
+      const uint32_t sel = (uint32_t)(p | (p + 4) << 4);
+      Word v;
+      if constexpr (NG == 8) {
+        const uint32_t hi = __byte_perm(__byte_perm(acc[3], acc[2], sel), __byte_perm(acc[1], acc[0], sel), 0x5410);
+        const uint32_t lo = __byte_perm(__byte_perm(acc[7], acc[6], sel), __byte_perm(acc[5], acc[4], sel), 0x5410);
+        v = (Word)(((((uint64_t)hi) << 32) | lo) >> (64 - NB));
+      } else {
+        const uint32_t w32 = __byte_perm(__byte_perm(acc[3], acc[2], sel), __byte_perm(acc[1], acc[0], sel), 0x5410);
+        v = (Word)(w32 >> (32 - NB));
+      }
+      if (row_border || x < CSW || x >= W - CSW) v = right ? (Word)0xFFFFFFFFu : (Word)0;
+      out[x] = v;
+    }
+  }
+}
+
+// Both views in one launch (blockIdx.z), RY rows and 512 pixels per block.
+template <typename Word, int CSW, int CSH, int RY>
+__global__ void __launch_bounds__(128, 4) k_census4(const uint8_t* __restrict__ img_l, const uint8_t* __restrict__ img_r,
+                                                 Word* __restrict__ cs_l, Word* __restrict__ cs_r, int W, int H) {
+  __shared__ uint32_t tile[census4_tile_words<CSH, RY>()];
+  const bool right = blockIdx.z == 1;
+  census4_tile<Word, CSW, CSH, RY>(right ? img_r : img_l, right ? cs_r : cs_l, W, H, right, blockIdx.x * 512,
+                                   blockIdx.y * RY, tile);
+}
+
 // ---------------------------------------------------------------------------------------------
 // Recurrence step shared by every plain scan (reference cusgm_ca.cu:1517-1564 and its 32/128
 // twins): L_p(d) = C_p(d) + min(L_q(d), L_q(d-1)+P1, L_q(d+1)+P1, m_q+P2) - m_q, uint32,
