@@ -173,6 +173,23 @@ __device__ __forceinline__ uint32_t step_g(uint32_t (&L)[NT], const uint32_t (&c
 // Columns x < max(0, min_d) are not written (no path reads them).
 // ---------------------------------------------------------------------------------------------
 // 128 pixels [bx, bx + 128) of row y, view `view`, by a 128-thread block (every thread calls it).
+// D costs of one pixel: popc(a ^ wp[STEP * d]) packed four per word, 16-byte stores.
+template <int D, typename Word, int STEP>
+__device__ __forceinline__ void cost3_px(const Word a, const Word* wp, uint8_t* __restrict__ out) {
+#pragma unroll
+  for (int v = 0; v < D / 16; ++v) {
+    uint32_t q[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      uint32_t c[4];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) c[b] = popc_word((Word)(a ^ wp[STEP * (16 * v + 4 * j + b)]));
+      q[j] = __byte_perm(__byte_perm(c[0], c[1], 0x0040u), __byte_perm(c[2], c[3], 0x0040u), 0x5410u);
+    }
+    reinterpret_cast<uint4*>(out)[v] = make_uint4(q[0], q[1], q[2], q[3]);
+  }
+}
+
 template <int K, typename Word>
 __device__ __forceinline__ void cost3_block(const Word* __restrict__ cs_l, const Word* __restrict__ cs_r,
                                             uint8_t* __restrict__ cost, const PlainParams& P, int view, int y, int bx,
@@ -200,22 +217,9 @@ __device__ __forceinline__ void cost3_block(const Word* __restrict__ cs_l, const
   }
   uint8_t* out = cost + (size_t)view * P.vstride + ((size_t)y * W + x) * D;
   if (!lr_cost) {
-#pragma unroll
-    for (int v = 0; v < D / 16; ++v) {
-      uint32_t q[4];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        uint32_t packed = 0;
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-          const int d = 16 * v + 4 * j + b;
-          const Word p = win[view == 0 ? threadIdx.x + (D - 1) - d : threadIdx.x + d];
-          packed |= popc_word((Word)(a ^ p)) << (8 * b);
-        }
-        q[j] = packed;
-      }
-      reinterpret_cast<uint4*>(out)[v] = make_uint4(q[0], q[1], q[2], q[3]);
-    }
+    // partner of disparity d: view 0 at win[t + D-1 - d], view 1 at win[t + d] (immediate offsets)
+    if (view == 0) cost3_px<D, Word, -1>(a, win + threadIdx.x + (D - 1), out);
+    else cost3_px<D, Word, 1>(a, win + threadIdx.x, out);
   } else {  // 5x5 right view: this pixel keeps its left-to-right cost
     const Word* g_own = cs_r + (size_t)y * W;
     const Word own0 = g_own[0];
@@ -839,6 +843,42 @@ __device__ __forceinline__ void init_wta_pixel(const uint32_t (&S2)[ND / 2], uin
 // else the invalid cost; view 1: pos = x + d + base, partner oth[pos] for 0 < pos < W else oth[0].
 // One CTA per (row, view); the partner row's census words in shared memory (W words).
 // Row y of view `view` by one block (every thread calls it); oth_s: W words of shared memory.
+// The 32 costs of one pixel at an initial-disparity level. View 0: partner x - d - base, valid
+// iff 0 < pos < W, else the invalid cost; view 1: partner x + d + base, oth[0] when out of range.
+// The valid disparities form one interval, taken as a bit mask once per pixel; partner loads use
+// immediate offsets from oth_s + x -/+ base (made only for valid d).
+template <typename Word, bool V0>
+__device__ __forceinline__ void cost3_init_px(const Word a, const Word* oth_s, int x, int base, int W,
+                                              uint32_t invalid, uint8_t* __restrict__ dst) {
+  // valid d: view 0  x-base-W < d < x-base;  view 1  -x-base < d < W-x-base
+  const int lo = V0 ? x - base - W + 1 : 1 - x - base;
+  const int hi = V0 ? x - base - 1 : W - 1 - x - base;
+  const int l = max(lo, 0), h = min(hi, kLevelRange - 1);
+  const uint32_t mask = l <= h ? (0xFFFFFFFFu >> (31 - h)) & (0xFFFFFFFFu << l) : 0u;
+  const Word* p = oth_s + (V0 ? x - base : x + base);
+  const Word oth0 = oth_s[0];
+  uint32_t q[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    uint32_t c[4];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int d = 4 * i + b;
+      const bool ok = (mask >> d) & 1u;
+      if (V0) {
+        c[b] = ok ? ((popc_word((Word)(a ^ p[-d])) + cost_adjust(d)) & 0xFFu) : invalid;
+      } else {
+        const Word o = ok ? p[d] : oth0;
+        c[b] = (popc_word((Word)(a ^ o)) + cost_adjust(d)) & 0xFFu;
+      }
+    }
+    q[i] = __byte_perm(__byte_perm(c[0], c[1], 0x0040u), __byte_perm(c[2], c[3], 0x0040u), 0x5410u);
+  }
+  uint4* o = reinterpret_cast<uint4*>(dst);
+  o[0] = make_uint4(q[0], q[1], q[2], q[3]);
+  o[1] = make_uint4(q[4], q[5], q[6], q[7]);
+}
+
 template <typename Word>
 __device__ __forceinline__ void cost3_init_row(const Word* __restrict__ cs_l, const Word* __restrict__ cs_r,
                                                const int16_t* __restrict__ init_l, const int16_t* __restrict__ init_r,
@@ -853,29 +893,9 @@ __device__ __forceinline__ void cost3_init_row(const Word* __restrict__ cs_l, co
   uint8_t* crow = cost + (size_t)view * P.vstride + (size_t)y * W * kLevelRange;
   for (int x = P.x0 + threadIdx.x; x < W; x += blockDim.x) {
     const int base = ib[x];
-    const Word a = own[x];
-    uint32_t q[8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      uint32_t packed = 0;
-#pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        const int d = 4 * i + b;
-        uint32_t v;
-        if (view == 0) {
-          const int pos = x - d - base;
-          v = (pos > 0 && pos < W) ? ((popc_word((Word)(a ^ oth_s[pos])) + cost_adjust(d)) & 0xFFu) : P.invalid_cost;
-        } else {
-          const int pos = x + d + base;
-          v = (popc_word((Word)(a ^ ((pos > 0 && pos < W) ? oth_s[pos] : oth_s[0]))) + cost_adjust(d)) & 0xFFu;
-        }
-        packed |= v << (8 * b);
-      }
-      q[i] = packed;
-    }
-    uint4* o = reinterpret_cast<uint4*>(crow + (size_t)x * kLevelRange);
-    o[0] = make_uint4(q[0], q[1], q[2], q[3]);
-    o[1] = make_uint4(q[4], q[5], q[6], q[7]);
+    uint8_t* dst = crow + (size_t)x * kLevelRange;
+    if (view == 0) cost3_init_px<Word, true>(own[x], oth_s, x, base, W, P.invalid_cost, dst);
+    else cost3_init_px<Word, false>(own[x], oth_s, x, base, W, P.invalid_cost, dst);
   }
 }
 
