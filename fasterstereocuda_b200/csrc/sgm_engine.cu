@@ -130,6 +130,7 @@ void sgm_set_process_error(const char* msg) { set_error(nullptr, "%s", msg); }
 struct sgm_engine {
   bool ready = false;
   int dev = 0;
+  int nsm = 148;  // SMs of the device (set in init)
   int W = 0, H = 0, M = 0, D = 0;
   sgm_option_t opt{};
   sgm_ext_options_t ext = default_ext();
@@ -280,6 +281,7 @@ int engine_init(sgm_engine* e, int W, int H, int M, int D, const sgm_option_t* o
   const int v = validate(e, W, H, D, o);
   if (v != SGM_OK) return v;
   SGM_CUDA_TRY(e, cudaGetDevice(&e->dev));
+  SGM_CUDA_TRY(e, cudaDeviceGetAttribute(&e->nsm, cudaDevAttrMultiProcessorCount, e->dev));
   e->W = W; e->H = H; e->M = M; e->D = D;
   e->opt = *o;
   e->print_log = log;
@@ -603,14 +605,22 @@ int engine_enqueue(sgm_engine* e, const uint8_t* dl_img, const uint8_t* dr_img, 
   int st = SGM_OK;
   // census of both images
   {
+    // 8 rows per block, or 2 when that leaves fewer blocks than SMs (small pyramid levels)
     constexpr int RY = sgm::kCensusRows;
-    dim3 g((W + 511) / 512, (H + RY - 1) / RY, 2), b(128);
-    if (e->opt.cs_type == 1)
-      st = SGM_LAUNCH(e, e->stream, "census", sgm::k_census4<uint64_t, 4, 3, RY><<<g, b, 0, e->stream>>>(
-                                                  dl_img, dr_img, (uint64_t*)e->cs[0], (uint64_t*)e->cs[1], W, H));
-    else
-      st = SGM_LAUNCH(e, e->stream, "census", sgm::k_census4<uint32_t, 2, 2, RY><<<g, b, 0, e->stream>>>(
-                                                  dl_img, dr_img, (uint32_t*)e->cs[0], (uint32_t*)e->cs[1], W, H));
+    const bool tall = (long)((W + 511) / 512) * ((H + RY - 1) / RY) * 2 >= e->nsm;
+    auto go = [&](auto kern, int ry, auto* csl, auto* csr) {
+      dim3 g((W + 511) / 512, (H + ry - 1) / ry, 2), b(128);
+      return SGM_LAUNCH(e, e->stream, "census", kern<<<g, b, 0, e->stream>>>(dl_img, dr_img, csl, csr, W, H));
+    };
+    if (e->opt.cs_type == 1) {
+      auto* l = (uint64_t*)e->cs[0];
+      auto* r = (uint64_t*)e->cs[1];
+      st = tall ? go(sgm::k_census4<uint64_t, 4, 3, RY>, RY, l, r) : go(sgm::k_census4<uint64_t, 4, 3, 2>, 2, l, r);
+    } else {
+      auto* l = (uint32_t*)e->cs[0];
+      auto* r = (uint32_t*)e->cs[1];
+      st = tall ? go(sgm::k_census4<uint32_t, 2, 2, RY>, RY, l, r) : go(sgm::k_census4<uint32_t, 2, 2, 2>, 2, l, r);
+    }
   }
   // right-view initial disparities when checking consistency at an init level
   const int16_t* dinit_r = nullptr;
