@@ -101,6 +101,10 @@ __device__ __forceinline__ float fstep(float (&L)[K], const float (&c)[K], float
   return warp_min(mn);
 }
 
+// Inputs of the next kPF pixels are loaded ahead in a register ring (each line owns its pixels, so
+// the running sum can be read ahead of the stores of earlier pixels).
+constexpr int kPF = 4;
+
 template <int K>
 __global__ void __launch_bounds__(256) k_float_fwd(const float* __restrict__ cost, const float* __restrict__ p1m,
                                                    const float* __restrict__ p2m, float* __restrict__ sum,
@@ -110,29 +114,51 @@ __global__ void __launch_bounds__(256) k_float_fwd(const float* __restrict__ cos
   if (line >= g.lines) return;
   const int D = 32 * K;
   float* ck = ckpt + (size_t)line * g.nseg * D;
-  float L[K], c[K];
+  float L[K];
   int ch[K];
   float m = 0.f;
-  for (int s = 0; s < g.len; ++s) {
+  float rc[kPF][K], rs[kPF][K], rp1[kPF], rp2[kPF];
+  auto fetch = [&](int j, int s) {
     const size_t p = pix(g, line, s);
-    const float* cp = cost + p * D + lane * K;
 #pragma unroll
-    for (int j = 0; j < K; ++j) c[j] = cp[j];
-    if (s % kSeg == 0 && s > 0) {  // state entering this segment
-#pragma unroll
-      for (int j = 0; j < K; ++j) ck[(size_t)(s / kSeg) * D + lane * K + j] = L[j];
+    for (int i = 0; i < K; ++i) {
+      rc[j][i] = cost[p * D + lane * K + i];
+      rs[j][i] = first ? 0.f : sum[p * D + lane * K + i];
     }
-    if (s == 0) {
-      float mn = kInf;
+    rp1[j] = p1m[p];
+    rp2[j] = p2m[p];
+  };
 #pragma unroll
-      for (int j = 0; j < K; ++j) { L[j] = c[j]; mn = fminf(mn, c[j]); }
-      m = warp_min(mn);
-    } else {
-      m = fstep<K>(L, c, m, p1m[p], p2m[p], lane, ch);
+  for (int j = 0; j < kPF; ++j)
+    if (j < g.len) fetch(j, j);
+  for (int s0 = 0; s0 < g.len; s0 += kPF) {
+#pragma unroll
+    for (int j = 0; j < kPF; ++j) {
+      const int s = s0 + j;
+      if (s < g.len) {
+        const size_t p = pix(g, line, s);
+        float c[K], old[K];
+#pragma unroll
+        for (int i = 0; i < K; ++i) { c[i] = rc[j][i]; old[i] = rs[j][i]; }
+        const float P1 = rp1[j], P2 = rp2[j];
+        if (s + kPF < g.len) fetch(j, s + kPF);
+        if (s % kSeg == 0 && s > 0) {  // state entering this segment
+#pragma unroll
+          for (int i = 0; i < K; ++i) ck[(size_t)(s / kSeg) * D + lane * K + i] = L[i];
+        }
+        if (s == 0) {
+          float mn = kInf;
+#pragma unroll
+          for (int i = 0; i < K; ++i) { L[i] = c[i]; mn = fminf(mn, c[i]); }
+          m = warp_min(mn);
+        } else {
+          m = fstep<K>(L, c, m, P1, P2, lane, ch);
+        }
+        float* sp = sum + p * D + lane * K;
+#pragma unroll
+        for (int i = 0; i < K; ++i) sp[i] = first ? L[i] : old[i] + L[i];
+      }
     }
-    float* sp = sum + p * D + lane * K;
-#pragma unroll
-    for (int j = 0; j < K; ++j) sp[j] = first ? L[j] : sp[j] + L[j];
   }
 }
 
@@ -204,33 +230,72 @@ __global__ void __launch_bounds__(128) k_float_bwd(const float* __restrict__ cos
       for (int j = 0; j < K; ++j) mn = fminf(mn, L[j]);
       m = warp_min(mn);
     }
-    for (int s = s0; s < s1; ++s) {
-      const size_t p = pix(g, line, s);
-      const float* cp = cost + p * D + lane * K;
+    {
+      // inputs of the segment's pixels through a kPF-deep register ring
+      float rc[kPF][K], rp1[kPF], rp2[kPF];
+      auto fetch = [&](int j, int s) {
+        const size_t p = pix(g, line, s);
 #pragma unroll
-      for (int j = 0; j < K; ++j) c[j] = cp[j];
-      if (s == 0) {
-        float mn = kInf;
+        for (int i = 0; i < K; ++i) rc[j][i] = cost[p * D + lane * K + i];
+        rp1[j] = p1m[p];
+        rp2[j] = p2m[p];
+      };
 #pragma unroll
-        for (int j = 0; j < K; ++j) { L[j] = c[j]; mn = fminf(mn, c[j]); }
-        m = warp_min(mn);
-      } else {
-        m = fstep<K>(L, c, m, p1m[p], p2m[p], lane, ch);
+      for (int j = 0; j < kPF; ++j)
+        if (s0 + j < s1) fetch(j, s0 + j);
+      for (int b = s0; b < s1; b += kPF) {
+#pragma unroll
+        for (int j = 0; j < kPF; ++j) {
+          const int s = b + j;
+          if (s < s1) {
+#pragma unroll
+            for (int i = 0; i < K; ++i) c[i] = rc[j][i];
+            const float P1 = rp1[j], P2 = rp2[j];
+            if (s + kPF < s1) fetch(j, s + kPF);
+            if (s == 0) {
+              float mn = kInf;
+#pragma unroll
+              for (int i = 0; i < K; ++i) { L[i] = c[i]; mn = fminf(mn, c[i]); }
+              m = warp_min(mn);
+            } else {
+              m = fstep<K>(L, c, m, P1, P2, lane, ch);
+            }
+#pragma unroll
+            for (int i = 0; i < K; ++i) st[(size_t)(1 + s - s0) * D + lane * K + i] = L[i];
+          }
+        }
       }
-#pragma unroll
-      for (int j = 0; j < K; ++j) st[(size_t)(1 + s - s0) * D + lane * K + j] = L[j];
     }
     __syncwarp();
-    // adjoint through the segment, last pixel first
-    for (int s = s1 - 1; s >= s0; --s) {
+    // adjoint through the segment, last pixel first; its inputs through a register ring
+    float rg[kPF][K], rgc[kPF][K], rq1[kPF], rq2[kPF];
+    auto fetch_b = [&](int j, int s) {
       const size_t p = pix(g, line, s);
-      const float* gs = gsum + p * D + lane * K;
-      float gl[K];
 #pragma unroll
-      for (int j = 0; j < K; ++j) gl[j] = gs[j] + gnext[j];
+      for (int i = 0; i < K; ++i) {
+        rg[j][i] = gsum[p * D + lane * K + i];
+        rgc[j][i] = first ? 0.f : gcost[p * D + lane * K + i];
+      }
+      rq1[j] = p1m[p];
+      rq2[j] = p2m[p];
+    };
+#pragma unroll
+    for (int j = 0; j < kPF; ++j)
+      if (s1 - 1 - j >= s0) fetch_b(j, s1 - 1 - j);
+    for (int b = s1 - 1; b >= s0; b -= kPF)
+#pragma unroll
+    for (int jj = 0; jj < kPF; ++jj) {
+      const int s = b - jj;
+      if (s < s0) break;
+      const size_t p = pix(g, line, s);
+      float gl[K], gco[K];
+#pragma unroll
+      for (int j = 0; j < K; ++j) { gl[j] = rg[jj][j] + gnext[j]; gco[j] = rgc[jj][j]; }
+      const float P1 = rq1[jj], P2 = rq2[jj];
+      if (s - kPF >= s0) fetch_b(jj, s - kPF);
       float* gc = gcost + p * D + lane * K;
 #pragma unroll
-      for (int j = 0; j < K; ++j) gc[j] = first ? gl[j] : gc[j] + gl[j];
+      for (int j = 0; j < K; ++j) gc[j] = first ? gl[j] : gco[j] + gl[j];
       if (s == 0) break;
       // previous state L_q = L(s-1): slot (s - s0) (slot 0 = checkpoint when s == s0)
       const float* q = st + (size_t)(s - s0) * D;
@@ -250,7 +315,7 @@ __global__ void __launch_bounds__(128) k_float_bwd(const float* __restrict__ cos
       // choices at p
       float lm[K], lp[K];
       neighbours<K>(Lq, lane, lm, lp);
-      const float P1 = p1m[p], P2 = p2m[p], jump = mq + P2;
+      const float jump = mq + P2;
       float g1 = 0.f, g2 = 0.f, gall = 0.f;
       float gsame[K], gm1[K], gp1v[K];
 #pragma unroll
