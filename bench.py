@@ -317,7 +317,7 @@ def run_ours(a, rank, world, local_rank):
         bit_exact = bool(np.array_equal(outs[0].cpu().numpy().view(np.uint32), exp.view(np.uint32)))
 
     # autotune: the lane split of the scanline kernels that is fastest at this concurrency
-    # (every split gives the same disparities); two untimed steps per candidate
+    # (every split gives the same disparities); one untimed and six timed steps per candidate
     tuning = a.tuning or None
     chosen, chosen_init = None, None  # tunings applied to matchers made later
     if not a.tuning:
@@ -326,7 +326,7 @@ def run_ours(a, rank, world, local_rank):
             step()
             torch.cuda.synchronize()
             t0c = time.perf_counter()
-            for _ in range(2):
+            for _ in range(6):
                 step()
             torch.cuda.synchronize()
             return max_over_ranks(time.perf_counter() - t0c)

@@ -808,6 +808,7 @@ __device__ __forceinline__ void fill_p2_table(uint32_t* tab, const InitParams& P
 }
 __device__ __forceinline__ uint32_t p2_term(const uint32_t* tab, int k, const InitParams& P) {
   if (k < kP2Tab) return tab[k];
+  if (P.p2s >= 0 && k > P.p2s) return (uint32_t)(P.p1s > 0 ? P.p1s : 0);  // P2 / k == 0
   const int32_t q = P.p2s / k;
   return (uint32_t)(P.p1s > q ? P.p1s : q);
 }
