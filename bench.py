@@ -146,6 +146,8 @@ def alg_bytes(kernel, W, H, D, nviews, census_bytes):
     n = W * H
     if kernel.startswith("hpaths"):
         return nviews * (2 * V + 2 * census_bytes * n)
+    if kernel.startswith("vpaths_bt"):  # the bottom-to-top column pass launched on its own: no
+        return 0                          # counterpart in the minimal design's traffic
     if kernel.startswith("vpaths"):
         return nviews * (2 * V + 4 * n)
     if kernel == "census":

@@ -138,6 +138,8 @@ struct sgm_engine {
   bool has_cam = false;
   sgm_camera_t cam{};
   cudaStream_t stream = nullptr;
+  cudaStream_t side = nullptr;                       // the bottom-to-top column pass beside the row scans
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;  // around the side stream's work
   std::string err;
   int64_t launches = 0;
   // device buffers
@@ -198,6 +200,11 @@ struct sgm_engine {
     dfree(init_tmp); dfree(key); dfree(label); dfree(count);
     if (stream) cudaStreamDestroy(stream);
     stream = nullptr;
+    if (side) cudaStreamDestroy(side);
+    side = nullptr;
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    ev_fork = ev_join = nullptr;
     ready = false;
   }
 };
@@ -286,6 +293,9 @@ int engine_init(sgm_engine* e, int W, int H, int M, int D, const sgm_option_t* o
   e->opt = *o;
   e->print_log = log;
   SGM_CUDA_TRY(e, cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+  SGM_CUDA_TRY(e, cudaStreamCreateWithFlags(&e->side, cudaStreamNonBlocking));
+  SGM_CUDA_TRY(e, cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming));
+  SGM_CUDA_TRY(e, cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming));
   const size_t N = e->npix();
   const size_t V = e->vol() * e->nviews();  // the right view's volumes only with the LR check
   for (int i = 0; i < 2; ++i) {
@@ -361,11 +371,10 @@ constexpr bool lanes_ok(int G) {
 constexpr int kDefaultRowLanes = 8, kDefaultColLanes = 4;
 
 template <int K>
-int launch_rows3(sgm_engine* e, int G, const sgm::PlainParams& P, int nv) {
+int launch_rows3(sgm_engine* e, int G, const sgm::PlainParams& P, int nv, cudaStream_t s) {
   if (!lanes_ok<K>(G)) G = kDefaultRowLanes;
   const long threads = (long)nv * 2 * e->H * G;
   const int blocks = (int)((threads + 127) / 128);
-  cudaStream_t s = e->stream;
   auto go = [&](auto kern) {
     return SGM_LAUNCH(e, s, "hpaths_plain", kern<<<blocks, 128, 0, s>>>(e->cost, e->lr, e->rl, P, nv));
   };
@@ -381,27 +390,47 @@ int launch_rows3(sgm_engine* e, int G, const sgm::PlainParams& P, int nv) {
   }
 }
 
-template <int K>
-int launch_cols3(sgm_engine* e, int G, const sgm::PlainParams& P, const sgm::WtaParams& Q, float* wta, int nv) {
+// pass: 0 both column passes, 1 bottom-to-top only, 2 top-to-bottom + sum + WTA only
+template <int K, int PASS>
+int launch_cols3_pass(sgm_engine* e, int G, const sgm::PlainParams& P, const sgm::WtaParams& Q, float* wta, int nv,
+                      cudaStream_t s) {
   if (!lanes_ok<K>(G)) G = kDefaultColLanes;
   const long threads = (long)e->W * G;
   dim3 grid((unsigned)((threads + 127) / 128), nv);
   const size_t smem = (size_t)(128 / G) * sgm::vpaths3_col_smem<K>();
-  cudaStream_t s = e->stream;
+  const char* name = PASS == 1 ? "vpaths_bt_plain" : "vpaths_wta_plain";
   auto go = [&](auto kern) {
-    return SGM_LAUNCH(e, s, "vpaths_wta_plain",
-                      kern<<<grid, 128, smem, s>>>(e->cost, e->lr, e->rl, e->bt, wta, P, Q));
+    return SGM_LAUNCH(e, s, name, kern<<<grid, 128, smem, s>>>(e->cost, e->lr, e->rl, e->bt, wta, P, Q));
   };
   if constexpr (K == 4) {
-    return G == 2 ? go(sgm::k_vpaths3<K, 2, pf3v<K, 2>()>) : go(sgm::k_vpaths3<K, 4, pf3v<K, 4>()>);
+    return G == 2 ? go(sgm::k_vpaths3<K, 2, pf3v<K, 2>(), PASS>) : go(sgm::k_vpaths3<K, 4, pf3v<K, 4>(), PASS>);
   } else {
     switch (G) {
-      case 1: return go(sgm::k_vpaths3<K, 1, pf3v<K, 1>()>);
-      case 2: return go(sgm::k_vpaths3<K, 2, pf3v<K, 2>()>);
-      case 8: return go(sgm::k_vpaths3<K, 8, pf3v<K, 8>()>);
-      default: return go(sgm::k_vpaths3<K, 4, pf3v<K, 4>()>);
+      case 1: return go(sgm::k_vpaths3<K, 1, pf3v<K, 1>(), PASS>);
+      case 2: return go(sgm::k_vpaths3<K, 2, pf3v<K, 2>(), PASS>);
+      case 8: return go(sgm::k_vpaths3<K, 8, pf3v<K, 8>(), PASS>);
+      default: return go(sgm::k_vpaths3<K, 4, pf3v<K, 4>(), PASS>);
     }
   }
+}
+
+// The bottom-to-top column pass depends only on the cost volume, so it runs on the matcher's side
+// stream while the row scans run on s; the top-to-bottom pass (which sums all four paths) follows
+// the join. In a captured graph the side stream joins the capture through ev_fork.
+constexpr bool kSplitColumns = true;
+
+template <typename SideWork, typename MainWork>
+int fork_join(sgm_engine* e, cudaStream_t s, SideWork side_work, MainWork main_work) {
+  SGM_CUDA_TRY(e, cudaEventRecord(e->ev_fork, s));
+  SGM_CUDA_TRY(e, cudaStreamWaitEvent(e->side, e->ev_fork, 0));
+  int st = side_work(e->side);
+  if (!st) st = main_work(s);
+  // join even after an error, so that a capture in progress is not left with a forked stream
+  const cudaError_t r = cudaEventRecord(e->ev_join, e->side);
+  const cudaError_t w = r == cudaSuccess ? cudaStreamWaitEvent(s, e->ev_join, 0) : r;
+  if (st) return st;
+  SGM_CUDA_TRY(e, w);
+  return SGM_OK;
 }
 
 template <int K, typename Word>
@@ -416,11 +445,28 @@ int launch_plain(sgm_engine* e, const Word* csl, const Word* csr, float* wta) {
                      e->opt.p2_init >= e->opt.p1 &&
                      (e->ext.tie_rule == sgm::kTieLowest || e->ext.tie_rule == sgm::kTieRefB200);
   int st;
+  const bool cols_v3 = (e->tune_col_kernel == 3 || e->tune_col_kernel == 0) && v3_ok;
+  sgm::WtaParams Q;
+  Q.uniqueness = e->opt.unique_threshold;
+  Q.tie_rule = e->ext.tie_rule;
+  const bool warp_kernel = (K <= 4);
+  Q.rows = warp_kernel ? (e->H / 2) * 2 : e->H;
+  Q.dmax_excl = warp_kernel ? 32 * K : 32 * K - 1;
+  Q.dstride = e->npix();
   if ((e->tune_row_kernel == 3 || e->tune_row_kernel == 0) && v3_ok) {
     dim3 cg((e->W + 127) / 128, e->H, nv);
     st = SGM_LAUNCH(e, e->stream, "cost", sgm::k_cost3<K, Word><<<cg, 128, 0, e->stream>>>(csl, csr, e->cost, P));
     if (st) return st;
-    st = launch_rows3<K>(e, e->tune_row_lanes, P, nv);
+    if (kSplitColumns && cols_v3) {
+      e->bt_stored = true;
+      const int gc = e->tune_col_lanes;
+      st = fork_join(
+          e, e->stream, [&](cudaStream_t ss) { return launch_cols3_pass<K, 1>(e, gc, P, Q, wta, nv, ss); },
+          [&](cudaStream_t ms) { return launch_rows3<K>(e, e->tune_row_lanes, P, nv, ms); });
+      if (st) return st;
+      return launch_cols3_pass<K, 2>(e, gc, P, Q, wta, nv, e->stream);
+    }
+    st = launch_rows3<K>(e, e->tune_row_lanes, P, nv, e->stream);
   } else if (e->tune_row_kernel == 1) {  // whole census rows of R scanlines in shared memory
     const int R = e->tune_rows > 0 ? e->tune_rows : rows_per_cta(e->W, sizeof(Word), false);
     const size_t smem = (size_t)R * 2 * e->W * sizeof(Word);
@@ -441,18 +487,11 @@ int launch_plain(sgm_engine* e, const Word* csl, const Word* csr, float* wta) {
     st = SGM_LAUNCH(e, e->stream, "hpaths_plain", hk<<<hg, hb, smem, e->stream>>>(csl, csr, e->cost, e->lr, e->rl, P));
   }
   if (st) return st;
-  sgm::WtaParams Q;
-  Q.uniqueness = e->opt.unique_threshold;
-  Q.tie_rule = e->ext.tie_rule;
-  const bool warp_kernel = (K <= 4);
-  Q.rows = warp_kernel ? (e->H / 2) * 2 : e->H;
-  Q.dmax_excl = warp_kernel ? 32 * K : 32 * K - 1;
-  Q.dstride = e->npix();
   int C = 8, bt_smem = 0;
   size_t vsmem = 0;
-  if ((e->tune_col_kernel == 3 || e->tune_col_kernel == 0) && v3_ok) {
+  if (cols_v3) {
     e->bt_stored = true;
-    return launch_cols3<K>(e, e->tune_col_lanes, P, Q, wta, nv);
+    return launch_cols3_pass<K, 0>(e, e->tune_col_lanes, P, Q, wta, nv, e->stream);
   }
   if (e->tune_col_kernel != 2) {
     C = e->tune_cols > 0 ? e->tune_cols : 8;
@@ -474,39 +513,43 @@ int launch_plain(sgm_engine* e, const Word* csl, const Word* csr, float* wta) {
 constexpr int kDefaultInitRowLanes = 8, kDefaultInitColLanes = 8;
 
 template <typename Word>
-int launch_init3(sgm_engine* e, const Word* csl, const Word* csr, const int16_t* il, const int16_t* ir, float* wta,
-                 const sgm::InitParams& P, const sgm::WtaParams& Q, bool rows3, bool cols3) {
+int init3_cost(sgm_engine* e, const Word* csl, const Word* csr, const int16_t* il, const int16_t* ir,
+               const sgm::InitParams& P, cudaStream_t s) {
+  const size_t csmem = (size_t)e->W * sizeof(Word);
+  auto ck = sgm::k_cost3_init<Word>;
+  SGM_CUDA_TRY(e, sgm::allow_max_dynamic_smem(ck));
+  return SGM_LAUNCH(e, s, "cost", ck<<<dim3(e->H, e->nviews()), 256, csmem, s>>>(csl, csr, il, ir, e->cost, P));
+}
+
+inline int init3_rows(sgm_engine* e, const int16_t* il, const int16_t* ir, const sgm::InitParams& P,
+                      cudaStream_t s) {
   const int nv = e->nviews();
-  cudaStream_t s = e->stream;
-  int st = SGM_OK;
-  if (rows3) {
-    const size_t csmem = (size_t)e->W * sizeof(Word);
-    auto ck = sgm::k_cost3_init<Word>;
-    SGM_CUDA_TRY(e, sgm::allow_max_dynamic_smem(ck));
-    st = SGM_LAUNCH(e, s, "cost", ck<<<dim3(e->H, nv), 256, csmem, s>>>(csl, csr, il, ir, e->cost, P));
-    if (st) return st;
-    int G = e->tune_row_lanes;
-    if (G != 2 && G != 4 && G != 8) G = kDefaultInitRowLanes;
-    const long threads = (long)nv * 2 * e->H * G;
-    const int blocks = (int)((threads + 127) / 128);
-    auto go = [&](auto kern) {
-      return SGM_LAUNCH(e, s, "hpaths_init", kern<<<blocks, 128, 0, s>>>(e->cost, il, ir, e->lr, e->rl, P, nv));
-    };
-    st = G == 2 ? go(sgm::k_hpaths3_init<2, 8>) : G == 8 ? go(sgm::k_hpaths3_init<8, 8>) : go(sgm::k_hpaths3_init<4, 8>);
-    if (st) return st;
-  }
-  if (cols3) {
-    int G = e->tune_col_lanes;
-    if (G != 2 && G != 4 && G != 8) G = kDefaultInitColLanes;
-    e->bt_stored = true;
-    dim3 grid((unsigned)(((long)e->W * G + 127) / 128), nv);
-    auto go = [&](auto kern) {
-      return SGM_LAUNCH(e, s, "vpaths_wta_init",
-                        kern<<<grid, 128, 0, s>>>(e->cost, e->lr, e->rl, il, ir, e->bt, wta, P, Q));
-    };
-    st = G == 2 ? go(sgm::k_vpaths3_init<2, 1>) : G == 8 ? go(sgm::k_vpaths3_init<8, 4>) : go(sgm::k_vpaths3_init<4, 4>);
-  }
-  return st;
+  int G = e->tune_row_lanes;
+  if (G != 2 && G != 4 && G != 8) G = kDefaultInitRowLanes;
+  const long threads = (long)nv * 2 * e->H * G;
+  const int blocks = (int)((threads + 127) / 128);
+  auto go = [&](auto kern) {
+    return SGM_LAUNCH(e, s, "hpaths_init", kern<<<blocks, 128, 0, s>>>(e->cost, il, ir, e->lr, e->rl, P, nv));
+  };
+  return G == 2 ? go(sgm::k_hpaths3_init<2, 8>) : G == 8 ? go(sgm::k_hpaths3_init<8, 8>) : go(sgm::k_hpaths3_init<4, 8>);
+}
+
+// PASS as in launch_cols3_pass
+template <int PASS>
+int init3_cols(sgm_engine* e, const int16_t* il, const int16_t* ir, float* wta, const sgm::InitParams& P,
+               const sgm::WtaParams& Q, cudaStream_t s) {
+  const int nv = e->nviews();
+  int G = e->tune_col_lanes;
+  if (G != 2 && G != 4 && G != 8) G = kDefaultInitColLanes;
+  e->bt_stored = true;
+  dim3 grid((unsigned)(((long)e->W * G + 127) / 128), nv);
+  const char* name = PASS == 1 ? "vpaths_bt_init" : "vpaths_wta_init";
+  auto go = [&](auto kern) {
+    return SGM_LAUNCH(e, s, name, kern<<<grid, 128, 0, s>>>(e->cost, e->lr, e->rl, il, ir, e->bt, wta, P, Q));
+  };
+  return G == 2   ? go(sgm::k_vpaths3_init<2, 1, PASS>)
+         : G == 8 ? go(sgm::k_vpaths3_init<8, 4, PASS>)
+                  : go(sgm::k_vpaths3_init<4, 4, PASS>);
 }
 
 template <typename Word>
@@ -528,8 +571,17 @@ int launch_init(sgm_engine* e, const Word* csl, const Word* csr, const int16_t* 
   const bool rows3 = v3_ok && (e->tune_row_kernel == 0 || e->tune_row_kernel == 3);
   const bool cols3 = v3_ok && (e->tune_col_kernel == 0 || e->tune_col_kernel == 3);
   int st;
+  if (rows3 && cols3 && kSplitColumns) {  // bottom-to-top column pass beside the row scans
+    st = init3_cost<Word>(e, csl, csr, il, ir, P, e->stream);
+    if (!st)
+      st = fork_join(
+          e, e->stream, [&](cudaStream_t ss) { return init3_cols<1>(e, il, ir, wta, P, Q3, ss); },
+          [&](cudaStream_t ms) { return init3_rows(e, il, ir, P, ms); });
+    return st ? st : init3_cols<2>(e, il, ir, wta, P, Q3, e->stream);
+  }
   if (rows3) {
-    st = launch_init3<Word>(e, csl, csr, il, ir, wta, P, Q3, true, false);
+    st = init3_cost<Word>(e, csl, csr, il, ir, P, e->stream);
+    if (!st) st = init3_rows(e, il, ir, P, e->stream);
   } else if (e->tune_row_kernel == 1) {  // whole census rows of R scanlines in shared memory
     const int R = e->tune_rows > 0 ? e->tune_rows : rows_per_cta(e->W, sizeof(Word), true);
     const size_t smem = (size_t)R * e->W * (2 * sizeof(Word) + 2);
@@ -566,7 +618,7 @@ int launch_init(sgm_engine* e, const Word* csl, const Word* csr, const int16_t* 
   Q.dstride = e->npix();
   int C = 8, bt_smem = 0;
   size_t vsmem = 0;
-  if (cols3) return launch_init3<Word>(e, csl, csr, il, ir, wta, P, Q3, false, true);
+  if (cols3) return init3_cols<0>(e, il, ir, wta, P, Q3, e->stream);
   if (e->tune_col_kernel != 2) {
     C = e->tune_cols > 0 ? e->tune_cols : 8;
     e->bt_stored = true;

@@ -308,7 +308,8 @@ template <int K, int G, int PF>
 // five CTAs per SM (at most 96 registers) where a lane holds at most 32 disparities and G >= 2:
 // many concurrent pairs are occupancy-bound (plain 1242x375x64: +5 % pairs/s over the
 // unconstrained 113-128 registers); wider slices would spill
-__global__ void __launch_bounds__(128, (G >= 2 && 32 * K / G <= 32) ? 5 : 1) k_hpaths3(const uint8_t* __restrict__ cost, uint8_t* __restrict__ lr,
+__global__ void __launch_bounds__(128, (G >= 2 && 32 * K / G <= 32) ? 5 : 1)
+    k_hpaths3(const uint8_t* __restrict__ cost, uint8_t* __restrict__ lr,
                                                  uint8_t* __restrict__ rl, PlainParams P, int nviews) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   hpaths3_lane<K, G, PF>(cost, lr, rl, P, nviews, t / G, threadIdx.x % G);
@@ -328,7 +329,9 @@ __host__ __device__ constexpr size_t vpaths3_col_smem() { return (size_t)(16 * K
 // Column xc of view `view` (lane g of its G lanes); colS: this column's D/2 + 1 words of shared
 // memory. Every lane of the warp calls it (same H); xc >= W: the lane follows column W-1 without
 // storing.
-template <int K, int G, int PF>
+// PASS: 0 both passes, 1 the bottom-to-top pass only, 2 the top-to-bottom pass only (reads the
+// stored bottom-to-top volume), so that the two can be launched around the row scans.
+template <int K, int G, int PF, int PASS = 0>
 __device__ __forceinline__ void vpaths3_lane(const uint8_t* __restrict__ cost, const uint8_t* __restrict__ lr,
                                              const uint8_t* __restrict__ rl, uint8_t* __restrict__ bt,
                                              float* __restrict__ disp, const PlainParams& P, const WtaParams& Q,
@@ -349,170 +352,175 @@ __device__ __forceinline__ void vpaths3_lane(const uint8_t* __restrict__ cost, c
   uint32_t L[NT], c[NT], out[NR];
   uint32_t ring[PF][NR];
   uint32_t m = 0;
-  // bottom -> top
+  if constexpr (PASS != 2) {  // bottom-to-top pass (stores its path costs)
+    // bottom -> top
 #pragma unroll
-  for (int j = 0; j < PF; ++j)
-    if (j < H) ld_slice<NR>(cv + (size_t)(H - 1 - j) * rs, ring[j]);
-  for (int s0 = 0; s0 < H; s0 += PF) {
+    for (int j = 0; j < PF; ++j)
+      if (j < H) ld_slice<NR>(cv + (size_t)(H - 1 - j) * rs, ring[j]);
+    for (int s0 = 0; s0 < H; s0 += PF) {
 #pragma unroll
-    for (int j = 0; j < PF; ++j) {
-      const int s = s0 + j;
-      if (s < H) {
-        const int y = H - 1 - s;
-        widen_slice<NR>(ring[j], c);
-        if (s + PF < H) ld_slice<NR>(cv + (size_t)(y - PF) * rs, ring[j]);
-        m = s == 0 ? first_g<NT, G>(L, c) : step_g<NT, G>(L, c, m, p1x2, p2m1, g);
-        narrow_slice<NR>(L, out);
-        if (computed) st_slice<NR>(btv + (size_t)y * rs, out);
+      for (int j = 0; j < PF; ++j) {
+        const int s = s0 + j;
+        if (s < H) {
+          const int y = H - 1 - s;
+          widen_slice<NR>(ring[j], c);
+          if (s + PF < H) ld_slice<NR>(cv + (size_t)(y - PF) * rs, ring[j]);
+          m = s == 0 ? first_g<NT, G>(L, c) : step_g<NT, G>(L, c, m, p1x2, p2m1, g);
+          narrow_slice<NR>(L, out);
+          if (computed) st_slice<NR>(btv + (size_t)y * rs, out);
+        }
       }
     }
   }
-  // top -> bottom + sum + WTA; the other three paths of row y + PF are loaded at row y
-  const uint8_t* lrv = lr + vo;
-  const uint8_t* rlv = rl + vo;
-  uint32_t ra[PF][NR], rb[PF][NR], re[PF][NR];
-#pragma unroll
-  for (int j = 0; j < PF; ++j) {
-    if (j < H) {
-      ld_slice<NR>(cv + (size_t)j * rs, ring[j]);
-      ld_slice<NR>(btv + (size_t)j * rs, ra[j]);
-      ld_slice<NR>(lrv + (size_t)j * rs, rb[j]);
-      ld_slice<NR>(rlv + (size_t)j * rs, re[j]);
-    }
-  }
-  for (int y0 = 0; y0 < H; y0 += PF) {
+  if constexpr (PASS != 1) {  // top-to-bottom pass with the 4-path sum and the WTA
+    // top -> bottom + sum + WTA; the other three paths of row y + PF are loaded at row y
+    const uint8_t* lrv = lr + vo;
+    const uint8_t* rlv = rl + vo;
+    uint32_t ra[PF][NR], rb[PF][NR], re[PF][NR];
 #pragma unroll
     for (int j = 0; j < PF; ++j) {
-      const int y = y0 + j;
-      if (y < H) {
-        uint32_t wa[NT], wb[NT], we[NT];
-        widen_slice<NR>(ring[j], c);
-        widen_slice<NR>(ra[j], wa);
-        widen_slice<NR>(rb[j], wb);
-        widen_slice<NR>(re[j], we);
-        if (y + PF < H) {
-          const size_t o = (size_t)(y + PF) * rs;
-          ld_slice<NR>(cv + o, ring[j]);
-          ld_slice<NR>(btv + o, ra[j]);
-          ld_slice<NR>(lrv + o, rb[j]);
-          ld_slice<NR>(rlv + o, re[j]);
-        }
-        m = y == 0 ? first_g<NT, G>(L, c) : step_g<NT, G>(L, c, m, p1x2, p2m1, g);
-        if (y >= 5 && y <= H - 5 && y < Q.rows) {  // uniform over the warp
-          // S = the four u8 path costs summed (< 1024). Keys S << 6 | (d mod 64) per block of
-          // disparities: D = 32 one block; D = 64: d < 32 (A) and d >= 32 (B), the reference's two
-          // stores; D = 128: d < 64 and d >= 64.
-          constexpr int SPLIT = D == 32 ? 64 : (D == 64 ? 32 : 64);  // first d of the second block
-          uint32_t acc0 = 0xFFFFFFFFu, acc1 = 0xFFFFFFFFu;
-          if constexpr (G > 1) {
-            // every d of this lane lies in one block: one tree of SIMD minima
-            uint32_t key[NT];
-            const uint32_t dl = (uint32_t)((g * SB) & 63) * 0x10001u + 0x10000u;  // (d, d+1) mod 64 of word 0
+      if (j < H) {
+        ld_slice<NR>(cv + (size_t)j * rs, ring[j]);
+        ld_slice<NR>(btv + (size_t)j * rs, ra[j]);
+        ld_slice<NR>(lrv + (size_t)j * rs, rb[j]);
+        ld_slice<NR>(rlv + (size_t)j * rs, re[j]);
+      }
+    }
+    for (int y0 = 0; y0 < H; y0 += PF) {
 #pragma unroll
-            for (int k = 0; k < NT; ++k) {
-              const uint32_t sk = (L[k] & 0x00FF00FFu) + wa[k] + wb[k] + we[k];
-              myS[k] = sk;
-              key[k] = sk * 64u + dl + (uint32_t)(2 * k) * 0x10001u;
-            }
-            uint32_t t = key[0];
-            if constexpr (NT > 1) {
-#pragma unroll
-              for (int st = 1; st < NT; st *= 3) {
-#pragma unroll
-                for (int k = 0; k + st < NT; k += 3 * st)
-                  key[k] = k + 2 * st < NT ? __vimin3_u16x2(key[k], key[k + st], key[k + 2 * st])
-                                           : min16x2(key[k], key[k + st]);
-              }
-              t = key[0];
-            }
-            if (g * SB < SPLIT) acc0 = t;
-            else acc1 = t;
-          } else {
-#pragma unroll
-            for (int k = 0; k < NT; ++k) {
-              const uint32_t sk = (L[k] & 0x00FF00FFu) + wa[k] + wb[k] + we[k];
-              myS[k] = sk;
-              const uint32_t d0 = (uint32_t)(2 * (g * NT + k));
-              const uint32_t key = sk * 64u + ((d0 & 63u) | (((d0 + 1u) & 63u) << 16));
-              if ((int)d0 < SPLIT) acc0 = min16x2(acc0, key);
-              else acc1 = min16x2(acc1, key);
-            }
+      for (int j = 0; j < PF; ++j) {
+        const int y = y0 + j;
+        if (y < H) {
+          uint32_t wa[NT], wb[NT], we[NT];
+          widen_slice<NR>(ring[j], c);
+          widen_slice<NR>(ra[j], wa);
+          widen_slice<NR>(rb[j], wb);
+          widen_slice<NR>(re[j], we);
+          if (y + PF < H) {
+            const size_t o = (size_t)(y + PF) * rs;
+            ld_slice<NR>(cv + o, ring[j]);
+            ld_slice<NR>(btv + o, ra[j]);
+            ld_slice<NR>(lrv + o, rb[j]);
+            ld_slice<NR>(rlv + o, re[j]);
           }
-          const uint32_t k0 = group_min<G>(hmin16(acc0)), k1 = group_min<G>(hmin16(acc1));
-          __syncwarp();
-          uint32_t sm;
-          int ds;
-          if constexpr (D == 32) {
-            sm = k0 >> 6;
-            ds = (int)(k0 & 63);
-          } else if constexpr (D == 64) {
-            const uint32_t SA = k0 >> 6, SB2 = k1 >> 6;
-            sm = min(SA, SB2);
-            ds = (int)(min(k0, k1) & 63);  // lowest d among the minima
-            // A non-empty: odd rows take A; even rows take B = {t : S(t+32) == m, S(t) != m}
-            // when non-empty, which needs the minimum in both blocks (rare); computed by every
-            // lane of a warp where one column needs it (the shuffles must not diverge)
-            if (Q.tie_rule == kTieRefB200 && (y & 1) == 0 && __any_sync(kFull, SA == SB2)) {
-              const uint32_t mm = rep16(sm);
-              uint32_t ax = 0xFFFFFFFFu;
+          m = y == 0 ? first_g<NT, G>(L, c) : step_g<NT, G>(L, c, m, p1x2, p2m1, g);
+          if (y >= 5 && y <= H - 5 && y < Q.rows) {  // uniform over the warp
+            // S = the four u8 path costs summed (< 1024). Keys S << 6 | (d mod 64) per block of
+            // disparities: D = 32 one block; D = 64: d < 32 (A) and d >= 32 (B), the reference's two
+            // stores; D = 128: d < 64 and d >= 64.
+            constexpr int SPLIT = D == 32 ? 64 : (D == 64 ? 32 : 64);  // first d of the second block
+            uint32_t acc0 = 0xFFFFFFFFu, acc1 = 0xFFFFFFFFu;
+            if constexpr (G > 1) {
+              // every d of this lane lies in one block: one tree of SIMD minima
+              uint32_t key[NT];
+              const uint32_t dl = (uint32_t)((g * SB) & 63) * 0x10001u + 0x10000u;  // (d, d+1) mod 64 of word 0
 #pragma unroll
               for (int k = 0; k < NT; ++k) {
-                const int w = g * NT + k;  // word index; B words are 16..31
-                if (w >= 16) {
-                  const uint32_t z = colS[w - 16] - mm + 0x7FFF7FFFu;  // half >= 0x8000 iff S(t) != m
-                  const uint32_t eq = ~z & 0x80008000u;               // bit 15 of a half iff S(t) == m
-                  const uint32_t hx = myS[k] + (eq >> 5);              // excluded lanes get + 1024
-                  const uint32_t t0 = (uint32_t)(2 * (w - 16));
-                  ax = min16x2(ax, hx * 32u + (t0 | ((t0 + 1u) << 16)));
+                const uint32_t sk = (L[k] & 0x00FF00FFu) + wa[k] + wb[k] + we[k];
+                myS[k] = sk;
+                key[k] = sk * 64u + dl + (uint32_t)(2 * k) * 0x10001u;
+              }
+              uint32_t t = key[0];
+              if constexpr (NT > 1) {
+#pragma unroll
+                for (int st = 1; st < NT; st *= 3) {
+#pragma unroll
+                  for (int k = 0; k + st < NT; k += 3 * st)
+                    key[k] = k + 2 * st < NT ? __vimin3_u16x2(key[k], key[k + st], key[k + 2 * st])
+                                             : min16x2(key[k], key[k + st]);
+                }
+                t = key[0];
+              }
+              if (g * SB < SPLIT) acc0 = t;
+              else acc1 = t;
+            } else {
+#pragma unroll
+              for (int k = 0; k < NT; ++k) {
+                const uint32_t sk = (L[k] & 0x00FF00FFu) + wa[k] + wb[k] + we[k];
+                myS[k] = sk;
+                const uint32_t d0 = (uint32_t)(2 * (g * NT + k));
+                const uint32_t key = sk * 64u + ((d0 & 63u) | (((d0 + 1u) & 63u) << 16));
+                if ((int)d0 < SPLIT) acc0 = min16x2(acc0, key);
+                else acc1 = min16x2(acc1, key);
+              }
+            }
+            const uint32_t k0 = group_min<G>(hmin16(acc0)), k1 = group_min<G>(hmin16(acc1));
+            __syncwarp();
+            uint32_t sm;
+            int ds;
+            if constexpr (D == 32) {
+              sm = k0 >> 6;
+              ds = (int)(k0 & 63);
+            } else if constexpr (D == 64) {
+              const uint32_t SA = k0 >> 6, SB2 = k1 >> 6;
+              sm = min(SA, SB2);
+              ds = (int)(min(k0, k1) & 63);  // lowest d among the minima
+              // A non-empty: odd rows take A; even rows take B = {t : S(t+32) == m, S(t) != m}
+              // when non-empty, which needs the minimum in both blocks (rare); computed by every
+              // lane of a warp where one column needs it (the shuffles must not diverge)
+              if (Q.tie_rule == kTieRefB200 && (y & 1) == 0 && __any_sync(kFull, SA == SB2)) {
+                const uint32_t mm = rep16(sm);
+                uint32_t ax = 0xFFFFFFFFu;
+#pragma unroll
+                for (int k = 0; k < NT; ++k) {
+                  const int w = g * NT + k;  // word index; B words are 16..31
+                  if (w >= 16) {
+                    const uint32_t z = colS[w - 16] - mm + 0x7FFF7FFFu;  // half >= 0x8000 iff S(t) != m
+                    const uint32_t eq = ~z & 0x80008000u;               // bit 15 of a half iff S(t) == m
+                    const uint32_t hx = myS[k] + (eq >> 5);              // excluded lanes get + 1024
+                    const uint32_t t0 = (uint32_t)(2 * (w - 16));
+                    ax = min16x2(ax, hx * 32u + (t0 | ((t0 + 1u) << 16)));
+                  }
+                }
+                const uint32_t kx = group_min<G>(hmin16(ax));
+                if (SA == sm) {
+                  ds = (int)(k0 & 63);
+                  if ((y & 1) == 0 && (kx >> 5) == sm) ds = 32 + (int)(kx & 31);
                 }
               }
-              const uint32_t kx = group_min<G>(hmin16(ax));
-              if (SA == sm) {
-                ds = (int)(k0 & 63);
-                if ((y & 1) == 0 && (kx >> 5) == sm) ds = 32 + (int)(kx & 31);
-              }
-            }
-          } else {
-            const uint32_t s0 = k0 >> 6, s1 = k1 >> 6;
-            sm = min(s0, s1);
-            ds = s0 <= s1 ? (int)(k0 & 63) : 64 + (int)(k1 & 63);
-          }
-          float dv = kInvalidFloat;
-          if (col_ok && ds > 0 && ds < Q.dmax_excl) {
-            const uint32_t w1 = colS[(ds - 1) >> 1];
-            const float c1 = (float)(((ds - 1) & 1) ? (w1 >> 16) : (w1 & 0xFFFFu));
-            const float c2 = (float)sm;
-            float c3;
-            if (ds + 1 < D) {
-              const uint32_t w3 = colS[(ds + 1) >> 1];
-              c3 = (float)(((ds + 1) & 1) ? (w3 >> 16) : (w3 & 0xFFFFu));
             } else {
-              c3 = (float)ds;
+              const uint32_t s0 = k0 >> 6, s1 = k1 >> 6;
+              sm = min(s0, s1);
+              ds = s0 <= s1 ? (int)(k0 & 63) : 64 + (int)(k1 & 63);
             }
-            const float d12 = __fsub_rn(c1, c2), d32 = __fsub_rn(c3, c2);
-            const float uq = d12 < d32 ? d12 : d32;
-            if (!(uq <= __fmul_rn(c2, __fsub_rn(1.0f, Q.uniqueness))))
-              dv = __fadd_rn((float)(ds + P.min_d), subpix_bias(c1, c2, c3));
+            float dv = kInvalidFloat;
+            if (col_ok && ds > 0 && ds < Q.dmax_excl) {
+              const uint32_t w1 = colS[(ds - 1) >> 1];
+              const float c1 = (float)(((ds - 1) & 1) ? (w1 >> 16) : (w1 & 0xFFFFu));
+              const float c2 = (float)sm;
+              float c3;
+              if (ds + 1 < D) {
+                const uint32_t w3 = colS[(ds + 1) >> 1];
+                c3 = (float)(((ds + 1) & 1) ? (w3 >> 16) : (w3 & 0xFFFFu));
+              } else {
+                c3 = (float)ds;
+              }
+              const float d12 = __fsub_rn(c1, c2), d32 = __fsub_rn(c3, c2);
+              const float uq = d12 < d32 ? d12 : d32;
+              if (!(uq <= __fmul_rn(c2, __fsub_rn(1.0f, Q.uniqueness))))
+                dv = __fadd_rn((float)(ds + P.min_d), subpix_bias(c1, c2, c3));
+            }
+            __syncwarp();
+            if (valid && g == 0) dout[(size_t)y * W] = dv;
+          } else if (valid && g == 0) {
+            dout[(size_t)y * W] = kInvalidFloat;
           }
-          __syncwarp();
-          if (valid && g == 0) dout[(size_t)y * W] = dv;
-        } else if (valid && g == 0) {
-          dout[(size_t)y * W] = kInvalidFloat;
         }
       }
     }
   }
 }
 
-template <int K, int G, int PF>
 // five CTAs per SM (at most 96 registers) where a lane holds at most 32 disparities and G >= 2:
 // many concurrent pairs are occupancy-bound (plain 1242x375x64: +5 % pairs/s over the
 // unconstrained 113-128 registers); wider slices would spill
-__global__ void __launch_bounds__(128, (G >= 2 && 32 * K / G <= 32) ? 5 : 1) k_vpaths3(const uint8_t* __restrict__ cost, const uint8_t* __restrict__ lr,
+template <int K, int G, int PF, int PASS = 0>
+__global__ void __launch_bounds__(128, (G >= 2 && 32 * K / G <= 32) ? 5 : 1)
+    k_vpaths3(const uint8_t* __restrict__ cost, const uint8_t* __restrict__ lr,
                                                  const uint8_t* __restrict__ rl, uint8_t* __restrict__ bt,
                                                  float* __restrict__ disp, PlainParams P, WtaParams Q) {
   extern __shared__ uint32_t s_sum[];
-  vpaths3_lane<K, G, PF>(cost, lr, rl, bt, disp, P, Q, blockIdx.y, (blockIdx.x * blockDim.x + threadIdx.x) / G,
+  vpaths3_lane<K, G, PF, PASS>(cost, lr, rl, bt, disp, P, Q, blockIdx.y, (blockIdx.x * blockDim.x + threadIdx.x) / G,
                          threadIdx.x % G, s_sum + (threadIdx.x / G) * (16 * K + 1));
 }
 
@@ -1025,7 +1033,8 @@ __global__ void __launch_bounds__(128) k_hpaths3_init(const uint8_t* __restrict_
 // Kernel_ComputeDisparityByWTA for initial disparities): d in [2, 30]; tie rule kTieRefB200 =
 // the lowest tied d whose uniqueness test passes (every tied lane writes its own result, a valid
 // one wins), kTieLowest = the lowest tied d, then tested.
-template <int G, int PF>
+// PASS as in vpaths3_lane.
+template <int G, int PF, int PASS = 0>
 __device__ __forceinline__ void vpaths3_init_lane(const uint8_t* __restrict__ cost, const uint8_t* __restrict__ lr,
                                                   const uint8_t* __restrict__ rl, const int16_t* __restrict__ init_l,
                                                   const int16_t* __restrict__ init_r, uint8_t* __restrict__ bt,
@@ -1049,153 +1058,157 @@ __device__ __forceinline__ void vpaths3_init_lane(const uint8_t* __restrict__ co
   uint32_t m = 0;
   const int base0 = ib[0];
   int last_base = base0;
-  // bottom -> top: 16-bit steps with a prefetch ring up to s_wide, then 32-bit steps
-  int s_wide = narrow_ok ? H : 0;
-  static_assert(PF <= kNarrowBlock, "the 16-bit bound holds for kNarrowBlock steps");
-  if (s_wide > 0) {
-    uint32_t ring[PF][NR];
-    int rbase[PF];
-#pragma unroll
-    for (int j = 0; j < PF; ++j) {
-      if (j < H) {
-        ld_slice<NR>(cv + (size_t)(H - 1 - j) * rs, ring[j]);
-        rbase[j] = ib[(size_t)(H - 1 - j) * W];
-      }
-    }
-    for (int s0 = 0; s0 < s_wide; s0 += PF) {
+  if constexpr (PASS != 2) {  // bottom-to-top pass (stores its path costs)
+    // bottom -> top: 16-bit steps with a prefetch ring up to s_wide, then 32-bit steps
+    int s_wide = narrow_ok ? H : 0;
+    static_assert(PF <= kNarrowBlock, "the 16-bit bound holds for kNarrowBlock steps");
+    if (s_wide > 0) {
+      uint32_t ring[PF][NR];
+      int rbase[PF];
 #pragma unroll
       for (int j = 0; j < PF; ++j) {
-        const int s = s0 + j;
-        if (s < s_wide) {
-          const int y = H - 1 - s;
-          uint32_t r[NR];
-#pragma unroll
-          for (int k = 0; k < NR; ++k) r[k] = ring[j][k];
-          const int base = rbase[j];
-          if (s + PF < H) {
-            ld_slice<NR>(cv + (size_t)(y - PF) * rs, ring[j]);
-            rbase[j] = ib[(size_t)(y - PF) * W];
-          }
-          if (s == 0) m = init_first<ND, G>(L, r, false);
-          else init_advance16<ND, G>(L, r, m, last_base, base, P, p2tab, row, g);
-          if ((s == 0 || base != kInvalidShort) && computed) {
-#pragma unroll
-            for (int i = 0; i < NR; ++i) out[i] = narrow(L[2 * i], L[2 * i + 1]);
-            st_slice<NR>(btv + (size_t)y * rs, out);
-          }
+        if (j < H) {
+          ld_slice<NR>(cv + (size_t)(H - 1 - j) * rs, ring[j]);
+          rbase[j] = ib[(size_t)(H - 1 - j) * W];
         }
       }
-      if (__any_sync(kFull, !narrow_m_ok(m))) s_wide = min(H, s0 + PF);
-    }
-  }
-  if (s_wide < H) {
-    init_go_wide<ND, G>(L, s_wide, P, row, g);
-    for (int s = s_wide; s < H; ++s) {
-      const int y = H - 1 - s;
-      uint32_t r[NR];
-      ld_slice<NR>(cv + (size_t)y * rs, r);
-      const int base = ib[(size_t)y * W];
-      if (s == 0) m = init_first<ND, G>(L, r, true);
-      else init_advance32<ND, G>(L, r, m, last_base, base, P, p2tab, row, g);
-      if ((s == 0 || base != kInvalidShort) && computed) {
-        pack_bytes<ND>(L, out);
-        st_slice<NR>(btv + (size_t)y * rs, out);
-      }
-    }
-    init_go_narrow<G>(P, row, g);
-  }
-  // top -> bottom + sum + WTA (a new scanline)
-  const uint8_t* lrv = lr + vo;
-  const uint8_t* rlv = rl + vo;
-  last_base = base0;
-  int y_wide = narrow_ok ? H : 0;
-  if (y_wide > 0) {
-    uint32_t ring[PF][NR], ra[PF][NR], rb[PF][NR], re[PF][NR];
-    int rbase[PF];
+      for (int s0 = 0; s0 < s_wide; s0 += PF) {
 #pragma unroll
-    for (int j = 0; j < PF; ++j) {
-      if (j < H) {
-        const size_t o = (size_t)j * rs;
-        ld_slice<NR>(cv + o, ring[j]);
-        ld_slice<NR>(btv + o, ra[j]);
-        ld_slice<NR>(lrv + o, rb[j]);
-        ld_slice<NR>(rlv + o, re[j]);
-        rbase[j] = ib[(size_t)j * W];
+        for (int j = 0; j < PF; ++j) {
+          const int s = s0 + j;
+          if (s < s_wide) {
+            const int y = H - 1 - s;
+            uint32_t r[NR];
+#pragma unroll
+            for (int k = 0; k < NR; ++k) r[k] = ring[j][k];
+            const int base = rbase[j];
+            if (s + PF < H) {
+              ld_slice<NR>(cv + (size_t)(y - PF) * rs, ring[j]);
+              rbase[j] = ib[(size_t)(y - PF) * W];
+            }
+            if (s == 0) m = init_first<ND, G>(L, r, false);
+            else init_advance16<ND, G>(L, r, m, last_base, base, P, p2tab, row, g);
+            if ((s == 0 || base != kInvalidShort) && computed) {
+#pragma unroll
+              for (int i = 0; i < NR; ++i) out[i] = narrow(L[2 * i], L[2 * i + 1]);
+              st_slice<NR>(btv + (size_t)y * rs, out);
+            }
+          }
+        }
+        if (__any_sync(kFull, !narrow_m_ok(m))) s_wide = min(H, s0 + PF);
       }
     }
-    for (int y0 = 0; y0 < y_wide; y0 += PF) {
+    if (s_wide < H) {
+      init_go_wide<ND, G>(L, s_wide, P, row, g);
+      for (int s = s_wide; s < H; ++s) {
+        const int y = H - 1 - s;
+        uint32_t r[NR];
+        ld_slice<NR>(cv + (size_t)y * rs, r);
+        const int base = ib[(size_t)y * W];
+        if (s == 0) m = init_first<ND, G>(L, r, true);
+        else init_advance32<ND, G>(L, r, m, last_base, base, P, p2tab, row, g);
+        if ((s == 0 || base != kInvalidShort) && computed) {
+          pack_bytes<ND>(L, out);
+          st_slice<NR>(btv + (size_t)y * rs, out);
+        }
+      }
+      init_go_narrow<G>(P, row, g);
+    }
+  }
+  if constexpr (PASS != 1) {  // top-to-bottom pass with the 4-path sum and the WTA
+    // top -> bottom + sum + WTA (a new scanline)
+    const uint8_t* lrv = lr + vo;
+    const uint8_t* rlv = rl + vo;
+    last_base = base0;
+    int y_wide = narrow_ok ? H : 0;
+    if (y_wide > 0) {
+      uint32_t ring[PF][NR], ra[PF][NR], rb[PF][NR], re[PF][NR];
+      int rbase[PF];
 #pragma unroll
       for (int j = 0; j < PF; ++j) {
-        const int y = y0 + j;
-        if (y < y_wide) {
-          uint32_t r[NR], S2[NW];
+        if (j < H) {
+          const size_t o = (size_t)j * rs;
+          ld_slice<NR>(cv + o, ring[j]);
+          ld_slice<NR>(btv + o, ra[j]);
+          ld_slice<NR>(lrv + o, rb[j]);
+          ld_slice<NR>(rlv + o, re[j]);
+          rbase[j] = ib[(size_t)j * W];
+        }
+      }
+      for (int y0 = 0; y0 < y_wide; y0 += PF) {
+#pragma unroll
+        for (int j = 0; j < PF; ++j) {
+          const int y = y0 + j;
+          if (y < y_wide) {
+            uint32_t r[NR], S2[NW];
+#pragma unroll
+            for (int k = 0; k < NR; ++k) {
+              r[k] = ring[j][k];
+              // sums of the three stored paths, two disparities per word (each half <= 765)
+              S2[2 * k] = widen_lo(ra[j][k]) + widen_lo(rb[j][k]) + widen_lo(re[j][k]);
+              S2[2 * k + 1] = widen_hi(ra[j][k]) + widen_hi(rb[j][k]) + widen_hi(re[j][k]);
+            }
+            const int base = rbase[j];
+            if (y + PF < H) {
+              const size_t o = (size_t)(y + PF) * rs;
+              ld_slice<NR>(cv + o, ring[j]);
+              ld_slice<NR>(btv + o, ra[j]);
+              ld_slice<NR>(lrv + o, rb[j]);
+              ld_slice<NR>(rlv + o, re[j]);
+              rbase[j] = ib[(size_t)(y + PF) * W];
+            }
+            if (y == 0) m = init_first<ND, G>(L, r, false);
+            else init_advance16<ND, G>(L, r, m, last_base, base, P, p2tab, row, g);
+            const bool skipped = y > 0 && base == kInvalidShort;
+            if (y >= 5 && y <= H - 5 && y < Q.rows) {  // uniform over the warp
+#pragma unroll
+              for (int k = 0; k < NW; ++k) S2[k] += L[k] & 0x00FF00FFu;  // + this path (<= 1020 per half)
+              init_wta_pixel<ND, G>(S2, colS, g, base, col_ok && base != kInvalidShort && !skipped, Q, valid,
+                                    dout + (size_t)y * W);
+            } else if (valid && g == 0) {
+              dout[(size_t)y * W] = kInvalidFloat;
+            }
+          }
+        }
+        if (__any_sync(kFull, !narrow_m_ok(m))) y_wide = min(H, y0 + PF);
+      }
+    }
+    if (y_wide < H) {
+      init_go_wide<ND, G>(L, y_wide, P, row, g);
+      for (int y = y_wide; y < H; ++y) {
+        const size_t o = (size_t)y * rs;
+        uint32_t r[NR], S2[NW];
+        ld_slice<NR>(cv + o, r);
+        {
+          uint32_t qa[NR], qb[NR], qe[NR];
+          ld_slice<NR>(btv + o, qa);
+          ld_slice<NR>(lrv + o, qb);
+          ld_slice<NR>(rlv + o, qe);
 #pragma unroll
           for (int k = 0; k < NR; ++k) {
-            r[k] = ring[j][k];
-            // sums of the three stored paths, two disparities per word (each half <= 765)
-            S2[2 * k] = widen_lo(ra[j][k]) + widen_lo(rb[j][k]) + widen_lo(re[j][k]);
-            S2[2 * k + 1] = widen_hi(ra[j][k]) + widen_hi(rb[j][k]) + widen_hi(re[j][k]);
-          }
-          const int base = rbase[j];
-          if (y + PF < H) {
-            const size_t o = (size_t)(y + PF) * rs;
-            ld_slice<NR>(cv + o, ring[j]);
-            ld_slice<NR>(btv + o, ra[j]);
-            ld_slice<NR>(lrv + o, rb[j]);
-            ld_slice<NR>(rlv + o, re[j]);
-            rbase[j] = ib[(size_t)(y + PF) * W];
-          }
-          if (y == 0) m = init_first<ND, G>(L, r, false);
-          else init_advance16<ND, G>(L, r, m, last_base, base, P, p2tab, row, g);
-          const bool skipped = y > 0 && base == kInvalidShort;
-          if (y >= 5 && y <= H - 5 && y < Q.rows) {  // uniform over the warp
-#pragma unroll
-            for (int k = 0; k < NW; ++k) S2[k] += L[k] & 0x00FF00FFu;  // + this path (<= 1020 per half)
-            init_wta_pixel<ND, G>(S2, colS, g, base, col_ok && base != kInvalidShort && !skipped, Q, valid,
-                                  dout + (size_t)y * W);
-          } else if (valid && g == 0) {
-            dout[(size_t)y * W] = kInvalidFloat;
+            S2[2 * k] = widen_lo(qa[k]) + widen_lo(qb[k]) + widen_lo(qe[k]);
+            S2[2 * k + 1] = widen_hi(qa[k]) + widen_hi(qb[k]) + widen_hi(qe[k]);
           }
         }
-      }
-      if (__any_sync(kFull, !narrow_m_ok(m))) y_wide = min(H, y0 + PF);
-    }
-  }
-  if (y_wide < H) {
-    init_go_wide<ND, G>(L, y_wide, P, row, g);
-    for (int y = y_wide; y < H; ++y) {
-      const size_t o = (size_t)y * rs;
-      uint32_t r[NR], S2[NW];
-      ld_slice<NR>(cv + o, r);
-      {
-        uint32_t qa[NR], qb[NR], qe[NR];
-        ld_slice<NR>(btv + o, qa);
-        ld_slice<NR>(lrv + o, qb);
-        ld_slice<NR>(rlv + o, qe);
+        const int base = ib[(size_t)y * W];
+        if (y == 0) m = init_first<ND, G>(L, r, true);
+        else init_advance32<ND, G>(L, r, m, last_base, base, P, p2tab, row, g);
+        const bool skipped = y > 0 && base == kInvalidShort;
+        if (y >= 5 && y <= H - 5 && y < Q.rows) {
 #pragma unroll
-        for (int k = 0; k < NR; ++k) {
-          S2[2 * k] = widen_lo(qa[k]) + widen_lo(qb[k]) + widen_lo(qe[k]);
-          S2[2 * k + 1] = widen_hi(qa[k]) + widen_hi(qb[k]) + widen_hi(qe[k]);
+          for (int k = 0; k < NW; ++k) S2[k] += (L[2 * k] & 0xFFu) | ((L[2 * k + 1] & 0xFFu) << 16);
+          init_wta_pixel<ND, G>(S2, colS, g, base, col_ok && base != kInvalidShort && !skipped, Q, valid,
+                                dout + (size_t)y * W);
+        } else if (valid && g == 0) {
+          dout[(size_t)y * W] = kInvalidFloat;
         }
       }
-      const int base = ib[(size_t)y * W];
-      if (y == 0) m = init_first<ND, G>(L, r, true);
-      else init_advance32<ND, G>(L, r, m, last_base, base, P, p2tab, row, g);
-      const bool skipped = y > 0 && base == kInvalidShort;
-      if (y >= 5 && y <= H - 5 && y < Q.rows) {
-#pragma unroll
-        for (int k = 0; k < NW; ++k) S2[k] += (L[2 * k] & 0xFFu) | ((L[2 * k + 1] & 0xFFu) << 16);
-        init_wta_pixel<ND, G>(S2, colS, g, base, col_ok && base != kInvalidShort && !skipped, Q, valid,
-                              dout + (size_t)y * W);
-      } else if (valid && g == 0) {
-        dout[(size_t)y * W] = kInvalidFloat;
-      }
+      init_go_narrow<G>(P, row, g);
     }
-    init_go_narrow<G>(P, row, g);
   }
 }
 
-template <int G, int PF>
+template <int G, int PF, int PASS = 0>
 __global__ void __launch_bounds__(128) k_vpaths3_init(const uint8_t* __restrict__ cost,
                                                       const uint8_t* __restrict__ lr, const uint8_t* __restrict__ rl,
                                                       const int16_t* __restrict__ init_l,
@@ -1209,7 +1222,7 @@ __global__ void __launch_bounds__(128) k_vpaths3_init(const uint8_t* __restrict_
   init_row_pad<G>(row, P.p1, true, threadIdx.x % G);
   __syncthreads();
   const int xc = (blockIdx.x * blockDim.x + threadIdx.x) / G;
-  vpaths3_init_lane<G, PF>(cost, lr, rl, init_l, init_r, bt, disp, P, Q, blockIdx.y, xc, threadIdx.x % G, row,
+  vpaths3_init_lane<G, PF, PASS>(cost, lr, rl, init_l, init_r, bt, disp, P, Q, blockIdx.y, xc, threadIdx.x % G, row,
                            sums + threadIdx.x / G, p2tab);
 }
 
