@@ -736,6 +736,7 @@ struct sgm_batch_pyr {
   int dev = 0, nsm = 148, layers = 1, word = 8;
   cudaStream_t stream = nullptr;
   std::vector<cudaStream_t> side;
+  std::vector<cudaStream_t> side2;  // the bottom-to-top column pass of each 32-disparity bucket
   std::vector<cudaEvent_t> ev;
   std::vector<sgm_batch_pair_t> pairs;
   sgm_ext_options_t ext{};
@@ -775,6 +776,8 @@ struct sgm_batch_pyr {
     queues = nullptr;
     for (auto s : side) cudaStreamDestroy(s);
     side.clear();
+    for (auto s : side2) cudaStreamDestroy(s);
+    side2.clear();
     for (auto e : ev) cudaEventDestroy(e);
     ev.clear();
     if (stream) cudaStreamDestroy(stream);
@@ -831,6 +834,9 @@ int init_rows(sgm_batch_pyr* p, PLevel& L, PBucket& k, cudaStream_t s, int* queu
   return G == 2 ? go(kb_rows3_init<2, 8>) : G == 4 ? go(kb_rows3_init<4, 8>) : go(kb_rows3_init<8, 8>);
 }
 
+// PASS: 0 both column passes, 1 bottom-to-top only, 2 top-to-bottom + WTA only (the persistent
+// grid is sized for PASS 0; the queue counts any grid).
+template <int PASS = 0>
 int init_cols(sgm_batch_pyr* p, PLevel& L, PBucket& k, cudaStream_t s, int* queue, bool prepare) {
   const int G = k.cols_lanes, li = lanes_index(G), n = (int)k.members.size();
   const int* ids = p->dtab + k.ids;
@@ -841,7 +847,10 @@ int init_cols(sgm_batch_pyr* p, PLevel& L, PBucket& k, cudaStream_t s, int* queu
     PTRY(p, cudaGetLastError());
     return SGM_OK;
   };
-  return G == 2 ? go(kb_cols3_init<2, 1>) : G == 4 ? go(kb_cols3_init<4, 4>) : go(kb_cols3_init<8, 4>);
+  if (prepare) return G == 2 ? go(kb_cols3_init<2, 1>) : G == 4 ? go(kb_cols3_init<4, 4>) : go(kb_cols3_init<8, 4>);
+  return G == 2   ? go(kb_cols3_init<2, 1, PASS>)
+         : G == 4 ? go(kb_cols3_init<4, 4, PASS>)
+                  : go(kb_cols3_init<8, 4, PASS>);
 }
 
 int init_cost(sgm_batch_pyr* p, PLevel& L, PBucket& k, cudaStream_t s) {
@@ -911,7 +920,7 @@ int pyr_autotune(sgm_batch_pyr* p) {
     if (st0) return st0;
     for (size_t bi = 0; bi < L.buckets.size(); ++bi) {
       auto& k = L.buckets[bi];
-      int* q = p->queues + L.queue0 + 2 * bi;
+      int* q = p->queues + L.queue0 + 3 * bi;
       int st = init_cost(p, L, k, p->stream);
       if (st) return st;
       float best = 1e30f;
@@ -1033,11 +1042,18 @@ int pyr_capture(sgm_batch_pyr* p) {
     if (!st) { st = level_census(p, L.ddesc, L.census_prefix, L.census_items, n, s); kernels++; }
     if (!st)
       fork_join((int)L.buckets.size(), [&](int i, cudaStream_t t) {
-        int* q = p->queues + L.queue0 + 2 * i;
+        // the bottom-to-top pass (cost volume only) on side2 beside the row scans
+        int* q = p->queues + L.queue0 + 3 * i;
         int r = init_cost(p, L, L.buckets[i], t);
+        cudaStream_t t2 = p->side2[i];
+        cudaEventRecord(p->ev[evi], t);
+        cudaStreamWaitEvent(t2, p->ev[evi++], 0);
+        if (!r) r = init_cols<1>(p, L, L.buckets[i], t2, q + 1, false);
         if (!r) r = init_rows(p, L, L.buckets[i], t, q, false);
-        if (!r) r = init_cols(p, L, L.buckets[i], t, q + 1, false);
-        kernels += 3;
+        cudaEventRecord(p->ev[evi], t2);
+        cudaStreamWaitEvent(t, p->ev[evi++], 0);
+        if (!r) r = init_cols<2>(p, L, L.buckets[i], t, q + 2, false);
+        kernels += 4;
         return r;
       });
     if (!st) { st = level_post(p, L.ddesc, p->dtab + L.tile_prefix, L.tile_items, n, L.opt, s); kernels++; }
@@ -1295,7 +1311,7 @@ int sgm_batch_pyr_init(sgm_batch_pyr_t p, const sgm_batch_pair_t* pairs, int32_t
       L.buckets.push_back(k);
     }
     L.queue0 = nq;
-    nq += 2 * (int)L.buckets.size();
+    nq += 3 * (int)L.buckets.size();  // rows, bottom-to-top, top-to-bottom + WTA
   }
   PTRY(p, cudaMalloc(&p->dtab, tab.size() * sizeof(int)));
   PTRY(p, cudaMemcpy(p->dtab, tab.data(), tab.size() * sizeof(int), cudaMemcpyHostToDevice));
@@ -1305,12 +1321,14 @@ int sgm_batch_pyr_init(sgm_batch_pyr_t p, const sgm_batch_pair_t* pairs, int32_t
   int nev = 1 + (int)p->coarse->buckets.size();
   for (auto& L : p->lv) {
     nside = std::max(nside, L.buckets.size());
-    nev += 1 + (int)L.buckets.size();
+    nev += 1 + 3 * (int)L.buckets.size();
   }
   for (size_t i = 0; i < nside; ++i) {
     cudaStream_t t;
     PTRY(p, cudaStreamCreateWithFlags(&t, cudaStreamNonBlocking));
     p->side.push_back(t);
+    PTRY(p, cudaStreamCreateWithFlags(&t, cudaStreamNonBlocking));
+    p->side2.push_back(t);
   }
   for (int i = 0; i < nev; ++i) {
     cudaEvent_t e;

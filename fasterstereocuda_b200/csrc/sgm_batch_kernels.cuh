@@ -349,7 +349,7 @@ __global__ void __launch_bounds__(128) kb_rows3_init(const BatchPair* __restrict
   }
 }
 
-template <int G, int PF>
+template <int G, int PF, int PASS = 0>
 __global__ void __launch_bounds__(128) kb_cols3_init(const BatchPair* __restrict__ pairs, const int* __restrict__ ids,
                                                      const int* __restrict__ prefix, int n, int* __restrict__ queue) {
   constexpr int S = 32 / G;
@@ -372,8 +372,8 @@ __global__ void __launch_bounds__(128) kb_cols3_init(const BatchPair* __restrict
     const int per_view = (d.P.W + S - 1) / S;
     const int view = local / per_view;
     const int grp = local - view * per_view;
-    sgm::vpaths3_init_lane<G, PF>(d.cost, d.lr, d.rl, d.init, d.init, d.bt, d.wta, d.IP, d.Q, view, grp * S + lane / G,
-                                  lane % G, row, colS, p2tab);
+    sgm::vpaths3_init_lane<G, PF, PASS>(d.cost, d.lr, d.rl, d.init, d.init, d.bt, d.wta, d.IP, d.Q, view,
+                                        grp * S + lane / G, lane % G, row, colS, p2tab);
     __syncwarp();
   }
 }

@@ -531,7 +531,9 @@ inline int init3_rows(sgm_engine* e, const int16_t* il, const int16_t* ir, const
   auto go = [&](auto kern) {
     return SGM_LAUNCH(e, s, "hpaths_init", kern<<<blocks, 128, 0, s>>>(e->cost, il, ir, e->lr, e->rl, P, nv));
   };
-  return G == 2 ? go(sgm::k_hpaths3_init<2, 8>) : G == 8 ? go(sgm::k_hpaths3_init<8, 8>) : go(sgm::k_hpaths3_init<4, 8>);
+  return G == 2   ? go(sgm::k_hpaths3_init<2, 8>)
+         : G == 8 ? go(sgm::k_hpaths3_init<8, 8>)
+                  : go(sgm::k_hpaths3_init<4, 8>);
 }
 
 // PASS as in launch_cols3_pass
