@@ -59,6 +59,7 @@ struct sgm_batch {
   bool ready = false;
   cudaStream_t stream = nullptr;
   std::vector<cudaStream_t> side;
+  std::vector<cudaStream_t> side2;  // the bottom-to-top column pass of each bucket
   std::vector<cudaEvent_t> ev;
   std::vector<sgm_batch_pair_t> pairs;
   sgm_option_t opt{};
@@ -107,6 +108,8 @@ struct sgm_batch {
     queues = nullptr;
     for (auto s : side) cudaStreamDestroy(s);
     side.clear();
+    for (auto s : side2) cudaStreamDestroy(s);
+    side2.clear();
     for (auto e : ev) cudaEventDestroy(e);
     ev.clear();
     if (stream) cudaStreamDestroy(stream);
@@ -216,7 +219,7 @@ int cols_warp_t(sgm_batch* b, sgm_batch::Bucket& k, cudaStream_t s, int* queue, 
   return SGM_OK;
 }
 
-template <int K>
+template <int K, int PASS = 0>
 int cols_t(sgm_batch* b, sgm_batch::Bucket& k, cudaStream_t s, int* queue, bool prepare) {
   const int G = k.tune.cols_lanes;
   if (G == 0) {
@@ -239,10 +242,12 @@ int cols_t(sgm_batch* b, sgm_batch::Bucket& k, cudaStream_t s, int* queue, bool 
   };
   int st;
   if constexpr (K == 4) {
-    st = G == 4 ? go(kb_cols3<K, 4, pf_cols<K, 4>()>) : go(kb_cols3<K, 2, pf_cols<K, 2>()>);
+    st = G == 4 ? go(kb_cols3<K, 4, pf_cols<K, 4>(), PASS>) : go(kb_cols3<K, 2, pf_cols<K, 2>(), PASS>);
   } else {
-    st = G == 1 ? go(kb_cols3<K, 1, pf_cols<K, 1>()>) : G == 2 ? go(kb_cols3<K, 2, pf_cols<K, 2>()>)
-       : G == 4 ? go(kb_cols3<K, 4, pf_cols<K, 4>()>) : go(kb_cols3<K, 8, pf_cols<K, 8>()>);
+    st = G == 1   ? go(kb_cols3<K, 1, pf_cols<K, 1>(), PASS>)
+         : G == 2 ? go(kb_cols3<K, 2, pf_cols<K, 2>(), PASS>)
+         : G == 4 ? go(kb_cols3<K, 4, pf_cols<K, 4>(), PASS>)
+                  : go(kb_cols3<K, 8, pf_cols<K, 8>(), PASS>);
   }
   if (st || prepare) return st;
   BTRY(b, cudaGetLastError());
@@ -258,11 +263,14 @@ int rows(sgm_batch* b, sgm_batch::Bucket& k, cudaStream_t s, int* queue, bool pr
   }
 }
 
+// PASS: 0 both column passes, 1 bottom-to-top only, 2 top-to-bottom + WTA only (thread-per-
+// scanline column bodies; the persistent grid is sized for PASS 0, the queue counts any grid)
+template <int PASS = 0>
 int cols(sgm_batch* b, sgm_batch::Bucket& k, cudaStream_t s, int* queue, bool prepare) {
   switch (k.K) {
-    case 1: return cols_t<1>(b, k, s, queue, prepare);
-    case 2: return cols_t<2>(b, k, s, queue, prepare);
-    default: return cols_t<4>(b, k, s, queue, prepare);
+    case 1: return cols_t<1, PASS>(b, k, s, queue, prepare);
+    case 2: return cols_t<2, PASS>(b, k, s, queue, prepare);
+    default: return cols_t<4, PASS>(b, k, s, queue, prepare);
   }
 }
 
@@ -292,6 +300,30 @@ int launch_rows(sgm_batch* b, sgm_batch::Bucket& k, cudaStream_t s, int* queue) 
 int launch_cols(sgm_batch* b, sgm_batch::Bucket& k, cudaStream_t s, int* queue) {
   return cols(b, k, s, queue, false);
 }
+// Row and column scans of one bucket on t. When both run the thread-per-scanline bodies (the
+// cost volume exists before the rows), the bottom-to-top column pass runs on t2 beside the row
+// scans and the top-to-bottom pass follows the join. Queues q, q + 1, q + 2.
+int bucket_scans(sgm_batch* b, sgm_batch::Bucket& k, cudaStream_t t, cudaStream_t t2, cudaEvent_t ea,
+                 cudaEvent_t eb, int* q, int64_t* kernels) {
+  if (k.tune.cols_lanes == 0 || k.tune.rows_lanes == 0) {
+    int r = launch_rows(b, k, t, q);
+    if (!r) r = launch_cols(b, k, t, q + 1);
+    *kernels += k.tune.rows_lanes ? 3 : 2;
+    return r;
+  }
+  int r = launch_cost(b, k, t);
+  cudaEventRecord(ea, t);
+  cudaStreamWaitEvent(t2, ea, 0);
+  if (!r) r = cols<1>(b, k, t2, q + 1, false);
+  if (!r) r = rows(b, k, t, q, false);
+  cudaEventRecord(eb, t2);
+  cudaStreamWaitEvent(t, eb, 0);
+  if (!r) r = cols<2>(b, k, t, q + 2, false);
+  if (!r && cudaGetLastError() != cudaSuccess) r = berr(b, SGM_ERR_CUDA, "column pass launch failed");
+  *kernels += 4;
+  return r;
+}
+
 int prepare_bucket(sgm_batch* b, sgm_batch::Bucket& k) {
   const int st = rows(b, k, nullptr, nullptr, true);
   return st ? st : cols(b, k, nullptr, nullptr, true);
@@ -366,7 +398,7 @@ int autotune(sgm_batch* b, bool force) {
         continue;
       }
     }
-    int* q = b->queues + 2 * i;
+    int* q = b->queues + 3 * i;
     auto reset = [&]() { return cudaMemsetAsync(q, 0, 2 * sizeof(int), b->stream) == cudaSuccess ? SGM_OK : SGM_ERR_CUDA; };
     // row scans: warp per scanline (4 or 8 warps per CTA), or G lanes per scanline (+ cost kernel)
     std::vector<std::pair<int, int>> rc = {{0, 4}, {0, 8}};
@@ -435,9 +467,8 @@ int capture(sgm_batch* b) {
   for (size_t i = 0; !st && i < b->buckets.size(); ++i) {
     cudaStream_t t = b->side[i];
     cudaStreamWaitEvent(t, b->ev[0], 0);
-    st = launch_rows(b, b->buckets[i], t, b->queues + 2 * i);
-    if (!st) st = launch_cols(b, b->buckets[i], t, b->queues + 2 * i + 1);
-    kernels += b->buckets[i].tune.rows_lanes ? 3 : 2;
+    const size_t e2 = 1 + b->buckets.size() + 2 * i;
+    st = bucket_scans(b, b->buckets[i], t, b->side2[i], b->ev[e2], b->ev[e2 + 1], b->queues + 3 * i, &kernels);
     cudaEventRecord(b->ev[1 + i], t);
     cudaStreamWaitEvent(s, b->ev[1 + i], 0);
   }
@@ -599,14 +630,16 @@ int sgm_batch_init(sgm_batch_t b, const sgm_batch_pair_t* pairs, int32_t count, 
   }
   BTRY(b, cudaMalloc(&b->dtab, tab.size() * sizeof(int)));
   BTRY(b, cudaMemcpy(b->dtab, tab.data(), tab.size() * sizeof(int), cudaMemcpyHostToDevice));
-  b->nqueues = 2 * (int)b->buckets.size();
+  b->nqueues = 3 * (int)b->buckets.size();
   BTRY(b, cudaMalloc(&b->queues, b->nqueues * sizeof(int)));
   for (size_t i = 0; i < b->buckets.size(); ++i) {
     cudaStream_t t;
     BTRY(b, cudaStreamCreateWithFlags(&t, cudaStreamNonBlocking));
     b->side.push_back(t);
+    BTRY(b, cudaStreamCreateWithFlags(&t, cudaStreamNonBlocking));
+    b->side2.push_back(t);
   }
-  for (size_t i = 0; i < b->buckets.size() + 1; ++i) {
+  for (size_t i = 0; i < 3 * b->buckets.size() + 1; ++i) {
     cudaEvent_t e;
     BTRY(b, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     b->ev.push_back(e);
@@ -1023,10 +1056,8 @@ int pyr_capture(sgm_batch_pyr* p) {
   if (!st) { st = launch_census(c, s); kernels++; }
   if (!st)
     fork_join((int)c->buckets.size(), [&](int i, cudaStream_t t) {
-      int r = launch_rows(c, c->buckets[i], t, c->queues + 2 * i);
-      if (!r) r = launch_cols(c, c->buckets[i], t, c->queues + 2 * i + 1);
-      kernels += c->buckets[i].tune.rows_lanes ? 3 : 2;
-      return r;
+      const int ea = evi++, eb = evi++;
+      return bucket_scans(c, c->buckets[i], t, p->side2[i], p->ev[ea], p->ev[eb], c->queues + 3 * i, &kernels);
     });
   if (!st) { st = launch_post(c, s); kernels++; }
   if (!st)
@@ -1318,7 +1349,7 @@ int sgm_batch_pyr_init(sgm_batch_pyr_t p, const sgm_batch_pair_t* pairs, int32_t
   p->nqueues = nq;
   if (nq) PTRY(p, cudaMalloc(&p->queues, nq * sizeof(int)));
   size_t nside = p->coarse->buckets.size();
-  int nev = 1 + (int)p->coarse->buckets.size();
+  int nev = 1 + 3 * (int)p->coarse->buckets.size();
   for (auto& L : p->lv) {
     nside = std::max(nside, L.buckets.size());
     nev += 1 + 3 * (int)L.buckets.size();

@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(256) kb_rows3(const BatchPair* __restrict__ pa
   }
 }
 
-template <int K, int G, int PF>
+template <int K, int G, int PF, int PASS = 0>
 __global__ void __launch_bounds__(256) kb_cols3(const BatchPair* __restrict__ pairs, const int* __restrict__ ids,
                                                 const int* __restrict__ prefix, int n, int* __restrict__ queue) {
   constexpr int S = 32 / G;
@@ -177,7 +177,8 @@ __global__ void __launch_bounds__(256) kb_cols3(const BatchPair* __restrict__ pa
     const int per_view = (d.P.W + S - 1) / S;
     const int view = local / per_view;
     const int grp = local - view * per_view;
-    sgm::vpaths3_lane<K, G, PF>(d.cost, d.lr, d.rl, d.bt, d.wta, d.P, d.Q, view, grp * S + lane / G, lane % G, colS);
+    sgm::vpaths3_lane<K, G, PF, PASS>(d.cost, d.lr, d.rl, d.bt, d.wta, d.P, d.Q, view, grp * S + lane / G, lane % G,
+                                      colS);
     __syncwarp();
   }
 }
