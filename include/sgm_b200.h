@@ -53,8 +53,8 @@ typedef struct sgm_option_s {
   bool using_constant_p2;
   bool do_remove_peaks;
   float peaks_ratio_threshold;
-  int32_t post_filter_type; /* 0 = none (only value supported) */
-  int32_t morphology_type;  /* 0 = none, 2 = dilation */
+  int32_t post_filter_type; /* 0 = none, 1 = Gauss, 2 = bilateral (cusgm_df.cu:94-195) */
+  int32_t morphology_type;  /* 0 = none, 1 = erosion, 2 = dilation, 3 = open, 4 = close */
 } sgm_option_t;
 
 /* Same layout as StereoROI_T (SgmStereoCuda/sgm_types.h:89-92). */
