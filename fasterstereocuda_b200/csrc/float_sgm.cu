@@ -5,16 +5,25 @@
 // The recurrence is the reference's path recurrence (cusgm_ca.cu:1517-1564) in float with the
 // penalties read at the current pixel and +inf beyond d = 0 and d = D-1:
 //   L_p(d) = C_p(d) + min(L_q(d), L_q(d-1)+P1(p), L_q(d+1)+P1(p), m_q+P2(p)) - m_q,  m_q = min_k L_q(k)
-//   S(p,d) = sum over the four paths;  disp(p) = sum_d d * softmax_d(-S(p,d)/T)
+//   S(p,d) = ((L_0 + L_1) + L_2) + L_3;  disp(p) = sum_d d * softmax_d(-S(p,d)/T)
 // Ties of the hard minima are broken in the fixed order same d, d-1, d+1, jump (lowest k for m_q).
+//
+// Mapping: a scanline is held by G = D/8 lanes of a warp, 8 disparities per lane, so a warp scans
+// 32/G lines at once and the per-pixel minimum is a 3-level (D=64) or 2-level (D=32) butterfly.
+// All four directions run in ONE launch (their blocks side by side, the long row scans first),
+// each writing its own path volume; the soft-argmin kernel adds the four in path order. The
+// backward launch likewise runs the four adjoint scans at once, each writing its own gradient
+// volume and penalty-map gradients, and a last kernel adds them in path order.
 //
 // Backward: per path, scanlines are walked backwards segment by segment; each segment of
 // kSeg pixels is recomputed from the state stored when the forward pass entered it, so no
-// D-deep path volume is kept (only one state per kSeg pixels). The adjoint routes the gradient
-// of every L_p(d) to C_p(d), to P1(p) or P2(p) through the recorded minimum, and to L_q.
+// D-deep path volume is kept for the backward (only one state per kSeg pixels). The adjoint
+// routes the gradient of every L_p(d) to C_p(d), to P1(p) or P2(p) through the recorded minimum,
+// and to L_q.
 //
-// Layouts: cost/sum/grad volumes float [B][H][W][D]; maps float [B][H][W]; checkpoints float
-// [4 paths][lines][segments][D]. Paths: 0 top->bottom, 1 left->right, 2 bottom->top, 3 right->left.
+// Layouts: cost/sum/grad volumes float [B][H][W][D] (16-byte aligned); maps float [B][H][W];
+// checkpoints float [4 paths][lines][segments][D]. Paths: 0 top->bottom, 1 left->right,
+// 2 bottom->top, 3 right->left.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -27,7 +36,10 @@ void sgm_set_process_error(const char* msg);
 namespace {
 
 constexpr unsigned kFullMask = 0xFFFFFFFFu;
-constexpr int kSeg = 16;
+constexpr int kK = 8;       // disparities per lane
+constexpr int kSeg = 16;    // pixels per recomputed segment
+constexpr int kPF = 4;      // depth of the register ring of per-pixel inputs
+constexpr int kWarps = 4;   // warps per block of the scan kernels
 #define kInf __int_as_float(0x7f800000)
 
 struct Geo {
@@ -46,199 +58,321 @@ __host__ __device__ inline Geo make_geo(int B, int H, int W, int D, int dir) {
   return g;
 }
 
-// pixel index (b*H + y)*W + x of scan position s on line `line`
-__device__ __forceinline__ size_t pix(const Geo& g, int line, int s) {
-  const bool fwd = g.dir == 0 || g.dir == 1;
-  const int k = fwd ? s : g.len - 1 - s;
-  if (g.dir == 1 || g.dir == 3) return (size_t)line * g.W + k;  // line = b*H + y
-  const int b = line / g.W, x = line - b * g.W;
-  return ((size_t)b * g.H + k) * g.W + x;
+// pixel index (b*H + y)*W + x of scan position 0 of `line`, and the pixel stride of one step
+__device__ __forceinline__ void line_origin(const Geo& g, int line, long long& base, long long& step) {
+  if (g.dir == 1 || g.dir == 3) {  // line = b*H + y
+    base = (long long)line * g.W + (g.dir == 3 ? g.W - 1 : 0);
+    step = g.dir == 3 ? -1 : 1;
+  } else {  // line = b*W + x
+    const int b = line / g.W, x = line - b * g.W;
+    base = ((long long)b * g.H + (g.dir == 2 ? g.H - 1 : 0)) * g.W + x;
+    step = g.dir == 2 ? -(long long)g.W : (long long)g.W;
+  }
 }
 
-__device__ __forceinline__ float warp_min(float v) {
+// Bulk prefetch of `bytes` (a multiple of 16, 16-byte aligned, inside one allocation) into L2.
+__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// The D-deep slices of scan steps [a, a + kSeg) of a line into L2: one request for a row scan
+// (contiguous pixels), one per pixel for a column scan, spread over the line's G lanes.
+template <int G>
+__device__ __forceinline__ void prefetch_segment(const float* vol, const Geo& g, long long base, long long step,
+                                                 int a, int gl) {
+  constexpr int D = G * kK;
+  const int n = min(kSeg, g.len - a);
+  if (n <= 0) return;
+  if (step == 1 || step == -1) {
+    if (gl == 0) {
+      const long long lo = step > 0 ? base + a : base - a - (n - 1);
+      prefetch_l2(vol + lo * D, (uint32_t)(n * D * sizeof(float)));
+    }
+  } else {
+    for (int i = gl; i < n; i += G) prefetch_l2(vol + (base + (long long)(a + i) * step) * D, D * sizeof(float));
+  }
+}
+
+template <int G>
+__device__ __forceinline__ float group_min(float v) {
 #pragma unroll
-  for (int o = 16; o; o >>= 1) v = fminf(v, __shfl_xor_sync(kFullMask, v, o));
+  for (int o = G / 2; o; o >>= 1) v = fminf(v, __shfl_xor_sync(kFullMask, v, o));
   return v;
 }
-__device__ __forceinline__ float warp_sum(float v) {
+template <int G>
+__device__ __forceinline__ float group_sum(float v) {
 #pragma unroll
-  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(kFullMask, v, o);
+  for (int o = G / 2; o; o >>= 1) v += __shfl_xor_sync(kFullMask, v, o);
   return v;
 }
 
-// lane holds d = lane*K + j
-template <int K>
-__device__ __forceinline__ void neighbours(const float (&L)[K], int lane, float (&lm)[K], float (&lp)[K]) {
-  const float left = __shfl_up_sync(kFullMask, L[K - 1], 1);
+__device__ __forceinline__ float min8(const float (&v)[kK]) {
+  return fminf(fminf(fminf(v[0], v[1]), fminf(v[2], v[3])), fminf(fminf(v[4], v[5]), fminf(v[6], v[7])));
+}
+
+__device__ __forceinline__ void load8(const float* p, float (&v)[kK]) {
+  const float4 a = __ldg(reinterpret_cast<const float4*>(p)), b = __ldg(reinterpret_cast<const float4*>(p) + 1);
+  v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+}
+__device__ __forceinline__ void store8(float* p, const float (&v)[kK]) {
+  reinterpret_cast<float4*>(p)[0] = make_float4(v[0], v[1], v[2], v[3]);
+  reinterpret_cast<float4*>(p)[1] = make_float4(v[4], v[5], v[6], v[7]);
+}
+
+// Neighbours of the lane's disparities d = gl*8 + j within the line's group of G lanes.
+template <int G>
+__device__ __forceinline__ void neighbours(const float (&L)[kK], int gl, float (&lm)[kK], float (&lp)[kK]) {
+  const float left = __shfl_up_sync(kFullMask, L[kK - 1], 1);
   const float right = __shfl_down_sync(kFullMask, L[0], 1);
 #pragma unroll
-  for (int j = 0; j < K; ++j) {
-    lm[j] = j > 0 ? L[j - 1] : (lane > 0 ? left : kInf);
-    lp[j] = j < K - 1 ? L[j + 1] : (lane < 31 ? right : kInf);
+  for (int j = 0; j < kK; ++j) {
+    lm[j] = j > 0 ? L[j - 1] : (gl > 0 ? left : kInf);
+    lp[j] = j < kK - 1 ? L[j + 1] : (gl < G - 1 ? right : kInf);
   }
 }
 
-// One forward step: returns the new minimum. ch receives 0 same, 1 d-1, 2 d+1, 3 jump.
-template <int K>
-__device__ __forceinline__ float fstep(float (&L)[K], const float (&c)[K], float m, float p1, float p2, int lane,
-                                       int (&ch)[K]) {
-  float lm[K], lp[K];
-  neighbours<K>(L, lane, lm, lp);
+// One forward step; returns the new minimum.
+template <int G>
+__device__ __forceinline__ float fstep(float (&L)[kK], const float (&c)[kK], float m, float p1, float p2, int gl) {
+  float lm[kK], lp[kK];
+  neighbours<G>(L, gl, lm, lp);
   const float jump = m + p2;
-  float mn = kInf;
 #pragma unroll
-  for (int j = 0; j < K; ++j) {
-    float t = L[j];
-    int k = 0;
-    const float a = lm[j] + p1, b = lp[j] + p1;
-    if (a < t) { t = a; k = 1; }
-    if (b < t) { t = b; k = 2; }
-    if (jump < t) { t = jump; k = 3; }
-    ch[j] = k;
+  for (int j = 0; j < kK; ++j) {
+    const float t = fminf(fminf(L[j], lm[j] + p1), fminf(lp[j] + p1, jump));
     L[j] = c[j] + t - m;
-    mn = fminf(mn, L[j]);
   }
-  return warp_min(mn);
+  return group_min<G>(min8(L));
 }
 
-// Inputs of the next kPF pixels are loaded ahead in a register ring (each line owns its pixels, so
-// the running sum can be read ahead of the stores of earlier pixels).
-constexpr int kPF = 4;
+// Blocks of the four directions side by side in one grid: slot i (direction order[i]) owns blocks
+// [first_block[i], first_block[i + 1]).
+struct Grid4 {
+  Geo g[4];
+  int order[4];
+  int first_block[5];
+};
 
-template <int K>
-__global__ void __launch_bounds__(256) k_float_fwd(const float* __restrict__ cost, const float* __restrict__ p1m,
-                                                   const float* __restrict__ p2m, float* __restrict__ sum,
-                                                   float* __restrict__ ckpt, Geo g, int first) {
-  const int line = blockIdx.x * blockDim.y + threadIdx.y;
-  const int lane = threadIdx.x;
-  if (line >= g.lines) return;
-  const int D = 32 * K;
-  float* ck = ckpt + (size_t)line * g.nseg * D;
-  float L[K];
-  int ch[K];
-  float m = 0.f;
-  float rc[kPF][K], rs[kPF][K], rp1[kPF], rp2[kPF];
+struct Line {
+  int dir, slot, line;
+  bool live;  // false for the padding lanes of a warp past the direction's last line
+};
+
+// The line of this thread; false if the whole warp is past the direction's lines.
+template <int G>
+__device__ __forceinline__ bool locate(const Grid4& q, Line& ln, Geo& g) {
+  const int b = blockIdx.x;
+  const int slot = (b >= q.first_block[1]) + (b >= q.first_block[2]) + (b >= q.first_block[3]);
+  ln.slot = slot;
+  ln.dir = q.order[slot];
+  g = q.g[ln.dir];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wline = ((b - q.first_block[slot]) * kWarps + warp) * (32 / G);
+  if (wline >= g.lines) return false;
+  const int mine = wline + lane / G;
+  ln.live = mine < g.lines;
+  ln.line = ln.live ? mine : g.lines - 1;
+  return true;
+}
+
+struct FwdArgs {
+  const float* cost;
+  const float* p1;
+  const float* p2;
+  float* out[4];   // path volumes, one per direction
+  float* ckpt[4];  // segment entry states, one slab per direction
+  Grid4 q;
+};
+
+template <int G>
+__global__ void __launch_bounds__(kWarps * 32) k_float_fwd(const FwdArgs a) {
+  constexpr int D = G * kK;
+  Line ln;
+  Geo g;
+  if (!locate<G>(a.q, ln, g)) return;
+  const int gl = threadIdx.x % G;
+  long long base, step;
+  line_origin(g, ln.line, base, step);
+  float* out = a.out[ln.dir];
+  float* ck = a.ckpt[ln.dir] + (size_t)ln.line * g.nseg * D + gl * kK;
+  float rc[kPF][kK], rp1[kPF], rp2[kPF];
   auto fetch = [&](int j, int s) {
-    const size_t p = pix(g, line, s);
-#pragma unroll
-    for (int i = 0; i < K; ++i) {
-      rc[j][i] = cost[p * D + lane * K + i];
-      rs[j][i] = first ? 0.f : sum[p * D + lane * K + i];
-    }
-    rp1[j] = p1m[p];
-    rp2[j] = p2m[p];
+    const long long p = base + s * step;
+    load8(a.cost + p * D + gl * kK, rc[j]);
+    rp1[j] = __ldg(a.p1 + p);
+    rp2[j] = __ldg(a.p2 + p);
   };
+  prefetch_segment<G>(a.cost, g, base, step, 0, gl);
 #pragma unroll
   for (int j = 0; j < kPF; ++j)
     if (j < g.len) fetch(j, j);
+  float L[kK];
+  float m = 0.f;
   for (int s0 = 0; s0 < g.len; s0 += kPF) {
 #pragma unroll
     for (int j = 0; j < kPF; ++j) {
       const int s = s0 + j;
       if (s < g.len) {
-        const size_t p = pix(g, line, s);
-        float c[K], old[K];
+        if (s % kSeg == 0) {
+          prefetch_segment<G>(a.cost, g, base, step, s + kSeg, gl);
+          if (s > 0 && ln.live) store8(ck + (size_t)(s / kSeg) * D, L);  // state entering this segment
+        }
+        float c[kK];
 #pragma unroll
-        for (int i = 0; i < K; ++i) { c[i] = rc[j][i]; old[i] = rs[j][i]; }
+        for (int i = 0; i < kK; ++i) c[i] = rc[j][i];
         const float P1 = rp1[j], P2 = rp2[j];
         if (s + kPF < g.len) fetch(j, s + kPF);
-        if (s % kSeg == 0 && s > 0) {  // state entering this segment
-#pragma unroll
-          for (int i = 0; i < K; ++i) ck[(size_t)(s / kSeg) * D + lane * K + i] = L[i];
-        }
         if (s == 0) {
-          float mn = kInf;
 #pragma unroll
-          for (int i = 0; i < K; ++i) { L[i] = c[i]; mn = fminf(mn, c[i]); }
-          m = warp_min(mn);
+          for (int i = 0; i < kK; ++i) L[i] = c[i];
+          m = group_min<G>(min8(L));
         } else {
-          m = fstep<K>(L, c, m, P1, P2, lane, ch);
+          m = fstep<G>(L, c, m, P1, P2, gl);
         }
-        float* sp = sum + p * D + lane * K;
-#pragma unroll
-        for (int i = 0; i < K; ++i) sp[i] = first ? L[i] : old[i] + L[i];
+        if (ln.live) store8(out + (base + s * step) * D + gl * kK, L);
       }
     }
   }
 }
 
-// disp = sum_d d softmax(-S/T); dS = -gdisp/T * w(d) * (d - disp) when gdisp is given
-template <int K>
-__global__ void __launch_bounds__(256) k_soft_argmin(const float* __restrict__ sum, float* __restrict__ disp,
-                                                     const float* __restrict__ gdisp, float* __restrict__ gsum,
-                                                     size_t npix, float inv_t) {
-  const size_t p = (size_t)blockIdx.x * blockDim.y + threadIdx.y;
-  const int lane = threadIdx.x;
-  if (p >= npix) return;
-  const int D = 32 * K;
-  const float* sp = sum + p * D + lane * K;
-  float S[K], mn = kInf;
+// S = ((L0 + L1) + L2) + L3 written over L0; disp = sum_d d softmax(-S/T)
+template <int G>
+__global__ void __launch_bounds__(256) k_soft_argmin_fwd(float* __restrict__ sum, const float* __restrict__ l1,
+                                                         const float* __restrict__ l2, const float* __restrict__ l3,
+                                                         float* __restrict__ disp, size_t npix, float inv_t) {
+  constexpr int D = G * kK;
+  const size_t first = ((size_t)blockIdx.x * 8 + (threadIdx.x >> 5)) * (32 / G);
+  if (first >= npix) return;
+  const size_t mine = first + (threadIdx.x & 31) / G;
+  const bool live = mine < npix;
+  const size_t p = live ? mine : npix - 1;
+  const int gl = threadIdx.x % G;
+  const size_t off = p * D + gl * kK;
+  float S[kK], b[kK], c[kK], d[kK];
+  load8(sum + off, S);
+  load8(l1 + off, b);
+  load8(l2 + off, c);
+  load8(l3 + off, d);
 #pragma unroll
-  for (int j = 0; j < K; ++j) { S[j] = sp[j]; mn = fminf(mn, S[j]); }
-  mn = warp_min(mn);
-  float e[K], z = 0.f, num = 0.f;
+  for (int j = 0; j < kK; ++j) S[j] = ((S[j] + b[j]) + c[j]) + d[j];
+  if (live) store8(sum + off, S);
+  const float mn = group_min<G>(min8(S));
+  float z = 0.f, num = 0.f;
 #pragma unroll
-  for (int j = 0; j < K; ++j) {
+  for (int j = 0; j < kK; ++j) {
+    const float e = expf(-(S[j] - mn) * inv_t);
+    z += e;
+    num += e * (float)(gl * kK + j);
+  }
+  z = group_sum<G>(z);
+  num = group_sum<G>(num);
+  if (live && gl == 0) disp[p] = num / z;
+}
+
+// dS = -gdisp/T * w(d) * (d - disp), w = softmax(-S/T)
+template <int G>
+__global__ void __launch_bounds__(256) k_soft_argmin_bwd(const float* __restrict__ sum,
+                                                         const float* __restrict__ gdisp, float* __restrict__ gsum,
+                                                         size_t npix, float inv_t) {
+  constexpr int D = G * kK;
+  const size_t first = ((size_t)blockIdx.x * 8 + (threadIdx.x >> 5)) * (32 / G);
+  if (first >= npix) return;
+  const size_t mine = first + (threadIdx.x & 31) / G;
+  const bool live = mine < npix;
+  const size_t p = live ? mine : npix - 1;
+  const int gl = threadIdx.x % G;
+  const size_t off = p * D + gl * kK;
+  float S[kK], e[kK];
+  load8(sum + off, S);
+  const float mn = group_min<G>(min8(S));
+  float z = 0.f, num = 0.f;
+#pragma unroll
+  for (int j = 0; j < kK; ++j) {
     e[j] = expf(-(S[j] - mn) * inv_t);
     z += e[j];
-    num += e[j] * (float)(lane * K + j);
+    num += e[j] * (float)(gl * kK + j);
   }
-  z = warp_sum(z);
-  num = warp_sum(num);
-  const float d = num / z;
-  if (!gdisp) {
-    if (lane == 0) disp[p] = d;
-    return;
-  }
-  const float gd = gdisp[p];
-  float* gp = gsum + p * D + lane * K;
+  z = group_sum<G>(z);
+  num = group_sum<G>(num);
+  const float dd = num / z;
+  const float gd = __ldg(gdisp + p);
+  const float scale = -gd * inv_t / z;
+  float gs[kK];
 #pragma unroll
-  for (int j = 0; j < K; ++j) gp[j] = -gd * inv_t * (e[j] / z) * ((float)(lane * K + j) - d);
+  for (int j = 0; j < kK; ++j) gs[j] = scale * e[j] * ((float)(gl * kK + j) - dd);
+  if (live) store8(gsum + off, gs);
 }
 
-template <int K>
-__global__ void __launch_bounds__(128) k_float_bwd(const float* __restrict__ cost, const float* __restrict__ p1m,
-                                                   const float* __restrict__ p2m, const float* __restrict__ ckpt,
-                                                   const float* __restrict__ gsum, float* __restrict__ gcost,
-                                                   float* __restrict__ gp1, float* __restrict__ gp2, Geo g,
-                                                   int first) {
-  const int D = 32 * K;
-  extern __shared__ float seg_smem[];
-  const int line = blockIdx.x * blockDim.y + threadIdx.y;
-  const int lane = threadIdx.x;
-  if (line >= g.lines) return;
-  // per warp: (kSeg + 1) states of D floats; slot 0 = state entering the segment
-  float* st = seg_smem + (size_t)threadIdx.y * (kSeg + 1) * D;
-  const float* ck = ckpt + (size_t)line * g.nseg * D;
-  float gnext[K];
+struct BwdArgs {
+  const float* cost;
+  const float* p1;
+  const float* p2;
+  const float* gsum;
+  const float* ckpt[4];
+  float* gout[4];  // gradient volumes, one per direction (written)
+  float* gp1[4];   // penalty-map gradients, one per direction (written)
+  float* gp2[4];
+  Grid4 q;
+};
+
+// Shared memory of one line: (kSeg + 1) states of D floats (slot 0 = state entering the segment),
+// each stored as D/4 float4 in the order (half h, lane gl) so a group's 128-bit accesses are
+// contiguous.
+template <int G>
+constexpr size_t bwd_smem_bytes() {
+  return (size_t)kWarps * (32 / G) * (kSeg + 1) * G * kK * sizeof(float);
+}
+
+template <int G>
+__global__ void __launch_bounds__(kWarps * 32) k_float_bwd(const BwdArgs a) {
+  constexpr int D = G * kK, Q = D / 4;
+  extern __shared__ float4 seg_smem[];
+  Line ln;
+  Geo g;
+  if (!locate<G>(a.q, ln, g)) return;
+  const int lane = threadIdx.x & 31, gl = lane % G, grp = lane / G;
+  long long base, step;
+  line_origin(g, ln.line, base, step);
+  float4* st = seg_smem + (size_t)((threadIdx.x >> 5) * (32 / G) + grp) * (kSeg + 1) * Q;
+  auto st_put = [&](int slot, const float (&v)[kK]) {
+    st[slot * Q + gl] = make_float4(v[0], v[1], v[2], v[3]);
+    st[slot * Q + G + gl] = make_float4(v[4], v[5], v[6], v[7]);
+  };
+  auto st_get = [&](int slot, float (&v)[kK]) {
+    const float4 x = st[slot * Q + gl], y = st[slot * Q + G + gl];
+    v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w; v[4] = y.x; v[5] = y.y; v[6] = y.z; v[7] = y.w;
+  };
+  const float* ck = a.ckpt[ln.dir] + (size_t)ln.line * g.nseg * D + gl * kK;
+  float* gout = a.gout[ln.dir];
+  float* gp1 = a.gp1[ln.dir];
+  float* gp2 = a.gp2[ln.dir];
+  float gnext[kK];
 #pragma unroll
-  for (int j = 0; j < K; ++j) gnext[j] = 0.f;
-  for (int k = g.nseg - 1; k >= 0; --k) {
+  for (int j = 0; j < kK; ++j) gnext[j] = 0.f;
+  const int last = g.nseg - 1;
+  prefetch_segment<G>(a.cost, g, base, step, last * kSeg, gl);
+  prefetch_segment<G>(a.gsum, g, base, step, last * kSeg, gl);
+  for (int k = last; k >= 0; --k) {
     const int s0 = k * kSeg, s1 = min(g.len, s0 + kSeg);
-    // recompute the segment: st[1 + (s - s0)] = L(s)
-    float L[K], c[K];
-    int ch[K];
+    if (k > 0) {  // the next segment's inputs, while this one is processed
+      prefetch_segment<G>(a.cost, g, base, step, s0 - kSeg, gl);
+      prefetch_segment<G>(a.gsum, g, base, step, s0 - kSeg, gl);
+    }
+    // recompute the segment: slot 1 + (s - s0) = L(s)
+    float L[kK];
     float m = 0.f;
     if (k > 0) {
-#pragma unroll
-      for (int j = 0; j < K; ++j) {
-        L[j] = ck[(size_t)k * D + lane * K + j];
-        st[lane * K + j] = L[j];
-      }
-      float mn = kInf;
-#pragma unroll
-      for (int j = 0; j < K; ++j) mn = fminf(mn, L[j]);
-      m = warp_min(mn);
+      load8(ck + (size_t)k * D, L);
+      st_put(0, L);
+      m = group_min<G>(min8(L));
     }
     {
-      // inputs of the segment's pixels through a kPF-deep register ring
-      float rc[kPF][K], rp1[kPF], rp2[kPF];
+      float rc[kPF][kK], rp1[kPF], rp2[kPF];
       auto fetch = [&](int j, int s) {
-        const size_t p = pix(g, line, s);
-#pragma unroll
-        for (int i = 0; i < K; ++i) rc[j][i] = cost[p * D + lane * K + i];
-        rp1[j] = p1m[p];
-        rp2[j] = p2m[p];
+        const long long p = base + s * step;
+        load8(a.cost + p * D + gl * kK, rc[j]);
+        rp1[j] = __ldg(a.p1 + p);
+        rp2[j] = __ldg(a.p2 + p);
       };
 #pragma unroll
       for (int j = 0; j < kPF; ++j)
@@ -248,110 +382,140 @@ __global__ void __launch_bounds__(128) k_float_bwd(const float* __restrict__ cos
         for (int j = 0; j < kPF; ++j) {
           const int s = b + j;
           if (s < s1) {
+            float c[kK];
 #pragma unroll
-            for (int i = 0; i < K; ++i) c[i] = rc[j][i];
+            for (int i = 0; i < kK; ++i) c[i] = rc[j][i];
             const float P1 = rp1[j], P2 = rp2[j];
             if (s + kPF < s1) fetch(j, s + kPF);
             if (s == 0) {
-              float mn = kInf;
 #pragma unroll
-              for (int i = 0; i < K; ++i) { L[i] = c[i]; mn = fminf(mn, c[i]); }
-              m = warp_min(mn);
+              for (int i = 0; i < kK; ++i) L[i] = c[i];
+              m = group_min<G>(min8(L));
             } else {
-              m = fstep<K>(L, c, m, P1, P2, lane, ch);
+              m = fstep<G>(L, c, m, P1, P2, gl);
             }
-#pragma unroll
-            for (int i = 0; i < K; ++i) st[(size_t)(1 + s - s0) * D + lane * K + i] = L[i];
+            st_put(1 + s - s0, L);
           }
         }
       }
     }
     __syncwarp();
     // adjoint through the segment, last pixel first; its inputs through a register ring
-    float rg[kPF][K], rgc[kPF][K], rq1[kPF], rq2[kPF];
+    float rg[kPF][kK], rq1[kPF], rq2[kPF];
     auto fetch_b = [&](int j, int s) {
-      const size_t p = pix(g, line, s);
-#pragma unroll
-      for (int i = 0; i < K; ++i) {
-        rg[j][i] = gsum[p * D + lane * K + i];
-        rgc[j][i] = first ? 0.f : gcost[p * D + lane * K + i];
-      }
-      rq1[j] = p1m[p];
-      rq2[j] = p2m[p];
+      const long long p = base + s * step;
+      load8(a.gsum + p * D + gl * kK, rg[j]);
+      rq1[j] = __ldg(a.p1 + p);
+      rq2[j] = __ldg(a.p2 + p);
     };
 #pragma unroll
     for (int j = 0; j < kPF; ++j)
       if (s1 - 1 - j >= s0) fetch_b(j, s1 - 1 - j);
-    for (int b = s1 - 1; b >= s0; b -= kPF)
+    for (int b = s1 - 1; b >= s0; b -= kPF) {
 #pragma unroll
-    for (int jj = 0; jj < kPF; ++jj) {
-      const int s = b - jj;
-      if (s < s0) break;
-      const size_t p = pix(g, line, s);
-      float gl[K], gco[K];
+      for (int jj = 0; jj < kPF; ++jj) {
+        const int s = b - jj;
+        if (s < s0) break;
+        const long long p = base + s * step;
+        float gl8[kK];
 #pragma unroll
-      for (int j = 0; j < K; ++j) { gl[j] = rg[jj][j] + gnext[j]; gco[j] = rgc[jj][j]; }
-      const float P1 = rq1[jj], P2 = rq2[jj];
-      if (s - kPF >= s0) fetch_b(jj, s - kPF);
-      float* gc = gcost + p * D + lane * K;
+        for (int j = 0; j < kK; ++j) gl8[j] = rg[jj][j] + gnext[j];
+        const float P1 = rq1[jj], P2 = rq2[jj];
+        if (s - kPF >= s0) fetch_b(jj, s - kPF);
+        if (ln.live) store8(gout + p * D + gl * kK, gl8);
+        if (s == 0) {  // the first pixel of a path adds nothing to the penalties
+          if (ln.live && gl == 0) {
+            gp1[p] = 0.f;
+            gp2[p] = 0.f;
+          }
+          break;
+        }
+        // previous state L_q = L(s-1): slot (s - s0) (slot 0 = checkpoint when s == s0)
+        float Lq[kK];
+        st_get(s - s0, Lq);
+        // m_q and its (lowest) index
+        float mn = Lq[0];
+        int mi = gl * kK;
 #pragma unroll
-      for (int j = 0; j < K; ++j) gc[j] = first ? gl[j] : gco[j] + gl[j];
-      if (s == 0) break;
-      // previous state L_q = L(s-1): slot (s - s0) (slot 0 = checkpoint when s == s0)
-      const float* q = st + (size_t)(s - s0) * D;
-      float Lq[K];
+        for (int j = 1; j < kK; ++j)
+          if (Lq[j] < mn) { mn = Lq[j]; mi = gl * kK + j; }
+        const float mq = group_min<G>(mn);
+        const unsigned hit = (__ballot_sync(kFullMask, mn == mq) >> (grp * G)) & ((1u << G) - 1u);
+        const int kq = __shfl_sync(kFullMask, mi, grp * G + __ffs(hit) - 1);
+        // choices at p
+        float lm[kK], lp[kK];
+        neighbours<G>(Lq, gl, lm, lp);
+        const float jump = mq + P2;
+        float g1 = 0.f, g2 = 0.f, gall = 0.f;
+        float gsame[kK], gm1[kK], gp1v[kK];
 #pragma unroll
-      for (int j = 0; j < K; ++j) Lq[j] = q[lane * K + j];
-      // m_q and its (lowest) index
-      float mn = kInf;
-      int mi = 0;
+        for (int j = 0; j < kK; ++j) {
+          float t = Lq[j];
+          int c3 = 0;
+          if (lm[j] + P1 < t) { t = lm[j] + P1; c3 = 1; }
+          if (lp[j] + P1 < t) { t = lp[j] + P1; c3 = 2; }
+          if (jump < t) { c3 = 3; }
+          gsame[j] = c3 == 0 ? gl8[j] : 0.f;
+          gm1[j] = c3 == 1 ? gl8[j] : 0.f;   // flows to L_q(d-1)
+          gp1v[j] = c3 == 2 ? gl8[j] : 0.f;  // flows to L_q(d+1)
+          if (c3 == 1 || c3 == 2) g1 += gl8[j];
+          if (c3 == 3) g2 += gl8[j];
+          gall += gl8[j];
+        }
+        g1 = group_sum<G>(g1);
+        g2 = group_sum<G>(g2);
+        gall = group_sum<G>(gall);
+        if (ln.live && gl == 0) {
+          gp1[p] = g1;
+          gp2[p] = g2;
+        }
+        // gradient of L_q: same d, from d+1 choosing d-1 (i.e. d), from d-1 choosing d+1 (i.e. d)
+        const float from_up = __shfl_down_sync(kFullMask, gm1[0], 1);      // gm1 of d+1, for d = gl*8+7
+        const float from_down = __shfl_up_sync(kFullMask, gp1v[kK - 1], 1); // gp1 of d-1, for d = gl*8
 #pragma unroll
-      for (int j = 0; j < K; ++j)
-        if (Lq[j] < mn) { mn = Lq[j]; mi = lane * K + j; }
-      const float mq = warp_min(mn);
-      const unsigned hit = __ballot_sync(kFullMask, mn == mq);
-      const int src = __ffs(hit) - 1;
-      const int kq = __shfl_sync(kFullMask, mi, src);
-      // choices at p
-      float lm[K], lp[K];
-      neighbours<K>(Lq, lane, lm, lp);
-      const float jump = mq + P2;
-      float g1 = 0.f, g2 = 0.f, gall = 0.f;
-      float gsame[K], gm1[K], gp1v[K];
-#pragma unroll
-      for (int j = 0; j < K; ++j) {
-        float t = Lq[j];
-        int c3 = 0;
-        if (lm[j] + P1 < t) { t = lm[j] + P1; c3 = 1; }
-        if (lp[j] + P1 < t) { t = lp[j] + P1; c3 = 2; }
-        if (jump < t) { c3 = 3; }
-        gsame[j] = c3 == 0 ? gl[j] : 0.f;
-        gm1[j] = c3 == 1 ? gl[j] : 0.f;   // flows to L_q(d-1)
-        gp1v[j] = c3 == 2 ? gl[j] : 0.f;  // flows to L_q(d+1)
-        if (c3 == 1 || c3 == 2) g1 += gl[j];
-        if (c3 == 3) g2 += gl[j];
-        gall += gl[j];
-      }
-      g1 = warp_sum(g1);
-      g2 = warp_sum(g2);
-      gall = warp_sum(gall);
-      if (lane == 0) {
-        gp1[p] += g1;
-        gp2[p] += g2;
-      }
-      // gradient of L_q: same d, from d+1 choosing d-1 (i.e. d), from d-1 choosing d+1 (i.e. d)
-      const float from_up = __shfl_down_sync(kFullMask, gm1[0], 1);     // d = lane*K+K-1 receives gm1 of d+1
-      const float from_down = __shfl_up_sync(kFullMask, gp1v[K - 1], 1); // d = lane*K receives gp1 of d-1
-#pragma unroll
-      for (int j = 0; j < K; ++j) {
-        float v = gsame[j];
-        v += j < K - 1 ? gm1[j + 1] : (lane < 31 ? from_up : 0.f);
-        v += j > 0 ? gp1v[j - 1] : (lane > 0 ? from_down : 0.f);
-        if (lane * K + j == kq) v += g2 - gall;
-        gnext[j] = v;
+        for (int j = 0; j < kK; ++j) {
+          float v = gsame[j];
+          v += j < kK - 1 ? gm1[j + 1] : (gl < G - 1 ? from_up : 0.f);
+          v += j > 0 ? gp1v[j - 1] : (gl > 0 ? from_down : 0.f);
+          if (gl * kK + j == kq) v += g2 - gall;
+          gnext[j] = v;
+        }
       }
     }
     __syncwarp();
+  }
+}
+
+// grad_cost = ((G0 + G1) + G2) + G3 in place over G0; grad_p = (((0 + a0) + a1) + a2) + a3
+struct SumArgs {
+  float4* g0;
+  const float4* g1;
+  const float4* g2;
+  const float4* g3;
+  size_t n4;
+  float* gp1;
+  float* gp2;
+  const float* a1[4];
+  const float* a2[4];
+  size_t npix;
+};
+
+__global__ void __launch_bounds__(256) k_grad_sum(const SumArgs a) {
+  const size_t n = a.n4 + a.npix;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    if (i < a.n4) {
+      float4 x = a.g0[i];
+      const float4 y = __ldg(a.g1 + i), z = __ldg(a.g2 + i), w = __ldg(a.g3 + i);
+      x.x = ((x.x + y.x) + z.x) + w.x;
+      x.y = ((x.y + y.y) + z.y) + w.y;
+      x.z = ((x.z + y.z) + z.z) + w.z;
+      x.w = ((x.w + y.w) + z.w) + w.w;
+      a.g0[i] = x;
+    } else {
+      const size_t p = i - a.n4;
+      a.gp1[p] = (((0.f + a.a1[0][p]) + a.a1[1][p]) + a.a1[2][p]) + a.a1[3][p];
+      a.gp2[p] = (((0.f + a.a2[0][p]) + a.a2[1][p]) + a.a2[2][p]) + a.a2[3][p];
+    }
   }
 }
 
@@ -370,7 +534,111 @@ int validate(int B, int H, int W, int D) {
     sgm_set_process_error("float SGM: B, H, W > 0 and D in {32, 64} required");
     return SGM_ERR_ARG;
   }
+  if ((size_t)B * H * W * D > ((size_t)1 << 40)) {
+    sgm_set_process_error("float SGM: volume too large");
+    return SGM_ERR_ARG;
+  }
   return SGM_OK;
+}
+
+int check_aligned(std::initializer_list<const void*> ptrs) {
+  for (const void* p : ptrs)
+    if (reinterpret_cast<uintptr_t>(p) & 15) {
+      sgm_set_process_error("float SGM: cost, sum, gradient and workspace arrays must be 16-byte aligned");
+      return SGM_ERR_ARG;
+    }
+  return SGM_OK;
+}
+
+size_t slab_elems(int B, int H, int W, int D) { return sgm_float_checkpoint_elems(B, H, W, D) / 4; }
+
+// The four directions of one launch, row scans first (their scanlines are the longest).
+template <int G>
+Grid4 make_grid(int B, int H, int W, int D) {
+  Grid4 q;
+  const int order[4] = {1, 3, 0, 2};
+  const int lines_per_block = kWarps * (32 / G);
+  q.first_block[0] = 0;
+  for (int i = 0; i < 4; ++i) {
+    q.order[i] = order[i];
+    q.g[i] = make_geo(B, H, W, D, i);  // indexed by direction
+  }
+  for (int i = 0; i < 4; ++i)
+    q.first_block[i + 1] = q.first_block[i] + (q.g[order[i]].lines + lines_per_block - 1) / lines_per_block;
+  return q;
+}
+
+template <int G>
+int forward_impl(const float* cost, const float* p1, const float* p2, int B, int H, int W, float inv_t, float* sum,
+                 float* ckpt, float* work, float* disp, cudaStream_t s) {
+  constexpr int D = G * kK;
+  const size_t V = (size_t)B * H * W * D, npix = (size_t)B * H * W;
+  FwdArgs a;
+  a.cost = cost;
+  a.p1 = p1;
+  a.p2 = p2;
+  a.out[0] = sum;
+  for (int i = 1; i < 4; ++i) a.out[i] = work + (i - 1) * V;
+  const size_t slab = slab_elems(B, H, W, D);
+  for (int i = 0; i < 4; ++i) a.ckpt[i] = ckpt + slab * i;
+  a.q = make_grid<G>(B, H, W, D);
+  k_float_fwd<G><<<a.q.first_block[4], kWarps * 32, 0, s>>>(a);
+  int st = check("float forward");
+  if (st) return st;
+  const size_t px_per_block = 8 * (32 / G);
+  k_soft_argmin_fwd<G><<<(unsigned)((npix + px_per_block - 1) / px_per_block), 256, 0, s>>>(
+      sum, a.out[1], a.out[2], a.out[3], disp, npix, inv_t);
+  return check("soft argmin");
+}
+
+template <int G>
+int backward_impl(const float* cost, const float* p1, const float* p2, int B, int H, int W, float inv_t,
+                  const float* sum, const float* ckpt, const float* grad_disp, float* grad_sum, float* work,
+                  float* grad_cost, float* grad_p1, float* grad_p2, cudaStream_t s) {
+  constexpr int D = G * kK;
+  const size_t V = (size_t)B * H * W * D, npix = (size_t)B * H * W;
+  const size_t px_per_block = 8 * (32 / G);
+  k_soft_argmin_bwd<G><<<(unsigned)((npix + px_per_block - 1) / px_per_block), 256, 0, s>>>(
+      sum, grad_disp, grad_sum, npix, inv_t);
+  int st = check("soft argmin backward");
+  if (st) return st;
+  BwdArgs a;
+  a.cost = cost;
+  a.p1 = p1;
+  a.p2 = p2;
+  a.gsum = grad_sum;
+  const size_t slab = slab_elems(B, H, W, D);
+  float* maps = work + 3 * V;
+  for (int i = 0; i < 4; ++i) {
+    a.ckpt[i] = ckpt + slab * i;
+    a.gout[i] = i == 0 ? grad_cost : work + (i - 1) * V;
+    a.gp1[i] = maps + i * npix;
+    a.gp2[i] = maps + (4 + i) * npix;
+  }
+  a.q = make_grid<G>(B, H, W, D);
+  constexpr size_t smem = bwd_smem_bytes<G>();
+  if (cudaFuncSetAttribute(k_float_bwd<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return check("float backward attribute");
+  k_float_bwd<G><<<a.q.first_block[4], kWarps * 32, smem, s>>>(a);
+  if ((st = check("float backward"))) return st;
+  SumArgs r;
+  r.g0 = reinterpret_cast<float4*>(grad_cost);
+  r.g1 = reinterpret_cast<const float4*>(a.gout[1]);
+  r.g2 = reinterpret_cast<const float4*>(a.gout[2]);
+  r.g3 = reinterpret_cast<const float4*>(a.gout[3]);
+  r.n4 = V / 4;
+  r.gp1 = grad_p1;
+  r.gp2 = grad_p2;
+  for (int i = 0; i < 4; ++i) {
+    r.a1[i] = a.gp1[i];
+    r.a2[i] = a.gp2[i];
+  }
+  r.npix = npix;
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  k_grad_sum<<<nsm * 8, 256, 0, s>>>(r);
+  return check("float backward sum");
 }
 
 }  // namespace
@@ -386,59 +654,31 @@ size_t sgm_float_checkpoint_elems(int32_t B, int32_t H, int32_t W, int32_t D) {
   return 4 * n;
 }
 
+size_t sgm_float_workspace_elems(int32_t B, int32_t H, int32_t W, int32_t D) {
+  return 3 * (size_t)B * H * W * D + 8 * (size_t)B * H * W;
+}
+
 int sgm_float_forward(const float* cost, const float* p1, const float* p2, int32_t B, int32_t H, int32_t W,
-                      int32_t D, float temperature, float* sum, float* ckpt, float* disp, void* stream) {
+                      int32_t D, float temperature, float* sum, float* ckpt, float* work, float* disp, void* stream) {
   int st = validate(B, H, W, D);
-  if (st) return st;
+  if (st || (st = check_aligned({cost, sum, ckpt, work}))) return st;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  // path checkpoints are laid out with the largest per-path size so every path has its own slab
-  const size_t slab = sgm_float_checkpoint_elems(B, H, W, D) / 4;
-  const int order[4] = {0, 1, 2, 3};
-  for (int i = 0; i < 4; ++i) {
-    Geo g = make_geo(B, H, W, D, order[i]);
-    float* ck = ckpt + slab * order[i];
-    dim3 blk(32, 8), grd((g.lines + 7) / 8);
-    if (D == 64) k_float_fwd<2><<<grd, blk, 0, s>>>(cost, p1, p2, sum, ck, g, i == 0);
-    else k_float_fwd<1><<<grd, blk, 0, s>>>(cost, p1, p2, sum, ck, g, i == 0);
-    if ((st = check("float forward"))) return st;
-  }
-  const size_t npix = (size_t)B * H * W;
-  dim3 blk(32, 8), grd((unsigned)((npix + 7) / 8));
-  if (D == 64) k_soft_argmin<2><<<grd, blk, 0, s>>>(sum, disp, nullptr, nullptr, npix, 1.0f / temperature);
-  else k_soft_argmin<1><<<grd, blk, 0, s>>>(sum, disp, nullptr, nullptr, npix, 1.0f / temperature);
-  return check("soft argmin");
+  const float inv_t = 1.0f / temperature;
+  return D == 64 ? forward_impl<8>(cost, p1, p2, B, H, W, inv_t, sum, ckpt, work, disp, s)
+                 : forward_impl<4>(cost, p1, p2, B, H, W, inv_t, sum, ckpt, work, disp, s);
 }
 
 int sgm_float_backward(const float* cost, const float* p1, const float* p2, int32_t B, int32_t H, int32_t W, int32_t D,
                        float temperature, const float* sum, const float* ckpt, const float* grad_disp,
-                       float* grad_sum, float* grad_cost, float* grad_p1, float* grad_p2, void* stream) {
+                       float* grad_sum, float* work, float* grad_cost, float* grad_p1, float* grad_p2, void* stream) {
   int st = validate(B, H, W, D);
-  if (st) return st;
+  if (st || (st = check_aligned({cost, sum, ckpt, grad_sum, work, grad_cost}))) return st;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const size_t npix = (size_t)B * H * W;
-  {
-    dim3 blk(32, 8), grd((unsigned)((npix + 7) / 8));
-    if (D == 64) k_soft_argmin<2><<<grd, blk, 0, s>>>(sum, nullptr, grad_disp, grad_sum, npix, 1.0f / temperature);
-    else k_soft_argmin<1><<<grd, blk, 0, s>>>(sum, nullptr, grad_disp, grad_sum, npix, 1.0f / temperature);
-    if ((st = check("soft argmin backward"))) return st;
-  }
-  // P1/P2 gradients accumulate over the paths; the first pixel of a path adds nothing
-  if (cudaMemsetAsync(grad_p1, 0, npix * sizeof(float), s) != cudaSuccess ||
-      cudaMemsetAsync(grad_p2, 0, npix * sizeof(float), s) != cudaSuccess)
-    return check("float backward memset");
-  const size_t slab = sgm_float_checkpoint_elems(B, H, W, D) / 4;
-  for (int i = 0; i < 4; ++i) {
-    Geo g = make_geo(B, H, W, D, i);
-    const float* ck = ckpt + slab * i;
-    dim3 blk(32, 4), grd((g.lines + 3) / 4);
-    const size_t smem = (size_t)4 * (kSeg + 1) * D * sizeof(float);
-    if (D == 64)
-      k_float_bwd<2><<<grd, blk, smem, s>>>(cost, p1, p2, ck, grad_sum, grad_cost, grad_p1, grad_p2, g, i == 0);
-    else
-      k_float_bwd<1><<<grd, blk, smem, s>>>(cost, p1, p2, ck, grad_sum, grad_cost, grad_p1, grad_p2, g, i == 0);
-    if ((st = check("float backward"))) return st;
-  }
-  return SGM_OK;
+  const float inv_t = 1.0f / temperature;
+  return D == 64 ? backward_impl<8>(cost, p1, p2, B, H, W, inv_t, sum, ckpt, grad_disp, grad_sum, work, grad_cost,
+                                    grad_p1, grad_p2, s)
+                 : backward_impl<4>(cost, p1, p2, B, H, W, inv_t, sum, ckpt, grad_disp, grad_sum, work, grad_cost,
+                                    grad_p1, grad_p2, s);
 }
 
 }  // extern "C"

@@ -21,12 +21,19 @@ def _lib():
         vp, i32, f32 = C.c_void_p, C.c_int32, C.c_float
         lib.sgm_float_checkpoint_elems.argtypes = [i32, i32, i32, i32]
         lib.sgm_float_checkpoint_elems.restype = C.c_size_t
-        lib.sgm_float_forward.argtypes = [vp, vp, vp, i32, i32, i32, i32, f32, vp, vp, vp, vp]
+        lib.sgm_float_workspace_elems.argtypes = [i32, i32, i32, i32]
+        lib.sgm_float_workspace_elems.restype = C.c_size_t
+        lib.sgm_float_forward.argtypes = [vp, vp, vp, i32, i32, i32, i32, f32, vp, vp, vp, vp, vp]
         lib.sgm_float_forward.restype = i32
-        lib.sgm_float_backward.argtypes = [vp, vp, vp, i32, i32, i32, i32, f32, vp, vp, vp, vp, vp, vp, vp, vp]
+        lib.sgm_float_backward.argtypes = [vp, vp, vp, i32, i32, i32, i32, f32, vp, vp, vp, vp, vp, vp, vp, vp, vp]
         lib.sgm_float_backward.restype = i32
         lib._float_sgm_bound = True
     return lib
+
+
+def _aligned(t):
+    """the kernels read the cost volume with 16-byte vector loads"""
+    return t if t.data_ptr() % 16 == 0 else t.clone()
 
 
 class FloatSGM(torch.autograd.Function):
@@ -34,14 +41,15 @@ class FloatSGM(torch.autograd.Function):
     def forward(ctx, cost, p1, p2, temperature=1.0):
         if not (cost.is_cuda and cost.dtype == torch.float32 and cost.dim() == 4):
             raise ValueError("cost must be a float32 CUDA tensor [B,H,W,D]")
-        cost, p1, p2 = cost.contiguous(), p1.contiguous().float(), p2.contiguous().float()
+        cost, p1, p2 = _aligned(cost.contiguous()), p1.contiguous().float(), p2.contiguous().float()
         B, H, W, D = cost.shape
         lib = _lib()
         sum_ = torch.empty_like(cost)
         ckpt = torch.empty(lib.sgm_float_checkpoint_elems(B, H, W, D), dtype=torch.float32, device=cost.device)
+        work = torch.empty(lib.sgm_float_workspace_elems(B, H, W, D), dtype=torch.float32, device=cost.device)
         disp = torch.empty((B, H, W), dtype=torch.float32, device=cost.device)
         st = lib.sgm_float_forward(cost.data_ptr(), p1.data_ptr(), p2.data_ptr(), B, H, W, D, float(temperature),
-                                   sum_.data_ptr(), ckpt.data_ptr(), disp.data_ptr(),
+                                   sum_.data_ptr(), ckpt.data_ptr(), work.data_ptr(), disp.data_ptr(),
                                    torch.cuda.current_stream(cost.device).cuda_stream)
         if st != 0:
             raise RuntimeError(f"float SGM forward failed: {lib.sgm_last_error(None).decode()}")
@@ -59,9 +67,10 @@ class FloatSGM(torch.autograd.Function):
         gcost = torch.empty_like(cost)
         gp1 = torch.empty_like(p1)
         gp2 = torch.empty_like(p2)
+        work = torch.empty(lib.sgm_float_workspace_elems(B, H, W, D), dtype=torch.float32, device=cost.device)
         st = lib.sgm_float_backward(cost.data_ptr(), p1.data_ptr(), p2.data_ptr(), B, H, W, D, ctx.temperature,
                                     sum_.data_ptr(), ckpt.data_ptr(), g.data_ptr(), gsum.data_ptr(),
-                                    gcost.data_ptr(), gp1.data_ptr(), gp2.data_ptr(),
+                                    work.data_ptr(), gcost.data_ptr(), gp1.data_ptr(), gp2.data_ptr(),
                                     torch.cuda.current_stream(cost.device).cuda_stream)
         if st != 0:
             raise RuntimeError(f"float SGM backward failed: {lib.sgm_last_error(None).decode()}")

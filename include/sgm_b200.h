@@ -235,19 +235,25 @@ SGM_API int sgm_batch_bucket(sgm_batch_t b, int32_t index, sgm_batch_bucket_t* b
 
 /* No counterpart in the reference. Float32 4-path hard-min SGM with per-pixel P1/P2 maps and a
  * soft-argmin disparity: L_p(d) = C_p(d) + min(L_q(d), L_q(d±1)+P1(p), m_q+P2(p)) - m_q,
- * S = sum of the paths, disp = sum_d d*softmax(-S/T). Device pointers: cost [B][H][W][D],
- * p1/p2/disp [B][H][W], sum [B][H][W][D] (kept for the backward pass), ckpt of
- * sgm_float_checkpoint_elems floats (path states every 16 pixels). D = 32 or 64. */
+ * S = ((L_0 + L_1) + L_2) + L_3 over the paths (top->bottom, left->right, bottom->top,
+ * right->left), disp = sum_d d*softmax(-S/T). Device pointers: cost [B][H][W][D],
+ * p1/p2/disp [B][H][W], sum [B][H][W][D] (S, kept for the backward pass), ckpt of
+ * sgm_float_checkpoint_elems floats (path states every 16 pixels, kept for the backward pass),
+ * work of sgm_float_workspace_elems floats (scratch, free after the call's work completes on
+ * `stream`). D = 32 or 64; cost, sum, ckpt and work 16-byte aligned. */
 SGM_API size_t sgm_float_checkpoint_elems(int32_t B, int32_t H, int32_t W, int32_t D);
+SGM_API size_t sgm_float_workspace_elems(int32_t B, int32_t H, int32_t W, int32_t D);
 SGM_API int sgm_float_forward(const float* cost, const float* p1, const float* p2, int32_t B, int32_t H, int32_t W,
-                              int32_t D, float temperature, float* sum, float* ckpt, float* disp, void* stream);
+                              int32_t D, float temperature, float* sum, float* ckpt, float* work, float* disp,
+                              void* stream);
 /* No counterpart in the reference. Gradients of sum(grad_disp * disp) with respect to cost, p1
- * and p2 (written, not accumulated); grad_sum [B][H][W][D] is scratch. Each path's states are
- * recomputed from the checkpoints, 16 pixels at a time. */
+ * and p2 (written, not accumulated); grad_sum [B][H][W][D] and work (sgm_float_workspace_elems
+ * floats) are scratch. Each path's states are recomputed from the checkpoints, 16 pixels at a
+ * time. grad_sum and grad_cost 16-byte aligned. */
 SGM_API int sgm_float_backward(const float* cost, const float* p1, const float* p2, int32_t B, int32_t H, int32_t W,
                                int32_t D, float temperature, const float* sum, const float* ckpt,
-                               const float* grad_disp, float* grad_sum, float* grad_cost, float* grad_p1,
-                               float* grad_p2, void* stream);
+                               const float* grad_disp, float* grad_sum, float* work, float* grad_cost,
+                               float* grad_p1, float* grad_p2, void* stream);
 
 /* ---------------- pyramid matcher (FasterStereoCuda) ---------------- */
 

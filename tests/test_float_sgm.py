@@ -96,6 +96,37 @@ def test_backward_matches_fp64_finite_differences_and_autograd(oracle_mod, D):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("D", [32, 64])
+def test_ragged_sizes_match_autograd_and_repeat(oracle_mod, D):
+    """Line counts that leave part of a warp idle and scanlines ending inside a segment: forward
+    and gradients against the FP64 autograd reference; a second run gives the same bits."""
+    from fasterstereocuda_b200.float_sgm import float_sgm
+    c64 = torch.tensor(jittered_cost(oracle_mod, 37, 29, D, B=2, seed=91), dtype=torch.float64)
+    gen = torch.Generator().manual_seed(3)
+    p1 = 8.0 + 4 * torch.rand(c64.shape[:-1], generator=gen, dtype=torch.float64)
+    p2 = 100.0 + 60 * torch.rand(c64.shape[:-1], generator=gen, dtype=torch.float64)
+    w = torch.randn(c64.shape[:-1], generator=gen, dtype=torch.float64)
+
+    def run():
+        c = c64.float().cuda().requires_grad_()
+        q1 = p1.float().cuda().requires_grad_()
+        q2 = p2.float().cuda().requires_grad_()
+        d = float_sgm(c, q1, q2)
+        (d * w.float().cuda()).sum().backward()
+        return [t.detach().cpu() for t in (d, c.grad, q1.grad, q2.grad)]
+    first, again = run(), run()
+    for a, b in zip(first, again):
+        assert torch.equal(a, b)
+    cr, r1, r2 = (t.clone().requires_grad_() for t in (c64, p1, p2))
+    dr = reference_sgm(cr, r1, r2)
+    assert torch.allclose(first[0].double(), dr.detach(), rtol=1e-4, atol=1e-4), (first[0].double() - dr).abs().max()
+    (dr * w).sum().backward()
+    for a, b, name in zip(first[1:], (cr.grad, r1.grad, r2.grad), ("cost", "p1", "p2")):
+        rel = (a.double() - b).norm() / max(b.norm(), 1e-12)
+        assert rel < 1e-3, (name, rel)
+
+
+@pytest.mark.gpu
 def test_fitting_penalty_maps_reduces_l1(oracle_mod):
     """Demo: fit per-pixel P1/P2 maps to the ground-truth disparity under an L1 loss."""
     from fasterstereocuda_b200.float_sgm import float_sgm
