@@ -667,8 +667,18 @@ def extra_float_sgm():
             b.record()
             torch.cuda.synchronize()
             fwd.append(a.elapsed_time(b))
-    return {"workload": "float32 SGM 4 x 1242x375, D=64, 4 paths + soft-argmin", "fwd_bwd_ms": e0.elapsed_time(e1) / n,
-            "fwd_ms": statistics.median(fwd)}
+    ms = e0.elapsed_time(e1) / n
+    # algorithmic bytes of one forward + backward: the cost volume read and its gradient written
+    # (4 B per voxel each), the penalty maps read and their gradients written, disparity and its
+    # gradient (4 B per pixel each)
+    vox, pix = B * H * W * D, B * H * W
+    alg = 8 * vox + 4 * 6 * pix
+    peak, src = peaks()
+    return {"workload": "float32 SGM 4 x 1242x375, D=64, 4 paths + soft-argmin", "fwd_bwd_ms": ms,
+            "fwd_ms": statistics.median(fwd),
+            "roofline": {"bound": "latency: each row scan is a chain of 1242 dependent steps",
+                         "alg_bytes": alg, "achieved_gbs": alg / (ms * 1e6), "peak_gbs": peak,
+                         "frac": alg / (ms * 1e6) / peak, "peak_source": src}}
 
 
 def extra_large_pyramid():

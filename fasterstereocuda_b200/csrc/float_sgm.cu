@@ -8,8 +8,10 @@
 //   S(p,d) = ((L_0 + L_1) + L_2) + L_3;  disp(p) = sum_d d * softmax_d(-S(p,d)/T)
 // Ties of the hard minima are broken in the fixed order same d, d-1, d+1, jump (lowest k for m_q).
 //
-// Mapping: a scanline is held by G = D/8 lanes of a warp, 8 disparities per lane, so a warp scans
-// 32/G lines at once and the per-pixel minimum is a 3-level (D=64) or 2-level (D=32) butterfly.
+// Mapping: a scanline is held by G lanes of a warp, K = D/G disparities per lane, so a warp scans
+// 32/G lines at once and the per-pixel minimum is a log2(G)-level butterfly. The forward scans use
+// K = 4 (the shortest instruction stream per step: the row scans are a chain of W dependent
+// steps), the backward scans K = 8 (their segment buffers fit more lines per SM).
 // All four directions run in ONE launch (their blocks side by side, the long row scans first),
 // each writing its own path volume; the soft-argmin kernel adds the four in path order. The
 // backward launch likewise runs the four adjoint scans at once, each writing its own gradient
@@ -36,10 +38,14 @@ void sgm_set_process_error(const char* msg);
 namespace {
 
 constexpr unsigned kFullMask = 0xFFFFFFFFu;
-constexpr int kK = 8;       // disparities per lane
+constexpr int kK = 8;       // disparities per lane of the soft-argmin kernels
 constexpr int kSeg = 16;    // pixels per recomputed segment
 constexpr int kPF = 4;      // depth of the register ring of per-pixel inputs
 constexpr int kWarps = 4;   // warps per block of the scan kernels
+// lanes per scanline of the forward and backward scans at D = 64 and D = 32 (any choice gives the
+// same path states: the per-disparity arithmetic and the exact minimum do not depend on it)
+constexpr int kFwdLanes64 = 16, kBwdLanes64 = 8;
+constexpr int kFwdLanes32 = 8, kBwdLanes32 = 4;
 #define kInf __int_as_float(0x7f800000)
 
 struct Geo {
@@ -77,10 +83,9 @@ __device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
 
 // The D-deep slices of scan steps [a, a + kSeg) of a line into L2: one request for a row scan
 // (contiguous pixels), one per pixel for a column scan, spread over the line's G lanes.
-template <int G>
+template <int G, int D>
 __device__ __forceinline__ void prefetch_segment(const float* vol, const Geo& g, long long base, long long step,
                                                  int a, int gl) {
-  constexpr int D = G * kK;
   const int n = min(kSeg, g.len - a);
   if (n <= 0) return;
   if (step == 1 || step == -1) {
@@ -106,43 +111,59 @@ __device__ __forceinline__ float group_sum(float v) {
   return v;
 }
 
-__device__ __forceinline__ float min8(const float (&v)[kK]) {
-  return fminf(fminf(fminf(v[0], v[1]), fminf(v[2], v[3])), fminf(fminf(v[4], v[5]), fminf(v[6], v[7])));
+// minimum of K values as a balanced tree
+template <int K>
+__device__ __forceinline__ float minK(const float (&v)[K]) {
+  float t[K];
+#pragma unroll
+  for (int i = 0; i < K; ++i) t[i] = v[i];
+#pragma unroll
+  for (int w = 1; w < K; w *= 2)
+#pragma unroll
+    for (int i = 0; i + w < K; i += 2 * w) t[i] = fminf(t[i], t[i + w]);
+  return t[0];
 }
 
-__device__ __forceinline__ void load8(const float* p, float (&v)[kK]) {
-  const float4 a = __ldg(reinterpret_cast<const float4*>(p)), b = __ldg(reinterpret_cast<const float4*>(p) + 1);
-  v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+template <int K>
+__device__ __forceinline__ void loadK(const float* p, float (&v)[K]) {
+#pragma unroll
+  for (int h = 0; h < K / 4; ++h) {
+    const float4 a = __ldg(reinterpret_cast<const float4*>(p) + h);
+    v[4 * h] = a.x; v[4 * h + 1] = a.y; v[4 * h + 2] = a.z; v[4 * h + 3] = a.w;
+  }
 }
-__device__ __forceinline__ void store8(float* p, const float (&v)[kK]) {
-  reinterpret_cast<float4*>(p)[0] = make_float4(v[0], v[1], v[2], v[3]);
-  reinterpret_cast<float4*>(p)[1] = make_float4(v[4], v[5], v[6], v[7]);
+template <int K>
+__device__ __forceinline__ void storeK(float* p, const float (&v)[K]) {
+#pragma unroll
+  for (int h = 0; h < K / 4; ++h)
+    reinterpret_cast<float4*>(p)[h] = make_float4(v[4 * h], v[4 * h + 1], v[4 * h + 2], v[4 * h + 3]);
 }
 
-// Neighbours of the lane's disparities d = gl*8 + j within the line's group of G lanes.
-template <int G>
-__device__ __forceinline__ void neighbours(const float (&L)[kK], int gl, float (&lm)[kK], float (&lp)[kK]) {
-  const float left = __shfl_up_sync(kFullMask, L[kK - 1], 1);
+// Neighbours of the lane's disparities d = gl*K + j within the line's group of G lanes.
+template <int G, int K>
+__device__ __forceinline__ void neighbours(const float (&L)[K], int gl, float (&lm)[K], float (&lp)[K]) {
+  const float left = __shfl_up_sync(kFullMask, L[K - 1], 1);
   const float right = __shfl_down_sync(kFullMask, L[0], 1);
 #pragma unroll
-  for (int j = 0; j < kK; ++j) {
+  for (int j = 0; j < K; ++j) {
     lm[j] = j > 0 ? L[j - 1] : (gl > 0 ? left : kInf);
-    lp[j] = j < kK - 1 ? L[j + 1] : (gl < G - 1 ? right : kInf);
+    lp[j] = j < K - 1 ? L[j + 1] : (gl < G - 1 ? right : kInf);
   }
 }
 
-// One forward step; returns the new minimum.
-template <int G>
-__device__ __forceinline__ float fstep(float (&L)[kK], const float (&c)[kK], float m, float p1, float p2, int gl) {
-  float lm[kK], lp[kK];
-  neighbours<G>(L, gl, lm, lp);
+// One forward step from the previous state Lq into L; returns the new minimum.
+template <int G, int K>
+__device__ __forceinline__ float fstep(const float (&Lq)[K], float (&L)[K], const float (&c)[K], float m, float p1,
+                                       float p2, int gl) {
+  float lm[K], lp[K];
+  neighbours<G, K>(Lq, gl, lm, lp);
   const float jump = m + p2;
 #pragma unroll
-  for (int j = 0; j < kK; ++j) {
-    const float t = fminf(fminf(L[j], lm[j] + p1), fminf(lp[j] + p1, jump));
+  for (int j = 0; j < K; ++j) {
+    const float t = fminf(fminf(Lq[j], lm[j] + p1), fminf(lp[j] + p1, jump));
     L[j] = c[j] + t - m;
   }
-  return group_min<G>(min8(L));
+  return group_min<G>(minK<K>(L));
 }
 
 // Blocks of the four directions side by side in one grid: slot i (direction order[i]) owns blocks
@@ -184,9 +205,9 @@ struct FwdArgs {
   Grid4 q;
 };
 
-template <int G>
-__global__ void __launch_bounds__(kWarps * 32) k_float_fwd(const FwdArgs a) {
-  constexpr int D = G * kK;
+template <int G, int K>
+__global__ void __launch_bounds__(kWarps * 32, 3) k_float_fwd(const FwdArgs a) {
+  constexpr int D = G * K;
   Line ln;
   Geo g;
   if (!locate<G>(a.q, ln, g)) return;
@@ -194,42 +215,46 @@ __global__ void __launch_bounds__(kWarps * 32) k_float_fwd(const FwdArgs a) {
   long long base, step;
   line_origin(g, ln.line, base, step);
   float* out = a.out[ln.dir];
-  float* ck = a.ckpt[ln.dir] + (size_t)ln.line * g.nseg * D + gl * kK;
-  float rc[kPF][kK], rp1[kPF], rp2[kPF];
+  float* ck = a.ckpt[ln.dir] + (size_t)ln.line * g.nseg * D + gl * K;
+  float rc[kPF][K], rp1[kPF], rp2[kPF];
   auto fetch = [&](int j, int s) {
     const long long p = base + s * step;
-    load8(a.cost + p * D + gl * kK, rc[j]);
+    loadK<K>(a.cost + p * D + gl * K, rc[j]);
     rp1[j] = __ldg(a.p1 + p);
     rp2[j] = __ldg(a.p2 + p);
   };
-  prefetch_segment<G>(a.cost, g, base, step, 0, gl);
+  prefetch_segment<G, D>(a.cost, g, base, step, 0, gl);
 #pragma unroll
   for (int j = 0; j < kPF; ++j)
     if (j < g.len) fetch(j, j);
-  float L[kK];
+  // states of even / odd scan positions: a step computes into the array the previous step's
+  // store is not reading (kPF is even, so the parity of j is the parity of s)
+  float LA[K], LB[K];
   float m = 0.f;
   for (int s0 = 0; s0 < g.len; s0 += kPF) {
 #pragma unroll
     for (int j = 0; j < kPF; ++j) {
       const int s = s0 + j;
+      float(&L)[K] = (j & 1) ? LB : LA;
+      float(&Lq)[K] = (j & 1) ? LA : LB;
       if (s < g.len) {
         if (s % kSeg == 0) {
-          prefetch_segment<G>(a.cost, g, base, step, s + kSeg, gl);
-          if (s > 0 && ln.live) store8(ck + (size_t)(s / kSeg) * D, L);  // state entering this segment
+          prefetch_segment<G, D>(a.cost, g, base, step, s + kSeg, gl);
+          if (s > 0 && ln.live) storeK<K>(ck + (size_t)(s / kSeg) * D, Lq);  // state entering this segment
         }
-        float c[kK];
+        float c[K];
 #pragma unroll
-        for (int i = 0; i < kK; ++i) c[i] = rc[j][i];
+        for (int i = 0; i < K; ++i) c[i] = rc[j][i];
         const float P1 = rp1[j], P2 = rp2[j];
         if (s + kPF < g.len) fetch(j, s + kPF);
         if (s == 0) {
 #pragma unroll
-          for (int i = 0; i < kK; ++i) L[i] = c[i];
-          m = group_min<G>(min8(L));
+          for (int i = 0; i < K; ++i) L[i] = c[i];
+          m = group_min<G>(minK<K>(L));
         } else {
-          m = fstep<G>(L, c, m, P1, P2, gl);
+          m = fstep<G, K>(Lq, L, c, m, P1, P2, gl);
         }
-        if (ln.live) store8(out + (base + s * step) * D + gl * kK, L);
+        if (ln.live) storeK<K>(out + (base + s * step) * D + gl * K, L);
       }
     }
   }
@@ -249,14 +274,14 @@ __global__ void __launch_bounds__(256) k_soft_argmin_fwd(float* __restrict__ sum
   const int gl = threadIdx.x % G;
   const size_t off = p * D + gl * kK;
   float S[kK], b[kK], c[kK], d[kK];
-  load8(sum + off, S);
-  load8(l1 + off, b);
-  load8(l2 + off, c);
-  load8(l3 + off, d);
+  loadK<kK>(sum + off, S);
+  loadK<kK>(l1 + off, b);
+  loadK<kK>(l2 + off, c);
+  loadK<kK>(l3 + off, d);
 #pragma unroll
   for (int j = 0; j < kK; ++j) S[j] = ((S[j] + b[j]) + c[j]) + d[j];
-  if (live) store8(sum + off, S);
-  const float mn = group_min<G>(min8(S));
+  if (live) storeK<kK>(sum + off, S);
+  const float mn = group_min<G>(minK<kK>(S));
   float z = 0.f, num = 0.f;
 #pragma unroll
   for (int j = 0; j < kK; ++j) {
@@ -283,8 +308,8 @@ __global__ void __launch_bounds__(256) k_soft_argmin_bwd(const float* __restrict
   const int gl = threadIdx.x % G;
   const size_t off = p * D + gl * kK;
   float S[kK], e[kK];
-  load8(sum + off, S);
-  const float mn = group_min<G>(min8(S));
+  loadK<kK>(sum + off, S);
+  const float mn = group_min<G>(minK<kK>(S));
   float z = 0.f, num = 0.f;
 #pragma unroll
   for (int j = 0; j < kK; ++j) {
@@ -300,7 +325,7 @@ __global__ void __launch_bounds__(256) k_soft_argmin_bwd(const float* __restrict
   float gs[kK];
 #pragma unroll
   for (int j = 0; j < kK; ++j) gs[j] = scale * e[j] * ((float)(gl * kK + j) - dd);
-  if (live) store8(gsum + off, gs);
+  if (live) storeK<kK>(gsum + off, gs);
 }
 
 struct BwdArgs {
@@ -318,14 +343,14 @@ struct BwdArgs {
 // Shared memory of one line: (kSeg + 1) states of D floats (slot 0 = state entering the segment),
 // each stored as D/4 float4 in the order (half h, lane gl) so a group's 128-bit accesses are
 // contiguous.
-template <int G>
+template <int G, int K>
 constexpr size_t bwd_smem_bytes() {
-  return (size_t)kWarps * (32 / G) * (kSeg + 1) * G * kK * sizeof(float);
+  return (size_t)kWarps * (32 / G) * (kSeg + 1) * G * K * sizeof(float);
 }
 
-template <int G>
+template <int G, int K>
 __global__ void __launch_bounds__(kWarps * 32) k_float_bwd(const BwdArgs a) {
-  constexpr int D = G * kK, Q = D / 4;
+  constexpr int D = G * K, Q = D / 4;
   extern __shared__ float4 seg_smem[];
   Line ln;
   Geo g;
@@ -334,43 +359,47 @@ __global__ void __launch_bounds__(kWarps * 32) k_float_bwd(const BwdArgs a) {
   long long base, step;
   line_origin(g, ln.line, base, step);
   float4* st = seg_smem + (size_t)((threadIdx.x >> 5) * (32 / G) + grp) * (kSeg + 1) * Q;
-  auto st_put = [&](int slot, const float (&v)[kK]) {
-    st[slot * Q + gl] = make_float4(v[0], v[1], v[2], v[3]);
-    st[slot * Q + G + gl] = make_float4(v[4], v[5], v[6], v[7]);
+  auto st_put = [&](int slot, const float (&v)[K]) {
+#pragma unroll
+    for (int h = 0; h < K / 4; ++h)
+      st[slot * Q + h * G + gl] = make_float4(v[4 * h], v[4 * h + 1], v[4 * h + 2], v[4 * h + 3]);
   };
-  auto st_get = [&](int slot, float (&v)[kK]) {
-    const float4 x = st[slot * Q + gl], y = st[slot * Q + G + gl];
-    v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w; v[4] = y.x; v[5] = y.y; v[6] = y.z; v[7] = y.w;
+  auto st_get = [&](int slot, float (&v)[K]) {
+#pragma unroll
+    for (int h = 0; h < K / 4; ++h) {
+      const float4 x = st[slot * Q + h * G + gl];
+      v[4 * h] = x.x; v[4 * h + 1] = x.y; v[4 * h + 2] = x.z; v[4 * h + 3] = x.w;
+    }
   };
-  const float* ck = a.ckpt[ln.dir] + (size_t)ln.line * g.nseg * D + gl * kK;
+  const float* ck = a.ckpt[ln.dir] + (size_t)ln.line * g.nseg * D + gl * K;
   float* gout = a.gout[ln.dir];
   float* gp1 = a.gp1[ln.dir];
   float* gp2 = a.gp2[ln.dir];
-  float gnext[kK];
+  float gnext[K];
 #pragma unroll
-  for (int j = 0; j < kK; ++j) gnext[j] = 0.f;
+  for (int j = 0; j < K; ++j) gnext[j] = 0.f;
   const int last = g.nseg - 1;
-  prefetch_segment<G>(a.cost, g, base, step, last * kSeg, gl);
-  prefetch_segment<G>(a.gsum, g, base, step, last * kSeg, gl);
+  prefetch_segment<G, D>(a.cost, g, base, step, last * kSeg, gl);
+  prefetch_segment<G, D>(a.gsum, g, base, step, last * kSeg, gl);
   for (int k = last; k >= 0; --k) {
     const int s0 = k * kSeg, s1 = min(g.len, s0 + kSeg);
     if (k > 0) {  // the next segment's inputs, while this one is processed
-      prefetch_segment<G>(a.cost, g, base, step, s0 - kSeg, gl);
-      prefetch_segment<G>(a.gsum, g, base, step, s0 - kSeg, gl);
+      prefetch_segment<G, D>(a.cost, g, base, step, s0 - kSeg, gl);
+      prefetch_segment<G, D>(a.gsum, g, base, step, s0 - kSeg, gl);
     }
     // recompute the segment: slot 1 + (s - s0) = L(s)
-    float L[kK];
+    float LA[K], LB[K];  // states of even / odd scan positions (s0 is even)
     float m = 0.f;
     if (k > 0) {
-      load8(ck + (size_t)k * D, L);
-      st_put(0, L);
-      m = group_min<G>(min8(L));
+      loadK<K>(ck + (size_t)k * D, LB);
+      st_put(0, LB);
+      m = group_min<G>(minK<K>(LB));
     }
     {
-      float rc[kPF][kK], rp1[kPF], rp2[kPF];
+      float rc[kPF][K], rp1[kPF], rp2[kPF];
       auto fetch = [&](int j, int s) {
         const long long p = base + s * step;
-        load8(a.cost + p * D + gl * kK, rc[j]);
+        loadK<K>(a.cost + p * D + gl * K, rc[j]);
         rp1[j] = __ldg(a.p1 + p);
         rp2[j] = __ldg(a.p2 + p);
       };
@@ -381,18 +410,20 @@ __global__ void __launch_bounds__(kWarps * 32) k_float_bwd(const BwdArgs a) {
 #pragma unroll
         for (int j = 0; j < kPF; ++j) {
           const int s = b + j;
+          float(&L)[K] = (j & 1) ? LB : LA;
+          float(&Lq)[K] = (j & 1) ? LA : LB;
           if (s < s1) {
-            float c[kK];
+            float c[K];
 #pragma unroll
-            for (int i = 0; i < kK; ++i) c[i] = rc[j][i];
+            for (int i = 0; i < K; ++i) c[i] = rc[j][i];
             const float P1 = rp1[j], P2 = rp2[j];
             if (s + kPF < s1) fetch(j, s + kPF);
             if (s == 0) {
 #pragma unroll
-              for (int i = 0; i < kK; ++i) L[i] = c[i];
-              m = group_min<G>(min8(L));
+              for (int i = 0; i < K; ++i) L[i] = c[i];
+              m = group_min<G>(minK<K>(L));
             } else {
-              m = fstep<G>(L, c, m, P1, P2, gl);
+              m = fstep<G, K>(Lq, L, c, m, P1, P2, gl);
             }
             st_put(1 + s - s0, L);
           }
@@ -401,10 +432,10 @@ __global__ void __launch_bounds__(kWarps * 32) k_float_bwd(const BwdArgs a) {
     }
     __syncwarp();
     // adjoint through the segment, last pixel first; its inputs through a register ring
-    float rg[kPF][kK], rq1[kPF], rq2[kPF];
+    float rg[kPF][K], rq1[kPF], rq2[kPF];
     auto fetch_b = [&](int j, int s) {
       const long long p = base + s * step;
-      load8(a.gsum + p * D + gl * kK, rg[j]);
+      loadK<K>(a.gsum + p * D + gl * K, rg[j]);
       rq1[j] = __ldg(a.p1 + p);
       rq2[j] = __ldg(a.p2 + p);
     };
@@ -417,12 +448,12 @@ __global__ void __launch_bounds__(kWarps * 32) k_float_bwd(const BwdArgs a) {
         const int s = b - jj;
         if (s < s0) break;
         const long long p = base + s * step;
-        float gl8[kK];
+        float gv[K];
 #pragma unroll
-        for (int j = 0; j < kK; ++j) gl8[j] = rg[jj][j] + gnext[j];
+        for (int j = 0; j < K; ++j) gv[j] = rg[jj][j] + gnext[j];
         const float P1 = rq1[jj], P2 = rq2[jj];
         if (s - kPF >= s0) fetch_b(jj, s - kPF);
-        if (ln.live) store8(gout + p * D + gl * kK, gl8);
+        if (ln.live) storeK<K>(gout + p * D + gl * K, gv);
         if (s == 0) {  // the first pixel of a path adds nothing to the penalties
           if (ln.live && gl == 0) {
             gp1[p] = 0.f;
@@ -431,36 +462,36 @@ __global__ void __launch_bounds__(kWarps * 32) k_float_bwd(const BwdArgs a) {
           break;
         }
         // previous state L_q = L(s-1): slot (s - s0) (slot 0 = checkpoint when s == s0)
-        float Lq[kK];
+        float Lq[K];
         st_get(s - s0, Lq);
         // m_q and its (lowest) index
         float mn = Lq[0];
-        int mi = gl * kK;
+        int mi = gl * K;
 #pragma unroll
-        for (int j = 1; j < kK; ++j)
-          if (Lq[j] < mn) { mn = Lq[j]; mi = gl * kK + j; }
+        for (int j = 1; j < K; ++j)
+          if (Lq[j] < mn) { mn = Lq[j]; mi = gl * K + j; }
         const float mq = group_min<G>(mn);
         const unsigned hit = (__ballot_sync(kFullMask, mn == mq) >> (grp * G)) & ((1u << G) - 1u);
         const int kq = __shfl_sync(kFullMask, mi, grp * G + __ffs(hit) - 1);
         // choices at p
-        float lm[kK], lp[kK];
-        neighbours<G>(Lq, gl, lm, lp);
+        float lm[K], lp[K];
+        neighbours<G, K>(Lq, gl, lm, lp);
         const float jump = mq + P2;
         float g1 = 0.f, g2 = 0.f, gall = 0.f;
-        float gsame[kK], gm1[kK], gp1v[kK];
+        float gsame[K], gm1[K], gp1v[K];
 #pragma unroll
-        for (int j = 0; j < kK; ++j) {
+        for (int j = 0; j < K; ++j) {
           float t = Lq[j];
           int c3 = 0;
           if (lm[j] + P1 < t) { t = lm[j] + P1; c3 = 1; }
           if (lp[j] + P1 < t) { t = lp[j] + P1; c3 = 2; }
           if (jump < t) { c3 = 3; }
-          gsame[j] = c3 == 0 ? gl8[j] : 0.f;
-          gm1[j] = c3 == 1 ? gl8[j] : 0.f;   // flows to L_q(d-1)
-          gp1v[j] = c3 == 2 ? gl8[j] : 0.f;  // flows to L_q(d+1)
-          if (c3 == 1 || c3 == 2) g1 += gl8[j];
-          if (c3 == 3) g2 += gl8[j];
-          gall += gl8[j];
+          gsame[j] = c3 == 0 ? gv[j] : 0.f;
+          gm1[j] = c3 == 1 ? gv[j] : 0.f;   // flows to L_q(d-1)
+          gp1v[j] = c3 == 2 ? gv[j] : 0.f;  // flows to L_q(d+1)
+          if (c3 == 1 || c3 == 2) g1 += gv[j];
+          if (c3 == 3) g2 += gv[j];
+          gall += gv[j];
         }
         g1 = group_sum<G>(g1);
         g2 = group_sum<G>(g2);
@@ -471,13 +502,13 @@ __global__ void __launch_bounds__(kWarps * 32) k_float_bwd(const BwdArgs a) {
         }
         // gradient of L_q: same d, from d+1 choosing d-1 (i.e. d), from d-1 choosing d+1 (i.e. d)
         const float from_up = __shfl_down_sync(kFullMask, gm1[0], 1);      // gm1 of d+1, for d = gl*8+7
-        const float from_down = __shfl_up_sync(kFullMask, gp1v[kK - 1], 1); // gp1 of d-1, for d = gl*8
+        const float from_down = __shfl_up_sync(kFullMask, gp1v[K - 1], 1); // gp1 of d-1, for d = gl*8
 #pragma unroll
-        for (int j = 0; j < kK; ++j) {
+        for (int j = 0; j < K; ++j) {
           float v = gsame[j];
-          v += j < kK - 1 ? gm1[j + 1] : (gl < G - 1 ? from_up : 0.f);
+          v += j < K - 1 ? gm1[j + 1] : (gl < G - 1 ? from_up : 0.f);
           v += j > 0 ? gp1v[j - 1] : (gl > 0 ? from_down : 0.f);
-          if (gl * kK + j == kq) v += g2 - gall;
+          if (gl * K + j == kq) v += g2 - gall;
           gnext[j] = v;
         }
       }
@@ -568,10 +599,10 @@ Grid4 make_grid(int B, int H, int W, int D) {
   return q;
 }
 
-template <int G>
+template <int G, int K>
 int forward_impl(const float* cost, const float* p1, const float* p2, int B, int H, int W, float inv_t, float* sum,
                  float* ckpt, float* work, float* disp, cudaStream_t s) {
-  constexpr int D = G * kK;
+  constexpr int D = G * K;
   const size_t V = (size_t)B * H * W * D, npix = (size_t)B * H * W;
   FwdArgs a;
   a.cost = cost;
@@ -582,23 +613,25 @@ int forward_impl(const float* cost, const float* p1, const float* p2, int B, int
   const size_t slab = slab_elems(B, H, W, D);
   for (int i = 0; i < 4; ++i) a.ckpt[i] = ckpt + slab * i;
   a.q = make_grid<G>(B, H, W, D);
-  k_float_fwd<G><<<a.q.first_block[4], kWarps * 32, 0, s>>>(a);
+  k_float_fwd<G, K><<<a.q.first_block[4], kWarps * 32, 0, s>>>(a);
   int st = check("float forward");
   if (st) return st;
-  const size_t px_per_block = 8 * (32 / G);
-  k_soft_argmin_fwd<G><<<(unsigned)((npix + px_per_block - 1) / px_per_block), 256, 0, s>>>(
+  constexpr int GS = D / kK;  // lanes per pixel of the soft-argmin kernels
+  const size_t px_per_block = 8 * (32 / GS);
+  k_soft_argmin_fwd<GS><<<(unsigned)((npix + px_per_block - 1) / px_per_block), 256, 0, s>>>(
       sum, a.out[1], a.out[2], a.out[3], disp, npix, inv_t);
   return check("soft argmin");
 }
 
-template <int G>
+template <int G, int K>
 int backward_impl(const float* cost, const float* p1, const float* p2, int B, int H, int W, float inv_t,
                   const float* sum, const float* ckpt, const float* grad_disp, float* grad_sum, float* work,
                   float* grad_cost, float* grad_p1, float* grad_p2, cudaStream_t s) {
-  constexpr int D = G * kK;
+  constexpr int D = G * K;
   const size_t V = (size_t)B * H * W * D, npix = (size_t)B * H * W;
-  const size_t px_per_block = 8 * (32 / G);
-  k_soft_argmin_bwd<G><<<(unsigned)((npix + px_per_block - 1) / px_per_block), 256, 0, s>>>(
+  constexpr int GS = D / kK;  // lanes per pixel of the soft-argmin kernels
+  const size_t px_per_block = 8 * (32 / GS);
+  k_soft_argmin_bwd<GS><<<(unsigned)((npix + px_per_block - 1) / px_per_block), 256, 0, s>>>(
       sum, grad_disp, grad_sum, npix, inv_t);
   int st = check("soft argmin backward");
   if (st) return st;
@@ -616,10 +649,10 @@ int backward_impl(const float* cost, const float* p1, const float* p2, int B, in
     a.gp2[i] = maps + (4 + i) * npix;
   }
   a.q = make_grid<G>(B, H, W, D);
-  constexpr size_t smem = bwd_smem_bytes<G>();
-  if (cudaFuncSetAttribute(k_float_bwd<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+  constexpr size_t smem = bwd_smem_bytes<G, K>();
+  if (cudaFuncSetAttribute(k_float_bwd<G, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return check("float backward attribute");
-  k_float_bwd<G><<<a.q.first_block[4], kWarps * 32, smem, s>>>(a);
+  k_float_bwd<G, K><<<a.q.first_block[4], kWarps * 32, smem, s>>>(a);
   if ((st = check("float backward"))) return st;
   SumArgs r;
   r.g0 = reinterpret_cast<float4*>(grad_cost);
@@ -664,8 +697,8 @@ int sgm_float_forward(const float* cost, const float* p1, const float* p2, int32
   if (st || (st = check_aligned({cost, sum, ckpt, work}))) return st;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const float inv_t = 1.0f / temperature;
-  return D == 64 ? forward_impl<8>(cost, p1, p2, B, H, W, inv_t, sum, ckpt, work, disp, s)
-                 : forward_impl<4>(cost, p1, p2, B, H, W, inv_t, sum, ckpt, work, disp, s);
+  return D == 64 ? forward_impl<kFwdLanes64, 64 / kFwdLanes64>(cost, p1, p2, B, H, W, inv_t, sum, ckpt, work, disp, s)
+                 : forward_impl<kFwdLanes32, 32 / kFwdLanes32>(cost, p1, p2, B, H, W, inv_t, sum, ckpt, work, disp, s);
 }
 
 int sgm_float_backward(const float* cost, const float* p1, const float* p2, int32_t B, int32_t H, int32_t W, int32_t D,
@@ -675,9 +708,9 @@ int sgm_float_backward(const float* cost, const float* p1, const float* p2, int3
   if (st || (st = check_aligned({cost, sum, ckpt, grad_sum, work, grad_cost}))) return st;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const float inv_t = 1.0f / temperature;
-  return D == 64 ? backward_impl<8>(cost, p1, p2, B, H, W, inv_t, sum, ckpt, grad_disp, grad_sum, work, grad_cost,
+  return D == 64 ? backward_impl<kBwdLanes64, 64 / kBwdLanes64>(cost, p1, p2, B, H, W, inv_t, sum, ckpt, grad_disp, grad_sum, work, grad_cost,
                                     grad_p1, grad_p2, s)
-                 : backward_impl<4>(cost, p1, p2, B, H, W, inv_t, sum, ckpt, grad_disp, grad_sum, work, grad_cost,
+                 : backward_impl<kBwdLanes32, 32 / kBwdLanes32>(cost, p1, p2, B, H, W, inv_t, sum, ckpt, grad_disp, grad_sum, work, grad_cost,
                                     grad_p1, grad_p2, s);
 }
 
