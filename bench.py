@@ -58,6 +58,7 @@ def parse():
     ap.add_argument("--extra", choices=["batch_pyramid", "batch", "batch_uneven", "float_sgm", "large_pyramid"],
                     default="", help="run one extra workload alone and print its JSON (e.g. for a profiler)")
     ap.add_argument("--extra-pairs", type=int, default=64, help="pairs of the --extra batch workloads")
+    ap.add_argument("--float-batch", type=int, default=4, help="pairs of the --extra float_sgm workload")
     return ap.parse_args()
 
 
@@ -633,11 +634,11 @@ def extra_batches(pool):
     return out
 
 
-def extra_float_sgm():
-    """Differentiable float32 SGM: forward + backward of 4 x 1242x375 x 64 (device-timed)."""
+def extra_float_sgm(B=4):
+    """Differentiable float32 SGM: forward + backward of B x 1242x375 x 64 (device-timed)."""
     import torch
     from fasterstereocuda_b200.float_sgm import float_sgm
-    B, H, W, D = 4, H_, W_, DMAX
+    H, W, D = H_, W_, DMAX
     g = torch.Generator(device="cuda").manual_seed(0)
     cost = (torch.randint(0, 64, (B, H, W, D), generator=g, device="cuda").float()
             + torch.rand((B, H, W, D), generator=g, device="cuda") * 0.5).requires_grad_()
@@ -674,7 +675,7 @@ def extra_float_sgm():
     vox, pix = B * H * W * D, B * H * W
     alg = 8 * vox + 4 * 6 * pix
     peak, src = peaks()
-    return {"workload": "float32 SGM 4 x 1242x375, D=64, 4 paths + soft-argmin", "fwd_bwd_ms": ms,
+    return {"workload": f"float32 SGM {B} x 1242x375, D=64, 4 paths + soft-argmin", "fwd_bwd_ms": ms,
             "fwd_ms": statistics.median(fwd),
             "roofline": {"bound": "latency: each row scan is a chain of 1242 dependent steps",
                          "alg_bytes": alg, "achieved_gbs": alg / (ms * 1e6), "peak_gbs": peak,
@@ -742,7 +743,7 @@ def run_extra(a):
     from fasterstereocuda_b200 import scenes
     n = a.extra_pairs
     if a.extra == "float_sgm":
-        out = extra_float_sgm()
+        out = extra_float_sgm(a.float_batch)
     elif a.extra == "large_pyramid":
         out = extra_large_pyramid()
     elif a.extra == "batch_uneven":

@@ -30,6 +30,7 @@
 
 #include <cstdint>
 #include <string>
+#include <type_traits>
 
 #include "../../include/sgm_b200.h"
 
@@ -39,7 +40,9 @@ namespace {
 
 constexpr unsigned kFullMask = 0xFFFFFFFFu;
 constexpr int kK = 8;       // disparities per lane of the soft-argmin kernels
-constexpr int kSeg = 16;    // pixels per recomputed segment
+constexpr int kSeg = 8;     // pixels per recomputed segment (checkpoint interval)
+constexpr int kPrefetchPx = 16;  // pixels per L2 prefetch request of the forward row scans
+constexpr int kBwdPF = 2;   // depth of the backward register rings (two interleaved scans per step)
 constexpr int kPF = 4;      // depth of the register ring of per-pixel inputs
 constexpr int kWarps = 4;   // warps per block of the scan kernels
 // lanes per scanline of the forward and backward scans at D = 64 and D = 32 (any choice gives the
@@ -81,12 +84,12 @@ __device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
-// The D-deep slices of scan steps [a, a + kSeg) of a line into L2: one request for a row scan
+// The D-deep slices of scan steps [a, a + kPrefetchPx) of a line into L2: one request for a row scan
 // (contiguous pixels), one per pixel for a column scan, spread over the line's G lanes.
 template <int G, int D>
 __device__ __forceinline__ void prefetch_segment(const float* vol, const Geo& g, long long base, long long step,
                                                  int a, int gl) {
-  const int n = min(kSeg, g.len - a);
+  const int n = min(kPrefetchPx, g.len - a);
   if (n <= 0) return;
   if (step == 1 || step == -1) {
     if (gl == 0) {
@@ -238,10 +241,9 @@ __global__ void __launch_bounds__(kWarps * 32, 3) k_float_fwd(const FwdArgs a) {
       float(&L)[K] = (j & 1) ? LB : LA;
       float(&Lq)[K] = (j & 1) ? LA : LB;
       if (s < g.len) {
-        if (s % kSeg == 0) {
-          prefetch_segment<G, D>(a.cost, g, base, step, s + kSeg, gl);
-          if (s > 0 && ln.live) storeK<K>(ck + (size_t)(s / kSeg) * D, Lq);  // state entering this segment
-        }
+        if (s % kPrefetchPx == 0) prefetch_segment<G, D>(a.cost, g, base, step, s + kPrefetchPx, gl);
+        if (s % kSeg == 0 && s > 0 && ln.live)
+          storeK<K>(ck + (size_t)(s / kSeg) * D, Lq);  // state entering this segment
         float c[K];
 #pragma unroll
         for (int i = 0; i < K; ++i) c[i] = rc[j][i];
@@ -340,17 +342,18 @@ struct BwdArgs {
   Grid4 q;
 };
 
-// Shared memory of one line: (kSeg + 1) states of D floats (slot 0 = state entering the segment),
-// each stored as D/4 float4 in the order (half h, lane gl) so a group's 128-bit accesses are
-// contiguous.
+// Shared memory of one line: two buffers of (kSeg + 1) states of D floats (slot 0 = state entering
+// the segment), so the recompute of one segment fills one buffer while the adjoint of the segment
+// after it reads the other. Each state is D/4 float4 in the order (quarter h, lane gl); a lane
+// reads back only what it wrote.
 template <int G, int K>
 constexpr size_t bwd_smem_bytes() {
-  return (size_t)kWarps * (32 / G) * (kSeg + 1) * G * K * sizeof(float);
+  return (size_t)kWarps * (32 / G) * 2 * (kSeg + 1) * G * K * sizeof(float);
 }
 
 template <int G, int K>
-__global__ void __launch_bounds__(kWarps * 32) k_float_bwd(const BwdArgs a) {
-  constexpr int D = G * K, Q = D / 4;
+__global__ void __launch_bounds__(kWarps * 32, 3) k_float_bwd(const BwdArgs a) {
+  constexpr int D = G * K, Q = D / 4, kSlots = kSeg + 1;
   extern __shared__ float4 seg_smem[];
   Line ln;
   Geo g;
@@ -358,16 +361,16 @@ __global__ void __launch_bounds__(kWarps * 32) k_float_bwd(const BwdArgs a) {
   const int lane = threadIdx.x & 31, gl = lane % G, grp = lane / G;
   long long base, step;
   line_origin(g, ln.line, base, step);
-  float4* st = seg_smem + (size_t)((threadIdx.x >> 5) * (32 / G) + grp) * (kSeg + 1) * Q;
-  auto st_put = [&](int slot, const float (&v)[K]) {
+  float4* st = seg_smem + (size_t)((threadIdx.x >> 5) * (32 / G) + grp) * 2 * kSlots * Q;
+  auto st_put = [&](int buf, int slot, const float (&v)[K]) {
 #pragma unroll
     for (int h = 0; h < K / 4; ++h)
-      st[slot * Q + h * G + gl] = make_float4(v[4 * h], v[4 * h + 1], v[4 * h + 2], v[4 * h + 3]);
+      st[(buf * kSlots + slot) * Q + h * G + gl] = make_float4(v[4 * h], v[4 * h + 1], v[4 * h + 2], v[4 * h + 3]);
   };
-  auto st_get = [&](int slot, float (&v)[K]) {
+  auto st_get = [&](int buf, int slot, float (&v)[K]) {
 #pragma unroll
     for (int h = 0; h < K / 4; ++h) {
-      const float4 x = st[slot * Q + h * G + gl];
+      const float4 x = st[(buf * kSlots + slot) * Q + h * G + gl];
       v[4 * h] = x.x; v[4 * h + 1] = x.y; v[4 * h + 2] = x.z; v[4 * h + 3] = x.w;
     }
   };
@@ -378,92 +381,79 @@ __global__ void __launch_bounds__(kWarps * 32) k_float_bwd(const BwdArgs a) {
   float gnext[K];
 #pragma unroll
   for (int j = 0; j < K; ++j) gnext[j] = 0.f;
+  float LA[K], LB[K];  // recomputed states of even / odd scan positions (segment starts are even)
+  float m = 0.f;
+  float rc[kBwdPF][K], rp1[kBwdPF], rp2[kBwdPF];  // inputs of the recompute steps
+  float rg[kBwdPF][K], rq1[kBwdPF], rq2[kBwdPF];  // inputs of the adjoint steps
+  auto fetch_r = [&](int j, int s) {
+    const long long p = base + s * step;
+    loadK<K>(a.cost + p * D + gl * K, rc[j]);
+    rp1[j] = __ldg(a.p1 + p);
+    rp2[j] = __ldg(a.p2 + p);
+  };
+  auto fetch_a = [&](int j, int s) {
+    const long long p = base + s * step;
+    loadK<K>(a.gsum + p * D + gl * K, rg[j]);
+    rq1[j] = __ldg(a.p1 + p);
+    rq2[j] = __ldg(a.p2 + p);
+  };
+  // Phase ph recomputes segment kr = last - ph (while ph <= last) and, interleaved with it step
+  // by step, runs the adjoint backwards through segment kr + 1 (from ph = 1 on) over the states
+  // the previous phase recomputed: two independent dependency chains per step.
   const int last = g.nseg - 1;
-  prefetch_segment<G, D>(a.cost, g, base, step, last * kSeg, gl);
-  prefetch_segment<G, D>(a.gsum, g, base, step, last * kSeg, gl);
-  for (int k = last; k >= 0; --k) {
-    const int s0 = k * kSeg, s1 = min(g.len, s0 + kSeg);
-    if (k > 0) {  // the next segment's inputs, while this one is processed
-      prefetch_segment<G, D>(a.cost, g, base, step, s0 - kSeg, gl);
-      prefetch_segment<G, D>(a.gsum, g, base, step, s0 - kSeg, gl);
-    }
-    // recompute the segment: slot 1 + (s - s0) = L(s)
-    float LA[K], LB[K];  // states of even / odd scan positions (s0 is even)
-    float m = 0.f;
-    if (k > 0) {
-      loadK<K>(ck + (size_t)k * D, LB);
-      st_put(0, LB);
+  for (int ph = 0; ph <= last + 1; ++ph) {
+    const int kr = last - ph, ka = kr + 1;
+    const int r0 = kr * kSeg, nr = kr >= 0 ? min(g.len, r0 + kSeg) - r0 : 0;
+    const int a0 = ka * kSeg, na = ph >= 1 ? min(g.len, a0 + kSeg) - a0 : 0;
+    const int br = kr & 1, ba = ka & 1;
+    if (kr > 0) {
+      loadK<K>(ck + (size_t)kr * D, LB);
+      st_put(br, 0, LB);
       m = group_min<G>(minK<K>(LB));
     }
-    {
-      float rc[kPF][K], rp1[kPF], rp2[kPF];
-      auto fetch = [&](int j, int s) {
-        const long long p = base + s * step;
-        loadK<K>(a.cost + p * D + gl * K, rc[j]);
-        rp1[j] = __ldg(a.p1 + p);
-        rp2[j] = __ldg(a.p2 + p);
-      };
 #pragma unroll
-      for (int j = 0; j < kPF; ++j)
-        if (s0 + j < s1) fetch(j, s0 + j);
-      for (int b = s0; b < s1; b += kPF) {
-#pragma unroll
-        for (int j = 0; j < kPF; ++j) {
-          const int s = b + j;
-          float(&L)[K] = (j & 1) ? LB : LA;
-          float(&Lq)[K] = (j & 1) ? LA : LB;
-          if (s < s1) {
-            float c[K];
-#pragma unroll
-            for (int i = 0; i < K; ++i) c[i] = rc[j][i];
-            const float P1 = rp1[j], P2 = rp2[j];
-            if (s + kPF < s1) fetch(j, s + kPF);
-            if (s == 0) {
-#pragma unroll
-              for (int i = 0; i < K; ++i) L[i] = c[i];
-              m = group_min<G>(minK<K>(L));
-            } else {
-              m = fstep<G, K>(Lq, L, c, m, P1, P2, gl);
-            }
-            st_put(1 + s - s0, L);
-          }
-        }
-      }
+    for (int j = 0; j < kBwdPF; ++j) {
+      if (j < nr) fetch_r(j, r0 + j);
+      if (j < na) fetch_a(j, a0 + na - 1 - j);
     }
-    __syncwarp();
-    // adjoint through the segment, last pixel first; its inputs through a register ring
-    float rg[kPF][K], rq1[kPF], rq2[kPF];
-    auto fetch_b = [&](int j, int s) {
-      const long long p = base + s * step;
-      loadK<K>(a.gsum + p * D + gl * K, rg[j]);
-      rq1[j] = __ldg(a.p1 + p);
-      rq2[j] = __ldg(a.p2 + p);
+    // one recompute step into slot 1 + i of buffer br (L(r0 + i)); one adjoint step at
+    // s = a0 + na - 1 - i (last pixel first). `at_start`: the step may be the path's first pixel.
+    auto r_step = [&](int jr, int i, int n, auto at_start) {
+      const int s = r0 + i;
+      float(&L)[K] = (jr & 1) ? LB : LA;
+      float(&Lq)[K] = (jr & 1) ? LA : LB;
+      float c[K];
+#pragma unroll
+      for (int t = 0; t < K; ++t) c[t] = rc[jr][t];
+      const float P1 = rp1[jr], P2 = rp2[jr];
+      if (i + kBwdPF < n) fetch_r(jr, s + kBwdPF);
+      if (decltype(at_start)::value && s == 0) {
+#pragma unroll
+        for (int t = 0; t < K; ++t) L[t] = c[t];
+        m = group_min<G>(minK<K>(L));
+      } else {
+        m = fstep<G, K>(Lq, L, c, m, P1, P2, gl);
+      }
+      st_put(br, 1 + i, L);
     };
+    auto a_step = [&](int jr, int i, int n, auto at_start) {
+      const int s = a0 + na - 1 - i;
+      const long long p = base + s * step;
+      float gv[K];
 #pragma unroll
-    for (int j = 0; j < kPF; ++j)
-      if (s1 - 1 - j >= s0) fetch_b(j, s1 - 1 - j);
-    for (int b = s1 - 1; b >= s0; b -= kPF) {
-#pragma unroll
-      for (int jj = 0; jj < kPF; ++jj) {
-        const int s = b - jj;
-        if (s < s0) break;
-        const long long p = base + s * step;
-        float gv[K];
-#pragma unroll
-        for (int j = 0; j < K; ++j) gv[j] = rg[jj][j] + gnext[j];
-        const float P1 = rq1[jj], P2 = rq2[jj];
-        if (s - kPF >= s0) fetch_b(jj, s - kPF);
-        if (ln.live) storeK<K>(gout + p * D + gl * K, gv);
-        if (s == 0) {  // the first pixel of a path adds nothing to the penalties
-          if (ln.live && gl == 0) {
-            gp1[p] = 0.f;
-            gp2[p] = 0.f;
-          }
-          break;
+      for (int t = 0; t < K; ++t) gv[t] = rg[jr][t] + gnext[t];
+      const float P1 = rq1[jr], P2 = rq2[jr];
+      if (i + kBwdPF < n) fetch_a(jr, s - kBwdPF);
+      if (ln.live) storeK<K>(gout + p * D + gl * K, gv);
+      if (decltype(at_start)::value && s == 0) {  // the first pixel of a path adds nothing to the penalties
+        if (ln.live && gl == 0) {
+          gp1[p] = 0.f;
+          gp2[p] = 0.f;
         }
-        // previous state L_q = L(s-1): slot (s - s0) (slot 0 = checkpoint when s == s0)
+      } else {
+        // previous state L_q = L(s-1): slot (s - a0) (slot 0 = checkpoint when s == a0)
         float Lq[K];
-        st_get(s - s0, Lq);
+        st_get(ba, s - a0, Lq);
         // m_q and its (lowest) index
         float mn = Lq[0];
         int mi = gl * K;
@@ -510,6 +500,24 @@ __global__ void __launch_bounds__(kWarps * 32) k_float_bwd(const BwdArgs a) {
           v += j > 0 ? gp1v[j - 1] : (gl > 0 ? from_down : 0.f);
           if (gl * K + j == kq) v += g2 - gall;
           gnext[j] = v;
+        }
+      }
+    };
+    if (kr > 0 && nr == kSeg && na == kSeg) {
+      // both chains over a whole segment, away from the path's first pixel: fully unrolled, so
+      // the two steps of one iteration are one block of independent instructions
+#pragma unroll
+      for (int i = 0; i < kSeg; ++i) {
+        r_step(i % kBwdPF, i, kSeg, std::false_type{});
+        a_step(i % kBwdPF, i, kSeg, std::false_type{});
+      }
+    } else {
+      for (int i0 = 0; i0 < max(nr, na); i0 += kBwdPF) {
+#pragma unroll
+        for (int jr = 0; jr < kBwdPF; ++jr) {
+          const int i = i0 + jr;
+          if (i < nr) r_step(jr, i, nr, std::true_type{});
+          if (i < na) a_step(jr, i, na, std::true_type{});
         }
       }
     }
