@@ -178,7 +178,7 @@ struct Grid4 {
 };
 
 struct Line {
-  int dir, slot, line;
+  int dir, line;
   bool live;  // false for the padding lanes of a warp past the direction's last line
 };
 
@@ -187,7 +187,6 @@ template <int G>
 __device__ __forceinline__ bool locate(const Grid4& q, Line& ln, Geo& g) {
   const int b = blockIdx.x;
   const int slot = (b >= q.first_block[1]) + (b >= q.first_block[2]) + (b >= q.first_block[3]);
-  ln.slot = slot;
   ln.dir = q.order[slot];
   g = q.g[ln.dir];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -716,10 +715,10 @@ int sgm_float_backward(const float* cost, const float* p1, const float* p2, int3
   if (st || (st = check_aligned({cost, sum, ckpt, grad_sum, work, grad_cost}))) return st;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const float inv_t = 1.0f / temperature;
-  return D == 64 ? backward_impl<kBwdLanes64, 64 / kBwdLanes64>(cost, p1, p2, B, H, W, inv_t, sum, ckpt, grad_disp, grad_sum, work, grad_cost,
-                                    grad_p1, grad_p2, s)
-                 : backward_impl<kBwdLanes32, 32 / kBwdLanes32>(cost, p1, p2, B, H, W, inv_t, sum, ckpt, grad_disp, grad_sum, work, grad_cost,
-                                    grad_p1, grad_p2, s);
+  return D == 64 ? backward_impl<kBwdLanes64, 64 / kBwdLanes64>(cost, p1, p2, B, H, W, inv_t, sum, ckpt, grad_disp,
+                                                                grad_sum, work, grad_cost, grad_p1, grad_p2, s)
+                 : backward_impl<kBwdLanes32, 32 / kBwdLanes32>(cost, p1, p2, B, H, W, inv_t, sum, ckpt, grad_disp,
+                                                                grad_sum, work, grad_cost, grad_p1, grad_p2, s);
 }
 
 }  // extern "C"
