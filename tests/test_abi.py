@@ -77,6 +77,24 @@ def test_argument_errors_without_device(engine_lib):
     assert "not initialised" in s.last_error()
 
 
+def test_float_sgm_sizes_and_argument_errors_without_device(engine_lib):
+    """Float-SGM buffer sizes, and argument checks that return before any CUDA call."""
+    from fasterstereocuda_b200.float_sgm import _lib
+    lib = _lib()
+    B, H, W, D = 2, 29, 37, 64
+    assert lib.sgm_float_workspace_elems(B, H, W, D) == 3 * B * H * W * D + 8 * B * H * W
+    seg = 8  # checkpoint interval of the scans
+    per_dir = max(B * H * ((W + seg - 1) // seg), B * W * ((H + seg - 1) // seg)) * D
+    assert lib.sgm_float_checkpoint_elems(B, H, W, D) == 4 * per_dir
+    a16 = 1 << 20  # 16-byte aligned addresses; never dereferenced on these paths
+    st = lib.sgm_float_forward(a16, a16, a16, B, H, W, 48, 1.0, a16, a16, a16, a16, None)
+    assert st == -1 and b"D in {32, 64}" in lib.sgm_last_error(None)
+    st = lib.sgm_float_forward(a16 + 4, a16, a16, B, H, W, D, 1.0, a16, a16, a16, a16, None)
+    assert st == -1 and b"16-byte aligned" in lib.sgm_last_error(None)
+    st = lib.sgm_float_backward(a16, a16, a16, B, H, W, D, 1.0, a16, a16, a16, a16 + 8, a16, a16, a16, a16, None)
+    assert st == -1 and b"16-byte aligned" in lib.sgm_last_error(None)
+
+
 def test_roi_from_disp_map(engine_lib):
     import fasterstereocuda_b200 as fsc
     d = np.full((20, 30), -999999.0, np.float32)
