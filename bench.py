@@ -224,8 +224,8 @@ def workload_config(a, batch):
 # ------------------------------------------------------------------------------------ our arm
 def run_ours(a, rank, world, local_rank):
     import torch
-    import torch.distributed as dist
     import fasterstereocuda_b200 as fsc
+    from fasterstereocuda_b200 import replicas
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
@@ -296,15 +296,10 @@ def run_ours(a, rank, world, local_rank):
         return launches
 
     def barrier():
-        if world > 1:
-            dist.barrier()
+        replicas.barrier(world)
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(x, world, dev)
 
     # parity: first output vs the oracle (outside every timed region)
     bit_exact = None
