@@ -92,6 +92,47 @@ class StereoOption1(C.Structure):
             setattr(self, k, v)
 
 
+class CamParam(C.Structure):
+    """CamParam_T (SgmStereoCuda/sgm_types.h:70-84): principal points, focal length (pixels) and
+    baseline of a rectified pair; depth = baseline * focus / (d + x0_right - x0_left)."""
+    _fields_ = [("x0_left", C.c_double), ("y0_left", C.c_double), ("x0_right", C.c_double),
+                ("y0_right", C.c_double), ("focus", C.c_double), ("baseline", C.c_double)]
+
+    def __init__(self, **kw):
+        super().__init__()
+        for k, v in kw.items():
+            setattr(self, k, v)
+
+
+class EpipolarStereoParam(C.Structure):
+    """FasterStereoCuda::EpipolarStereoParam (FasterStereoCuda/FasterStereoCuda.h:17-27); note the
+    member order differs from CamParam_T (baseline before focus)."""
+    _fields_ = [("x0_left", C.c_double), ("y0_left", C.c_double), ("x0_right", C.c_double),
+                ("y0_right", C.c_double), ("baseline", C.c_double), ("focus", C.c_double)]
+
+    def __init__(self, **kw):
+        super().__init__()
+        for k, v in kw.items():
+            setattr(self, k, v)
+
+
+class StereoOption2(C.Structure):
+    """FasterStereoCuda::StereoOption2 (FasterStereoCuda/FasterStereoCuda.h:45-69): the search range
+    given as a depth range seen by the camera `epi`."""
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("min_depth", C.c_float), ("max_depth", C.c_float),
+                ("num_layers", C.c_int32), ("do_lr_check", C.c_bool), ("do_rm_peaks", C.c_bool),
+                ("do_smooth", C.c_bool), ("epi", EpipolarStereoParam)]
+
+    def __init__(self, **kw):
+        super().__init__()
+        self.num_layers = 1
+        self.do_lr_check = True
+        self.do_rm_peaks = True
+        self.do_smooth = False
+        for k, v in kw.items():
+            setattr(self, k, v)
+
+
 class LevelOverride(C.Structure):
     """Census type and penalties applied to every pyramid level (sgm_level_override_t)."""
     _fields_ = [("cs_type", C.c_int32), ("p1", C.c_int32), ("p2", C.c_int32)]
@@ -148,6 +189,10 @@ def load_library(path: Optional[os.PathLike] = None):
         "sgm_last_error": (C.c_char_p, [vp]), "sgm_kernel_launches": (i64, [vp]),
         "sgm_pyr_create": (i32, [C.POINTER(vp)]), "sgm_pyr_destroy": (i32, [vp]),
         "sgm_pyr_init": (i32, [vp, C.POINTER(StereoOption1), C.POINTER(LevelOverride), C.POINTER(ExtOptions)]),
+        "sgm_pyr_init2": (i32, [vp, C.POINTER(StereoOption2), C.POINTER(LevelOverride), C.POINTER(ExtOptions)]),
+        "sgm_pyr_match2": (i32, [vp, vp, vp, vp]),
+        "sgm_init2": (i32, [vp, i32, i32, i32, i32, C.POINTER(CuSGMOption), C.POINTER(CamParam), i32]),
+        "sgm_match2": (i32, [vp, vp, vp, vp, vp, C.POINTER(StereoROI), C.POINTER(StereoROI)]),
         "sgm_pyr_match": (i32, [vp, vp, vp, vp]), "sgm_pyr_match_device": (i32, [vp, vp, vp, vp, vp]),
         "sgm_pyr_release": (i32, [vp]),
         "sgm_pyr_level_info": (i32, [vp, i32, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)]),
@@ -247,6 +292,28 @@ class StereoCuda:
             self.width, self.height = width, height
         return self.status == 0
 
+    def Init2(self, width: int, height: int, min_disparity: int, disp_range: int, sgm_option: CuSGMOption,
+              cam_param: CamParam, print_log: bool = False) -> bool:
+        """StereoCuda::Init2 (SgmStereoCuda/StereoCuda.h:57): Init plus the camera used by Match2."""
+        self.status = self._lib.sgm_init2(self._h, width, height, min_disparity, disp_range, C.byref(sgm_option),
+                                          C.byref(cam_param), int(print_log))
+        if self.status == 0:
+            self.width, self.height = width, height
+        return self.status == 0
+
+    def Match2(self, img_left, img_right, depth_left, init_disp_left=None,
+               ste_roi_left: Optional[StereoROI] = None, ste_roi_right: Optional[StereoROI] = None) -> bool:
+        """StereoCuda::Match2 (SgmStereoCuda/StereoCuda.h:69): the left disparity map of Match turned
+        into depth (INVALID kept), written into the host array depth_left."""
+        for a, t, n in ((img_left, np.uint8, "img_left"), (img_right, np.uint8, "img_right"),
+                        (depth_left, np.float32, "depth_left"), (init_disp_left, np.int16, "init_disp_left")):
+            self._check_host(a, t, n)
+        self.status = self._lib.sgm_match2(
+            self._h, _ptr(img_left), _ptr(img_right), _ptr(depth_left), _ptr(init_disp_left),
+            C.byref(ste_roi_left) if ste_roi_left is not None else None,
+            C.byref(ste_roi_right) if ste_roi_right is not None else None)
+        return self.status == 0
+
     def _check_host(self, a, dtype, name):
         if a is None:
             return
@@ -343,6 +410,26 @@ class FasterStereoCuda:
                                              C.byref(ext) if ext is not None else None)
         if self.status == 0:
             self.width, self.height = option.width, option.height
+        return self.status == 0
+
+    def Init2(self, option: StereoOption2, override: Optional[LevelOverride] = None,
+              ext: Optional[ExtOptions] = None) -> bool:
+        """FasterStereoCuda::Init2 (FasterStereoCuda/FasterStereoCuda.h:102): the coarsest level's
+        disparity range from the depth range and the camera scaled to that level."""
+        self.status = self._lib.sgm_pyr_init2(self._h, C.byref(option),
+                                              C.byref(override) if override is not None else None,
+                                              C.byref(ext) if ext is not None else None)
+        if self.status == 0:
+            self.width, self.height = option.width, option.height
+        return self.status == 0
+
+    def Match2(self, bytes_left, bytes_right, depth_data) -> bool:
+        """FasterStereoCuda::Match2 (FasterStereoCuda/FasterStereoCuda.h:123): depth of the finest level."""
+        n = self.width * self.height
+        for a, t in ((bytes_left, np.uint8), (bytes_right, np.uint8), (depth_data, np.float32)):
+            if not isinstance(a, np.ndarray) or a.dtype != t or a.size != n:
+                raise ValueError("expected host arrays of width*height elements")
+        self.status = self._lib.sgm_pyr_match2(self._h, _ptr(bytes_left), _ptr(bytes_right), _ptr(depth_data))
         return self.status == 0
 
     def set_tuning(self, tuning: Tuning, level: int = -1) -> bool:

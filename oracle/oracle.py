@@ -230,3 +230,43 @@ def set_threads(n: int) -> None:
 
 def max_threads() -> int:
     return lib().orc_max_threads()
+
+
+def depth_from_disp(disp: np.ndarray, x0_left: float, x0_right: float, focus: float,
+                    baseline: float) -> np.ndarray:
+    """Depth of a disparity map, as StereoCudaImpl::Match2 (SgmStereoCuda/StereoCudaImpl.cpp:548-583)
+    computes it with Kernel_ComputeDepth (SgmStereoCuda/cusgm_util.cu:7-34): in double,
+    depth = (baseline * focus) / ((double)d + (x0_right - x0_left)), rounded to float; INVALID stays
+    INVALID."""
+    d = np.ascontiguousarray(disp, np.float32)
+    f1 = float(baseline) * float(focus)
+    f2 = float(x0_right) - float(x0_left)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        depth = (f1 / (d.astype(np.float64) + f2)).astype(np.float32)
+    return np.where(d == INVALID_FLOAT, INVALID_FLOAT, depth)
+
+
+def pyr_init2_coarsest(width: int, num_layers: int, min_depth: float, max_depth: float, x0_left: float,
+                       x0_right: float, focus: float, baseline: float) -> tuple[int, int]:
+    """(min disparity, disparity range) of the coarsest pyramid level that HierSgmCudaImpl::Init2
+    (FasterStereoCuda/FasterStereoCuda.cpp:370-395) derives from a depth range, with the camera
+    scaled to that level by CamParam_T::Scale (SgmStereoCuda/sgm_types.h:76-83); the range is the
+    next power of two >= 64 above the span, halved once if above twice the full width, and a minimum
+    at or past the width is pulled back (not below -width). min_depth/max_depth are floats there."""
+    layers = max(1, int(num_layers))
+    s = 2 ** (layers - 1)
+    x0l, x0r, f = x0_left / s, x0_right / s, focus / s
+    lo = baseline * f / float(np.float32(max_depth)) - x0r + x0l
+    hi = baseline * f / float(np.float32(min_depth)) - x0r + x0l
+    span = hi - lo
+    k = 6
+    while 2.0 ** k < span:
+        k += 1
+    rng = 2.0 ** k
+    if rng > 2 * width:
+        rng /= 2
+    if lo >= width:
+        lo = width - rng
+        if lo < -width:
+            lo = -width
+    return int(np.floor(lo)), int(rng)
