@@ -238,7 +238,7 @@ SGM_API int sgm_batch_bucket(sgm_batch_t b, int32_t index, sgm_batch_bucket_t* b
  * S = ((L_0 + L_1) + L_2) + L_3 over the paths (top->bottom, left->right, bottom->top,
  * right->left), disp = sum_d d*softmax(-S/T). Device pointers: cost [B][H][W][D],
  * p1/p2/disp [B][H][W], sum [B][H][W][D] (S, kept for the backward pass), ckpt of
- * sgm_float_checkpoint_elems floats (path states every 16 pixels, kept for the backward pass),
+ * sgm_float_checkpoint_elems floats (path states every 8 pixels, kept for the backward pass),
  * work of sgm_float_workspace_elems floats (scratch, free after the call's work completes on
  * `stream`). D = 32 or 64; cost, sum, ckpt and work 16-byte aligned. */
 SGM_API size_t sgm_float_checkpoint_elems(int32_t B, int32_t H, int32_t W, int32_t D);
@@ -248,7 +248,7 @@ SGM_API int sgm_float_forward(const float* cost, const float* p1, const float* p
                               void* stream);
 /* No counterpart in the reference. Gradients of sum(grad_disp * disp) with respect to cost, p1
  * and p2 (written, not accumulated); grad_sum [B][H][W][D] and work (sgm_float_workspace_elems
- * floats) are scratch. Each path's states are recomputed from the checkpoints, 16 pixels at a
+ * floats) are scratch. Each path's states are recomputed from the checkpoints, 8 pixels at a
  * time. grad_sum and grad_cost 16-byte aligned. */
 SGM_API int sgm_float_backward(const float* cost, const float* p1, const float* p2, int32_t B, int32_t H, int32_t W,
                                int32_t D, float temperature, const float* sum, const float* ckpt,
