@@ -28,6 +28,7 @@
 // 2 bottom->top, 3 right->left.
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdint>
 #include <string>
 #include <type_traits>
@@ -567,9 +568,13 @@ int check(const char* what) {
   return SGM_OK;
 }
 
-int validate(int B, int H, int W, int D) {
+int validate(int B, int H, int W, int D, float temperature) {
   if (B <= 0 || H <= 0 || W <= 0 || (D != 32 && D != 64)) {
     sgm_set_process_error("float SGM: B, H, W > 0 and D in {32, 64} required");
+    return SGM_ERR_ARG;
+  }
+  if (!(temperature > 0.0f) || !std::isfinite(1.0f / temperature)) {
+    sgm_set_process_error("float SGM: temperature must be > 0 with a finite reciprocal");
     return SGM_ERR_ARG;
   }
   if ((size_t)B * H * W * D > ((size_t)1 << 40)) {
@@ -700,7 +705,7 @@ size_t sgm_float_workspace_elems(int32_t B, int32_t H, int32_t W, int32_t D) {
 
 int sgm_float_forward(const float* cost, const float* p1, const float* p2, int32_t B, int32_t H, int32_t W,
                       int32_t D, float temperature, float* sum, float* ckpt, float* work, float* disp, void* stream) {
-  int st = validate(B, H, W, D);
+  int st = validate(B, H, W, D, temperature);
   if (st || (st = check_aligned({cost, sum, ckpt, work}))) return st;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const float inv_t = 1.0f / temperature;
@@ -711,7 +716,7 @@ int sgm_float_forward(const float* cost, const float* p1, const float* p2, int32
 int sgm_float_backward(const float* cost, const float* p1, const float* p2, int32_t B, int32_t H, int32_t W, int32_t D,
                        float temperature, const float* sum, const float* ckpt, const float* grad_disp,
                        float* grad_sum, float* work, float* grad_cost, float* grad_p1, float* grad_p2, void* stream) {
-  int st = validate(B, H, W, D);
+  int st = validate(B, H, W, D, temperature);
   if (st || (st = check_aligned({cost, sum, ckpt, grad_sum, work, grad_cost}))) return st;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const float inv_t = 1.0f / temperature;

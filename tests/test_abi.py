@@ -93,6 +93,9 @@ def test_float_sgm_sizes_and_argument_errors_without_device(engine_lib):
     assert st == -1 and b"16-byte aligned" in lib.sgm_last_error(None)
     st = lib.sgm_float_backward(a16, a16, a16, B, H, W, D, 1.0, a16, a16, a16, a16 + 8, a16, a16, a16, a16, None)
     assert st == -1 and b"16-byte aligned" in lib.sgm_last_error(None)
+    for t in (0.0, -1.0, float("nan"), 1e-40):
+        st = lib.sgm_float_forward(a16, a16, a16, B, H, W, D, t, a16, a16, a16, a16, None)
+        assert st == -1 and b"temperature" in lib.sgm_last_error(None), t
 
 
 def test_roi_from_disp_map(engine_lib):
