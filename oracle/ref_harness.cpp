@@ -192,6 +192,70 @@ int ref_match_dump(const ref_case_t* c, const uint8_t* left, const uint8_t* righ
   return 0;
 }
 
+// StereoCudaImpl::Init2 / Match2 (StereoCudaImpl.cpp:263-278, :548-583): depth of the left view
+// with the case's options. cam = {x0_left, y0_left, x0_right, y0_right, focus, baseline}.
+// Same case restrictions and row-padding check as ref_match_dump.
+int ref_match2(const ref_case_t* c, const double* cam, const uint8_t* left, const uint8_t* right, float* depth) {
+  if (check_case(c, false)) return -1;
+  const int W = c->width, H = c->height;
+  std::vector<uint8_t> L(left, left + (size_t)W * H), R(right, right + (size_t)W * H);
+  CamParam_T p{};
+  p.x0_left = cam[0];
+  p.y0_left = cam[1];
+  p.x0_right = cam[2];
+  p.y0_right = cam[3];
+  p.focus = cam[4];
+  p.baseline = cam[5];
+  StereoCudaImpl impl;
+  const CuSGMOption o = make_option(c, c->do_lr_check != 0, c->do_median != 0, c->do_remove_peaks != 0, c->morphology);
+  if (!impl.Init2(W, H, c->min_disp, c->disp_range, o, p, false)) {
+    g_msg = "reference Init2 failed";
+    return -2;
+  }
+  if (!padding_ok(impl.aggregator_->dp_psize_, (size_t)W * sizeof(float), 4 * sizeof(float))) {
+    g_msg = "pitch padding too small for the reference's row overrun";
+    impl.Release();
+    return -3;
+  }
+  const bool ok = impl.Match2(L.data(), R.data(), depth);
+  if (cudaDeviceSynchronize() != cudaSuccess || !ok) {
+    g_msg = "reference Match2 failed";
+    impl.Release();
+    return -4;
+  }
+  impl.Release();
+  return 0;
+}
+
+// FasterStereoCuda::Init2 / Match2 through the reference's public API (FasterStereoCuda.cpp:297-406,
+// :531-635): depth of the finest level for a depth range. epi = {x0_left, y0_left, x0_right,
+// y0_right, baseline, focus}. Never released, like ref_pyr_match. Only ranges whose levels all
+// run D = 32 or 64 are safe to run (the D = 128 / 256 kernels index shared memory out of range):
+// the caller checks the coarsest range first.
+int ref_pyr_match2(int width, int height, float min_depth, float max_depth, int layers, int lr, int peaks,
+                   const double* epi, const uint8_t* left, const uint8_t* right, float* depth) {
+  FasterStereoCuda& s = *new FasterStereoCuda;  // leaked on purpose, see ref_pyr_match
+  FasterStereoCuda::StereoOption2 o;
+  o.width = width;
+  o.height = height;
+  o.min_depth = min_depth;
+  o.max_depth = max_depth;
+  o.num_layers = layers;
+  o.do_lr_check = lr != 0;
+  o.do_rm_peaks = peaks != 0;
+  o.do_smooth = false;
+  o.epi.x0_left = epi[0];
+  o.epi.y0_left = epi[1];
+  o.epi.x0_right = epi[2];
+  o.epi.y0_right = epi[3];
+  o.epi.baseline = epi[4];
+  o.epi.focus = epi[5];
+  if (!s.Init2(o)) { g_msg = "FasterStereoCuda::Init2 failed"; return -2; }
+  const bool ok = s.Match2(left, right, depth);
+  if (!ok || cudaDeviceSynchronize() != cudaSuccess) { g_msg = "FasterStereoCuda::Match2 failed"; return -4; }
+  return 0;
+}
+
 // FasterStereoCuda::Match through the reference's public API (per-level options as the
 // reference hard-codes them). Returns 0 on success.
 // The matcher is deliberately never released: HierSgmCudaImpl::Release (FasterStereoCuda.cpp:

@@ -10,7 +10,8 @@ oracle/build_ref.sh into oracle/_ref/libsgmref.so:
 
   python tests/golden/make_golden.py refdump --out DIR
       on a CUDA machine: the reference's stage buffers (census, cost, four path volumes,
-      WTA, left-right check, filtered output) for the cases below -> DIR/<case>.npz
+      WTA, left-right check, filtered output) for the cases below, and its depth maps
+      (Init2 / Match2 of both classes) -> DIR/<case>.npz
 
   python tests/golden/make_golden.py finalize DIR
       compares the dumps with the oracle, prints the agreement, and writes the compact
@@ -63,6 +64,10 @@ def ref_lib():
     lib.ref_time_match.restype = C.c_double
     lib.ref_pyr_levels.argtypes = [C.c_int] * 7 + [vp, vp, vp, vp]
     lib.ref_pyr_levels.restype = C.c_int
+    lib.ref_match2.argtypes = [C.POINTER(RefCase), vp, vp, vp, vp]
+    lib.ref_match2.restype = C.c_int
+    lib.ref_pyr_match2.argtypes = [C.c_int, C.c_int, C.c_float, C.c_float, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp]
+    lib.ref_pyr_match2.restype = C.c_int
     return lib
 
 
@@ -118,6 +123,13 @@ def cases():
 # name: (seed, width, height, min_disp, max_disp, layers, lr check, small-region removal)
 PYR_CASES = {"pyr_kitti": (17, 1242, 375, 0, 64, 3, 1, 1), "pyr_cone": (16, 450, 375, 0, 64, 2, 1, 1),
              "pyr_kitti_nolr": (18, 1242, 375, 0, 64, 3, 0, 1)}
+
+# Depth output (Init2 / Match2). Camera: x0_left, y0_left, x0_right, y0_right, focus, baseline.
+CAM = (600.0, 180.0, 610.0, 180.0, 720.0, 540.0)
+# single-level cases (from cases()) whose stages have no thread races, matched to depth
+DEPTH_CASES = ("peaks_only", "dil_only")
+# name: (seed, width, height, min_depth, max_depth, layers, lr check, small-region removal)
+DEPTH_PYR_CASES = {"depthpyr_kitti": (43, 1242, 375, 5000.0, 60000.0, 3, 1, 1)}
 
 
 # ----------------------------------------------------------------------------- host ops
@@ -210,6 +222,35 @@ def refdump(out_dir: Path, only=None):
             np.savez_compressed(out_dir / f"levels_{name}.npz", left=L, right=R, disp_levels=dl, init_levels=il,
                                 case=np.array(json.dumps(dict(width=w, height=h, min_disp=dmin, max_disp=dmax,
                                                               num_layers=layers, lr=lr, peaks=pk))))
+    cam = np.array(CAM, np.float64)
+    all_cases = cases()
+    for base_name in DEPTH_CASES:
+        name = "depth_" + base_name
+        if only and name not in only:
+            continue
+        f, L, R, _, _ = all_cases[base_name]
+        depth = np.zeros((f["height"], f["width"]), np.float32)
+        rc = lib.ref_match2(C.byref(RefCase(**f)), _p(cam), _p(L), _p(R), _p(depth))
+        print(name, "rc", rc, lib.ref_last_message().decode(), flush=True)
+        if rc == 0:
+            np.savez_compressed(out_dir / f"{name}.npz", left=L, right=R, depth=depth, cam=cam,
+                                case=np.array(json.dumps(f)))
+    epi = np.array([CAM[0], CAM[1], CAM[2], CAM[3], CAM[5], CAM[4]], np.float64)  # baseline before focus
+    for name, (seed, w, h, zmin, zmax, layers, lr, pk) in DEPTH_PYR_CASES.items():
+        if only and name not in only:
+            continue
+        m0, d0 = O.pyr_init2_coarsest(w, layers, zmin, zmax, CAM[0], CAM[2], CAM[4], CAM[5])
+        if d0 != 64:  # the reference's 128- and 256-disparity kernels index shared memory out of range
+            print(name, "skipped: coarsest range", d0, flush=True)
+            continue
+        L, R, _ = scenes.kitti_like(seed, w, h)
+        depth = np.zeros((h, w), np.float32)
+        rc = lib.ref_pyr_match2(w, h, zmin, zmax, layers, lr, pk, _p(epi), _p(L), _p(R), _p(depth))
+        print(name, "rc", rc, lib.ref_last_message().decode(), flush=True)
+        if rc == 0:
+            np.savez_compressed(out_dir / f"{name}.npz", left=L, right=R, depth=depth, cam=cam,
+                                case=np.array(json.dumps(dict(width=w, height=h, min_depth=zmin, max_depth=zmax,
+                                                              num_layers=layers, lr=lr, peaks=pk))))
     (out_dir / "meta.json").write_text(json.dumps(meta))
     print("meta", meta)
 
@@ -288,6 +329,37 @@ def _levels_report(z, case, meta):
     return out
 
 
+def oracle_depth(z, case, peaks_strips):
+    """The oracle's depth map for a depth dump (single level or pyramid), with the rows the
+    reference writes."""
+    cam = z["cam"]
+    if "num_layers" in case:  # pyramid: the coarsest range from the depth range, as Init2 derives it
+        layers = case["num_layers"]
+        m0, d0 = O.pyr_init2_coarsest(case["width"], layers, case["min_depth"], case["max_depth"], cam[0], cam[2],
+                                      cam[4], cam[5])
+        s = 2 ** (layers - 1)
+        pc = O.PyrConfig(width=case["width"], height=case["height"], min_disp=m0 * s, max_disp=(m0 + d0) * s,
+                         num_layers=layers, override_enable=0, peaks_strips=peaks_strips,
+                         do_lr_check=case["lr"], do_rm_peaks=case["peaks"])
+        d = O.pyr_match(pc, z["left"], z["right"])
+    else:
+        cfg = O.Config(width=case["width"], height=case["height"], min_disp=case["min_disp"],
+                       disp_range=case["disp_range"], cs_type=case["cs_type"], p1=case["p1"], p2=case["p2"],
+                       uniqueness=case["uniqueness"], do_lr_check=case["do_lr_check"],
+                       lr_threshold=case["lr_threshold"], do_median=case["do_median"],
+                       morphology_dilation=int(case["morphology"] == 2), do_remove_peaks=case["do_remove_peaks"],
+                       peaks_ratio=case["peaks_ratio"], peaks_strips=peaks_strips, tie_rule=4, init_tie_rule=4)
+        d = O.match(cfg, z["left"], z["right"])["disp"]
+    rows = np.zeros(d.shape, bool)
+    rows[:d.shape[0] - 1 if d.shape[0] % 2 else d.shape[0]] = True  # the reference never writes the last odd row
+    return O.depth_from_disp(d, cam[0], cam[2], cam[4], cam[5]), rows
+
+
+def depth_report(z, case, meta):
+    want, rows = oracle_depth(z, case, meta["peaks_strips"])
+    return {"depth_equal": float((want.view(np.uint32) == z["depth"].view(np.uint32))[rows].mean())}
+
+
 def finalize(dump_dir: Path, write: bool = True):
     meta = json.loads((dump_dir / "meta.json").read_text())
     report = {}
@@ -299,6 +371,12 @@ def finalize(dump_dir: Path, write: bool = True):
             report[name] = _levels_report(z, case, meta)
             if write:
                 np.savez_compressed(GOLDEN / f"ref_{name}.npz", **z, peaks_strips=np.int32(meta["peaks_strips"]))
+            continue
+        if name.startswith("depth"):
+            report[name] = depth_report(z, case, meta)
+            if write:
+                np.savez_compressed(GOLDEN / f"ref_{name}.npz", left=z["left"], right=z["right"], depth=z["depth"],
+                                    cam=z["cam"], case=z["case"], peaks_strips=np.int32(meta["peaks_strips"]))
             continue
         if name.startswith("pyr_"):
             pc = O.PyrConfig(width=case["width"], height=case["height"], min_disp=case["min_disp"],

@@ -16,7 +16,9 @@ import numpy as np
 import pytest
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
-CASES = sorted(p.stem[4:] for p in GOLDEN.glob("ref_*.npz") if not p.stem.startswith(("ref_pyr", "ref_levels")))
+CASES = sorted(p.stem[4:] for p in GOLDEN.glob("ref_*.npz")
+               if not p.stem.startswith(("ref_pyr", "ref_levels", "ref_depth")))
+DEPTH = sorted(p.stem[4:] for p in GOLDEN.glob("ref_depth*.npz"))
 PYR = sorted(p.stem[4:] for p in GOLDEN.glob("ref_pyr*.npz"))
 LEVELS = sorted(p.stem[4:] for p in GOLDEN.glob("ref_levels_*.npz"))
 INV = np.float32(-999999.0)
@@ -200,3 +202,18 @@ def test_pyramid_levels_against_reference(oracle_mod, name):
             ioff += wn * hn
             assert np.array_equal(O.init_next_level(ref, wn, hn), ref_init), n
             init = ref_init
+
+
+@pytest.mark.parametrize("name", DEPTH)
+def test_depth_against_reference(oracle_mod, name):
+    """Depth maps of the reference's Init2 / Match2 (both classes): the oracle's disparity turned
+    into depth. Exact on the single-level cases without racy stages; the pyramid inherits the
+    median races of its disparities."""
+    from tests.golden.make_golden import oracle_depth
+    z, case = load(name)
+    want, rows = oracle_depth(z, case, int(z["peaks_strips"]))
+    eq = (want.view(np.uint32) == z["depth"].view(np.uint32))[rows].mean()
+    if "num_layers" in case:
+        assert eq > 0.9, eq
+    else:
+        assert eq == 1.0, eq
