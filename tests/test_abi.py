@@ -116,3 +116,58 @@ def test_cxx_classes_export_the_reference_symbols(engine_lib):
     have = {l.split()[-1] for l in out.stdout.splitlines() if "10StereoCuda" in l or "16FasterStereoCuda" in l}
     assert len(want) == 28
     assert want == have, (sorted(want - have), sorted(have - want))
+
+
+C_CALLER = r"""
+#include <stdio.h>
+#include "sgm_b200.h"
+int main(void) {
+  float disp[6] = {-999999.0f, 2.0f, 3.0f, -999999.0f, 4.0f, -999999.0f};
+  sgm_roi_t roi;
+  sgm_handle_t h;
+  sgm_option_t o = {10, 150, 0, 1, 4, true, true, 1.0f, 0.95f, true, false, 0.0f, 0, 0};
+  int st;
+  sgm_roi_from_disp_map(disp, 3, 2, &roi);
+  if (sgm_create(&h) != SGM_OK) return 1;
+  st = sgm_init(h, 0, 10, 0, 64, &o, 0);
+  printf("%g %d %d %d %d %d\n", sgm_invalid_float(), roi.x, roi.y, roi.w, roi.h, st);
+  sgm_destroy(h);
+  return 0;
+}
+"""
+
+CXX_CALLER = r"""
+#include <cstdio>
+#include "FasterStereoCuda.h"
+#include "StereoCuda.h"
+int main() {
+  FasterStereoCuda stereo;  // the reference console's use
+  FasterStereoCuda::StereoOption1 opt;
+  opt.width = 0; opt.height = 375; opt.max_disp = 64; opt.num_layers = 3;
+  const bool ok = stereo.Init(opt);
+  StereoROI_T roi;
+  float disp[4] = {StereoCuda::get_invad_float(), 1.0f, 2.0f, StereoCuda::get_invad_float()};
+  StereoCuda::GetRoiFromDispMap(disp, 2, 2, roi);
+  std::printf("%d %g %d %d %d %d %d\n", ok, StereoCuda::get_invad_float(), StereoCuda::get_level_range(),
+              roi.x, roi.y, roi.w, roi.h);
+  return 0;
+}
+"""
+
+
+@pytest.mark.parametrize("lang", ["c", "c++"])
+def test_c_and_cxx_callers_build_against_the_headers(engine_lib, tmp_path, lang):
+    """A C caller of include/sgm_b200.h and a C++ caller of the reference's classes compile with
+    warnings as errors, link against the library and run the calls that need no GPU."""
+    libdir = ROOT / "fasterstereocuda_b200" / "_lib"
+    src = tmp_path / ("caller.c" if lang == "c" else "caller.cpp")
+    src.write_text(C_CALLER if lang == "c" else CXX_CALLER)
+    exe = tmp_path / "caller"
+    cc = ["gcc", "-std=c99"] if lang == "c" else ["g++", "-std=c++17"]
+    subprocess.run(cc + ["-Wall", "-Werror", "-I", str(ROOT / "include"), str(src), "-L", str(libdir), "-lsgmb200",
+                         f"-Wl,-rpath,{libdir}", "-o", str(exe)], check=True, capture_output=True, text=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
+    if lang == "c":
+        assert out == ["-999999", "1", "0", "2", "2", "-1"]   # ROI of the valid pixels; w = 0 rejected
+    else:
+        assert out == ["0", "-999999", "32", "0", "0", "2", "2"]
