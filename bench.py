@@ -201,8 +201,58 @@ def run_reference(a, rank, world):
             "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": cores, "kind": "port",
                              "sample": f"{sample} pairs per step, oracle/ C restatement, OpenMP {cores} threads"},
             "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if not a.no_extras:
+        line["ref_cuda_build"] = ref_cuda_build(a)
     print(json.dumps(line), flush=True)
     return 0
+
+
+def ref_cuda_build(a):
+    """The reference's own CUDA build (its sources compiled for sm_100a into oracle/_ref/ by
+    oracle/build_ref.sh) timed through its public API with host buffers in and out, as its console
+    measures itself: StereoCuda::Match on the plain workload (census 9x7, P1 10, P2 150, LR check,
+    median) and FasterStereoCuda::Match on the 3-level pyramid with the reference's own per-level
+    parameters, each with 1 host thread and with --streams host threads (one instance each, the
+    concurrency the engine's throughput figure uses). Only 64- and 32-disparity levels run: the
+    reference's 128-disparity row kernel indexes shared memory past its allocation."""
+    import ctypes as C
+    lib_path = ROOT / "oracle" / "_ref" / "libsgmref.so"
+    if not lib_path.exists():
+        return {"unavailable": "oracle/_ref/libsgmref.so not built (needs the reference sources)"}
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return {"unavailable": "no CUDA device"}
+        from tests.golden.make_golden import RefCase
+        lib = C.CDLL(str(lib_path))
+        vp = C.c_void_p
+        lib.ref_throughput_match.argtypes = [C.POINTER(RefCase), vp, vp, C.c_int, C.c_int, C.c_int]
+        lib.ref_throughput_match.restype = C.c_double
+        lib.ref_throughput_pyr.argtypes = [C.c_int] * 7 + [vp, vp, C.c_int, C.c_int, C.c_int]
+        lib.ref_throughput_pyr.restype = C.c_double
+        L, R = make_pool(1)[0]
+        plain = RefCase(width=W_, height=H_, min_disp=0, disp_range=DMAX, cs_type=1, p1=10, p2=150, uniqueness=0.95,
+                        do_lr_check=1, lr_threshold=1.0, do_median=1, morphology=0, do_remove_peaks=0,
+                        peaks_ratio=0.0, post_filter=0)
+        T = max(1, a.streams)
+        out = {"api": "StereoCuda::Match / FasterStereoCuda::Match, host buffers, one instance per host thread",
+               "threads": [1, T]}
+        res = {}
+        for th, n in ((1, 200), (T, max(4, 400 // T))):
+            res[f"plain_{th}"] = lib.ref_throughput_match(C.byref(plain), L.ctypes.data, R.ctypes.data, 3, n, th)
+        for th, n in ((1, 150), (T, max(4, 300 // T))):
+            res[f"pyramid_{th}"] = lib.ref_throughput_pyr(W_, H_, 0, DMAX, LAYERS, 1, 1, L.ctypes.data, R.ctypes.data,
+                                                          3, n, th)
+        out["plain_1242x375x64_census9x7_p10_p150_lr_median_pairs_per_s"] = {str(k.split("_")[1]): v
+                                                                             for k, v in res.items()
+                                                                             if k.startswith("plain")}
+        out["pyramid_1242x375_3layers_reference_params_pairs_per_s"] = {str(k.split("_")[1]): v
+                                                                        for k, v in res.items()
+                                                                        if k.startswith("pyramid")}
+        out["pyramid_params"] = "census 5x5, P1 8, P2 32 per level (SetSgmParameters, FasterStereoCuda.cpp:169-199)"
+        return out
+    except Exception as e:  # the CPU arm's line stands without it
+        return {"unavailable": f"{type(e).__name__}: {e}"}
 
 
 def metric_name(workload):
@@ -357,15 +407,47 @@ def run_ours(a, rank, world, local_rank):
     ms = max_over_ranks(t0.elapsed_time(t1))
     value = a.steps * a.batch * world / (ms / 1e3)
 
-    # per-kernel CUDA events over a serialised pass (one matcher, one stream, one pair at a time),
-    # so each launch's duration is its own: the roofline of the dominant kernel comes from here
+    # single-pair latency: one matcher alone on the GPU, one pair at a time, CUDA events around
+    # each pair. Few scanlines in flight favour more lanes per scanline, so the lane split is tuned
+    # for this case on its own (every split gives the same disparities).
+    lat_m = make_matcher()
+
+    def pair_ms(n):
+        ts = []
+        for j in range(n):
+            i = j % len(dL)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(main)
+            run_one(lat_m, dL[i], dR[i], outs[0], main.cuda_stream)
+            e1.record(main)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return statistics.median(ts)
+    lat_tuning = a.tuning or None
+    if not a.tuning:
+        cands = {}
+        for lanes in ((8, 8), (8, 4), (4, 4), (2, 2)):
+            apply_tuning((0, 0, 0, 0, 0) + lanes, ms=[lat_m])
+            pair_ms(3)
+            cands[lanes] = pair_ms(8)
+        best_lanes = min(cands, key=cands.get)
+        apply_tuning((0, 0, 0, 0, 0) + best_lanes, ms=[lat_m])
+        lat_tuning = "row_lanes,col_lanes = %d,%d" % best_lanes
+    pair_ms(3)
+    latency = {"ms_per_pair": pair_ms(20), "tuning": lat_tuning,
+               "how": "one matcher, one stream, one pair at a time, inputs in HBM, CUDA events around each "
+                      "match_device call (median of 20)"}
+
+    # per-kernel CUDA events over a serialised pass (the latency matcher, one stream, one pair at a
+    # time), so each launch's duration is its own: the roofline of the dominant kernel comes from here
     fsc.profile_enable(True)
     for j in range(a.profile_pairs):
         i = j % len(dL)
-        run_one(matchers[0], dL[i], dR[i], outs[0], main.cuda_stream)
+        run_one(lat_m, dL[i], dR[i], outs[0], main.cuda_stream)
     torch.cuda.synchronize()
     prof = fsc.profile_read()
     fsc.profile_enable(False)
+    latency["kernel_ms_per_pair"] = sum(v["ms"] for v in prof.values()) / max(1, a.profile_pairs)
 
     # e2e: the host-buffer API (synchronous Match, like the reference's), pinned host memory, one
     # host thread per matcher (the reference API is per object; ctypes releases the GIL)
@@ -430,7 +512,8 @@ def run_ours(a, rank, world, local_rank):
                     "traffic_source": "ncu DRAM bytes per voxel of this kernel x voxels per launch",
                     "avg_launch_us": total_ms / prof[dom]["launches"] * 1e3,
                     "alg_bytes_per_launch": per_call_bytes.get(dom, 0) / max(1, prof[dom]["launches"] // calls),
-                    "timing": f"CUDA events around each launch, serialised pass of {calls} pairs on one stream"}
+                    "timing": f"CUDA events around each launch, serialised pass of {calls} pairs on one stream "
+                              f"(the single-pair latency matcher)"}
     if roofline is not None:
         # the path is integer-ALU bound: algorithmic int ops per view 34*W*H*D + 248*W*H (xor+popc,
         # 7 per path step x 4 paths, 3 adds, 1 min per voxel; census per pixel), over all levels,
@@ -453,7 +536,8 @@ def run_ours(a, rank, world, local_rank):
     extras = None
     if not a.no_extras:
         cpu = cpu_baseline(a, pool)
-        extras = extra_batches(pool)
+        extras = {"equal_concurrency": equal_concurrency(pool[:8], max(1, a.streams))}
+        extras.update(extra_batches(pool))
         extras["float_sgm"] = extra_float_sgm()
         extras["large_pyramid"] = extra_large_pyramid()
     clocks = clk_summary
@@ -468,13 +552,66 @@ def run_ours(a, rank, world, local_rank):
                     "h2d_bytes_per_step": a.batch * 2 * W_ * H_, "d2h_bytes_per_step": a.batch * 4 * W_ * H_,
                     "api": ("FasterStereoCuda.Match" if a.workload == "pyramid" else "StereoCuda.Match")
                     + f" (host buffers, synchronous), {E} host threads with one matcher each"},
-            "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
+            "latency": latency, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
+            "gpu_launches": launches,
             "bit_exact_vs_oracle": bit_exact, "kernels": kernels, "extras": extras}
     print(json.dumps(line), flush=True)
     return 0
 
 
 # ------------------------------------------------------------------------------------ extras
+def equal_concurrency(pairs, T):
+    """The engine through the same host-buffer calls and at the same concurrency as the reference
+    arm's timing of the reference CUDA build: StereoCuda.Match on the plain workload (census 9x7,
+    P1 10, P2 150, LR check, median) and FasterStereoCuda.Match on the 3-level pyramid with the
+    reference's own per-level parameters (no override), with 1 host thread and with T host threads,
+    one matcher each, pinned host buffers."""
+    import torch
+    import fasterstereocuda_b200 as fsc
+    from concurrent.futures import ThreadPoolExecutor
+
+    def make(kind):
+        if kind == "plain":
+            m = fsc.StereoCuda()
+            ok = m.Init(W_, H_, 0, DMAX, fsc.CuSGMOption(p1=10, p2_init=150, cs_type=1, num_paths=4,
+                                                          do_median_filter=True, do_lr_check=True,
+                                                          lr_threshold=1.0, unique_threshold=0.95,
+                                                          using_constant_p2=True))
+        else:
+            m = fsc.FasterStereoCuda()
+            ok = m.Init(fsc.StereoOption1(width=W_, height=H_, min_disp=0, max_disp=DMAX, num_layers=LAYERS,
+                                          do_lr_check=True, do_rm_peaks=True))
+        if not ok:
+            raise RuntimeError(m.last_error())
+        return m
+
+    hl = [torch.from_numpy(L).pin_memory().numpy() for L, _ in pairs]
+    hr = [torch.from_numpy(R).pin_memory().numpy() for _, R in pairs]
+    out = {"api": "StereoCuda.Match / FasterStereoCuda.Match, host buffers, one matcher per host thread",
+           "threads": [1, T]}
+    for kind, key in (("plain", "plain_1242x375x64_census9x7_p10_p150_lr_median_pairs_per_s"),
+                      ("pyramid", "pyramid_1242x375_3layers_reference_params_pairs_per_s")):
+        rates = {}
+        for th in (1, T):
+            ms = [make(kind) for _ in range(th)]
+            outs = [torch.empty((H_, W_), dtype=torch.float32).pin_memory().numpy() for _ in range(th)]
+            n = max(8, (400 if kind == "plain" else 300) // th)
+
+            def work(k, count):
+                for j in range(count):
+                    i = (k + j) % len(hl)
+                    if not ms[k].Match(hl[i], hr[i], outs[k]):
+                        raise RuntimeError(ms[k].last_error())
+            with ThreadPoolExecutor(max_workers=th) as ex:
+                list(ex.map(lambda k: work(k, 3), range(th)))
+                t = time.perf_counter()
+                list(ex.map(lambda k: work(k, n), range(th)))
+                rates[str(th)] = th * n / (time.perf_counter() - t)
+            del ms
+        out[key] = rates
+    return out
+
+
 def _dev_copy(dst_addr, src_tensor):
     from cuda.bindings import runtime as rt
     (err,) = rt.cudaMemcpy(dst_addr, src_tensor.data_ptr(), src_tensor.numel() * src_tensor.element_size(),

@@ -47,7 +47,7 @@ def build_engine(force: bool = False, verbose: bool = False) -> Path:
     if not force and not _stale(ENGINE_LIB, deps):
         return ENGINE_LIB
     LIB_DIR.mkdir(exist_ok=True)
-    objs = []
+    objs, cmds = [], []
     for src in sources:
         obj = LIB_DIR / (src.stem + ".o")
         cmd = [_nvcc(), "-std=c++17", "-O3", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC,-fvisibility=hidden",
@@ -56,8 +56,14 @@ def build_engine(force: bool = False, verbose: bool = False) -> Path:
             cmd[1:1] = ["-x", "cu"]
         if verbose:
             cmd.append("-Xptxas=-v")
-        subprocess.run(cmd, check=True)
+        cmds.append(cmd)
         objs.append(str(obj))
+    # the translation units are independent: compile them side by side
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for r in list(ex.map(lambda c: subprocess.run(c), cmds)):
+            if r.returncode != 0:
+                raise subprocess.CalledProcessError(r.returncode, r.args)
     tmp = ENGINE_LIB.with_suffix(".so.tmp")
     subprocess.run([_nvcc(), *ARCH, "-shared", "-o", str(tmp), *objs, "-lcudart"], check=True)
     os.replace(tmp, ENGINE_LIB)

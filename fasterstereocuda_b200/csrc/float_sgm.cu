@@ -577,10 +577,25 @@ int validate(int B, int H, int W, int D, float temperature) {
     sgm_set_process_error("float SGM: temperature must be > 0 with a finite reciprocal");
     return SGM_ERR_ARG;
   }
-  if ((size_t)B * H * W * D > ((size_t)1 << 40)) {
-    sgm_set_process_error("float SGM: volume too large");
-    return SGM_ERR_ARG;
+  // B*H*W*D voxels, bounded factor by factor so that no product can wrap
+  const uint64_t kMaxVoxels = (uint64_t)1 << 40;
+  uint64_t n = 1;
+  for (const int32_t f : {B, H, W, D}) {
+    if ((uint64_t)f > kMaxVoxels / n) {
+      sgm_set_process_error("float SGM: volume too large");
+      return SGM_ERR_ARG;
+    }
+    n *= (uint64_t)f;
   }
+  return SGM_OK;
+}
+
+int check_present(std::initializer_list<const void*> ptrs) {
+  for (const void* p : ptrs)
+    if (!p) {
+      sgm_set_process_error("float SGM: null device pointer");
+      return SGM_ERR_ARG;
+    }
   return SGM_OK;
 }
 
@@ -706,7 +721,9 @@ size_t sgm_float_workspace_elems(int32_t B, int32_t H, int32_t W, int32_t D) {
 int sgm_float_forward(const float* cost, const float* p1, const float* p2, int32_t B, int32_t H, int32_t W,
                       int32_t D, float temperature, float* sum, float* ckpt, float* work, float* disp, void* stream) {
   int st = validate(B, H, W, D, temperature);
-  if (st || (st = check_aligned({cost, sum, ckpt, work}))) return st;
+  if (st || (st = check_present({cost, p1, p2, sum, ckpt, work, disp})) ||
+      (st = check_aligned({cost, sum, ckpt, work})))
+    return st;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const float inv_t = 1.0f / temperature;
   return D == 64 ? forward_impl<kFwdLanes64, 64 / kFwdLanes64>(cost, p1, p2, B, H, W, inv_t, sum, ckpt, work, disp, s)
@@ -717,7 +734,9 @@ int sgm_float_backward(const float* cost, const float* p1, const float* p2, int3
                        float temperature, const float* sum, const float* ckpt, const float* grad_disp,
                        float* grad_sum, float* work, float* grad_cost, float* grad_p1, float* grad_p2, void* stream) {
   int st = validate(B, H, W, D, temperature);
-  if (st || (st = check_aligned({cost, sum, ckpt, grad_sum, work, grad_cost}))) return st;
+  if (st || (st = check_present({cost, p1, p2, sum, ckpt, grad_disp, grad_sum, work, grad_cost, grad_p1, grad_p2})) ||
+      (st = check_aligned({cost, sum, ckpt, grad_sum, work, grad_cost})))
+    return st;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const float inv_t = 1.0f / temperature;
   return D == 64 ? backward_impl<kBwdLanes64, 64 / kBwdLanes64>(cost, p1, p2, B, H, W, inv_t, sum, ckpt, grad_disp,

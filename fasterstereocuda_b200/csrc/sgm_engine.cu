@@ -151,6 +151,9 @@ struct sgm_engine {
   float* post2 = nullptr;   // dilation output
   float* dr_out = nullptr;  // right map after the LR marks
   float* out = nullptr;     // final left map for the host path
+  // map the depth of Match2 is taken from, set by every match (the final map, or the map before a
+  // lone post filter / morphology step, see engine_enqueue)
+  const float* depth_src = nullptr;
   int16_t* init[2] = {nullptr, nullptr};
   int16_t* init_tmp = nullptr;
   unsigned* key = nullptr;
@@ -248,9 +251,15 @@ int check_launch(sgm_engine* e, const char* what) {
 
 bool supported_range(int D) { return D == 32 || D == 64 || D == 128 || D == 256; }
 
-int validate(sgm_engine* e, int W, int H, int D, const sgm_option_t* o) {
+int validate(sgm_engine* e, int W, int H, int M, int D, const sgm_option_t* o) {
   if (W <= 0 || H <= 0 || D <= 0) {
     set_error(&e->err, "image size or disparity range error (w=%d h=%d d=%d)", W, H, D);
+    return SGM_ERR_ARG;
+  }
+  // the reference's grids cover columns [max(0, min_disparity), W) (cusgm_ca.cu:3991-3999): an
+  // empty range launches nothing sensible there, so it is refused here
+  if (M >= W) {
+    set_error(&e->err, "minimum disparity %d leaves no pixel of a %d-pixel row to match", M, W);
     return SGM_ERR_ARG;
   }
   if (!supported_range(D)) {
@@ -285,7 +294,7 @@ int validate(sgm_engine* e, int W, int H, int D, const sgm_option_t* o) {
 int engine_init(sgm_engine* e, int W, int H, int M, int D, const sgm_option_t* o, bool log, bool volumes = true) {
   if (e->ready) e->free_all();
   e->own_volumes = volumes;
-  const int v = validate(e, W, H, D, o);
+  const int v = validate(e, W, H, M, D, o);
   if (v != SGM_OK) return v;
   SGM_CUDA_TRY(e, cudaGetDevice(&e->dev));
   SGM_CUDA_TRY(e, cudaDeviceGetAttribute(&e->nsm, cudaDevAttrMultiProcessorCount, e->dev));
@@ -745,6 +754,12 @@ int engine_enqueue(sgm_engine* e, const uint8_t* dl_img, const uint8_t* dr_img, 
                                                      e->wta, nullptr, nullptr, dst, W, H, 0.0f));
     cur = dst;
   }
+  // StereoCudaImpl::Match2 (StereoCudaImpl.cpp:548-583) takes the depth from the aggregator's
+  // buffer unless small-region removal ran; DisparityFilter::Filter (cusgm_df.cu:275-339) leaves a
+  // lone post filter or morphology step in its own buffer and writes a morphology step after a
+  // post filter back into the aggregator's buffer. So the depth of a map with exactly one of the
+  // two steps and no removal is the depth of the map before that step.
+  const float* agg = cur;
   if (!st && pf) {
     float* dst = next_out();
     if (pf == 1)
@@ -786,6 +801,7 @@ int engine_enqueue(sgm_engine* e, const uint8_t* dl_img, const uint8_t* dr_img, 
                                                        dout, e->label, e->count, W, H, tiles, e->opt.peaks_ratio_threshold));
     }
   }
+  e->depth_src = (!peaks && ((pf != 0) != (morph != 0))) ? agg : dout;
   e->stream = saved;
   return st;
 }
@@ -929,7 +945,7 @@ int pyr_enqueue(sgm_pyramid* p, const uint8_t* dl, const uint8_t* dr, float* dou
     const int64_t before = e->launches;
     if (n == 0 && p->depth_mode) o = p->disp0;
     st = engine_enqueue(e, il, ir, n < L - 1 ? p->init[n] : nullptr, o, nullptr, s);
-    if (!st && n == 0 && p->depth_mode) st = enqueue_depth(e, p->disp0, dout, p->cam0, s);
+    if (!st && n == 0 && p->depth_mode) st = enqueue_depth(e, e->depth_src, dout, p->cam0, s);
     p->launches += e->launches - before;
     if (st) {
       p->err = e->err;
@@ -1166,9 +1182,10 @@ int sgm_match2(sgm_handle_t h, const uint8_t* img_left, const uint8_t* img_right
   if (init_disp_left)
     SGM_CUDA_TRY(h, cudaMemcpyAsync(h->init[0], init_disp_left, N * sizeof(int16_t), cudaMemcpyHostToDevice, h->stream));
   int st = engine_enqueue(h, h->img[0], h->img[1], init_disp_left ? h->init[0] : nullptr, h->out, nullptr, h->stream);
-  if (!st) st = enqueue_depth(h, h->out, h->post2, h->cam, h->stream);
+  // the depth source is the final map, the LR / median output or the WTA map, never h->post
+  if (!st) st = enqueue_depth(h, h->depth_src, h->post, h->cam, h->stream);
   if (st) return st;
-  SGM_CUDA_TRY(h, cudaMemcpyAsync(depth_left, h->post2, N * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+  SGM_CUDA_TRY(h, cudaMemcpyAsync(depth_left, h->post, N * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
   SGM_CUDA_TRY(h, wait_stream(h->stream, &h->done));
   return SGM_OK;
 }
@@ -1181,6 +1198,10 @@ int sgm_release(sgm_handle_t h) {
 
 int sgm_set_min_disparity(sgm_handle_t h, int32_t min_disparity) {
   if (!h) return SGM_ERR_ARG;
+  if (h->ready && min_disparity >= h->W) {
+    set_error(&h->err, "minimum disparity %d leaves no pixel of a %d-pixel row to match", min_disparity, h->W);
+    return SGM_ERR_ARG;
+  }
   h->M = min_disparity;
   h->drop_graph();  // kernel parameters are part of the graph
   return SGM_OK;

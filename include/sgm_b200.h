@@ -167,9 +167,9 @@ SGM_API int sgm_profile_enable(int32_t enable);
 SGM_API int sgm_profile_read(char* buf, size_t cap);
 
 /* No counterpart in the reference. Single-level matching that allocates no memory, for callers
- * that cannot call cudaMalloc while they run: code recording a CUDA graph or running inside
- * stream capture (an allocation would break or escape the capture), real-time loops that forbid
- * allocation after start-up, and plugin hosts that own the GPU memory budget.
+ * that may not call cudaMalloc once they are running: real-time loops that forbid allocation after
+ * start-up (an allocation can stall and synchronise the device), and plugin hosts that own the GPU
+ * memory budget and hand a plugin only its input and output buffers.
  * Inputs and output are dense device arrays the caller owns (width*height uint8 images, float
  * disparity). All working memory lives in one 64 MiB array inside the library, which every GPU
  * that loads the library keeps until the process exits. The working memory of a call is
@@ -177,11 +177,14 @@ SGM_API int sgm_profile_read(char* buf, size_t cap);
  * each term rounded up to 256; larger requests are rejected with SGM_ERR_ARG and a message in
  * sgm_last_error(NULL). Supported: D = 32, 64 or 128, census, penalties, uniqueness, LR check,
  * median; small-region removal, morphology, post filters and initial disparities are not
- * (SGM_ERR_UNSUPPORTED). Results equal sgm_match_device with the default extended options.
+ * (SGM_ERR_UNSUPPORTED). Also refused (SGM_ERR_ARG): heights above 65535 and a minimum disparity
+ * at or past the width. Results equal sgm_match_device with the default extended options.
  * Calls share the working memory: calls whose work overlaps on the GPU (two streams, two host
- * threads) race and must be serialised by the caller. The first call on each device looks up the
- * array's device address (cudaGetSymbolAddress); make it before any stream capture starts.
- * Enqueued on `stream` (a cudaStream_t), not synchronised. */
+ * threads) race and must be serialised by the caller. The first call on each device does the
+ * set-up -- it looks up the array's device address (cudaGetSymbolAddress) and loads the kernels --
+ * so make it before any stream capture starts. A CUDA error left pending by earlier work makes the
+ * call fail with SGM_ERR_CUDA without clearing it. Enqueued on `stream` (a cudaStream_t), not
+ * synchronised. */
 SGM_API int sgm_match_noalloc(const uint8_t* d_left, const uint8_t* d_right, float* d_disp_left, int32_t width,
                               int32_t height, int32_t min_disparity, int32_t disp_range, const sgm_option_t* option,
                               void* stream);

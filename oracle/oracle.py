@@ -25,7 +25,10 @@ class _Cfg(C.Structure):
         ("morphology_dilation", C.c_int32), ("do_remove_peaks", C.c_int32), ("peaks_ratio", C.c_float),
         ("peaks_strips", C.c_int32), ("peaks_abs_mode", C.c_int32), ("tie_rule", C.c_int32),
         ("init_tie_rule", C.c_int32), ("p2_div0", C.c_int32), ("threads", C.c_int32),
-        ("post_filter", C.c_int32), ("morphology", C.c_int32)]]
+        ("post_filter", C.c_int32), ("morphology", C.c_int32),
+        ("roi_l_enable", C.c_int32), ("roi_l_x", C.c_int32), ("roi_l_y", C.c_int32), ("roi_l_w", C.c_int32),
+        ("roi_l_h", C.c_int32), ("roi_r_enable", C.c_int32), ("roi_r_x", C.c_int32), ("roi_r_y", C.c_int32),
+        ("roi_r_w", C.c_int32), ("roi_r_h", C.c_int32)]]
 
 
 class _PyrCfg(C.Structure):
@@ -60,6 +63,25 @@ class Config:
     threads: int = 0
     post_filter: int = 0
     morphology: int = 0
+    roi_l_enable: int = 0
+    roi_l_x: int = 0
+    roi_l_y: int = 0
+    roi_l_w: int = 0
+    roi_l_h: int = 0
+    roi_r_enable: int = 0
+    roi_r_x: int = 0
+    roi_r_y: int = 0
+    roi_r_w: int = 0
+    roi_r_h: int = 0
+
+    def with_roi(self, left=None, right=None) -> "Config":
+        """A copy with the regions of interest (x, y, w, h) of the left / right view."""
+        kw = dict(self.__dict__)
+        for tag, r in (("l", left), ("r", right)):
+            if r is not None:
+                kw.update({f"roi_{tag}_enable": 1, f"roi_{tag}_x": r[0], f"roi_{tag}_y": r[1], f"roi_{tag}_w": r[2],
+                           f"roi_{tag}_h": r[3]})
+        return Config(**kw)
 
     def c(self) -> _Cfg:
         s = _Cfg()
@@ -244,6 +266,20 @@ def depth_from_disp(disp: np.ndarray, x0_left: float, x0_right: float, focus: fl
     with np.errstate(divide="ignore", invalid="ignore"):
         depth = (f1 / (d.astype(np.float64) + f2)).astype(np.float32)
     return np.where(d == INVALID_FLOAT, INVALID_FLOAT, depth)
+
+
+def depth_source_config(cfg: Config) -> Config:
+    """The options whose final map StereoCudaImpl::Match2 turns into depth. Match2
+    (SgmStereoCuda/StereoCudaImpl.cpp:548-583) reads the aggregator's disparity buffer unless
+    small-region removal ran (then the host map after it). DisparityFilter::Filter
+    (SgmStereoCuda/cusgm_df.cu:275-339) filters the median in place in that buffer, writes a post
+    filter or a morphology step alone into its own buffer, and writes the morphology that follows a
+    post filter back into the aggregator's buffer. So with exactly one of post filter / morphology
+    and no small-region removal, the depth comes from the map before that step."""
+    mp = cfg.morphology or (2 if cfg.morphology_dilation else 0)
+    if cfg.do_remove_peaks or (cfg.post_filter != 0) == (mp != 0):
+        return cfg
+    return Config(**{**cfg.__dict__, "post_filter": 0, "morphology": 0, "morphology_dilation": 0})
 
 
 def pyr_init2_coarsest(width: int, num_layers: int, min_depth: float, max_depth: float, x0_left: float,

@@ -13,6 +13,7 @@
 // past their allocation (D = 32 without initial disparities, D = 128, D = 256).
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <chrono>
 #include <cstdint>
 #include <cstdio>
@@ -42,9 +43,10 @@ struct ref_case_t {
   int32_t do_lr_check;
   float lr_threshold;
   int32_t do_median;
-  int32_t morphology;  // 0 none, 2 dilation
+  int32_t morphology;  // 0 none, 1 erosion, 2 dilation, 3 open, 4 close
   int32_t do_remove_peaks;
   float peaks_ratio;
+  int32_t post_filter;  // 0 none, 1 Gauss, 2 bilateral
 };
 
 int ref_remove_peaks(float* disp, int32_t* segid, int w, int h, int threshold) {
@@ -83,7 +85,7 @@ static void copy_pitched_volume(const cudaPitchedPtr& p, int W, int H, int D, ui
 
 static void clear_pitched_volume(const cudaPitchedPtr& p, int H) { cudaMemset(p.ptr, 0, p.pitch * p.ysize * H); }
 
-static CuSGMOption make_option(const ref_case_t* c, bool lr, bool median, bool peaks, int morph) {
+static CuSGMOption make_option(const ref_case_t* c, bool lr, bool median, bool peaks, int morph, int pf) {
   CuSGMOption o;
   o.p1 = c->p1;
   o.p2_init = c->p2;
@@ -97,8 +99,12 @@ static CuSGMOption make_option(const ref_case_t* c, bool lr, bool median, bool p
   o.using_constant_p2 = true;
   o.do_remove_peaks = peaks;
   o.peaks_ratio_threshold = c->peaks_ratio;
-  o.post_filter_type = CuSGMOption::PF_NONE;
-  o.morphology_type = morph == 2 ? CuSGMOption::MP_DILATION : CuSGMOption::MP_NONE;
+  o.post_filter_type = pf == 1 ? CuSGMOption::PF_GAUSS : (pf == 2 ? CuSGMOption::PF_BILATERAL : CuSGMOption::PF_NONE);
+  o.morphology_type = morph == 1   ? CuSGMOption::MP_EROSION
+                      : morph == 2 ? CuSGMOption::MP_DILATION
+                      : morph == 3 ? CuSGMOption::MP_OPEN
+                      : morph == 4 ? CuSGMOption::MP_CLOSE
+                                   : CuSGMOption::MP_NONE;
   return o;
 }
 
@@ -130,8 +136,9 @@ int ref_match_dump(const ref_case_t* c, const uint8_t* left, const uint8_t* righ
     const bool median = run == 2 ? c->do_median != 0 : false;
     const bool peaks = run == 2 ? c->do_remove_peaks != 0 : false;
     const int morph = run == 2 ? c->morphology : 0;
+    const int pf = run == 2 ? c->post_filter : 0;
     StereoCudaImpl impl;
-    if (!impl.Init(W, H, c->min_disp, D, make_option(c, lr, median, peaks, morph), false)) {
+    if (!impl.Init(W, H, c->min_disp, D, make_option(c, lr, median, peaks, morph, pf), false)) {
       g_msg = "reference Init failed";
       return -2;
     }
@@ -192,6 +199,66 @@ int ref_match_dump(const ref_case_t* c, const uint8_t* left, const uint8_t* righ
   return 0;
 }
 
+// Stage dumps of a match with regions of interest (roi = {x, y, w, h}; roi_r may be NULL):
+//   run A (LR, median, peaks off; left ROI):  cost_lr, paths_lr (4 volumes), wta_l
+//   run B (LR on, median off; both ROIs):     cost_rl, paths_rl (the right view's cost and paths)
+// Runs only rectangles inside the image whose width is a multiple of 4: the reference's WTA launch
+// covers ceil(w/4)*4 columns and floor(h/2)*2 rows from (x, y) (cusgm_ca.cu:4139-4165) and writes
+// without a column bound, and its scans start at x / y and run to x+w / y+h (:1478-1598); inside
+// these limits every access of the plain D = 64 path stays in its allocation.
+int ref_match_roi_dump(const ref_case_t* c, const uint8_t* left, const uint8_t* right, const int32_t* roi_l,
+                       const int32_t* roi_r, uint8_t* cost_lr, uint8_t* paths_lr, float* wta_l, uint8_t* cost_rl,
+                       uint8_t* paths_rl) {
+  if (check_case(c, false)) return -1;
+  const int W = c->width, H = c->height, D = c->disp_range;
+  for (const int32_t* r : {roi_l, roi_r}) {
+    if (!r) continue;
+    if (r[0] < 0 || r[1] < 0 || r[2] <= 0 || r[3] <= 0 || r[0] + r[2] > W || r[1] + r[3] > H || r[2] % 4) {
+      g_msg = "ROI outside the image or its width not a multiple of 4";
+      return -1;
+    }
+  }
+  if (!roi_l) { g_msg = "a left ROI is required"; return -1; }
+  StereoROI_T rl{roi_l[0], roi_l[1], roi_l[2], roi_l[3]};
+  StereoROI_T rr{};
+  if (roi_r) rr = StereoROI_T{roi_r[0], roi_r[1], roi_r[2], roi_r[3]};
+  std::vector<uint8_t> L(left, left + (size_t)W * H), R(right, right + (size_t)W * H);
+  std::vector<float> tmp_l((size_t)W * H), tmp_r((size_t)W * H);
+  for (int run = 0; run < 2; ++run) {
+    StereoCudaImpl impl;
+    if (!impl.Init(W, H, c->min_disp, D, make_option(c, run == 1, false, false, 0, 0), false)) {
+      g_msg = "reference Init failed";
+      return -2;
+    }
+    const size_t dp = impl.aggregator_->dp_psize_;
+    if (!padding_ok(dp, (size_t)W * sizeof(float), 4 * sizeof(float))) {
+      g_msg = "pitch padding too small for the reference's row overrun";
+      impl.Release();
+      return -3;
+    }
+    clear_pitched_volume(*impl.computor_->cost_, H);
+    for (int k = 0; k < 4; ++k) clear_pitched_volume(impl.aggregator_->cost_aggr_dir_[k], H);
+    cudaMemset(impl.aggregator_->disp_map_, 0, dp * H);
+    cudaMemset(impl.aggregator_->disp_map_r_, 0, dp * H);
+    cudaDeviceSynchronize();
+    const bool ok = impl.Match(L.data(), R.data(), tmp_l.data(), tmp_r.data(), nullptr, &rl, roi_r ? &rr : nullptr);
+    if (cudaDeviceSynchronize() != cudaSuccess || !ok) {
+      g_msg = "reference Match failed";
+      impl.Release();
+      return -4;
+    }
+    uint8_t* cost = run == 0 ? cost_lr : cost_rl;
+    uint8_t* paths = run == 0 ? paths_lr : paths_rl;
+    if (cost) copy_pitched_volume(*impl.computor_->cost_, W, H, D, cost);
+    if (paths)
+      for (int k = 0; k < 4; ++k)
+        copy_pitched_volume(impl.aggregator_->cost_aggr_dir_[k], W, H, D, paths + (size_t)k * W * H * D);
+    if (run == 0 && wta_l) memcpy(wta_l, tmp_l.data(), sizeof(float) * W * H);
+    impl.Release();
+  }
+  return 0;
+}
+
 // StereoCudaImpl::Init2 / Match2 (StereoCudaImpl.cpp:263-278, :548-583): depth of the left view
 // with the case's options. cam = {x0_left, y0_left, x0_right, y0_right, focus, baseline}.
 // Same case restrictions and row-padding check as ref_match_dump.
@@ -207,7 +274,8 @@ int ref_match2(const ref_case_t* c, const double* cam, const uint8_t* left, cons
   p.focus = cam[4];
   p.baseline = cam[5];
   StereoCudaImpl impl;
-  const CuSGMOption o = make_option(c, c->do_lr_check != 0, c->do_median != 0, c->do_remove_peaks != 0, c->morphology);
+  const CuSGMOption o =
+      make_option(c, c->do_lr_check != 0, c->do_median != 0, c->do_remove_peaks != 0, c->morphology, c->post_filter);
   if (!impl.Init2(W, H, c->min_disp, c->disp_range, o, p, false)) {
     g_msg = "reference Init2 failed";
     return -2;
@@ -285,7 +353,8 @@ double ref_time_match(const ref_case_t* c, const uint8_t* left, const uint8_t* r
   if (check_case(c, false)) return -1.0;
   StereoCudaImpl impl;
   if (!impl.Init(c->width, c->height, c->min_disp, c->disp_range,
-                 make_option(c, c->do_lr_check != 0, c->do_median != 0, c->do_remove_peaks != 0, c->morphology),
+                 make_option(c, c->do_lr_check != 0, c->do_median != 0, c->do_remove_peaks != 0, c->morphology,
+                             c->post_filter),
                  false))
     return -2.0;
   std::vector<uint8_t> L(left, left + (size_t)c->width * c->height), R(right, right + (size_t)c->width * c->height);
@@ -390,6 +459,86 @@ double ref_time_pyr(int width, int height, int min_disp, int max_disp, int layer
   cudaDeviceSynchronize();
   const auto t1 = std::chrono::steady_clock::now();
   return std::chrono::duration<double, std::milli>(t1 - t0).count() / n;
+}
+
+}  // extern "C"
+
+// Runs body(k) for k = 0 .. threads-1, one host thread each; every thread first runs its warm-up
+// part, then all start the timed part together. Returns the wall time of the timed part in s.
+template <typename Warm, typename Body>
+static double timed_threads(int threads, Warm warm, Body body) {
+  std::atomic<int> ready{0};
+  std::atomic<bool> go{false};
+  std::vector<std::thread> pool;
+  for (int k = 0; k < threads; ++k)
+    pool.emplace_back([&, k] {
+      warm(k);
+      ready.fetch_add(1);
+      while (!go.load()) std::this_thread::yield();
+      body(k);
+    });
+  while (ready.load() < threads) std::this_thread::yield();
+  cudaDeviceSynchronize();
+  const auto t0 = std::chrono::steady_clock::now();
+  go.store(true);
+  for (auto& t : pool) t.join();
+  cudaDeviceSynchronize();
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+extern "C" {
+
+// Pairs per second of `threads` host threads, each with its own StereoCudaImpl, matching the pair
+// n times through StereoCuda::Match (host buffers in and out); < 0 on failure.
+double ref_throughput_match(const ref_case_t* c, const uint8_t* left, const uint8_t* right, int warmup, int n,
+                            int threads) {
+  if (check_case(c, false) || threads < 1) return -1.0;
+  const size_t N = (size_t)c->width * c->height;
+  std::vector<StereoCudaImpl*> impl(threads, nullptr);
+  const CuSGMOption o =
+      make_option(c, c->do_lr_check != 0, c->do_median != 0, c->do_remove_peaks != 0, c->morphology, c->post_filter);
+  for (int k = 0; k < threads; ++k) {
+    impl[k] = new StereoCudaImpl;
+    if (!impl[k]->Init(c->width, c->height, c->min_disp, c->disp_range, o, false)) {
+      for (int j = 0; j <= k; ++j) { impl[j]->Release(); delete impl[j]; }
+      return -2.0;
+    }
+  }
+  std::vector<std::vector<uint8_t>> L(threads, std::vector<uint8_t>(left, left + N)),
+      R(threads, std::vector<uint8_t>(right, right + N));
+  std::vector<std::vector<float>> d(threads, std::vector<float>(N));
+  const double s = timed_threads(
+      threads, [&](int k) { for (int i = 0; i < warmup; ++i) impl[k]->Match(L[k].data(), R[k].data(), d[k].data()); },
+      [&](int k) { for (int i = 0; i < n; ++i) impl[k]->Match(L[k].data(), R[k].data(), d[k].data()); });
+  for (int k = 0; k < threads; ++k) { impl[k]->Release(); delete impl[k]; }
+  return s > 0 ? (double)threads * n / s : -3.0;
+}
+
+// The same for FasterStereoCuda::Match (the reference's per-level parameters); the matchers are
+// leaked for the reason given at ref_pyr_match.
+double ref_throughput_pyr(int width, int height, int min_disp, int max_disp, int layers, int lr, int peaks,
+                          const uint8_t* left, const uint8_t* right, int warmup, int n, int threads) {
+  if (threads < 1) return -1.0;
+  std::vector<FasterStereoCuda*> m(threads, nullptr);
+  FasterStereoCuda::StereoOption1 o;
+  o.width = width;
+  o.height = height;
+  o.min_disp = min_disp;
+  o.max_disp = max_disp;
+  o.num_layers = layers;
+  o.do_lr_check = lr != 0;
+  o.do_rm_peaks = peaks != 0;
+  o.do_smooth = false;
+  for (int k = 0; k < threads; ++k) {
+    m[k] = new FasterStereoCuda;
+    if (!m[k]->Init(o)) return -2.0;
+  }
+  const size_t N = (size_t)width * height;
+  std::vector<std::vector<float>> d(threads, std::vector<float>(N));
+  const double s = timed_threads(
+      threads, [&](int k) { for (int i = 0; i < warmup; ++i) m[k]->Match(left, right, d[k].data()); },
+      [&](int k) { for (int i = 0; i < n; ++i) m[k]->Match(left, right, d[k].data()); });
+  return s > 0 ? (double)threads * n / s : -3.0;
 }
 
 }  // extern "C"

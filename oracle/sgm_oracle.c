@@ -74,16 +74,18 @@ static inline uint8_t hamming(uint64_t a, uint64_t b) { return (uint8_t)__builti
  * Only x in [max(0,min_d), W) is written. The 5x5 right-to-left kernel stops one pixel
  * short in every block of D pixels (cusgm_cc.cu:288): those pixels keep what the
  * buffer held before (the left-to-right cost of the same call), so `cost` is in/out. */
-void orc_cost_plain(const uint64_t* cl, const uint64_t* cr, int W, int H, int min_d, int D, int cs_type,
-                    int left2right, uint8_t* cost) {
+/* blk_x0: first column of the kernel's D-pixel blocks (x0, or the ROI's x for the right view of a
+ * match with a region of interest, cusgm_cc.cu:478-488 via LRCheck :4191). */
+static void cost_plain_blocks(const uint64_t* cl, const uint64_t* cr, int W, int H, int min_d, int D, int cs_type,
+                              int left2right, int blk_x0, uint8_t* cost) {
   const int x0 = imax(0, min_d);
 #pragma omp parallel for num_threads(nthreads()) schedule(static)
   for (int y = 0; y < H; ++y) {
     const uint64_t* l = cl + (size_t)y * W;
     const uint64_t* r = cr + (size_t)y * W;
     for (int x = x0; x < W; ++x) {
-      if (!left2right && cs_type == 0) {
-        const int blk_start = x0 + ((x - x0) / D) * D;
+      if (!left2right && cs_type == 0 && x >= blk_x0) {
+        const int blk_start = blk_x0 + ((x - blk_x0) / D) * D;
         const int iend = imin(D, W - blk_start);
         if (x == blk_start + iend - 1) continue; /* stale pixel */
       }
@@ -95,6 +97,11 @@ void orc_cost_plain(const uint64_t* cl, const uint64_t* cr, int W, int H, int mi
       }
     }
   }
+}
+
+void orc_cost_plain(const uint64_t* cl, const uint64_t* cr, int W, int H, int min_d, int D, int cs_type,
+                    int left2right, uint8_t* cost) {
+  cost_plain_blocks(cl, cr, W, H, min_d, D, cs_type, left2right, imax(0, min_d), cost);
 }
 
 /* CostAdjust, cusgm_cc.cu:14-21: (uint8)expf(4*|d-16|/16) with integer division, i.e.
@@ -157,12 +164,15 @@ static inline uint32_t step_plain(const uint8_t* c, const uint32_t* Lq, uint32_t
  * :4082-4123 (directions: 0 top->bottom, 1 left->right, 2 bottom->top, 3 right->left).
  * Paths cover x in [x0, W) and every row. The stored value is (uint8)L.
  * The reference never stores the first pixel of a path; here it stores (uint8)C there. */
-void orc_path_plain(const uint8_t* cost, int W, int H, int x0, int D, int32_t p1, int32_t p2, int dir,
-                    uint8_t* out) {
+/* The same over a region of interest (StereoCuda::Match with a StereoROI_T): horizontal paths run
+ * along rows [y0, y1) from x0 to x1-1 (or back), vertical paths along columns [x0, x1) from y0 to
+ * y1-1 (or back): the kernels' xoffset / xEnd / yoffset / yend (cusgm_ca.cu:3991-3999, :1478-1598). */
+static void path_plain_region(const uint8_t* cost, int W, int x0, int x1, int y0, int y1, int D, int32_t p1,
+                              int32_t p2, int dir, uint8_t* out) {
   const int horizontal = (dir == 1 || dir == 3);
   const int forward = (dir == 0 || dir == 1);
-  const int nlines = horizontal ? H : (W - x0);
-  const int len = horizontal ? (W - x0) : H;
+  const int nlines = horizontal ? (y1 - y0) : (x1 - x0);
+  const int len = horizontal ? (x1 - x0) : (y1 - y0);
   if (nlines <= 0 || len <= 0) return;
 #pragma omp parallel num_threads(nthreads())
   {
@@ -174,7 +184,7 @@ void orc_path_plain(const uint8_t* cost, int W, int H, int x0, int D, int32_t p1
       for (int s = 0; s < len; ++s) {
         const int k = forward ? s : len - 1 - s;
         const int x = horizontal ? x0 + k : x0 + line;
-        const int y = horizontal ? line : k;
+        const int y = horizontal ? y0 + line : y0 + k;
         const size_t off = ((size_t)y * W + x) * D;
         const uint8_t* c = cost + off;
         if (s == 0) {
@@ -190,6 +200,11 @@ void orc_path_plain(const uint8_t* cost, int W, int H, int x0, int D, int32_t p1
     free(Lq);
     free(Lp);
   }
+}
+
+void orc_path_plain(const uint8_t* cost, int W, int H, int x0, int D, int32_t p1, int32_t p2, int dir,
+                    uint8_t* out) {
+  path_plain_region(cost, W, x0, W, 0, H, D, p1, p2, dir, out);
 }
 
 /* Path aggregation with per-pixel base disparities (D = 32 levels of the pyramid).
@@ -308,10 +323,14 @@ static int pick_tie(const uint32_t* S, int D, uint32_t m, int rule, int y) {
  *   d* <= 0 or d* >= D (generic: d* >= D-1) -> INVALID;
  *   c3 at d* = D-1 reads the slot that holds the winning index, i.e. the value D-1;
  *   min(c1-c2, c3-c2) <= c2*(1-u) -> INVALID; else d* + min_d + bias. */
-void orc_wta_plain(const uint8_t* const paths[4], int W, int H, int x0, int min_d, int D, float uniqueness,
-                   int tie_rule, float* disp) {
+/* With a region of interest (columns [x0, x1), rows [y0, y1)) the launch covers the region's
+ * columns and floor((y1-y0)/2)*2 rows from y0 (cusgm_ca.cu:4139-4165 with roi_x/roi_y/roi_w/roi_h);
+ * the border test stays in image coordinates, and the measured tie rule's row parity is the row's
+ * position in its two-row block, i.e. y - y0. Everything outside is INVALID. */
+static void wta_plain_region(const uint8_t* const paths[4], int W, int H, int x0, int x1, int y0, int y1, int min_d,
+                             int D, float uniqueness, int tie_rule, float* disp) {
   const int warp_kernel = (D == 32 || D == 64 || D == 128);
-  const int rows = warp_kernel ? (H / 2) * 2 : H;
+  const int rows = warp_kernel ? ((y1 - y0) / 2) * 2 : (y1 - y0);
   const float ut = 1.0f - uniqueness;
 #pragma omp parallel num_threads(nthreads())
   {
@@ -321,7 +340,7 @@ void orc_wta_plain(const uint8_t* const paths[4], int W, int H, int x0, int min_
       for (int x = 0; x < W; ++x) {
         float* out = disp + (size_t)y * W + x;
         *out = ORC_INVALID_FLOAT;
-        if (y >= rows || x < x0) continue;
+        if (y < y0 || y >= y0 + rows || x < x0 || x >= x1) continue;
         if (x > W - 5 || y > H - 5 || x < 5 || y < 5) continue;
         const size_t off = ((size_t)y * W + x) * D;
         uint32_t m = 0xFFFFFFFFu;
@@ -329,7 +348,7 @@ void orc_wta_plain(const uint8_t* const paths[4], int W, int H, int x0, int min_
           S[d] = (uint32_t)paths[0][off + d] + paths[1][off + d] + paths[2][off + d] + paths[3][off + d];
           m = umin(m, S[d]);
         }
-        const int ds = pick_tie(S, D, m, tie_rule, y);
+        const int ds = pick_tie(S, D, m, tie_rule, y - y0);
         if (ds <= 0 || ds >= (warp_kernel ? D : D - 1)) continue;
         const float c1 = (float)S[ds - 1];
         const float c2 = (float)m;
@@ -342,6 +361,11 @@ void orc_wta_plain(const uint8_t* const paths[4], int W, int H, int x0, int min_
     }
     free(S);
   }
+}
+
+void orc_wta_plain(const uint8_t* const paths[4], int W, int H, int x0, int min_d, int D, float uniqueness,
+                   int tie_rule, float* disp) {
+  wta_plain_region(paths, W, H, x0, W, 0, H, min_d, D, uniqueness, tie_rule, disp);
 }
 
 /* Output of one winning candidate d at an init-disparity level (cusgm_ca.cu:3488-3509). */
@@ -626,9 +650,12 @@ int orc_remove_peaks_strip(float* disp, int w, int h, int threshold, int abs_mod
  * rm_tiles = floor(H / strips); strip i covers rows [i*rm_tiles, (i+1)*rm_tiles);
  * rows at and below strips*rm_tiles are not processed;
  * threshold = (int)((float)(W*h_strip) * ratio). */
-int orc_remove_peaks(float* disp, int W, int H, int strips, float ratio, int abs_mode) {
+/* With a region of interest the strips cover the region's rows: rm_tiles = floor(roi_h / strips),
+ * strip i rows [roi_y + i*rm_tiles, min(H, roi_y + (i+1)*rm_tiles)) (StereoCudaImpl.cpp:463-498). */
+static int remove_peaks_rows(float* disp, int W, int H, int y_off, int rows_h, int strips, float ratio,
+                             int abs_mode) {
   if (strips <= 0) return 0;
-  const int tiles = H / strips;
+  const int tiles = rows_h / strips;
   if (tiles <= 0) return 0;
   int total = 0;
 #pragma omp parallel num_threads(nthreads()) reduction(+ : total)
@@ -637,8 +664,9 @@ int orc_remove_peaks(float* disp, int W, int H, int strips, float ratio, int abs
     int32_t* queue = (int32_t*)malloc(sizeof(int32_t) * (size_t)W * tiles);
 #pragma omp for schedule(dynamic, 1)
     for (int i = 0; i < strips; ++i) {
-      const int start = i * tiles;
-      const int end = imin(H, (i + 1) * tiles);
+      const int start = imax(0, y_off + i * tiles);
+      const int end = imin(H, y_off + (i + 1) * tiles);
+      if (end <= start) continue;
       const int h = end - start;
       const int threshold = (int)((float)(W * h) * ratio);
       total += remove_peaks_strip(disp + (size_t)start * W, W, h, threshold, abs_mode, label, queue);
@@ -647,6 +675,10 @@ int orc_remove_peaks(float* disp, int W, int H, int strips, float ratio, int abs
     free(queue);
   }
   return total;
+}
+
+int orc_remove_peaks(float* disp, int W, int H, int strips, float ratio, int abs_mode) {
+  return remove_peaks_rows(disp, W, H, 0, H, strips, ratio, abs_mode);
 }
 
 /* Even-sample decimation by 2. FasterStereoCuda.cpp:114-136. */
@@ -713,25 +745,52 @@ static void right_init(const int16_t* init_l, int16_t* init_r, int W, int H) {
   free(tmp);
 }
 
+/* Region of one view: columns [x0, x1), rows [y0, y1), and the origin of the cost kernel's
+ * D-pixel blocks. Without an ROI: columns from max(0, min_disp), every row (cusgm_ca.cu:3991-3999).
+ * With an ROI: its rectangle, columns clipped to start at max(0, min_disp) (the left view's cost,
+ * computed without the ROI, covers only those, StereoCudaImpl.cpp:403). */
+typedef struct { int x0, x1, y0, y1, bx; } orc_region_t;
+
+static orc_region_t view_region(const orc_config_t* c, int left_view) {
+  const int xmin = imax(0, c->min_disp);
+  orc_region_t r = {xmin, c->width, 0, c->height, xmin};
+  const int en = left_view ? c->roi_l_enable : c->roi_r_enable;
+  if (en) {
+    const int rx = left_view ? c->roi_l_x : c->roi_r_x, ry = left_view ? c->roi_l_y : c->roi_r_y;
+    const int rw = left_view ? c->roi_l_w : c->roi_r_w, rh = left_view ? c->roi_l_h : c->roi_r_h;
+    r.x0 = imax(rx, xmin);
+    r.x1 = rx + rw;
+    r.y0 = ry;
+    r.y1 = ry + rh;
+    r.bx = rx;
+  }
+  return r;
+}
+
+static int roi_ok(int en, int x, int y, int w, int h, int W, int H) {
+  return !en || (x >= 0 && y >= 0 && w > 0 && h > 0 && x + w <= W && y + h <= H);
+}
+
 static int run_view(const orc_config_t* c, const uint64_t* cl, const uint64_t* cr, const int16_t* init,
                     int left2right, uint8_t* cost, uint8_t* paths, float* wta, uint8_t* cost_dump,
                     uint8_t* paths_dump) {
   const int W = c->width, H = c->height, D = c->disp_range;
   const size_t V = (size_t)W * H * D;
   const int x0 = imax(0, c->min_disp);
+  const orc_region_t r = view_region(c, left2right);
   if (init) orc_cost_init(cl, cr, init, W, H, x0, D, c->cs_type, left2right, cost);
-  else orc_cost_plain(cl, cr, W, H, c->min_disp, D, c->cs_type, left2right, cost);
+  else cost_plain_blocks(cl, cr, W, H, c->min_disp, D, c->cs_type, left2right, r.bx, cost);
   if (cost_dump) memcpy(cost_dump, cost, V);
   const uint8_t* P[4];
   for (int dir = 0; dir < 4; ++dir) {
     uint8_t* out = paths + (size_t)dir * V;
     if (init) orc_path_init(cost, init, W, H, x0, D, c->p1, c->p2, c->p2_div0, dir, out);
-    else orc_path_plain(cost, W, H, x0, D, c->p1, c->p2, dir, out);
+    else path_plain_region(cost, W, r.x0, r.x1, r.y0, r.y1, D, c->p1, c->p2, dir, out);
     P[dir] = out;
   }
   if (paths_dump) memcpy(paths_dump, paths, 4 * V);
   if (init) orc_wta_init(P, init, W, H, x0, D, c->uniqueness, c->init_tie_rule, wta);
-  else orc_wta_plain(P, W, H, x0, c->min_disp, D, c->uniqueness, c->tie_rule, wta);
+  else wta_plain_region(P, W, H, r.x0, r.x1, r.y0, r.y1, c->min_disp, D, c->uniqueness, c->tie_rule, wta);
   return 0;
 }
 
@@ -742,6 +801,10 @@ int orc_match_dump(const orc_config_t* c, const uint8_t* left, const uint8_t* ri
                    uint8_t* cost_rl, uint8_t* paths_rl, float* wta_r, float* disp_l, float* disp_r) {
   const int W = c->width, H = c->height, D = c->disp_range;
   if (W <= 0 || H <= 0 || D <= 0 || !left || !right || !disp_l) return -1;
+  if (!roi_ok(c->roi_l_enable, c->roi_l_x, c->roi_l_y, c->roi_l_w, c->roi_l_h, W, H) ||
+      !roi_ok(c->roi_r_enable, c->roi_r_x, c->roi_r_y, c->roi_r_w, c->roi_r_h, W, H))
+    return -1;
+  if (init && (c->roi_l_enable || c->roi_r_enable)) return -3; /* ROI at initial-disparity levels: not built */
   const size_t N = (size_t)W * H, V = N * D;
   uint64_t* cl = (uint64_t*)malloc(sizeof(uint64_t) * N);
   uint64_t* cr = (uint64_t*)malloc(sizeof(uint64_t) * N);
@@ -796,7 +859,12 @@ int orc_match_dump(const orc_config_t* c, const uint8_t* left, const uint8_t* ri
       memcpy(dl, tmp, sizeof(float) * N);
     }
   }
-  if (c->do_remove_peaks) orc_remove_peaks(dl, W, H, c->peaks_strips, c->peaks_ratio, c->peaks_abs_mode);
+  if (c->do_remove_peaks) {
+    if (c->roi_l_enable)
+      remove_peaks_rows(dl, W, H, c->roi_l_y, c->roi_l_h, c->peaks_strips, c->peaks_ratio, c->peaks_abs_mode);
+    else
+      orc_remove_peaks(dl, W, H, c->peaks_strips, c->peaks_ratio, c->peaks_abs_mode);
+  }
   memcpy(disp_l, dl, sizeof(float) * N);
   if (disp_r) memcpy(disp_r, dr, sizeof(float) * N);
 done:

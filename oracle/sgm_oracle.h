@@ -67,6 +67,10 @@ typedef struct {
   int32_t threads;          /* OpenMP threads, <= 0: runtime default */
   int32_t post_filter;      /* 0 none, 1 Gauss, 2 bilateral (after the median) */
   int32_t morphology;       /* 0: as morphology_dilation; 1 erosion, 2 dilation, 3 open, 4 close */
+  /* regions of interest (StereoROI_T of StereoCuda::Match) of the left and the right view; the
+   * rectangle must lie inside the image. Plain levels only. */
+  int32_t roi_l_enable, roi_l_x, roi_l_y, roi_l_w, roi_l_h;
+  int32_t roi_r_enable, roi_r_x, roi_r_y, roi_r_w, roi_r_h;
 } orc_config_t;
 
 /* ---- stages ---- */

@@ -43,7 +43,8 @@ class RefCase(C.Structure):
     _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("min_disp", C.c_int32), ("disp_range", C.c_int32),
                 ("cs_type", C.c_int32), ("p1", C.c_int32), ("p2", C.c_int32), ("uniqueness", C.c_float),
                 ("do_lr_check", C.c_int32), ("lr_threshold", C.c_float), ("do_median", C.c_int32),
-                ("morphology", C.c_int32), ("do_remove_peaks", C.c_int32), ("peaks_ratio", C.c_float)]
+                ("morphology", C.c_int32), ("do_remove_peaks", C.c_int32), ("peaks_ratio", C.c_float),
+                ("post_filter", C.c_int32)]
 
 
 def ref_lib():
@@ -117,7 +118,24 @@ def cases():
     out["dil_only"] = (dict(base, width=621, height=187, do_lr_check=0, do_median=0, morphology=2), L, R, None, False)
     out["peaks_only"] = (dict(base, width=621, height=187, do_lr_check=0, do_median=0, do_remove_peaks=1,
                               peaks_ratio=0.005), L, R, None, False)
+    # post filters and morphology (DisparityFilter::Filter, cusgm_df.cu:275-339) on the WTA map
+    # (no LR check, no median: both race in the reference); each writes a separate buffer. An even
+    # height: the WTA writes every row, so no filter window reads a row the reference leaves unset
+    L, R, _ = scenes.kitti_like(19, 620, 186)
+    flt = dict(base, width=620, height=186, do_lr_check=0, do_median=0)
+    out["gauss_only"] = (dict(flt, post_filter=1), L, R, None, False)
+    out["bilateral_only"] = (dict(flt, post_filter=2), L, R, None, False)
+    out["erosion_only"] = (dict(flt, morphology=1), L, R, None, False)
+    out["open_only"] = (dict(flt, morphology=3), L, R, None, False)
+    out["close_only"] = (dict(flt, morphology=4), L, R, None, False)
+    out["gauss_erosion"] = (dict(flt, post_filter=1, morphology=1), L, R, None, False)
+    out["bilateral_close"] = (dict(flt, post_filter=2, morphology=4), L, R, None, False)
     return out
+
+
+# single-level cases whose final map comes from a post filter (compared within FILTER_TOL of the
+# reference's map on the CPU: the oracle's expf/exp are the C library's, the reference's CUDA's)
+FILTER_CASES = ("gauss_only", "bilateral_only", "gauss_erosion", "bilateral_close")
 
 
 # name: (seed, width, height, min_disp, max_disp, layers, lr check, small-region removal)
@@ -126,8 +144,10 @@ PYR_CASES = {"pyr_kitti": (17, 1242, 375, 0, 64, 3, 1, 1), "pyr_cone": (16, 450,
 
 # Depth output (Init2 / Match2). Camera: x0_left, y0_left, x0_right, y0_right, focus, baseline.
 CAM = (600.0, 180.0, 610.0, 180.0, 720.0, 540.0)
-# single-level cases (from cases()) whose stages have no thread races, matched to depth
-DEPTH_CASES = ("peaks_only", "dil_only")
+# single-level cases (from cases()) whose stages have no thread races, matched to depth: with one
+# of post filter / morphology and no small-region removal the reference takes the depth from the
+# map before that filter (StereoCudaImpl::Match2, StereoCudaImpl.cpp:548-583)
+DEPTH_CASES = ("peaks_only", "dil_only", "gauss_only", "erosion_only", "gauss_erosion")
 # name: (seed, width, height, min_depth, max_depth, layers, lr check, small-region removal)
 DEPTH_PYR_CASES = {"depthpyr_kitti": (43, 1242, 375, 5000.0, 60000.0, 3, 1, 1)}
 
@@ -347,9 +367,10 @@ def oracle_depth(z, case, peaks_strips):
                        disp_range=case["disp_range"], cs_type=case["cs_type"], p1=case["p1"], p2=case["p2"],
                        uniqueness=case["uniqueness"], do_lr_check=case["do_lr_check"],
                        lr_threshold=case["lr_threshold"], do_median=case["do_median"],
-                       morphology_dilation=int(case["morphology"] == 2), do_remove_peaks=case["do_remove_peaks"],
-                       peaks_ratio=case["peaks_ratio"], peaks_strips=peaks_strips, tie_rule=4, init_tie_rule=4)
-        d = O.match(cfg, z["left"], z["right"])["disp"]
+                       morphology=case["morphology"], post_filter=case.get("post_filter", 0),
+                       do_remove_peaks=case["do_remove_peaks"], peaks_ratio=case["peaks_ratio"],
+                       peaks_strips=peaks_strips, tie_rule=4, init_tie_rule=4)
+        d = O.match(O.depth_source_config(cfg), z["left"], z["right"])["disp"]
     rows = np.zeros(d.shape, bool)
     rows[:d.shape[0] - 1 if d.shape[0] % 2 else d.shape[0]] = True  # the reference never writes the last odd row
     return O.depth_from_disp(d, cam[0], cam[2], cam[4], cam[5]), rows
@@ -428,13 +449,18 @@ def finalize(dump_dir: Path, write: bool = True):
             r["lr_right_all"] = float((a["disp_r"].view(np.uint32) == z["lr_r"].view(np.uint32))[written].mean())
         # full options
         cf = O.Config(**{**cfg.__dict__, "do_lr_check": case["do_lr_check"], "do_median": case["do_median"],
-                         "morphology_dilation": int(case["morphology"] == 2),
+                         "morphology": case["morphology"], "post_filter": case.get("post_filter", 0),
                          "do_remove_peaks": case["do_remove_peaks"], "peaks_ratio": case["peaks_ratio"]})
         full = O.match(cf, z["left"], z["right"], init)["disp"]
         rows = np.zeros((H, W), bool)
         rows[:H - 1 if H % 2 else H] = True  # the reference never writes the last odd row
         eq = full.view(np.uint32) == z["disp_l"].view(np.uint32)
         r["disp_all"] = float(eq[rows].mean())
+        if case.get("post_filter", 0):
+            a_, b_ = full[rows], z["disp_l"][rows]
+            both = (a_ != INV) & (b_ != INV)
+            r["disp_invalid_equal"] = bool(np.array_equal(a_ == INV, b_ == INV))
+            r["disp_max_abs_diff"] = float(np.abs(a_[both] - b_[both]).max()) if both.any() else 0.0
         if case["do_median"] and not case["do_remove_peaks"] and case["morphology"] == 0:
             pre = z["lr_l"] if case["do_lr_check"] else z["wta_l"]
             mf, _ = _race_free_median(O, pre)

@@ -70,6 +70,9 @@ def test_argument_errors_without_device(engine_lib):
     assert not s.Init(100, 100, 0, 64, fsc.CuSGMOption(p1=-1)) and s.status == -1
     assert not s.Init(100, 100, 0, 64, fsc.CuSGMOption(post_filter_type=3)) and s.status == -1
     assert not s.Init(100, 100, 0, 64, fsc.CuSGMOption(morphology_type=5)) and s.status == -1
+    # a minimum disparity at or past the width leaves nothing to match: refused
+    assert not s.Init(100, 100, 100, 64, opt) and s.status == -1
+    assert "minimum disparity" in s.last_error()
     img = np.zeros((10, 10), np.uint8)
     d = np.zeros((10, 10), np.float32)
     s.width = s.height = 10
@@ -93,6 +96,11 @@ def test_float_sgm_sizes_and_argument_errors_without_device(engine_lib):
     assert st == -1 and b"16-byte aligned" in lib.sgm_last_error(None)
     st = lib.sgm_float_backward(a16, a16, a16, B, H, W, D, 1.0, a16, a16, a16, a16 + 8, a16, a16, a16, a16, None)
     assert st == -1 and b"16-byte aligned" in lib.sgm_last_error(None)
+    st = lib.sgm_float_forward(a16, a16, a16, B, H, W, D, 1.0, a16, a16, a16, None, None)
+    assert st == -1 and b"null device pointer" in lib.sgm_last_error(None)
+    big = (1 << 31) - 1  # B*H*W*D would wrap a 64-bit product
+    st = lib.sgm_float_forward(a16, a16, a16, big, big, big, D, 1.0, a16, a16, a16, a16, None)
+    assert st == -1 and b"too large" in lib.sgm_last_error(None)
     for t in (0.0, -1.0, float("nan"), 1e-40):
         st = lib.sgm_float_forward(a16, a16, a16, B, H, W, D, t, a16, a16, a16, a16, None)
         assert st == -1 and b"temperature" in lib.sgm_last_error(None), t

@@ -94,3 +94,58 @@ def test_pyramid_init2_match2(engine_lib, oracle_mod, layers):
                              CAM["baseline"])
     assert np.array_equal(depth.view(np.uint32), want.view(np.uint32)), int((depth != want).sum())
     assert (depth != INV).mean() > 0.3
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("pf,morph", [(1, 0), (0, 1), (2, 4)])
+def test_match2_depth_source_rule(engine_lib, oracle_mod, pf, morph):
+    """StereoCudaImpl::Match2 (StereoCudaImpl.cpp:548-583) reads the aggregator's buffer: with
+    exactly one of post filter / morphology (and no small-region removal) that holds the map before
+    the step; after both, the morphology result (cusgm_df.cu:275-339)."""
+    import fasterstereocuda_b200 as fsc
+    O = oracle_mod
+    W, H = 450, 376
+    L, R, _ = scenes.planar_pair(62, W, H)
+    opt = fsc.CuSGMOption(p1=10, p2_init=150, cs_type=1, num_paths=4, do_median_filter=True, do_lr_check=True,
+                          lr_threshold=1.0, unique_threshold=0.95, using_constant_p2=True, post_filter_type=pf,
+                          morphology_type=morph)
+    s = fsc.StereoCuda()
+    assert s.Init2(W, H, 0, 64, opt, fsc.CamParam(**CAM)), s.last_error()
+    depth = np.empty((H, W), np.float32)
+    assert s.Match2(L, R, depth), s.last_error()
+    if pf and morph:  # the final map: the engine's own Match output, turned into depth
+        disp = np.empty((H, W), np.float32)
+        assert s.Match(L, R, disp), s.last_error()
+    else:  # the map before the lone step, which has no smoothing in it
+        cfg = O.Config(width=W, height=H, disp_range=64, post_filter=pf, morphology=morph)
+        disp = O.match(O.depth_source_config(cfg), L, R)["disp"]
+    want = O.depth_from_disp(disp, CAM["x0_left"], CAM["x0_right"], CAM["focus"], CAM["baseline"])
+    assert np.array_equal(depth.view(np.uint32), want.view(np.uint32)), int((depth != want).sum())
+
+
+@pytest.mark.gpu
+def test_pyramid_match2_with_smoothing_takes_depth_before_the_gauss_filter(engine_lib, oracle_mod):
+    """FasterStereoCuda::Match2 with do_smooth: the finest level runs the Gauss filter
+    (SetSgmParameters, FasterStereoCuda.cpp:169-199) without small-region removal, so its depth is
+    that of the map before the filter (StereoCudaImpl.cpp:548-583)."""
+    import fasterstereocuda_b200 as fsc
+    O = oracle_mod
+    W, H, layers = 1242, 375, 3
+    L, R, _ = scenes.kitti_like(44, W, H)
+    epi = fsc.EpipolarStereoParam(x0_left=CAM["x0_left"], y0_left=CAM["y0_left"], x0_right=CAM["x0_right"],
+                                  y0_right=CAM["y0_right"], baseline=CAM["baseline"], focus=CAM["focus"])
+    opt = fsc.StereoOption2(width=W, height=H, min_depth=5000.0, max_depth=60000.0, num_layers=layers,
+                            do_lr_check=True, do_rm_peaks=True, do_smooth=True, epi=epi)
+    p = fsc.FasterStereoCuda()
+    assert p.Init2(opt, fsc.LevelOverride(cs_type=1, p1=10, p2=150), fsc.ExtOptions(peaks_strips=STRIPS)), \
+        p.last_error()
+    depth = np.empty((H, W), np.float32)
+    assert p.Match2(L, R, depth), p.last_error()
+    m0, d0 = O.pyr_init2_coarsest(W, layers, 5000.0, 60000.0, CAM["x0_left"], CAM["x0_right"], CAM["focus"],
+                                  CAM["baseline"])
+    scale = 2 ** (layers - 1)
+    pc = O.PyrConfig(width=W, height=H, min_disp=m0 * scale, max_disp=(m0 + d0) * scale, num_layers=layers,
+                     override_enable=1, cs_type=1, p1=10, p2=150, peaks_strips=STRIPS, do_smooth=0)
+    want = O.depth_from_disp(O.pyr_match(pc, L, R), CAM["x0_left"], CAM["x0_right"], CAM["focus"],
+                             CAM["baseline"])
+    assert np.array_equal(depth.view(np.uint32), want.view(np.uint32)), int((depth != want).sum())

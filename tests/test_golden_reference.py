@@ -215,5 +215,47 @@ def test_depth_against_reference(oracle_mod, name):
     eq = (want.view(np.uint32) == z["depth"].view(np.uint32))[rows].mean()
     if "num_layers" in case:
         assert eq > 0.9, eq
+    elif case.get("post_filter", 0) and (case["morphology"] or case["do_remove_peaks"]):
+        # the depth of a smoothed map: the filter's weights come from different exp implementations
+        a, b = want[rows], z["depth"][rows]
+        assert np.array_equal(a == INV, b == INV)
+        ok = a != INV
+        np.testing.assert_allclose(a[ok], b[ok], rtol=1e-5)
     else:
         assert eq == 1.0, eq
+
+
+# post filter / morphology fixtures (620x186, WTA map filtered, no LR check or median)
+FILTER_TOL = 3e-5  # px: the oracle's expf/exp are the C library's, the reference's CUDA's (<= 2 ulp per weight)
+MORPH = [c for c in CASES if c in ("erosion_only", "open_only", "close_only")]
+FILTERED = [c for c in CASES if c in ("gauss_only", "bilateral_only", "gauss_erosion", "bilateral_close")]
+
+
+def _full_options(O, z, case):
+    return O.match(config(O, case, z["peaks_strips"], do_lr_check=case["do_lr_check"], do_median=case["do_median"],
+                          morphology=case["morphology"], post_filter=case.get("post_filter", 0)),
+                   z["left"], z["right"])["disp"]
+
+
+@pytest.mark.parametrize("name", MORPH)
+def test_morphology_against_reference(oracle_mod, name):
+    """Erosion, OPEN, CLOSE of DisparityFilter::Filter (cusgm_df.cu:275-339): exact on every pixel
+    (the reference's OPEN leaves the dilation, its CLOSE the erosion)."""
+    z, case = load(name)
+    full = _full_options(oracle_mod, z, case)
+    assert np.array_equal(full.view(np.uint32), z["disp_l"].view(np.uint32)), int((full != z["disp_l"]).sum())
+
+
+@pytest.mark.parametrize("name", FILTERED)
+def test_post_filters_against_reference(oracle_mod, name):
+    """Gauss / bilateral smoothing (cusgm_df.cu:94-162), alone and before a morphology step:
+    the same INVALID pixels as the reference, values within FILTER_TOL (the weights come from
+    different exp implementations), and almost every pixel bit for bit."""
+    z, case = load(name)
+    full = _full_options(oracle_mod, z, case)
+    ref = z["disp_l"]
+    assert np.array_equal(full == INV, ref == INV)
+    both = (full != INV) & (ref != INV)
+    assert both.mean() > 0.3
+    assert float(np.abs(full[both] - ref[both]).max()) <= FILTER_TOL
+    assert (full.view(np.uint32) == ref.view(np.uint32)).mean() > 0.9

@@ -73,6 +73,7 @@ CASES = {
     "dilation_peaks": (200, 150, 0, 64, 0, 8, 32, 1.0, 1, 1, 1, 2, 22),
     "cfg0_450x375": (450, 375, 0, 64, 1, 10, 150, 0.95, 1, 1, 0, 0, 23),
     "tall_global_bt": (96, 1700, 0, 64, 1, 10, 150, 0.95, 1, 1, 0, 0, 24),  # B->T volume beyond shared memory
+    "plain_1242x375x64": (1242, 375, 0, 64, 1, 10, 150, 0.95, 1, 1, 0, 0, 25),  # the single-level metric shape
 }
 
 
