@@ -411,15 +411,16 @@ def run_ours(a, rank, world, local_rank):
     # each pair. Few scanlines in flight favour more lanes per scanline, so the lane split is tuned
     # for this case on its own (every split gives the same disparities).
     lat_m = make_matcher()
+    lat_s = torch.cuda.Stream(device=dev)  # a stream of its own: the events must see the matcher's work
 
     def pair_ms(n):
         ts = []
         for j in range(n):
             i = j % len(dL)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(main)
-            run_one(lat_m, dL[i], dR[i], outs[0], main.cuda_stream)
-            e1.record(main)
+            e0.record(lat_s)
+            run_one(lat_m, dL[i], dR[i], outs[0], lat_s.cuda_stream)
+            e1.record(lat_s)
             torch.cuda.synchronize()
             ts.append(e0.elapsed_time(e1))
         return statistics.median(ts)
@@ -443,7 +444,7 @@ def run_ours(a, rank, world, local_rank):
     fsc.profile_enable(True)
     for j in range(a.profile_pairs):
         i = j % len(dL)
-        run_one(lat_m, dL[i], dR[i], outs[0], main.cuda_stream)
+        run_one(lat_m, dL[i], dR[i], outs[0], lat_s.cuda_stream)
     torch.cuda.synchronize()
     prof = fsc.profile_read()
     fsc.profile_enable(False)

@@ -31,6 +31,7 @@
 #include <vector>
 
 #include "../../include/sgm_b200.h"
+#include "sgm_alloc.h"
 #include "sgm_batch_kernels.cuh"
 #include "sgm_levels.h"
 
@@ -98,10 +99,10 @@ struct sgm_batch {
     if (graph) cudaGraphDestroy(graph);
     exec = nullptr;
     graph = nullptr;
-    if (arena) cudaFree(arena);
-    if (ddesc) cudaFree(ddesc);
-    if (dtab) cudaFree(dtab);
-    if (queues) cudaFree(queues);
+    if (arena) sgm_dev_free(arena);
+    if (ddesc) sgm_dev_free(ddesc);
+    if (dtab) sgm_dev_free(dtab);
+    if (queues) sgm_dev_free(queues);
     arena = nullptr;
     ddesc = nullptr;
     dtab = nullptr;
@@ -505,8 +506,8 @@ int sgm_batch_destroy(sgm_batch_t b) {
 
 const char* sgm_batch_last_error(sgm_batch_t b) { return b ? b->err.c_str() : ""; }
 
-int sgm_batch_init(sgm_batch_t b, const sgm_batch_pair_t* pairs, int32_t count, const sgm_option_t* option,
-                   const sgm_ext_options_t* ext) {
+static int batch_init_impl(sgm_batch_t b, const sgm_batch_pair_t* pairs, int32_t count, const sgm_option_t* option,
+                           const sgm_ext_options_t* ext) {
   if (!b) return SGM_ERR_ARG;
   if (!pairs || !option || count <= 0) return berr(b, SGM_ERR_ARG, "empty batch or null argument");
   if (count > 4096) return berr(b, SGM_ERR_ARG, "at most 4096 pairs per batch (got %d)", count);
@@ -553,7 +554,7 @@ int sgm_batch_init(sgm_batch_t b, const sgm_batch_pair_t* pairs, int32_t count, 
     total += 2 * sz[i].img + 2 * sz[i].cs + 4 * sz[i].vol + sz[i].wta + sz[i].out;
   }
   b->arena_bytes = total;
-  BTRY(b, cudaMalloc(&b->arena, total));
+  BTRY(b, sgm_dev_malloc(&b->arena, total));
   b->hdesc.resize(count);
   for (int i = 0; i < count; ++i) {
     unsigned char* p = b->arena + off[i];
@@ -577,9 +578,10 @@ int sgm_batch_init(sgm_batch_t b, const sgm_batch_pair_t* pairs, int32_t count, 
     d.Q.rows = (q.height / 2) * 2;
     d.Q.dmax_excl = q.disp_range;
     d.Q.dstride = (size_t)q.width * q.height;
+    d.Q.image_border(q.width, q.height);
     d.nv = nv;
   }
-  BTRY(b, cudaMalloc(&b->ddesc, sizeof(BatchPair) * count));
+  BTRY(b, sgm_dev_malloc(&b->ddesc, sizeof(BatchPair) * count));
   BTRY(b, cudaMemcpy(b->ddesc, b->hdesc.data(), sizeof(BatchPair) * count, cudaMemcpyHostToDevice));
 
   // buckets by (D, width class); item tables
@@ -628,10 +630,10 @@ int sgm_batch_init(sgm_batch_t b, const sgm_batch_pair_t* pairs, int32_t count, 
     }
     b->buckets.push_back(k);
   }
-  BTRY(b, cudaMalloc(&b->dtab, tab.size() * sizeof(int)));
+  BTRY(b, sgm_dev_malloc(&b->dtab, tab.size() * sizeof(int)));
   BTRY(b, cudaMemcpy(b->dtab, tab.data(), tab.size() * sizeof(int), cudaMemcpyHostToDevice));
   b->nqueues = 3 * (int)b->buckets.size();
-  BTRY(b, cudaMalloc(&b->queues, b->nqueues * sizeof(int)));
+  BTRY(b, sgm_dev_malloc(&b->queues, b->nqueues * sizeof(int)));
   for (size_t i = 0; i < b->buckets.size(); ++i) {
     cudaStream_t t;
     BTRY(b, cudaStreamCreateWithFlags(&t, cudaStreamNonBlocking));
@@ -658,6 +660,13 @@ int sgm_batch_init(sgm_batch_t b, const sgm_batch_pair_t* pairs, int32_t count, 
   BTRY(b, cudaStreamSynchronize(b->stream));
   b->ready = true;
   return SGM_OK;
+}
+
+int sgm_batch_init(sgm_batch_t b, const sgm_batch_pair_t* pairs, int32_t count, const sgm_option_t* option,
+                   const sgm_ext_options_t* ext) {
+  const int st = batch_init_impl(b, pairs, count, option, ext);
+  if (st && b) b->free_all();  // a batch whose init failed keeps no device memory
+  return st;
 }
 
 int sgm_batch_autotune(sgm_batch_t b) {
@@ -799,11 +808,11 @@ struct sgm_batch_pyr {
     }
     coarse = nullptr;
     for (auto& L : lv)
-      if (L.ddesc) cudaFree(L.ddesc);
+      if (L.ddesc) sgm_dev_free(L.ddesc);
     lv.clear();
-    if (arena) cudaFree(arena);
-    if (dtab) cudaFree(dtab);
-    if (queues) cudaFree(queues);
+    if (arena) sgm_dev_free(arena);
+    if (dtab) sgm_dev_free(dtab);
+    if (queues) sgm_dev_free(queues);
     arena = nullptr;
     dtab = nullptr;
     queues = nullptr;
@@ -1124,8 +1133,9 @@ int sgm_batch_pyr_destroy(sgm_batch_pyr_t p) {
 
 const char* sgm_batch_pyr_last_error(sgm_batch_pyr_t p) { return p ? p->err.c_str() : ""; }
 
-int sgm_batch_pyr_init(sgm_batch_pyr_t p, const sgm_batch_pair_t* pairs, int32_t count,
-                       const sgm_pyr_option1_t* option, const sgm_level_override_t* ov, const sgm_ext_options_t* ext) {
+static int batch_pyr_init_impl(sgm_batch_pyr_t p, const sgm_batch_pair_t* pairs, int32_t count,
+                               const sgm_pyr_option1_t* option, const sgm_level_override_t* ov,
+                               const sgm_ext_options_t* ext) {
   if (!p) return SGM_ERR_ARG;
   if (!pairs || !option || count <= 0) return perr(p, SGM_ERR_ARG, "empty batch or null argument");
   if (count > 4096) return perr(p, SGM_ERR_ARG, "at most 4096 pairs per batch (got %d)", count);
@@ -1208,7 +1218,7 @@ int sgm_batch_pyr_init(sgm_batch_pyr_t p, const sgm_batch_pair_t* pairs, int32_t
     total += (cdil || cpf ? align256(N * 4) : 0) + (cpeaks ? 2 * align256(N * 4) : 0);
   }
   p->arena_bytes = total + p->coarse->arena_bytes;
-  if (total) PTRY(p, cudaMalloc(&p->arena, total));
+  if (total) PTRY(p, sgm_dev_malloc(&p->arena, total));
   // coarsest-level descriptors: post-processing buffers
   int strips = ex.peaks_strips > 0 ? ex.peaks_strips : default_peaks_strips();
   for (int i = 0; i < count; ++i) {
@@ -1272,13 +1282,14 @@ int sgm_batch_pyr_init(sgm_batch_pyr_t p, const sgm_batch_pair_t* pairs, int32_t
       d.Q.rows = (h / 4) * 4;
       d.Q.dmax_excl = sgm::kLevelRange - 1;
       d.Q.dstride = N;
+      d.Q.image_border(w, h);
       d.nv = 1;
       d.IP.W = w; d.IP.H = h; d.IP.x0 = 0;
       d.IP.p1 = (uint32_t)lo.p1; d.IP.p1s = lo.p1; d.IP.p2s = lo.p2_init; d.IP.p2_div0 = ex.p2_div0;
       d.IP.invalid_cost = lo.cs_type == 1 ? 0xFFu : sgm::kInvalidCost;
       d.IP.vstride = N * sgm::kLevelRange;
     }
-    PTRY(p, cudaMalloc(&L.ddesc, sizeof(BatchPair) * count));
+    PTRY(p, sgm_dev_malloc(&L.ddesc, sizeof(BatchPair) * count));
     PTRY(p, cudaMemcpy(L.ddesc, L.hdesc.data(), sizeof(BatchPair) * count, cudaMemcpyHostToDevice));
   }
   // item tables
@@ -1344,10 +1355,10 @@ int sgm_batch_pyr_init(sgm_batch_pyr_t p, const sgm_batch_pair_t* pairs, int32_t
     L.queue0 = nq;
     nq += 3 * (int)L.buckets.size();  // rows, bottom-to-top, top-to-bottom + WTA
   }
-  PTRY(p, cudaMalloc(&p->dtab, tab.size() * sizeof(int)));
+  PTRY(p, sgm_dev_malloc(&p->dtab, tab.size() * sizeof(int)));
   PTRY(p, cudaMemcpy(p->dtab, tab.data(), tab.size() * sizeof(int), cudaMemcpyHostToDevice));
   p->nqueues = nq;
-  if (nq) PTRY(p, cudaMalloc(&p->queues, nq * sizeof(int)));
+  if (nq) PTRY(p, sgm_dev_malloc(&p->queues, nq * sizeof(int)));
   size_t nside = p->coarse->buckets.size();
   int nev = 1 + 3 * (int)p->coarse->buckets.size();
   for (auto& L : p->lv) {
@@ -1383,6 +1394,13 @@ int sgm_batch_pyr_init(sgm_batch_pyr_t p, const sgm_batch_pair_t* pairs, int32_t
   PTRY(p, cudaStreamSynchronize(p->stream));
   p->ready = true;
   return SGM_OK;
+}
+
+int sgm_batch_pyr_init(sgm_batch_pyr_t p, const sgm_batch_pair_t* pairs, int32_t count,
+                       const sgm_pyr_option1_t* option, const sgm_level_override_t* ov, const sgm_ext_options_t* ext) {
+  const int st = batch_pyr_init_impl(p, pairs, count, option, ov, ext);
+  if (st && p) p->free_all();  // a batch whose init failed keeps no device memory
+  return st;
 }
 
 int sgm_batch_pyr_pair_buffers(sgm_batch_pyr_t p, int32_t index, uint8_t** d_left, uint8_t** d_right,

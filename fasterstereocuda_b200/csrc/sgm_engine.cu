@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "../../include/sgm_b200.h"
+#include "sgm_alloc.h"
 #include "sgm_kernels3.cuh"
 #include "sgm_levels.h"
 
@@ -113,16 +114,48 @@ template <typename T>
 cudaError_t dalloc(T** p, size_t count) {
   *p = nullptr;
   if (count == 0) return cudaSuccess;
-  return cudaMalloc(reinterpret_cast<void**>(p), count * sizeof(T));
+  return sgm_dev_malloc(reinterpret_cast<void**>(p), count * sizeof(T));
 }
 
 template <typename T>
 void dfree(T*& p) {
-  if (p) cudaFree(p);
+  if (p) sgm_dev_free(p);
   p = nullptr;
 }
 
+// Fault injection and live-allocation count of sgm_dev_malloc (process-wide).
+std::mutex g_alloc_mu;
+int64_t g_alloc_live = 0;
+int64_t g_alloc_fail_after = -1;  // < 0: never fail; else allocations left before one fails
+
 }  // namespace
+
+cudaError_t sgm_dev_malloc(void** p, size_t bytes) {
+  {
+    std::lock_guard<std::mutex> lk(g_alloc_mu);
+    if (g_alloc_fail_after == 0) {
+      g_alloc_fail_after = -1;  // one failure per arming
+      *p = nullptr;
+      return cudaErrorMemoryAllocation;
+    }
+    if (g_alloc_fail_after > 0) --g_alloc_fail_after;
+  }
+  const cudaError_t st = cudaMalloc(p, bytes);
+  if (st == cudaSuccess) {
+    std::lock_guard<std::mutex> lk(g_alloc_mu);
+    ++g_alloc_live;
+  }
+  return st;
+}
+
+cudaError_t sgm_dev_free(void* p) {
+  if (!p) return cudaSuccess;
+  {
+    std::lock_guard<std::mutex> lk(g_alloc_mu);
+    --g_alloc_live;
+  }
+  return cudaFree(p);
+}
 
 void sgm_set_process_error(const char* msg) { set_error(nullptr, "%s", msg); }
 
@@ -192,7 +225,7 @@ struct sgm_engine {
     for (int i = 0; i < 2; ++i) {
       dfree(img[i]);
       dfree(init[i]);
-      if (cs[i]) cudaFree(cs[i]);
+      if (cs[i]) sgm_dev_free(cs[i]);
       cs[i] = nullptr;
     }
     if (own_volumes) {
@@ -309,7 +342,7 @@ int engine_init(sgm_engine* e, int W, int H, int M, int D, const sgm_option_t* o
   const size_t V = e->vol() * e->nviews();  // the right view's volumes only with the LR check
   for (int i = 0; i < 2; ++i) {
     SGM_CUDA_TRY(e, dalloc(&e->img[i], N));
-    SGM_CUDA_TRY(e, cudaMalloc(&e->cs[i], N * 8));
+    SGM_CUDA_TRY(e, sgm_dev_malloc(&e->cs[i], N * 8));
     SGM_CUDA_TRY(e, dalloc(&e->init[i], N));
   }
   if (volumes) {
@@ -462,6 +495,7 @@ int launch_plain(sgm_engine* e, const Word* csl, const Word* csr, float* wta) {
   Q.rows = warp_kernel ? (e->H / 2) * 2 : e->H;
   Q.dmax_excl = warp_kernel ? 32 * K : 32 * K - 1;
   Q.dstride = e->npix();
+  Q.image_border(e->W, e->H);
   if ((e->tune_row_kernel == 3 || e->tune_row_kernel == 0) && v3_ok) {
     dim3 cg((e->W + 127) / 128, e->H, nv);
     st = SGM_LAUNCH(e, e->stream, "cost", sgm::k_cost3<K, Word><<<cg, 128, 0, e->stream>>>(csl, csr, e->cost, P));
@@ -516,6 +550,125 @@ int launch_plain(sgm_engine* e, const Word* csl, const Word* csr, float* wta) {
   dim3 vg((e->W + C - 1) / C, nv), vb(32, C);
   return SGM_LAUNCH(e, e->stream, "vpaths_wta_plain",
                     vk<<<vg, vb, vsmem, e->stream>>>(e->cost, e->lr, e->rl, e->bt, wta, P, Q, bt_smem));
+}
+
+// ------------------------------------------------------------------------------------------
+// Regions of interest (StereoCuda::Match with StereoROI_T; reference: cost cusgm_cc.cu:478-488,
+// scans cusgm_ca.cu:3991-3999 and :4179-4192, WTA grid :4139-4165, small-region strips
+// StereoCudaImpl.cpp:463-498). A view's region is matched as a sub-image of its own: its cost
+// (partners from the whole image) goes into a compact [h][w][D] sub-volume, the thread-per-scanline
+// scans and WTA run on it with the image border shifted, and the region's map is scattered into the
+// view's full map, INVALID outside.
+// ------------------------------------------------------------------------------------------
+struct RoiRegion {
+  int x0, y0, w, h;  // columns [x0, x0 + w), rows [y0, y0 + h)
+  int bx;            // first column of the cost kernel's D-pixel blocks (the ROI's own x)
+};
+
+// Regions of both views. Without an ROI a view covers columns [max(0, min_disp), W) and every
+// row; with one, its rectangle (which must lie inside the image), columns clipped to start at
+// max(0, min_disp): the reference computes the left view's cost without the ROI, from that column.
+int roi_regions(sgm_engine* e, const sgm_roi_t* roi_l, const sgm_roi_t* roi_r, RoiRegion reg[2]) {
+  const int x0 = std::max(0, e->M);
+  for (int v = 0; v < 2; ++v) {
+    const sgm_roi_t* r = v == 0 ? roi_l : roi_r;
+    reg[v] = RoiRegion{x0, 0, e->W - x0, e->H, x0};
+    if (!r) continue;
+    if (r->x < 0 || r->y < 0 || r->w <= 0 || r->h <= 0 || r->x > e->W - r->w || r->y > e->H - r->h) {
+      set_error(&e->err, "ROI (%d, %d, %d, %d) does not lie inside the %dx%d image", r->x, r->y, r->w, r->h, e->W,
+                e->H);
+      return SGM_ERR_ARG;
+    }
+    const int c0 = std::max(r->x, x0);
+    if (c0 >= r->x + r->w) {
+      set_error(&e->err, "ROI (%d, %d, %d, %d) has no column at or right of the minimum disparity %d", r->x, r->y,
+                r->w, r->h, e->M);
+      return SGM_ERR_ARG;
+    }
+    reg[v] = RoiRegion{c0, r->y, r->x + r->w - c0, r->h, r->x};
+  }
+  return SGM_OK;
+}
+
+template <int K>
+int roi_rows(sgm_engine* e, int G, const uint8_t* cost, uint8_t* lr, uint8_t* rl, const sgm::PlainParams& P,
+             cudaStream_t s) {
+  if (!lanes_ok<K>(G)) G = kDefaultRowLanes;
+  const int blocks = (int)((2L * P.H * G + 127) / 128);
+  auto go = [&](auto kern) {
+    return SGM_LAUNCH(e, s, "hpaths_roi", kern<<<blocks, 128, 0, s>>>(cost, lr, rl, P, 1));
+  };
+  if constexpr (K == 4) {
+    return G == 2 ? go(sgm::k_hpaths3<K, 2, pf3<K, 2>()>) : go(sgm::k_hpaths3<K, 4, pf3<K, 4>()>);
+  } else {
+    switch (G) {
+      case 1: return go(sgm::k_hpaths3<K, 1, pf3<K, 1>()>);
+      case 4: return go(sgm::k_hpaths3<K, 4, pf3<K, 4>()>);
+      case 8: return go(sgm::k_hpaths3<K, 8, pf3<K, 8>()>);
+      default: return go(sgm::k_hpaths3<K, 2, pf3<K, 2>()>);
+    }
+  }
+}
+
+template <int K>
+int roi_cols(sgm_engine* e, int G, const uint8_t* cost, const uint8_t* lr, const uint8_t* rl, uint8_t* bt,
+             float* wta, const sgm::PlainParams& P, const sgm::WtaParams& Q, cudaStream_t s) {
+  if (!lanes_ok<K>(G)) G = kDefaultColLanes;
+  const dim3 grid((unsigned)(((long)P.W * G + 127) / 128), 1);
+  const size_t smem = (size_t)(128 / G) * sgm::vpaths3_col_smem<K>();
+  auto go = [&](auto kern) {
+    return SGM_LAUNCH(e, s, "vpaths_wta_roi", kern<<<grid, 128, smem, s>>>(cost, lr, rl, bt, wta, P, Q));
+  };
+  if constexpr (K == 4) {
+    return G == 2 ? go(sgm::k_vpaths3<K, 2, pf3v<K, 2>(), 0>) : go(sgm::k_vpaths3<K, 4, pf3v<K, 4>(), 0>);
+  } else {
+    switch (G) {
+      case 1: return go(sgm::k_vpaths3<K, 1, pf3v<K, 1>(), 0>);
+      case 2: return go(sgm::k_vpaths3<K, 2, pf3v<K, 2>(), 0>);
+      case 8: return go(sgm::k_vpaths3<K, 8, pf3v<K, 8>(), 0>);
+      default: return go(sgm::k_vpaths3<K, 4, pf3v<K, 4>(), 0>);
+    }
+  }
+}
+
+// Cost, scans and WTA of each view's region, scattered into wta (view v at wta + v * W * H).
+template <int K, typename Word>
+int launch_roi(sgm_engine* e, const Word* csl, const Word* csr, const RoiRegion reg[2], float* wta) {
+  constexpr int D = 32 * K;
+  cudaStream_t s = e->stream;
+  const size_t V = e->vol(), N = e->npix();
+  sgm::PlainParams Pg;  // whole-image geometry for the cost kernel
+  Pg.W = e->W; Pg.H = e->H; Pg.min_d = e->M; Pg.x0 = std::max(0, e->M);
+  Pg.p1 = (uint32_t)e->opt.p1; Pg.p2 = (uint32_t)e->opt.p2_init;
+  Pg.vstride = V;
+  for (int v = 0; v < e->nviews(); ++v) {
+    const RoiRegion& r = reg[v];
+    uint8_t* cost = e->cost + v * V;
+    uint8_t* lr = e->lr + v * V;
+    uint8_t* rl = e->rl + v * V;
+    uint8_t* bt = e->bt + v * V;
+    float* region_map = v == 0 ? e->post : e->post2;
+    int st = SGM_LAUNCH(e, s, "cost_roi", sgm::k_cost_roi<K, Word><<<dim3((r.w + 127) / 128, r.h), 128, 0, s>>>(
+                                              csl, csr, cost, Pg, v, r.x0, r.y0, r.w, r.bx));
+    if (st) return st;
+    sgm::PlainParams P = Pg;  // the region as a sub-image
+    P.W = r.w; P.H = r.h; P.x0 = 0;
+    P.vstride = (size_t)r.w * r.h * D;
+    if ((st = roi_rows<K>(e, e->tune_row_lanes, cost, lr, rl, P, s))) return st;
+    sgm::WtaParams Q;
+    Q.uniqueness = e->opt.unique_threshold;
+    Q.tie_rule = e->ext.tie_rule;
+    Q.rows = (r.h / 2) * 2;  // the reference's WTA launch: floor(h/2) blocks of two rows from the ROI's y
+    Q.dmax_excl = D;
+    Q.dstride = (size_t)r.w * r.h;
+    Q.image_border(e->W, e->H, r.x0, r.y0);
+    if ((st = roi_cols<K>(e, e->tune_col_lanes, cost, lr, rl, bt, region_map, P, Q, s))) return st;
+    st = SGM_LAUNCH(e, s, "roi_scatter", sgm::k_roi_scatter<<<dim3((e->W + 127) / 128, e->H), 128, 0, s>>>(
+                                             region_map, wta + v * N, e->W, e->H, r.x0, r.y0, r.w, r.h));
+    if (st) return st;
+  }
+  e->bt_stored = true;
+  return SGM_OK;
 }
 
 // Initial-disparity levels, thread-per-scanline kernels (uint32 per disparity): G = 2, 4 or 8.
@@ -577,6 +730,7 @@ int launch_init(sgm_engine* e, const Word* csl, const Word* csr, const int16_t* 
   Q3.rows = (e->H / 4) * 4;
   Q3.dmax_excl = sgm::kLevelRange - 1;
   Q3.dstride = e->npix();
+  Q3.image_border(e->W, e->H);
   // thread-per-scanline kernels: uint32 arithmetic (exact for any penalties); WTA rules 0 and 4
   const bool v3_ok = e->ext.init_tie_rule == sgm::kTieLowest || e->ext.init_tie_rule == sgm::kTieRefB200;
   const bool rows3 = v3_ok && (e->tune_row_kernel == 0 || e->tune_row_kernel == 3);
@@ -627,6 +781,7 @@ int launch_init(sgm_engine* e, const Word* csl, const Word* csr, const int16_t* 
   Q.rows = (e->H / 4) * 4;
   Q.dmax_excl = sgm::kLevelRange - 1;
   Q.dstride = e->npix();
+  Q.image_border(e->W, e->H);
   int C = 8, bt_smem = 0;
   size_t vsmem = 0;
   if (cols3) return init3_cols<0>(e, il, ir, wta, P, Q3, e->stream);
@@ -647,11 +802,32 @@ int launch_init(sgm_engine* e, const Word* csl, const Word* csr, const int16_t* 
 }
 
 // Enqueues one full match of this level on s. Inputs/outputs are dense device arrays.
+// roi_l / roi_r: regions of interest of the views (NULL: the whole view), plain levels only.
 int engine_enqueue(sgm_engine* e, const uint8_t* dl_img, const uint8_t* dr_img, const int16_t* dinit, float* dout,
-                   float* dout_r, cudaStream_t s) {
+                   float* dout_r, cudaStream_t s, const sgm_roi_t* roi_l = nullptr,
+                   const sgm_roi_t* roi_r = nullptr) {
   if (!e->ready) {
     set_error(&e->err, "matcher not initialised");
     return SGM_ERR_STATE;
+  }
+  if (!e->opt.do_lr_check) roi_r = nullptr;  // no right view is matched (the reference ignores it too)
+  const bool roi = roi_l || roi_r;
+  RoiRegion reg[2];
+  if (roi) {
+    if (dinit) {
+      set_error(&e->err, "ROI matching at initial-disparity levels is not supported (the reference's pyramid "
+                         "never passes an ROI: is_using_roi is false, FasterStereoCuda.cpp:575)");
+      return SGM_ERR_UNSUPPORTED;
+    }
+    const bool v3_ok = e->D <= 128 && e->opt.p1 <= (int)sgm::kMaxPenalty16 &&
+                       e->opt.p2_init <= (int)sgm::kMaxPenalty16 && e->opt.p2_init >= e->opt.p1 &&
+                       (e->ext.tie_rule == sgm::kTieLowest || e->ext.tie_rule == sgm::kTieRefB200);
+    if (!v3_ok) {
+      set_error(&e->err, "ROI matching needs D <= 128, P1 <= P2 <= %u and tie rule 0 or 4", sgm::kMaxPenalty16);
+      return SGM_ERR_UNSUPPORTED;
+    }
+    const int rs = roi_regions(e, roi_l, roi_r, reg);
+    if (rs) return rs;
   }
   if (dinit && e->D != sgm::kLevelRange) {
     set_error(&e->err, "initial disparities need a disparity range of %d (got %d)", sgm::kLevelRange, e->D);
@@ -705,7 +881,17 @@ int engine_enqueue(sgm_engine* e, const uint8_t* dl_img, const uint8_t* dr_img, 
   // cost + four paths + WTA, both views
   if (!st) {
     const bool w64 = e->opt.cs_type == 1;
-    if (dinit) {
+    if (roi) {
+      const auto* l64 = (const uint64_t*)e->cs[0];
+      const auto* r64 = (const uint64_t*)e->cs[1];
+      const auto* l32 = (const uint32_t*)e->cs[0];
+      const auto* r32 = (const uint32_t*)e->cs[1];
+      switch (e->D) {
+        case 32: st = w64 ? launch_roi<1>(e, l64, r64, reg, e->wta) : launch_roi<1>(e, l32, r32, reg, e->wta); break;
+        case 64: st = w64 ? launch_roi<2>(e, l64, r64, reg, e->wta) : launch_roi<2>(e, l32, r32, reg, e->wta); break;
+        default: st = w64 ? launch_roi<4>(e, l64, r64, reg, e->wta) : launch_roi<4>(e, l32, r32, reg, e->wta); break;
+      }
+    } else if (dinit) {
       st = w64 ? launch_init<uint64_t>(e, (const uint64_t*)e->cs[0], (const uint64_t*)e->cs[1], dinit, dinit_r, e->wta)
                : launch_init<uint32_t>(e, (const uint32_t*)e->cs[0], (const uint32_t*)e->cs[1], dinit, dinit_r, e->wta);
     } else {
@@ -785,20 +971,27 @@ int engine_enqueue(sgm_engine* e, const uint8_t* dl_img, const uint8_t* dr_img, 
   }
   if (!st && peaks) {
     const int strips = e->ext.peaks_strips > 0 ? e->ext.peaks_strips : default_peaks_strips();
-    const int tiles = H / strips;
+    // strips of floor(h / strips) rows from the ROI's first row, or from row 0 (StereoCudaImpl.cpp:
+    // 463-498); they are labelled as a sub-image of the rows they cover
+    const int y_off = roi_l ? roi_l->y : 0, Hs = roi_l ? roi_l->h : H;
+    float* dsub = dout + (size_t)y_off * W;
+    const size_t Ns = (size_t)W * Hs;
+    const int tiles = Hs / strips;
     if (tiles > 0) {
       const int rows = strips * tiles;
-      const unsigned nb = (unsigned)((N + 255) / 256);
-      st = SGM_LAUNCH(e, e->stream, "cc_rows", sgm::k_cc_rows<<<(H + 7) / 8, dim3(32, 8), 0, e->stream>>>(
-                                                   dout, e->label, e->count, W, H, rows, e->ext.peaks_abs_mode));
+      const unsigned nb = (unsigned)((Ns + 255) / 256);
+      st = SGM_LAUNCH(e, e->stream, "cc_rows", sgm::k_cc_rows<<<(Hs + 7) / 8, dim3(32, 8), 0, e->stream>>>(
+                                                   dsub, e->label, e->count, W, Hs, rows, e->ext.peaks_abs_mode));
       if (!st && tiles > 1)
         st = SGM_LAUNCH(e, e->stream, "cc_vert", sgm::k_cc_vert<<<nb, 256, 0, e->stream>>>(
-                                                     dout, e->label, W, H, tiles, rows, e->ext.peaks_abs_mode));
+                                                     dsub, e->label, W, Hs, tiles, rows, e->ext.peaks_abs_mode));
       if (!st)
-        st = SGM_LAUNCH(e, e->stream, "cc_count", sgm::k_cc_count<<<nb, 256, 0, e->stream>>>(e->label, e->count, (int)N));
+        st = SGM_LAUNCH(e, e->stream, "cc_count", sgm::k_cc_count<<<nb, 256, 0, e->stream>>>(e->label, e->count,
+                                                                                               (int)Ns));
       if (!st)
         st = SGM_LAUNCH(e, e->stream, "cc_filter", sgm::k_cc_filter<<<nb, 256, 0, e->stream>>>(
-                                                       dout, e->label, e->count, W, H, tiles, e->opt.peaks_ratio_threshold));
+                                                       dsub, e->label, e->count, W, Hs, tiles,
+                                                       e->opt.peaks_ratio_threshold));
     }
   }
   e->depth_src = (!peaks && ((pf != 0) != (morph != 0))) ? agg : dout;
@@ -897,21 +1090,21 @@ struct sgm_pyramid {
     drop_graph();
     if (done) cudaEventDestroy(done);
     done = nullptr;
-    if (disp0) cudaFree(disp0);
+    if (disp0) sgm_dev_free(disp0);
     disp0 = nullptr;
     depth_mode = false;
     for (auto* e : lv) {
       if (e) { e->free_all(); delete e; }
     }
     lv.clear();
-    for (auto* p : imgs_l) if (p) cudaFree(p);
-    for (auto* p : imgs_r) if (p) cudaFree(p);
-    for (auto* p : disp) if (p) cudaFree(p);
-    for (auto* p : init) if (p) cudaFree(p);
+    for (auto* p : imgs_l) if (p) sgm_dev_free(p);
+    for (auto* p : imgs_r) if (p) sgm_dev_free(p);
+    for (auto* p : disp) if (p) sgm_dev_free(p);
+    for (auto* p : init) if (p) sgm_dev_free(p);
     imgs_l.clear(); imgs_r.clear(); disp.clear(); init.clear();
-    if (in_l) cudaFree(in_l);
-    if (in_r) cudaFree(in_r);
-    if (out) cudaFree(out);
+    if (in_l) sgm_dev_free(in_l);
+    if (in_r) sgm_dev_free(in_r);
+    if (out) sgm_dev_free(out);
     in_l = in_r = nullptr;
     out = nullptr;
     if (stream) cudaStreamDestroy(stream);
@@ -1112,10 +1305,6 @@ int sgm_match(sgm_handle_t h, const uint8_t* img_left, const uint8_t* img_right,
     set_error(&h->err, "matcher not initialised");
     return SGM_ERR_STATE;
   }
-  if (roi_left || roi_right) {
-    set_error(&h->err, "ROI matching is not supported");
-    return SGM_ERR_UNSUPPORTED;
-  }
   const size_t N = h->npix();
   h->launches = 0;
   SGM_CUDA_TRY(h, cudaMemcpyAsync(h->img[0], img_left, N, cudaMemcpyHostToDevice, h->stream));
@@ -1123,10 +1312,11 @@ int sgm_match(sgm_handle_t h, const uint8_t* img_left, const uint8_t* img_right,
   if (init_disp_left)
     SGM_CUDA_TRY(h, cudaMemcpyAsync(h->init[0], init_disp_left, N * sizeof(int16_t), cudaMemcpyHostToDevice, h->stream));
   const bool right = disp_right && h->opt.do_lr_check;
-  int st = (!init_disp_left && !right)
+  const bool roi = roi_left || (roi_right && h->opt.do_lr_check);
+  int st = (!init_disp_left && !right && !roi)
                ? engine_run(h, h->img[0], h->img[1], h->out, h->stream)
                : engine_enqueue(h, h->img[0], h->img[1], init_disp_left ? h->init[0] : nullptr, h->out,
-                                right ? h->dr_out : nullptr, h->stream);
+                                right ? h->dr_out : nullptr, h->stream, roi_left, roi_right);
   if (st) return st;
   SGM_CUDA_TRY(h, cudaMemcpyAsync(disp_left, h->out, N * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
   if (disp_right && h->opt.do_lr_check)
@@ -1171,17 +1361,14 @@ int sgm_match2(sgm_handle_t h, const uint8_t* img_left, const uint8_t* img_right
     return SGM_ERR_STATE;
   }
   if (!img_left || !img_right || !depth_left) return SGM_ERR_ARG;
-  if (roi_left || roi_right) {
-    set_error(&h->err, "ROI matching is not supported");
-    return SGM_ERR_UNSUPPORTED;
-  }
   const size_t N = h->npix();
   h->launches = 0;
   SGM_CUDA_TRY(h, cudaMemcpyAsync(h->img[0], img_left, N, cudaMemcpyHostToDevice, h->stream));
   SGM_CUDA_TRY(h, cudaMemcpyAsync(h->img[1], img_right, N, cudaMemcpyHostToDevice, h->stream));
   if (init_disp_left)
     SGM_CUDA_TRY(h, cudaMemcpyAsync(h->init[0], init_disp_left, N * sizeof(int16_t), cudaMemcpyHostToDevice, h->stream));
-  int st = engine_enqueue(h, h->img[0], h->img[1], init_disp_left ? h->init[0] : nullptr, h->out, nullptr, h->stream);
+  int st = engine_enqueue(h, h->img[0], h->img[1], init_disp_left ? h->init[0] : nullptr, h->out, nullptr, h->stream,
+                          roi_left, roi_right);
   // the depth source is the final map, the LR / median output or the WTA map, never h->post
   if (!st) st = enqueue_depth(h, h->depth_src, h->post, h->cam, h->stream);
   if (st) return st;
@@ -1291,6 +1478,17 @@ int sgm_debug_read(sgm_handle_t h, int32_t which, int32_t view, void* dst, size_
   return cudaMemcpy(dst, src, n, cudaMemcpyDeviceToHost) == cudaSuccess ? SGM_OK : SGM_ERR_CUDA;
 }
 
+int sgm_debug_fail_device_alloc(int64_t after) {
+  std::lock_guard<std::mutex> lk(g_alloc_mu);
+  g_alloc_fail_after = after < 0 ? -1 : after;
+  return SGM_OK;
+}
+
+int64_t sgm_debug_live_device_allocations(void) {
+  std::lock_guard<std::mutex> lk(g_alloc_mu);
+  return g_alloc_live;
+}
+
 int sgm_profile_enable(int32_t enable) {
   std::lock_guard<std::mutex> lk(g_prof_mu);
   g_prof.collect();
@@ -1365,18 +1563,19 @@ int sgm_pyr_init(sgm_pyr_handle_t h, const sgm_pyr_option1_t* o, const sgm_level
     }
     const size_t n = (size_t)w * hh;
     if (i > 0) {
-      if (cudaMalloc(&h->imgs_l[i], n) || cudaMalloc(&h->imgs_r[i], n) || cudaMalloc(&h->disp[i], n * sizeof(float))) {
+      if (sgm_dev_malloc(&h->imgs_l[i], n) || sgm_dev_malloc(&h->imgs_r[i], n) ||
+          sgm_dev_malloc(&h->disp[i], n * sizeof(float))) {
         h->free_all();
         return SGM_ERR_NOMEM;
       }
     }
-    if (i < L - 1 && cudaMalloc(&h->init[i], n * sizeof(int16_t))) {
+    if (i < L - 1 && sgm_dev_malloc(&h->init[i], n * sizeof(int16_t))) {
       h->free_all();
       return SGM_ERR_NOMEM;
     }
   }
   const size_t N = (size_t)o->width * o->height;
-  if (cudaMalloc(&h->in_l, N) || cudaMalloc(&h->in_r, N) || cudaMalloc(&h->out, N * sizeof(float))) {
+  if (sgm_dev_malloc(&h->in_l, N) || sgm_dev_malloc(&h->in_r, N) || sgm_dev_malloc(&h->out, N * sizeof(float))) {
     h->free_all();
     return SGM_ERR_NOMEM;
   }
@@ -1466,7 +1665,7 @@ int sgm_pyr_init2(sgm_pyr_handle_t h, const sgm_pyr_option2_t* o, const sgm_leve
   h->cam0.y0_right = o->epi.y0_right;
   h->cam0.focus = o->epi.focus;
   h->cam0.baseline = o->epi.baseline;
-  if (cudaMalloc(&h->disp0, (size_t)o->width * o->height * sizeof(float)) != cudaSuccess) {
+  if (sgm_dev_malloc(&h->disp0, (size_t)o->width * o->height * sizeof(float)) != cudaSuccess) {
     h->free_all();
     return SGM_ERR_NOMEM;
   }

@@ -474,6 +474,17 @@ struct WtaParams {
   int rows;        // rows the reference's WTA launch covers
   int dmax_excl;   // d* must be < dmax_excl (D for the warp kernels, D-1 for the generic one)
   size_t dstride;  // elements between the views of the disparity maps (H*W)
+  // Pixels the thread-per-scanline WTA may make valid: x in [xlo, xhi], y in [ylo, yhi], in the
+  // launch's coordinates. The reference's border (x < 5, y < 5, x > W-5, y > H-5 INVALID,
+  // cusgm_ca.cu:3630) is in image coordinates; a region of interest scanned as its own sub-image
+  // starting at (gx, gy) shifts it.
+  int xlo, xhi, ylo, yhi;
+  __host__ __device__ void image_border(int W, int H, int gx = 0, int gy = 0) {
+    xlo = 5 - gx;
+    xhi = W - 5 - gx;
+    ylo = 5 - gy;
+    yhi = H - 5 - gy;
+  }
 };
 
 // Winner-take-all + uniqueness + subpixel on the summed path costs of one pixel.

@@ -251,6 +251,77 @@ __global__ void __launch_bounds__(128) k_cost3(const Word* __restrict__ cs_l, co
 }
 
 // ---------------------------------------------------------------------------------------------
+// Regions of interest (StereoCuda::Match with StereoROI_T). A view's region -- columns
+// [rx0, rx0 + rw), rows [ry0, ry0 + rh) -- is matched as a sub-image of its own: its cost is
+// stored compactly as [rh][rw][D] and the scan kernels run on that sub-volume, so every path
+// starts at the region's edge as the reference's ROI scans do (xoffset / xEnd / yoffset / yend,
+// cusgm_ca.cu:1478-1598 launched at :3991-3999).
+// ---------------------------------------------------------------------------------------------
+// Costs of 128 region pixels of one row (partners from the whole image, as in the full volume:
+// cusgm_cc.cu:118-172 / 238-293 with the ROI offsets of :478-488). 5x5 census, view 1: the last
+// pixel of every D-pixel block counted from the ROI's x (bx) is not written by the reference's
+// right-view kernel, so it keeps the left view's cost there (cusgm_cc.cu:288).
+template <int K, typename Word>
+__global__ void __launch_bounds__(128) k_cost_roi(const Word* __restrict__ cs_l, const Word* __restrict__ cs_r,
+                                                  uint8_t* __restrict__ cost, PlainParams P, int view, int rx0,
+                                                  int ry0, int rw, int bx) {
+  constexpr int D = 32 * K;
+  __shared__ Word win[128 + D];
+  const int W = P.W;
+  const int y = ry0 + blockIdx.y;
+  const int xb = rx0 + blockIdx.x * 128;
+  const Word* own = (view == 0 ? cs_l : cs_r) + (size_t)y * W;
+  const Word* oth = (view == 0 ? cs_r : cs_l) + (size_t)y * W;
+  const Word oth0 = oth[0];
+  const int ws = view == 0 ? xb - P.min_d - (D - 1) : xb + P.min_d;
+  for (int i = threadIdx.x; i < 128 + D - 1; i += 128) {
+    const int pos = ws + i;
+    win[i] = (pos >= 0 && pos < W) ? oth[pos] : oth0;
+  }
+  __syncthreads();
+  const int xr = blockIdx.x * 128 + threadIdx.x;  // column inside the region
+  if (xr >= rw) return;
+  const int x = rx0 + xr;
+  uint8_t* out = cost + ((size_t)blockIdx.y * rw + xr) * D;
+  bool lr_cost = false;
+  if (view == 1 && sizeof(Word) == 4) {
+    const int blk = bx + ((x - bx) / D) * D;
+    lr_cost = (x == blk + min(D, W - blk) - 1);
+  }
+  if (!lr_cost) {
+    if (view == 0) cost3_px<D, Word, -1>(own[x], win + threadIdx.x + (D - 1), out);
+    else cost3_px<D, Word, 1>(own[x], win + threadIdx.x, out);
+  } else {  // the left view's cost of this pixel
+    const Word* g_r = cs_r + (size_t)y * W;
+    const Word r0 = g_r[0];
+    const Word l = cs_l[(size_t)y * W + x];
+    for (int v = 0; v < D / 16; ++v) {
+      uint32_t q[4];
+      for (int j = 0; j < 4; ++j) {
+        uint32_t packed = 0;
+        for (int b = 0; b < 4; ++b) {
+          const int pos = x - P.min_d - (16 * v + 4 * j + b);
+          packed |= popc_word((Word)(l ^ ((pos >= 0 && pos < W) ? g_r[pos] : r0))) << (8 * b);
+        }
+        q[j] = packed;
+      }
+      reinterpret_cast<uint4*>(out)[v] = make_uint4(q[0], q[1], q[2], q[3]);
+    }
+  }
+}
+
+// Full disparity map of a view from its region's map: the region's values, INVALID elsewhere.
+static __global__ void k_roi_scatter(const float* __restrict__ region, float* __restrict__ full, int W, int H,
+                                     int rx0, int ry0, int rw, int rh) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= W) return;
+  const int xr = x - rx0, yr = y - ry0;
+  const bool in = xr >= 0 && xr < rw && yr >= 0 && yr < rh;
+  full[(size_t)y * W + x] = in ? region[(size_t)yr * rw + xr] : kInvalidFloat;
+}
+
+// ---------------------------------------------------------------------------------------------
 // Horizontal paths, G threads per scanline (view, direction, row): scanline index i -> group
 // i / H (view = group >> 1, dir = group & 1), y = i % H. Reads the cost volume, writes the
 // left-to-right (dir 0) or right-to-left (dir 1) path volume; the cost of step s + PF is loaded
@@ -342,7 +413,7 @@ __device__ __forceinline__ void vpaths3_lane(const uint8_t* __restrict__ cost, c
   const bool valid = xc < W;
   const int x = valid ? xc : W - 1;            // idle lanes follow the last column, without stores
   const bool computed = valid && x >= P.x0;    // columns left of x0 are INVALID
-  const bool col_ok = computed && x >= 5 && x <= W - 5;
+  const bool col_ok = computed && x >= Q.xlo && x <= Q.xhi;
   float* dout = disp + (size_t)view * Q.dstride + x;
   const size_t vo = (size_t)view * P.vstride + (size_t)x * D + (size_t)g * SB;
   const size_t rs = (size_t)W * D;
@@ -404,7 +475,7 @@ __device__ __forceinline__ void vpaths3_lane(const uint8_t* __restrict__ cost, c
             ld_slice<NR>(rlv + o, re[j]);
           }
           m = y == 0 ? first_g<NT, G>(L, c) : step_g<NT, G>(L, c, m, p1x2, p2m1, g);
-          if (y >= 5 && y <= H - 5 && y < Q.rows) {  // uniform over the warp
+          if (y >= Q.ylo && y <= Q.yhi && y < Q.rows) {  // uniform over the warp
             // S = the four u8 path costs summed (< 1024). Keys S << 6 | (d mod 64) per block of
             // disparities: D = 32 one block; D = 64: d < 32 (A) and d >= 32 (B), the reference's two
             // stores; D = 128: d < 64 and d >= 64.

@@ -149,6 +149,7 @@ int run(const uint8_t* dl, const uint8_t* dr, float* dout, int W, int H, int M, 
   Q.rows = (H / 2) * 2;
   Q.dmax_excl = D;
   Q.dstride = N;
+  Q.image_border(W, H);
   sgm::k_vpaths_wta_plain<K><<<dim3((W + 7) / 8, nv), dim3(32, 8), 0, s>>>(cost, lr, rl, bt, wta, P, Q);
   if ((st = launched("column scans"))) return st;
   const bool lrc = o->do_lr_check, med = o->do_median_filter;

@@ -159,6 +159,16 @@ SGM_API int64_t sgm_kernel_launches(sgm_handle_t h);
  * `bytes` must equal the buffer size. Synchronises the handle's stream. */
 SGM_API int sgm_debug_read(sgm_handle_t h, int32_t which, int32_t view, void* dst, size_t bytes);
 
+/* No counterpart in the reference: fault injection for tests of the out-of-memory paths. After
+ * sgm_debug_fail_device_alloc(n) the engine's (n+1)-th device allocation from then on fails as
+ * cudaMalloc does when the device is out of memory (once; n < 0 disarms). The reference's Init
+ * returns false when an allocation fails (SgmStereoCuda/StereoCudaImpl.cpp:138-207); sgm_init,
+ * sgm_pyr_init, sgm_init2, sgm_pyr_init2, sgm_batch_init and sgm_batch_pyr_init return SGM_ERR_NOMEM
+ * and free what they had allocated. sgm_debug_live_device_allocations counts the engine's device
+ * allocations that are currently held (process-wide). */
+SGM_API int sgm_debug_fail_device_alloc(int64_t after);
+SGM_API int64_t sgm_debug_live_device_allocations(void);
+
 /* No counterpart in the reference: per-kernel timing with CUDA events recorded on the launching
  * stream around every launch of every handle in the process. Enabling resets the counters. */
 SGM_API int sgm_profile_enable(int32_t enable);

@@ -69,6 +69,8 @@ def ref_lib():
     lib.ref_match2.restype = C.c_int
     lib.ref_pyr_match2.argtypes = [C.c_int, C.c_int, C.c_float, C.c_float, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp]
     lib.ref_pyr_match2.restype = C.c_int
+    lib.ref_match_roi_dump.argtypes = [C.POINTER(RefCase), vp, vp, vp, vp, vp, vp, vp, vp, vp]
+    lib.ref_match_roi_dump.restype = C.c_int
     return lib
 
 
@@ -136,6 +138,40 @@ def cases():
 # single-level cases whose final map comes from a post filter (compared within FILTER_TOL of the
 # reference's map on the CPU: the oracle's expf/exp are the C library's, the reference's CUDA's)
 FILTER_CASES = ("gauss_only", "bilateral_only", "gauss_erosion", "bilateral_close")
+
+
+# Matches with regions of interest (StereoCuda::Match with StereoROI_T, cusgm_cc.cu:478-488,
+# cusgm_ca.cu:3991-3999 / 4139-4165 / 4173-4192): name -> (seed, case fields, left ROI, right ROI),
+# rectangles (x, y, w, h) inside the image with widths a multiple of 4 (see ref_match_roi_dump)
+ROI_CASES = {
+    "roi9x7": (31, dict(width=162, height=120, cs_type=1, p1=10, p2=150), (20, 16, 100, 80), (8, 10, 120, 90)),
+    "roi5x5": (32, dict(width=162, height=120, cs_type=0, p1=8, p2=32), (12, 5, 136, 99), (4, 7, 140, 101)),
+}
+
+
+def roi_region(roi, min_disp):
+    """Columns [x0, x1) and rows [y0, y1) of a view's region (columns start at max(0, min_disp))."""
+    x, y, w, h = roi
+    return max(x, max(0, min_disp)), x + w, y, y + h
+
+
+def roi_masks(W, H, roi, min_disp):
+    """(paths mask [4][H][W], WTA mask [H][W]) of the pixels a region's dumps are compared on: its
+    path values except each path's first pixel (the reference never stores it, so the WTA reads
+    what the buffer held there), and the pixels its WTA writes away from those first lines."""
+    x0, x1, y0, y1 = roi_region(roi, min_disp)
+    reg = np.zeros((H, W), bool)
+    reg[y0:y1, x0:x1] = True
+    first = np.zeros((4, H, W), bool)
+    first[0, y0, x0:x1] = True        # top -> bottom
+    first[1, y0:y1, x0] = True        # left -> right
+    first[2, y1 - 1, x0:x1] = True    # bottom -> top
+    first[3, y0:y1, x1 - 1] = True    # right -> left
+    paths = np.broadcast_to(reg, (4, H, W)) & ~first
+    wta = np.zeros((H, W), bool)
+    wta[y0:y0 + ((y1 - y0) // 2) * 2, x0:x1] = True
+    wta &= ~first.any(0)
+    return paths, wta
 
 
 # name: (seed, width, height, min_disp, max_disp, layers, lr check, small-region removal)
@@ -242,6 +278,24 @@ def refdump(out_dir: Path, only=None):
             np.savez_compressed(out_dir / f"levels_{name}.npz", left=L, right=R, disp_levels=dl, init_levels=il,
                                 case=np.array(json.dumps(dict(width=w, height=h, min_disp=dmin, max_disp=dmax,
                                                               num_layers=layers, lr=lr, peaks=pk))))
+    base = dict(min_disp=0, disp_range=64, uniqueness=0.95, do_lr_check=1, lr_threshold=1.0, do_median=0,
+                morphology=0, do_remove_peaks=0, peaks_ratio=0.0005, post_filter=0)
+    for name, (seed, f, rl, rr) in ROI_CASES.items():
+        if only and name not in only:
+            continue
+        f = dict(base, **f)
+        W, H, D = f["width"], f["height"], f["disp_range"]
+        L, R, _ = scenes.planar_pair(seed, W, H)
+        arr = dict(cost_lr=np.zeros((H, W, D), np.uint8), paths_lr=np.zeros((4, H, W, D), np.uint8),
+                   wta_l=np.zeros((H, W), np.float32), cost_rl=np.zeros((H, W, D), np.uint8),
+                   paths_rl=np.zeros((4, H, W, D), np.uint8))
+        a_l, a_r = np.array(rl, np.int32), np.array(rr, np.int32)
+        rc = lib.ref_match_roi_dump(C.byref(RefCase(**f)), _p(L), _p(R), _p(a_l), _p(a_r), _p(arr["cost_lr"]),
+                                    _p(arr["paths_lr"]), _p(arr["wta_l"]), _p(arr["cost_rl"]), _p(arr["paths_rl"]))
+        print(name, "rc", rc, lib.ref_last_message().decode(), flush=True)
+        if rc == 0:
+            np.savez_compressed(out_dir / f"{name}.npz", left=L, right=R, roi_l=a_l, roi_r=a_r,
+                                case=np.array(json.dumps(f)), **arr)
     cam = np.array(CAM, np.float64)
     all_cases = cases()
     for base_name in DEPTH_CASES:
@@ -376,6 +430,47 @@ def oracle_depth(z, case, peaks_strips):
     return O.depth_from_disp(d, cam[0], cam[2], cam[4], cam[5]), rows
 
 
+def roi_oracle(z, case):
+    """The oracle's left and right views of a ROI case (LR check on, median off)."""
+    cfg = O.Config(width=case["width"], height=case["height"], min_disp=case["min_disp"],
+                   disp_range=case["disp_range"], cs_type=case["cs_type"], p1=case["p1"], p2=case["p2"],
+                   uniqueness=case["uniqueness"], do_lr_check=1, do_median=0, tie_rule=4, init_tie_rule=4)
+    a = O.match(cfg.with_roi(tuple(z["roi_l"]), tuple(z["roi_r"])), z["left"], z["right"], dump=True,
+                want_right=True)
+    return a
+
+
+def roi_digests(a, z, case):
+    """Digests of the compared parts of a ROI case's volumes (zeros elsewhere)."""
+    W, H, M = case["width"], case["height"], case["min_disp"]
+    pm_l, _ = roi_masks(W, H, tuple(z["roi_l"]), M)
+    pm_r, _ = roi_masks(W, H, tuple(z["roi_r"]), M)
+    cm_l = np.zeros((H, W), bool)
+    cm_l[:, max(0, M):] = True  # the left view's cost is computed without the ROI
+    x0, x1, y0, y1 = roi_region(tuple(z["roi_r"]), M)
+    cm_r = np.zeros((H, W), bool)
+    cm_r[y0:y1, x0:x1] = True
+    cost_lr = a["cost"] if "cost" in a else a["cost_lr"]   # oracle dump keys / reference dump keys
+    paths_lr = a["paths"] if "paths" in a else a["paths_lr"]
+    return {"digest_cost_lr": digest(np.where(cm_l[..., None], cost_lr, 0)),
+            "digest_paths_lr": digest(np.where(pm_l[..., None], paths_lr, 0)),
+            "digest_cost_rl": digest(np.where(cm_r[..., None], a["cost_rl"], 0)),
+            "digest_paths_rl": digest(np.where(pm_r[..., None], a["paths_rl"], 0))}
+
+
+def roi_report(z, case, meta):
+    a = roi_oracle(z, case)
+    ours = roi_digests(a, z, case)
+    ref = roi_digests(z, z, case)
+    W, H, M = case["width"], case["height"], case["min_disp"]
+    _, wm = roi_masks(W, H, tuple(z["roi_l"]), M)
+    r = {k: ours[k] == ref[k] for k in ours}
+    r["wta_compared"] = float((a["wta_l"].view(np.uint32) == z["wta_l"].view(np.uint32))[wm].mean())
+    keep = {k: z[k] for k in ("left", "right", "roi_l", "roi_r", "wta_l", "case")}
+    keep.update({k: np.array(v) for k, v in ref.items()})
+    return r, keep
+
+
 def depth_report(z, case, meta):
     want, rows = oracle_depth(z, case, meta["peaks_strips"])
     return {"depth_equal": float((want.view(np.uint32) == z["depth"].view(np.uint32))[rows].mean())}
@@ -392,6 +487,11 @@ def finalize(dump_dir: Path, write: bool = True):
             report[name] = _levels_report(z, case, meta)
             if write:
                 np.savez_compressed(GOLDEN / f"ref_{name}.npz", **z, peaks_strips=np.int32(meta["peaks_strips"]))
+            continue
+        if name.startswith("roi"):
+            report[name], keep = roi_report(z, case, meta)
+            if write:
+                np.savez_compressed(GOLDEN / f"ref_{name}.npz", **keep)
             continue
         if name.startswith("depth"):
             report[name] = depth_report(z, case, meta)

@@ -17,6 +17,10 @@ DEPTH = [n for n in ("depth_gauss_only", "depth_erosion_only", "depth_gauss_eros
          if (GOLDEN / f"ref_{n}.npz").exists()]
 
 
+def test_fixtures_present():
+    assert len(FILTER) == 7 and len(DEPTH) == 3, (FILTER, DEPTH)
+
+
 def load(name):
     z = dict(np.load(GOLDEN / f"ref_{name}.npz"))
     return z, json.loads(str(z["case"]))
