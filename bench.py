@@ -59,6 +59,8 @@ def parse():
                     default="", help="run one extra workload alone and print its JSON (e.g. for a profiler)")
     ap.add_argument("--extra-pairs", type=int, default=64, help="pairs of the --extra batch workloads")
     ap.add_argument("--float-batch", type=int, default=4, help="pairs of the --extra float_sgm workload")
+    ap.add_argument("--dry-run", action="store_true",
+                    help="launch, shard and time the ranks without CUDA (gloo); for testing the launcher")
     return ap.parse_args()
 
 
@@ -71,15 +73,17 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def make_pool(n_distinct, seed=100):
-    """n_distinct different pairs: 8 scenes, each shifted/flipped into many variants."""
+def make_pool(n_distinct, seed=100, indices=None):
+    """Distinct pairs of a global pool: pair i is one of 8 scenes (i % 8), rolled by a shift drawn
+    from i and flipped on every other group of 8. `indices` picks pairs of the global pool (a
+    rank's shard); by default the first n_distinct."""
     from fasterstereocuda_b200 import scenes
-    base = [scenes.kitti_like(seed + i, W_, H_)[:2] for i in range(8)]
+    idx = list(range(n_distinct)) if indices is None else list(indices)
+    base = {k: scenes.kitti_like(seed + k, W_, H_)[:2] for k in sorted({i % 8 for i in idx})}
     pool = []
-    rng = np.random.Generator(np.random.PCG64(seed))
-    for i in range(n_distinct):
+    for i in idx:
         L, R = base[i % 8]
-        dy = int(rng.integers(0, 40))
+        dy = int(np.random.Generator(np.random.PCG64([seed, i])).integers(0, 40))
         L2, R2 = np.roll(L, dy, 0), np.roll(R, dy, 0)
         if (i // 8) % 2:
             L2, R2 = L2[::-1].copy(), R2[::-1].copy()
@@ -320,7 +324,9 @@ def run_ours(a, rank, world, local_rank):
     S = max(1, a.streams)
     matchers = [make_matcher() for _ in range(S)]
     streams = [torch.cuda.Stream(device=dev) for _ in range(S)]
-    pool = make_pool(a.pool, seed=100 + 17 * rank)
+    # weak scaling: the pairs of a step and the pool of distinct pairs are split over the ranks
+    # (replicas.shard), every rank matching a.batch pairs per step from its own share of the pool
+    pool = make_pool(0, indices=replicas.shard(a.pool * world, rank, world))
     dL = [torch.from_numpy(L).to(dev) for L, _ in pool]
     dR = [torch.from_numpy(R).to(dev) for _, R in pool]
     outs = [torch.empty((H_, W_), dtype=torch.float32, device=dev) for _ in range(a.batch)]
@@ -846,9 +852,18 @@ def extra_large_pyramid():
     e1.record(s)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / n
+    peak = free0 - rt.cudaMemGetInfo()[1]  # no allocation happens while matching
+    # algorithmic bytes of a pair: 4*W*H*D + 6*W*H per view and level (the two-pass design's cost
+    # and path traffic plus images and maps); the coarsest level matches both views (LR check)
+    levels = [p.level_info(i) for i in range(4)]
+    alg = sum((2 if i == len(levels) - 1 else 1) * (4 * w * h * d + 6 * w * h) for i, (w, h, _, d) in enumerate(levels))
+    hbm, src = peaks()
     return {"workload": "4800x3409, D=256, 4-level pyramid, census 9x7, P1=10 P2=150, fractal scene",
             "ms_per_pair": ms, "pairs_per_s": 1e3 / ms, "matcher_device_gib": used / 2**30,
-            "levels": [p.level_info(i) for i in range(4)]}
+            "peak_device_gib": (peak + dl.numel() * 2 + out.numel() * 4) / 2**30,
+            "roofline": {"bound": "hbm", "alg_bytes_per_pair": alg, "achieved_gbs": alg / (ms * 1e6), "peak_gbs": hbm,
+                         "frac": alg / (ms * 1e6) / hbm, "peak_source": src},
+            "levels": levels}
 
 
 def cpu_baseline(a, pool):
@@ -894,11 +909,46 @@ def run_extra(a):
     return 0
 
 
+def relaunch(a):
+    """--gpus N without a launcher: one process per GPU under torch.distributed.run (which sets
+    RANK / LOCAL_RANK / WORLD_SIZE), this script's arguments passed through."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={a.gpus}",
+           "--master-addr=127.0.0.1", f"--master-port={port}", str(Path(__file__).resolve()), *sys.argv[1:]]
+    return subprocess.run(cmd).returncode
+
+
+def run_dry(a, rank, world):
+    """The launcher's plumbing without CUDA: each rank takes its shard of a step's pairs, the ranks
+    meet at the barriers of a timed region whose length differs per rank, and rank 0 prints the
+    maximum over ranks and every rank's shard."""
+    from fasterstereocuda_b200 import replicas
+    mine = replicas.shard(a.batch * world, rank, world)
+    replicas.barrier(world)
+    t = time.perf_counter()
+    time.sleep(0.02 * (rank + 1))
+    replicas.barrier(world)
+    ms = replicas.max_over_ranks((time.perf_counter() - t) * 1e3, world)
+    shards = replicas.gather_to_rank0([mine.start, mine.stop], world, rank)
+    if rank == 0:
+        print(json.dumps({"dry_run": True, "n_gpus": world, "pairs_per_step": a.batch * world, "shards": shards,
+                          "ms_per_step": ms}), flush=True)
+    return 0
+
+
 def main():
     a = parse()
+    if "WORLD_SIZE" not in os.environ and a.gpus > 1:
+        return relaunch(a)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != a.gpus:
+        print(f"bench.py: --gpus {a.gpus} but {world} ranks were launched", file=sys.stderr)
+        return 2
     if a.impl == "reference":
         return run_reference(a, rank, world)
     if a.extra:
@@ -907,11 +957,14 @@ def main():
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local_rank)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local_rank))
+        if a.dry_run:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
+        else:
+            torch.cuda.set_device(local_rank)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", local_rank))
     try:
-        return run_ours(a, rank, world, local_rank)
+        return run_dry(a, rank, world) if a.dry_run else run_ours(a, rank, world, local_rank)
     finally:
         if world > 1:
             import torch.distributed as dist

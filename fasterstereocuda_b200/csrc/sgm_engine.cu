@@ -7,6 +7,7 @@
 // a match is one stream of kernels with no host synchronisation inside it; small-region
 // removal runs on the GPU; the pyramid keeps every level on the device.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cmath>
@@ -207,6 +208,14 @@ struct sgm_engine {
   int direct_runs = 0;
   int64_t graph_launches = 0;
   cudaEvent_t done = nullptr;  // blocking-sync event of the synchronous host API
+  // Stages of a match: an NVTX range each, and with print_log a CUDA event at every stage boundary
+  // for the per-stage report of the synchronous host API.
+  static constexpr int kMaxStages = 10;
+  bool stage_timing = false;
+  bool nvtx_open = false;
+  int nstage = 0;
+  cudaEvent_t stage_ev[kMaxStages] = {};
+  const char* stage_name[kMaxStages] = {};
   void drop_graph() {
     if (gexec) cudaGraphExecDestroy(gexec);
     gexec = nullptr;
@@ -222,6 +231,11 @@ struct sgm_engine {
     drop_graph();
     if (done) cudaEventDestroy(done);
     done = nullptr;
+    for (auto& ev : stage_ev) {
+      if (ev) cudaEventDestroy(ev);
+      ev = nullptr;
+    }
+    stage_timing = false;
     for (int i = 0; i < 2; ++i) {
       dfree(img[i]);
       dfree(init[i]);
@@ -257,6 +271,18 @@ cudaError_t wait_stream(cudaStream_t s, cudaEvent_t* ev) {
   }
   const cudaError_t st = cudaEventRecord(*ev, s);
   return st != cudaSuccess ? st : cudaEventSynchronize(*ev);
+}
+
+// Starts stage `name` of the match being enqueued (ends the previous one); name == nullptr ends
+// the last stage. NVTX ranges cost next to nothing without a tool attached.
+void stage_mark(sgm_engine* e, const char* name) {
+  if (e->nvtx_open) nvtxRangePop();
+  e->nvtx_open = name != nullptr;
+  if (name) nvtxRangePushA(name);
+  if (e->stage_timing && e->nstage < sgm_engine::kMaxStages) {
+    cudaEventRecord(e->stage_ev[e->nstage], e->stream);
+    e->stage_name[e->nstage++] = name;
+  }
 }
 
 #define SGM_CUDA_TRY(e, expr)                                                          \
@@ -843,6 +869,7 @@ int engine_enqueue(sgm_engine* e, const uint8_t* dl_img, const uint8_t* dr_img, 
   const size_t N = e->npix();
   int st = SGM_OK;
   // census of both images
+  stage_mark(e, "census");
   {
     // 8 rows per block, or 2 when that leaves fewer blocks than SMs (small pyramid levels)
     constexpr int RY = sgm::kCensusRows;
@@ -879,6 +906,7 @@ int engine_enqueue(sgm_engine* e, const uint8_t* dl_img, const uint8_t* dr_img, 
     dinit_r = e->init[1];
   }
   // cost + four paths + WTA, both views
+  stage_mark(e, "cost + aggregation + WTA");
   if (!st) {
     const bool w64 = e->opt.cs_type == 1;
     if (roi) {
@@ -927,6 +955,7 @@ int engine_enqueue(sgm_engine* e, const uint8_t* dl_img, const uint8_t* dr_img, 
   }
   const dim3 fb(32, 8), fg((W + 31) / 32, (H + 7) / 8);
   if (!st && (lr || med)) {
+    stage_mark(e, "left-right check + median");
     float* dst = next_out();
     float* marks = lr ? dout_r : nullptr;
     if (lr && med)
@@ -946,6 +975,7 @@ int engine_enqueue(sgm_engine* e, const uint8_t* dl_img, const uint8_t* dr_img, 
   // post filter back into the aggregator's buffer. So the depth of a map with exactly one of the
   // two steps and no removal is the depth of the map before that step.
   const float* agg = cur;
+  if (!st && (pf || morph)) stage_mark(e, "post filter + morphology");
   if (!st && pf) {
     float* dst = next_out();
     if (pf == 1)
@@ -970,6 +1000,7 @@ int engine_enqueue(sgm_engine* e, const uint8_t* dl_img, const uint8_t* dr_img, 
     cur = dout;
   }
   if (!st && peaks) {
+    stage_mark(e, "small-region removal");
     const int strips = e->ext.peaks_strips > 0 ? e->ext.peaks_strips : default_peaks_strips();
     // strips of floor(h / strips) rows from the ROI's first row, or from row 0 (StereoCudaImpl.cpp:
     // 463-498); they are labelled as a sub-image of the rows they cover
@@ -994,6 +1025,7 @@ int engine_enqueue(sgm_engine* e, const uint8_t* dl_img, const uint8_t* dr_img, 
                                                        e->opt.peaks_ratio_threshold));
     }
   }
+  stage_mark(e, nullptr);
   e->depth_src = (!peaks && ((pf != 0) != (morph != 0))) ? agg : dout;
   e->stream = saved;
   return st;
@@ -1307,23 +1339,48 @@ int sgm_match(sgm_handle_t h, const uint8_t* img_left, const uint8_t* img_right,
   }
   const size_t N = h->npix();
   h->launches = 0;
+  // with print_log: per-stage times, printed like the reference's timers (StereoCudaImpl.cpp:
+  // 365-460, 530-543); the match then runs its kernels directly instead of as a graph
+  h->stage_timing = h->print_log;
+  h->nstage = 0;
+  if (h->stage_timing)
+    for (auto& ev : h->stage_ev)
+      if (!ev) SGM_CUDA_TRY(h, cudaEventCreate(&ev));
+  stage_mark(h, "input");
   SGM_CUDA_TRY(h, cudaMemcpyAsync(h->img[0], img_left, N, cudaMemcpyHostToDevice, h->stream));
   SGM_CUDA_TRY(h, cudaMemcpyAsync(h->img[1], img_right, N, cudaMemcpyHostToDevice, h->stream));
   if (init_disp_left)
     SGM_CUDA_TRY(h, cudaMemcpyAsync(h->init[0], init_disp_left, N * sizeof(int16_t), cudaMemcpyHostToDevice, h->stream));
   const bool right = disp_right && h->opt.do_lr_check;
   const bool roi = roi_left || (roi_right && h->opt.do_lr_check);
-  int st = (!init_disp_left && !right && !roi)
+  int st = (!init_disp_left && !right && !roi && !h->stage_timing)
                ? engine_run(h, h->img[0], h->img[1], h->out, h->stream)
                : engine_enqueue(h, h->img[0], h->img[1], init_disp_left ? h->init[0] : nullptr, h->out,
                                 right ? h->dr_out : nullptr, h->stream, roi_left, roi_right);
-  if (st) return st;
+  if (st) {
+    h->stage_timing = false;
+    return st;
+  }
+  if (h->stage_timing) stage_mark(h, "output");
   SGM_CUDA_TRY(h, cudaMemcpyAsync(disp_left, h->out, N * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
   if (disp_right && h->opt.do_lr_check)
     SGM_CUDA_TRY(h, cudaMemcpyAsync(disp_right, h->dr_out, N * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+  if (h->stage_timing) stage_mark(h, nullptr);
   SGM_CUDA_TRY(h, wait_stream(h->stream, &h->done));
   if (disp_right && !h->opt.do_lr_check)
     for (size_t i = 0; i < N; ++i) disp_right[i] = sgm::kInvalidFloat;
+  if (h->stage_timing) {
+    printf("Timing:\n");
+    float total = 0.0f;
+    for (int i = 0; i + 1 < h->nstage; ++i) {
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, h->stage_ev[i], h->stage_ev[i + 1]);
+      if (h->stage_name[i]) printf("** %-28s %.3f ms\n", h->stage_name[i], ms);
+      total += ms;
+    }
+    printf("** %-28s %.3f ms\n", "total", total);
+    h->stage_timing = false;
+  }
   return SGM_OK;
 }
 

@@ -116,7 +116,13 @@ SGM_API int sgm_set_tuning(sgm_handle_t h, const sgm_tuning_t* t);
 SGM_API int sgm_get_tuning(sgm_handle_t h, sgm_tuning_t* t);
 /* StereoCuda::Match -- SgmStereoCuda/StereoCuda.h:44, StereoCudaImpl.cpp:507-546.
  * Host buffers of width*height elements. disp_right, init_disp_left, roi_* may be NULL.
- * Returns after the disparity has been copied back (synchronous, like the reference). */
+ * Returns after the disparity has been copied back (synchronous, like the reference).
+ * roi_left / roi_right (cusgm_cc.cu:478-488, cusgm_ca.cu:3991-3999): a view's rectangle, inside the
+ * image, matched as a sub-image whose paths start at its edges (columns from max(x, min_disparity));
+ * the WTA covers floor(h/2)*2 of its rows, everything outside is INVALID, small-region removal runs
+ * in strips of the left rectangle's rows. roi_right is used with the LR check only. Plain levels
+ * with disp_range <= 128, P1 <= P2 <= 16383 and tie rule 0 or 4, else SGM_ERR_UNSUPPORTED.
+ * With print_log set at init, prints the time of every stage (CUDA events). */
 SGM_API int sgm_match(sgm_handle_t h, const uint8_t* img_left, const uint8_t* img_right, float* disp_left,
                       float* disp_right, const int16_t* init_disp_left, const sgm_roi_t* roi_left,
                       const sgm_roi_t* roi_right);
@@ -130,12 +136,15 @@ SGM_API int sgm_match_device(sgm_handle_t h, const uint8_t* d_left, const uint8_
 SGM_API int sgm_init2(sgm_handle_t h, int32_t width, int32_t height, int32_t min_disparity, int32_t disp_range,
                       const sgm_option_t* option, const sgm_camera_t* camera, int32_t print_log);
 /* StereoCuda::Match2 -- SgmStereoCuda/StereoCuda.h:69, StereoCudaImpl.cpp:548-583: match, then
- * depth = baseline*focus / (d + x0_right - x0_left) in double, INVALID kept (cusgm_util.cu:7-34). */
+ * depth = baseline*focus / (d + x0_right - x0_left) in double, INVALID kept (cusgm_util.cu:7-34).
+ * The disparity is the final map, except with exactly one of post filter / morphology and no
+ * small-region removal: then the map before that step (the reference's aggregator buffer). */
 SGM_API int sgm_match2(sgm_handle_t h, const uint8_t* img_left, const uint8_t* img_right, float* depth_left,
                        const int16_t* init_disp_left, const sgm_roi_t* roi_left, const sgm_roi_t* roi_right);
 /* StereoCuda::Release -- SgmStereoCuda/StereoCuda.h:75, StereoCudaImpl.cpp:281-332 */
 SGM_API int sgm_release(sgm_handle_t h);
-/* StereoCuda::SetMinDisparity / GetDispartyRange -- SgmStereoCuda/StereoCuda.h:71-72 */
+/* StereoCuda::SetMinDisparity / GetDispartyRange -- SgmStereoCuda/StereoCuda.h:71-72.
+ * A minimum disparity at or past the width is refused (SGM_ERR_ARG, the previous value kept). */
 SGM_API int sgm_set_min_disparity(sgm_handle_t h, int32_t min_disparity);
 SGM_API int32_t sgm_get_disparity_range(sgm_handle_t h);
 /* StereoCuda::GetRoiFromDispMap -- SgmStereoCuda/StereoCudaImpl.cpp:585-628 */

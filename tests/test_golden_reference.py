@@ -282,3 +282,7 @@ def test_roi_against_reference(oracle_mod, name):
     neq = (a["wta_l"].view(np.uint32) != z["wta_l"].view(np.uint32)) & wm
     assert int(neq.sum()) == 0, np.argwhere(neq)[:5]
     assert wm.mean() > 0.3
+
+
+def test_roi_fixtures_present():
+    assert ROI == ["roi5x5", "roi9x7"], ROI

@@ -273,8 +273,8 @@ def test_errors_on_device(engine_lib):
     out = np.empty((H, W), np.float32)
     init = np.zeros((H, W), np.int16)
     assert not s.Match(img, img, out, None, init) and s.status == -4   # init needs D=32
-    roi = fsc.StereoROI(0, 0, 10, 10)
-    assert not s.Match(img, img, out, None, None, roi) and s.status == -4
+    roi = fsc.StereoROI(120, 0, 10, 10)  # leaves the 128-pixel-wide image
+    assert not s.Match(img, img, out, None, None, roi) and s.status == -1
     s.Release()
     assert not s.Match(img, img, out) and s.status == -2
 

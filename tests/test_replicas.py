@@ -79,3 +79,29 @@ def test_single_rank_needs_no_process_group():
     assert replicas.max_over_ranks(1.5, 1) == 1.5
     assert replicas.gather_to_rank0({"a": 1}, 1, 0) == [{"a": 1}]
     replicas.barrier(1)
+
+
+def test_bench_launches_one_rank_per_gpu_and_shards_the_pairs():
+    """bench.py --gpus 2 without a launcher starts two ranks (torch.distributed.run), splits each
+    step's pairs between them and reports the slowest rank's time; --dry-run keeps CUDA out (gloo)."""
+    import json
+    import subprocess
+    import sys
+    from pathlib import Path
+    root = Path(__file__).resolve().parent.parent
+    env = {k: v for k, v in os.environ.items() if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK", "MASTER_ADDR",
+                                                            "MASTER_PORT")}
+    r = subprocess.run([sys.executable, str(root / "bench.py"), "--gpus", "2", "--dry-run", "--batch", "8"],
+                       capture_output=True, text=True, env=env, timeout=300, cwd=root)
+    assert r.returncode == 0, r.stderr[-3000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1, r.stdout  # rank 0 alone prints
+    out = json.loads(lines[0])
+    assert out["n_gpus"] == 2 and out["pairs_per_step"] == 16
+    assert out["shards"] == [[0, 8], [8, 16]]
+    assert out["ms_per_step"] >= 40.0  # rank 1's 40 ms, the maximum over ranks
+    # a launcher that started fewer ranks than --gpus asks for is refused
+    env1 = dict(env, WORLD_SIZE="1", RANK="0", LOCAL_RANK="0")
+    r = subprocess.run([sys.executable, str(root / "bench.py"), "--gpus", "2", "--dry-run"], capture_output=True,
+                       text=True, env=env1, timeout=120, cwd=root)
+    assert r.returncode == 2 and "ranks were launched" in r.stderr
