@@ -389,11 +389,12 @@ def run_ours(a, rank, world, local_rank):
         chosen = (0, 0, 0, 0, 0) + best[1]
         tuning = "autotuned row_lanes,col_lanes = %d,%d" % best[1]
         if a.workload == "pyramid":  # then the 32-disparity levels on their own
-            best_i = min(((timed(chosen, (0, 0, 0, 0, 0) + lanes), lanes) for lanes in ((8, 8), (4, 4), (2, 2))),
+            best_i = min(((timed(chosen, t), t) for t in ((0, 0, 0, 0, 0, 8, 8), (0, 0, 0, 0, 0, 4, 4),
+                                                            (0, 0, 0, 0, 0, 2, 2), (4, 0, 4, 0, 0, 0, 0))),
                          key=lambda r: r[0])
             if best_i[0] < best[0]:
-                chosen_init = (0, 0, 0, 0, 0) + best_i[1]
-                tuning += "; 32-disparity levels %d,%d" % best_i[1]
+                chosen_init = best_i[1]
+                tuning += "; 32-disparity levels " + ",".join(str(v) for v in best_i[1])
         apply_tuning(chosen, chosen_init)
     for _ in range(a.warmup):
         step()
@@ -432,14 +433,18 @@ def run_ours(a, rank, world, local_rank):
         return statistics.median(ts)
     lat_tuning = a.tuning or None
     if not a.tuning:
+        # kernel variants (row_kernel, rows_per_cta, col_kernel, cols_per_cta, bt_smem, row_lanes,
+        # col_lanes); variant 4 (one warp per scanline, bulk-copied chunks) runs at the 32-disparity
+        # levels, the default elsewhere
         cands = {}
-        for lanes in ((8, 8), (8, 4), (4, 4), (2, 2)):
-            apply_tuning((0, 0, 0, 0, 0) + lanes, ms=[lat_m])
+        for t in ((0, 0, 0, 0, 0, 8, 8), (0, 0, 0, 0, 0, 8, 4), (4, 0, 4, 0, 0, 8, 8), (4, 0, 3, 0, 0, 8, 8),
+                  (3, 0, 4, 0, 0, 8, 8), (2, 1, 2, 1, 0, 8, 8)):
+            apply_tuning(t, ms=[lat_m])
             pair_ms(3)
-            cands[lanes] = pair_ms(8)
-        best_lanes = min(cands, key=cands.get)
-        apply_tuning((0, 0, 0, 0, 0) + best_lanes, ms=[lat_m])
-        lat_tuning = "row_lanes,col_lanes = %d,%d" % best_lanes
+            cands[t] = pair_ms(8)
+        best_t = min(cands, key=cands.get)
+        apply_tuning(best_t, ms=[lat_m])
+        lat_tuning = "tuning " + ",".join(str(v) for v in best_t)
     pair_ms(3)
     latency = {"ms_per_pair": pair_ms(20), "tuning": lat_tuning,
                "how": "one matcher, one stream, one pair at a time, inputs in HBM, CUDA events around each "

@@ -21,7 +21,7 @@
 
 #include "../../include/sgm_b200.h"
 #include "sgm_alloc.h"
-#include "sgm_kernels3.cuh"
+#include "sgm_kernels4.cuh"
 #include "sgm_levels.h"
 
 namespace {
@@ -513,7 +513,10 @@ int launch_plain(sgm_engine* e, const Word* csl, const Word* csr, float* wta) {
                      e->opt.p2_init >= e->opt.p1 &&
                      (e->ext.tie_rule == sgm::kTieLowest || e->ext.tie_rule == sgm::kTieRefB200);
   int st;
-  const bool cols_v3 = (e->tune_col_kernel == 3 || e->tune_col_kernel == 0) && v3_ok;
+  // variant 4 exists for the 32-disparity levels only; plain levels take the default for it
+  const int tune_row = e->tune_row_kernel == 4 ? 0 : e->tune_row_kernel;
+  const int tune_col = e->tune_col_kernel == 4 ? 0 : e->tune_col_kernel;
+  const bool cols_v3 = (tune_col == 3 || tune_col == 0) && v3_ok;
   sgm::WtaParams Q;
   Q.uniqueness = e->opt.unique_threshold;
   Q.tie_rule = e->ext.tie_rule;
@@ -522,7 +525,7 @@ int launch_plain(sgm_engine* e, const Word* csl, const Word* csr, float* wta) {
   Q.dmax_excl = warp_kernel ? 32 * K : 32 * K - 1;
   Q.dstride = e->npix();
   Q.image_border(e->W, e->H);
-  if ((e->tune_row_kernel == 3 || e->tune_row_kernel == 0) && v3_ok) {
+  if ((tune_row == 3 || tune_row == 0) && v3_ok) {
     dim3 cg((e->W + 127) / 128, e->H, nv);
     st = SGM_LAUNCH(e, e->stream, "cost", sgm::k_cost3<K, Word><<<cg, 128, 0, e->stream>>>(csl, csr, e->cost, P));
     if (st) return st;
@@ -536,7 +539,7 @@ int launch_plain(sgm_engine* e, const Word* csl, const Word* csr, float* wta) {
       return launch_cols3_pass<K, 2>(e, gc, P, Q, wta, nv, e->stream);
     }
     st = launch_rows3<K>(e, e->tune_row_lanes, P, nv, e->stream);
-  } else if (e->tune_row_kernel == 1) {  // whole census rows of R scanlines in shared memory
+  } else if (tune_row == 1) {  // whole census rows of R scanlines in shared memory
     const int R = e->tune_rows > 0 ? e->tune_rows : rows_per_cta(e->W, sizeof(Word), false);
     const size_t smem = (size_t)R * 2 * e->W * sizeof(Word);
     if (smem > 227 * 1024) {
@@ -562,7 +565,7 @@ int launch_plain(sgm_engine* e, const Word* csl, const Word* csr, float* wta) {
     e->bt_stored = true;
     return launch_cols3_pass<K, 0>(e, e->tune_col_lanes, P, Q, wta, nv, e->stream);
   }
-  if (e->tune_col_kernel != 2) {
+  if (tune_col != 2) {
     C = e->tune_cols > 0 ? e->tune_cols : 8;
     e->bt_stored = true;
     dim3 vg((e->W + C - 1) / C, nv), vb(32, C);
@@ -742,6 +745,28 @@ int init3_cols(sgm_engine* e, const int16_t* il, const int16_t* ir, float* wta, 
                   : go(sgm::k_vpaths3_init<4, 4, PASS>);
 }
 
+// Initial-disparity levels, latency form (variant 4): one warp per scanline, chunks staged by
+// bulk async copies (sgm_kernels4.cuh). Exact for any penalties and tie rule.
+constexpr int kScan4RowWarps = 2, kScan4ColWarps = 4;
+
+inline int init4_rows(sgm_engine* e, const int16_t* il, const int16_t* ir, const sgm::InitParams& P,
+                      cudaStream_t s) {
+  const int nv = e->nviews();
+  const int blocks = (nv * 2 * e->H + kScan4RowWarps - 1) / kScan4RowWarps;
+  return SGM_LAUNCH(e, s, "hpaths_init", sgm::k_hscan_init4<kScan4RowWarps><<<blocks, 32 * kScan4RowWarps, 0, s>>>(
+                                             e->cost, il, ir, e->lr, e->rl, P, nv));
+}
+
+template <int PASS>
+int init4_cols(sgm_engine* e, const int16_t* il, const int16_t* ir, float* wta, const sgm::InitParams& P,
+               const sgm::WtaParams& Q, cudaStream_t s) {
+  e->bt_stored = true;
+  const dim3 grid((unsigned)((e->W + kScan4ColWarps - 1) / kScan4ColWarps), e->nviews());
+  const char* name = PASS == 1 ? "vpaths_bt_init" : "vpaths_wta_init";
+  return SGM_LAUNCH(e, s, name, sgm::k_vscan_init4<kScan4ColWarps, PASS><<<grid, 32 * kScan4ColWarps, 0, s>>>(
+                                    e->cost, e->lr, e->rl, il, ir, e->bt, wta, P, Q));
+}
+
 template <typename Word>
 int launch_init(sgm_engine* e, const Word* csl, const Word* csr, const int16_t* il, const int16_t* ir, float* wta) {
   sgm::InitParams P;
@@ -761,18 +786,22 @@ int launch_init(sgm_engine* e, const Word* csl, const Word* csr, const int16_t* 
   const bool v3_ok = e->ext.init_tie_rule == sgm::kTieLowest || e->ext.init_tie_rule == sgm::kTieRefB200;
   const bool rows3 = v3_ok && (e->tune_row_kernel == 0 || e->tune_row_kernel == 3);
   const bool cols3 = v3_ok && (e->tune_col_kernel == 0 || e->tune_col_kernel == 3);
+  const bool rows4 = e->tune_row_kernel == 4, cols4 = e->tune_col_kernel == 4;
+  // rows reading the cost volume (variants 3 and 4) and columns split into two passes
+  auto rows_cv = [&](cudaStream_t ms) { return rows4 ? init4_rows(e, il, ir, P, ms) : init3_rows(e, il, ir, P, ms); };
+  auto cols_bt = [&](cudaStream_t ss) {
+    return cols4 ? init4_cols<1>(e, il, ir, wta, P, Q3, ss) : init3_cols<1>(e, il, ir, wta, P, Q3, ss);
+  };
   int st;
-  if (rows3 && cols3 && kSplitColumns) {  // bottom-to-top column pass beside the row scans
+  if ((rows3 || rows4) && (cols3 || cols4) && kSplitColumns) {  // bottom-to-top pass beside the row scans
     st = init3_cost<Word>(e, csl, csr, il, ir, P, e->stream);
-    if (!st)
-      st = fork_join(
-          e, e->stream, [&](cudaStream_t ss) { return init3_cols<1>(e, il, ir, wta, P, Q3, ss); },
-          [&](cudaStream_t ms) { return init3_rows(e, il, ir, P, ms); });
-    return st ? st : init3_cols<2>(e, il, ir, wta, P, Q3, e->stream);
+    if (!st) st = fork_join(e, e->stream, cols_bt, rows_cv);
+    if (st) return st;
+    return cols4 ? init4_cols<2>(e, il, ir, wta, P, Q3, e->stream) : init3_cols<2>(e, il, ir, wta, P, Q3, e->stream);
   }
-  if (rows3) {
+  if (rows3 || rows4) {
     st = init3_cost<Word>(e, csl, csr, il, ir, P, e->stream);
-    if (!st) st = init3_rows(e, il, ir, P, e->stream);
+    if (!st) st = rows_cv(e->stream);
   } else if (e->tune_row_kernel == 1) {  // whole census rows of R scanlines in shared memory
     const int R = e->tune_rows > 0 ? e->tune_rows : rows_per_cta(e->W, sizeof(Word), true);
     const size_t smem = (size_t)R * e->W * (2 * sizeof(Word) + 2);
@@ -811,6 +840,10 @@ int launch_init(sgm_engine* e, const Word* csl, const Word* csr, const int16_t* 
   int C = 8, bt_smem = 0;
   size_t vsmem = 0;
   if (cols3) return init3_cols<0>(e, il, ir, wta, P, Q3, e->stream);
+  if (cols4) {
+    st = init4_cols<1>(e, il, ir, wta, P, Q3, e->stream);
+    return st ? st : init4_cols<2>(e, il, ir, wta, P, Q3, e->stream);
+  }
   if (e->tune_col_kernel != 2) {
     C = e->tune_cols > 0 ? e->tune_cols : 8;
     e->bt_stored = true;
@@ -1286,7 +1319,7 @@ int sgm_get_ext_options(sgm_handle_t h, sgm_ext_options_t* ext) {
 namespace {
 bool tuning_ok(const sgm_tuning_t* t) {
   const int r = t->rows_per_cta, c = t->cols_per_cta;
-  return t->row_kernel >= 0 && t->row_kernel <= 3 && t->col_kernel >= 0 && t->col_kernel <= 3 &&
+  return t->row_kernel >= 0 && t->row_kernel <= 4 && t->col_kernel >= 0 && t->col_kernel <= 4 &&
          (r == 0 || r == 1 || r == 2 || r == 4) && c >= 0 && c <= 8 && (t->bt_smem == 0 || t->bt_smem == 1) &&
          (t->row_lanes == 0 || t->row_lanes == 1 || t->row_lanes == 2 || t->row_lanes == 4 || t->row_lanes == 8) &&
          (t->col_lanes == 0 || t->col_lanes == 1 || t->col_lanes == 2 || t->col_lanes == 4 || t->col_lanes == 8);
@@ -1305,7 +1338,7 @@ void apply_tuning(sgm_engine* e, const sgm_tuning_t* t) {
 int sgm_set_tuning(sgm_handle_t h, const sgm_tuning_t* t) {
   if (!h || !t) return SGM_ERR_ARG;
   if (!tuning_ok(t)) {
-    set_error(&h->err, "tuning out of range (kernels 0-3, rows per CTA 0/1/2/4, columns per CTA 0-8, bt_smem 0/1)");
+    set_error(&h->err, "tuning out of range (kernels 0-4, rows per CTA 0/1/2/4, columns per CTA 0-8, bt_smem 0/1)");
     return SGM_ERR_ARG;
   }
   apply_tuning(h, t);
@@ -1533,6 +1566,12 @@ int sgm_debug_read(sgm_handle_t h, int32_t which, int32_t view, void* dst, size_
   }
   if (bytes != n) return SGM_ERR_ARG;
   return cudaMemcpy(dst, src, n, cudaMemcpyDeviceToHost) == cudaSuccess ? SGM_OK : SGM_ERR_CUDA;
+}
+
+int64_t sgm_debug_wait_timeouts(void) {
+  unsigned int n = 0;
+  if (cudaMemcpyFromSymbol(&n, sgm::g_scan_wait_timeouts, sizeof(n)) != cudaSuccess) return -1;
+  return n;
 }
 
 int sgm_debug_fail_device_alloc(int64_t after) {
@@ -1765,7 +1804,7 @@ int sgm_pyr_set_tuning(sgm_pyr_handle_t h, int32_t level, const sgm_tuning_t* t)
     return SGM_ERR_ARG;
   }
   if (!tuning_ok(t)) {
-    h->err = "tuning out of range (kernels 0-3, rows per CTA 0/1/2/4, columns per CTA 0-8, bt_smem 0/1)";
+    h->err = "tuning out of range (kernels 0-4, rows per CTA 0/1/2/4, columns per CTA 0-8, bt_smem 0/1)";
     return SGM_ERR_ARG;
   }
   for (int i = 0; i < h->layers; ++i)

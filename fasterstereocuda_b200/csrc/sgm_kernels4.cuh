@@ -1,0 +1,359 @@
+// Latency form of the 32-disparity scans (pyramid levels below the coarsest), variant 4.
+//
+// A pair alone on the GPU offers few scanlines (375 rows x 2 directions at 1242x375), so the time
+// of a scan is its number of steps times the length of one step's dependency chain. Here one warp
+// owns a scanline and lane d holds disparity d in 32 bits, the reference's own arithmetic
+// (Kernel_Aggregate_{Horizontal,Vertical}_Warp, cusgm_ca.cu:1181-1338). A step's chain is then
+//   m = prev_invalid ? 127 : min_d L(d)            one redux.sync, issued beside the shuffles
+//   a, b = L(d + s - 1), L(d + s + 1)              two shuffles (s = base - last_base)
+//   L'(d) = C(d) + min(L(d), a + P1, b + P1, m + P2') - m
+// and everything that does not depend on L is taken off it:
+//   * the chunk's 32 steps of costs (and, for the top-to-bottom pass, of the three stored paths)
+//     are staged in shared memory by bulk async copies (cp.async.bulk with an mbarrier), one chunk
+//     ahead, double-buffered; a row chunk is one contiguous 1 KB copy, a column chunk one 32-byte
+//     copy per step;
+//   * the per-step bookkeeping of the initial disparities -- the realignment shift, P2' =
+//     max(P1, P2 / |last_base - base + 1|), which steps are skipped for an INVALID base -- is
+//     computed for the whole chunk at once, one step per lane (ballot for the last valid base);
+//   * path costs go to a shared-memory chunk and leave with 16-byte stores.
+// Every wait on an mbarrier is bounded: after kMaxWaitTries polls the warp records the timeout in
+// g_scan_wait_timeouts (read by sgm_debug_wait_timeouts) and stops.
+#pragma once
+#include "sgm_kernels3.cuh"
+
+namespace sgm {
+
+constexpr int kScanChunk = 32;          // steps per staged chunk
+constexpr int kMaxWaitTries = 1 << 22;  // polls of an mbarrier before a wait is given up
+
+static __device__ unsigned int g_scan_wait_timeouts;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+// Generic-proxy accesses of shared memory before async-proxy writes into it.
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// `bytes` (a multiple of 16) from global src to shared dst (both 16-byte aligned), completing on bar.
+__device__ __forceinline__ void bulk_to_smem(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+// Waits for the phase of bar with the given parity; false after kMaxWaitTries polls.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  const uint32_t a = smem_u32(bar);
+  for (int it = 0; it < kMaxWaitTries; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+// A wait that ran out: record it, then wait (again bounded) for the copies still in flight into
+// this warp's buffers before the warp leaves.
+// phase: bit b = the parity of the phase buffer b waits for next.
+__device__ __forceinline__ void scan_give_up(uint64_t* bars, uint32_t phase, int nbars) {
+  if ((threadIdx.x & 31) == 0) atomicAdd(&g_scan_wait_timeouts, 1u);
+  for (int b = 0; b < nbars; ++b) mbar_wait(bars + b, (phase >> b) & 1u);
+}
+
+// Per-step parameters of a chunk, one step per lane (lane j = step j): packed as
+// shift (8 bits, clamped to +-64: any |shift| > 33 puts both neighbours out of range) |
+// kStepValid | kPrevInvalid, and P2'.
+constexpr uint32_t kStepValid = 1u << 8, kPrevInvalid = 1u << 9;
+
+struct ChunkState {
+  int carry_base;      // base of the last step that set last_base before the chunk
+  bool carry_invalid;  // the last step before the chunk was skipped (INVALID base)
+};
+
+// b: this lane's step base (INVALID for lanes past the chunk); gs0: global index of the chunk's
+// first step; n: steps in the chunk; first_sets_base: the scanline's first pixel sets last_base
+// (horizontal scans) or keeps the one given (vertical scans, cusgm_ca.cu:1291).
+__device__ __forceinline__ void chunk_params(int b, int gs0, int n, bool first_sets_base, const InitParams& P,
+                                             ChunkState& st, uint32_t& flags, uint32_t& p2) {
+  const int j = threadIdx.x & 31;
+  const bool in = j < n;
+  const bool first = gs0 + j == 0;
+  const bool step_valid = in && !first && b != kInvalidShort;
+  const bool sets_base = in && (step_valid || (first && first_sets_base));
+  const unsigned vm = __ballot_sync(kFull, sets_base);
+  const unsigned prev = vm & ((1u << j) - 1u);
+  const int from_prev = __shfl_sync(kFull, b, prev ? 31 - __clz(prev) : 0);
+  const int lb = prev ? from_prev : st.carry_base;
+  const int s = b - lb;
+  const int sc = s < -64 ? -64 : (s > 64 ? 64 : s);
+  const int k = abs(lb - b + 1);
+  const int32_t q = k ? P.p2s / k : P.p2_div0;
+  p2 = (uint32_t)(P.p1s > q ? P.p1s : q);
+  // the previous step was skipped: the chunk's carry for lane 0, the left neighbour's flag else
+  const unsigned inv = __ballot_sync(kFull, in && !first && b == kInvalidShort);
+  const bool prev_inv = j == 0 ? st.carry_invalid : ((inv >> (j - 1)) & 1u);
+  flags = (uint32_t)(sc & 0xFF) | (step_valid ? kStepValid : 0u) | (prev_inv ? kPrevInvalid : 0u);
+  const int last_set = __shfl_sync(kFull, b, vm ? 31 - __clz(vm) : 0);
+  if (vm) st.carry_base = last_set;
+  if (n > 0) st.carry_invalid = (inv >> (n - 1)) & 1u;
+}
+
+// One step of the scanline held by the warp (lane = disparity). L: this lane's state; c: its cost.
+__device__ __forceinline__ void scan_step(uint32_t& L, uint32_t c, uint32_t flags, uint32_t p2, uint32_t p1) {
+  const int lane = threadIdx.x & 31;
+  const int s = (int)(int8_t)(flags & 0xFFu);
+  const uint32_t mr = __reduce_min_sync(kFull, L);
+  const int i1 = lane + s - 1, i2 = lane + s + 1;
+  const uint32_t a = __shfl_sync(kFull, L, i1 & 31);
+  const uint32_t b = __shfl_sync(kFull, L, i2 & 31);
+  const uint32_t m = (flags & kPrevInvalid) ? kInvalidCost : mr;
+  const uint32_t A = (unsigned)i1 < 32u ? a + p1 : kInvalidCost;
+  const uint32_t B = (unsigned)i2 < 32u ? b + p1 : kInvalidCost;
+  const uint32_t t = min(__vimin3_u32(L, A, B), m + p2);
+  const uint32_t Ln = c + (t - m);
+  if (flags & kStepValid) L = Ln;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Horizontal scans: warp w of the grid owns scanline i = (view, dir, y) as in hpaths3_lane.
+// ---------------------------------------------------------------------------------------------
+template <int WPB>
+__global__ void __launch_bounds__(32 * WPB) k_hscan_init4(const uint8_t* __restrict__ cost,
+                                                          const int16_t* __restrict__ init_l,
+                                                          const int16_t* __restrict__ init_r,
+                                                          uint8_t* __restrict__ lr, uint8_t* __restrict__ rl,
+                                                          InitParams P, int nviews) {
+  constexpr int D = kLevelRange, C = kScanChunk;
+  __shared__ __align__(128) uint8_t cbuf[WPB][2][C * D];
+  __shared__ __align__(16) uint8_t obuf[WPB][C * D];
+  __shared__ __align__(8) uint64_t bars[WPB][2];
+  __shared__ uint32_t par[WPB][2][C];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) {
+    mbar_init(&bars[w][0], 1);
+    mbar_init(&bars[w][1], 1);
+    mbar_fence_init();
+  }
+  __syncwarp();
+  const int H = P.H, W = P.W;
+  const int i = blockIdx.x * WPB + w;
+  if (i >= nviews * 2 * H) return;  // the whole warp
+  const int grp = i / H, y = i - grp * H;
+  const int view = grp >> 1, dir = grp & 1;
+  const int len = W - P.x0;
+  if (len <= 0) return;
+  const size_t ro = (size_t)view * P.vstride + (size_t)y * W * D;
+  const uint8_t* crow = cost + ro;
+  uint8_t* orow = (dir == 0 ? lr : rl) + ro;
+  const int16_t* ib = (view == 0 ? init_l : init_r) + (size_t)y * W;
+  const int nch = (len + C - 1) / C;
+  // chunk c: steps [c*C, c*C + n), pixels [xa, xa + n) in memory order
+  auto chunk_n = [&](int c) { return min(C, len - c * C); };
+  auto chunk_x = [&](int c) { return dir == 0 ? P.x0 + c * C : W - (c * C + chunk_n(c)); };
+  auto issue = [&](int c, int buf) {
+    if (lane == 0) {
+      const uint32_t bytes = (uint32_t)chunk_n(c) * D;
+      mbar_expect_tx(&bars[w][buf], bytes);
+      bulk_to_smem(cbuf[w][buf], crow + (size_t)chunk_x(c) * D, bytes, &bars[w][buf]);
+    }
+  };
+  auto base_of = [&](int c) {  // this lane's step of chunk c
+    const int n = chunk_n(c);
+    if (lane >= n) return (int)kInvalidShort;
+    const int x = dir == 0 ? P.x0 + c * C + lane : W - 1 - (c * C + lane);
+    return (int)ib[x];
+  };
+  issue(0, 0);
+  if (nch > 1) issue(1, 1);
+  uint32_t phase = 0u;  // bit b: parity of buffer b's next phase
+  ChunkState st{0, false};
+  int bnext = base_of(0);
+  uint32_t L = 0;
+  for (int c = 0; c < nch; ++c) {
+    const int buf = c & 1, n = chunk_n(c);
+    const int bcur = bnext;
+    if (c + 1 < nch) bnext = base_of(c + 1);  // a chunk ahead
+    uint32_t flags, p2;
+    chunk_params(bcur, c * C, n, true, P, st, flags, p2);
+    par[w][0][lane] = flags;
+    par[w][1][lane] = p2;
+    if (!mbar_wait(&bars[w][buf], (phase >> buf) & 1u)) {
+      scan_give_up(bars[w], phase, 2);
+      return;
+    }
+    phase ^= 1u << buf;
+    __syncwarp();
+    const uint8_t* cb = cbuf[w][buf];
+    uint8_t* ob = obuf[w];
+#pragma unroll
+    for (int j = 0; j < C; ++j) {
+      if (j < n) {  // uniform over the warp
+        const int px = dir == 0 ? j : n - 1 - j;
+        const uint32_t cv = cb[px * D + lane];
+        if (c == 0 && j == 0) {
+          L = cv;  // first pixel of the scanline
+        } else {
+          scan_step(L, cv, par[w][0][j], par[w][1][j], P.p1);
+        }
+        ob[px * D + lane] = (uint8_t)L;
+      }
+    }
+    __syncwarp();
+    // the chunk's path costs: lane j writes pixel xa + j (32 bytes)
+    if (lane < n) {
+      const uint4* src = reinterpret_cast<const uint4*>(ob + lane * D);
+      uint4* dst = reinterpret_cast<uint4*>(orow + (size_t)(chunk_x(c) + lane) * D);
+      const uint4 v0 = src[0], v1 = src[1];
+      dst[0] = v0;
+      dst[1] = v1;
+    }
+    __syncwarp();
+    if (c + 2 < nch) {
+      fence_proxy_async();
+      issue(c + 2, buf);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Vertical scans: warp (blockIdx.x * WPB + w) owns column x of view blockIdx.y. PASS 1: bottom to
+// top, storing its path costs. PASS 2: top to bottom with the 4-path sum and the WTA of an
+// initial-disparity level (as vpaths3_init_lane / k_vpaths_wta_init). Both start last_base from
+// row 0's base (cusgm_ca.cu:1291); the first pixel of a vertical path does not set it.
+// ---------------------------------------------------------------------------------------------
+template <int WPB, int PASS>
+__global__ void __launch_bounds__(32 * WPB) k_vscan_init4(const uint8_t* __restrict__ cost,
+                                                          const uint8_t* __restrict__ lr,
+                                                          const uint8_t* __restrict__ rl,
+                                                          const int16_t* __restrict__ init_l,
+                                                          const int16_t* __restrict__ init_r,
+                                                          uint8_t* __restrict__ bt, float* __restrict__ disp,
+                                                          InitParams P, WtaParams Q) {
+  constexpr int D = kLevelRange, C = kScanChunk;
+  constexpr int NV = PASS == 2 ? 4 : 1;  // staged volumes: cost (+ bottom->top, L->R, R->L)
+  __shared__ __align__(128) uint8_t cbuf[WPB][2][NV][C * D];
+  __shared__ __align__(16) uint8_t obuf[WPB][PASS == 1 ? C * D : 16];
+  __shared__ __align__(8) uint64_t bars[WPB][2];
+  __shared__ uint32_t par[WPB][2][C];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) {
+    mbar_init(&bars[w][0], 1);
+    mbar_init(&bars[w][1], 1);
+    mbar_fence_init();
+  }
+  __syncwarp();
+  const int W = P.W, H = P.H;
+  const int x = blockIdx.x * WPB + w;
+  const int view = blockIdx.y;
+  if (x >= W) return;  // the whole warp
+  float* dout = disp + (size_t)view * Q.dstride + x;
+  if (x < P.x0) {
+    if (PASS == 2)
+      for (int y = lane; y < H; y += 32) dout[(size_t)y * W] = kInvalidFloat;
+    return;
+  }
+  const size_t vo = (size_t)view * P.vstride + (size_t)x * D;
+  const size_t rs = (size_t)W * D;  // bytes between rows
+  const uint8_t* vol[4] = {cost + vo, bt + vo, lr + vo, rl + vo};
+  const int16_t* ib = (view == 0 ? init_l : init_r) + x;
+  const int nch = (H + C - 1) / C;
+  auto chunk_n = [&](int c) { return min(C, H - c * C); };
+  auto row_of = [&](int s) { return PASS == 1 ? H - 1 - s : s; };
+  auto issue = [&](int c, int buf) {
+    const int n = chunk_n(c);
+    if (lane == 0) mbar_expect_tx(&bars[w][buf], (uint32_t)(n * D * NV));
+    __syncwarp();
+    if (lane < n) {
+      const size_t ro = (size_t)row_of(c * C + lane) * rs;
+#pragma unroll
+      for (int v = 0; v < NV; ++v) bulk_to_smem(cbuf[w][buf][v] + lane * D, vol[v] + ro, D, &bars[w][buf]);
+    }
+  };
+  auto base_of = [&](int c) {
+    const int n = chunk_n(c);
+    return lane < n ? (int)ib[(size_t)row_of(c * C + lane) * W] : (int)kInvalidShort;
+  };
+  issue(0, 0);
+  if (nch > 1) issue(1, 1);
+  uint32_t phase = 0u;  // bit b: parity of buffer b's next phase
+  ChunkState st{(int)ib[0], false};  // row 0's base
+  int bnext = base_of(0);
+  uint32_t L = 0;
+  const bool col_ok = x >= Q.xlo && x <= Q.xhi;
+  for (int c = 0; c < nch; ++c) {
+    const int buf = c & 1, n = chunk_n(c);
+    const int bcur = bnext;
+    if (c + 1 < nch) bnext = base_of(c + 1);
+    uint32_t flags, p2;
+    chunk_params(bcur, c * C, n, false, P, st, flags, p2);
+    par[w][0][lane] = flags;
+    par[w][1][lane] = p2;
+    // the WTA needs each step's base (PASS 2); kept in a register of lane j
+    const int my_base = bcur;
+    if (!mbar_wait(&bars[w][buf], (phase >> buf) & 1u)) {
+      scan_give_up(bars[w], phase, 2);
+      return;
+    }
+    phase ^= 1u << buf;
+    __syncwarp();
+    float dv_keep = kInvalidFloat;  // lane j: the disparity of step j (PASS 2)
+#pragma unroll
+    for (int j = 0; j < C; ++j) {
+      if (j < n) {
+        const uint32_t cv = cbuf[w][buf][0][j * D + lane];
+        const uint32_t fl = par[w][0][j];
+        if (c == 0 && j == 0) L = cv;
+        else scan_step(L, cv, fl, par[w][1][j], P.p1);
+        if constexpr (PASS == 1) {
+          obuf[w][j * D + lane] = (uint8_t)L;
+        } else {
+          const int y = c * C + j;
+          const int base = __shfl_sync(kFull, my_base, j);
+          const bool skipped = y > 0 && base == kInvalidShort;
+          float dv = kInvalidFloat;
+          if (y >= Q.ylo && y <= Q.yhi && y < Q.rows) {  // uniform over the warp
+            const uint32_t S = (L & 0xFFu) + cbuf[w][buf][1][j * D + lane] + cbuf[w][buf][2][j * D + lane] +
+                               cbuf[w][buf][3][j * D + lane];
+            if (col_ok && !skipped && base != kInvalidShort) {
+              if (Q.tie_rule == kTieRefB200) {
+                dv = wta_pixel_init_ref(S, lane, base, Q);
+              } else {
+                uint32_t S1[1] = {S};
+                dv = wta_pixel<1>(S1, lane, base, Q, 1, y);
+              }
+            }
+          }
+          if (lane == j) dv_keep = dv;
+        }
+      }
+    }
+    __syncwarp();
+    if (lane < n) {
+      const size_t ro = (size_t)row_of(c * C + lane) * rs;
+      if constexpr (PASS == 1) {
+        const uint4* src = reinterpret_cast<const uint4*>(obuf[w] + lane * D);
+        uint4* dst = reinterpret_cast<uint4*>(bt + vo + ro);
+        const uint4 v0 = src[0], v1 = src[1];
+        dst[0] = v0;
+        dst[1] = v1;
+      } else {
+        dout[(size_t)(c * C + lane) * W] = dv_keep;
+      }
+    }
+    __syncwarp();
+    if (c + 2 < nch) {
+      fence_proxy_async();
+      issue(c + 2, buf);
+    }
+  }
+}
+
+}  // namespace sgm

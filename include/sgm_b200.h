@@ -99,13 +99,17 @@ SGM_API int sgm_get_ext_options(sgm_handle_t h, sgm_ext_options_t* ext);
 typedef struct sgm_tuning_t {
   int32_t row_kernel;   /* horizontal scans: 1 = whole census rows in shared memory,
                            2 = census window and 32-pixel cost chunks in shared memory,
-                           3 = cost-volume kernel + row_lanes lanes per scanline (u16x2 SIMD);
+                           3 = cost-volume kernel + row_lanes lanes per scanline (u16x2 SIMD),
+                           4 = (32-disparity pyramid levels; elsewhere the default) one warp per
+                           scanline with cost chunks staged by bulk async copies: the shortest
+                           step chain, for one pair in flight;
                            0 (default) = 3 where it is exact (see below), else 2 */
   int32_t rows_per_cta; /* scanlines per CTA of the horizontal scans: 0 (default), 1, 2 or 4 */
   int32_t col_kernel;   /* vertical scans + WTA: 1 = one warp per column, plain loads, 2 = the same with
                            an 8-row prefetch ring, 3 = col_lanes lanes per column (u16x2 SIMD, WTA in
-                           the lanes); 0 (default) = 3 where it is exact, else 1. Variant 3 is exact
-                           for D <= 128, P1 <= P2 <= 16383 and tie rule 0 or 4 (else 2 / 1 run) */
+                           the lanes), 4 = as row_kernel 4 (32-disparity levels); 0 (default) = 3
+                           where it is exact, else 1. Variant 3 is exact for D <= 128,
+                           P1 <= P2 <= 16383 and tie rule 0 or 4 (else 2 / 1 run) */
   int32_t cols_per_cta; /* columns (one warp each) per CTA of the vertical scans: 0 (default) .. 8 */
   int32_t bt_smem;      /* 1: keep bottom-to-top path costs in shared memory when they fit */
   int32_t row_lanes;    /* variant 3: lanes per scanline of the horizontal scans, 1/2/4/8 (0: 8) */
@@ -176,6 +180,10 @@ SGM_API int sgm_debug_read(sgm_handle_t h, int32_t which, int32_t view, void* ds
  * and free what they had allocated. sgm_debug_live_device_allocations counts the engine's device
  * allocations that are currently held (process-wide). */
 SGM_API int sgm_debug_fail_device_alloc(int64_t after);
+/* No counterpart in the reference: number of waits on a bulk-copy barrier that the variant-4 scan
+ * kernels gave up on (each is bounded; a warp that gives up stops and leaves its outputs
+ * incomplete). 0 in every correct run; -1 if it cannot be read. */
+SGM_API int64_t sgm_debug_wait_timeouts(void);
 SGM_API int64_t sgm_debug_live_device_allocations(void);
 
 /* No counterpart in the reference: per-kernel timing with CUDA events recorded on the launching

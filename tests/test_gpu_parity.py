@@ -134,18 +134,24 @@ def _init_for(O, L, R, cs, p1, p2):
     return O.init_next_level(coarse, w, h)
 
 
+@pytest.mark.parametrize("variant", [None, (4, 0, 4, 0, 0), (4, 0, 3, 0, 0, 0, 8), (3, 0, 4, 0, 0, 8, 0)])
 @pytest.mark.parametrize("tie", [4, 0])
 @pytest.mark.parametrize("cs,p1,p2,lr,u", [(1, 10, 150, 0, 1.0), (0, 8, 32, 0, 0.95), (1, 10, 150, 1, 0.95),
                                            (0, 8, 32, 1, 1.0)])
-def test_init_disparity_parity(engine_lib, oracle_mod, cs, p1, p2, lr, u, tie):
+def test_init_disparity_parity(engine_lib, oracle_mod, cs, p1, p2, lr, u, tie, variant):
+    """Initial-disparity levels, stage by stage; `variant`: the latency kernels (variant 4) for the
+    row scans, the column scans or both (None: the default kernels)."""
     import fasterstereocuda_b200 as fsc
     O = oracle_mod
     W, H = 162, 121
     L, R, _ = scenes.planar_pair(31 + cs, W, H)
     init = _init_for(O, L, R, cs, p1, p2)
     s = make_engine(fsc, W, H, 0, 32, cs, p1, p2, u, lr, 1, tie=tie)
+    if variant is not None:
+        assert s.set_tuning(fsc.Tuning(*variant)), s.last_error()
     disp = np.empty((H, W), np.float32)
     assert s.Match(L, R, disp, None, init), s.last_error()
+    assert engine_lib.sgm_debug_wait_timeouts() == 0
     cfg = O.Config(width=W, height=H, disp_range=32, cs_type=cs, p1=p1, p2=p2, uniqueness=u, do_lr_check=lr,
                    do_median=1, peaks_strips=STRIPS, tie_rule=tie, init_tie_rule=tie)
     ref = O.match(cfg, L, R, init, dump=True, want_right=True)
@@ -281,7 +287,8 @@ def test_errors_on_device(engine_lib):
 
 TUNINGS = [(1, 0, 1, 0, 0), (1, 2, 1, 4, 0), (2, 1, 2, 8, 1), (2, 2, 2, 2, 0), (2, 4, 2, 1, 1), (1, 4, 2, 8, 0),
            (3, 0, 3, 0, 0), (3, 0, 1, 0, 0), (2, 0, 3, 0, 0), (3, 0, 3, 0, 0, 2, 2), (3, 0, 3, 0, 0, 4, 8),
-           (3, 0, 3, 0, 0, 8, 1)]
+           (3, 0, 3, 0, 0, 8, 1), (4, 0, 4, 0, 0), (4, 0, 3, 0, 0, 0, 8), (3, 0, 4, 0, 0, 8, 0), (4, 0, 1, 0, 0),
+           (2, 0, 4, 0, 0)]
 
 
 @pytest.mark.parametrize("tuning", TUNINGS)
