@@ -19,6 +19,8 @@
 // Every wait on an mbarrier is bounded: after kMaxWaitTries polls the warp records the timeout in
 // g_scan_wait_timeouts (read by sgm_debug_wait_timeouts) and stops.
 #pragma once
+#include <type_traits>
+
 #include "sgm_kernels3.cuh"
 
 namespace sgm {
@@ -122,6 +124,55 @@ __device__ __forceinline__ void scan_step(uint32_t& L, uint32_t c, uint32_t flag
   if (flags & kStepValid) L = Ln;
 }
 
+// WTA of one pixel of an initial-disparity level from its four stored path rows (32 bytes each;
+// S(d) = sum of the four), computed by one lane: Kernel_ComputeDisparityByWTA for initial
+// disparities (cusgm_ca.cu:3425-3512). d* <= 1 or d* >= 31 -> INVALID; uniqueness and the
+// +0.5-shifted parabola as in wta_pixel; tie rules: kTieRefB200 the lowest tied d whose candidate
+// is valid (every tied lane stores its own result there, a valid one wins), 1 / 2 the highest tied
+// d, 0 / 3 the lowest (one disparity per lane: lane order is disparity order).
+__device__ __forceinline__ float init_wta_serial(const uint8_t* a, const uint8_t* b, const uint8_t* c,
+                                                 const uint8_t* e, int base, const WtaParams& Q) {
+  constexpr int D = kLevelRange;
+  uint32_t S[D];
+#pragma unroll
+  for (int k = 0; k < D / 4; ++k) {
+    const uint32_t wa = reinterpret_cast<const uint32_t*>(a)[k], wb = reinterpret_cast<const uint32_t*>(b)[k];
+    const uint32_t wc = reinterpret_cast<const uint32_t*>(c)[k], we = reinterpret_cast<const uint32_t*>(e)[k];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      S[4 * k + q] = ((wa >> (8 * q)) & 0xFFu) + ((wb >> (8 * q)) & 0xFFu) + ((wc >> (8 * q)) & 0xFFu) +
+                     ((we >> (8 * q)) & 0xFFu);
+  }
+  uint32_t m = S[0];
+#pragma unroll
+  for (int d = 1; d < D; ++d) m = min(m, S[d]);
+  const float ut = __fsub_rn(1.0f, Q.uniqueness);
+  // S at a runtime d, summed again from the rows (S[] stays in registers, indexed statically)
+  auto sum_at = [&](int d) { return (uint32_t)a[d] + b[d] + c[d] + e[d]; };
+  auto candidate = [&](int d) {
+    if (d <= 1 || d >= Q.dmax_excl) return kInvalidFloat;
+    const float c1 = (float)sum_at(d - 1), c2 = (float)m, c3 = (float)sum_at(d + 1);
+    const float d12 = __fsub_rn(c1, c2), d32 = __fsub_rn(c3, c2);
+    const float uq = d12 < d32 ? d12 : d32;
+    if (uq <= __fmul_rn(c2, ut)) return kInvalidFloat;
+    return __fadd_rn((float)(d + base), subpix_bias(c1, c2, c3));
+  };
+  uint32_t tied = 0;
+#pragma unroll
+  for (int d = 0; d < D; ++d) tied |= (S[d] == m ? 1u : 0u) << d;
+  if (Q.tie_rule == kTieRefB200) {
+    while (tied) {
+      const int d = __ffs(tied) - 1;
+      const float v = candidate(d);
+      if (v != kInvalidFloat) return v;
+      tied &= tied - 1u;
+    }
+    return kInvalidFloat;
+  }
+  const bool high = Q.tie_rule == kTieHighest || Q.tie_rule == kTieLaneHigh;
+  return candidate(high ? 31 - __clz(tied) : __ffs(tied) - 1);
+}
+
 // ---------------------------------------------------------------------------------------------
 // Horizontal scans: warp w of the grid owns scanline i = (view, dir, y) as in hpaths3_lane.
 // ---------------------------------------------------------------------------------------------
@@ -135,7 +186,7 @@ __global__ void __launch_bounds__(32 * WPB) k_hscan_init4(const uint8_t* __restr
   __shared__ __align__(128) uint8_t cbuf[WPB][2][C * D];
   __shared__ __align__(16) uint8_t obuf[WPB][C * D];
   __shared__ __align__(8) uint64_t bars[WPB][2];
-  __shared__ uint32_t par[WPB][2][C];
+  __shared__ __align__(16) uint32_t par[WPB][2][C];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   if (lane == 0) {
     mbar_init(&bars[w][0], 1);
@@ -193,18 +244,22 @@ __global__ void __launch_bounds__(32 * WPB) k_hscan_init4(const uint8_t* __restr
     __syncwarp();
     const uint8_t* cb = cbuf[w][buf];
     uint8_t* ob = obuf[w];
+    // the chunk's step parameters and this lane's costs in registers: the chain below then
+    // touches no memory but the stores of its results
+    uint32_t fl[C], pp[C], cvr[C];
 #pragma unroll
     for (int j = 0; j < C; ++j) {
-      if (j < n) {  // uniform over the warp
-        const int px = dir == 0 ? j : n - 1 - j;
-        const uint32_t cv = cb[px * D + lane];
-        if (c == 0 && j == 0) {
-          L = cv;  // first pixel of the scanline
-        } else {
-          scan_step(L, cv, par[w][0][j], par[w][1][j], P.p1);
-        }
-        ob[px * D + lane] = (uint8_t)L;
-      }
+      fl[j] = par[w][0][j];
+      pp[j] = par[w][1][j];
+      cvr[j] = cb[(j < n ? (dir == 0 ? j : n - 1 - j) : 0) * D + lane];
+    }
+    // all 32 steps run: past the end of a short last chunk the steps are marked skipped (their
+    // flags have no kStepValid), so the state is kept and nothing is stored
+#pragma unroll
+    for (int j = 0; j < C; ++j) {
+      if (c == 0 && j == 0) L = cvr[0];  // first pixel of the scanline
+      else scan_step(L, cvr[j], fl[j], pp[j], P.p1);
+      if (j < n) ob[(dir == 0 ? j : n - 1 - j) * D + lane] = (uint8_t)L;
     }
     __syncwarp();
     // the chunk's path costs: lane j writes pixel xa + j (32 bytes)
@@ -240,9 +295,9 @@ __global__ void __launch_bounds__(32 * WPB) k_vscan_init4(const uint8_t* __restr
   constexpr int D = kLevelRange, C = kScanChunk;
   constexpr int NV = PASS == 2 ? 4 : 1;  // staged volumes: cost (+ bottom->top, L->R, R->L)
   __shared__ __align__(128) uint8_t cbuf[WPB][2][NV][C * D];
-  __shared__ __align__(16) uint8_t obuf[WPB][PASS == 1 ? C * D : 16];
+  __shared__ __align__(16) uint8_t obuf[WPB][C * D];
   __shared__ __align__(8) uint64_t bars[WPB][2];
-  __shared__ uint32_t par[WPB][2][C];
+  __shared__ __align__(16) uint32_t par[WPB][2][C];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   if (lane == 0) {
     mbar_init(&bars[w][0], 1);
@@ -294,46 +349,41 @@ __global__ void __launch_bounds__(32 * WPB) k_vscan_init4(const uint8_t* __restr
     if (c + 1 < nch) bnext = base_of(c + 1);
     uint32_t flags, p2;
     chunk_params(bcur, c * C, n, false, P, st, flags, p2);
-    par[w][0][lane] = flags;
+    // flags in the low 16 bits, the step's base in the high 16 (the WTA needs it, PASS 2)
+    par[w][0][lane] = flags | ((uint32_t)(uint16_t)(int16_t)bcur << 16);
     par[w][1][lane] = p2;
-    // the WTA needs each step's base (PASS 2); kept in a register of lane j
-    const int my_base = bcur;
     if (!mbar_wait(&bars[w][buf], (phase >> buf) & 1u)) {
       scan_give_up(bars[w], phase, 2);
       return;
     }
     phase ^= 1u << buf;
     __syncwarp();
-    float dv_keep = kInvalidFloat;  // lane j: the disparity of step j (PASS 2)
+    // the chunk's step parameters and this lane's costs in registers: the chain below touches no
+    // memory but the stores of its results
+    uint32_t fl[C], pp[C], cvr[C];
 #pragma unroll
     for (int j = 0; j < C; ++j) {
-      if (j < n) {
-        const uint32_t cv = cbuf[w][buf][0][j * D + lane];
-        const uint32_t fl = par[w][0][j];
-        if (c == 0 && j == 0) L = cv;
-        else scan_step(L, cv, fl, par[w][1][j], P.p1);
-        if constexpr (PASS == 1) {
-          obuf[w][j * D + lane] = (uint8_t)L;
-        } else {
-          const int y = c * C + j;
-          const int base = __shfl_sync(kFull, my_base, j);
-          const bool skipped = y > 0 && base == kInvalidShort;
-          float dv = kInvalidFloat;
-          if (y >= Q.ylo && y <= Q.yhi && y < Q.rows) {  // uniform over the warp
-            const uint32_t S = (L & 0xFFu) + cbuf[w][buf][1][j * D + lane] + cbuf[w][buf][2][j * D + lane] +
-                               cbuf[w][buf][3][j * D + lane];
-            if (col_ok && !skipped && base != kInvalidShort) {
-              if (Q.tie_rule == kTieRefB200) {
-                dv = wta_pixel_init_ref(S, lane, base, Q);
-              } else {
-                uint32_t S1[1] = {S};
-                dv = wta_pixel<1>(S1, lane, base, Q, 1, y);
-              }
-            }
-          }
-          if (lane == j) dv_keep = dv;
-        }
-      }
+      fl[j] = par[w][0][j];
+      pp[j] = par[w][1][j];
+      cvr[j] = cbuf[w][buf][0][j * D + lane];
+    }
+    // all 32 steps run (steps past a short last chunk are marked skipped and store nothing)
+#pragma unroll
+    for (int j = 0; j < C; ++j) {
+      if (c == 0 && j == 0) L = cvr[0];
+      else scan_step(L, cvr[j], fl[j], pp[j], P.p1);
+      if (j < n) obuf[w][j * D + lane] = (uint8_t)L;
+    }
+    __syncwarp();
+    float dv_keep = kInvalidFloat;  // lane j: the disparity of step j (PASS 2)
+    if constexpr (PASS == 2) {
+      // the WTA of the chunk's pixels, lane j = pixel j (off the steps' dependency chain)
+      const int y = c * C + lane;
+      const int base = (int)(int16_t)(par[w][0][lane] >> 16);
+      const bool skipped = y > 0 && base == kInvalidShort;
+      if (lane < n && y >= Q.ylo && y <= Q.yhi && y < Q.rows && col_ok && !skipped && base != kInvalidShort)
+        dv_keep = init_wta_serial(obuf[w] + lane * D, cbuf[w][buf][1] + lane * D, cbuf[w][buf][2] + lane * D,
+                                  cbuf[w][buf][3] + lane * D, base, Q);
     }
     __syncwarp();
     if (lane < n) {
