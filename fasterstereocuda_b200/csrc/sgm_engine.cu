@@ -482,6 +482,33 @@ int launch_cols3_pass(sgm_engine* e, int G, const sgm::PlainParams& P, const sgm
   }
 }
 
+// Warp-per-scanline kernels (variant 4, D <= 128): the row scans, and the column passes (pass 1
+// bottom-to-top, pass 2 top-to-bottom + sum + WTA).
+template <int K>
+int launch_rows4(sgm_engine* e, const sgm::PlainParams& P, int nv, cudaStream_t s) {
+  if constexpr (K <= 4) {
+    constexpr int wpb = sgm::hscan_plain4_warps<K>();
+    const int blocks = (nv * 2 * e->H + wpb - 1) / wpb;
+    return SGM_LAUNCH(e, s, "hpaths_plain",
+                      sgm::k_hscan_plain4<K><<<blocks, 32 * wpb, 0, s>>>(e->cost, e->lr, e->rl, P, nv));
+  } else {
+    return SGM_ERR_UNSUPPORTED;
+  }
+}
+
+template <int K, int PASS>
+int launch_cols4(sgm_engine* e, const sgm::PlainParams& P, const sgm::WtaParams& Q, float* wta, int nv,
+                 cudaStream_t s) {
+  if constexpr (K <= 4) {
+    constexpr int wpb = sgm::vscan_plain4_warps<K>();
+    const dim3 grid((e->W + wpb - 1) / wpb, nv);
+    return SGM_LAUNCH(e, s, PASS == 1 ? "vpaths_bt_plain" : "vpaths_wta_plain",
+                      sgm::k_vscan_plain4<K, PASS><<<grid, 32 * wpb, 0, s>>>(e->cost, e->lr, e->rl, e->bt, wta, P, Q));
+  } else {
+    return SGM_ERR_UNSUPPORTED;
+  }
+}
+
 // The bottom-to-top column pass depends only on the cost volume, so it runs on the matcher's side
 // stream while the row scans run on s; the top-to-bottom pass (which sums all four paths) follows
 // the join. In a captured graph the side stream joins the capture through ev_fork.
@@ -513,10 +540,14 @@ int launch_plain(sgm_engine* e, const Word* csl, const Word* csr, float* wta) {
                      e->opt.p2_init >= e->opt.p1 &&
                      (e->ext.tie_rule == sgm::kTieLowest || e->ext.tie_rule == sgm::kTieRefB200);
   int st;
-  // variant 4 exists for the 32-disparity levels only; plain levels take the default for it
-  const int tune_row = e->tune_row_kernel == 4 ? 0 : e->tune_row_kernel;
-  const int tune_col = e->tune_col_kernel == 4 ? 0 : e->tune_col_kernel;
+  // warp-per-scanline kernels: D <= 128 and the tie rules of their serial WTA; otherwise the
+  // default takes their place
+  const bool v4_ok = K <= 4 && (e->ext.tie_rule == sgm::kTieLowest || e->ext.tie_rule == sgm::kTieHighest ||
+                                e->ext.tie_rule == sgm::kTieRefB200);
+  const int tune_row = e->tune_row_kernel == 4 && !v4_ok ? 0 : e->tune_row_kernel;
+  const int tune_col = e->tune_col_kernel == 4 && !v4_ok ? 0 : e->tune_col_kernel;
   const bool cols_v3 = (tune_col == 3 || tune_col == 0) && v3_ok;
+  const bool cols_v4 = tune_col == 4;
   sgm::WtaParams Q;
   Q.uniqueness = e->opt.unique_threshold;
   Q.tie_rule = e->ext.tie_rule;
@@ -525,20 +556,27 @@ int launch_plain(sgm_engine* e, const Word* csl, const Word* csr, float* wta) {
   Q.dmax_excl = warp_kernel ? 32 * K : 32 * K - 1;
   Q.dstride = e->npix();
   Q.image_border(e->W, e->H);
-  if ((tune_row == 3 || tune_row == 0) && v3_ok) {
+  if (((tune_row == 3 || tune_row == 0) && v3_ok) || tune_row == 4) {
     dim3 cg((e->W + 127) / 128, e->H, nv);
     st = SGM_LAUNCH(e, e->stream, "cost", sgm::k_cost3<K, Word><<<cg, 128, 0, e->stream>>>(csl, csr, e->cost, P));
     if (st) return st;
-    if (kSplitColumns && cols_v3) {
+    const auto rows = [&](cudaStream_t ms) {
+      return tune_row == 4 ? launch_rows4<K>(e, P, nv, ms) : launch_rows3<K>(e, e->tune_row_lanes, P, nv, ms);
+    };
+    if (kSplitColumns && (cols_v3 || cols_v4)) {
       e->bt_stored = true;
       const int gc = e->tune_col_lanes;
       st = fork_join(
-          e, e->stream, [&](cudaStream_t ss) { return launch_cols3_pass<K, 1>(e, gc, P, Q, wta, nv, ss); },
-          [&](cudaStream_t ms) { return launch_rows3<K>(e, e->tune_row_lanes, P, nv, ms); });
+          e, e->stream,
+          [&](cudaStream_t ss) {
+            return cols_v4 ? launch_cols4<K, 1>(e, P, Q, wta, nv, ss) : launch_cols3_pass<K, 1>(e, gc, P, Q, wta, nv, ss);
+          },
+          rows);
       if (st) return st;
-      return launch_cols3_pass<K, 2>(e, gc, P, Q, wta, nv, e->stream);
+      return cols_v4 ? launch_cols4<K, 2>(e, P, Q, wta, nv, e->stream)
+                     : launch_cols3_pass<K, 2>(e, gc, P, Q, wta, nv, e->stream);
     }
-    st = launch_rows3<K>(e, e->tune_row_lanes, P, nv, e->stream);
+    st = rows(e->stream);
   } else if (tune_row == 1) {  // whole census rows of R scanlines in shared memory
     const int R = e->tune_rows > 0 ? e->tune_rows : rows_per_cta(e->W, sizeof(Word), false);
     const size_t smem = (size_t)R * 2 * e->W * sizeof(Word);
@@ -564,6 +602,11 @@ int launch_plain(sgm_engine* e, const Word* csl, const Word* csr, float* wta) {
   if (cols_v3) {
     e->bt_stored = true;
     return launch_cols3_pass<K, 0>(e, e->tune_col_lanes, P, Q, wta, nv, e->stream);
+  }
+  if (cols_v4) {
+    e->bt_stored = true;
+    st = launch_cols4<K, 1>(e, P, Q, wta, nv, e->stream);
+    return st ? st : launch_cols4<K, 2>(e, P, Q, wta, nv, e->stream);
   }
   if (tune_col != 2) {
     C = e->tune_cols > 0 ? e->tune_cols : 8;

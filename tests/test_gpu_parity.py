@@ -78,16 +78,17 @@ CASES = {
 
 
 SCANLINE = {"warp": (2, 0, 1, 0, 0, 0, 0), "scanline_g1": (3, 0, 3, 0, 0, 1, 1),
-            "scanline_g8": (3, 0, 3, 0, 0, 8, 8)}
+            "scanline_g8": (3, 0, 3, 0, 0, 8, 8), "latency": (4, 0, 4, 0, 0, 0, 0)}
 
 
 @pytest.mark.parametrize("name", list(CASES))
 @pytest.mark.parametrize("tie", [4, 0, 2])
-@pytest.mark.parametrize("variant", ["default", "warp", "scanline_g1", "scanline_g8"])
+@pytest.mark.parametrize("variant", ["default", "warp", "scanline_g1", "scanline_g8", "latency"])
 def test_plain_parity(engine_lib, oracle_mod, name, tie, variant):
     """Every stage against the oracle. 'default' runs the u16x2 scanline kernels where they are
     exact (else the warp kernels), 'warp' the lane-per-disparity kernels, 'scanline_g*' the
-    scanline kernels with one and eight lanes per scanline."""
+    scanline kernels with one and eight lanes per scanline, 'latency' the warp-per-scanline
+    kernels with bulk-copied chunks (the default takes their place for D = 256 and tie rule 2)."""
     import fasterstereocuda_b200 as fsc
     O = oracle_mod
     W, H, M, D, cs, p1, p2, u, lr, med, peaks, morph, seed = CASES[name]
@@ -97,7 +98,7 @@ def test_plain_parity(engine_lib, oracle_mod, name, tie, variant):
     ratio = 0.005 if peaks else 0.0005
     s = make_engine(fsc, W, H, M, D, cs, p1, p2, u, lr, med, peaks, ratio, morph, tie)
     if variant != "default":
-        if tie != 4 and variant != "warp":
+        if tie != 4 and variant not in ("warp", "latency"):
             pytest.skip("tie rule variants with the default lane split only")
         assert s.set_tuning(fsc.Tuning(*SCANLINE[variant])), s.last_error()
     disp = np.empty((H, W), np.float32)
