@@ -6,6 +6,7 @@
 // FasterStereoCuda.cpp:201-635). Differences by design: all allocation happens in init;
 // a match is one stream of kernels with no host synchronisation inside it; small-region
 // removal runs on the GPU; the pyramid keeps every level on the device.
+#include <cuda.h>  // CUtensorMap, cuTensorMapEncodeTiled (looked up through the runtime)
 #include <cuda_runtime.h>
 #include <nvtx3/nvToolsExt.h>
 
@@ -202,6 +203,13 @@ struct sgm_engine {
   int tune_row_lanes = 0;   // variant 3: lanes per scanline (0: default)
   int tune_col_lanes = 0;
   bool bt_stored = true;    // the last match wrote the bottom->top volume to global memory
+  // tensor maps of the cost, bt, lr and rl volumes for the column kernels' box copies, and what
+  // each was built for (base, W, H, D, views)
+  CUtensorMap tmap[4];
+  struct TmapKey {
+    const void* base = nullptr;
+    int W = 0, H = 0, D = 0, nv = 0;
+  } tmap_key[4];
   // img[0], img[1] -> out captured as a CUDA graph after a first direct run (matches without
   // initial disparities or a right map); later matches copy in, launch it, copy out.
   cudaGraphExec_t gexec = nullptr;
@@ -482,6 +490,52 @@ int launch_cols3_pass(sgm_engine* e, int G, const sgm::PlainParams& P, const sgm
   }
 }
 
+// cuTensorMapEncodeTiled from the driver, looked up once through the runtime (no link against
+// the driver library).
+using EncodeTiledFn = decltype(&cuTensorMapEncodeTiled);
+EncodeTiledFn encode_tiled() {
+  static const EncodeTiledFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<EncodeTiledFn>(p);
+  }();
+  return fn;
+}
+
+// Tensor map i (0 cost, 1 bt, 2 lr, 3 rl) of the engine's volumes, [nv][H][W * D] bytes, in boxes
+// of 32 rows x D bytes with the D-byte swizzle (k_vscan_plain4); rebuilt when the volume moved.
+int volume_map(sgm_engine* e, int i, const uint8_t* base, int nv, const CUtensorMap** out) {
+  sgm_engine::TmapKey& k = e->tmap_key[i];
+  if (k.base != base || k.W != e->W || k.H != e->H || k.D != e->D || k.nv != nv) {
+    const EncodeTiledFn fn = encode_tiled();
+    if (!fn) {
+      set_error(&e->err, "cuTensorMapEncodeTiled is not available from the driver");
+      return SGM_ERR_CUDA;
+    }
+    const cuuint64_t dims[3] = {(cuuint64_t)e->W * e->D, (cuuint64_t)e->H, (cuuint64_t)nv};
+    const cuuint64_t strides[2] = {(cuuint64_t)e->W * e->D, (cuuint64_t)e->W * e->H * e->D};
+    const cuuint32_t box[3] = {(cuuint32_t)e->D, (cuuint32_t)sgm::kScanChunk, 1u};
+    const cuuint32_t estr[3] = {1u, 1u, 1u};
+    const CUtensorMapSwizzle sw = e->D == 32   ? CU_TENSOR_MAP_SWIZZLE_32B
+                                  : e->D == 64 ? CU_TENSOR_MAP_SWIZZLE_64B
+                                               : CU_TENSOR_MAP_SWIZZLE_128B;
+    const CUresult r = fn(&e->tmap[i], CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<uint8_t*>(base), dims, strides,
+                          box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+      k = sgm_engine::TmapKey{};
+      set_error(&e->err, "cuTensorMapEncodeTiled failed (%d) for a %dx%dx%d volume", (int)r, e->W, e->H, e->D);
+      return SGM_ERR_CUDA;
+    }
+    k = sgm_engine::TmapKey{base, e->W, e->H, e->D, nv};
+  }
+  *out = &e->tmap[i];
+  return SGM_OK;
+}
+
 // Warp-per-scanline kernels (variant 4, D <= 128): the row scans, and the column passes (pass 1
 // bottom-to-top, pass 2 top-to-bottom + sum + WTA).
 template <int K>
@@ -502,8 +556,14 @@ int launch_cols4(sgm_engine* e, const sgm::PlainParams& P, const sgm::WtaParams&
   if constexpr (K <= 4) {
     constexpr int wpb = sgm::vscan_plain4_warps<K>();
     const dim3 grid((e->W + wpb - 1) / wpb, nv);
+    const CUtensorMap *mc, *mb, *ml, *mr;
+    int st = volume_map(e, 0, e->cost, nv, &mc);
+    if (!st) st = volume_map(e, 1, e->bt, nv, &mb);
+    if (!st) st = volume_map(e, 2, e->lr, nv, &ml);
+    if (!st) st = volume_map(e, 3, e->rl, nv, &mr);
+    if (st) return st;
     return SGM_LAUNCH(e, s, PASS == 1 ? "vpaths_bt_plain" : "vpaths_wta_plain",
-                      sgm::k_vscan_plain4<K, PASS><<<grid, 32 * wpb, 0, s>>>(e->cost, e->lr, e->rl, e->bt, wta, P, Q));
+                      sgm::k_vscan_plain4<K, PASS><<<grid, 32 * wpb, 0, s>>>(*mc, *mb, *ml, *mr, e->bt, wta, P, Q));
   } else {
     return SGM_ERR_UNSUPPORTED;
   }

@@ -19,6 +19,8 @@
 // Every wait on an mbarrier is bounded: after kMaxWaitTries polls the warp records the timeout in
 // g_scan_wait_timeouts (read by sgm_debug_wait_timeouts) and stops.
 #pragma once
+#include <cuda.h>  // CUtensorMap
+
 #include <type_traits>
 
 #include "sgm_kernels3.cuh"
@@ -416,16 +418,19 @@ __global__ void __launch_bounds__(32 * WPB) k_vscan_init4(const uint8_t* __restr
 namespace sgm {
 
 // =============================================================================================
-// Plain levels (no initial disparities), latency form. One warp owns a scanline; lane l holds
-// d = l + 32k, k < K, in 32 bits (the reference's Kernel_Aggregate_*_Warpfor{32,64,128},
-// cusgm_ca.cu:1343-1888, computes the same recurrence). A step:
+// Plain levels (no initial disparities), latency form. One warp owns a scanline; lane l holds the
+// K consecutive disparities d = K l + k in 32 bits, the reference's lane mapping
+// (Kernel_Aggregate_*_Warpfor{32,64,128}, cusgm_ca.cu:1343-1888). A step:
 //   m = min_d L(d)                       one redux.sync of the lanes' K-wide minima
-//   L(d - 1), L(d + 1)                   2K shuffles (lane - 1 / lane + 1, across the k words)
+//   L(d - 1) + P1, L(d + 1) + P1         in the lane, or one shuffle up / down at its edges
 //   L'(d) = C(d) + min(L(d), L(d-1) + P1 | 127, L(d+1) + P1 | 127, m + P2) - m
+// and a lane moves its K bytes of costs and path costs as one 8/16/32-bit shared access.
 // Chunks of 32 steps move between global and shared memory with bulk async copies; a step's path
 // costs overwrite its costs in the chunk buffer, which then leaves with a bulk store (rows: one
-// contiguous copy; columns: one per step), three buffers deep so a load never waits for the store
-// of the chunk before. The WTA of the top-to-bottom pass runs per chunk with lane = pixel.
+// contiguous copy; columns: one tensor-map box of 32 rows), three buffers deep so a load never
+// waits for the store of the chunk before. Every chunk runs all 32 steps: the steps past a scanline's end read and
+// write rows of the buffer that hold nothing of this scanline and are neither stored nor used.
+// The WTA of the top-to-bottom pass runs per chunk with lane = pixel.
 // =============================================================================================
 
 // `bytes` (a multiple of 16) from shared src to global dst (both 16-byte aligned), in the calling
@@ -451,10 +456,22 @@ __device__ __forceinline__ void scan_give_up_mask(uint64_t* bars, uint32_t phase
     if ((pending >> b) & 1u) mbar_wait(bars + b, (phase >> b) & 1u);
 }
 
-// Shared-memory row of one step: D bytes padded to D + 16, so that 16-byte loads of 8 lanes at
-// consecutive rows fall in distinct banks.
-template <int D>
-__host__ __device__ constexpr int plain_row_stride() { return D + 16; }
+// A lane's K bytes of a step row, as one shared-memory word.
+template <int K>
+using LaneBytes = std::conditional_t<K == 1, uint8_t, std::conditional_t<K == 2, uint16_t, uint32_t>>;
+
+template <int K>
+__device__ __forceinline__ void unpack_bytes(uint32_t w, uint32_t (&c)[K]) {
+#pragma unroll
+  for (int k = 0; k < K; ++k) c[k] = k == 0 && K == 1 ? w : __byte_perm(w, 0u, 0x4440u + k);
+}
+template <int K>
+__device__ __forceinline__ uint32_t pack_bytes(const uint32_t (&L)[K]) {
+  if constexpr (K == 1) return L[0];
+  if constexpr (K == 2) return __byte_perm(L[0], L[1], 0x0040u);
+  if constexpr (K == 4) return __byte_perm(__byte_perm(L[0], L[1], 0x0040u), __byte_perm(L[2], L[3], 0x0040u), 0x5410u);
+  return 0u;
+}
 
 template <int K>
 __device__ __forceinline__ void plain_step4(uint32_t (&L)[K], const uint32_t (&c)[K], uint32_t p1, uint32_t p2) {
@@ -463,65 +480,51 @@ __device__ __forceinline__ void plain_step4(uint32_t (&L)[K], const uint32_t (&c
 #pragma unroll
   for (int k = 1; k < K; ++k) lm = min(lm, L[k]);
   const uint32_t m = __reduce_min_sync(kFull, lm);
-  uint32_t r[K], q[K];
+  uint32_t Lp[K];
 #pragma unroll
-  for (int k = 0; k < K; ++k) {
-    r[k] = __shfl_sync(kFull, L[k], (lane + 31) & 31);  // L(d - 1), lanes 1..31
-    q[k] = __shfl_sync(kFull, L[k], (lane + 1) & 31);   // L(d + 1), lanes 0..30
-  }
+  for (int k = 0; k < K; ++k) Lp[k] = L[k] + p1;
+  const uint32_t up = __shfl_up_sync(kFull, Lp[K - 1], 1);  // L(K l - 1) + P1 from lane l - 1
+  const uint32_t dn = __shfl_down_sync(kFull, Lp[0], 1);    // L(K l + K) + P1 from lane l + 1
+  const uint32_t a0 = lane > 0 ? up : kInvalidCost;
+  const uint32_t bK = lane < 31 ? dn : kInvalidCost;
   const uint32_t l4 = m + p2;
-  uint32_t n[K];
 #pragma unroll
   for (int k = 0; k < K; ++k) {
-    // lane 0: d - 1 is lane 31 of word k - 1 (its r[k - 1]); lane 31: d + 1 is lane 0 of word k + 1
-    const uint32_t A = lane > 0 ? r[k] + p1 : (k > 0 ? r[k - 1] + p1 : kInvalidCost);
-    const uint32_t B = lane < 31 ? q[k] + p1 : (k < K - 1 ? q[k + 1] + p1 : kInvalidCost);
+    const uint32_t A = k == 0 ? a0 : Lp[k - 1];
+    const uint32_t B = k == K - 1 ? bK : Lp[k + 1];
     const uint32_t t = min(__vimin3_u32(L[k], A, B), l4);
-    n[k] = c[k] + (t - m);
+    L[k] = c[k] + t - m;
   }
-#pragma unroll
-  for (int k = 0; k < K; ++k) L[k] = n[k];
 }
 
-// The 32 steps of a chunk held in shared memory: step j reads its costs from row(j) (byte
-// lane + 32k) and leaves its path costs there. first: step 0 starts the scanline (L = C).
-// Costs are read R steps ahead.
-template <int K, typename RowOf>
-__device__ __forceinline__ void plain_chunk(uint8_t* buf, RowOf row, int n, bool first, uint32_t (&L)[K],
-                                            uint32_t p1, uint32_t p2) {
-  constexpr int C = kScanChunk, R = 32 / K;
-  const int lane = threadIdx.x & 31;
-  uint32_t ring[R][K];
+// The 32 steps of a chunk held in shared memory: at step j this lane reads its K bytes of costs
+// at at(j) (a LaneBytes<K> pointer) and leaves its path costs there. first: step 0 starts the
+// scanline (L = C). Costs are read R steps ahead.
+template <int K, typename At>
+__device__ __forceinline__ void plain_chunk(At at, bool first, uint32_t (&L)[K], uint32_t p1, uint32_t p2) {
+  constexpr int C = kScanChunk, R = 16;
+  uint32_t ring[R];
 #pragma unroll
-  for (int j = 0; j < R; ++j)
-#pragma unroll
-    for (int k = 0; k < K; ++k) ring[j][k] = j < n ? buf[row(j) + lane + 32 * k] : 0u;
+  for (int j = 0; j < R; ++j) ring[j] = *at(j);
 #pragma unroll
   for (int j = 0; j < C; ++j) {
-    if (j < n) {  // uniform over the warp
-      uint32_t c[K];
+    uint32_t c[K];
+    unpack_bytes<K>(ring[j % R], c);
+    if (j + R < C) ring[j % R] = *at(j + R);
+    if (j == 0 && first) {
 #pragma unroll
-      for (int k = 0; k < K; ++k) c[k] = ring[j % R][k];
-      if (j + R < C && j + R < n) {
-#pragma unroll
-        for (int k = 0; k < K; ++k) ring[j % R][k] = buf[row(j + R) + lane + 32 * k];
-      }
-      if (j == 0 && first) {
-#pragma unroll
-        for (int k = 0; k < K; ++k) L[k] = c[k];
-      } else {
-        plain_step4<K>(L, c, p1, p2);
-      }
-      uint8_t* o = buf + row(j) + lane;
-#pragma unroll
-      for (int k = 0; k < K; ++k) o[32 * k] = (uint8_t)L[k];
+      for (int k = 0; k < K; ++k) L[k] = c[k];
+    } else {
+      plain_step4<K>(L, c, p1, p2);
     }
+    *at(j) = (LaneBytes<K>)pack_bytes<K>(L);
   }
 }
 
 // Horizontal scans of a plain level; warp (blockIdx.x * WPB + w) owns scanline i = (view, dir, y)
 // as in hpaths3_lane. A chunk is 32 consecutive pixels of the row: one contiguous bulk copy in,
-// one out.
+// one out. Right-to-left scans place a short (last) chunk at the end of the buffer, so that step
+// j of every chunk reads row 31 - j.
 template <int K>
 __host__ __device__ constexpr int hscan_plain4_warps() { return K == 4 ? 2 : 4; }
 
@@ -550,11 +553,12 @@ __global__ void __launch_bounds__(32 * WPB) k_hscan_plain4(const uint8_t* __rest
   const int nch = (len + C - 1) / C;
   auto chunk_n = [&](int c) { return min(C, len - c * C); };
   auto chunk_x = [&](int c) { return dir == 0 ? P.x0 + c * C : W - (c * C + chunk_n(c)); };
+  auto chunk_off = [&](int c) { return dir == 0 ? 0 : (C - chunk_n(c)) * D; };  // bytes into the buffer
   auto issue = [&](int c) {  // lane 0
     const int b = c % NB;
     const uint32_t bytes = (uint32_t)chunk_n(c) * D;
     mbar_expect_tx(&bars[w][b], bytes);
-    bulk_to_smem(cbuf[w][b], crow + (size_t)chunk_x(c) * D, bytes, &bars[w][b]);
+    bulk_to_smem(cbuf[w][b] + chunk_off(c), crow + (size_t)chunk_x(c) * D, bytes, &bars[w][b]);
   };
   if (lane == 0) {
     issue(0);
@@ -571,14 +575,15 @@ __global__ void __launch_bounds__(32 * WPB) k_hscan_plain4(const uint8_t* __rest
     }
     phase ^= 1u << b;
     __syncwarp();
+    LaneBytes<K>* lb = reinterpret_cast<LaneBytes<K>*>(cbuf[w][b]) + lane;
     if (dir == 0)
-      plain_chunk<K>(cbuf[w][b], [](int j) { return j * D; }, n, c == 0, L, P.p1, P.p2);
+      plain_chunk<K>([lb](int j) { return lb + j * 32; }, c == 0, L, P.p1, P.p2);
     else
-      plain_chunk<K>(cbuf[w][b], [n](int j) { return (n - 1 - j) * D; }, n, c == 0, L, P.p1, P.p2);
+      plain_chunk<K>([lb](int j) { return lb + (C - 1 - j) * 32; }, c == 0, L, P.p1, P.p2);
     fence_proxy_async();  // the chunk's path costs (and its cost reads) before the bulk copies
     __syncwarp();
     if (lane == 0) {
-      bulk_to_global(orow + (size_t)chunk_x(c) * D, cbuf[w][b], (uint32_t)n * D);
+      bulk_to_global(orow + (size_t)chunk_x(c) * D, cbuf[w][b] + chunk_off(c), (uint32_t)n * D);
       bulk_commit();
       if (c + 2 < nch) {
         bulk_wait_read<1>();  // the store of chunk c - 1 has left the buffer chunk c + 2 goes to
@@ -590,62 +595,79 @@ __global__ void __launch_bounds__(32 * WPB) k_hscan_plain4(const uint8_t* __rest
 }
 
 // WTA of one plain-level pixel from its four path rows (D bytes each), by one lane:
-// Kernel_ComputeDisparityByWTA_Warpfor{32,64,128} (cusgm_ca.cu:3514-3809). S(d) is summed in
-// 16-bit halves (at most 4 x 255). d* = 0 or d* >= Q.dmax_excl -> INVALID; c3 at d* = D - 1 is
-// the index itself; uniqueness and the +0.5-shifted parabola as in wta_pixel. Tie rules: kTieRefB200
-// at D = 64 (A = {t < 32 : S(t) = m}, B = {t < 32 : S(t + 32) = m, S(t) != m}; even rows of the
-// launch take the lowest of B (+ 32) if any, else of A; odd rows the lowest of A if any, else of B
-// (+ 32)); kTieHighest the highest tied d; the rest the lowest.
+// Kernel_ComputeDisparityByWTA_Warpfor{32,64,128} (cusgm_ca.cu:3514-3809). S(d) (at most 4 x 255)
+// is summed in 16-bit halves and searched as the 16-bit key S(d) * 64 + (d mod 64) -- the lowest
+// key of a block of 64 disparities is its minimum at its lowest d (with 63 - (d mod 64): at its
+// highest d). d* = 0 or d* >= Q.dmax_excl -> INVALID; c3 at d* = D - 1 is the index itself;
+// uniqueness and the +0.5-shifted parabola as in wta_pixel. Tie rules: kTieRefB200 at D = 64
+// (A = {t < 32 : S(t) = m}, B = {t < 32 : S(t + 32) = m, S(t) != m}; even rows of the launch take
+// the lowest of B (+ 32) if any, else of A; odd rows the lowest of A if any, else of B (+ 32));
+// kTieHighest the highest tied d; the rest the lowest.
+// a, b, c, e: the pixel's rows in four swizzled boxes (16-byte unit u of the row at u ^ sw).
 template <int D>
 __device__ __forceinline__ float plain_wta_rows(const uint8_t* a, const uint8_t* b, const uint8_t* c,
-                                                const uint8_t* e, int min_d, int y, const WtaParams& Q) {
-  constexpr int NW = D / 4, NB = D / 32;
-  constexpr uint32_t M8 = 0x00FF00FFu;
-  uint32_t lo[NW], hi[NW];  // lo[k] = S(4k) | S(4k + 2) << 16, hi[k] = S(4k + 1) | S(4k + 3) << 16
+                                                const uint8_t* e, int sw, int min_d, int y, const WtaParams& Q) {
+  constexpr int SPLIT = D == 64 ? 32 : 64;  // first d of the second key block (D = 64: A / B halves)
+  const bool high = Q.tie_rule == kTieHighest;
+  const uint32_t flip = high ? 63u * 0x10001u : 0u;
+  uint32_t acc0 = 0xFFFFFFFFu, acc1 = 0xFFFFFFFFu;
 #pragma unroll
   for (int q = 0; q < D / 16; ++q) {
-    const uint4 va = reinterpret_cast<const uint4*>(a)[q], vb = reinterpret_cast<const uint4*>(b)[q];
-    const uint4 vc = reinterpret_cast<const uint4*>(c)[q], ve = reinterpret_cast<const uint4*>(e)[q];
+    const int u = q ^ sw;
+    const uint4 va = reinterpret_cast<const uint4*>(a)[u], vb = reinterpret_cast<const uint4*>(b)[u];
+    const uint4 vc = reinterpret_cast<const uint4*>(c)[u], ve = reinterpret_cast<const uint4*>(e)[u];
     const uint32_t wa[4] = {va.x, va.y, va.z, va.w}, wb[4] = {vb.x, vb.y, vb.z, vb.w};
     const uint32_t wc[4] = {vc.x, vc.y, vc.z, vc.w}, we[4] = {ve.x, ve.y, ve.z, ve.w};
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
-      lo[4 * q + t] = (wa[t] & M8) + (wb[t] & M8) + (wc[t] & M8) + (we[t] & M8);
-      hi[4 * q + t] = ((wa[t] >> 8) & M8) + ((wb[t] >> 8) & M8) + ((wc[t] >> 8) & M8) + ((we[t] >> 8) & M8);
+      const int d0 = 16 * q + 4 * t;  // the word's first disparity
+      // lo = S(d0) | S(d0 + 2) << 16, hi = S(d0 + 1) | S(d0 + 3) << 16
+      const uint32_t lo = __byte_perm(wa[t], 0u, 0x4240u) + __byte_perm(wb[t], 0u, 0x4240u) +
+                          __byte_perm(wc[t], 0u, 0x4240u) + __byte_perm(we[t], 0u, 0x4240u);
+      const uint32_t hi = __byte_perm(wa[t], 0u, 0x4341u) + __byte_perm(wb[t], 0u, 0x4341u) +
+                          __byte_perm(wc[t], 0u, 0x4341u) + __byte_perm(we[t], 0u, 0x4341u);
+      const uint32_t dlo = (uint32_t)(d0 & 63) | ((uint32_t)((d0 + 2) & 63) << 16);
+      const uint32_t dhi = dlo + 0x10001u;
+      const uint32_t klo = (lo << 6) | (dlo ^ flip), khi = (hi << 6) | (dhi ^ flip);
+      if (d0 < SPLIT) acc0 = __vimin3_u16x2(acc0, klo, khi);
+      else acc1 = __vimin3_u16x2(acc1, klo, khi);
     }
   }
-  uint32_t mm = __vminu2(lo[0], hi[0]);
-#pragma unroll
-  for (int k = 1; k < NW; ++k) mm = __vminu2(mm, __vminu2(lo[k], hi[k]));
-  const uint32_t m = min(mm & 0xFFFFu, mm >> 16);
-  const uint32_t m2 = m * 0x10001u;
-  uint32_t word[NB];  // bit t of word[k]: S(32k + t) == m
-#pragma unroll
-  for (int k = 0; k < NB; ++k) word[k] = 0u;
-#pragma unroll
-  for (int k = 0; k < NW; ++k) {
-    const uint32_t el = __vcmpeq2(lo[k], m2), eh = __vcmpeq2(hi[k], m2);
-    const uint32_t nib = (el & 1u) | ((eh & 1u) << 1) | ((el >> 14) & 4u) | ((eh >> 13) & 8u);
-    word[k / 8] |= nib << (4 * (k % 8));
-  }
+  const uint32_t k0 = min(acc0 & 0xFFFFu, acc0 >> 16), k1 = min(acc1 & 0xFFFFu, acc1 >> 16);
+  const uint32_t s0 = k0 >> 6, s1 = k1 >> 6;
+  // the disparities of the two keys (block 1 of D = 128 starts at 64; D = 64's halves share d mod 64 = d)
+  const int t0 = (int)((k0 & 63u) ^ (flip & 63u)), t1 = (D == 128 ? 64 : 0) + (int)((k1 & 63u) ^ (flip & 63u));
+  uint32_t m;
   int ds;
-  if (D == 64 && Q.tie_rule == kTieRefB200) {
-    const uint32_t A = word[0], B = word[NB - 1] & ~word[0];
-    if ((y & 1) == 0) ds = B ? (__ffs(B) - 1 + 32) : (__ffs(A) - 1);
-    else ds = A ? (__ffs(A) - 1) : (__ffs(B) - 1 + 32);
-  } else if (Q.tie_rule == kTieHighest) {
-    ds = -1;
-#pragma unroll
-    for (int k = 0; k < NB; ++k)
-      if (word[k]) ds = 32 * k + 31 - __clz(word[k]);
+  if constexpr (D == 32) {
+    m = s0;
+    ds = t0;
   } else {
-    ds = -1;
-#pragma unroll
-    for (int k = NB - 1; k >= 0; --k)
-      if (word[k]) ds = 32 * k + __ffs(word[k]) - 1;
+    m = min(s0, s1);
+    // the lowest (highest) tied d of the two blocks
+    ds = s0 < s1 || (s0 == s1 && !high) ? t0 : t1;
+    if (D == 64 && Q.tie_rule == kTieRefB200 && s0 == s1) {
+      // both halves hold the minimum: odd rows take A's lowest (t0); even rows B's lowest if B is
+      // not empty (a t with S(t + 32) = m and S(t) != m; rare, searched directly)
+      ds = t0;
+      if ((y & 1) == 0) {
+        for (int t = 0; t < 32; ++t) {
+          const int ob = (t + 32) ^ (sw << 4), oa = t ^ (sw << 4);
+          const uint32_t sb = (uint32_t)a[ob] + b[ob] + c[ob] + e[ob];
+          const uint32_t sa = (uint32_t)a[oa] + b[oa] + c[oa] + e[oa];
+          if (sb == m && sa != m) {
+            ds = t + 32;
+            break;
+          }
+        }
+      }
+    }
   }
   if (ds <= 0 || ds >= Q.dmax_excl) return kInvalidFloat;
-  auto sum_at = [&](int d) { return (uint32_t)a[d] + b[d] + c[d] + e[d]; };
+  auto sum_at = [&](int d) {
+    const int o = d ^ (sw << 4);
+    return (uint32_t)a[o] + b[o] + c[o] + e[o];
+  };
   const float c1 = (float)sum_at(ds - 1);
   const float c2 = (float)m;
   const float c3 = (ds + 1 < D) ? (float)sum_at(ds + 1) : (float)ds;
@@ -655,24 +677,50 @@ __device__ __forceinline__ float plain_wta_rows(const uint8_t* a, const uint8_t*
   return __fadd_rn((float)(ds + min_d), subpix_bias(c1, c2, c3));
 }
 
-// Warps per CTA of the column kernels (shared memory: PASS 1 three chunk buffers, PASS 2 two
-// chunk buffers and the three stored paths of a chunk, each C x (D + 16) bytes per warp).
+// Column chunks are boxes of 32 rows x D bytes of one view's volume, copied by the tensor-memory
+// accelerator (a 3D tensor map: bytes of a row, rows, views) with the 32/64/128-byte swizzle: the
+// 16-byte unit u of box row r lands at unit u ^ box_sw(r) (bits 4.. of the shared address XORed
+// with bits 7..), so that 8 lanes reading 8 consecutive rows hit distinct banks.
+template <int D>
+__host__ __device__ constexpr int box_sw(int r) { return ((r * D) >> 7) & (D / 16 - 1); }
+
+// One box from global memory (tensor coordinates x = byte of the row, y = row, z = view; rows
+// outside the tensor read as 0), completing on bar.
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+// One box to global memory (y >= 0), in the calling thread's current bulk group.
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, int x, int y, int z, const void* src) {
+  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(map),
+               "r"(x), "r"(y), "r"(z), "r"(smem_u32(src))
+               : "memory");
+}
+
+// Warps per CTA of the column kernels (shared memory per warp: PASS 1 three boxes, PASS 2 two
+// boxes of costs and three of stored paths, C x D bytes each).
 template <int K>
-__host__ __device__ constexpr int vscan_plain4_warps() { return K == 1 ? 4 : 2; }
+__host__ __device__ constexpr int vscan_plain4_warps() { return K == 4 ? 2 : 4; }
 
 // Vertical scans of a plain level: warp (blockIdx.x * WPB + w) owns column x of view blockIdx.y.
-// PASS 1: bottom to top, storing its path costs (bt). PASS 2: top to bottom, then per chunk the
-// WTA of its 32 pixels with lane = pixel (rows >= Q.rows INVALID, as the reference's two-row WTA
-// blocks leave them; border and columns left of x0 INVALID).
+// PASS 1: bottom to top over boxes ending at rows H - 32c (the last one starts above row 0 and
+// reads zeros there), storing its path costs (bt) box by box -- the last box row by row. PASS 2:
+// top to bottom over boxes starting at rows 32c, then per box the WTA of its pixels with lane =
+// pixel (rows >= Q.rows INVALID, as the reference's two-row WTA blocks leave them; border and
+// columns left of x0 INVALID). Maps: the cost, bt, lr and rl volumes, [views][H][W * D] bytes.
 template <int K, int PASS>
 __global__ void __launch_bounds__(32 * vscan_plain4_warps<K>())
-    k_vscan_plain4(const uint8_t* __restrict__ cost, const uint8_t* __restrict__ lr, const uint8_t* __restrict__ rl,
+    k_vscan_plain4(const __grid_constant__ CUtensorMap m_cost, const __grid_constant__ CUtensorMap m_bt,
+                   const __grid_constant__ CUtensorMap m_lr, const __grid_constant__ CUtensorMap m_rl,
                    uint8_t* __restrict__ bt, float* __restrict__ disp, PlainParams P, WtaParams Q) {
-  constexpr int D = 32 * K, C = kScanChunk, RS = plain_row_stride<D>();
+  constexpr int D = 32 * K, C = kScanChunk, BOX = C * D, NSW = D / 16;
   constexpr int WPB = vscan_plain4_warps<K>();
-  constexpr int NB = PASS == 1 ? 3 : 2;        // cost chunk buffers
-  constexpr int NS = PASS == 1 ? 0 : 3;        // stored-path buffers (bt, lr, rl)
-  __shared__ __align__(128) uint8_t cbuf[WPB][NB + NS][C * RS];
+  constexpr int NB = PASS == 1 ? 3 : 2;  // cost boxes
+  constexpr int NS = PASS == 1 ? 0 : 3;  // stored-path boxes (bt, lr, rl)
+  __shared__ __align__(1024) uint8_t cbuf[WPB][NB + NS][BOX];
   __shared__ __align__(8) uint64_t bars[WPB][NB + 1];  // bars[NB]: the stored paths
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   if (lane == 0) {
@@ -690,56 +738,72 @@ __global__ void __launch_bounds__(32 * vscan_plain4_warps<K>())
       for (int y = lane; y < H; y += 32) dout[(size_t)y * W] = kInvalidFloat;
     return;
   }
-  const size_t vo = (size_t)view * P.vstride + (size_t)x * D;
-  const size_t rs = (size_t)W * D;
+  // the swizzle pattern is a function of the shared address: the boxes must start on 1 KB
+  if (smem_u32(&cbuf[0][0][0]) & 1023u) {
+    if (lane == 0) atomicAdd(&g_scan_wait_timeouts, 1u);
+    return;
+  }
   const int nch = (H + C - 1) / C;
-  auto chunk_n = [&](int c) { return min(C, H - c * C); };
-  auto row_of = [&](int s) { return PASS == 1 ? H - 1 - s : s; };
-  // chunk c's cost rows into buffer c % NB (lane j: step j)
-  auto issue_cost = [&](int c) {
-    const int b = c % NB, n = chunk_n(c);
-    if (lane == 0) mbar_expect_tx(&bars[w][b], (uint32_t)(n * D));
-    __syncwarp();
-    if (lane < n) bulk_to_smem(cbuf[w][b] + lane * RS, cost + vo + (size_t)row_of(c * C + lane) * rs, D, &bars[w][b]);
+  auto box_y = [&](int c) { return PASS == 1 ? H - C * (c + 1) : C * c; };  // first row of chunk c's box
+  auto issue_cost = [&](int c) {  // lane 0
+    const int b = c % NB;
+    mbar_expect_tx(&bars[w][b], BOX);
+    tma_load_3d(cbuf[w][b], &m_cost, x * D, box_y(c), view, &bars[w][b]);
   };
-  // chunk c's stored paths (PASS 2)
-  auto issue_paths = [&](int c) {
-    const int n = chunk_n(c);
-    if (lane == 0) mbar_expect_tx(&bars[w][NB], (uint32_t)(3 * n * D));
-    __syncwarp();
-    if (lane < n) {
-      const size_t ro = vo + (size_t)row_of(c * C + lane) * rs;
-      bulk_to_smem(cbuf[w][NB + 0] + lane * RS, bt + ro, D, &bars[w][NB]);
-      bulk_to_smem(cbuf[w][NB + 1] + lane * RS, lr + ro, D, &bars[w][NB]);
-      bulk_to_smem(cbuf[w][NB + 2] + lane * RS, rl + ro, D, &bars[w][NB]);
-    }
+  auto issue_paths = [&](int c) {  // lane 0
+    mbar_expect_tx(&bars[w][NB], 3 * BOX);
+    tma_load_3d(cbuf[w][NB + 0], &m_bt, x * D, box_y(c), view, &bars[w][NB]);
+    tma_load_3d(cbuf[w][NB + 1], &m_lr, x * D, box_y(c), view, &bars[w][NB]);
+    tma_load_3d(cbuf[w][NB + 2], &m_rl, x * D, box_y(c), view, &bars[w][NB]);
   };
-  issue_cost(0);
-  if (nch > 1) issue_cost(1);
-  if (PASS == 2) issue_paths(0);
+  if (lane == 0) {
+    issue_cost(0);
+    if (nch > 1) issue_cost(1);
+    if (PASS == 2) issue_paths(0);
+  }
+  // this lane's K bytes of a box row under each of the NSW swizzle patterns
+  int lane_off[NSW];
+#pragma unroll
+  for (int v = 0; v < NSW; ++v) lane_off[v] = (K * lane) ^ (v << 4);
   uint32_t phase = 0u;  // bit b: parity awaited on bars[w][b]
   uint32_t L[K];
   const bool col_ok = x >= Q.xlo && x <= Q.xhi;
   for (int c = 0; c < nch; ++c) {
-    const int b = c % NB, n = chunk_n(c);
+    const int b = c % NB;
     const uint32_t pend_cost = (1u << b) | (c + 1 < nch ? 1u << ((c + 1) % NB) : 0u);
     if (!mbar_wait_warp(&bars[w][b], (phase >> b) & 1u)) {
       scan_give_up_mask(bars[w], phase, pend_cost | (PASS == 2 ? 1u << NB : 0u));
-      bulk_wait_all();
+      if (lane == 0) bulk_wait_all();
       return;
     }
     phase ^= 1u << b;
     __syncwarp();
-    plain_chunk<K>(cbuf[w][b], [](int j) { return j * RS; }, n, c == 0, L, P.p1, P.p2);
+    uint8_t* box = cbuf[w][b];
+    // step j: box row C - 1 - j (PASS 1) or j (PASS 2)
+    plain_chunk<K>(
+        [&](int j) {
+          const int r = PASS == 1 ? C - 1 - j : j;
+          return reinterpret_cast<LaneBytes<K>*>(box + r * D + lane_off[box_sw<D>(r)]);
+        },
+        c == 0, L, P.p1, P.p2);
     if constexpr (PASS == 1) {
       fence_proxy_async();
       __syncwarp();
-      if (lane < n) {
-        bulk_to_global(bt + vo + (size_t)row_of(c * C + lane) * rs, cbuf[w][b] + lane * RS, D);
-        bulk_commit();
+      const int y0 = box_y(c);
+      if (y0 >= 0) {
+        if (lane == 0) {
+          tma_store_3d(&m_bt, x * D, y0, view, box);
+          bulk_commit();
+        }
+      } else if (lane < C + y0) {  // the top box: rows 0 .. C + y0 - 1 of the column, one per lane
+        const int r = lane - y0;     // box row of image row `lane`
+        const uint4* src = reinterpret_cast<const uint4*>(box + r * D);
+        uint4* dst = reinterpret_cast<uint4*>(bt + (size_t)view * P.vstride + ((size_t)lane * W + x) * D);
+#pragma unroll
+        for (int u = 0; u < NSW; ++u) dst[u] = src[u ^ box_sw<D>(r)];
       }
-      if (c + 2 < nch) {
-        bulk_wait_read<1>();  // this lane's store of chunk c - 1 has left buffer (c + 2) % 3
+      if (lane == 0 && c + 2 < nch) {
+        bulk_wait_read<1>();  // the store of chunk c - 1 has left the box chunk c + 2 goes to
         issue_cost(c + 2);
       }
     } else {
@@ -749,21 +813,23 @@ __global__ void __launch_bounds__(32 * vscan_plain4_warps<K>())
         return;
       }
       phase ^= 1u << NB;
-      if (lane < n) {
-        const int y = c * C + lane;
+      const int y = C * c + lane;
+      if (y < H) {
         float dv = kInvalidFloat;
         if (col_ok && y >= Q.ylo && y <= Q.yhi && y < Q.rows)
-          dv = plain_wta_rows<D>(cbuf[w][b] + lane * RS, cbuf[w][NB] + lane * RS, cbuf[w][NB + 1] + lane * RS,
-                                 cbuf[w][NB + 2] + lane * RS, P.min_d, y, Q);
+          dv = plain_wta_rows<D>(box + lane * D, cbuf[w][NB] + lane * D, cbuf[w][NB + 1] + lane * D,
+                                 cbuf[w][NB + 2] + lane * D, box_sw<D>(lane), P.min_d, y, Q);
         dout[(size_t)y * W] = dv;
       }
-      fence_proxy_async();  // the reads of both buffers before the copies that refill them
+      fence_proxy_async();  // the reads of the boxes before the copies that refill them
       __syncwarp();
-      if (c + 1 < nch) issue_paths(c + 1);
-      if (c + 2 < nch) issue_cost(c + 2);
+      if (lane == 0) {
+        if (c + 1 < nch) issue_paths(c + 1);
+        if (c + 2 < nch) issue_cost(c + 2);
+      }
     }
   }
-  if (PASS == 1) bulk_wait_all();
+  if (PASS == 1 && lane == 0) bulk_wait_all();
 }
 
 }  // namespace sgm

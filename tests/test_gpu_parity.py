@@ -82,7 +82,7 @@ SCANLINE = {"warp": (2, 0, 1, 0, 0, 0, 0), "scanline_g1": (3, 0, 3, 0, 0, 1, 1),
 
 
 @pytest.mark.parametrize("name", list(CASES))
-@pytest.mark.parametrize("tie", [4, 0, 2])
+@pytest.mark.parametrize("tie", [4, 0, 2, 1])
 @pytest.mark.parametrize("variant", ["default", "warp", "scanline_g1", "scanline_g8", "latency"])
 def test_plain_parity(engine_lib, oracle_mod, name, tie, variant):
     """Every stage against the oracle. 'default' runs the u16x2 scanline kernels where they are
@@ -125,6 +125,7 @@ def test_plain_parity(engine_lib, oracle_mod, name, tie, variant):
         assert_same("disp right", disp_r, ref["disp_r"])
     assert_same("disp left", disp, ref["disp"])
     assert s.kernel_launches() >= 3
+    assert engine_lib.sgm_debug_wait_timeouts() == 0
 
 
 def _init_for(O, L, R, cs, p1, p2):
