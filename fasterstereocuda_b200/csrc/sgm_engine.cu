@@ -864,10 +864,17 @@ template <int PASS>
 int init4_cols(sgm_engine* e, const int16_t* il, const int16_t* ir, float* wta, const sgm::InitParams& P,
                const sgm::WtaParams& Q, cudaStream_t s) {
   e->bt_stored = true;
-  const dim3 grid((unsigned)((e->W + kScan4ColWarps - 1) / kScan4ColWarps), e->nviews());
+  const int nv = e->nviews();
+  const dim3 grid((unsigned)((e->W + kScan4ColWarps - 1) / kScan4ColWarps), nv);
   const char* name = PASS == 1 ? "vpaths_bt_init" : "vpaths_wta_init";
+  const CUtensorMap *mc, *mb, *ml, *mr;
+  int st = volume_map(e, 0, e->cost, nv, &mc);
+  if (!st) st = volume_map(e, 1, e->bt, nv, &mb);
+  if (!st) st = volume_map(e, 2, e->lr, nv, &ml);
+  if (!st) st = volume_map(e, 3, e->rl, nv, &mr);
+  if (st) return st;
   return SGM_LAUNCH(e, s, name, sgm::k_vscan_init4<kScan4ColWarps, PASS><<<grid, 32 * kScan4ColWarps, 0, s>>>(
-                                    e->cost, e->lr, e->rl, il, ir, e->bt, wta, P, Q));
+                                    *mc, *mb, *ml, *mr, il, ir, e->bt, wta, P, Q));
 }
 
 template <typename Word>

@@ -77,6 +77,52 @@ __device__ __forceinline__ void scan_give_up(uint64_t* bars, uint32_t phase, int
   for (int b = 0; b < nbars; ++b) mbar_wait(bars + b, (phase >> b) & 1u);
 }
 
+// `bytes` (a multiple of 16) from shared src to global dst (both 16-byte aligned), in the calling
+// thread's current bulk group.
+__device__ __forceinline__ void bulk_to_global(void* dst, const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_u32(src)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// All but the newest N of this thread's bulk groups have finished reading shared memory.
+template <int N>
+__device__ __forceinline__ void bulk_wait_read() {
+  asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
+// All of this thread's bulk groups are complete.
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+// As scan_give_up, for the buffers whose bit is set in `pending` only.
+__device__ __forceinline__ void scan_give_up_mask(uint64_t* bars, uint32_t phase, uint32_t pending) {
+  if ((threadIdx.x & 31) == 0) atomicAdd(&g_scan_wait_timeouts, 1u);
+  for (int b = 0; b < 32; ++b)
+    if ((pending >> b) & 1u) mbar_wait(bars + b, (phase >> b) & 1u);
+}
+
+// Column chunks are boxes of 32 rows x D bytes of one view's volume, copied by the tensor-memory
+// accelerator (a 3D tensor map: bytes of a row, rows, views) with the 32/64/128-byte swizzle: the
+// 16-byte unit u of box row r lands at unit u ^ box_sw(r) (bits 4.. of the shared address XORed
+// with bits 7..), so that 8 lanes reading 8 consecutive rows hit distinct banks.
+template <int D>
+__host__ __device__ constexpr int box_sw(int r) { return ((r * D) >> 7) & (D / 16 - 1); }
+
+// One box from global memory (tensor coordinates x = byte of the row, y = row, z = view; rows
+// outside the tensor read as 0), completing on bar.
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+// One box to global memory (y >= 0), in the calling thread's current bulk group.
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, int x, int y, int z, const void* src) {
+  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(map),
+               "r"(x), "r"(y), "r"(z), "r"(smem_u32(src))
+               : "memory");
+}
+
 // Per-step parameters of a chunk, one step per lane (lane j = step j): packed as
 // shift (8 bits, clamped to +-64: any |shift| > 33 puts both neighbours out of range) |
 // kStepValid | kPrevInvalid, and P2'.
@@ -137,14 +183,16 @@ __device__ __forceinline__ void scan_step(uint32_t& L, uint32_t c, uint32_t flag
 // +0.5-shifted parabola as in wta_pixel; tie rules: kTieRefB200 the lowest tied d whose candidate
 // is valid (every tied lane stores its own result there, a valid one wins), 1 / 2 the highest tied
 // d, 0 / 3 the lowest (one disparity per lane: lane order is disparity order).
+// a, b, c, e: the pixel's rows in four swizzled boxes (16-byte unit u of the row at u ^ sw).
 __device__ __forceinline__ float init_wta_serial(const uint8_t* a, const uint8_t* b, const uint8_t* c,
-                                                 const uint8_t* e, int base, const WtaParams& Q) {
+                                                 const uint8_t* e, int sw, int base, const WtaParams& Q) {
   constexpr int D = kLevelRange;
   uint32_t S[D];
 #pragma unroll
   for (int k = 0; k < D / 4; ++k) {
-    const uint32_t wa = reinterpret_cast<const uint32_t*>(a)[k], wb = reinterpret_cast<const uint32_t*>(b)[k];
-    const uint32_t wc = reinterpret_cast<const uint32_t*>(c)[k], we = reinterpret_cast<const uint32_t*>(e)[k];
+    const int wk = (((k >> 2) ^ sw) << 2) | (k & 3);  // the word's place in the swizzled row
+    const uint32_t wa = reinterpret_cast<const uint32_t*>(a)[wk], wb = reinterpret_cast<const uint32_t*>(b)[wk];
+    const uint32_t wc = reinterpret_cast<const uint32_t*>(c)[wk], we = reinterpret_cast<const uint32_t*>(e)[wk];
 #pragma unroll
     for (int q = 0; q < 4; ++q)
       S[4 * k + q] = ((wa >> (8 * q)) & 0xFFu) + ((wb >> (8 * q)) & 0xFFu) + ((wc >> (8 * q)) & 0xFFu) +
@@ -155,7 +203,10 @@ __device__ __forceinline__ float init_wta_serial(const uint8_t* a, const uint8_t
   for (int d = 1; d < D; ++d) m = min(m, S[d]);
   const float ut = __fsub_rn(1.0f, Q.uniqueness);
   // S at a runtime d, summed again from the rows (S[] stays in registers, indexed statically)
-  auto sum_at = [&](int d) { return (uint32_t)a[d] + b[d] + c[d] + e[d]; };
+  auto sum_at = [&](int d) {
+    const int o = d ^ (sw << 4);
+    return (uint32_t)a[o] + b[o] + c[o] + e[o];
+  };
   auto candidate = [&](int d) {
     if (d <= 1 || d >= Q.dmax_excl) return kInvalidFloat;
     const float c1 = (float)sum_at(d - 1), c2 = (float)m, c3 = (float)sum_at(d + 1);
@@ -290,25 +341,26 @@ __global__ void __launch_bounds__(32 * WPB) k_hscan_init4(const uint8_t* __restr
 // top, storing its path costs. PASS 2: top to bottom with the 4-path sum and the WTA of an
 // initial-disparity level (as vpaths3_init_lane / k_vpaths_wta_init). Both start last_base from
 // row 0's base (cusgm_ca.cu:1291); the first pixel of a vertical path does not set it.
+// Chunks are swizzled tensor-map boxes of 32 rows x 32 bytes, as in k_vscan_plain4: PASS 1 boxes
+// end at rows H - 32c (the last one starts above row 0 and reads zeros there; its steps past row
+// 0 are marked skipped), PASS 2 boxes start at rows 32c. A step's path costs overwrite its costs
+// in the box; PASS 1 stores the box (the last one row by row), PASS 2 runs the WTA on it.
 // ---------------------------------------------------------------------------------------------
 template <int WPB, int PASS>
-__global__ void __launch_bounds__(32 * WPB) k_vscan_init4(const uint8_t* __restrict__ cost,
-                                                          const uint8_t* __restrict__ lr,
-                                                          const uint8_t* __restrict__ rl,
-                                                          const int16_t* __restrict__ init_l,
-                                                          const int16_t* __restrict__ init_r,
-                                                          uint8_t* __restrict__ bt, float* __restrict__ disp,
-                                                          InitParams P, WtaParams Q) {
-  constexpr int D = kLevelRange, C = kScanChunk;
-  constexpr int NV = PASS == 2 ? 4 : 1;  // staged volumes: cost (+ bottom->top, L->R, R->L)
-  __shared__ __align__(128) uint8_t cbuf[WPB][2][NV][C * D];
-  __shared__ __align__(16) uint8_t obuf[WPB][C * D];
-  __shared__ __align__(8) uint64_t bars[WPB][2];
+__global__ void __launch_bounds__(32 * WPB)
+    k_vscan_init4(const __grid_constant__ CUtensorMap m_cost, const __grid_constant__ CUtensorMap m_bt,
+                  const __grid_constant__ CUtensorMap m_lr, const __grid_constant__ CUtensorMap m_rl,
+                  const int16_t* __restrict__ init_l, const int16_t* __restrict__ init_r, uint8_t* __restrict__ bt,
+                  float* __restrict__ disp, InitParams P, WtaParams Q) {
+  constexpr int D = kLevelRange, C = kScanChunk, BOX = C * D;
+  constexpr int NV = PASS == 2 ? 4 : 1;  // boxes a chunk needs: cost (+ bottom->top, L->R, R->L)
+  constexpr int NB = PASS == 1 ? 3 : 2;  // chunks in flight
+  __shared__ __align__(1024) uint8_t cbuf[WPB][NB][NV][BOX];
+  __shared__ __align__(8) uint64_t bars[WPB][NB];
   __shared__ __align__(16) uint32_t par[WPB][2][C];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   if (lane == 0) {
-    mbar_init(&bars[w][0], 1);
-    mbar_init(&bars[w][1], 1);
+    for (int b = 0; b < NB; ++b) mbar_init(&bars[w][b], 1);
     mbar_fence_init();
   }
   __syncwarp();
@@ -322,36 +374,42 @@ __global__ void __launch_bounds__(32 * WPB) k_vscan_init4(const uint8_t* __restr
       for (int y = lane; y < H; y += 32) dout[(size_t)y * W] = kInvalidFloat;
     return;
   }
-  const size_t vo = (size_t)view * P.vstride + (size_t)x * D;
-  const size_t rs = (size_t)W * D;  // bytes between rows
-  const uint8_t* vol[4] = {cost + vo, bt + vo, lr + vo, rl + vo};
+  // the swizzle pattern is a function of the shared address: the boxes must start on 1 KB
+  if (smem_u32(&cbuf[0][0][0][0]) & 1023u) {
+    if (lane == 0) atomicAdd(&g_scan_wait_timeouts, 1u);
+    return;
+  }
   const int16_t* ib = (view == 0 ? init_l : init_r) + x;
   const int nch = (H + C - 1) / C;
   auto chunk_n = [&](int c) { return min(C, H - c * C); };
   auto row_of = [&](int s) { return PASS == 1 ? H - 1 - s : s; };
-  auto issue = [&](int c, int buf) {
-    const int n = chunk_n(c);
-    if (lane == 0) mbar_expect_tx(&bars[w][buf], (uint32_t)(n * D * NV));
-    __syncwarp();
-    if (lane < n) {
-      const size_t ro = (size_t)row_of(c * C + lane) * rs;
-#pragma unroll
-      for (int v = 0; v < NV; ++v) bulk_to_smem(cbuf[w][buf][v] + lane * D, vol[v] + ro, D, &bars[w][buf]);
+  auto box_y = [&](int c) { return PASS == 1 ? H - C * (c + 1) : C * c; };  // first row of chunk c's box
+  auto issue = [&](int c) {  // lane 0
+    const int b = c % NB;
+    mbar_expect_tx(&bars[w][b], NV * BOX);
+    tma_load_3d(cbuf[w][b][0], &m_cost, x * D, box_y(c), view, &bars[w][b]);
+    if (PASS == 2) {
+      tma_load_3d(cbuf[w][b][1], &m_bt, x * D, box_y(c), view, &bars[w][b]);
+      tma_load_3d(cbuf[w][b][2], &m_lr, x * D, box_y(c), view, &bars[w][b]);
+      tma_load_3d(cbuf[w][b][3], &m_rl, x * D, box_y(c), view, &bars[w][b]);
     }
   };
   auto base_of = [&](int c) {
     const int n = chunk_n(c);
     return lane < n ? (int)ib[(size_t)row_of(c * C + lane) * W] : (int)kInvalidShort;
   };
-  issue(0, 0);
-  if (nch > 1) issue(1, 1);
+  if (lane == 0) {
+    issue(0);
+    if (nch > 1) issue(1);
+  }
   uint32_t phase = 0u;  // bit b: parity of buffer b's next phase
   ChunkState st{(int)ib[0], false};  // row 0's base
   int bnext = base_of(0);
   uint32_t L = 0;
   const bool col_ok = x >= Q.xlo && x <= Q.xhi;
+  const int lo0 = lane, lo1 = lane ^ 16;  // this lane's byte of a box row under the two swizzles
   for (int c = 0; c < nch; ++c) {
-    const int buf = c & 1, n = chunk_n(c);
+    const int b = c % NB, n = chunk_n(c);
     const int bcur = bnext;
     if (c + 1 < nch) bnext = base_of(c + 1);
     uint32_t flags, p2;
@@ -359,12 +417,19 @@ __global__ void __launch_bounds__(32 * WPB) k_vscan_init4(const uint8_t* __restr
     // flags in the low 16 bits, the step's base in the high 16 (the WTA needs it, PASS 2)
     par[w][0][lane] = flags | ((uint32_t)(uint16_t)(int16_t)bcur << 16);
     par[w][1][lane] = p2;
-    if (!mbar_wait_warp(&bars[w][buf], (phase >> buf) & 1u)) {
-      scan_give_up(bars[w], phase, 2);
+    if (!mbar_wait_warp(&bars[w][b], (phase >> b) & 1u)) {
+      scan_give_up_mask(bars[w], phase, (1u << b) | (c + 1 < nch ? 1u << ((c + 1) % NB) : 0u));
+      if (lane == 0) bulk_wait_all();
       return;
     }
-    phase ^= 1u << buf;
+    phase ^= 1u << b;
     __syncwarp();
+    uint8_t* box = cbuf[w][b][0];
+    // step j: box row C - 1 - j (PASS 1) or j (PASS 2); this lane's byte of it
+    auto at = [&](int j) {
+      const int r = PASS == 1 ? C - 1 - j : j;
+      return box + r * D + (box_sw<D>(r) ? lo1 : lo0);
+    };
     // the chunk's step parameters and this lane's costs in registers: the chain below touches no
     // memory but the stores of its results
     uint32_t fl[C], pp[C], cvr[C];
@@ -372,45 +437,58 @@ __global__ void __launch_bounds__(32 * WPB) k_vscan_init4(const uint8_t* __restr
     for (int j = 0; j < C; ++j) {
       fl[j] = par[w][0][j];
       pp[j] = par[w][1][j];
-      cvr[j] = cbuf[w][buf][0][j * D + lane];
+      cvr[j] = *at(j);
     }
-    // all 32 steps run (steps past a short last chunk are marked skipped and store nothing)
+    // all 32 steps run (steps past a short last chunk are marked skipped)
 #pragma unroll
     for (int j = 0; j < C; ++j) {
       if (c == 0 && j == 0) L = cvr[0];
       else scan_step(L, cvr[j], fl[j], pp[j], P.p1);
-      if (j < n) obuf[w][j * D + lane] = (uint8_t)L;
+      *at(j) = (uint8_t)L;
     }
-    __syncwarp();
-    float dv_keep = kInvalidFloat;  // lane j: the disparity of step j (PASS 2)
-    if constexpr (PASS == 2) {
+    if constexpr (PASS == 1) {
+      fence_proxy_async();
+      __syncwarp();
+      const int y0 = box_y(c);
+      if (y0 >= 0) {
+        if (lane == 0) {
+          tma_store_3d(&m_bt, x * D, y0, view, box);
+          bulk_commit();
+        }
+      } else if (lane < C + y0) {  // the top box: rows 0 .. C + y0 - 1 of the column, one per lane
+        const int r = lane - y0;     // box row of image row `lane`
+        const uint4* src = reinterpret_cast<const uint4*>(box + r * D);
+        uint4* dst = reinterpret_cast<uint4*>(bt + (size_t)view * P.vstride + ((size_t)lane * W + x) * D);
+        const int sw = box_sw<D>(r);
+        const uint4 v0 = src[sw], v1 = src[sw ^ 1];
+        dst[0] = v0;
+        dst[1] = v1;
+      }
+      if (lane == 0 && c + 2 < nch) {
+        bulk_wait_read<1>();  // the store of chunk c - 1 has left the box chunk c + 2 goes to
+        issue(c + 2);
+      }
+    } else {
+      __syncwarp();  // the chunk's path costs, written by disparity, are read by pixel
       // the WTA of the chunk's pixels, lane j = pixel j (off the steps' dependency chain)
       const int y = c * C + lane;
       const int base = (int)(int16_t)(par[w][0][lane] >> 16);
       const bool skipped = y > 0 && base == kInvalidShort;
-      if (lane < n && y >= Q.ylo && y <= Q.yhi && y < Q.rows && col_ok && !skipped && base != kInvalidShort)
-        dv_keep = init_wta_serial(obuf[w] + lane * D, cbuf[w][buf][1] + lane * D, cbuf[w][buf][2] + lane * D,
-                                  cbuf[w][buf][3] + lane * D, base, Q);
-    }
-    __syncwarp();
-    if (lane < n) {
-      const size_t ro = (size_t)row_of(c * C + lane) * rs;
-      if constexpr (PASS == 1) {
-        const uint4* src = reinterpret_cast<const uint4*>(obuf[w] + lane * D);
-        uint4* dst = reinterpret_cast<uint4*>(bt + vo + ro);
-        const uint4 v0 = src[0], v1 = src[1];
-        dst[0] = v0;
-        dst[1] = v1;
-      } else {
-        dout[(size_t)(c * C + lane) * W] = dv_keep;
+      if (lane < n) {
+        float dv = kInvalidFloat;
+        if (y >= Q.ylo && y <= Q.yhi && y < Q.rows && col_ok && !skipped && base != kInvalidShort) {
+          const int o = lane * D;
+          dv = init_wta_serial(box + o, cbuf[w][b][1] + o, cbuf[w][b][2] + o, cbuf[w][b][3] + o, box_sw<D>(lane),
+                               base, Q);
+        }
+        dout[(size_t)y * W] = dv;
       }
-    }
-    __syncwarp();
-    if (c + 2 < nch) {
-      fence_proxy_async();
-      issue(c + 2, buf);
+      fence_proxy_async();  // the reads of the boxes before the copies that refill them
+      __syncwarp();
+      if (lane == 0 && c + 2 < nch) issue(c + 2);
     }
   }
+  if (PASS == 1 && lane == 0) bulk_wait_all();
 }
 
 }  // namespace sgm
@@ -432,29 +510,6 @@ namespace sgm {
 // write rows of the buffer that hold nothing of this scanline and are neither stored nor used.
 // The WTA of the top-to-bottom pass runs per chunk with lane = pixel.
 // =============================================================================================
-
-// `bytes` (a multiple of 16) from shared src to global dst (both 16-byte aligned), in the calling
-// thread's current bulk group.
-__device__ __forceinline__ void bulk_to_global(void* dst, const void* src, uint32_t bytes) {
-  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_u32(src)),
-               "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-// All but the newest N of this thread's bulk groups have finished reading shared memory.
-template <int N>
-__device__ __forceinline__ void bulk_wait_read() {
-  asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
-}
-// All of this thread's bulk groups are complete.
-__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
-
-// As scan_give_up, for the buffers whose bit is set in `pending` only.
-__device__ __forceinline__ void scan_give_up_mask(uint64_t* bars, uint32_t phase, uint32_t pending) {
-  if ((threadIdx.x & 31) == 0) atomicAdd(&g_scan_wait_timeouts, 1u);
-  for (int b = 0; b < 32; ++b)
-    if ((pending >> b) & 1u) mbar_wait(bars + b, (phase >> b) & 1u);
-}
 
 // A lane's K bytes of a step row, as one shared-memory word.
 template <int K>
@@ -675,29 +730,6 @@ __device__ __forceinline__ float plain_wta_rows(const uint8_t* a, const uint8_t*
   const float uq = d12 < d32 ? d12 : d32;
   if (uq <= __fmul_rn(c2, __fsub_rn(1.0f, Q.uniqueness))) return kInvalidFloat;
   return __fadd_rn((float)(ds + min_d), subpix_bias(c1, c2, c3));
-}
-
-// Column chunks are boxes of 32 rows x D bytes of one view's volume, copied by the tensor-memory
-// accelerator (a 3D tensor map: bytes of a row, rows, views) with the 32/64/128-byte swizzle: the
-// 16-byte unit u of box row r lands at unit u ^ box_sw(r) (bits 4.. of the shared address XORed
-// with bits 7..), so that 8 lanes reading 8 consecutive rows hit distinct banks.
-template <int D>
-__host__ __device__ constexpr int box_sw(int r) { return ((r * D) >> 7) & (D / 16 - 1); }
-
-// One box from global memory (tensor coordinates x = byte of the row, y = row, z = view; rows
-// outside the tensor read as 0), completing on bar.
-__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
-      "[%5];" ::"r"(smem_u32(dst)),
-      "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
-      : "memory");
-}
-// One box to global memory (y >= 0), in the calling thread's current bulk group.
-__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, int x, int y, int z, const void* src) {
-  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(map),
-               "r"(x), "r"(y), "r"(z), "r"(smem_u32(src))
-               : "memory");
 }
 
 // Warps per CTA of the column kernels (shared memory per warp: PASS 1 three boxes, PASS 2 two
