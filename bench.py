@@ -165,10 +165,15 @@ def alg_bytes(kernel, W, H, D, nviews, census_bytes):
 
 
 # DRAM bytes per voxel (W*H*D*views of the launch) measured by ncu (dram__bytes_read.sum +
-# dram__bytes_write.sum) for the default kernels at 1242x375x64, one pair per launch: the plain
-# kernels on the single-level workload, the 32-disparity kernels on the pyramid's finest level.
-NCU_DRAM_BYTES_PER_VOXEL = {"hpaths_plain": 2.82, "vpaths_wta_plain": 5.35, "hpaths_init": 1.07,
-                            "vpaths_wta_init": 3.29}
+# dram__bytes_write.sum) at 1242x375x64, one pair per launch: the plain kernels on the
+# single-level workload, the 32-disparity kernels on the pyramid's finest level; per kernel
+# family: "v3" the thread-per-scanline kernels, "v4" the warp-per-scanline kernels.
+NCU_DRAM_BYTES_PER_VOXEL = {
+    "v3": {"hpaths_plain": 2.83, "vpaths_bt_plain": 1.25, "vpaths_wta_plain": 4.04, "hpaths_init": 1.07,
+           "vpaths_wta_init": 3.29},
+    "v4": {"hpaths_plain": 2.73, "vpaths_bt_plain": 1.22, "vpaths_wta_plain": 4.05, "hpaths_init": 1.06,
+           "vpaths_bt_init": 1.06, "vpaths_wta_init": 4.08},
+}
 
 
 # ------------------------------------------------------------------------------------ reference arm
@@ -266,7 +271,7 @@ def metric_name(workload):
 
 
 def workload_config(a, batch):
-    c = {"workload": f"{W_}x{H_} D={DMAX} " + ("3-level pyramid (configs[1] scene)" if a.workload == "pyramid"
+    c = {"workload": f"{W_}x{H_} D={DMAX} " + ("3-level pyramid, slanted ground plane + 12 boxes scene" if a.workload == "pyramid"
                                                  else "single-level plain SGM"),
          "width": W_, "height": H_, "disparities": DMAX, "census": "9x7", "p1": 10, "p2": 150,
          "batch_pairs": batch}
@@ -384,10 +389,12 @@ def run_ours(a, rank, world, local_rank):
                 step()
             torch.cuda.synchronize()
             return max_over_ranks(time.perf_counter() - t0c)
-        best = min(((timed((0, 0, 0, 0, 0) + lanes), lanes) for lanes in ((8, 8), (8, 4), (4, 4), (4, 2), (2, 2))),
-                   key=lambda r: r[0])
-        chosen = (0, 0, 0, 0, 0) + best[1]
-        tuning = "autotuned row_lanes,col_lanes = %d,%d" % best[1]
+        # the thread-per-scanline kernels with each lane split, and the warp-per-scanline kernels
+        cands = [(0, 0, 0, 0, 0) + lanes for lanes in ((8, 8), (8, 4), (4, 4), (4, 2), (2, 2))]
+        cands.append((4, 0, 4, 0, 0, 0, 0))
+        best = min(((timed(t), t) for t in cands), key=lambda r: r[0])
+        chosen = best[1]
+        tuning = "autotuned " + ",".join(str(v) for v in chosen)
         if a.workload == "pyramid":  # then the 32-disparity levels on their own
             best_i = min(((timed(chosen, t), t) for t in ((0, 0, 0, 0, 0, 8, 8), (0, 0, 0, 0, 0, 4, 4),
                                                             (0, 0, 0, 0, 0, 2, 2), (4, 0, 4, 0, 0, 0, 0))),
@@ -509,19 +516,26 @@ def run_ours(a, rank, world, local_rank):
                 if not k.startswith(("hpaths", "vpaths")) or k.endswith(kind)]
         per_call_bytes[k] = sum(alg_bytes(k, w, h, d, nv, 8) for (w, h, d, nv) in mine)
         per_call_voxels[k] = sum(w * h * d * nv for (w, h, d, nv) in mine)
-    dom = max(prof, key=lambda k: prof[k]["ms"]) if prof else None
+    # the dominant kernel among those with a counterpart in the minimal design (the bottom-to-top
+    # pass launched on its own has none)
+    cand = [k for k in prof if per_call_bytes.get(k, 0) > 0]
+    dom = max(cand, key=lambda k: prof[k]["ms"]) if cand else None
     calls = a.profile_pairs
+    # kernel family of the latency matcher's row / column scans
+    lat_t = [int(v) for v in lat_tuning.split()[-1].split(",")] if lat_tuning else [0, 0, 0]
+    fam = lambda k: "v4" if (lat_t[0] if k.startswith("hpaths") else lat_t[2]) == 4 else "v3"  # noqa: E731
     roofline = None
     if dom:
         total_ms = prof[dom]["ms"]
         byts = per_call_bytes.get(dom, 0) * calls
         ach = byts / (total_ms / 1e3) / 1e9 if total_ms > 0 else 0.0
         per_launch = max(1, prof[dom]["launches"] // calls)
-        bpv = NCU_DRAM_BYTES_PER_VOXEL.get(dom)
+        bpv = NCU_DRAM_BYTES_PER_VOXEL[fam(dom)].get(dom)
         traffic = bpv * per_call_voxels.get(dom, 0) / per_launch if bpv else None
         roofline = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
                     "frac": ach / hbm_peak, "traffic": traffic, "peak_kind": peak_kind,
                     "traffic_source": "ncu DRAM bytes per voxel of this kernel x voxels per launch",
+                    "kernel_family": fam(dom),
                     "avg_launch_us": total_ms / prof[dom]["launches"] * 1e3,
                     "alg_bytes_per_launch": per_call_bytes.get(dom, 0) / max(1, prof[dom]["launches"] // calls),
                     "timing": f"CUDA events around each launch, serialised pass of {calls} pairs on one stream "
