@@ -894,9 +894,12 @@ int launch_init(sgm_engine* e, const Word* csl, const Word* csr, const int16_t* 
   Q3.image_border(e->W, e->H);
   // thread-per-scanline kernels: uint32 arithmetic (exact for any penalties); WTA rules 0 and 4
   const bool v3_ok = e->ext.init_tie_rule == sgm::kTieLowest || e->ext.init_tie_rule == sgm::kTieRefB200;
-  const bool rows3 = v3_ok && (e->tune_row_kernel == 0 || e->tune_row_kernel == 3);
+  // the warp-per-scanline row kernel packs P2' into 22 bits; larger penalties take the default
+  const bool pack_ok = e->opt.p1 >= 0 && e->opt.p1 < (1 << 22) && e->opt.p2_init < (1 << 22) && e->ext.p2_div0 < (1 << 22);
+  const int tune_row = e->tune_row_kernel == 4 && !pack_ok ? 0 : e->tune_row_kernel;
+  const bool rows3 = v3_ok && (tune_row == 0 || tune_row == 3);
   const bool cols3 = v3_ok && (e->tune_col_kernel == 0 || e->tune_col_kernel == 3);
-  const bool rows4 = e->tune_row_kernel == 4, cols4 = e->tune_col_kernel == 4;
+  const bool rows4 = tune_row == 4, cols4 = e->tune_col_kernel == 4;
   // rows reading the cost volume (variants 3 and 4) and columns split into two passes
   auto rows_cv = [&](cudaStream_t ms) { return rows4 ? init4_rows(e, il, ir, P, ms) : init3_rows(e, il, ir, P, ms); };
   auto cols_bt = [&](cudaStream_t ss) {
@@ -912,7 +915,7 @@ int launch_init(sgm_engine* e, const Word* csl, const Word* csr, const int16_t* 
   if (rows3 || rows4) {
     st = init3_cost<Word>(e, csl, csr, il, ir, P, e->stream);
     if (!st) st = rows_cv(e->stream);
-  } else if (e->tune_row_kernel == 1) {  // whole census rows of R scanlines in shared memory
+  } else if (tune_row == 1) {  // whole census rows of R scanlines in shared memory
     const int R = e->tune_rows > 0 ? e->tune_rows : rows_per_cta(e->W, sizeof(Word), true);
     const size_t smem = (size_t)R * e->W * (2 * sizeof(Word) + 2);
     if (smem > 227 * 1024) {

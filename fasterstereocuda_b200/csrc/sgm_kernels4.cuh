@@ -177,6 +177,21 @@ __device__ __forceinline__ void scan_step(uint32_t& L, uint32_t c, uint32_t flag
   if (flags & kStepValid) L = Ln;
 }
 
+// scan_step for a step that is valid and follows a valid one (no INVALID base at either): the
+// same result with P1 added before the shuffles and the m + P2' bound taken off their path.
+__device__ __forceinline__ void scan_step_fast(uint32_t& L, uint32_t c, int s, uint32_t p2, uint32_t p1) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t m = __reduce_min_sync(kFull, L);
+  const uint32_t Lp = L + p1;
+  const int i1 = lane + s - 1, i2 = lane + s + 1;
+  const uint32_t a = __shfl_sync(kFull, Lp, i1 & 31);
+  const uint32_t b = __shfl_sync(kFull, Lp, i2 & 31);
+  const uint32_t A = (unsigned)i1 < 32u ? a : kInvalidCost;
+  const uint32_t B = (unsigned)i2 < 32u ? b : kInvalidCost;
+  const uint32_t t = __vimin3_u32(min(L, m + p2), A, B);
+  L = c + t - m;
+}
+
 // WTA of one pixel of an initial-disparity level from its four stored path rows (32 bytes each;
 // S(d) = sum of the four), computed by one lane: Kernel_ComputeDisparityByWTA for initial
 // disparities (cusgm_ca.cu:3425-3512). d* <= 1 or d* >= 31 -> INVALID; uniqueness and the
@@ -232,7 +247,16 @@ __device__ __forceinline__ float init_wta_serial(const uint8_t* a, const uint8_t
 }
 
 // ---------------------------------------------------------------------------------------------
-// Horizontal scans: warp w of the grid owns scanline i = (view, dir, y) as in hpaths3_lane.
+// Horizontal scans: warp w of the grid owns scanline i = (view, dir, y) as in hpaths3_lane. A
+// chunk is 32 consecutive pixels of the row, one contiguous bulk copy (double-buffered); its
+// costs go to registers at once, which frees the buffer for the chunk after next. Right-to-left
+// scans place a short (last) chunk at the end of the buffer, so that step j of every chunk reads
+// row 31 - j; every chunk runs all 32 steps (the steps past a short chunk are marked skipped and
+// keep the state). Each step stores its 32 path costs straight to global memory (one 32-byte
+// segment per warp). The step parameters of the next chunk are computed
+// beside the steps of this one (they do not depend on the path costs), and a chunk whose steps
+// all have valid bases (the usual case) runs scan_step_fast. Step parameters: kStepValid,
+// kPrevInvalid and the shift in bits 0-9, P2' above them (P1, P2 < 2^22).
 // ---------------------------------------------------------------------------------------------
 template <int WPB>
 __global__ void __launch_bounds__(32 * WPB) k_hscan_init4(const uint8_t* __restrict__ cost,
@@ -240,15 +264,13 @@ __global__ void __launch_bounds__(32 * WPB) k_hscan_init4(const uint8_t* __restr
                                                           const int16_t* __restrict__ init_r,
                                                           uint8_t* __restrict__ lr, uint8_t* __restrict__ rl,
                                                           InitParams P, int nviews) {
-  constexpr int D = kLevelRange, C = kScanChunk;
-  __shared__ __align__(128) uint8_t cbuf[WPB][2][C * D];
-  __shared__ __align__(16) uint8_t obuf[WPB][C * D];
-  __shared__ __align__(8) uint64_t bars[WPB][2];
-  __shared__ __align__(16) uint32_t par[WPB][2][C];
+  constexpr int D = kLevelRange, C = kScanChunk, NB = 2;
+  __shared__ __align__(128) uint8_t cbuf[WPB][NB][C * D];
+  __shared__ __align__(8) uint64_t bars[WPB][NB];
+  __shared__ uint32_t par[WPB][C];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   if (lane == 0) {
-    mbar_init(&bars[w][0], 1);
-    mbar_init(&bars[w][1], 1);
+    for (int b = 0; b < NB; ++b) mbar_init(&bars[w][b], 1);
     mbar_fence_init();
   }
   __syncwarp();
@@ -264,15 +286,15 @@ __global__ void __launch_bounds__(32 * WPB) k_hscan_init4(const uint8_t* __restr
   uint8_t* orow = (dir == 0 ? lr : rl) + ro;
   const int16_t* ib = (view == 0 ? init_l : init_r) + (size_t)y * W;
   const int nch = (len + C - 1) / C;
-  // chunk c: steps [c*C, c*C + n), pixels [xa, xa + n) in memory order
+  // chunk c: steps [c*C, c*C + n), pixels [chunk_x, chunk_x + n) in memory order (n <= 0: none)
   auto chunk_n = [&](int c) { return min(C, len - c * C); };
   auto chunk_x = [&](int c) { return dir == 0 ? P.x0 + c * C : W - (c * C + chunk_n(c)); };
-  auto issue = [&](int c, int buf) {
-    if (lane == 0) {
-      const uint32_t bytes = (uint32_t)chunk_n(c) * D;
-      mbar_expect_tx(&bars[w][buf], bytes);
-      bulk_to_smem(cbuf[w][buf], crow + (size_t)chunk_x(c) * D, bytes, &bars[w][buf]);
-    }
+  auto chunk_off = [&](int c) { return dir == 0 ? 0 : (C - chunk_n(c)) * D; };  // bytes into the buffer
+  auto issue = [&](int c) {  // lane 0
+    const int b = c % NB;
+    const uint32_t bytes = (uint32_t)chunk_n(c) * D;
+    mbar_expect_tx(&bars[w][b], bytes);
+    bulk_to_smem(cbuf[w][b] + chunk_off(c), crow + (size_t)chunk_x(c) * D, bytes, &bars[w][b]);
   };
   auto base_of = [&](int c) {  // this lane's step of chunk c
     const int n = chunk_n(c);
@@ -280,58 +302,70 @@ __global__ void __launch_bounds__(32 * WPB) k_hscan_init4(const uint8_t* __restr
     const int x = dir == 0 ? P.x0 + c * C + lane : W - 1 - (c * C + lane);
     return (int)ib[x];
   };
-  issue(0, 0);
-  if (nch > 1) issue(1, 1);
-  uint32_t phase = 0u;  // bit b: parity of buffer b's next phase
   ChunkState st{0, false};
-  int bnext = base_of(0);
+  // packed step parameters of chunk c (lane j: step j) and whether it takes the fast path
+  auto params = [&](int c, int bse, uint32_t& pk, bool& fast) {
+    uint32_t flags, p2;
+    chunk_params(bse, c * C, chunk_n(c), true, P, st, flags, p2);
+    pk = (p2 << 10) | flags;
+    fast = __all_sync(kFull, (flags & (kStepValid | kPrevInvalid)) == kStepValid || (c == 0 && lane == 0));
+  };
+  if (lane == 0) {
+    issue(0);
+    if (nch > 1) issue(1);
+  }
+  uint32_t pk;
+  bool fast;
+  params(0, base_of(0), pk, fast);
+  int bnext = base_of(1);
+  uint32_t phase = 0u;  // bit b: parity of buffer b's next phase
   uint32_t L = 0;
   for (int c = 0; c < nch; ++c) {
-    const int buf = c & 1, n = chunk_n(c);
-    const int bcur = bnext;
-    if (c + 1 < nch) bnext = base_of(c + 1);  // a chunk ahead
-    uint32_t flags, p2;
-    chunk_params(bcur, c * C, n, true, P, st, flags, p2);
-    par[w][0][lane] = flags;
-    par[w][1][lane] = p2;
-    if (!mbar_wait_warp(&bars[w][buf], (phase >> buf) & 1u)) {
-      scan_give_up(bars[w], phase, 2);
+    const int b = c % NB, n = chunk_n(c);
+    if (!mbar_wait_warp(&bars[w][b], (phase >> b) & 1u)) {
+      scan_give_up_mask(bars[w], phase, (1u << b) | (c + 1 < nch ? 1u << ((c + 1) % NB) : 0u));
       return;
     }
-    phase ^= 1u << buf;
+    phase ^= 1u << b;
     __syncwarp();
-    const uint8_t* cb = cbuf[w][buf];
-    uint8_t* ob = obuf[w];
-    // the chunk's step parameters and this lane's costs in registers: the chain below then
-    // touches no memory but the stores of its results
-    uint32_t fl[C], pp[C], cvr[C];
+    const uint8_t* cb = cbuf[w][b] + lane;
+    const int r0 = dir == 0 ? 0 : (C - 1) * D, dr = dir == 0 ? D : -D;  // row of step j: r0 + j * dr
+    uint32_t cvr[C];
 #pragma unroll
-    for (int j = 0; j < C; ++j) {
-      fl[j] = par[w][0][j];
-      pp[j] = par[w][1][j];
-      cvr[j] = cb[(j < n ? (dir == 0 ? j : n - 1 - j) : 0) * D + lane];
-    }
-    // all 32 steps run: past the end of a short last chunk the steps are marked skipped (their
-    // flags have no kStepValid), so the state is kept and nothing is stored
+    for (int j = 0; j < C; ++j) cvr[j] = cb[r0 + j * dr];
+    fence_proxy_async();  // this lane's reads of the buffer before the copy that refills it
+    __syncwarp();
+    if (lane == 0 && c + 2 < nch) issue(c + 2);
+    uint8_t* op = orow + (size_t)chunk_x(c) * D + lane + (dir == 0 ? 0 : (n - 1) * D);  // step 0's byte
+    const int od = dir == 0 ? D : -D;
+    const int bn = bnext;
+    bnext = base_of(c + 2);  // a chunk ahead (no load past the scanline)
+    // this chunk's step parameters to every lane
+    par[w][lane] = pk;
+    __syncwarp();
+    uint32_t q[C];
 #pragma unroll
-    for (int j = 0; j < C; ++j) {
-      if (c == 0 && j == 0) L = cvr[0];  // first pixel of the scanline
-      else scan_step(L, cvr[j], fl[j], pp[j], P.p1);
-      if (j < n) ob[(dir == 0 ? j : n - 1 - j) * D + lane] = (uint8_t)L;
-    }
+    for (int j = 0; j < C; ++j) q[j] = par[w][j];
     __syncwarp();
-    // the chunk's path costs: lane j writes pixel xa + j (32 bytes)
-    if (lane < n) {
-      const uint4* src = reinterpret_cast<const uint4*>(ob + lane * D);
-      uint4* dst = reinterpret_cast<uint4*>(orow + (size_t)(chunk_x(c) + lane) * D);
-      const uint4 v0 = src[0], v1 = src[1];
-      dst[0] = v0;
-      dst[1] = v1;
-    }
-    __syncwarp();
-    if (c + 2 < nch) {
-      fence_proxy_async();
-      issue(c + 2, buf);
+    if (fast) {  // a full chunk (a short one has skipped steps)
+      params(c + 1, bn, pk, fast);
+#pragma unroll
+      for (int j = 0; j < C; ++j) {
+        uint32_t Ls = L;
+        scan_step_fast(Ls, cvr[j], (int)(int8_t)(q[j] & 0xFFu), q[j] >> 10, P.p1);
+        L = (j == 0 && c == 0) ? cvr[0] : Ls;  // the first pixel of the scanline starts it
+        op[j * od] = (uint8_t)L;
+      }
+    } else {
+      params(c + 1, bn, pk, fast);
+#pragma unroll
+      for (int j = 0; j < C; ++j) {
+        uint32_t Ls = L;
+        scan_step(Ls, cvr[j], q[j] & 0x3FFu, q[j] >> 10, P.p1);
+        L = (j == 0 && c == 0) ? cvr[0] : Ls;
+        // a skipped step past a short chunk keeps L: it rewrites the chunk's last pixel
+        op[min(j, n - 1) * od] = (uint8_t)L;
+      }
     }
   }
 }
