@@ -171,7 +171,7 @@ def alg_bytes(kernel, W, H, D, nviews, census_bytes):
 NCU_DRAM_BYTES_PER_VOXEL = {
     "v3": {"hpaths_plain": 2.83, "vpaths_bt_plain": 1.25, "vpaths_wta_plain": 4.04, "hpaths_init": 1.07,
            "vpaths_wta_init": 3.29},
-    "v4": {"hpaths_plain": 2.73, "vpaths_bt_plain": 1.22, "vpaths_wta_plain": 4.05, "hpaths_init": 1.06,
+    "v4": {"hpaths_plain": 2.76, "vpaths_bt_plain": 1.22, "vpaths_wta_plain": 4.05, "hpaths_init": 1.06,
            "vpaths_bt_init": 1.06, "vpaths_wta_init": 4.08},
 }
 
