@@ -8,10 +8,15 @@
 //   S(p,d) = ((L_0 + L_1) + L_2) + L_3;  disp(p) = sum_d d * softmax_d(-S(p,d)/T)
 // Ties of the hard minima are broken in the fixed order same d, d-1, d+1, jump (lowest k for m_q).
 //
-// Mapping: a scanline is held by G lanes of a warp, K = D/G disparities per lane, so a warp scans
-// 32/G lines at once and the per-pixel minimum is a log2(G)-level butterfly. The forward scans use
-// K = 4 (the shortest instruction stream per step: the row scans are a chain of W dependent
-// steps), the backward scans K = 8 (their segment buffers fit more lines per SM).
+// Mapping, forward: one warp per scanline, lane l holding the K = D/32 consecutive disparities
+// K l .. K l + K - 1; the per-pixel minimum is one REDUX on order-preserving 32-bit keys of the
+// floats (exactly the minimum), the d +- 1 terms stay in the lane except at its edges (one shuffle
+// up, one down). Inputs move in chunks of kFC steps: a row chunk is one contiguous bulk copy, a
+// column chunk one box of a 3D tensor map (TMA), double-buffered on mbarriers with bounded waits;
+// the penalties of a chunk's steps are loaded one chunk ahead, one step per lane. A row scan is a
+// chain of W dependent steps, so everything that does not depend on the path costs is kept off it.
+// Backward: a scanline is held by G lanes of a warp, K = D/G disparities per lane (8 lanes, K = 8
+// at D = 64: the segment buffers fit more lines per SM), minima and sums by butterflies.
 // All four directions run in ONE launch (their blocks side by side, the long row scans first),
 // each writing its own path volume; the soft-argmin kernel adds the four in path order. The
 // backward launch likewise runs the four adjoint scans at once, each writing its own gradient
@@ -34,6 +39,8 @@
 #include <type_traits>
 
 #include "../../include/sgm_b200.h"
+#include "sgm_async.cuh"
+#include "sgm_tma.h"
 
 void sgm_set_process_error(const char* msg);
 
@@ -42,14 +49,12 @@ namespace {
 constexpr unsigned kFullMask = 0xFFFFFFFFu;
 constexpr int kK = 8;       // disparities per lane of the soft-argmin kernels
 constexpr int kSeg = 8;     // pixels per recomputed segment (checkpoint interval)
-constexpr int kPrefetchPx = 16;  // pixels per L2 prefetch request of the forward row scans
 constexpr int kBwdPF = 2;   // depth of the backward register rings (two interleaved scans per step)
-constexpr int kPF = 4;      // depth of the register ring of per-pixel inputs
 constexpr int kWarps = 4;   // warps per block of the scan kernels
-// lanes per scanline of the forward and backward scans at D = 64 and D = 32 (any choice gives the
-// same path states: the per-disparity arithmetic and the exact minimum do not depend on it)
-constexpr int kFwdLanes64 = 16, kBwdLanes64 = 8;
-constexpr int kFwdLanes32 = 8, kBwdLanes32 = 4;
+constexpr int kFC = 16;     // steps per staged chunk of the forward scans (a multiple of kSeg)
+// lanes per scanline of the backward scans at D = 64 and D = 32 (any choice gives the same path
+// states: the per-disparity arithmetic and the exact minimum do not depend on it)
+constexpr int kBwdLanes64 = 8, kBwdLanes32 = 4;
 #define kInf __int_as_float(0x7f800000)
 
 struct Geo {
@@ -77,28 +82,6 @@ __device__ __forceinline__ void line_origin(const Geo& g, int line, long long& b
     const int b = line / g.W, x = line - b * g.W;
     base = ((long long)b * g.H + (g.dir == 2 ? g.H - 1 : 0)) * g.W + x;
     step = g.dir == 2 ? -(long long)g.W : (long long)g.W;
-  }
-}
-
-// Bulk prefetch of `bytes` (a multiple of 16, 16-byte aligned, inside one allocation) into L2.
-__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
-
-// The D-deep slices of scan steps [a, a + kPrefetchPx) of a line into L2: one request for a row scan
-// (contiguous pixels), one per pixel for a column scan, spread over the line's G lanes.
-template <int G, int D>
-__device__ __forceinline__ void prefetch_segment(const float* vol, const Geo& g, long long base, long long step,
-                                                 int a, int gl) {
-  const int n = min(kPrefetchPx, g.len - a);
-  if (n <= 0) return;
-  if (step == 1 || step == -1) {
-    if (gl == 0) {
-      const long long lo = step > 0 ? base + a : base - a - (n - 1);
-      prefetch_l2(vol + lo * D, (uint32_t)(n * D * sizeof(float)));
-    }
-  } else {
-    for (int i = gl; i < n; i += G) prefetch_l2(vol + (base + (long long)(a + i) * step) * D, D * sizeof(float));
   }
 }
 
@@ -205,60 +188,165 @@ struct FwdArgs {
   const float* p2;
   float* out[4];   // path volumes, one per direction
   float* ckpt[4];  // segment entry states, one slab per direction
-  Grid4 q;
+  Grid4 q;         // one line per warp
 };
 
-template <int G, int K>
-__global__ void __launch_bounds__(kWarps * 32, 3) k_float_fwd(const FwdArgs a) {
-  constexpr int D = G * K;
+// Order-preserving 32-bit key of a (non-NaN) float and back: the unsigned order of the keys is the
+// order of the values, so a REDUX minimum of keys is exactly the minimum.
+__device__ __forceinline__ uint32_t fkey(float f) {
+  const uint32_t b = __float_as_uint(f);
+  return b ^ ((uint32_t)((int32_t)b >> 31) | 0x80000000u);
+}
+__device__ __forceinline__ float funkey(uint32_t k) {
+  return __uint_as_float(k ^ ((uint32_t)((int32_t)~k >> 31) | 0x80000000u));
+}
+__device__ __forceinline__ float warp_min(float v) { return funkey(__reduce_min_sync(kFullMask, fkey(v))); }
+
+// One forward step of a warp-held scanline (lane l: d = K l + j), the arithmetic of fstep.
+template <int K>
+__device__ __forceinline__ void fstep_warp(float (&L)[K], const float (&c)[K], float& m, float p1, float p2) {
+  const int lane = threadIdx.x & 31;
+  const float left = __shfl_up_sync(kFullMask, L[K - 1], 1);
+  const float right = __shfl_down_sync(kFullMask, L[0], 1);
+  const float jump = m + p2;
+  float n[K];
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    const float lm = j > 0 ? L[j - 1] : (lane > 0 ? left : kInf);
+    const float lp = j < K - 1 ? L[j + 1] : (lane < 31 ? right : kInf);
+    const float t = fminf(fminf(L[j], lm + p1), fminf(lp + p1, jump));
+    n[j] = c[j] + t - m;
+  }
+#pragma unroll
+  for (int j = 0; j < K; ++j) L[j] = n[j];
+  m = warp_min(minK<K>(L));
+}
+
+template <int K>
+__device__ __forceinline__ void ld_lane(const float* p, float (&v)[K]) {
+  if constexpr (K == 2) {
+    const float2 x = *reinterpret_cast<const float2*>(p);
+    v[0] = x.x;
+    v[1] = x.y;
+  } else {
+#pragma unroll
+    for (int j = 0; j < K; ++j) v[j] = p[j];
+  }
+}
+template <int K>
+__device__ __forceinline__ void st_lane(float* p, const float (&v)[K]) {
+  if constexpr (K == 2) {
+    *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
+  } else {
+#pragma unroll
+    for (int j = 0; j < K; ++j) p[j] = v[j];
+  }
+}
+
+// Shared memory of the forward kernel: per warp two chunk buffers of kFC x D floats.
+template <int K>
+constexpr size_t fwd_smem_bytes() {
+  return (size_t)kWarps * 2 * kFC * 32 * K * sizeof(float);
+}
+
+// tm_cost: the cost volume as a 3D tensor map (floats of a row, rows, images), boxes of D x kFC x 1.
+template <int K>
+__global__ void __launch_bounds__(kWarps * 32) k_float_fwd(const __grid_constant__ CUtensorMap tm_cost,
+                                                           const FwdArgs a) {
+  constexpr int D = 32 * K, C = kFC, NB = 2;
+  extern __shared__ __align__(128) float fsm[];
+  __shared__ __align__(8) uint64_t bars[kWarps][NB];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) {
+    for (int b = 0; b < NB; ++b) sgm::mbar_init(&bars[w][b], 1);
+    sgm::mbar_fence_init();
+  }
+  __syncwarp();
   Line ln;
   Geo g;
-  if (!locate<G>(a.q, ln, g)) return;
-  const int gl = threadIdx.x % G;
+  if (!locate<32>(a.q, ln, g)) return;  // the whole warp
   long long base, step;
   line_origin(g, ln.line, base, step);
-  float* out = a.out[ln.dir];
-  float* ck = a.ckpt[ln.dir] + (size_t)ln.line * g.nseg * D + gl * K;
-  float rc[kPF][K], rp1[kPF], rp2[kPF];
-  auto fetch = [&](int j, int s) {
-    const long long p = base + s * step;
-    loadK<K>(a.cost + p * D + gl * K, rc[j]);
-    rp1[j] = __ldg(a.p1 + p);
-    rp2[j] = __ldg(a.p2 + p);
-  };
-  prefetch_segment<G, D>(a.cost, g, base, step, 0, gl);
-#pragma unroll
-  for (int j = 0; j < kPF; ++j)
-    if (j < g.len) fetch(j, j);
-  // states of even / odd scan positions: a step computes into the array the previous step's
-  // store is not reading (kPF is even, so the parity of j is the parity of s)
-  float LA[K], LB[K];
-  float m = 0.f;
-  for (int s0 = 0; s0 < g.len; s0 += kPF) {
-#pragma unroll
-    for (int j = 0; j < kPF; ++j) {
-      const int s = s0 + j;
-      float(&L)[K] = (j & 1) ? LB : LA;
-      float(&Lq)[K] = (j & 1) ? LA : LB;
-      if (s < g.len) {
-        if (s % kPrefetchPx == 0) prefetch_segment<G, D>(a.cost, g, base, step, s + kPrefetchPx, gl);
-        if (s % kSeg == 0 && s > 0 && ln.live)
-          storeK<K>(ck + (size_t)(s / kSeg) * D, Lq);  // state entering this segment
-        float c[K];
-#pragma unroll
-        for (int i = 0; i < K; ++i) c[i] = rc[j][i];
-        const float P1 = rp1[j], P2 = rp2[j];
-        if (s + kPF < g.len) fetch(j, s + kPF);
-        if (s == 0) {
-#pragma unroll
-          for (int i = 0; i < K; ++i) L[i] = c[i];
-          m = group_min<G>(minK<K>(L));
-        } else {
-          m = fstep<G, K>(Lq, L, c, m, P1, P2, gl);
-        }
-        if (ln.live) storeK<K>(out + (base + s * step) * D + gl * K, L);
-      }
+  const bool horiz = g.dir == 1 || g.dir == 3;
+  const bool rev = g.dir == 2 || g.dir == 3;  // step j of a chunk at buffer row C - 1 - j
+  float* box0 = fsm + (size_t)w * NB * C * D;
+  const int len = g.len, nch = (len + C - 1) / C;
+  auto chunk_n = [&](int c) { return min(C, len - c * C); };
+  auto issue = [&](int c) {  // lane 0
+    const int b = c % NB, n = chunk_n(c);
+    float* dst = box0 + b * C * D;
+    if (horiz) {  // pixels base + (cC + j) step, contiguous; right-to-left: a short chunk at the buffer's end
+      const long long lo = step > 0 ? base + (long long)c * C : base - ((long long)c * C + n - 1);
+      const uint32_t bytes = (uint32_t)(n * D * sizeof(float));
+      sgm::mbar_expect_tx(&bars[w][b], bytes);
+      sgm::bulk_to_smem(dst + (step > 0 ? 0 : (C - n) * D), a.cost + lo * D, bytes, &bars[w][b]);
+    } else {  // column x of image bi: top-to-bottom boxes start at row cC, bottom-to-top ones end at H - cC
+      const int bi = ln.line / g.W, x = ln.line - bi * g.W;
+      const int y0 = g.dir == 0 ? c * C : g.H - C * (c + 1);
+      sgm::mbar_expect_tx(&bars[w][b], (uint32_t)(C * D * sizeof(float)));
+      sgm::tma_load_3d(dst, &tm_cost, x * D, y0, bi, &bars[w][b]);
     }
+  };
+  // the penalties of step `lane` of chunk c
+  auto pen = [&](int c, float& q1, float& q2) {
+    q1 = q2 = 0.f;
+    if (lane < chunk_n(c)) {
+      const long long p = base + ((long long)c * C + lane) * step;
+      q1 = __ldg(a.p1 + p);
+      q2 = __ldg(a.p2 + p);
+    }
+  };
+  if (lane == 0) {
+    issue(0);
+    if (nch > 1) issue(1);
+  }
+  float c1, c2, n1 = 0.f, n2 = 0.f;
+  pen(0, c1, c2);
+  uint32_t phase = 0u;  // bit b: parity of buffer b's next phase
+  float L[K], m = 0.f;
+  float* out = a.out[g.dir] + lane * K;
+  float* ck = a.ckpt[g.dir] + (size_t)ln.line * g.nseg * D + lane * K;
+  for (int c = 0; c < nch; ++c) {
+    const int b = c % NB, n = chunk_n(c);
+    pen(c + 1, n1, n2);  // a chunk ahead
+    if (!sgm::mbar_wait_warp(&bars[w][b], (phase >> b) & 1u)) {
+      sgm::scan_give_up_mask(bars[w], phase, (1u << b) | (c + 1 < nch ? 1u << ((c + 1) % NB) : 0u));
+      return;
+    }
+    phase ^= 1u << b;
+    __syncwarp();
+    const float* bx = box0 + b * C * D + lane * K;
+    float cv[C][K];
+#pragma unroll
+    for (int j = 0; j < C; ++j) ld_lane<K>(bx + (rev ? C - 1 - j : j) * D, cv[j]);
+    sgm::fence_proxy_async();  // this lane's reads of the buffer before the copy that refills it
+    __syncwarp();
+    if (lane == 0 && c + 2 < nch) issue(c + 2);
+    float* op = out + (base + (long long)c * C * step) * D;  // step 0 of the chunk
+    const long long od = step * D;
+    auto one = [&](int j) {
+      const float P1 = __shfl_sync(kFullMask, c1, j), P2 = __shfl_sync(kFullMask, c2, j);
+      const int s = c * C + j;
+      if (j % kSeg == 0 && (j > 0 || c > 0)) st_lane<K>(ck + (size_t)(s / kSeg) * D, L);  // state entering
+      if (j == 0 && c == 0) {
+#pragma unroll
+        for (int t = 0; t < K; ++t) L[t] = cv[0][t];
+        m = warp_min(minK<K>(L));
+      } else {
+        fstep_warp<K>(L, cv[j], m, P1, P2);
+      }
+      st_lane<K>(op + j * od, L);
+    };
+    if (n == C) {
+#pragma unroll
+      for (int j = 0; j < C; ++j) one(j);
+    } else {  // the last, short chunk
+#pragma unroll
+      for (int j = 0; j < C; ++j)
+        if (j < n) one(j);
+    }
+    c1 = n1;
+    c2 = n2;
   }
 }
 
@@ -626,10 +714,32 @@ Grid4 make_grid(int B, int H, int W, int D) {
   return q;
 }
 
-template <int G, int K>
+// The cost volume [B][H][W][D] floats as a 3D tensor map (floats of a row, rows, images) with
+// boxes of D x kFC x 1: the forward column scans' chunks.
+int cost_map(const float* cost, int B, int H, int W, int D, CUtensorMap* map) {
+  const sgm::EncodeTiledFn fn = sgm::encode_tiled();
+  if (!fn) {
+    sgm_set_process_error("float SGM: cuTensorMapEncodeTiled is not available from the driver");
+    return SGM_ERR_CUDA;
+  }
+  const cuuint64_t dims[3] = {(cuuint64_t)W * D, (cuuint64_t)H, (cuuint64_t)B};
+  const cuuint64_t strides[2] = {(cuuint64_t)W * D * sizeof(float), (cuuint64_t)H * W * D * sizeof(float)};
+  const cuuint32_t box[3] = {(cuuint32_t)D, (cuuint32_t)kFC, 1u};
+  const cuuint32_t estr[3] = {1u, 1u, 1u};
+  const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(cost), dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    sgm_set_process_error("float SGM: cuTensorMapEncodeTiled failed for the cost volume");
+    return SGM_ERR_CUDA;
+  }
+  return SGM_OK;
+}
+
+template <int K>
 int forward_impl(const float* cost, const float* p1, const float* p2, int B, int H, int W, float inv_t, float* sum,
                  float* ckpt, float* work, float* disp, cudaStream_t s) {
-  constexpr int D = G * K;
+  constexpr int D = 32 * K;
   const size_t V = (size_t)B * H * W * D, npix = (size_t)B * H * W;
   FwdArgs a;
   a.cost = cost;
@@ -639,9 +749,15 @@ int forward_impl(const float* cost, const float* p1, const float* p2, int B, int
   for (int i = 1; i < 4; ++i) a.out[i] = work + (i - 1) * V;
   const size_t slab = slab_elems(B, H, W, D);
   for (int i = 0; i < 4; ++i) a.ckpt[i] = ckpt + slab * i;
-  a.q = make_grid<G>(B, H, W, D);
-  k_float_fwd<G, K><<<a.q.first_block[4], kWarps * 32, 0, s>>>(a);
-  int st = check("float forward");
+  a.q = make_grid<32>(B, H, W, D);
+  CUtensorMap tm;
+  int st = cost_map(cost, B, H, W, D, &tm);
+  if (st) return st;
+  constexpr size_t smem = fwd_smem_bytes<K>();
+  if (cudaFuncSetAttribute(k_float_fwd<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return check("float forward attribute");
+  k_float_fwd<K><<<a.q.first_block[4], kWarps * 32, smem, s>>>(tm, a);
+  st = check("float forward");
   if (st) return st;
   constexpr int GS = D / kK;  // lanes per pixel of the soft-argmin kernels
   const size_t px_per_block = 8 * (32 / GS);
@@ -703,6 +819,13 @@ int backward_impl(const float* cost, const float* p1, const float* p2, int B, in
 
 }  // namespace
 
+// Waits of the forward scans that ran out (sgm_debug_wait_timeouts adds them to the engine's).
+int64_t sgm_float_wait_timeouts() {
+  unsigned int n = 0;
+  if (cudaMemcpyFromSymbol(&n, sgm::g_scan_wait_timeouts, sizeof(n)) != cudaSuccess) return -1;
+  return n;
+}
+
 extern "C" {
 
 size_t sgm_float_checkpoint_elems(int32_t B, int32_t H, int32_t W, int32_t D) {
@@ -726,8 +849,8 @@ int sgm_float_forward(const float* cost, const float* p1, const float* p2, int32
     return st;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const float inv_t = 1.0f / temperature;
-  return D == 64 ? forward_impl<kFwdLanes64, 64 / kFwdLanes64>(cost, p1, p2, B, H, W, inv_t, sum, ckpt, work, disp, s)
-                 : forward_impl<kFwdLanes32, 32 / kFwdLanes32>(cost, p1, p2, B, H, W, inv_t, sum, ckpt, work, disp, s);
+  return D == 64 ? forward_impl<2>(cost, p1, p2, B, H, W, inv_t, sum, ckpt, work, disp, s)
+                 : forward_impl<1>(cost, p1, p2, B, H, W, inv_t, sum, ckpt, work, disp, s);
 }
 
 int sgm_float_backward(const float* cost, const float* p1, const float* p2, int32_t B, int32_t H, int32_t W, int32_t D,

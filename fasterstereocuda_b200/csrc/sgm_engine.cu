@@ -24,6 +24,7 @@
 #include "sgm_alloc.h"
 #include "sgm_kernels4.cuh"
 #include "sgm_levels.h"
+#include "sgm_tma.h"
 
 namespace {
 
@@ -160,6 +161,7 @@ cudaError_t sgm_dev_free(void* p) {
 }
 
 void sgm_set_process_error(const char* msg) { set_error(nullptr, "%s", msg); }
+int64_t sgm_float_wait_timeouts();  // float_sgm.cu
 
 // One matching level (the state of one StereoCuda instance).
 struct sgm_engine {
@@ -490,20 +492,8 @@ int launch_cols3_pass(sgm_engine* e, int G, const sgm::PlainParams& P, const sgm
   }
 }
 
-// cuTensorMapEncodeTiled from the driver, looked up once through the runtime (no link against
-// the driver library).
-using EncodeTiledFn = decltype(&cuTensorMapEncodeTiled);
-EncodeTiledFn encode_tiled() {
-  static const EncodeTiledFn fn = [] {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
-    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) != cudaSuccess ||
-        q != cudaDriverEntryPointSuccess)
-      p = nullptr;
-    return reinterpret_cast<EncodeTiledFn>(p);
-  }();
-  return fn;
-}
+using sgm::EncodeTiledFn;
+using sgm::encode_tiled;
 
 // Tensor map i (0 cost, 1 bt, 2 lr, 3 rl) of the engine's volumes, [nv][H][W * D] bytes, in boxes
 // of 32 rows x D bytes with the D-byte swizzle (k_vscan_plain4); rebuilt when the volume moved.
@@ -1684,7 +1674,8 @@ int sgm_debug_read(sgm_handle_t h, int32_t which, int32_t view, void* dst, size_
 int64_t sgm_debug_wait_timeouts(void) {
   unsigned int n = 0;
   if (cudaMemcpyFromSymbol(&n, sgm::g_scan_wait_timeouts, sizeof(n)) != cudaSuccess) return -1;
-  return n;
+  const int64_t f = sgm_float_wait_timeouts();
+  return f < 0 ? -1 : n + f;
 }
 
 int sgm_debug_fail_device_alloc(int64_t after) {
