@@ -181,7 +181,7 @@ def _blocky_pair(seed, W, H, shift=5):
     return L, R
 
 
-@pytest.mark.parametrize("lanes", [(2, 2), (8, 8)])
+@pytest.mark.parametrize("lanes", [(2, 2), (8, 8), "latency"])
 @pytest.mark.parametrize("tie", [4, 0])
 def test_init_disparity_ties_low_texture(engine_lib, oracle_mod, tie, lanes):
     import fasterstereocuda_b200 as fsc
@@ -191,7 +191,8 @@ def test_init_disparity_ties_low_texture(engine_lib, oracle_mod, tie, lanes):
     init = np.full((H, W), 3, np.int16)
     init[:, ::17] = 9
     s = make_engine(fsc, W, H, 0, 32, 1, 10, 150, 0.95, 1, 1, tie=tie)
-    assert s.set_tuning(fsc.Tuning(3, 0, 3, 0, 0, *lanes)), s.last_error()
+    t = (4, 0, 4, 0, 0) if lanes == "latency" else (3, 0, 3, 0, 0, *lanes)
+    assert s.set_tuning(fsc.Tuning(*t)), s.last_error()
     disp = np.empty((H, W), np.float32)
     assert s.Match(L, R, disp, None, init), s.last_error()
     cfg = O.Config(width=W, height=H, disp_range=32, cs_type=1, p1=10, p2=150, uniqueness=0.95, do_lr_check=1,
@@ -200,6 +201,71 @@ def test_init_disparity_ties_low_texture(engine_lib, oracle_mod, tie, lanes):
     assert_same("wta left", s.debug_read("wta", 0), ref["wta_l"])
     assert_same("wta right", s.debug_read("wta", 1), ref["wta_r"])
     assert_same("disp left", disp, ref["disp"])
+
+
+@pytest.mark.parametrize("variant", [None, (4, 0, 4, 0, 0)])
+def test_init_disparity_invalid_runs_and_jumps(engine_lib, oracle_mod, variant):
+    """Initial disparities with 30 % INVALID pixels, INVALID runs longer than a 32-step chunk (whole
+    chunks skipped, a scanline starting INVALID) and base jumps beyond the 32-disparity range:
+    every stage against the oracle, for the default and the warp-per-scanline kernels."""
+    import fasterstereocuda_b200 as fsc
+    O = oracle_mod
+    W, H = 203, 97
+    L, R, _ = scenes.planar_pair(57, W, H)
+    rng = np.random.default_rng(5)
+    init = rng.integers(0, 41, (H, W)).astype(np.int16)
+    init[rng.random((H, W)) < 0.3] = -32768
+    init[10:20, 30:110] = -32768   # rows with a run of 80 INVALID pixels
+    init[:, 0] = -32768            # every row starts INVALID
+    init[40:60, 150:190] = -32768  # columns with a run of 20
+    init[5:90, 170:172] = -32768   # columns with a run of 85
+    init[::7, ::5] = 0             # realignments of up to 40 between neighbours
+    init[3::7, 2::5] = 40
+    s = make_engine(fsc, W, H, 0, 32, 1, 10, 150, 0.95, 1, 1)
+    if variant is not None:
+        assert s.set_tuning(fsc.Tuning(*variant)), s.last_error()
+    disp = np.empty((H, W), np.float32)
+    assert s.Match(L, R, disp, None, init), s.last_error()
+    assert engine_lib.sgm_debug_wait_timeouts() == 0
+    cfg = O.Config(width=W, height=H, disp_range=32, do_lr_check=1, do_median=1, peaks_strips=STRIPS)
+    ref = O.match(cfg, L, R, init, dump=True, want_right=True)
+    valid = init != -32768
+    assert_same("path L->R", s.debug_read("lr"), ref["paths"][1], valid)
+    assert_same("path R->L", s.debug_read("rl"), ref["paths"][3], valid)
+    bt = read_bt(s)
+    if bt is not None:
+        assert_same("path B->T", bt, ref["paths"][2], valid)
+    assert_same("wta left", s.debug_read("wta", 0), ref["wta_l"])
+    assert_same("wta right", s.debug_read("wta", 1), ref["wta_r"])
+    assert_same("disp left", disp, ref["disp"])
+
+
+@pytest.mark.parametrize("kind", ["plain64", "plain128", "init32"])
+@pytest.mark.parametrize("p1,p2", [(10, 5_000_000), (3_000_000, 5_000_000)])
+def test_latency_kernels_large_penalties(engine_lib, oracle_mod, kind, p1, p2):
+    """The warp-per-scanline kernels compute in 32 bits like the reference: any penalties are exact
+    (the 32-disparity row scan packs P2' into 22 bits and leaves larger penalties to the default)."""
+    import fasterstereocuda_b200 as fsc
+    O = oracle_mod
+    W, H = 150, 83
+    L, R, _ = scenes.planar_pair(71, W, H)
+    disp = np.empty((H, W), np.float32)
+    if kind == "init32":
+        init = _init_for(O, L, R, 1, 10, 150)
+        s = make_engine(fsc, W, H, 0, 32, 1, p1, p2, 0.95, 1, 1)
+        assert s.set_tuning(fsc.Tuning(4, 0, 4, 0, 0)), s.last_error()
+        assert s.Match(L, R, disp, None, init), s.last_error()
+        ref = O.match(O.Config(width=W, height=H, disp_range=32, p1=p1, p2=p2, do_lr_check=1, do_median=1,
+                               peaks_strips=STRIPS), L, R, init)
+    else:
+        D = 64 if kind == "plain64" else 128
+        s = make_engine(fsc, W, H, 0, D, 1, p1, p2, 0.95, 1, 1)
+        assert s.set_tuning(fsc.Tuning(4, 0, 4, 0, 0)), s.last_error()
+        assert s.Match(L, R, disp), s.last_error()
+        ref = O.match(O.Config(width=W, height=H, disp_range=D, p1=p1, p2=p2, do_lr_check=1, do_median=1,
+                               peaks_strips=STRIPS), L, R)
+    assert engine_lib.sgm_debug_wait_timeouts() == 0
+    assert_same(f"disp {kind}", disp, ref["disp"])
 
 
 def test_init_disparity_tall_global_bt(engine_lib, oracle_mod):
