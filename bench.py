@@ -485,7 +485,7 @@ def run_ours(a, rank, world, local_rank):
     def host_worker(k, count):
         m = e2e_matchers[k]
         for j, b in enumerate(range(k, count, E)):
-            i = b % a.batch
+            i = b % len(hostL)
             if not m.Match(hostL[i], hostR[i], hostO[k][j % 2]):
                 raise RuntimeError(m.last_error())
 
