@@ -100,14 +100,16 @@ typedef struct sgm_tuning_t {
   int32_t row_kernel;   /* horizontal scans: 1 = whole census rows in shared memory,
                            2 = census window and 32-pixel cost chunks in shared memory,
                            3 = cost-volume kernel + row_lanes lanes per scanline (u16x2 SIMD),
-                           4 = (32-disparity pyramid levels; elsewhere the default) one warp per
-                           scanline with cost chunks staged by bulk async copies: the shortest
-                           step chain, for one pair in flight;
+                           4 = one warp per scanline with cost chunks staged by bulk async copies
+                           and 32-bit path costs: the shortest step chain, for one pair in flight
+                           (D <= 128 and tie rule 0, 1 or 4 at plain levels; any tie rule at the
+                           32-disparity pyramid levels; elsewhere the default);
                            0 (default) = 3 where it is exact (see below), else 2 */
   int32_t rows_per_cta; /* scanlines per CTA of the horizontal scans: 0 (default), 1, 2 or 4 */
   int32_t col_kernel;   /* vertical scans + WTA: 1 = one warp per column, plain loads, 2 = the same with
                            an 8-row prefetch ring, 3 = col_lanes lanes per column (u16x2 SIMD, WTA in
-                           the lanes), 4 = as row_kernel 4 (32-disparity levels); 0 (default) = 3
+                           the lanes), 4 = as row_kernel 4 (chunks of 32 rows as tensor-map boxes,
+                           the WTA per chunk with one lane per pixel); 0 (default) = 3
                            where it is exact, else 1. Variant 3 is exact for D <= 128,
                            P1 <= P2 <= 16383 and tie rule 0 or 4 (else 2 / 1 run) */
   int32_t cols_per_cta; /* columns (one warp each) per CTA of the vertical scans: 0 (default) .. 8 */
