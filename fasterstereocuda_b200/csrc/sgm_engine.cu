@@ -11,6 +11,7 @@
 #include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -213,10 +214,11 @@ struct sgm_engine {
     int W = 0, H = 0, D = 0, nv = 0;
   } tmap_key[4];
   // img[0], img[1] -> out captured as a CUDA graph after a first direct run (matches without
-  // initial disparities or a right map); later matches copy in, launch it, copy out.
-  cudaGraphExec_t gexec = nullptr;
-  int direct_runs = 0;
-  int64_t graph_launches = 0;
+  // initial disparities or a right map); later matches copy in, launch it, copy out. One graph
+  // per kernel mode (0: the matcher's tuning, 1: the latency kernels of KernelMode).
+  cudaGraphExec_t gexec[2] = {};
+  int direct_runs[2] = {};
+  int64_t graph_launches[2] = {};
   cudaEvent_t done = nullptr;  // blocking-sync event of the synchronous host API
   // Stages of a match: an NVTX range each, and with print_log a CUDA event at every stage boundary
   // for the per-stage report of the synchronous host API.
@@ -227,9 +229,15 @@ struct sgm_engine {
   cudaEvent_t stage_ev[kMaxStages] = {};
   const char* stage_name[kMaxStages] = {};
   void drop_graph() {
-    if (gexec) cudaGraphExecDestroy(gexec);
-    gexec = nullptr;
-    direct_runs = 0;
+    for (int k = 0; k < 2; ++k) {
+      if (gexec[k]) cudaGraphExecDestroy(gexec[k]);
+      gexec[k] = nullptr;
+      direct_runs[k] = 0;
+    }
+  }
+  bool tuning_is_default() const {
+    return !tune_rows && !tune_cols && !tune_bt_smem && !tune_row_kernel && !tune_col_kernel && !tune_row_lanes &&
+           !tune_col_lanes;
   }
 
   int nviews() const { return opt.do_lr_check ? 2 : 1; }
@@ -1173,18 +1181,19 @@ namespace {
 // A match without initial disparities or a right map on stream s (0: the matcher's own). Without
 // profiling, the second and later calls replay a CUDA graph of the match on the matcher's own
 // buffers, with device-to-device copies around it when the caller's buffers differ.
-int engine_run(sgm_engine* e, const uint8_t* dl, const uint8_t* dr, float* dout, cudaStream_t s) {
+int engine_run(sgm_engine* e, const uint8_t* dl, const uint8_t* dr, float* dout, cudaStream_t s, int mode = 0) {
   if (!s) s = e->stream;
   if (g_prof.on) {
     e->drop_graph();
     return engine_enqueue(e, dl, dr, nullptr, dout, nullptr, s);
   }
-  if (!e->gexec && e->direct_runs == 0) {
-    e->direct_runs++;
+  cudaGraphExec_t& gexec = e->gexec[mode];
+  if (!gexec && e->direct_runs[mode] == 0) {
+    e->direct_runs[mode]++;
     return engine_enqueue(e, dl, dr, nullptr, dout, nullptr, s);
   }
   const size_t N = e->npix();
-  if (!e->gexec) {
+  if (!gexec) {
     if (cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
       set_error(&e->err, "graph capture could not start");
       return SGM_ERR_CUDA;
@@ -1198,22 +1207,62 @@ int engine_run(sgm_engine* e, const uint8_t* dl, const uint8_t* dr, float* dout,
       if (!st) set_error(&e->err, "graph capture failed: %s", cudaGetErrorString(ce));
       return st ? st : SGM_ERR_CUDA;
     }
-    const cudaError_t ie = cudaGraphInstantiate(&e->gexec, g, 0);
+    const cudaError_t ie = cudaGraphInstantiate(&gexec, g, 0);
     cudaGraphDestroy(g);
     if (ie != cudaSuccess) {
-      e->gexec = nullptr;
+      gexec = nullptr;
       set_error(&e->err, "graph instantiation failed: %s", cudaGetErrorString(ie));
       return SGM_ERR_CUDA;
     }
-    e->graph_launches = e->launches;
+    e->graph_launches[mode] = e->launches;
   }
   if (dl != e->img[0]) SGM_CUDA_TRY(e, cudaMemcpyAsync(e->img[0], dl, N, cudaMemcpyDeviceToDevice, s));
   if (dr != e->img[1]) SGM_CUDA_TRY(e, cudaMemcpyAsync(e->img[1], dr, N, cudaMemcpyDeviceToDevice, s));
-  SGM_CUDA_TRY(e, cudaGraphLaunch(e->gexec, s));
+  SGM_CUDA_TRY(e, cudaGraphLaunch(gexec, s));
   if (dout != e->out) SGM_CUDA_TRY(e, cudaMemcpyAsync(dout, e->out, N * sizeof(float), cudaMemcpyDeviceToDevice, s));
-  e->launches = e->graph_launches;
+  e->launches = e->graph_launches[mode];
   return SGM_OK;
 }
+
+// The synchronous host API (the reference's Match) on a matcher left at the default tuning: while
+// at most kLatencyInFlight such calls run in the process -- one caller matching one frame at a
+// time, the reference's own use -- the match takes the warp-per-scanline kernels (variant 4, the
+// shortest step chains: a 1242x375x64 pyramid pair 0.37 instead of 1.46 ms alone); with more
+// calls in flight it takes the default thread-per-scanline kernels, which give more pairs per
+// second when many pairs share the GPU (36 % more at 32 in flight). Both give the same bits.
+constexpr int kLatencyInFlight = 2;
+std::atomic<int> g_host_in_flight{0};
+
+struct HostCall {
+  int n;
+  HostCall() : n(++g_host_in_flight) {}
+  ~HostCall() { --g_host_in_flight; }
+  HostCall(const HostCall&) = delete;
+  HostCall& operator=(const HostCall&) = delete;
+  bool latency() const { return n <= kLatencyInFlight; }
+};
+
+// Row and column kernels set to variant 4 on the given engines for the scope of one match, when
+// `latency` and every engine is at the default tuning; mode() is the graph slot to use.
+struct KernelMode {
+  sgm_engine* const* lv;
+  int n;
+  bool on = false;
+  KernelMode(sgm_engine* const* levels, int count, bool latency) : lv(levels), n(count) {
+    if (!latency) return;
+    for (int i = 0; i < n; ++i)
+      if (!lv[i]->tuning_is_default()) return;
+    on = true;
+    for (int i = 0; i < n; ++i) lv[i]->tune_row_kernel = lv[i]->tune_col_kernel = 4;
+  }
+  ~KernelMode() {
+    if (on)
+      for (int i = 0; i < n; ++i) lv[i]->tune_row_kernel = lv[i]->tune_col_kernel = 0;
+  }
+  KernelMode(const KernelMode&) = delete;
+  KernelMode& operator=(const KernelMode&) = delete;
+  int mode() const { return on ? 1 : 0; }
+};
 
 int enqueue_depth(sgm_engine* e, const float* disp, float* depth, const sgm_camera_t& c, cudaStream_t s) {
   const int n = (int)e->npix();
@@ -1242,16 +1291,18 @@ struct sgm_pyramid {
   sgm_camera_t cam0{};
   float* disp0 = nullptr;  // finest-level disparity in depth mode
   // The whole pyramid (in_l, in_r -> out) captured once as a CUDA graph after a first direct run;
-  // later matches copy in, launch it, copy out.
-  cudaGraphExec_t gexec = nullptr;
-  int direct_runs = 0;
-  int64_t graph_launches = 0;  // kernels inside the graph
+  // later matches copy in, launch it, copy out. One graph per kernel mode (see KernelMode).
+  cudaGraphExec_t gexec[2] = {};
+  int direct_runs[2] = {};
+  int64_t graph_launches[2] = {};  // kernels inside the graph
   cudaEvent_t done = nullptr;  // blocking-sync event of the synchronous host API
 
   void drop_graph() {
-    if (gexec) cudaGraphExecDestroy(gexec);
-    gexec = nullptr;
-    direct_runs = 0;
+    for (int k = 0; k < 2; ++k) {
+      if (gexec[k]) cudaGraphExecDestroy(gexec[k]);
+      gexec[k] = nullptr;
+      direct_runs[k] = 0;
+    }
   }
 
   void free_all() {
@@ -1328,17 +1379,18 @@ int pyr_enqueue(sgm_pyramid* p, const uint8_t* dl, const uint8_t* dr, float* dou
 // One pyramid match on stream s. Without profiling, the second and later calls replay a CUDA
 // graph of the whole pyramid on the matcher's own buffers (one launch instead of one per
 // kernel), with device-to-device copies around it when the caller's buffers differ.
-int pyr_run(sgm_pyramid* p, const uint8_t* dl, const uint8_t* dr, float* dout, cudaStream_t s) {
+int pyr_run(sgm_pyramid* p, const uint8_t* dl, const uint8_t* dr, float* dout, cudaStream_t s, int mode = 0) {
   if (g_prof.on) {
     p->drop_graph();
     return pyr_enqueue(p, dl, dr, dout, s);
   }
-  if (!p->gexec && p->direct_runs == 0) {
-    p->direct_runs++;
+  cudaGraphExec_t& gexec = p->gexec[mode];
+  if (!gexec && p->direct_runs[mode] == 0) {
+    p->direct_runs[mode]++;
     return pyr_enqueue(p, dl, dr, dout, s);
   }
   const size_t N = (size_t)p->W * p->H;
-  if (!p->gexec) {
+  if (!gexec) {
     if (cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
       p->err = "graph capture could not start";
       return SGM_ERR_CUDA;
@@ -1352,24 +1404,24 @@ int pyr_run(sgm_pyramid* p, const uint8_t* dl, const uint8_t* dr, float* dout, c
       if (!st) p->err = std::string("graph capture failed: ") + cudaGetErrorString(ce);
       return st ? st : SGM_ERR_CUDA;
     }
-    const cudaError_t ie = cudaGraphInstantiate(&p->gexec, g, 0);
+    const cudaError_t ie = cudaGraphInstantiate(&gexec, g, 0);
     cudaGraphDestroy(g);
     if (ie != cudaSuccess) {
-      p->gexec = nullptr;
+      gexec = nullptr;
       p->err = std::string("graph instantiation failed: ") + cudaGetErrorString(ie);
       return SGM_ERR_CUDA;
     }
-    p->graph_launches = p->launches;
+    p->graph_launches[mode] = p->launches;
   }
   if (dl != p->in_l && cudaMemcpyAsync(p->in_l, dl, N, cudaMemcpyDeviceToDevice, s) != cudaSuccess) return SGM_ERR_CUDA;
   if (dr != p->in_r && cudaMemcpyAsync(p->in_r, dr, N, cudaMemcpyDeviceToDevice, s) != cudaSuccess) return SGM_ERR_CUDA;
-  if (cudaGraphLaunch(p->gexec, s) != cudaSuccess) {
+  if (cudaGraphLaunch(gexec, s) != cudaSuccess) {
     p->err = "graph launch failed";
     return SGM_ERR_CUDA;
   }
   if (dout != p->out && cudaMemcpyAsync(dout, p->out, N * sizeof(float), cudaMemcpyDeviceToDevice, s) != cudaSuccess)
     return SGM_ERR_CUDA;
-  p->launches = p->graph_launches;
+  p->launches = p->graph_launches[mode];
   return SGM_OK;
 }
 
@@ -1475,6 +1527,8 @@ int sgm_match(sgm_handle_t h, const uint8_t* img_left, const uint8_t* img_right,
   }
   const size_t N = h->npix();
   h->launches = 0;
+  const HostCall call;
+  const KernelMode km(&h, 1, call.latency());
   // with print_log: per-stage times, printed like the reference's timers (StereoCudaImpl.cpp:
   // 365-460, 530-543); the match then runs its kernels directly instead of as a graph
   h->stage_timing = h->print_log;
@@ -1490,7 +1544,7 @@ int sgm_match(sgm_handle_t h, const uint8_t* img_left, const uint8_t* img_right,
   const bool right = disp_right && h->opt.do_lr_check;
   const bool roi = roi_left || (roi_right && h->opt.do_lr_check);
   int st = (!init_disp_left && !right && !roi && !h->stage_timing)
-               ? engine_run(h, h->img[0], h->img[1], h->out, h->stream)
+               ? engine_run(h, h->img[0], h->img[1], h->out, h->stream, km.mode())
                : engine_enqueue(h, h->img[0], h->img[1], init_disp_left ? h->init[0] : nullptr, h->out,
                                 right ? h->dr_out : nullptr, h->stream, roi_left, roi_right);
   if (st) {
@@ -1556,6 +1610,8 @@ int sgm_match2(sgm_handle_t h, const uint8_t* img_left, const uint8_t* img_right
   if (!img_left || !img_right || !depth_left) return SGM_ERR_ARG;
   const size_t N = h->npix();
   h->launches = 0;
+  const HostCall call;
+  const KernelMode km(&h, 1, call.latency());
   SGM_CUDA_TRY(h, cudaMemcpyAsync(h->img[0], img_left, N, cudaMemcpyHostToDevice, h->stream));
   SGM_CUDA_TRY(h, cudaMemcpyAsync(h->img[1], img_right, N, cudaMemcpyHostToDevice, h->stream));
   if (init_disp_left)
@@ -1789,10 +1845,12 @@ int sgm_pyr_match(sgm_pyr_handle_t h, const uint8_t* img_left, const uint8_t* im
   if (!img_left || !img_right || !disp) return SGM_ERR_ARG;
   const size_t N = (size_t)h->W * h->H;
   h->launches = 0;
+  const HostCall call;
+  const KernelMode km(h->lv.data(), (int)h->lv.size(), call.latency());
   if (cudaMemcpyAsync(h->in_l, img_left, N, cudaMemcpyHostToDevice, h->stream) ||
       cudaMemcpyAsync(h->in_r, img_right, N, cudaMemcpyHostToDevice, h->stream))
     return SGM_ERR_CUDA;
-  int st = pyr_run(h, h->in_l, h->in_r, h->out, h->stream);
+  int st = pyr_run(h, h->in_l, h->in_r, h->out, h->stream, km.mode());
   if (st) return st;
   if (cudaMemcpyAsync(disp, h->out, N * sizeof(float), cudaMemcpyDeviceToHost, h->stream)) return SGM_ERR_CUDA;
   if (wait_stream(h->stream, &h->done) != cudaSuccess) {

@@ -78,7 +78,8 @@ CASES = {
 
 
 SCANLINE = {"warp": (2, 0, 1, 0, 0, 0, 0), "scanline_g1": (3, 0, 3, 0, 0, 1, 1),
-            "scanline_g8": (3, 0, 3, 0, 0, 8, 8), "latency": (4, 0, 4, 0, 0, 0, 0)}
+            "scanline_g8": (3, 0, 3, 0, 0, 8, 8), "latency": (4, 0, 4, 0, 0, 0, 0),
+            "default": (0, 0, 0, 0, 0, 8, 4)}
 
 
 @pytest.mark.parametrize("name", list(CASES))
@@ -100,7 +101,9 @@ def test_plain_parity(engine_lib, oracle_mod, name, tie, variant):
     if variant != "default":
         if tie != 4 and variant not in ("warp", "latency"):
             pytest.skip("tie rule variants with the default lane split only")
-        assert s.set_tuning(fsc.Tuning(*SCANLINE[variant])), s.last_error()
+    # 'default': the default kernels and lane split, set explicitly (a matcher left at the default
+    # tuning runs the latency kernels when its synchronous host API is called by one caller)
+    assert s.set_tuning(fsc.Tuning(*SCANLINE[variant])), s.last_error()
     disp = np.empty((H, W), np.float32)
     disp_r = np.empty((H, W), np.float32)
     assert s.Match(L, R, disp, disp_r), s.last_error()
@@ -286,9 +289,13 @@ def test_init_disparity_tall_global_bt(engine_lib, oracle_mod):
     assert_same("disp left", disp, ref["disp"])
 
 
+@pytest.mark.parametrize("kernels", ["auto", "throughput"])
 @pytest.mark.parametrize("override", [True, False])
 @pytest.mark.parametrize("size,layers", [((1242, 375), 3), ((450, 375), 2), ((640, 480), 4)])
-def test_pyramid_parity(engine_lib, oracle_mod, override, size, layers):
+def test_pyramid_parity(engine_lib, oracle_mod, override, size, layers, kernels):
+    """'auto': the default tuning, which the synchronous host API runs with the latency kernels for
+    a single caller; 'throughput': the default thread-per-scanline kernels set explicitly. Three
+    matches: the direct run, the graph capture and a graph replay."""
     import fasterstereocuda_b200 as fsc
     O = oracle_mod
     W, H = size
@@ -298,17 +305,59 @@ def test_pyramid_parity(engine_lib, oracle_mod, override, size, layers):
                             do_rm_peaks=True)
     ov = fsc.LevelOverride(cs_type=1, p1=10, p2=150) if override else None
     assert p.Init(opt, ov, fsc.ExtOptions(peaks_strips=STRIPS)), p.last_error()
-    disp = np.empty((H, W), np.float32)
-    assert p.Match(L, R, disp)
+    if kernels == "throughput":
+        assert p.set_tuning(fsc.Tuning(0, 0, 0, 0, 0, 8, 4)), p.last_error()
     pc = O.PyrConfig(width=W, height=H, min_disp=0, max_disp=64, num_layers=layers, override_enable=int(override),
                      cs_type=1 if override else 0, p1=10 if override else 8, p2=150 if override else 32,
                      peaks_strips=STRIPS)
     ref = O.pyr_match(pc, L, R)
-    assert_same("pyramid disp", disp, ref)
+    for k in range(3):
+        disp = np.empty((H, W), np.float32)
+        assert p.Match(L, R, disp)
+        assert_same(f"pyramid disp, match {k}", disp, ref)
+    assert engine_lib.sgm_debug_wait_timeouts() == 0
     for lvl in range(layers):
         w, h, m, d = p.level_info(lvl)
         c = O.pyr_level_config(pc, lvl)
         assert (w, h, m, d) == (c.width, c.height, c.min_disp, c.disp_range)
+
+
+def test_host_api_kernel_modes_under_concurrency(engine_lib, oracle_mod):
+    """Default-tuned matchers called through the synchronous host API by one thread (the latency
+    kernels) and by six threads at once (the throughput kernels while more than two calls are in
+    flight): every match -- direct runs, captures and replays of both graphs -- equals the oracle."""
+    import fasterstereocuda_b200 as fsc
+    from concurrent.futures import ThreadPoolExecutor
+    O = oracle_mod
+    W, H = 450, 240
+    pairs = [scenes.kitti_like(60 + i, W, H)[:2] for i in range(2)]
+    pc = O.PyrConfig(width=W, height=H, min_disp=0, max_disp=64, num_layers=2, override_enable=1, cs_type=1,
+                     p1=10, p2=150, peaks_strips=STRIPS)
+    refs = [O.pyr_match(pc, L, R) for L, R in pairs]
+    ms = []
+    for _ in range(6):
+        p = fsc.FasterStereoCuda()
+        assert p.Init(fsc.StereoOption1(width=W, height=H, min_disp=0, max_disp=64, num_layers=2, do_lr_check=True,
+                                        do_rm_peaks=True), fsc.LevelOverride(1, 10, 150),
+                      fsc.ExtOptions(peaks_strips=STRIPS)), p.last_error()
+        ms.append(p)
+
+    def work(k, n):
+        out = []
+        for j in range(n):
+            i = (k + j) % 2
+            disp = np.empty((H, W), np.float32)
+            assert ms[k].Match(pairs[i][0], pairs[i][1], disp), ms[k].last_error()
+            out.append((i, disp))
+        return out
+    results = work(0, 4)  # one caller: latency kernels
+    with ThreadPoolExecutor(max_workers=6) as ex:
+        for r in ex.map(lambda k: work(k, 6), range(6)):
+            results += r
+    results += work(1, 3)  # alone again: the latency graph of a matcher that ran both
+    for i, disp in results:
+        assert_same("pyramid disp", disp, refs[i])
+    assert engine_lib.sgm_debug_wait_timeouts() == 0
 
 
 def test_device_api_matches_host_api(engine_lib, oracle_mod):
