@@ -95,7 +95,10 @@ SGM_API int sgm_set_ext_options(sgm_handle_t h, const sgm_ext_options_t* ext);
 SGM_API int sgm_get_ext_options(sgm_handle_t h, sgm_ext_options_t* ext);
 
 /* No counterpart in the reference. Kernel variants and launch shapes; results do not depend on
- * them (every variant is bit-exact), only speed does. 0 everywhere = defaults. */
+ * them (every variant is bit-exact), only speed does. 0 everywhere = defaults; a matcher left at
+ * the defaults runs, in the synchronous host API (sgm_match, sgm_match2, sgm_pyr_match,
+ * sgm_pyr_match2), row_kernel = col_kernel = 4 while at most two such calls are in flight in the
+ * process (one caller matching one frame at a time) and the defaults below otherwise. */
 typedef struct sgm_tuning_t {
   int32_t row_kernel;   /* horizontal scans: 1 = whole census rows in shared memory,
                            2 = census window and 32-pixel cost chunks in shared memory,
