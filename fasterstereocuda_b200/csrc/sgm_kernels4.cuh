@@ -1,23 +1,29 @@
-// Latency form of the 32-disparity scans (pyramid levels below the coarsest), variant 4.
+// Latency form of the scans, variant 4: the 32-disparity pyramid levels (first half of this file)
+// and plain levels with D <= 128 (second half).
 //
 // A pair alone on the GPU offers few scanlines (375 rows x 2 directions at 1242x375), so the time
 // of a scan is its number of steps times the length of one step's dependency chain. Here one warp
-// owns a scanline and lane d holds disparity d in 32 bits, the reference's own arithmetic
-// (Kernel_Aggregate_{Horizontal,Vertical}_Warp, cusgm_ca.cu:1181-1338). A step's chain is then
+// owns a scanline and holds its path costs in 32 bits, the reference's own arithmetic
+// (Kernel_Aggregate_{Horizontal,Vertical}_Warp*, cusgm_ca.cu:1181-1888). At a 32-disparity level
+// lane d holds disparity d and a step's chain is
 //   m = prev_invalid ? 127 : min_d L(d)            one redux.sync, issued beside the shuffles
 //   a, b = L(d + s - 1), L(d + s + 1)              two shuffles (s = base - last_base)
 //   L'(d) = C(d) + min(L(d), a + P1, b + P1, m + P2') - m
 // and everything that does not depend on L is taken off it:
-//   * the chunk's 32 steps of costs (and, for the top-to-bottom pass, of the three stored paths)
-//     are staged in shared memory by bulk async copies (cp.async.bulk with an mbarrier), one chunk
-//     ahead, double-buffered; a row chunk is one contiguous 1 KB copy, a column chunk one 32-byte
-//     copy per step;
+//   * costs (and, for the top-to-bottom pass, the three stored paths) arrive in chunks of 32 steps
+//     staged in shared memory by asynchronous copies completing on mbarriers: a row chunk is one
+//     contiguous cp.async.bulk copy, a column chunk one box of a 3D tensor map
+//     (cp.async.bulk.tensor, swizzled so that lanes reading consecutive box rows hit distinct
+//     banks), issued ahead of use;
 //   * the per-step bookkeeping of the initial disparities -- the realignment shift, P2' =
 //     max(P1, P2 / |last_base - base + 1|), which steps are skipped for an INVALID base -- is
-//     computed for the whole chunk at once, one step per lane (ballot for the last valid base);
-//   * path costs go to a shared-memory chunk and leave with 16-byte stores.
+//     computed for a whole chunk at once, one step per lane (ballot for the last valid base), the
+//     next chunk's beside the current chunk's steps;
+//   * path costs leave per step (row scans at the 32-disparity levels) or per chunk with one bulk
+//     or tensor store, and the top-to-bottom pass takes the WTA per chunk with lane = pixel.
 // Every wait on an mbarrier is bounded: after kMaxWaitTries polls the warp records the timeout in
-// g_scan_wait_timeouts (read by sgm_debug_wait_timeouts) and stops.
+// g_scan_wait_timeouts (read by sgm_debug_wait_timeouts), waits (bounded again) for its copies in
+// flight and stops.
 #pragma once
 #include <cuda.h>  // CUtensorMap
 
