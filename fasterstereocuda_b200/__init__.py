@@ -200,7 +200,8 @@ def load_library(path: Optional[os.PathLike] = None):
         "sgm_debug_read": (i32, [vp, i32, i32, vp, C.c_size_t]),
         "sgm_profile_enable": (i32, [i32]), "sgm_profile_read": (i32, [C.c_char_p, C.c_size_t]),
         "sgm_debug_fail_device_alloc": (i32, [i64]), "sgm_debug_live_device_allocations": (i64, []),
-        "sgm_debug_wait_timeouts": (i64, []),
+        "sgm_debug_wait_timeouts": (i64, []), "sgm_debug_scan_wait": (i32, [i64, i32]),
+        "sgm_debug_reset_wait_timeouts": (i32, []),
         "sgm_batch_create": (i32, [C.POINTER(vp)]), "sgm_batch_destroy": (i32, [vp]),
         "sgm_batch_last_error": (C.c_char_p, [vp]),
         "sgm_batch_init": (i32, [vp, C.POINTER(BatchPair), i32, C.POINTER(CuSGMOption), C.POINTER(ExtOptions)]),

@@ -14,6 +14,11 @@ constexpr int kScanChunk = 32;          // steps per staged chunk
 constexpr int kMaxWaitTries = 1 << 22;  // polls of an mbarrier before a wait is given up
 
 static __device__ unsigned int g_scan_wait_timeouts;
+// Tests of the give-up path (set by sgm_debug_scan_wait): the poll limit of every wait, and a
+// switch that makes the plain row scans expect 16 bytes more than their first copy delivers, so
+// that wait runs out.
+static __device__ unsigned int g_wait_limit = kMaxWaitTries;
+static __device__ unsigned int g_short_copy;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -33,10 +38,11 @@ __device__ __forceinline__ void bulk_to_smem(void* dst, const void* src, uint32_
                "l"(src), "r"(bytes), "r"(smem_u32(bar))
                : "memory");
 }
-// Waits for the phase of bar with the given parity; false after kMaxWaitTries polls.
+// Waits for the phase of bar with the given parity; false after g_wait_limit polls.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   const uint32_t a = smem_u32(bar);
-  for (int it = 0; it < kMaxWaitTries; ++it) {
+  const unsigned int limit = g_wait_limit;
+  for (unsigned int it = 0; it < limit; ++it) {
     uint32_t done;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"

@@ -1734,6 +1734,21 @@ int64_t sgm_debug_wait_timeouts(void) {
   return f < 0 ? -1 : n + f;
 }
 
+int sgm_debug_scan_wait(int64_t max_polls, int32_t short_copy) {
+  const unsigned int limit = max_polls > 0 && max_polls < sgm::kMaxWaitTries ? (unsigned int)max_polls
+                                                                               : (unsigned int)sgm::kMaxWaitTries;
+  const unsigned int sc = short_copy ? 1u : 0u;
+  if (cudaMemcpyToSymbol(sgm::g_wait_limit, &limit, sizeof(limit)) != cudaSuccess ||
+      cudaMemcpyToSymbol(sgm::g_short_copy, &sc, sizeof(sc)) != cudaSuccess)
+    return SGM_ERR_CUDA;
+  return SGM_OK;
+}
+
+int sgm_debug_reset_wait_timeouts(void) {
+  const unsigned int z = 0;
+  return cudaMemcpyToSymbol(sgm::g_scan_wait_timeouts, &z, sizeof(z)) == cudaSuccess ? SGM_OK : SGM_ERR_CUDA;
+}
+
 int sgm_debug_fail_device_alloc(int64_t after) {
   std::lock_guard<std::mutex> lk(g_alloc_mu);
   g_alloc_fail_after = after < 0 ? -1 : after;

@@ -557,7 +557,7 @@ __global__ void __launch_bounds__(32 * WPB) k_hscan_plain4(const uint8_t* __rest
   auto issue = [&](int c) {  // lane 0
     const int b = c % NB;
     const uint32_t bytes = (uint32_t)chunk_n(c) * D;
-    mbar_expect_tx(&bars[w][b], bytes);
+    mbar_expect_tx(&bars[w][b], bytes + (c == 0 && g_short_copy ? 16u : 0u));
     bulk_to_smem(cbuf[w][b] + chunk_off(c), crow + (size_t)chunk_x(c) * D, bytes, &bars[w][b]);
   };
   if (lane == 0) {

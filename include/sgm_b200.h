@@ -189,6 +189,12 @@ SGM_API int sgm_debug_fail_device_alloc(int64_t after);
  * kernels gave up on (each is bounded; a warp that gives up stops and leaves its outputs
  * incomplete). 0 in every correct run; -1 if it cannot be read. */
 SGM_API int64_t sgm_debug_wait_timeouts(void);
+/* Tests of that path: every such wait gives up after max_polls polls (<= 0: the default, 2^22),
+ * and with short_copy != 0 the warp-per-scanline plain row scans expect 16 bytes more than their
+ * first copy delivers, so that wait runs out (no memory is touched beyond the copies). The
+ * context stays usable. sgm_debug_reset_wait_timeouts sets the counter back to 0. */
+SGM_API int sgm_debug_scan_wait(int64_t max_polls, int32_t short_copy);
+SGM_API int sgm_debug_reset_wait_timeouts(void);
 SGM_API int64_t sgm_debug_live_device_allocations(void);
 
 /* No counterpart in the reference: per-kernel timing with CUDA events recorded on the launching
