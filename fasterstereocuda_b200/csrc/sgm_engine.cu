@@ -184,6 +184,7 @@ struct sgm_engine {
   uint8_t* img[2] = {nullptr, nullptr};
   void* cs[2] = {nullptr, nullptr};
   uint8_t *cost = nullptr, *lr = nullptr, *rl = nullptr, *bt = nullptr;
+  uint8_t* tb = nullptr;  // top-to-bottom path costs (warp-per-scanline column kernels; on first use)
   float* wta = nullptr;     // [2][H][W]
   float* post = nullptr;    // LR/median output
   float* post2 = nullptr;   // dilation output
@@ -206,13 +207,13 @@ struct sgm_engine {
   int tune_row_lanes = 0;   // variant 3: lanes per scanline (0: default)
   int tune_col_lanes = 0;
   bool bt_stored = true;    // the last match wrote the bottom->top volume to global memory
-  // tensor maps of the cost, bt, lr and rl volumes for the column kernels' box copies, and what
-  // each was built for (base, W, H, D, views)
-  CUtensorMap tmap[4];
+  // tensor maps of the cost, bt, lr, rl and tb volumes for the column kernels' box copies, and
+  // what each was built for (base, W, H, D, views)
+  CUtensorMap tmap[5];
   struct TmapKey {
     const void* base = nullptr;
     int W = 0, H = 0, D = 0, nv = 0;
-  } tmap_key[4];
+  } tmap_key[5];
   // img[0], img[1] -> out captured as a CUDA graph after a first direct run (matches without
   // initial disparities or a right map); later matches copy in, launch it, copy out. One graph
   // per kernel mode (0: the matcher's tuning, 1: the latency kernels of KernelMode).
@@ -264,6 +265,7 @@ struct sgm_engine {
       dfree(cost); dfree(lr); dfree(rl); dfree(bt);
     }
     cost = lr = rl = bt = nullptr;
+    dfree(tb);
     dfree(wta); dfree(post); dfree(post2); dfree(dr_out); dfree(out);
     dfree(init_tmp); dfree(key); dfree(label); dfree(count);
     if (stream) cudaStreamDestroy(stream);
@@ -503,7 +505,7 @@ int launch_cols3_pass(sgm_engine* e, int G, const sgm::PlainParams& P, const sgm
 using sgm::EncodeTiledFn;
 using sgm::encode_tiled;
 
-// Tensor map i (0 cost, 1 bt, 2 lr, 3 rl) of the engine's volumes, [nv][H][W * D] bytes, in boxes
+// Tensor map i (0 cost, 1 bt, 2 lr, 3 rl, 4 tb) of the engine's volumes, [nv][H][W * D] bytes, in boxes
 // of 32 rows x D bytes with the D-byte swizzle (k_vscan_plain4); rebuilt when the volume moved.
 int volume_map(sgm_engine* e, int i, const uint8_t* base, int nv, const CUtensorMap** out) {
   sgm_engine::TmapKey& k = e->tmap_key[i];
@@ -546,6 +548,19 @@ int launch_rows4(sgm_engine* e, const sgm::PlainParams& P, int nv, cudaStream_t 
   } else {
     return SGM_ERR_UNSUPPORTED;
   }
+}
+
+// The top-to-bottom volume of the warp-per-scanline column kernels, allocated on first use (a
+// direct run: never inside a graph capture of the matcher's own).
+int ensure_tb(sgm_engine* e, int nv) {
+  if (e->tb) return SGM_OK;
+  const cudaError_t r = dalloc(&e->tb, e->vol() * nv);
+  if (r != cudaSuccess) {
+    e->tb = nullptr;
+    set_error(&e->err, "device allocation of the top-to-bottom volume failed: %s", cudaGetErrorString(r));
+    return r == cudaErrorMemoryAllocation ? SGM_ERR_NOMEM : SGM_ERR_CUDA;
+  }
+  return SGM_OK;
 }
 
 template <int K, int PASS>
@@ -858,21 +873,34 @@ inline int init4_rows(sgm_engine* e, const int16_t* il, const int16_t* ir, const
                                              e->cost, il, ir, e->lr, e->rl, P, nv));
 }
 
+// PASS 1: bottom-to-top into bt; PASS 3: top-to-bottom into tb.
 template <int PASS>
-int init4_cols(sgm_engine* e, const int16_t* il, const int16_t* ir, float* wta, const sgm::InitParams& P,
-               const sgm::WtaParams& Q, cudaStream_t s) {
+int init4_cols(sgm_engine* e, const int16_t* il, const int16_t* ir, const sgm::InitParams& P, cudaStream_t s) {
   e->bt_stored = true;
   const int nv = e->nviews();
   const dim3 grid((unsigned)((e->W + kScan4ColWarps - 1) / kScan4ColWarps), nv);
-  const char* name = PASS == 1 ? "vpaths_bt_init" : "vpaths_wta_init";
-  const CUtensorMap *mc, *mb, *ml, *mr;
-  int st = volume_map(e, 0, e->cost, nv, &mc);
-  if (!st) st = volume_map(e, 1, e->bt, nv, &mb);
-  if (!st) st = volume_map(e, 2, e->lr, nv, &ml);
-  if (!st) st = volume_map(e, 3, e->rl, nv, &mr);
+  int st = PASS == 3 ? ensure_tb(e, nv) : SGM_OK;
+  uint8_t* out = PASS == 1 ? e->bt : e->tb;
+  const CUtensorMap *mc, *mo;
+  if (!st) st = volume_map(e, 0, e->cost, nv, &mc);
+  if (!st) st = volume_map(e, PASS == 1 ? 1 : 4, out, nv, &mo);
   if (st) return st;
-  return SGM_LAUNCH(e, s, name, sgm::k_vscan_init4<kScan4ColWarps, PASS><<<grid, 32 * kScan4ColWarps, 0, s>>>(
-                                    *mc, *mb, *ml, *mr, il, ir, e->bt, wta, P, Q));
+  return SGM_LAUNCH(e, s, PASS == 1 ? "vpaths_bt_init" : "vpaths_tb_init",
+                    sgm::k_vscan_init4<kScan4ColWarps, PASS><<<grid, 32 * kScan4ColWarps, 0, s>>>(
+                        *mc, *mo, il, ir, out, P));
+}
+
+inline int init4_cols_both(sgm_engine* e, const int16_t* il, const int16_t* ir, const sgm::InitParams& P,
+                           cudaStream_t s) {
+  const int st = init4_cols<1>(e, il, ir, P, s);
+  return st ? st : init4_cols<3>(e, il, ir, P, s);
+}
+
+inline int init4_wta(sgm_engine* e, const int16_t* il, const int16_t* ir, float* wta, const sgm::InitParams& P,
+                     const sgm::WtaParams& Q, cudaStream_t s) {
+  const dim3 grid((e->W + 127) / 128, e->H, e->nviews());
+  return SGM_LAUNCH(e, s, "wta_init",
+                    sgm::k_wta_init4<<<grid, 128, 0, s>>>(e->bt, e->tb, e->lr, e->rl, il, ir, wta, P, Q));
 }
 
 template <typename Word>
@@ -901,14 +929,14 @@ int launch_init(sgm_engine* e, const Word* csl, const Word* csr, const int16_t* 
   // rows reading the cost volume (variants 3 and 4) and columns split into two passes
   auto rows_cv = [&](cudaStream_t ms) { return rows4 ? init4_rows(e, il, ir, P, ms) : init3_rows(e, il, ir, P, ms); };
   auto cols_bt = [&](cudaStream_t ss) {
-    return cols4 ? init4_cols<1>(e, il, ir, wta, P, Q3, ss) : init3_cols<1>(e, il, ir, wta, P, Q3, ss);
+    return cols4 ? init4_cols_both(e, il, ir, P, ss) : init3_cols<1>(e, il, ir, wta, P, Q3, ss);
   };
   int st;
   if ((rows3 || rows4) && (cols3 || cols4) && kSplitColumns) {  // bottom-to-top pass beside the row scans
     st = init3_cost<Word>(e, csl, csr, il, ir, P, e->stream);
     if (!st) st = fork_join(e, e->stream, cols_bt, rows_cv);
     if (st) return st;
-    return cols4 ? init4_cols<2>(e, il, ir, wta, P, Q3, e->stream) : init3_cols<2>(e, il, ir, wta, P, Q3, e->stream);
+    return cols4 ? init4_wta(e, il, ir, wta, P, Q3, e->stream) : init3_cols<2>(e, il, ir, wta, P, Q3, e->stream);
   }
   if (rows3 || rows4) {
     st = init3_cost<Word>(e, csl, csr, il, ir, P, e->stream);
@@ -952,8 +980,8 @@ int launch_init(sgm_engine* e, const Word* csl, const Word* csr, const int16_t* 
   size_t vsmem = 0;
   if (cols3) return init3_cols<0>(e, il, ir, wta, P, Q3, e->stream);
   if (cols4) {
-    st = init4_cols<1>(e, il, ir, wta, P, Q3, e->stream);
-    return st ? st : init4_cols<2>(e, il, ir, wta, P, Q3, e->stream);
+    st = init4_cols_both(e, il, ir, P, e->stream);
+    return st ? st : init4_wta(e, il, ir, wta, P, Q3, e->stream);
   }
   if (e->tune_col_kernel != 2) {
     C = e->tune_cols > 0 ? e->tune_cols : 8;

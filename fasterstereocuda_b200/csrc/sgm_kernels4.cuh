@@ -103,60 +103,6 @@ __device__ __forceinline__ void scan_step_fast(uint32_t& L, uint32_t c, int s, u
   L = c + t - m;
 }
 
-// WTA of one pixel of an initial-disparity level from its four stored path rows (32 bytes each;
-// S(d) = sum of the four), computed by one lane: Kernel_ComputeDisparityByWTA for initial
-// disparities (cusgm_ca.cu:3425-3512). d* <= 1 or d* >= 31 -> INVALID; uniqueness and the
-// +0.5-shifted parabola as in wta_pixel; tie rules: kTieRefB200 the lowest tied d whose candidate
-// is valid (every tied lane stores its own result there, a valid one wins), 1 / 2 the highest tied
-// d, 0 / 3 the lowest (one disparity per lane: lane order is disparity order).
-// a, b, c, e: the pixel's rows in four swizzled boxes (16-byte unit u of the row at u ^ sw).
-__device__ __forceinline__ float init_wta_serial(const uint8_t* a, const uint8_t* b, const uint8_t* c,
-                                                 const uint8_t* e, int sw, int base, const WtaParams& Q) {
-  constexpr int D = kLevelRange;
-  uint32_t S[D];
-#pragma unroll
-  for (int k = 0; k < D / 4; ++k) {
-    const int wk = (((k >> 2) ^ sw) << 2) | (k & 3);  // the word's place in the swizzled row
-    const uint32_t wa = reinterpret_cast<const uint32_t*>(a)[wk], wb = reinterpret_cast<const uint32_t*>(b)[wk];
-    const uint32_t wc = reinterpret_cast<const uint32_t*>(c)[wk], we = reinterpret_cast<const uint32_t*>(e)[wk];
-#pragma unroll
-    for (int q = 0; q < 4; ++q)
-      S[4 * k + q] = ((wa >> (8 * q)) & 0xFFu) + ((wb >> (8 * q)) & 0xFFu) + ((wc >> (8 * q)) & 0xFFu) +
-                     ((we >> (8 * q)) & 0xFFu);
-  }
-  uint32_t m = S[0];
-#pragma unroll
-  for (int d = 1; d < D; ++d) m = min(m, S[d]);
-  const float ut = __fsub_rn(1.0f, Q.uniqueness);
-  // S at a runtime d, summed again from the rows (S[] stays in registers, indexed statically)
-  auto sum_at = [&](int d) {
-    const int o = d ^ (sw << 4);
-    return (uint32_t)a[o] + b[o] + c[o] + e[o];
-  };
-  auto candidate = [&](int d) {
-    if (d <= 1 || d >= Q.dmax_excl) return kInvalidFloat;
-    const float c1 = (float)sum_at(d - 1), c2 = (float)m, c3 = (float)sum_at(d + 1);
-    const float d12 = __fsub_rn(c1, c2), d32 = __fsub_rn(c3, c2);
-    const float uq = d12 < d32 ? d12 : d32;
-    if (uq <= __fmul_rn(c2, ut)) return kInvalidFloat;
-    return __fadd_rn((float)(d + base), subpix_bias(c1, c2, c3));
-  };
-  uint32_t tied = 0;
-#pragma unroll
-  for (int d = 0; d < D; ++d) tied |= (S[d] == m ? 1u : 0u) << d;
-  if (Q.tie_rule == kTieRefB200) {
-    while (tied) {
-      const int d = __ffs(tied) - 1;
-      const float v = candidate(d);
-      if (v != kInvalidFloat) return v;
-      tied &= tied - 1u;
-    }
-    return kInvalidFloat;
-  }
-  const bool high = Q.tie_rule == kTieHighest || Q.tie_rule == kTieLaneHigh;
-  return candidate(high ? 31 - __clz(tied) : __ffs(tied) - 1);
-}
-
 // ---------------------------------------------------------------------------------------------
 // Horizontal scans: warp w of the grid owns scanline i = (view, dir, y) as in hpaths3_lane. A
 // chunk is 32 consecutive pixels of the row, one contiguous bulk copy (double-buffered); its
@@ -282,25 +228,26 @@ __global__ void __launch_bounds__(32 * WPB) k_hscan_init4(const uint8_t* __restr
 }
 
 // ---------------------------------------------------------------------------------------------
-// Vertical scans: warp (blockIdx.x * WPB + w) owns column x of view blockIdx.y. PASS 1: bottom to
-// top, storing its path costs. PASS 2: top to bottom with the 4-path sum and the WTA of an
-// initial-disparity level (as vpaths3_init_lane / k_vpaths_wta_init). Both start last_base from
-// row 0's base (cusgm_ca.cu:1291); the first pixel of a vertical path does not set it.
-// Chunks are swizzled tensor-map boxes of 32 rows x 32 bytes, as in k_vscan_plain4: PASS 1 boxes
-// end at rows H - 32c (the last one starts above row 0 and reads zeros there; its steps past row
-// 0 are marked skipped), PASS 2 boxes start at rows 32c. A step's path costs overwrite its costs
-// in the box; PASS 1 stores the box (the last one row by row), PASS 2 runs the WTA on it.
+// Vertical scans: warp (blockIdx.x * WPB + w) owns column x of view blockIdx.y and stores its path
+// costs: PASS 1 bottom to top (bt), PASS 3 top to bottom (tb); the WTA follows in k_wta_init4, so
+// both passes can run beside the row scans. Both start last_base from row 0's base
+// (cusgm_ca.cu:1291); the first pixel of a vertical path does not set it. Chunks are swizzled
+// tensor-map boxes of 32 rows x 32 bytes, as in k_vscan_plain4: PASS 1 boxes end at rows H - 32c
+// (the last one starts above row 0 and reads zeros there; its steps past row 0 are marked
+// skipped), PASS 3 boxes start at rows 32c. A step's path costs overwrite its costs in the box,
+// which then leaves with one tensor store (a box that reaches past the column, row by row).
 // ---------------------------------------------------------------------------------------------
+// m_out / out: the volume the pass stores (bt or tb) as a tensor map and as a pointer.
 template <int WPB, int PASS>
 __global__ void __launch_bounds__(32 * WPB)
-    k_vscan_init4(const __grid_constant__ CUtensorMap m_cost, const __grid_constant__ CUtensorMap m_bt,
-                  const __grid_constant__ CUtensorMap m_lr, const __grid_constant__ CUtensorMap m_rl,
-                  const int16_t* __restrict__ init_l, const int16_t* __restrict__ init_r, uint8_t* __restrict__ bt,
-                  float* __restrict__ disp, InitParams P, WtaParams Q) {
+    k_vscan_init4(const __grid_constant__ CUtensorMap m_cost, const __grid_constant__ CUtensorMap m_out,
+                  const int16_t* __restrict__ init_l, const int16_t* __restrict__ init_r, uint8_t* __restrict__ out,
+                  InitParams P) {
+  static_assert(PASS == 1 || PASS == 3, "bottom-to-top or top-to-bottom");
   constexpr int D = kLevelRange, C = kScanChunk, BOX = C * D;
-  constexpr int NV = PASS == 2 ? 4 : 1;  // boxes a chunk needs: cost (+ bottom->top, L->R, R->L)
-  constexpr int NB = PASS == 1 ? 3 : 2;  // chunks in flight
-  __shared__ __align__(1024) uint8_t cbuf[WPB][NB][NV][BOX];
+  constexpr int NB = 3;  // chunks in flight
+  constexpr bool kUp = PASS == 1;
+  __shared__ __align__(1024) uint8_t cbuf[WPB][NB][BOX];
   __shared__ __align__(8) uint64_t bars[WPB][NB];
   __shared__ __align__(16) uint32_t par[WPB][2][C];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -312,32 +259,21 @@ __global__ void __launch_bounds__(32 * WPB)
   const int W = P.W, H = P.H;
   const int x = blockIdx.x * WPB + w;
   const int view = blockIdx.y;
-  if (x >= W) return;  // the whole warp
-  float* dout = disp + (size_t)view * Q.dstride + x;
-  if (x < P.x0) {
-    if (PASS == 2)
-      for (int y = lane; y < H; y += 32) dout[(size_t)y * W] = kInvalidFloat;
-    return;
-  }
+  if (x >= W || x < P.x0) return;  // the whole warp
   // the swizzle pattern is a function of the shared address: the boxes must start on 1 KB
-  if (smem_u32(&cbuf[0][0][0][0]) & 1023u) {
+  if (smem_u32(&cbuf[0][0][0]) & 1023u) {
     if (lane == 0) atomicAdd(&g_scan_wait_timeouts, 1u);
     return;
   }
   const int16_t* ib = (view == 0 ? init_l : init_r) + x;
   const int nch = (H + C - 1) / C;
   auto chunk_n = [&](int c) { return min(C, H - c * C); };
-  auto row_of = [&](int s) { return PASS == 1 ? H - 1 - s : s; };
-  auto box_y = [&](int c) { return PASS == 1 ? H - C * (c + 1) : C * c; };  // first row of chunk c's box
+  auto row_of = [&](int s) { return kUp ? H - 1 - s : s; };
+  auto box_y = [&](int c) { return kUp ? H - C * (c + 1) : C * c; };  // first row of chunk c's box
   auto issue = [&](int c) {  // lane 0
     const int b = c % NB;
-    mbar_expect_tx(&bars[w][b], NV * BOX);
-    tma_load_3d(cbuf[w][b][0], &m_cost, x * D, box_y(c), view, &bars[w][b]);
-    if (PASS == 2) {
-      tma_load_3d(cbuf[w][b][1], &m_bt, x * D, box_y(c), view, &bars[w][b]);
-      tma_load_3d(cbuf[w][b][2], &m_lr, x * D, box_y(c), view, &bars[w][b]);
-      tma_load_3d(cbuf[w][b][3], &m_rl, x * D, box_y(c), view, &bars[w][b]);
-    }
+    mbar_expect_tx(&bars[w][b], BOX);
+    tma_load_3d(cbuf[w][b], &m_cost, x * D, box_y(c), view, &bars[w][b]);
   };
   auto base_of = [&](int c) {
     const int n = chunk_n(c);
@@ -351,7 +287,6 @@ __global__ void __launch_bounds__(32 * WPB)
   ChunkState st{(int)ib[0], false};  // row 0's base
   int bnext = base_of(0);
   uint32_t L = 0;
-  const bool col_ok = x >= Q.xlo && x <= Q.xhi;
   const int lo0 = lane, lo1 = lane ^ 16;  // this lane's byte of a box row under the two swizzles
   for (int c = 0; c < nch; ++c) {
     const int b = c % NB, n = chunk_n(c);
@@ -359,8 +294,7 @@ __global__ void __launch_bounds__(32 * WPB)
     if (c + 1 < nch) bnext = base_of(c + 1);
     uint32_t flags, p2;
     chunk_params(bcur, c * C, n, false, P, st, flags, p2);
-    // flags in the low 16 bits, the step's base in the high 16 (the WTA needs it, PASS 2)
-    par[w][0][lane] = flags | ((uint32_t)(uint16_t)(int16_t)bcur << 16);
+    par[w][0][lane] = flags;
     par[w][1][lane] = p2;
     if (!mbar_wait_warp(&bars[w][b], (phase >> b) & 1u)) {
       scan_give_up_mask(bars[w], phase, (1u << b) | (c + 1 < nch ? 1u << ((c + 1) % NB) : 0u));
@@ -369,10 +303,10 @@ __global__ void __launch_bounds__(32 * WPB)
     }
     phase ^= 1u << b;
     __syncwarp();
-    uint8_t* box = cbuf[w][b][0];
-    // step j: box row C - 1 - j (PASS 1) or j (PASS 2); this lane's byte of it
+    uint8_t* box = cbuf[w][b];
+    // step j: box row C - 1 - j (PASS 1) or j (PASS 3); this lane's byte of it
     auto at = [&](int j) {
-      const int r = PASS == 1 ? C - 1 - j : j;
+      const int r = kUp ? C - 1 - j : j;
       return box + r * D + (box_sw<D>(r) ? lo1 : lo0);
     };
     // the chunk's step parameters and this lane's costs in registers: the chain below touches no
@@ -391,49 +325,112 @@ __global__ void __launch_bounds__(32 * WPB)
       else scan_step(L, cvr[j], fl[j], pp[j], P.p1);
       *at(j) = (uint8_t)L;
     }
-    if constexpr (PASS == 1) {
-      fence_proxy_async();
-      __syncwarp();
-      const int y0 = box_y(c);
-      if (y0 >= 0) {
-        if (lane == 0) {
-          tma_store_3d(&m_bt, x * D, y0, view, box);
-          bulk_commit();
-        }
-      } else if (lane < C + y0) {  // the top box: rows 0 .. C + y0 - 1 of the column, one per lane
-        const int r = lane - y0;     // box row of image row `lane`
-        const uint4* src = reinterpret_cast<const uint4*>(box + r * D);
-        uint4* dst = reinterpret_cast<uint4*>(bt + (size_t)view * P.vstride + ((size_t)lane * W + x) * D);
-        const int sw = box_sw<D>(r);
+    fence_proxy_async();
+    __syncwarp();
+    const int y0 = box_y(c);
+    if (y0 >= 0 && y0 + C <= H) {
+      if (lane == 0) {
+        tma_store_3d(&m_out, x * D, y0, view, box);
+        bulk_commit();
+      }
+    } else {  // a box reaching past row 0 or row H - 1: its rows inside the column, one per lane
+      const int y = y0 + lane;
+      if (y >= 0 && y < H) {
+        const uint4* src = reinterpret_cast<const uint4*>(box + lane * D);
+        uint4* dst = reinterpret_cast<uint4*>(out + (size_t)view * P.vstride + ((size_t)y * W + x) * D);
+        const int sw = box_sw<D>(lane);
         const uint4 v0 = src[sw], v1 = src[sw ^ 1];
         dst[0] = v0;
         dst[1] = v1;
       }
-      if (lane == 0 && c + 2 < nch) {
-        bulk_wait_read<1>();  // the store of chunk c - 1 has left the box chunk c + 2 goes to
-        issue(c + 2);
-      }
-    } else {
-      __syncwarp();  // the chunk's path costs, written by disparity, are read by pixel
-      // the WTA of the chunk's pixels, lane j = pixel j (off the steps' dependency chain)
-      const int y = c * C + lane;
-      const int base = (int)(int16_t)(par[w][0][lane] >> 16);
-      const bool skipped = y > 0 && base == kInvalidShort;
-      if (lane < n) {
-        float dv = kInvalidFloat;
-        if (y >= Q.ylo && y <= Q.yhi && y < Q.rows && col_ok && !skipped && base != kInvalidShort) {
-          const int o = lane * D;
-          dv = init_wta_serial(box + o, cbuf[w][b][1] + o, cbuf[w][b][2] + o, cbuf[w][b][3] + o, box_sw<D>(lane),
-                               base, Q);
-        }
-        dout[(size_t)y * W] = dv;
-      }
-      fence_proxy_async();  // the reads of the boxes before the copies that refill them
-      __syncwarp();
-      if (lane == 0 && c + 2 < nch) issue(c + 2);
+    }
+    if (lane == 0 && c + 2 < nch) {
+      bulk_wait_read<1>();  // the store of chunk c - 1 has left the box chunk c + 2 goes to
+      issue(c + 2);
     }
   }
-  if (PASS == 1 && lane == 0) bulk_wait_all();
+  if (lane == 0) bulk_wait_all();
+}
+
+// WTA of one pixel of an initial-disparity level from its four stored path rows (32 bytes each,
+// in global memory; S(d) = sum of the four): Kernel_ComputeDisparityByWTA for initial disparities
+// (cusgm_ca.cu:3425-3512). d* <= 1 or d* >= 31 -> INVALID; uniqueness and the +0.5-shifted
+// parabola as in wta_pixel; tie rules: kTieRefB200 the lowest tied d whose candidate is valid
+// (every tied lane stores its own result there, a valid one wins), 1 / 2 the highest tied d, 0 / 3
+// the lowest (one disparity per lane: lane order is disparity order). A row is read as two 16-byte
+// words; S(d) is summed in 16-bit halves, its minimum taken by SIMD minima and the tied set kept as
+// a bit mask; S at a candidate's neighbours comes from single bytes.
+__device__ __forceinline__ float init_wta_rows(const uint8_t* a, const uint8_t* b, const uint8_t* c,
+                                               const uint8_t* e, int base, const WtaParams& Q) {
+  constexpr int D = kLevelRange;
+  uint32_t lo[D / 4], hi[D / 4];  // lo[k] = S(4k) | S(4k + 2) << 16, hi[k] = S(4k + 1) | S(4k + 3) << 16
+#pragma unroll
+  for (int q = 0; q < D / 16; ++q) {
+    const uint4 va = reinterpret_cast<const uint4*>(a)[q], vb = reinterpret_cast<const uint4*>(b)[q];
+    const uint4 vc = reinterpret_cast<const uint4*>(c)[q], ve = reinterpret_cast<const uint4*>(e)[q];
+    const uint32_t wa[4] = {va.x, va.y, va.z, va.w}, wb[4] = {vb.x, vb.y, vb.z, vb.w};
+    const uint32_t wc[4] = {vc.x, vc.y, vc.z, vc.w}, we[4] = {ve.x, ve.y, ve.z, ve.w};
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      lo[4 * q + t] = __byte_perm(wa[t], 0u, 0x4240u) + __byte_perm(wb[t], 0u, 0x4240u) +
+                      __byte_perm(wc[t], 0u, 0x4240u) + __byte_perm(we[t], 0u, 0x4240u);
+      hi[4 * q + t] = __byte_perm(wa[t], 0u, 0x4341u) + __byte_perm(wb[t], 0u, 0x4341u) +
+                      __byte_perm(wc[t], 0u, 0x4341u) + __byte_perm(we[t], 0u, 0x4341u);
+    }
+  }
+  uint32_t mm = __vminu2(lo[0], hi[0]);
+#pragma unroll
+  for (int k = 1; k < D / 4; ++k) mm = __vminu2(mm, __vminu2(lo[k], hi[k]));
+  const uint32_t m = min(mm & 0xFFFFu, mm >> 16), m2 = m * 0x10001u;
+  uint32_t tied = 0;  // bit d: S(d) == m
+#pragma unroll
+  for (int k = 0; k < D / 4; ++k) {
+    const uint32_t el = __vcmpeq2(lo[k], m2), eh = __vcmpeq2(hi[k], m2);
+    tied |= ((el & 1u) | ((eh & 1u) << 1) | ((el >> 14) & 4u) | ((eh >> 13) & 8u)) << (4 * k);
+  }
+  const float ut = __fsub_rn(1.0f, Q.uniqueness);
+  auto sum_at = [&](int d) { return (uint32_t)a[d] + b[d] + c[d] + e[d]; };
+  auto candidate = [&](int d) {
+    if (d <= 1 || d >= Q.dmax_excl) return kInvalidFloat;
+    const float c1 = (float)sum_at(d - 1), c2 = (float)m, c3 = (float)sum_at(d + 1);
+    const float d12 = __fsub_rn(c1, c2), d32 = __fsub_rn(c3, c2);
+    const float uq = d12 < d32 ? d12 : d32;
+    if (uq <= __fmul_rn(c2, ut)) return kInvalidFloat;
+    return __fadd_rn((float)(d + base), subpix_bias(c1, c2, c3));
+  };
+  if (Q.tie_rule == kTieRefB200) {
+    while (tied) {
+      const float v = candidate(__ffs(tied) - 1);
+      if (v != kInvalidFloat) return v;
+      tied &= tied - 1u;
+    }
+    return kInvalidFloat;
+  }
+  const bool high = Q.tie_rule == kTieHighest || Q.tie_rule == kTieLaneHigh;
+  return candidate(high ? 31 - __clz(tied) : __ffs(tied) - 1);
+}
+
+// WTA of an initial-disparity level, one thread per pixel, from the four stored path volumes:
+// INVALID left of x0, on the image border, in rows >= Q.rows and where the pixel's base is
+// INVALID.
+__global__ void __launch_bounds__(128) k_wta_init4(const uint8_t* __restrict__ bt, const uint8_t* __restrict__ tb,
+                                                   const uint8_t* __restrict__ lr, const uint8_t* __restrict__ rl,
+                                                   const int16_t* __restrict__ init_l,
+                                                   const int16_t* __restrict__ init_r, float* __restrict__ disp,
+                                                   InitParams P, WtaParams Q) {
+  constexpr int D = kLevelRange;
+  const int x = blockIdx.x * 128 + threadIdx.x, y = blockIdx.y, view = blockIdx.z;
+  const int W = P.W;
+  if (x >= W) return;
+  float dv = kInvalidFloat;
+  if (x >= P.x0 && x >= Q.xlo && x <= Q.xhi && y >= Q.ylo && y <= Q.yhi && y < Q.rows) {
+    const int base = (view == 0 ? init_l : init_r)[(size_t)y * W + x];
+    if (base != kInvalidShort) {
+      const size_t o = (size_t)view * P.vstride + ((size_t)y * W + x) * D;
+      dv = init_wta_rows(tb + o, bt + o, lr + o, rl + o, base, Q);
+    }
+  }
+  disp[(size_t)view * Q.dstride + (size_t)y * W + x] = dv;
 }
 
 }  // namespace sgm

@@ -111,8 +111,10 @@ typedef struct sgm_tuning_t {
   int32_t rows_per_cta; /* scanlines per CTA of the horizontal scans: 0 (default), 1, 2 or 4 */
   int32_t col_kernel;   /* vertical scans + WTA: 1 = one warp per column, plain loads, 2 = the same with
                            an 8-row prefetch ring, 3 = col_lanes lanes per column (u16x2 SIMD, WTA in
-                           the lanes), 4 = as row_kernel 4 (chunks of 32 rows as tensor-map boxes,
-                           the WTA per chunk with one lane per pixel); 0 (default) = 3
+                           the lanes), 4 = as row_kernel 4 (chunks of 32 rows as tensor-map boxes;
+                           at the 32-disparity levels both directions beside the row scans, then a
+                           WTA launch: the first such match allocates one more path volume, so it
+                           must not run inside a stream capture); 0 (default) = 3
                            where it is exact, else 1. Variant 3 is exact for D <= 128,
                            P1 <= P2 <= 16383 and tie rule 0 or 4 (else 2 / 1 run) */
   int32_t cols_per_cta; /* columns (one warp each) per CTA of the vertical scans: 0 (default) .. 8 */
