@@ -1255,7 +1255,7 @@ int engine_run(sgm_engine* e, const uint8_t* dl, const uint8_t* dr, float* dout,
 // The synchronous host API (the reference's Match) on a matcher left at the default tuning: while
 // at most kLatencyInFlight such calls run in the process -- one caller matching one frame at a
 // time, the reference's own use -- the match takes the warp-per-scanline kernels (variant 4, the
-// shortest step chains: a 1242x375x64 pyramid pair 0.37 instead of 1.46 ms alone); with more
+// shortest step chains: a 1242x375x64 pyramid pair 0.33 instead of 1.46 ms alone); with more
 // calls in flight it takes the default thread-per-scanline kernels, which give more pairs per
 // second when many pairs share the GPU (36 % more at 32 in flight). Both give the same bits.
 constexpr int kLatencyInFlight = 2;
