@@ -151,9 +151,9 @@ def alg_bytes(kernel, W, H, D, nviews, census_bytes):
     n = W * H
     if kernel.startswith("hpaths"):
         return nviews * (2 * V + 2 * census_bytes * n)
-    if kernel.startswith("vpaths_bt"):  # the bottom-to-top column pass launched on its own: no
-        return 0                          # counterpart in the minimal design's traffic
-    if kernel.startswith("vpaths"):
+    if kernel.startswith(("vpaths_bt", "vpaths_tb")):  # a column pass launched on its own that
+        return 0                                         # stores its paths: no counterpart
+    if kernel.startswith(("vpaths", "wta")):  # the pass that ends in the disparity
         return nviews * (2 * V + 4 * n)
     if kernel == "census":
         return 2 * n + 2 * census_bytes * n
@@ -171,8 +171,8 @@ def alg_bytes(kernel, W, H, D, nviews, census_bytes):
 NCU_DRAM_BYTES_PER_VOXEL = {
     "v3": {"hpaths_plain": 2.83, "vpaths_bt_plain": 1.25, "vpaths_wta_plain": 4.04, "hpaths_init": 1.07,
            "vpaths_wta_init": 3.29},
-    "v4": {"hpaths_plain": 2.76, "vpaths_bt_plain": 1.22, "vpaths_wta_plain": 4.05, "hpaths_init": 1.06,
-           "vpaths_bt_init": 1.06, "vpaths_wta_init": 4.08},
+    "v4": {"hpaths_plain": 2.76, "vpaths_bt_plain": 1.22, "vpaths_wta_plain": 4.04, "hpaths_init": 1.07,
+           "vpaths_bt_init": 1.06, "vpaths_tb_init": 1.06, "wta_init": 3.42},
 }
 
 
@@ -513,7 +513,7 @@ def run_ours(a, rank, world, local_rank):
     per_call_bytes, per_call_voxels = {}, {}
     for k in prof:
         mine = [(w, h, d, nv) for (kind, w, h, d, nv) in levels
-                if not k.startswith(("hpaths", "vpaths")) or k.endswith(kind)]
+                if not k.startswith(("hpaths", "vpaths", "wta")) or k.endswith(kind)]
         per_call_bytes[k] = sum(alg_bytes(k, w, h, d, nv, 8) for (w, h, d, nv) in mine)
         per_call_voxels[k] = sum(w * h * d * nv for (w, h, d, nv) in mine)
     # the dominant kernel among those with a counterpart in the minimal design (the bottom-to-top
