@@ -543,6 +543,7 @@ int launch_rows4(sgm_engine* e, const sgm::PlainParams& P, int nv, cudaStream_t 
   if constexpr (K <= 4) {
     constexpr int wpb = sgm::hscan_plain4_warps<K>();
     const int blocks = (nv * 2 * e->H + wpb - 1) / wpb;
+    SGM_CUDA_TRY(e, sgm::prefer_max_shared(sgm::k_hscan_plain4<K>));
     return SGM_LAUNCH(e, s, "hpaths_plain",
                       sgm::k_hscan_plain4<K><<<blocks, 32 * wpb, 0, s>>>(e->cost, e->lr, e->rl, P, nv));
   } else {
@@ -575,6 +576,7 @@ int launch_cols4(sgm_engine* e, const sgm::PlainParams& P, const sgm::WtaParams&
     if (!st) st = volume_map(e, 2, e->lr, nv, &ml);
     if (!st) st = volume_map(e, 3, e->rl, nv, &mr);
     if (st) return st;
+    SGM_CUDA_TRY(e, sgm::prefer_max_shared(sgm::k_vscan_plain4<K, PASS>));
     return SGM_LAUNCH(e, s, PASS == 1 ? "vpaths_bt_plain" : "vpaths_wta_plain",
                       sgm::k_vscan_plain4<K, PASS><<<grid, 32 * wpb, 0, s>>>(*mc, *mb, *ml, *mr, e->bt, wta, P, Q));
   } else {
@@ -869,6 +871,7 @@ inline int init4_rows(sgm_engine* e, const int16_t* il, const int16_t* ir, const
                       cudaStream_t s) {
   const int nv = e->nviews();
   const int blocks = (nv * 2 * e->H + kScan4RowWarps - 1) / kScan4RowWarps;
+  SGM_CUDA_TRY(e, sgm::prefer_max_shared(sgm::k_hscan_init4<kScan4RowWarps>));
   return SGM_LAUNCH(e, s, "hpaths_init", sgm::k_hscan_init4<kScan4RowWarps><<<blocks, 32 * kScan4RowWarps, 0, s>>>(
                                              e->cost, il, ir, e->lr, e->rl, P, nv));
 }
@@ -885,6 +888,7 @@ int init4_cols(sgm_engine* e, const int16_t* il, const int16_t* ir, const sgm::I
   if (!st) st = volume_map(e, 0, e->cost, nv, &mc);
   if (!st) st = volume_map(e, PASS == 1 ? 1 : 4, out, nv, &mo);
   if (st) return st;
+  SGM_CUDA_TRY(e, sgm::prefer_max_shared(sgm::k_vscan_init4<kScan4ColWarps, PASS>));
   return SGM_LAUNCH(e, s, PASS == 1 ? "vpaths_bt_init" : "vpaths_tb_init",
                     sgm::k_vscan_init4<kScan4ColWarps, PASS><<<grid, 32 * kScan4ColWarps, 0, s>>>(
                         *mc, *mo, il, ir, out, P));
