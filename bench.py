@@ -841,45 +841,59 @@ def extra_float_sgm(B=4):
 
 
 def extra_large_pyramid():
-    """4800x3409, disparities 0..256, 4-level pyramid, census 9x7, P1=10, P2=150 (fractal scene):
-    device time per pair and the matcher's device memory."""
+    """4800x3409, disparities 0..256, 4-level pyramid, census 9x7, P1=10, P2=150 (fractal scene), one
+    pair alone: device time per pair and device memory, with the warp-per-scanline (latency)
+    kernels -- what a single caller of the host API gets -- and with the default kernels."""
     import torch
     import fasterstereocuda_b200 as fsc
     from fasterstereocuda_b200 import scenes
     from cuda.bindings import runtime as rt
     W, H = 4800, 3409
     L, R, _ = scenes.building_like(2, W, H)
-    torch.cuda.synchronize()
-    free0 = rt.cudaMemGetInfo()[1]
-    p = fsc.FasterStereoCuda()
-    if not p.Init(fsc.StereoOption1(width=W, height=H, min_disp=0, max_disp=256, num_layers=4),
-                  fsc.LevelOverride(1, 10, 150), fsc.ExtOptions()):
-        raise RuntimeError(p.last_error())
-    torch.cuda.synchronize()
-    used = free0 - rt.cudaMemGetInfo()[1]
     dl, dr = torch.from_numpy(L).cuda(), torch.from_numpy(R).cuda()
     out = torch.empty((H, W), dtype=torch.float32, device="cuda")
-    s = torch.cuda.Stream()
-    for _ in range(2):
-        p.match_device(dl, dr, out, s.cuda_stream)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    n = 5
-    e0.record(s)
-    for _ in range(n):
-        if not p.match_device(dl, dr, out, s.cuda_stream):
+
+    def run(tuning):
+        torch.cuda.synchronize()
+        free0 = rt.cudaMemGetInfo()[1]
+        p = fsc.FasterStereoCuda()
+        if not p.Init(fsc.StereoOption1(width=W, height=H, min_disp=0, max_disp=256, num_layers=4),
+                      fsc.LevelOverride(1, 10, 150), fsc.ExtOptions()):
             raise RuntimeError(p.last_error())
-    e1.record(s)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / n
-    peak = free0 - rt.cudaMemGetInfo()[1]  # no allocation happens while matching
+        if tuning and not p.set_tuning(fsc.Tuning(*tuning)):
+            raise RuntimeError(p.last_error())
+        torch.cuda.synchronize()
+        used = free0 - rt.cudaMemGetInfo()[1]
+        s = torch.cuda.Stream()
+        for _ in range(2):
+            p.match_device(dl, dr, out, s.cuda_stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        n = 5
+        e0.record(s)
+        for _ in range(n):
+            if not p.match_device(dl, dr, out, s.cuda_stream):
+                raise RuntimeError(p.last_error())
+        e1.record(s)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / n
+        peak = free0 - rt.cudaMemGetInfo()[1]  # after the first matches (the latency kernels' extra volume)
+        levels = [p.level_info(i) for i in range(4)]
+        p.Release()
+        torch.cuda.synchronize()
+        return ms, used, peak, levels
+
+    ms, used, peak, levels = run((4, 0, 4, 0, 0, 8, 8))
+    ms_d, used_d, peak_d, _ = run(None)
     # algorithmic bytes of a pair: 4*W*H*D + 6*W*H per view and level (the two-pass design's cost
     # and path traffic plus images and maps); the coarsest level matches both views (LR check)
-    levels = [p.level_info(i) for i in range(4)]
     alg = sum((2 if i == len(levels) - 1 else 1) * (4 * w * h * d + 6 * w * h) for i, (w, h, _, d) in enumerate(levels))
     hbm, src = peaks()
-    return {"workload": "4800x3409, D=256, 4-level pyramid, census 9x7, P1=10 P2=150, fractal scene",
-            "ms_per_pair": ms, "pairs_per_s": 1e3 / ms, "matcher_device_gib": used / 2**30,
-            "peak_device_gib": (peak + dl.numel() * 2 + out.numel() * 4) / 2**30,
+    extra = (dl.numel() * 2 + out.numel() * 4) / 2**30
+    return {"workload": "4800x3409, D=256, 4-level pyramid, census 9x7, P1=10 P2=150, fractal scene, one pair alone",
+            "ms_per_pair": ms, "pairs_per_s": 1e3 / ms, "kernels": "warp per scanline (row_kernel = col_kernel = 4)",
+            "matcher_device_gib": used / 2**30, "peak_device_gib": peak / 2**30 + extra,
+            "default_kernels": {"ms_per_pair": ms_d, "matcher_device_gib": used_d / 2**30,
+                                "peak_device_gib": peak_d / 2**30 + extra},
             "roofline": {"bound": "hbm", "alg_bytes_per_pair": alg, "achieved_gbs": alg / (ms * 1e6), "peak_gbs": hbm,
                          "frac": alg / (ms * 1e6) / hbm, "peak_source": src},
             "levels": levels}
