@@ -59,11 +59,12 @@ __device__ __forceinline__ bool mbar_wait_warp(uint64_t* bar, uint32_t parity) {
   return __all_sync(0xFFFFFFFFu, mbar_wait(bar, parity));
 }
 // A wait that ran out: record it, then wait (again bounded) for the copies still in flight into
-// this warp's buffers before the warp leaves.
-// phase: bit b = the parity of the phase buffer b waits for next.
-__device__ __forceinline__ void scan_give_up(uint64_t* bars, uint32_t phase, int nbars) {
+// this warp's buffers -- those whose bit is set in `pending` (bit b: bars[b]; phase bit b: the
+// parity bars[b] waits for next) -- before the warp leaves.
+__device__ __forceinline__ void scan_give_up_mask(uint64_t* bars, uint32_t phase, uint32_t pending) {
   if ((threadIdx.x & 31) == 0) atomicAdd(&g_scan_wait_timeouts, 1u);
-  for (int b = 0; b < nbars; ++b) mbar_wait(bars + b, (phase >> b) & 1u);
+  for (int b = 0; b < 32; ++b)
+    if ((pending >> b) & 1u) mbar_wait(bars + b, (phase >> b) & 1u);
 }
 
 // `bytes` (a multiple of 16) from shared src to global dst (both 16-byte aligned), in the calling
@@ -82,12 +83,6 @@ __device__ __forceinline__ void bulk_wait_read() {
 // All of this thread's bulk groups are complete.
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
-// As scan_give_up, for the buffers whose bit is set in `pending` only.
-__device__ __forceinline__ void scan_give_up_mask(uint64_t* bars, uint32_t phase, uint32_t pending) {
-  if ((threadIdx.x & 31) == 0) atomicAdd(&g_scan_wait_timeouts, 1u);
-  for (int b = 0; b < 32; ++b)
-    if ((pending >> b) & 1u) mbar_wait(bars + b, (phase >> b) & 1u);
-}
 
 // Column chunks are boxes of 32 rows x D bytes of one view's volume, copied by the tensor-memory
 // accelerator (a 3D tensor map: bytes of a row, rows, views) with the 32/64/128-byte swizzle: the
