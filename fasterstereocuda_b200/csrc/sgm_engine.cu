@@ -220,7 +220,8 @@ struct sgm_engine {
   cudaGraphExec_t gexec[2] = {};
   int direct_runs[2] = {};
   int64_t graph_launches[2] = {};
-  cudaEvent_t done = nullptr;  // blocking-sync event of the synchronous host API
+  // events of the synchronous host API: `done` blocking-sync, `done_poll` polled (see wait_stream)
+  cudaEvent_t done = nullptr, done_poll = nullptr;
   // Stages of a match: an NVTX range each, and with print_log a CUDA event at every stage boundary
   // for the per-stage report of the synchronous host API.
   static constexpr int kMaxStages = 10;
@@ -249,7 +250,8 @@ struct sgm_engine {
   void free_all() {
     drop_graph();
     if (done) cudaEventDestroy(done);
-    done = nullptr;
+    if (done_poll) cudaEventDestroy(done_poll);
+    done = done_poll = nullptr;
     for (auto& ev : stage_ev) {
       if (ev) cudaEventDestroy(ev);
       ev = nullptr;
@@ -281,16 +283,24 @@ struct sgm_engine {
 
 namespace {
 
-// Waits for everything enqueued on s so far without spinning a CPU core (a blocking-sync event):
-// callers that run many matchers from many host threads keep their cores for the other threads.
-// `ev` is the matcher's own event, created on first use on its device.
-cudaError_t wait_stream(cudaStream_t s, cudaEvent_t* ev) {
-  if (!*ev) {
-    const cudaError_t st = cudaEventCreateWithFlags(ev, cudaEventBlockingSync | cudaEventDisableTiming);
+// Waits for everything enqueued on s so far. poll = false: on a blocking-sync event, without
+// spinning a CPU core -- callers that run many matchers from many host threads keep their cores
+// for the other threads. poll = true: by polling an ordinary event, which returns as soon as the
+// work is done instead of after the sleeping thread is woken (about 0.2 ms per call for one caller
+// matching 1242x375 frames from page-locked buffers, whose copies do not block the thread).
+// `ev` / `ev_poll` are the matcher's own events, created on first use.
+cudaError_t wait_stream(cudaStream_t s, cudaEvent_t* ev, cudaEvent_t* ev_poll, bool poll) {
+  cudaEvent_t* e = poll ? ev_poll : ev;
+  if (!*e) {
+    const unsigned flags = poll ? cudaEventDisableTiming : cudaEventBlockingSync | cudaEventDisableTiming;
+    const cudaError_t st = cudaEventCreateWithFlags(e, flags);
     if (st != cudaSuccess) return st;
   }
-  const cudaError_t st = cudaEventRecord(*ev, s);
-  return st != cudaSuccess ? st : cudaEventSynchronize(*ev);
+  cudaError_t st = cudaEventRecord(*e, s);
+  if (st != cudaSuccess || !poll) return st != cudaSuccess ? st : cudaEventSynchronize(*e);
+  while ((st = cudaEventQuery(*e)) == cudaErrorNotReady) {
+  }
+  return st;
 }
 
 // Starts stage `name` of the match being enqueued (ends the previous one); name == nullptr ends
@@ -589,8 +599,14 @@ int launch_cols4(sgm_engine* e, const sgm::PlainParams& P, const sgm::WtaParams&
 // the join. In a captured graph the side stream joins the capture through ev_fork.
 constexpr bool kSplitColumns = true;
 
+// With per-kernel profiling on, both run on s one after the other, so that every launch is timed
+// alone.
 template <typename SideWork, typename MainWork>
 int fork_join(sgm_engine* e, cudaStream_t s, SideWork side_work, MainWork main_work) {
+  if (g_prof.on) {
+    const int st = side_work(s);
+    return st ? st : main_work(s);
+  }
   SGM_CUDA_TRY(e, cudaEventRecord(e->ev_fork, s));
   SGM_CUDA_TRY(e, cudaStreamWaitEvent(e->side, e->ev_fork, 0));
   int st = side_work(e->side);
@@ -1256,14 +1272,23 @@ int engine_run(sgm_engine* e, const uint8_t* dl, const uint8_t* dr, float* dout,
   return SGM_OK;
 }
 
-// The synchronous host API (the reference's Match) on a matcher left at the default tuning: while
-// at most kLatencyInFlight such calls run in the process -- one caller matching one frame at a
-// time, the reference's own use -- the match takes the warp-per-scanline kernels (variant 4, the
-// shortest step chains: a 1242x375x64 pyramid pair 0.33 instead of 1.46 ms alone); with more
-// calls in flight it takes the default thread-per-scanline kernels, which give more pairs per
-// second when many pairs share the GPU (36 % more at 32 in flight). Both give the same bits.
-constexpr int kLatencyInFlight = 2;
+// The synchronous host API (the reference's Match) adapts to the number of such calls in flight in
+// the process when the call starts (measured with page-locked buffers at 1242x375x64 on one B200):
+//  * kernels, on a matcher left at the default tuning: up to kLatencyInFlight calls take the
+//    warp-per-scanline kernels (variant 4, the shortest step chains: a pyramid pair 0.33 instead of
+//    1.46 ms alone), more take the default thread-per-scanline kernels, which give more pairs per
+//    second once many pairs share the GPU (16 callers: 7.4 k plain pairs/s against 6.0 k). Both
+//    give the same bits;
+//  * completion: up to one call per host core polls its completion event, more sleep on a
+//    blocking-sync event and leave the cores to the other callers (one caller: 3.3 k plain pairs/s
+//    polling, 2.0 k sleeping; 32 callers on 16 cores: 6.9 k pyramid pairs/s sleeping, 5.8 k polling).
+constexpr int kLatencyInFlight = 8;
 std::atomic<int> g_host_in_flight{0};
+
+int poll_in_flight() {
+  static const int n = std::max(1, (int)std::thread::hardware_concurrency());
+  return n;
+}
 
 struct HostCall {
   int n;
@@ -1272,6 +1297,7 @@ struct HostCall {
   HostCall(const HostCall&) = delete;
   HostCall& operator=(const HostCall&) = delete;
   bool latency() const { return n <= kLatencyInFlight; }
+  bool poll() const { return n <= poll_in_flight(); }
 };
 
 // Row and column kernels set to variant 4 on the given engines for the scope of one match, when
@@ -1327,7 +1353,8 @@ struct sgm_pyramid {
   cudaGraphExec_t gexec[2] = {};
   int direct_runs[2] = {};
   int64_t graph_launches[2] = {};  // kernels inside the graph
-  cudaEvent_t done = nullptr;  // blocking-sync event of the synchronous host API
+  // events of the synchronous host API: `done` blocking-sync, `done_poll` polled (see wait_stream)
+  cudaEvent_t done = nullptr, done_poll = nullptr;
 
   void drop_graph() {
     for (int k = 0; k < 2; ++k) {
@@ -1340,7 +1367,8 @@ struct sgm_pyramid {
   void free_all() {
     drop_graph();
     if (done) cudaEventDestroy(done);
-    done = nullptr;
+    if (done_poll) cudaEventDestroy(done_poll);
+    done = done_poll = nullptr;
     if (disp0) sgm_dev_free(disp0);
     disp0 = nullptr;
     depth_mode = false;
@@ -1588,7 +1616,7 @@ int sgm_match(sgm_handle_t h, const uint8_t* img_left, const uint8_t* img_right,
   if (disp_right && h->opt.do_lr_check)
     SGM_CUDA_TRY(h, cudaMemcpyAsync(disp_right, h->dr_out, N * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
   if (h->stage_timing) stage_mark(h, nullptr);
-  SGM_CUDA_TRY(h, wait_stream(h->stream, &h->done));
+  SGM_CUDA_TRY(h, wait_stream(h->stream, &h->done, &h->done_poll, call.poll()));
   if (disp_right && !h->opt.do_lr_check)
     for (size_t i = 0; i < N; ++i) disp_right[i] = sgm::kInvalidFloat;
   if (h->stage_timing) {
@@ -1654,7 +1682,7 @@ int sgm_match2(sgm_handle_t h, const uint8_t* img_left, const uint8_t* img_right
   if (!st) st = enqueue_depth(h, h->depth_src, h->post, h->cam, h->stream);
   if (st) return st;
   SGM_CUDA_TRY(h, cudaMemcpyAsync(depth_left, h->post, N * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
-  SGM_CUDA_TRY(h, wait_stream(h->stream, &h->done));
+  SGM_CUDA_TRY(h, wait_stream(h->stream, &h->done, &h->done_poll, call.poll()));
   return SGM_OK;
 }
 
@@ -1900,7 +1928,7 @@ int sgm_pyr_match(sgm_pyr_handle_t h, const uint8_t* img_left, const uint8_t* im
   int st = pyr_run(h, h->in_l, h->in_r, h->out, h->stream, km.mode());
   if (st) return st;
   if (cudaMemcpyAsync(disp, h->out, N * sizeof(float), cudaMemcpyDeviceToHost, h->stream)) return SGM_ERR_CUDA;
-  if (wait_stream(h->stream, &h->done) != cudaSuccess) {
+  if (wait_stream(h->stream, &h->done, &h->done_poll, call.poll()) != cudaSuccess) {
     set_error(&h->err, "pyramid match failed: %s", cudaGetErrorString(cudaGetLastError()));
     return SGM_ERR_CUDA;
   }

@@ -97,8 +97,10 @@ SGM_API int sgm_get_ext_options(sgm_handle_t h, sgm_ext_options_t* ext);
 /* No counterpart in the reference. Kernel variants and launch shapes; results do not depend on
  * them (every variant is bit-exact), only speed does. 0 everywhere = defaults; a matcher left at
  * the defaults runs, in the synchronous host API (sgm_match, sgm_match2, sgm_pyr_match,
- * sgm_pyr_match2), row_kernel = col_kernel = 4 while at most two such calls are in flight in the
- * process (one caller matching one frame at a time) and the defaults below otherwise. */
+ * sgm_pyr_match2), row_kernel = col_kernel = 4 while at most eight such calls are in flight in
+ * the process (a few callers matching one frame at a time) and the defaults below otherwise.
+ * Those calls wait for their results by polling while at most one call per host core is in
+ * flight, and sleep on a blocking-sync event beyond that. */
 typedef struct sgm_tuning_t {
   int32_t row_kernel;   /* horizontal scans: 1 = whole census rows in shared memory,
                            2 = census window and 32-pixel cost chunks in shared memory,
@@ -200,7 +202,10 @@ SGM_API int sgm_debug_reset_wait_timeouts(void);
 SGM_API int64_t sgm_debug_live_device_allocations(void);
 
 /* No counterpart in the reference: per-kernel timing with CUDA events recorded on the launching
- * stream around every launch of every handle in the process. Enabling resets the counters. */
+ * stream around every launch of every handle in the process. Enabling resets the counters. While
+ * it is on, matches run their kernels directly (no graph) and one after another on their stream
+ * (the column pass that otherwise overlaps the row scans on a second stream waits for them), so
+ * that each launch is timed alone. */
 SGM_API int sgm_profile_enable(int32_t enable);
 /* Writes {"kernel": {"launches": n, "ms": total}, ...} into buf; returns 0, or the size needed
  * (including the terminating NUL) when cap is too small. Synchronises on the recorded events. */

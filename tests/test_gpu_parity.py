@@ -324,8 +324,9 @@ def test_pyramid_parity(engine_lib, oracle_mod, override, size, layers, kernels)
 
 def test_host_api_kernel_modes_under_concurrency(engine_lib, oracle_mod):
     """Default-tuned matchers called through the synchronous host API by one thread (the latency
-    kernels) and by six threads at once (the throughput kernels while more than two calls are in
-    flight): every match -- direct runs, captures and replays of both graphs -- equals the oracle."""
+    kernels, polled completion) and by twelve threads at once (the throughput kernels while more
+    than eight calls are in flight; sleeping completion beyond one call per host core): every
+    match -- direct runs, captures and replays of both graphs -- equals the oracle."""
     import fasterstereocuda_b200 as fsc
     from concurrent.futures import ThreadPoolExecutor
     O = oracle_mod
@@ -335,7 +336,7 @@ def test_host_api_kernel_modes_under_concurrency(engine_lib, oracle_mod):
                      p1=10, p2=150, peaks_strips=STRIPS)
     refs = [O.pyr_match(pc, L, R) for L, R in pairs]
     ms = []
-    for _ in range(6):
+    for _ in range(12):
         p = fsc.FasterStereoCuda()
         assert p.Init(fsc.StereoOption1(width=W, height=H, min_disp=0, max_disp=64, num_layers=2, do_lr_check=True,
                                         do_rm_peaks=True), fsc.LevelOverride(1, 10, 150),
@@ -351,8 +352,8 @@ def test_host_api_kernel_modes_under_concurrency(engine_lib, oracle_mod):
             out.append((i, disp))
         return out
     results = work(0, 4)  # one caller: latency kernels
-    with ThreadPoolExecutor(max_workers=6) as ex:
-        for r in ex.map(lambda k: work(k, 6), range(6)):
+    with ThreadPoolExecutor(max_workers=12) as ex:
+        for r in ex.map(lambda k: work(k, 6), range(12)):
             results += r
     results += work(1, 3)  # alone again: the latency graph of a matcher that ran both
     for i, disp in results:
