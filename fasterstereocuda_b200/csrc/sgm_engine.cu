@@ -220,8 +220,7 @@ struct sgm_engine {
   cudaGraphExec_t gexec[2] = {};
   int direct_runs[2] = {};
   int64_t graph_launches[2] = {};
-  // events of the synchronous host API: `done` blocking-sync, `done_poll` polled (see wait_stream)
-  cudaEvent_t done = nullptr, done_poll = nullptr;
+  cudaEvent_t done = nullptr;  // blocking-sync event of the synchronous host API (see wait_stream)
   // Stages of a match: an NVTX range each, and with print_log a CUDA event at every stage boundary
   // for the per-stage report of the synchronous host API.
   static constexpr int kMaxStages = 10;
@@ -250,8 +249,7 @@ struct sgm_engine {
   void free_all() {
     drop_graph();
     if (done) cudaEventDestroy(done);
-    if (done_poll) cudaEventDestroy(done_poll);
-    done = done_poll = nullptr;
+    done = nullptr;
     for (auto& ev : stage_ev) {
       if (ev) cudaEventDestroy(ev);
       ev = nullptr;
@@ -283,24 +281,22 @@ struct sgm_engine {
 
 namespace {
 
-// Waits for everything enqueued on s so far. poll = false: on a blocking-sync event, without
-// spinning a CPU core -- callers that run many matchers from many host threads keep their cores
-// for the other threads. poll = true: by polling an ordinary event, which returns as soon as the
-// work is done instead of after the sleeping thread is woken (about 0.2 ms per call for one caller
-// matching 1242x375 frames from page-locked buffers, whose copies do not block the thread).
-// `ev` / `ev_poll` are the matcher's own events, created on first use.
-cudaError_t wait_stream(cudaStream_t s, cudaEvent_t* ev, cudaEvent_t* ev_poll, bool poll) {
-  cudaEvent_t* e = poll ? ev_poll : ev;
-  if (!*e) {
-    const unsigned flags = poll ? cudaEventDisableTiming : cudaEventBlockingSync | cudaEventDisableTiming;
-    const cudaError_t st = cudaEventCreateWithFlags(e, flags);
+// Waits for everything enqueued on s so far, on a blocking-sync event: a thread that has to wait
+// sleeps and leaves its core to the other threads (many matchers on many host threads). While
+// keep_polling() (non-null) holds, the event is polled instead: that returns as soon as the work
+// is done rather than when the sleeping thread is woken, about 0.2 ms sooner per call for one
+// caller matching 1242x375 frames from page-locked buffers (whose copies do not block the thread).
+// `ev` is the matcher's own event, created on first use on its device.
+cudaError_t wait_stream(cudaStream_t s, cudaEvent_t* ev, bool (*keep_polling)() = nullptr) {
+  if (!*ev) {
+    const cudaError_t st = cudaEventCreateWithFlags(ev, cudaEventBlockingSync | cudaEventDisableTiming);
     if (st != cudaSuccess) return st;
   }
-  cudaError_t st = cudaEventRecord(*e, s);
-  if (st != cudaSuccess || !poll) return st != cudaSuccess ? st : cudaEventSynchronize(*e);
-  while ((st = cudaEventQuery(*e)) == cudaErrorNotReady) {
-  }
-  return st;
+  cudaError_t st = cudaEventRecord(*ev, s);
+  if (st != cudaSuccess) return st;
+  while (keep_polling && keep_polling())
+    if ((st = cudaEventQuery(*ev)) != cudaErrorNotReady) return st;
+  return cudaEventSynchronize(*ev);
 }
 
 // Starts stage `name` of the match being enqueued (ends the previous one); name == nullptr ends
@@ -1273,22 +1269,19 @@ int engine_run(sgm_engine* e, const uint8_t* dl, const uint8_t* dr, float* dout,
 }
 
 // The synchronous host API (the reference's Match) adapts to the number of such calls in flight in
-// the process when the call starts (measured with page-locked buffers at 1242x375x64 on one B200):
-//  * kernels, on a matcher left at the default tuning: up to kLatencyInFlight calls take the
-//    warp-per-scanline kernels (variant 4, the shortest step chains: a pyramid pair 0.33 instead of
-//    1.46 ms alone), more take the default thread-per-scanline kernels, which give more pairs per
-//    second once many pairs share the GPU (16 callers: 7.4 k plain pairs/s against 6.0 k). Both
-//    give the same bits;
-//  * completion: up to one call per host core polls its completion event, more sleep on a
-//    blocking-sync event and leave the cores to the other callers (one caller: 3.3 k plain pairs/s
-//    polling, 2.0 k sleeping; 32 callers on 16 cores: 6.9 k pyramid pairs/s sleeping, 5.8 k polling).
+// the process (measured with page-locked buffers at 1242x375x64 on one B200, 16 host cores). While
+// at most kLatencyInFlight calls are in flight -- a few callers matching one frame at a time --
+//  * a matcher left at the default tuning takes the warp-per-scanline kernels (variant 4, the
+//    shortest step chains: a pyramid pair 0.33 instead of 1.46 ms alone); with more calls in flight
+//    the default thread-per-scanline kernels, which give more pairs per second once many pairs
+//    share the GPU (16 callers: 7.4 k plain pairs/s against 6.0 k). Both give the same bits;
+//  * the call polls for its results (one caller: 3.3 k plain pairs/s against 2.0 k sleeping),
+//    until more calls are in flight; then it sleeps, and the cores go to the callers that submit
+//    work (96 callers: 10.9 k pyramid pairs/s, 10.2 k when up to 16 of them poll).
 constexpr int kLatencyInFlight = 8;
 std::atomic<int> g_host_in_flight{0};
 
-int poll_in_flight() {
-  static const int n = std::max(1, (int)std::thread::hardware_concurrency());
-  return n;
-}
+bool few_host_calls() { return g_host_in_flight.load(std::memory_order_relaxed) <= kLatencyInFlight; }
 
 struct HostCall {
   int n;
@@ -1297,7 +1290,7 @@ struct HostCall {
   HostCall(const HostCall&) = delete;
   HostCall& operator=(const HostCall&) = delete;
   bool latency() const { return n <= kLatencyInFlight; }
-  bool poll() const { return n <= poll_in_flight(); }
+  bool (*poll() const)() { return latency() ? few_host_calls : nullptr; }
 };
 
 // Row and column kernels set to variant 4 on the given engines for the scope of one match, when
@@ -1353,8 +1346,7 @@ struct sgm_pyramid {
   cudaGraphExec_t gexec[2] = {};
   int direct_runs[2] = {};
   int64_t graph_launches[2] = {};  // kernels inside the graph
-  // events of the synchronous host API: `done` blocking-sync, `done_poll` polled (see wait_stream)
-  cudaEvent_t done = nullptr, done_poll = nullptr;
+  cudaEvent_t done = nullptr;  // blocking-sync event of the synchronous host API (see wait_stream)
 
   void drop_graph() {
     for (int k = 0; k < 2; ++k) {
@@ -1367,8 +1359,7 @@ struct sgm_pyramid {
   void free_all() {
     drop_graph();
     if (done) cudaEventDestroy(done);
-    if (done_poll) cudaEventDestroy(done_poll);
-    done = done_poll = nullptr;
+    done = nullptr;
     if (disp0) sgm_dev_free(disp0);
     disp0 = nullptr;
     depth_mode = false;
@@ -1616,7 +1607,7 @@ int sgm_match(sgm_handle_t h, const uint8_t* img_left, const uint8_t* img_right,
   if (disp_right && h->opt.do_lr_check)
     SGM_CUDA_TRY(h, cudaMemcpyAsync(disp_right, h->dr_out, N * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
   if (h->stage_timing) stage_mark(h, nullptr);
-  SGM_CUDA_TRY(h, wait_stream(h->stream, &h->done, &h->done_poll, call.poll()));
+  SGM_CUDA_TRY(h, wait_stream(h->stream, &h->done, call.poll()));
   if (disp_right && !h->opt.do_lr_check)
     for (size_t i = 0; i < N; ++i) disp_right[i] = sgm::kInvalidFloat;
   if (h->stage_timing) {
@@ -1682,7 +1673,7 @@ int sgm_match2(sgm_handle_t h, const uint8_t* img_left, const uint8_t* img_right
   if (!st) st = enqueue_depth(h, h->depth_src, h->post, h->cam, h->stream);
   if (st) return st;
   SGM_CUDA_TRY(h, cudaMemcpyAsync(depth_left, h->post, N * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
-  SGM_CUDA_TRY(h, wait_stream(h->stream, &h->done, &h->done_poll, call.poll()));
+  SGM_CUDA_TRY(h, wait_stream(h->stream, &h->done, call.poll()));
   return SGM_OK;
 }
 
@@ -1928,7 +1919,7 @@ int sgm_pyr_match(sgm_pyr_handle_t h, const uint8_t* img_left, const uint8_t* im
   int st = pyr_run(h, h->in_l, h->in_r, h->out, h->stream, km.mode());
   if (st) return st;
   if (cudaMemcpyAsync(disp, h->out, N * sizeof(float), cudaMemcpyDeviceToHost, h->stream)) return SGM_ERR_CUDA;
-  if (wait_stream(h->stream, &h->done, &h->done_poll, call.poll()) != cudaSuccess) {
+  if (wait_stream(h->stream, &h->done, call.poll()) != cudaSuccess) {
     set_error(&h->err, "pyramid match failed: %s", cudaGetErrorString(cudaGetLastError()));
     return SGM_ERR_CUDA;
   }
