@@ -99,8 +99,8 @@ SGM_API int sgm_get_ext_options(sgm_handle_t h, sgm_ext_options_t* ext);
  * the defaults runs, in the synchronous host API (sgm_match, sgm_match2, sgm_pyr_match,
  * sgm_pyr_match2), row_kernel = col_kernel = 4 while at most eight such calls are in flight in
  * the process (a few callers matching one frame at a time) and the defaults below otherwise.
- * Those calls wait for their results by polling while at most one call per host core is in
- * flight, and sleep on a blocking-sync event beyond that. */
+ * While at most eight calls are in flight they also wait for their results by polling; beyond
+ * that they sleep on a blocking-sync event. */
 typedef struct sgm_tuning_t {
   int32_t row_kernel;   /* horizontal scans: 1 = whole census rows in shared memory,
                            2 = census window and 32-pixel cost chunks in shared memory,

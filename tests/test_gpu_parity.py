@@ -324,9 +324,9 @@ def test_pyramid_parity(engine_lib, oracle_mod, override, size, layers, kernels)
 
 def test_host_api_kernel_modes_under_concurrency(engine_lib, oracle_mod):
     """Default-tuned matchers called through the synchronous host API by one thread (the latency
-    kernels, polled completion) and by twelve threads at once (the throughput kernels while more
-    than eight calls are in flight; sleeping completion beyond one call per host core): every
-    match -- direct runs, captures and replays of both graphs -- equals the oracle."""
+    kernels, polled completion) and by twelve threads at once (the throughput kernels and a
+    sleeping wait while more than eight calls are in flight): every match -- direct runs, captures
+    and replays of both graphs -- equals the oracle."""
     import fasterstereocuda_b200 as fsc
     from concurrent.futures import ThreadPoolExecutor
     O = oracle_mod
