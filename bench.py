@@ -172,12 +172,15 @@ def alg_bytes(kernel, W, H, D, nviews, census_bytes):
 # DRAM bytes per voxel (W*H*D*views of the launch) measured by ncu (dram__bytes_read.sum +
 # dram__bytes_write.sum) at 1242x375x64, one pair per launch: the plain kernels on the
 # single-level workload, the 32-disparity kernels on the pyramid's finest level; per kernel
-# family: "v3" the thread-per-scanline kernels, "v4" the warp-per-scanline kernels.
+# family: "v3" the thread-per-scanline kernels, "v4" the warp-per-scanline kernels; "batch" the
+# batched pyramid's persistent kernels as its graph runs them, 32 pairs per launch, over the
+# launches at both 32-disparity levels (1242x375 and 621x187).
 NCU_DRAM_BYTES_PER_VOXEL = {
     "v3": {"hpaths_plain": 2.83, "vpaths_bt_plain": 1.25, "vpaths_wta_plain": 4.04, "hpaths_init": 1.07,
            "vpaths_wta_init": 3.29},
     "v4": {"hpaths_plain": 2.76, "vpaths_bt_plain": 1.22, "vpaths_wta_plain": 4.04, "hpaths_init": 1.07,
            "vpaths_bt_init": 1.06, "vpaths_tb_init": 1.06, "wta_init": 3.42},
+    "batch": {"hpaths_init": 3.90, "vpaths_bt_init": 1.80, "vpaths_wta_init": 4.43},
 }
 
 
@@ -409,6 +412,16 @@ def run_ours(a, rank, world, local_rank):
         run_one(matchers[0], dL[0], dR[0], ref, main.cuda_stream)
         torch.cuda.synchronize()
         same = torch.equal(_read_dev(b.buffers(0)[2], H_, W_).view(torch.int32), ref.view(torch.int32))
+        # per-kernel CUDA events of two more runs of the same batch on the same stream, its kernels
+        # enqueued one after another instead of as the graph (no side branches), so that each
+        # launch's duration is its own; the roofline of this mode's dominant kernel comes from here
+        fsc.profile_enable(True)
+        for _ in range(2):
+            if not b.run(gs.cuda_stream):
+                raise RuntimeError(f"batch run failed: {b.last_error()}")
+        torch.cuda.synchronize()
+        gprof = fsc.profile_read()
+        fsc.profile_enable(False)
         info = b.info()
         del b
         torch.cuda.synchronize()
@@ -419,7 +432,7 @@ def run_ours(a, rank, world, local_rank):
                 "gpu_launches": info["kernels_per_run"] * a.steps, "kernels_per_graph": info["kernels_per_run"],
                 "arena_gib": info["arena_bytes"] / 2**30, "bit_exact_vs_per_pair": bool(same),
                 "l2": f"inputs larger than L2: {n} pairs ({inputs / 2**20:.0f} MiB of distinct input buffers)",
-                "clocks": gclk.summary()}
+                "clocks": gclk.summary(), "profile": {"runs": 2, "pairs_per_run": n, "kernels": gprof}}
 
     # parity: first output vs the oracle (outside every timed region)
     bit_exact = None
@@ -570,7 +583,6 @@ def run_ours(a, rank, world, local_rank):
     if rank != 0:
         return 0
     hbm_peak, peak_kind = peaks()
-    # per-kernel algorithmic bytes over the profiled pass
     # (kind, w, h, D, views) of each level a pair goes through
     levels = []
     if a.workload == "pyramid":
@@ -579,36 +591,49 @@ def run_ours(a, rank, world, local_rank):
             levels.append(("plain", w, h, d, 2) if lv == LAYERS - 1 else ("init", w, h, d, 1))
     else:
         levels.append(("plain", W_, H_, DMAX, 2))
-    per_call_bytes, per_call_voxels = {}, {}
-    for k in prof:
-        mine = [(w, h, d, nv) for (kind, w, h, d, nv) in levels
-                if not k.startswith(("hpaths", "vpaths", "wta")) or k.endswith(kind)]
-        per_call_bytes[k] = sum(alg_bytes(k, w, h, d, nv, 8) for (w, h, d, nv) in mine)
-        per_call_voxels[k] = sum(w * h * d * nv for (w, h, d, nv) in mine)
-    # the dominant kernel among those with a counterpart in the minimal design (the bottom-to-top
-    # pass launched on its own has none)
-    cand = [k for k in prof if per_call_bytes.get(k, 0) > 0]
-    dom = max(cand, key=lambda k: prof[k]["ms"]) if cand else None
-    calls = a.profile_pairs
+
+    def roofline_of(kprof, pairs, family, timing):
+        """Roofline of the dominant kernel of a profiled pass over `pairs` pairs: its algorithmic
+        bytes (per pair, over every level it runs at, x pairs) over its summed launch durations.
+        The dominant kernel is taken among those with a counterpart in the minimal design (the
+        bottom-to-top pass launched on its own has none); family(kernel) names the row of
+        NCU_DRAM_BYTES_PER_VOXEL that gives its measured traffic."""
+        pb, pv = {}, {}
+        for k in kprof:
+            mine = [(w, h, d, nv) for (kind, w, h, d, nv) in levels
+                    if not k.startswith(("hpaths", "vpaths", "wta")) or k.endswith(kind)]
+            pb[k] = sum(alg_bytes(k, w, h, d, nv, 8) for (w, h, d, nv) in mine)
+            pv[k] = sum(w * h * d * nv for (w, h, d, nv) in mine)
+        cand = [k for k in kprof if pb.get(k, 0) > 0 and kprof[k]["ms"] > 0]
+        if not cand:
+            return None
+        dom = max(cand, key=lambda k: kprof[k]["ms"])
+        total_ms, nl = kprof[dom]["ms"], max(1, kprof[dom]["launches"])
+        byts = pb[dom] * pairs
+        ach = byts / (total_ms / 1e3) / 1e9
+        bpv = NCU_DRAM_BYTES_PER_VOXEL[family(dom)].get(dom)
+        return {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
+                "frac": ach / hbm_peak, "traffic": bpv * pv[dom] * pairs / nl if bpv else None,
+                "peak_kind": peak_kind,
+                "traffic_source": "ncu DRAM bytes per voxel of this kernel x voxels per launch",
+                "kernel_family": family(dom), "avg_launch_us": total_ms / nl * 1e3,
+                "alg_bytes_per_launch": byts / nl, "timing": timing}
+
     # kernel family of the latency matcher's row / column scans
     lat_t = [int(v) for v in lat_tuning.split()[-1].split(",")] if lat_tuning else [0, 0, 0]
     fam = lambda k: "v4" if (lat_t[0] if k.startswith("hpaths") else lat_t[2]) == 4 else "v3"  # noqa: E731
-    roofline = None
-    if dom:
-        total_ms = prof[dom]["ms"]
-        byts = per_call_bytes.get(dom, 0) * calls
-        ach = byts / (total_ms / 1e3) / 1e9 if total_ms > 0 else 0.0
-        per_launch = max(1, prof[dom]["launches"] // calls)
-        bpv = NCU_DRAM_BYTES_PER_VOXEL[fam(dom)].get(dom)
-        traffic = bpv * per_call_voxels.get(dom, 0) / per_launch if bpv else None
-        roofline = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
-                    "frac": ach / hbm_peak, "traffic": traffic, "peak_kind": peak_kind,
-                    "traffic_source": "ncu DRAM bytes per voxel of this kernel x voxels per launch",
-                    "kernel_family": fam(dom),
-                    "avg_launch_us": total_ms / prof[dom]["launches"] * 1e3,
-                    "alg_bytes_per_launch": per_call_bytes.get(dom, 0) / max(1, prof[dom]["launches"] // calls),
-                    "timing": f"CUDA events around each launch, serialised pass of {calls} pairs on one stream "
-                              f"(the single-pair latency matcher)"}
+    calls = a.profile_pairs
+    roofline_single = roofline_of(prof, calls, fam,
+                                  f"CUDA events around each launch, serialised pass of {calls} pairs on one "
+                                  f"stream (the single-pair latency matcher)")
+    latency["roofline"] = roofline_single
+    roofline = roofline_single
+    if mode == "batched_graph":
+        gp = modes["batched_graph"]["profile"]
+        roofline = roofline_of(gp["kernels"], gp["runs"] * gp["pairs_per_run"], lambda k: "batch",
+                               f"CUDA events around each launch of {gp['runs']} runs of the timed batch "
+                               f"({gp['pairs_per_run']} pairs per launch), its kernels enqueued one after "
+                               f"another on the timed stream")
     if roofline is not None:
         # the path is integer-ALU bound: algorithmic int ops per view 34*W*H*D + 248*W*H (xor+popc,
         # 7 per path step x 4 paths, 3 adds, 1 min per voxel; census per pixel), over all levels,
@@ -623,9 +648,13 @@ def run_ours(a, rank, world, local_rank):
                            "frac_packed16x2": ops * value / world / (2 * peak),
                            "peak_kind": "nominal: 148 SMs x 128 INT32 lanes x median SM clock under load",
                            "per": "GPU"}
-    tot_ms = sum(x["ms"] for x in prof.values()) or 1.0
-    kernels = {k: {"launches": v["launches"], "avg_us": round(v["ms"] / max(1, v["launches"]) * 1e3, 2),
-                   "share": round(v["ms"] / tot_ms, 4)} for k, v in prof.items()}
+    def shares(kprof):
+        tot = sum(x["ms"] for x in kprof.values()) or 1.0
+        return {k: {"launches": v["launches"], "avg_us": round(v["ms"] / max(1, v["launches"]) * 1e3, 2),
+                    "share": round(v["ms"] / tot, 4)} for k, v in kprof.items()}
+    # per-kernel launches, average duration and share of the profiled pass of value's mode
+    latency["kernels"] = shares(prof)
+    kernels = shares(modes["batched_graph"]["profile"]["kernels"]) if mode == "batched_graph" else latency["kernels"]
 
     cpu = None
     extras = None

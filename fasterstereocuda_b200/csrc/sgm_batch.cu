@@ -36,12 +36,26 @@
 #include "sgm_levels.h"
 
 void sgm_set_process_error(const char* msg);
+// Per-launch profiler of the engine (sgm_profile_enable): while it is on, a run enqueues its
+// kernels directly on the caller's stream, one after another, each timed alone.
+bool sgm_prof_on();
+void sgm_prof_start(cudaStream_t s);
+void sgm_prof_end(const char* name);
 
 namespace {
 
 using namespace sgm::batch;
 
 size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
+
+// Runs fn, which enqueues one kernel on s; with prof, between the profiler's two events.
+template <typename F>
+int timed(bool prof, cudaStream_t s, const char* name, F&& fn) {
+  if (prof) sgm_prof_start(s);
+  const int r = fn();
+  if (prof) sgm_prof_end(name);
+  return r;
+}
 
 int width_class(int W) { return W <= 640 ? 0 : (W <= 1280 ? 1 : 2); }
 
@@ -73,7 +87,7 @@ struct sgm_batch {
   int* dtab = nullptr;  // all int tables
   int* queues = nullptr;
   int nqueues = 0;
-  int census_prefix = 0, tile_prefix = 0;  // offsets into dtab
+  int census_prefix = 0, tile_prefix = 0;  // offsets into dtab (tile: LR/median tiles, 32 x kLrmRows)
   int census_items = 0, tile_items = 0;
   struct Bucket {
     int K = 2, wclass = 0;
@@ -451,6 +465,31 @@ int autotune(sgm_batch* b, bool force) {
   return SGM_OK;
 }
 
+// bucket_scans with every launch on s in a valid order, each timed alone (the profiled run).
+int bucket_scans_timed(sgm_batch* b, sgm_batch::Bucket& k, cudaStream_t s, int* q) {
+  int r = SGM_OK;
+  if (k.tune.rows_lanes) r = timed(true, s, "cost", [&] { return launch_cost(b, k, s); });
+  if (k.tune.cols_lanes == 0 || k.tune.rows_lanes == 0) {
+    if (!r) r = timed(true, s, "hpaths_plain", [&] { return rows(b, k, s, q, false); });
+    if (!r) r = timed(true, s, "vpaths_wta_plain", [&] { return launch_cols(b, k, s, q + 1); });
+    return r;
+  }
+  if (!r) r = timed(true, s, "vpaths_bt_plain", [&] { return cols<1>(b, k, s, q + 1, false); });
+  if (!r) r = timed(true, s, "hpaths_plain", [&] { return rows(b, k, s, q, false); });
+  if (!r) r = timed(true, s, "vpaths_wta_plain", [&] { return cols<2>(b, k, s, q + 2, false); });
+  return r;
+}
+
+// The graph's work enqueued directly on s, one launch after another, each timed alone.
+int run_timed(sgm_batch* b, cudaStream_t s) {
+  if (cudaMemsetAsync(b->queues, 0, b->nqueues * sizeof(int), s) != cudaSuccess)
+    return berr(b, SGM_ERR_CUDA, "queue reset failed");
+  int st = timed(true, s, "census", [&] { return launch_census(b, s); });
+  for (size_t i = 0; !st && i < b->buckets.size(); ++i) st = bucket_scans_timed(b, b->buckets[i], s, b->queues + 3 * i);
+  if (!st) st = timed(true, s, "lr_median", [&] { return launch_post(b, s); });
+  return st;
+}
+
 // Captures census -> per-bucket [rows -> cols] branches -> LR/median into one graph.
 int capture(sgm_batch* b) {
   if (b->exec) cudaGraphExecDestroy(b->exec);
@@ -599,7 +638,9 @@ static int batch_init_impl(sgm_batch_t b, const sgm_batch_pair_t* pairs, int32_t
   for (int i = 0; i < count; ++i) all[i] = i;
   auto cp = prefix_of(all, [&](int i) { return 2 * ((pairs[i].height + sgm::kCensusRows - 1) / sgm::kCensusRows); });
   b->census_prefix = cp.first; b->census_items = cp.second;
-  auto tp = prefix_of(all, [&](int i) { return ((pairs[i].width + 31) / 32) * ((pairs[i].height + 7) / 8); });
+  auto tp = prefix_of(all, [&](int i) {  // LR/median tiles
+    return ((pairs[i].width + 31) / 32) * ((pairs[i].height + kLrmRows - 1) / kLrmRows);
+  });
   b->tile_prefix = tp.first; b->tile_items = tp.second;
   for (auto& g : groups) {
     sgm_batch::Bucket k;
@@ -690,6 +731,11 @@ int sgm_batch_pair_buffers(sgm_batch_t b, int32_t index, uint8_t** d_left, uint8
 int sgm_batch_run(sgm_batch_t b, void* stream) {
   if (!b || !b->ready) return b ? berr(b, SGM_ERR_STATE, "batch not initialised") : SGM_ERR_ARG;
   cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : b->stream;
+  if (sgm_prof_on()) {  // per-launch timing: the same work without the graph, one launch at a time
+    const int st = run_timed(b, s);
+    if (!st) b->runs++;
+    return st;
+  }
   const cudaError_t ce = cudaGraphLaunch(b->exec, s);
   if (ce != cudaSuccess) return berr(b, SGM_ERR_CUDA, "graph launch failed: %s", cudaGetErrorString(ce));
   b->runs++;
@@ -771,6 +817,7 @@ struct sgm_batch_pyr {
     BatchPair* ddesc = nullptr;
     int census_prefix = 0, census_items = 0, tile_prefix = 0, tile_items = 0;
     int row_prefix = 0, row_items = 0, pix_prefix = 0, pix_items = 0;
+    int lrm_prefix = 0, lrm_items = 0;  // LR/median tiles (32 x kLrmRows)
     std::vector<Bucket> buckets;
     int queue0 = 0;
   };
@@ -922,24 +969,28 @@ int level_post(sgm_batch_pyr* p, const BatchPair* d, const int* tpre, int tiles,
   return SGM_OK;
 }
 
-// Dilation and small-region removal of one level, when its options ask for them.
+// Dilation and small-region removal of one level, when its options ask for them (prof: each
+// launch timed alone).
 int level_filters(sgm_batch_pyr* p, const BatchPair* d, const sgm_option_t& o, int tpre, int tiles, int rpre, int rows,
-                  int ppre, int pix, int n, cudaStream_t s, int64_t* kernels) {
-  if (o.post_filter_type == 1) {  // the LR/median stage wrote `post`
-    kb_gauss<<<tiles, dim3(32, 8), 0, s>>>(d, p->dtab + tpre, n);
+                  int ppre, int pix, int n, cudaStream_t s, int64_t* kernels, bool prof = false) {
+  auto T = [&](const char* name, auto launch) {
+    timed(prof, s, name, [&] {
+      launch();
+      return SGM_OK;
+    });
     (*kernels)++;
-  }
-  if (o.morphology_type == 2) {
-    kb_dilation<<<tiles, dim3(32, 8), 0, s>>>(d, p->dtab + tpre, n);
-    (*kernels)++;
-  }
+  };
+  if (o.post_filter_type == 1)  // the LR/median stage wrote `post`
+    T("gauss", [&] { kb_gauss<<<tiles, dim3(32, 8), 0, s>>>(d, p->dtab + tpre, n); });
+  if (o.morphology_type == 2)
+    T("dilation", [&] { kb_dilation<<<tiles, dim3(32, 8), 0, s>>>(d, p->dtab + tpre, n); });
   if (o.do_remove_peaks) {
     const int am = p->ext.peaks_abs_mode;
-    kb_cc_rows<<<(rows + 7) / 8, dim3(32, 8), 0, s>>>(d, p->dtab + rpre, n, am);
-    kb_cc_vert<<<(pix + 255) / 256, 256, 0, s>>>(d, p->dtab + ppre, n, am);
-    kb_cc_count<<<(pix + 255) / 256, 256, 0, s>>>(d, p->dtab + ppre, n);
-    kb_cc_filter<<<(pix + 255) / 256, 256, 0, s>>>(d, p->dtab + ppre, n, o.peaks_ratio_threshold);
-    (*kernels) += 4;
+    T("cc_rows", [&] { kb_cc_rows<<<(rows + 7) / 8, dim3(32, 8), 0, s>>>(d, p->dtab + rpre, n, am); });
+    T("cc_vert", [&] { kb_cc_vert<<<(pix + 255) / 256, 256, 0, s>>>(d, p->dtab + ppre, n, am); });
+    T("cc_count", [&] { kb_cc_count<<<(pix + 255) / 256, 256, 0, s>>>(d, p->dtab + ppre, n); });
+    T("cc_filter",
+      [&] { kb_cc_filter<<<(pix + 255) / 256, 256, 0, s>>>(d, p->dtab + ppre, n, o.peaks_ratio_threshold); });
   }
   PTRY(p, cudaGetLastError());
   return SGM_OK;
@@ -1076,7 +1127,7 @@ int pyr_capture(sgm_batch_pyr* p) {
   for (int lvl = Lc - 1; lvl >= 0 && !st; --lvl) {
     PLevel& L = p->lv[lvl];
     const BatchPair* above = lvl == Lc - 1 ? c->ddesc : p->lv[lvl + 1].ddesc;
-    kb_init_next<<<(L.pix_items + 255) / 256, 256, 0, s>>>(L.ddesc, above, p->dtab + L.pix_prefix, n);
+    kb_init_next<<<(L.row_items + 7) / 8, dim3(32, 8), 0, s>>>(L.ddesc, above, p->dtab + L.row_prefix, n);
     kernels++;
     if (cudaGetLastError() != cudaSuccess) st = perr(p, SGM_ERR_CUDA, "initial-disparity launch failed");
     if (!st) { st = level_census(p, L.ddesc, L.census_prefix, L.census_items, n, s); kernels++; }
@@ -1096,7 +1147,7 @@ int pyr_capture(sgm_batch_pyr* p) {
         kernels += 4;
         return r;
       });
-    if (!st) { st = level_post(p, L.ddesc, p->dtab + L.tile_prefix, L.tile_items, n, L.opt, s); kernels++; }
+    if (!st) { st = level_post(p, L.ddesc, p->dtab + L.lrm_prefix, L.lrm_items, n, L.opt, s); kernels++; }
     if (!st)
       st = level_filters(p, L.ddesc, L.opt, L.tile_prefix, L.tile_items, L.row_prefix, L.row_items, L.pix_prefix,
                          L.pix_items, n, s, &kernels);
@@ -1112,6 +1163,57 @@ int pyr_capture(sgm_batch_pyr* p) {
   PTRY(p, cudaGraphInstantiate(&p->exec, g, 0));
   p->graph_kernels = kernels;
   return SGM_OK;
+}
+
+// pyr_capture's work enqueued directly on s, one launch after another in a valid order (the
+// column passes and the row scans of a bucket in sequence), each timed alone.
+int pyr_run_timed(sgm_batch_pyr* p, cudaStream_t s) {
+  sgm_batch* c = p->coarse;
+  const int n = (int)p->pairs.size();
+  const int Lc = p->layers - 1;
+  if (cudaMemsetAsync(c->queues, 0, c->nqueues * sizeof(int), s) != cudaSuccess ||
+      (p->nqueues && cudaMemsetAsync(p->queues, 0, p->nqueues * sizeof(int), s) != cudaSuccess))
+    return perr(p, SGM_ERR_CUDA, "queue reset failed");
+  int st = SGM_OK;
+  int64_t kernels = 0;
+  for (int lvl = 1; lvl < p->layers && !st; ++lvl) {
+    const BatchPair* dst = lvl == Lc ? c->ddesc : p->lv[lvl].ddesc;
+    st = timed(true, s, "decimate", [&] {
+      kb_decimate<<<p->dec_items[lvl], 128, 0, s>>>(dst, p->lv[0].ddesc, p->dtab + p->dec_prefix[lvl], n, lvl);
+      return cudaGetLastError() == cudaSuccess ? SGM_OK : perr(p, SGM_ERR_CUDA, "decimation launch failed");
+    });
+  }
+  if (!st) st = timed(true, s, "census", [&] { return launch_census(c, s); });
+  for (size_t i = 0; !st && i < c->buckets.size(); ++i) st = bucket_scans_timed(c, c->buckets[i], s, c->queues + 3 * i);
+  if (!st) st = timed(true, s, "lr_median", [&] { return launch_post(c, s); });
+  if (!st)
+    st = level_filters(p, c->ddesc, p->copt, p->c_tile_prefix, p->c_tile_items, p->c_row_prefix, p->c_row_items,
+                       p->c_pix_prefix, p->c_pix_items, n, s, &kernels, true);
+  for (int lvl = Lc - 1; lvl >= 0 && !st; --lvl) {
+    PLevel& L = p->lv[lvl];
+    const BatchPair* above = lvl == Lc - 1 ? c->ddesc : p->lv[lvl + 1].ddesc;
+    st = timed(true, s, "init_next_level", [&] {
+      kb_init_next<<<(L.row_items + 7) / 8, dim3(32, 8), 0, s>>>(L.ddesc, above, p->dtab + L.row_prefix, n);
+      return cudaGetLastError() == cudaSuccess ? SGM_OK : perr(p, SGM_ERR_CUDA, "initial-disparity launch failed");
+    });
+    if (!st)
+      st = timed(true, s, "census", [&] { return level_census(p, L.ddesc, L.census_prefix, L.census_items, n, s); });
+    for (size_t i = 0; !st && i < L.buckets.size(); ++i) {
+      PBucket& k = L.buckets[i];
+      int* q = p->queues + L.queue0 + 3 * i;
+      st = timed(true, s, "cost", [&] { return init_cost(p, L, k, s); });
+      if (!st) st = timed(true, s, "vpaths_bt_init", [&] { return init_cols<1>(p, L, k, s, q + 1, false); });
+      if (!st) st = timed(true, s, "hpaths_init", [&] { return init_rows(p, L, k, s, q, false); });
+      if (!st) st = timed(true, s, "vpaths_wta_init", [&] { return init_cols<2>(p, L, k, s, q + 2, false); });
+    }
+    if (!st)
+      st = timed(true, s, "lr_median",
+                 [&] { return level_post(p, L.ddesc, p->dtab + L.lrm_prefix, L.lrm_items, n, L.opt, s); });
+    if (!st)
+      st = level_filters(p, L.ddesc, L.opt, L.tile_prefix, L.tile_items, L.row_prefix, L.row_items, L.pix_prefix,
+                         L.pix_items, n, s, &kernels, true);
+  }
+  return st;
 }
 
 }  // namespace
@@ -1326,6 +1428,10 @@ static int batch_pyr_init_impl(sgm_batch_pyr_t p, const sgm_batch_pair_t* pairs,
     L.census_prefix = c.first; L.census_items = c.second;
     auto t = prefix_of(all, [&](int i) { return tiles_of(hw(i).first, hw(i).second); });
     L.tile_prefix = t.first; L.tile_items = t.second;
+    auto lt = prefix_of(all, [&](int i) {
+      return ((hw(i).first + 31) / 32) * ((hw(i).second + kLrmRows - 1) / kLrmRows);
+    });
+    L.lrm_prefix = lt.first; L.lrm_items = lt.second;
     auto r = prefix_of(all, [&](int i) { return hw(i).second; });
     L.row_prefix = r.first; L.row_items = r.second;
     auto x = prefix_of(all, [&](int i) { return hw(i).first * hw(i).second; });
@@ -1417,6 +1523,7 @@ int sgm_batch_pyr_pair_buffers(sgm_batch_pyr_t p, int32_t index, uint8_t** d_lef
 int sgm_batch_pyr_run(sgm_batch_pyr_t p, void* stream) {
   if (!p || !p->ready) return p ? perr(p, SGM_ERR_STATE, "batch not initialised") : SGM_ERR_ARG;
   cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : p->stream;
+  if (sgm_prof_on()) return pyr_run_timed(p, s);  // per-launch timing: the same work without the graph
   const cudaError_t ce = cudaGraphLaunch(p->exec, s);
   if (ce != cudaSuccess) return perr(p, SGM_ERR_CUDA, "graph launch failed: %s", cudaGetErrorString(ce));
   return SGM_OK;

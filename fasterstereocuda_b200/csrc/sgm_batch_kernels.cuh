@@ -183,19 +183,58 @@ __global__ void __launch_bounds__(256) kb_cols3(const BatchPair* __restrict__ pa
   }
 }
 
+// LR check + 3x3 median over tiles of 32 x kLrmRows pixels (one block of 32 x 8 threads, kLrmRows / 8
+// pixels per thread): the per-pixel values of sgm::lr_median_tile (a pure function of the
+// pixel's neighbourhood), with the tile's loads issued together and the pair lookup made once per
+// kLrmRows / 8 tiles of 32 x 8. item = (pair, tile) in row-major tile order.
+constexpr int kLrmRows = 32;
 template <bool LR, bool MED>
 __global__ void __launch_bounds__(256) kb_lr_median(const BatchPair* __restrict__ pairs,
                                                     const int* __restrict__ prefix, int n, float thr) {
-  __shared__ float tile[10][34];
+  constexpr int TR = kLrmRows + 2, NR = kLrmRows / 8;
+  __shared__ float tile[TR][34];
   const int item = blockIdx.x;
   const int b = find_pair(prefix, n, item);
-  const BatchPair d = pairs[b];
+  const BatchPair& d = pairs[b];
   const int local = item - __ldg(prefix + b);
-  const int tiles_x = (d.P.W + 31) / 32;
-  const int ty = local / tiles_x;
-  const int tx = local - ty * tiles_x;
-  sgm::lr_median_tile<LR, MED>(d.wta, d.wta + d.Q.dstride, nullptr, d.post ? d.post : d.out, d.P.W, d.P.H, thr,
-                               tx * 32, ty * 8, tile);
+  const int W = d.P.W, H = d.P.H;
+  const float* __restrict__ dl = d.wta;
+  const float* __restrict__ dr = d.wta + d.Q.dstride;
+  float* __restrict__ out = d.post ? d.post : d.out;
+  const int tiles_x = (W + 31) / 32;
+  const int tyi = local / tiles_x;
+  const int bx = (local - tyi * tiles_x) * 32, by = tyi * kLrmRows;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+#pragma unroll
+  for (int k = 0; k < (TR * 34 + 255) / 256; ++k) {
+    const int i = k * 256 + ty * 32 + tx;
+    if (i < TR * 34) {
+      const int ly = i / 34, lx = i - ly * 34;
+      const int gx = bx + lx - 1, gy = by + ly - 1;
+      float v = sgm::kInvalidFloat;
+      if (gx >= 0 && gx < W && gy >= 0 && gy < H) {
+        v = dl[(size_t)gy * W + gx];
+        if (LR) v = sgm::lr_value(v, gx, dr + (size_t)gy * W, nullptr, W, thr);
+      }
+      tile[ly][lx] = v;
+    }
+  }
+  __syncthreads();
+  const int x = bx + tx;
+  if (x >= W) return;
+  int ylim = 2 * ((W - 1) / 2);
+  ylim = ylim > H - 2 ? H - 2 : ylim;
+#pragma unroll
+  for (int r = 0; r < NR; ++r) {
+    const int ry = ty + 8 * r, y = by + ry;
+    if (y < H) {
+      float v = tile[ry + 1][tx + 1];
+      if (MED && x >= 1 && x <= W - 2 && y >= 1 && y <= ylim)
+        v = sgm::median9(tile[ry][tx], tile[ry][tx + 1], tile[ry][tx + 2], tile[ry + 1][tx], tile[ry + 1][tx + 1],
+                         tile[ry + 1][tx + 2], tile[ry + 2][tx], tile[ry + 2][tx + 1], tile[ry + 2][tx + 2]);
+      out[(size_t)y * W + x] = v;
+    }
+  }
 }
 
 // Deterministic noise for the autotuner's timing runs (overwritten by the caller's images).
@@ -289,18 +328,21 @@ static __global__ void __launch_bounds__(256) kb_cc_filter(const BatchPair* __re
   if (d.peaks_tiles > 0) sgm::cc_filter_px(d.out, d.label, d.count, d.P.W, d.peaks_tiles, ratio, i - __ldg(pprefix + b));
 }
 
-// Initial disparities of the finer level `next` from the coarser level's `out`.
+// Initial disparities of the finer level `next` from the coarser level's `out`: one warp per
+// (pair, row) item of rprefix (blocks of 32 x 8 threads), lanes along the row.
 static __global__ void __launch_bounds__(256) kb_init_next(const BatchPair* __restrict__ next,
                                                            const BatchPair* __restrict__ cur,
-                                                           const int* __restrict__ pprefix, int n) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= __ldg(pprefix + n)) return;
-  const int b = find_pair(pprefix, n, i);
-  const int local = i - __ldg(pprefix + b);
+                                                           const int* __restrict__ rprefix, int n) {
+  const int item = blockIdx.x * blockDim.y + threadIdx.y;
+  if (item >= __ldg(rprefix + n)) return;
+  const int b = find_pair(rprefix, n, item);
+  const int y = item - __ldg(rprefix + b);
   const int w = next[b].P.W, h = next[b].P.H;
-  const int y = local / w;
-  sgm::init_next_px(cur[b].out, (long)cur[b].P.W * cur[b].P.H, const_cast<int16_t*>(next[b].init), w, h, local - y * w,
-                    y);
+  const float* src = cur[b].out;
+  const long ncur = (long)cur[b].P.W * cur[b].P.H;
+  int16_t* dst = const_cast<int16_t*>(next[b].init);
+#pragma unroll 4
+  for (int x = threadIdx.x; x < w; x += 32) sgm::init_next_px(src, ncur, dst, w, h, x, y);
 }
 
 // Cost volume of a 32-disparity level: one block per (pair, view, row); `ids` gives the pair order.

@@ -134,6 +134,13 @@ int64_t g_alloc_fail_after = -1;  // < 0: never fail; else allocations left befo
 
 }  // namespace
 
+// The per-launch profiler as the batched engines (sgm_batch.cu) use it: with it on, a batch run
+// enqueues its kernels one after another on one stream, each between sgm_prof_start and
+// sgm_prof_end.
+bool sgm_prof_on() { return g_prof.on; }
+void sgm_prof_start(cudaStream_t s) { prof_start(s); }
+void sgm_prof_end(const char* name) { prof_end(name); }
+
 cudaError_t sgm_dev_malloc(void** p, size_t bytes) {
   {
     std::lock_guard<std::mutex> lk(g_alloc_mu);

@@ -205,7 +205,8 @@ SGM_API int64_t sgm_debug_live_device_allocations(void);
  * stream around every launch of every handle in the process. Enabling resets the counters. While
  * it is on, matches run their kernels directly (no graph) and one after another on their stream
  * (the column pass that otherwise overlaps the row scans on a second stream waits for them), so
- * that each launch is timed alone. */
+ * that each launch is timed alone; sgm_batch_run and sgm_batch_pyr_run likewise enqueue the
+ * batch's kernels on the given stream one at a time instead of launching its graph. */
 SGM_API int sgm_profile_enable(int32_t enable);
 /* Writes {"kernel": {"launches": n, "ms": total}, ...} into buf; returns 0, or the size needed
  * (including the terminating NUL) when cap is too small. Synchronises on the recorded events. */

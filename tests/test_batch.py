@@ -179,3 +179,62 @@ def test_batch_pyramid_equals_per_pair_pyramid(engine_lib, oracle_mod, layers, o
     else:
         assert np.array_equal(outs[1].view(np.uint32), ref.view(np.uint32))
     assert b.info()["pairs"] == len(PYR_PAIRS)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("pyramid", [True, False])
+def test_profiled_batch_run_equals_graph_run(engine_lib, pyramid):
+    """With the per-launch profiler on, a batch run enqueues its kernels one at a time on the
+    caller's stream instead of launching its graph: the same bits, and every kernel timed."""
+    import torch
+    import fasterstereocuda_b200 as fsc
+    if pyramid:
+        b = fsc.StereoBatchPyramid()
+        pairs = PYR_PAIRS
+        assert b.Init(pairs, fsc.StereoOption1(num_layers=3, do_lr_check=True, do_rm_peaks=True),
+                      fsc.LevelOverride(1, 10, 150), fsc.ExtOptions(peaks_strips=STRIPS)), b.last_error()
+        imgs = [scenes.kitti_like(520 + i, w, h)[:2] for i, (w, h, _, _) in enumerate(pairs)]
+    else:
+        b = fsc.StereoBatch()
+        pairs = SMALL
+        assert b.Init(pairs, option(fsc)), b.last_error()
+        imgs = _pairs(pairs, 470)
+    for i, (L, R) in enumerate(imgs):
+        tl, tr = torch.from_numpy(L).cuda(), torch.from_numpy(R).cuda()
+        dl, dr, _ = b.buffers(i)
+        _memcpy(dl, tl.data_ptr(), tl.numel())
+        _memcpy(dr, tr.data_ptr(), tr.numel())
+
+    def outputs():
+        res = []
+        for i, p in enumerate(pairs):
+            w, h = p[0], p[1]
+            got = torch.empty((h, w), dtype=torch.float32, device="cuda")
+            _memcpy(got.data_ptr(), b.buffers(i)[2], h * w * 4)
+            res.append(got.cpu().numpy())
+        return res
+
+    stream = torch.cuda.current_stream().cuda_stream
+    assert b.run(stream), b.last_error()
+    torch.cuda.synchronize()
+    want = outputs()
+    try:
+        fsc.profile_enable(True)
+        for i, p in enumerate(pairs):  # stale outputs must not pass
+            torch.cuda.synchronize()
+            fill = torch.full((p[1], p[0]), 3.0, dtype=torch.float32, device="cuda")
+            _memcpy(b.buffers(i)[2], fill.data_ptr(), p[0] * p[1] * 4)
+        assert b.run(stream), b.last_error()
+        torch.cuda.synchronize()
+        prof = fsc.profile_read()
+    finally:
+        fsc.profile_enable(False)
+    got = outputs()
+    for i in range(len(pairs)):
+        assert np.array_equal(got[i].view(np.uint32), want[i].view(np.uint32)), i
+    names = set(prof)
+    assert {"census", "lr_median"} <= names, names
+    assert any(k.startswith("hpaths") for k in names) and any(k.startswith("vpaths") for k in names), names
+    if pyramid:
+        assert {"decimate", "init_next_level", "hpaths_init", "vpaths_wta_init", "cc_rows"} <= names, names
+    assert all(v["launches"] >= 1 and v["ms"] > 0 for v in prof.values()), prof
