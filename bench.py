@@ -184,6 +184,37 @@ NCU_DRAM_BYTES_PER_VOXEL = {
 }
 
 
+def roofline_of(kprof, pairs, levels, family, hbm_peak, peak_kind, timing):
+    """Roofline of the dominant kernel of a profiled pass over `pairs` pairs.
+
+    kprof: {kernel: {"launches": n, "ms": total}} (sgm_profile_read); levels: (kind, w, h, D,
+    views) of each level a pair goes through. achieved = the kernel's algorithmic bytes (per pair,
+    over every level it runs at, x pairs) over its summed launch durations. The dominant kernel is
+    taken among those with a counterpart in the minimal design (the bottom-to-top pass launched on
+    its own has none); family(kernel) names the row of NCU_DRAM_BYTES_PER_VOXEL that gives its
+    measured traffic (bytes per voxel x voxels per launch)."""
+    pb, pv = {}, {}
+    for k in kprof:
+        mine = [(w, h, d, nv) for (kind, w, h, d, nv) in levels
+                if not k.startswith(("hpaths", "vpaths", "wta")) or k.endswith(kind)]
+        pb[k] = sum(alg_bytes(k, w, h, d, nv, 8) for (w, h, d, nv) in mine)
+        pv[k] = sum(w * h * d * nv for (w, h, d, nv) in mine)
+    cand = [k for k in kprof if pb.get(k, 0) > 0 and kprof[k]["ms"] > 0]
+    if not cand:
+        return None
+    dom = max(cand, key=lambda k: kprof[k]["ms"])
+    total_ms, nl = kprof[dom]["ms"], max(1, kprof[dom]["launches"])
+    byts = pb[dom] * pairs
+    ach = byts / (total_ms / 1e3) / 1e9
+    bpv = NCU_DRAM_BYTES_PER_VOXEL[family(dom)].get(dom)
+    return {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
+            "frac": ach / hbm_peak, "traffic": bpv * pv[dom] * pairs / nl if bpv else None,
+            "peak_kind": peak_kind,
+            "traffic_source": "ncu DRAM bytes per voxel of this kernel x voxels per launch",
+            "kernel_family": family(dom), "avg_launch_us": total_ms / nl * 1e3,
+            "alg_bytes_per_launch": byts / nl, "timing": timing}
+
+
 # ------------------------------------------------------------------------------------ reference arm
 def run_reference(a, rank, world):
     if rank != 0:
@@ -592,45 +623,19 @@ def run_ours(a, rank, world, local_rank):
     else:
         levels.append(("plain", W_, H_, DMAX, 2))
 
-    def roofline_of(kprof, pairs, family, timing):
-        """Roofline of the dominant kernel of a profiled pass over `pairs` pairs: its algorithmic
-        bytes (per pair, over every level it runs at, x pairs) over its summed launch durations.
-        The dominant kernel is taken among those with a counterpart in the minimal design (the
-        bottom-to-top pass launched on its own has none); family(kernel) names the row of
-        NCU_DRAM_BYTES_PER_VOXEL that gives its measured traffic."""
-        pb, pv = {}, {}
-        for k in kprof:
-            mine = [(w, h, d, nv) for (kind, w, h, d, nv) in levels
-                    if not k.startswith(("hpaths", "vpaths", "wta")) or k.endswith(kind)]
-            pb[k] = sum(alg_bytes(k, w, h, d, nv, 8) for (w, h, d, nv) in mine)
-            pv[k] = sum(w * h * d * nv for (w, h, d, nv) in mine)
-        cand = [k for k in kprof if pb.get(k, 0) > 0 and kprof[k]["ms"] > 0]
-        if not cand:
-            return None
-        dom = max(cand, key=lambda k: kprof[k]["ms"])
-        total_ms, nl = kprof[dom]["ms"], max(1, kprof[dom]["launches"])
-        byts = pb[dom] * pairs
-        ach = byts / (total_ms / 1e3) / 1e9
-        bpv = NCU_DRAM_BYTES_PER_VOXEL[family(dom)].get(dom)
-        return {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
-                "frac": ach / hbm_peak, "traffic": bpv * pv[dom] * pairs / nl if bpv else None,
-                "peak_kind": peak_kind,
-                "traffic_source": "ncu DRAM bytes per voxel of this kernel x voxels per launch",
-                "kernel_family": family(dom), "avg_launch_us": total_ms / nl * 1e3,
-                "alg_bytes_per_launch": byts / nl, "timing": timing}
-
     # kernel family of the latency matcher's row / column scans
     lat_t = [int(v) for v in lat_tuning.split()[-1].split(",")] if lat_tuning else [0, 0, 0]
     fam = lambda k: "v4" if (lat_t[0] if k.startswith("hpaths") else lat_t[2]) == 4 else "v3"  # noqa: E731
     calls = a.profile_pairs
-    roofline_single = roofline_of(prof, calls, fam,
+    roofline_single = roofline_of(prof, calls, levels, fam, hbm_peak, peak_kind,
                                   f"CUDA events around each launch, serialised pass of {calls} pairs on one "
                                   f"stream (the single-pair latency matcher)")
     latency["roofline"] = roofline_single
     roofline = roofline_single
     if mode == "batched_graph":
         gp = modes["batched_graph"]["profile"]
-        roofline = roofline_of(gp["kernels"], gp["runs"] * gp["pairs_per_run"], lambda k: "batch",
+        roofline = roofline_of(gp["kernels"], gp["runs"] * gp["pairs_per_run"], levels, lambda k: "batch",
+                               hbm_peak, peak_kind,
                                f"CUDA events around each launch of {gp['runs']} runs of the timed batch "
                                f"({gp['pairs_per_run']} pairs per launch), its kernels enqueued one after "
                                f"another on the timed stream")
